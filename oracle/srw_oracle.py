@@ -1,0 +1,1025 @@
+"""FP64 CPU restatement of SRW's wavefront-propagation path (drift / thin lens / aperture).
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the product (``srw_b200``) imports this module; only
+``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may use it, and
+only as the checker.
+
+This module restates, in double precision with numpy, the algorithm of the reference
+``srwlPropagElecField`` (cpp/src/lib/srwlib.cpp:1023) for SRWLOptC chains of drifts, thin
+lenses and rectangular/circular apertures/obstacles, with the per-element propagation
+parameter lists.  Each function cites the reference file:line it follows.  Mesh/integer logic
+follows the reference operation order exactly (so meshes are bit-exact in IEEE double); field
+arithmetic is FP64 (numpy.fft / pocketfft) instead of the reference's FP32 FFTW, so the field
+agrees with the reference to FP32 round-off (rel. L2 ~1e-6) and serves as the FP64 oracle.
+
+Parity pin: the restatement is checked against the reference itself (built from source by
+``oracle/Makefile`` into ``oracle/_ref/``) through the golden fixtures in ``tests/golden/``
+made by ``tests/golden/make_golden.py``.
+
+Not restated (documented gaps): ComputeRadMoments (sroptelm.cpp:1608) — statistical moments
+are propagated with the reference's analytic matrices only; the auto-resize Meth_1/Meth_2
+machinery (pp[0], pp[1] != 0); drift modes pp[3] = 1, 5 and >= 100; ne > 1.
+"""
+from __future__ import annotations
+
+import bisect
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# ----------------------------------------------------------------------------------------
+# FFT "good numbers" (cpp/src/ext/genmath/gmfft.cpp:26-154, NextCorrectNumberForFFT :156-228)
+# ----------------------------------------------------------------------------------------
+
+
+def _good_numbers():
+    """Even n <= 100000 of the form 2^a 3^b 5^c 7^d 11^e 13^f with e, f <= 1 (the reference's
+    table at gmfft.cpp:26 is exactly this set; pinned by tests/golden/good_numbers.json)."""
+    out = []
+    for n in range(2, 100001, 2):
+        m = n
+        for p, lim in ((2, 64), (3, 64), (5, 64), (7, 64), (11, 1), (13, 1)):
+            c = 0
+            while m % p == 0:
+                m //= p
+                c += 1
+            if c > lim:
+                break
+        else:
+            if m == 1:
+                out.append(n)
+    return out
+
+
+GOOD_NUMBERS = _good_numbers()
+
+
+def next_correct_number_for_fft(n: int) -> int:
+    """gmfft.cpp:156-228."""
+    if n < 4:
+        return 4
+    if n < 100001:
+        return GOOD_NUMBERS[bisect.bisect_left(GOOD_NUMBERS, n)]
+    mults = (10. / 9., 9. / 8., 6. / 5., 5. / 4., 4. / 3., 3. / 2., 8. / 5., 5. / 3., 16. / 9., 15. / 8.)
+    k = 99000
+    for _ in range(100):
+        for m in mults:
+            dk = k * m
+            kt = int(dk)
+            if (dk - float(kt)) >= 0.5:
+                kt += 1
+            if n <= kt:
+                return kt
+        k <<= 1
+        if n <= k:
+            return k
+    return n
+
+
+# ----------------------------------------------------------------------------------------
+# Wavefront state (srTSRWRadStructAccessData, cpp/src/core/srradstr.h:67)
+# ----------------------------------------------------------------------------------------
+
+
+@dataclass
+class Wfr:
+    ex: np.ndarray            # complex128 [nz, nx]
+    ey: np.ndarray
+    eStart: float
+    xStart: float
+    xStep: float
+    zStart: float
+    zStep: float
+    nx: int
+    nz: int
+    RobsX: float = 0.
+    RobsZ: float = 0.
+    RobsXAbsErr: float = 0.
+    RobsZAbsErr: float = 0.
+    xc: float = 0.
+    zc: float = 0.
+    xWfrMin: float = 0.
+    xWfrMax: float = 0.
+    zWfrMin: float = 0.
+    zWfrMax: float = 0.
+    Pres: int = 0
+    yStart: float = 0.     # longitudinal position (mesh.zStart)
+    avgPhotEn: float = 0.
+    momX: np.ndarray = field(default_factory=lambda: np.zeros(11))
+    momZ: np.ndarray = field(default_factory=lambda: np.zeros(11))
+    xStartTr: float = 0.
+    zStartTr: float = 0.
+    UseStartTrToShiftAtChangingRepresToCoord: bool = False
+    AuxLong1: int = 0
+    AuxLong2: int = 0
+    AuxLong3: int = 0
+    AuxLong4: int = 0
+    xLinOnly: bool = False      # m_xLinOnlyPhaseTermWasSubtracted
+    zLinOnly: bool = False
+    dxcSub: float = 0.
+    dzcSub: float = 0.
+    QuadX: bool = False         # WfrQuadTermCanBeTreatedAtResizeX
+    QuadZ: bool = False
+
+    # --- SRWLWfr <-> internal mesh (srradstr.cpp:501-634, 687-758)
+    @staticmethod
+    def from_srwl(ex, ey, mesh, Rx, Ry, dRx, dRy, xc, yc, presCA=0, momX=None, momY=None, avgPhotEn=0.):
+        """InSRWRadPtrs (srradstr.cpp:501).  ``mesh`` is a dict of SRWLRadMesh fields."""
+        nx, ny = int(mesh['nx']), int(mesh['ny'])
+        if nx <= 1:
+            xStart, xStep = 0.5 * (mesh['xStart'] + mesh['xFin']), 0.
+        else:
+            xStart, xStep = mesh['xStart'], (mesh['xFin'] - mesh['xStart']) / (nx - 1)
+        if ny <= 1:
+            zStart, zStep = 0.5 * (mesh['yStart'] + mesh['yFin']), 0.
+        else:
+            zStart, zStep = mesh['yStart'], (mesh['yFin'] - mesh['yStart']) / (ny - 1)
+        w = Wfr(ex=np.asarray(ex, np.complex128).reshape(ny, nx).copy(),
+                ey=np.asarray(ey, np.complex128).reshape(ny, nx).copy(),
+                eStart=mesh['eStart'], xStart=xStart, xStep=xStep, zStart=zStart, zStep=zStep,
+                nx=nx, nz=ny, RobsX=Rx, RobsZ=Ry, RobsXAbsErr=dRx, RobsZAbsErr=dRy, xc=xc, zc=yc,
+                xWfrMin=mesh['xStart'], xWfrMax=mesh['xFin'], zWfrMin=mesh['yStart'], zWfrMax=mesh['yFin'],
+                Pres=int(presCA), yStart=mesh.get('zStart', 0.), avgPhotEn=avgPhotEn)
+        if momX is not None:
+            w.momX = np.array(momX, np.float64)[:11].copy()
+        if momY is not None:
+            w.momZ = np.array(momY, np.float64)[:11].copy()
+        return w
+
+    def out_mesh(self):
+        """OutSRWRadPtrs (srradstr.cpp:687): SRWLRadMesh values."""
+        return dict(nx=self.nx, ny=self.nz, xStart=self.xStart, xFin=self.xStart + self.xStep * (self.nx - 1),
+                    yStart=self.zStart, yFin=self.zStart + self.zStep * (self.nz - 1), eStart=self.eStart,
+                    eFin=self.eStart, zStart=self.yStart)
+
+    def srwl_roundtrip(self):
+        """ModifyWfrNeNxNz (srradstr.cpp:760-797): OutSRWRadPtrs then InSRWRadPtrs on the same
+        SRWLWfr after the client re-allocates.  Only the mesh round trip matters here: the step is
+        re-derived from xFin and the non-zero limits reset to the mesh ends."""
+        m = self.out_mesh()
+        nx, nz = self.nx, self.nz
+        if nx <= 1:
+            self.xStart, self.xStep = 0.5 * (m['xStart'] + m['xFin']), 0.
+        else:
+            self.xStart, self.xStep = m['xStart'], (m['xFin'] - m['xStart']) / (nx - 1)
+        if nz <= 1:
+            self.zStart, self.zStep = 0.5 * (m['yStart'] + m['yFin']), 0.
+        else:
+            self.zStart, self.zStep = m['yStart'], (m['yFin'] - m['yStart']) / (nz - 1)
+        self.xWfrMin, self.xWfrMax = m['xStart'], m['xFin']
+        self.zWfrMin, self.zWfrMax = m['yStart'], m['yFin']
+
+    def set_full_range(self):
+        """SetNonZeroWavefrontLimitsToFullRange (srradstr.h:339)."""
+        self.xWfrMin = self.xStart
+        self.xWfrMax = self.xStart + self.nx * self.xStep
+        self.zWfrMin = self.zStart
+        self.zWfrMax = self.zStart + self.nz * self.zStep
+
+    def coords(self):
+        x = self.xStart + np.arange(self.nx) * self.xStep
+        z = self.zStart + np.arange(self.nz) * self.zStep
+        return x[None, :], z[:, None]
+
+    def mult(self, factor):
+        self.ex = self.ex * factor
+        self.ey = self.ey * factor
+
+
+# ----------------------------------------------------------------------------------------
+# Centred physical 2D FFT (CGenMathFFT2D::Make2DFFT, gmfft.cpp:295-897; helpers gmfft.h:232-480)
+# ----------------------------------------------------------------------------------------
+
+
+def _shift_table(N, t0, tStep):
+    """FillArrayShift (gmfft.h:250): exp(i 2 pi t0 (k - N/2) tStep) per index k."""
+    k = np.arange(N) - (N >> 1)
+    return np.exp(1j * 2. * math.pi * t0 * (k * tStep))
+
+
+def make_2d_fft(data, Nx, Ny, xStep, yStep, xStart, yStart, Dir, use_given=False, xStartTrIn=0., yStartTrIn=0.):
+    """Returns (transformed data, xStepTr, yStepTr, xStartTr, yStartTr)."""
+    RelShiftTol = 1.e-06
+    HalfNx, HalfNy = Nx >> 1, Ny >> 1
+    xStartTr = -0.5 / xStep                         # SetupLimitsTr (gmfft.h:232)
+    xStepTr = -xStartTr / HalfNx
+    yStartTr = -0.5 / yStep
+    yStepTr = -yStartTr / HalfNy
+    if use_given:
+        xStartTrOut, yStartTrOut = xStartTrIn, yStartTrIn
+    else:
+        xStartTrOut, yStartTrOut = xStartTr, yStartTr
+    xStepNx = Nx * xStep
+    yStepNy = Ny * yStep
+    x0_After = xStart + 0.5 * xStepNx
+    y0_After = yStart + 0.5 * yStepNy
+    needAfterX = abs(x0_After) > RelShiftTol * xStepNx
+    needAfterY = abs(y0_After) > RelShiftTol * yStepNy
+    needBefX = needBefY = False
+    x0_Before = y0_Before = 0.
+    if use_given:
+        x0_Before = xStartTrIn - xStartTr
+        y0_Before = yStartTrIn - yStartTr
+        needBefX = abs(x0_Before) > RelShiftTol * abs(xStartTr)
+        needBefY = abs(y0_Before) > RelShiftTol * abs(yStartTr)
+    sgn = -1. if Dir > 0 else 1.
+    d = np.array(data, np.complex128, copy=True)
+    if needBefX:
+        d = d * _shift_table(Nx, sgn * x0_Before, xStep)[None, :]
+    if needBefY:
+        d = d * _shift_table(Ny, sgn * y0_Before, yStep)[:, None]
+    Mult = xStep * yStep
+    iy = np.arange(Ny)[:, None]
+    ix = np.arange(Nx)[None, :]
+    sign = np.where(((ix + iy) & 1) == 1, -1., 1.)
+    if Dir > 0:
+        d = np.fft.fft2(d)
+        d = d * sign                                # RepairSignAfter2DFFT (gmfft.h:334)
+        d = np.roll(d, (HalfNy, HalfNx), axis=(0, 1))   # RotateDataAfter2DFFT (gmfft.h:279), even N
+    else:
+        d = np.roll(d, (HalfNy, HalfNx), axis=(0, 1))
+        d = d * sign
+        d = np.fft.ifft2(d) * (Nx * Ny)             # FFTW_BACKWARD is unnormalised
+    d = d * Mult
+    if needAfterX:
+        d = d * _shift_table(Nx, sgn * x0_After, xStepTr)[None, :]
+    if needAfterY:
+        d = d * _shift_table(Ny, sgn * y0_After, yStepTr)[:, None]
+    return d, xStepTr, yStepTr, xStartTrOut, yStartTrOut
+
+
+def set_rad_repres(w: Wfr, coord_or_ang: int):
+    """srTGenOptElem::SetRadRepres (sroptelm.cpp:1243-1528), ne == 1; the edge correction is never
+    enabled (WfrEdgeCorrShouldBeDone is 0 from Initialize, srradstr.cpp:1532)."""
+    if w.Pres == coord_or_ang:
+        return
+    Dir = -1 if coord_or_ang == 0 else 1
+    use_given = (w.AuxLong4 == 7777777) or ((coord_or_ang == 0) and w.UseStartTrToShiftAtChangingRepresToCoord)
+    res = None
+    for comp in ('ex', 'ey'):
+        d, xs, ys, x0, y0 = make_2d_fft(getattr(w, comp), w.nx, w.nz, w.xStep, w.zStep, w.xStart, w.zStart,
+                                        Dir, use_given, w.xStartTr, w.zStartTr)
+        setattr(w, comp, d)
+        res = (xs, ys, x0, y0)
+    w.xStep, w.zStep, w.xStart, w.zStart = res
+    w.Pres = coord_or_ang
+    w.set_full_range()
+
+
+def _apply_phase(w: Wfr, phase):
+    w.mult(np.exp(1j * phase))
+
+
+# ----------------------------------------------------------------------------------------
+# Drift space (cpp/src/core/sroptdrf.h, sroptdrf.cpp)
+# ----------------------------------------------------------------------------------------
+
+PI_D_LAMBDA_PER_EV = 2.53384080189E+06      # sroptdrf.h:479 (pi/lambda[m] per eV)
+INV_LAMBDA_PER_EV = 806546.577258           # sroptdrf.h:481
+LAMBDA_EV_M = 1.239842e-06                  # sroptdrf.h:617
+
+
+def _diff_lim_spot(w: Wfr, x_or_z, L):
+    """DiffractionLimitedPropagatedSpotSize (sroptdrf.h:1020)."""
+    lam = LAMBDA_EV_M / w.eStart
+    if x_or_z == 'x':
+        dLim = (w.nx - 1) * w.xStep
+        dWfr = w.xWfrMax - w.xWfrMin
+    else:
+        dLim = (w.nz - 1) * w.zStep
+        dWfr = w.zWfrMax - w.zWfrMin
+    d = dWfr if ((dWfr > 0.) and (dWfr < dLim)) else dLim
+    return lam * L / d
+
+
+def _mom_apply(mom, ax, az):
+    """MultSquareMatrByVect steps of AuxPropagateRadMoments (sroptdrf.cpp:22) / GenAuxPropagateRadMoments
+    (sroptelm.cpp:2095) on one 11-moment record [Tot, x, x', z, z', xx, xx', x'x', zz, zz', z'z']."""
+    bx = [[ax[0][0] * ax[0][0], 2. * ax[0][0] * ax[0][1], ax[0][1] * ax[0][1]],
+          [ax[0][0] * ax[1][0], ax[0][1] * ax[1][0] + ax[0][0] * ax[1][1], ax[0][1] * ax[1][1]],
+          [ax[1][0] * ax[1][0], 2. * ax[1][0] * ax[1][1], ax[1][1] * ax[1][1]]]
+    bz = [[az[0][0] * az[0][0], 2. * az[0][0] * az[0][1], az[0][1] * az[0][1]],
+          [az[0][0] * az[1][0], az[0][1] * az[1][0] + az[0][0] * az[1][1], az[0][1] * az[1][1]],
+          [az[1][0] * az[1][0], 2. * az[1][0] * az[1][1], az[1][1] * az[1][1]]]
+
+    def mv(a, v):
+        return [sum(a[i][j] * v[j] for j in range(len(v))) for i in range(len(v))]
+    m = mom
+    m[1], m[2] = mv(ax, [m[1], m[2]])
+    m[3], m[4] = mv(az, [m[3], m[4]])
+    m[5], m[6], m[7] = mv(bx, [m[5], m[6], m[7]])
+    m[8], m[9], m[10] = mv(bz, [m[8], m[9], m[10]])
+
+
+def drift_propagate_moments(w: Wfr, L):
+    """srTDriftSpace::PropagateRadMoments -> AuxPropagateRadMoments (sroptdrf.h:967, sroptdrf.cpp:22)."""
+    a = [[1., L], [0., 1.]]
+    for mom in (w.momX, w.momZ):
+        if mom[0] != 0.:
+            _mom_apply(mom, a, a)
+            sx = _diff_lim_spot(w, 'x', L)
+            if mom[5] - mom[1] * mom[1] < sx * sx:
+                mom[5] = sx * sx + mom[1] * mom[1]
+            sz = _diff_lim_spot(w, 'z', L)
+            if mom[8] - mom[3] * mom[3] < sz * sz:
+                mom[8] = sz * sz + mom[3] * mom[3]
+
+
+def drift_ang_repres(w: Wfr, L, treat):
+    """PropagateRadiationSimple_AngRepres (sroptdrf.h:348-411) + RadPointModifier_AngRepres (:615)."""
+    xStartOld, zStartOld = w.xStart, w.zStart
+    w.xStart = -(w.nx >> 1) * w.xStep
+    w.zStart = -(w.nz >> 1) * w.zStep
+    xShift, zShift = w.xStart - xStartOld, w.zStart - zStartOld
+    w.xWfrMin += xShift; w.xWfrMax += xShift
+    w.zWfrMin += zShift; w.zWfrMax += zShift
+    if w.Pres != 1:
+        set_rad_repres(w, 1)
+    qx, qz = w.coords()
+    lam = LAMBDA_EV_M / w.eStart
+    c0 = -3.1415926536 * L * lam
+    c1 = 0.25 * lam * lam
+    q2 = qx * qx + qz * qz
+    c1q2 = c1 * q2
+    ph = c0 * q2 * (1. + c1q2 + 2. * c1q2 * c1q2)
+    if treat == 1:
+        ph = ph + 5.067730652e+06 * L * w.eStart
+    _apply_phase(w, ph)
+    if w.UseStartTrToShiftAtChangingRepresToCoord:
+        w.xStartTr += xShift
+        w.zStartTr += zShift
+    set_rad_repres(w, 0)
+    w.xStart, w.zStart = xStartOld, zStartOld
+    if w.UseStartTrToShiftAtChangingRepresToCoord:
+        w.xStart = w.xStartTr - xShift
+        w.zStart = w.zStartTr - zShift
+    w.set_full_range()
+
+
+def drift_to_waist(w: Wfr, L, treat):
+    """PropagateRadiationSimple_PropToWaist (sroptdrf.cpp:356-489), SetupPropBufVars_PropToWaist
+    (sroptdrf.h:476-502), RadPointModifier_PropToWaist (sroptdrf.h:649-710)."""
+    w.set_full_range()
+    InvLength = 1. / L
+    Pi_d_LambdaM = w.eStart * PI_D_LAMBDA_PER_EV
+    Pi_d_LambdaM_d_Length = Pi_d_LambdaM * InvLength
+    InvLength_d_Lambda = InvLength * w.eStart * INV_LAMBDA_PER_EV
+    TwoPi_d_LambdaM = 2. * Pi_d_LambdaM
+    TwoPiXc_d_LambdaMRx = TwoPi_d_LambdaM * w.xc / w.RobsX
+    TwoPiZc_d_LambdaMRz = TwoPi_d_LambdaM * w.zc / w.RobsZ
+    if w.Pres != 0:
+        set_rad_repres(w, 0)
+    x, z = w.coords()
+    ph = Pi_d_LambdaM_d_Length * (x * x + z * z) + TwoPiXc_d_LambdaMRx * x + TwoPiZc_d_LambdaMRz * z
+    if treat == 1:
+        ph = ph + 5.067730652e+06 * L * w.eStart
+    _apply_phase(w, ph)
+    InvLambda_m = w.eStart * INV_LAMBDA_PER_EV
+    InvLambda_m_d_Length = InvLambda_m / L
+    LambdaM_Length = 1. / InvLambda_m_d_Length
+    r = None
+    for comp in ('ex', 'ey'):
+        d, xs, ys, x0, y0 = make_2d_fft(getattr(w, comp), w.nx, w.nz, w.xStep, w.zStep, w.xStart, w.zStart, 1)
+        setattr(w, comp, d)
+        r = (xs, ys, x0, y0)
+    xStepTr, yStepTr, xStartTr, yStartTr = r
+    qxCen = -w.xc * InvLambda_m / w.RobsX
+    qzCen = -w.zc * InvLambda_m / w.RobsZ
+    w.xStart = (xStartTr + qxCen) * LambdaM_Length
+    w.zStart = (yStartTr + qzCen) * LambdaM_Length
+    w.xStep = xStepTr * LambdaM_Length
+    w.zStep = yStepTr * LambdaM_Length
+    x, z = w.coords()
+    ph = Pi_d_LambdaM_d_Length * (x * x + z * z)
+    w.mult(np.exp(1j * ph) * (-1j * InvLength_d_Lambda))
+    if LambdaM_Length < 0:
+        mirror_field(w, -1, -1)
+        xEnd = w.xStart + w.xStep * (w.nx - 1)
+        w.xStart = xEnd
+        w.xStep *= -1.
+        zEnd = w.zStart + w.zStep * (w.nz - 1)
+        w.zStart = zEnd
+        w.zStep *= -1.
+
+
+def _sign(v):
+    return 1. if v > 0 else (-1. if v < 0 else 0.)
+
+
+def drift_quad(w: Wfr, L, treat, subtype):
+    """PropagateRadiationSimple_AnalytTreatQuadPhaseTerm (sroptdrf.cpp:726-887) with
+    SetupPropBufVars_AnalytTreatQuadPhaseTerm (:889-1083) and the pp[3]=2 radius estimate
+    EstimateWfrRadToSub2_AnalytTreatQuadPhaseTerm (:1085-1120); modifier sroptdrf.h:806-880."""
+    infLarge = 1E+23
+    xc, zc = w.xc, w.zc
+    invRx = invRz = 0.
+    Lx = Lz = 0.
+    invRxL = invRzL = 1. / L
+    kx = kxc = kz = kzc = infLarge
+    trueRx, trueRz = w.RobsX, w.RobsZ
+    if subtype == 2:
+        factRadEr = 3.
+        minAbsEffRx = factRadEr * w.RobsXAbsErr
+        minAbsEffRz = factRadEr * w.RobsZAbsErr
+        effRx_p_L = trueRx + L
+        if abs(trueRx) < minAbsEffRx:
+            trueRx = minAbsEffRx * (1. if trueRx >= 0 else -1.)
+        elif abs(effRx_p_L) < minAbsEffRx:
+            trueRx = minAbsEffRx * (1. if effRx_p_L >= 0 else -1.) - L
+        effRz_p_L = trueRz + L
+        if abs(trueRz) < minAbsEffRz:
+            trueRz = minAbsEffRz * (1. if trueRz >= 0 else -1.)
+        elif abs(effRz_p_L) < minAbsEffRz:
+            trueRz = minAbsEffRz * (1. if effRz_p_L >= 0 else -1.) - L
+    elif subtype == 1:
+        raise NotImplementedError("pp[3]=1 (moment-based radius estimate) is not restated")
+    if trueRx != 0:
+        invRx = 1. / trueRx
+        kx = (trueRx + L) * invRx
+        kxc = L / trueRx
+        if -L != trueRx:
+            Lx = L / (1. + L * invRx)
+            invRxL = 1. / (L + trueRx)
+        else:
+            Lx = infLarge
+            invRxL = infLarge
+    if trueRz != 0:
+        invRz = 1. / trueRz
+        kz = (trueRz + L) * invRz
+        kzc = L / trueRz
+        if -L != trueRz:
+            Lz = L / (1. + L * invRz)
+            invRzL = 1. / (L + trueRz)
+        else:
+            Lz = infLarge
+            invRzL = infLarge
+    sqrt_LxLz_d_L = math.sqrt(abs(Lx * Lz)) / L
+    phase_term_signLxLz = 0.25 * 3.141592653589793 * (2. - _sign(Lx) - _sign(Lz))
+
+    if w.Pres != 0:
+        set_rad_repres(w, 0)
+    lam = LAMBDA_EV_M / w.eStart
+    x, z = w.coords()
+    rx, rz = x - xc, z - zc
+    Pi_d_Lambda_m = 3.1415926536 / lam
+    _apply_phase(w, -Pi_d_Lambda_m * (invRx * rx * rx + invRz * rz * rz))
+    xStartOld, zStartOld = w.xStart, w.zStart
+    w.xStart = -(w.nx >> 1) * w.xStep
+    w.zStart = -(w.nz >> 1) * w.zStep
+    xShift, zShift = w.xStart - xStartOld, w.zStart - zStartOld
+    w.xWfrMin += xShift; w.xWfrMax += xShift
+    w.zWfrMin += zShift; w.zWfrMax += zShift
+    set_rad_repres(w, 1)
+    qx, qz = w.coords()
+    Pi_Lambda_m = 3.1415926536 * lam
+    c0x, c0z = -Pi_Lambda_m * Lx, -Pi_Lambda_m * Lz
+    w.mult(np.exp(1j * (c0x * qx * qx + c0z * qz * qz + phase_term_signLxLz)) * sqrt_LxLz_d_L)
+    if w.UseStartTrToShiftAtChangingRepresToCoord:
+        w.xStartTr += xShift
+        w.zStartTr += zShift
+    set_rad_repres(w, 0)
+    w.xStart, w.zStart = xStartOld, zStartOld
+    if w.UseStartTrToShiftAtChangingRepresToCoord:
+        w.xStart = w.xStartTr - xShift
+        w.zStart = w.zStartTr - zShift
+    w.xStart = kx * w.xStart - kxc * w.xc
+    w.xStep *= kx
+    w.zStart = kz * w.zStart - kzc * w.zc
+    w.zStep *= kz
+    x, z = w.coords()
+    rx, rz = x - xc, z - zc
+    ph = Pi_d_Lambda_m * (invRxL * rx * rx + invRzL * rz * rz)
+    if treat == 1:
+        ph = ph + 2 * Pi_d_Lambda_m * L
+    _apply_phase(w, ph)
+    mirror_field(w, int(_sign(kx)), int(_sign(kz)))
+    if kx < 0:
+        xEnd = w.xStart + (w.nx - 1) * w.xStep
+        w.xStart = xEnd
+        w.xStep *= -1
+    if kz < 0:
+        zEnd = w.zStart + (w.nz - 1) * w.zStep
+        w.zStart = zEnd
+        w.zStep *= -1
+    w.set_full_range()
+
+
+def mirror_field(w: Wfr, sx, sz):
+    """MirrorFieldData (srradstr.cpp:2707)."""
+    if sx < 0:
+        w.ex = w.ex[:, ::-1].copy(); w.ey = w.ey[:, ::-1].copy()
+    if sz < 0:
+        w.ex = w.ex[::-1, :].copy(); w.ey = w.ey[::-1, :].copy()
+
+
+def drift(w: Wfr, L, treat, anal_treatment):
+    """srTDriftSpace::PropagateRadiation (sroptdrf.h:116) -> ChooseLocalPropMode (:223) ->
+    PropagateRadiationSingleE_Meth_0 (:158): Simple, moments, radius, 4x4 matrix."""
+    if anal_treatment in (1, 2):
+        drift_quad(w, L, treat, anal_treatment)
+    elif anal_treatment == 4:
+        drift_to_waist(w, L, treat)
+    elif anal_treatment == 0:
+        drift_ang_repres(w, L, treat)
+    else:
+        raise NotImplementedError("drift mode pp[3]=%d is not restated" % anal_treatment)
+    drift_propagate_moments(w, L)
+    w.RobsX += L                             # PropagateWaveFrontRadius (sroptdrf.h:981)
+    w.RobsZ += L
+    w.set_full_range()
+
+
+# ----------------------------------------------------------------------------------------
+# Linear phase terms (srradstr.cpp:2610-2705)
+# ----------------------------------------------------------------------------------------
+
+
+def _mult_phase_lin(w: Wfr, xMult, zMult):
+    """MultiplyElFieldByPhaseLin (srradstr.h:509): exp(i(xMult x + zMult z))."""
+    x, z = w.coords()
+    _apply_phase(w, xMult * x + zMult * z)
+
+
+def check_and_subtract_phase_lin(w: Wfr, newXc, newZc):
+    ratAllowSubtract = 0.2
+    minNumOptCycles = 10
+    lambda_m = 3.1415926535898 / (w.eStart * 2.53384080189E+06)
+    twoPi = 2. * 3.1415926535898
+    xOK = False
+    dxcSubNew = newXc - w.xc
+    if w.RobsX != 0:
+        rng = w.xStep * (w.nx - 1)
+        ncyc = 0.25 * rng * rng / (lambda_m * w.RobsX)
+        xOK = (abs(w.RobsX) > abs(w.RobsXAbsErr)) and (ncyc > minNumOptCycles) and (abs(dxcSubNew) / rng > ratAllowSubtract)
+    if not xOK:
+        dxcSubNew = 0
+    zOK = False
+    dzcSubNew = newZc - w.zc
+    if w.RobsZ != 0:
+        rng = w.zStep * (w.nz - 1)
+        ncyc = 0.25 * rng * rng / (lambda_m * w.RobsZ)
+        zOK = (abs(w.RobsZ) > abs(w.RobsZAbsErr)) and (ncyc > minNumOptCycles) and (abs(dzcSubNew) / rng > ratAllowSubtract)
+    if not zOK:
+        dzcSubNew = 0
+    if (not xOK) and (not zOK):
+        return
+    dxc = dxcSubNew
+    if w.xLinOnly:
+        dxc -= w.dxcSub
+        if abs(dxc) / abs(w.dxcSub) < ratAllowSubtract:
+            dxc = 0; dxcSubNew = w.dxcSub
+    w.dxcSub = dxcSubNew
+    w.xLinOnly = (dxcSubNew != 0)
+    xMult = -twoPi * dxc / (lambda_m * w.RobsX)
+    dzc = dzcSubNew
+    if zOK and w.zLinOnly:
+        dzc -= w.dzcSub
+        if abs(dzc) / abs(w.dzcSub) < ratAllowSubtract:
+            dzc = 0; dzcSubNew = w.dzcSub
+    w.dzcSub = dzcSubNew
+    w.zLinOnly = (dzcSubNew != 0)
+    zMult = -twoPi * dzc / (lambda_m * w.RobsZ)
+    if xMult == 0 and zMult == 0:
+        return
+    _mult_phase_lin(w, xMult, zMult)
+
+
+def check_and_reset_phase_lin(w: Wfr):
+    if (not w.xLinOnly) and (not w.zLinOnly):
+        return
+    lambda_m = 3.1415926535898 / (w.eStart * 2.53384080189E+06)
+    twoPi = 2. * 3.1415926535898
+    xMult = zMult = 0.
+    if w.xLinOnly and w.dxcSub != 0 and w.RobsX != 0:
+        xMult = twoPi * w.dxcSub / (lambda_m * w.RobsX)
+    if w.zLinOnly and w.dzcSub != 0 and w.RobsZ != 0:
+        zMult = twoPi * w.dzcSub / (lambda_m * w.RobsZ)
+    w.xLinOnly = w.zLinOnly = False
+    w.dxcSub = w.dzcSub = 0
+    if xMult == 0 and zMult == 0:
+        return
+    _mult_phase_lin(w, xMult, zMult)
+
+
+# ----------------------------------------------------------------------------------------
+# Thin lens (cpp/src/core/sroptfoc.h:18-276)
+# ----------------------------------------------------------------------------------------
+
+
+def _fix_abs_err(w: Wfr):
+    """Tail of srTGenOptElem::PropagateRadiationMeth_0 (sroptel2.cpp:151-152, non-OpenMP build)."""
+    if w.RobsX != 0 and w.RobsXAbsErr == 0:
+        w.RobsXAbsErr = abs(0.1 * w.RobsX)
+    if w.RobsZ != 0 and w.RobsZAbsErr == 0:
+        w.RobsZAbsErr = abs(0.1 * w.RobsZ)
+
+
+def lens(w: Wfr, Fx, Fz, cx, cz):
+    check_and_subtract_phase_lin(w, cx, cz)
+    if w.Pres != 0:
+        set_rad_repres(w, 0)
+    x, z = w.coords()
+    Pi_d_Lambda_m = w.eStart * 2.533865612E+06
+    xr, zr = x - cx, z - cz
+    _apply_phase(w, -Pi_d_Lambda_m * (xr * xr / Fx + zr * zr / Fz))
+    ax = [[1., 0.], [-1. / Fx, 1.]]
+    az = [[1., 0.], [-1. / Fz, 1.]]
+    for mom in (w.momX, w.momZ):
+        _mom_apply(mom, ax, az)
+    dSmall = 1E-23                                # PropagateWaveFrontRadius (sroptfoc.h:37)
+    difX = dSmall if Fx == w.RobsX else Fx - w.RobsX
+    difZ = dSmall if Fz == w.RobsZ else Fz - w.RobsZ
+    MagnX, MagnZ = Fx / difX, Fz / difZ
+    w.RobsX *= MagnX
+    w.RobsZ *= MagnZ
+    w.RobsXAbsErr *= MagnX * MagnX
+    w.RobsZAbsErr *= MagnZ * MagnZ
+    w.xc = cx - (cx - w.xc) * MagnX
+    w.zc = cz - (cz - w.zc) * MagnZ
+    _fix_abs_err(w)
+    check_and_reset_phase_lin(w)
+
+
+# ----------------------------------------------------------------------------------------
+# Apertures / obstacles (cpp/src/core/sroptapt.h)
+# ----------------------------------------------------------------------------------------
+
+
+def aperture(w: Wfr, shape, ap_or_ob, Dx, Dy, cx, cy):
+    if w.Pres != 0:
+        set_rad_repres(w, 0)
+    x, z = w.coords()
+    xr, zr = x - cx, z - cy
+    if shape == 'r':
+        hx, hz = 0.5 * Dx + 1.E-10, 0.5 * Dy + 1.E-10
+        inside = (xr >= -hx) & (xr <= hx) & (zr >= -hz) & (zr <= hz)
+    else:
+        R = 0.5 * Dx
+        inside = ~(xr * xr + zr * zr > R * R)
+        if ap_or_ob in 'oO':
+            inside = (xr * xr + zr * zr > R * R)
+    if shape == 'r' and ap_or_ob in 'oO':
+        inside = ~inside
+    w.ex = np.where(inside, w.ex, 0.)
+    w.ey = np.where(inside, w.ey, 0.)
+    # SetNewNonZeroWfrLimits (apertures only; obstacles keep the limits in the cases used here)
+    if ap_or_ob in 'aA':
+        if shape == 'r':
+            hx, hz = 0.5 * Dx, 0.5 * Dy
+        else:
+            hx = hz = 0.5 * Dx
+        w.xWfrMin = max(w.xWfrMin, cx - hx)
+        w.xWfrMax = min(w.xWfrMax, cx + hx)
+        w.zWfrMin = max(w.zWfrMin, cy - hz)
+        w.zWfrMax = min(w.zWfrMax, cy + hz)
+    _fix_abs_err(w)
+
+
+# ----------------------------------------------------------------------------------------
+# Resizing (srTGenOptElem::RadResizeGen sroptelm.cpp:2242-3036, RadResizeCore :3038-3337)
+# ----------------------------------------------------------------------------------------
+
+
+def _int_offset_coord(xStart, xStep, xVal):
+    """IntegerOffsetCoord (sroptelm.h:995)."""
+    i = int((xVal - xStart) / xStep)
+    if abs(xVal - ((i + 1) * xStep + xStart)) < 1.E-05 * xStep:
+        i += 1
+    return i
+
+
+def _wavefront_term_can_be_treated(w: Wfr):
+    """WaveFrontTermCanBeTreated (sroptelm.cpp:4692), checkBenefit=false."""
+    w.QuadX = abs(w.RobsXAbsErr) < 0.4 * abs(w.RobsX)
+    w.QuadZ = abs(w.RobsZAbsErr) < 0.4 * abs(w.RobsZ)
+    return w.QuadX or w.QuadZ
+
+
+def _treat_strongly_oscillating(w: Wfr, add_or_rem):
+    """TreatStronglyOscillatingTerm (sroptelm.cpp:4774-5014), coordinate representation."""
+    Const = 3.14159265358979 * 1.E+06 / 1.23984186
+    if w.Pres == 0:
+        cRx = Const / w.RobsX if w.QuadX else 0.
+        cRz = Const / w.RobsZ if w.QuadZ else 0.
+    else:
+        lam = LAMBDA_EV_M / w.eStart
+        cRx = -Const * w.RobsX * lam * lam if w.QuadX else 0.
+        cRz = -Const * w.RobsZ * lam * lam if w.QuadZ else 0.
+    if add_or_rem == 'r':
+        cRx, cRz = -cRx, -cRz
+    x, z = w.coords()
+    x = x - w.xc
+    z = z - w.zc
+    ph = np.zeros((w.nz, w.nx))
+    if w.QuadZ:
+        ph = ph + cRz * w.eStart * z * z
+    if w.QuadX:
+        ph = ph + cRx * w.eStart * x * x
+    _apply_phase(w, ph)
+
+
+def _lagrange4(t):
+    """Cubic Lagrange weights on nodes -1, 0, 1, 2 (the reference's SetupInterpolAux02 /
+    InterpolF polynomial, sroptelm.h:560-640, is this interpolant in monomial form)."""
+    return np.stack([-t * (t - 1.) * (t - 2.) / 6., (t + 1.) * (t - 1.) * (t - 2.) / 2.,
+                     -(t + 1.) * t * (t - 2.) / 2., (t + 1.) * t * (t - 1.) / 6.])
+
+
+def _resize_core(old: Wfr, new: Wfr, quad_treat):
+    """RadResizeCore (sroptelm.cpp:3038-3337) for ne == 1, vectorised over new points.
+    Includes the low-order fallback (CheckForLowOrderInterp, sroptelm.h:700-760) and the
+    amplitude correction by the interpolated intensity (ImproveReAndIm, sroptelm.h:690)."""
+    ixS, ixE, izS, izE = new.AuxLong1, new.AuxLong2, new.AuxLong3, new.AuxLong4
+    outx = np.zeros((new.nz, new.nx), np.complex128)
+    outy = np.zeros((new.nz, new.nx), np.complex128)
+    if ixE < ixS or izE < izS:
+        return outx, outy
+    ix = np.arange(ixS, ixE + 1)
+    iz = np.arange(izS, izE + 1)
+    xStepInv, zStepInv = 1. / old.xStep, 1. / old.zStep
+
+    def axis(iv, start_new, step_new, start_old, step_old, inv, n_old):
+        a = start_new + iv * step_new
+        ic = ((a - start_old) * inv + 1.E-06).astype(np.int64)
+        rel = a - (start_old + ic * step_old)
+        st = ic - 1
+        st = np.where(ic == n_old - 1, ic - 3, st)
+        rel = np.where(ic == n_old - 1, rel + 2. * step_old, rel)
+        st = np.where(ic == n_old - 2, ic - 2, st)
+        rel = np.where(ic == n_old - 2, rel + step_old, rel)
+        st = np.where(ic == 0, ic, st)
+        rel = np.where(ic == 0, rel - step_old, rel)
+        return ic, st, rel * inv
+    ixc, ixst, xr = axis(ix, new.xStart, new.xStep, old.xStart, old.xStep, xStepInv, old.nx)
+    izc, izst, zr = axis(iz, new.zStart, new.zStep, old.zStart, old.zStep, zStepInv, old.nz)
+    wx = _lagrange4(xr)          # [4, nX]
+    wz = _lagrange4(zr)          # [4, nZ]
+    irx = np.clip(ixc - ixst, 0, 2)
+    irz = np.clip(izc - izst, 0, 2)
+    for src, dst in ((old.ex, outx), (old.ey, outy)):
+        blk = np.empty((4, 4, iz.size, ix.size), np.complex128)   # [dz, dx, Z, X]
+        for dz in range(4):
+            rows = src[izst + dz]
+            for dx in range(4):
+                blk[dz, dx] = rows[:, ixst + dx]
+        re_, im_ = blk.real, blk.imag
+        inten = re_ * re_ + im_ * im_
+        low = np.any((re_ == 0.) | (im_ == 0.), axis=(0, 1))
+        W = wz[:, None, :, None] * wx[None, :, None, :]
+        F = np.sum(W * blk, axis=(0, 1))
+        FI = np.maximum(np.sum(W * inten, axis=(0, 1)), 0.)
+        # low-order (bilinear on the 2x2 sub-cell picked by the clipped relative indices,
+        # evaluated with the same xRel/zRel: reproduces the reference also at grid edges)
+        X = xr[None, :]
+        Z = zr[:, None]
+        r0 = irz[:, None] * np.ones_like(irx)[None, :]
+        c0 = np.ones_like(irz)[:, None] * irx[None, :]
+        Zi = np.arange(iz.size)[:, None] * np.ones(ix.size, np.int64)[None, :]
+        Xi = np.ones(iz.size, np.int64)[:, None] * np.arange(ix.size)[None, :]
+
+        def pick(arr, dr, dc):
+            return arr[r0 + dr, c0 + dc, Zi, Xi]
+        f00, f10, f01, f11 = pick(blk, 0, 0), pick(blk, 0, 1), pick(blk, 1, 0), pick(blk, 1, 1)
+        FL = f00 + (f10 - f00) * X + (f01 - f00) * Z + (f00 - f01 - f10 + f11) * X * Z
+        i00, i10, i01, i11 = pick(inten, 0, 0), pick(inten, 0, 1), pick(inten, 1, 0), pick(inten, 1, 1)
+        FIL = np.maximum(i00 + (i10 - i00) * X + (i01 - i00) * Z + (i00 - i01 - i10 + i11) * X * Z, 0.)
+        F = np.where(low, FL, F)
+        FI = np.where(low, FIL, FI)
+        app = np.abs(F) ** 2
+        fac = np.where(app != 0., np.sqrt(np.where(app != 0., FI / np.where(app != 0., app, 1.), 1.)), 1.)
+        dst[izS:izE + 1, ixS:ixE + 1] = F * fac
+    return outx, outy
+
+
+def _resize_core_only_larger_range(old: Wfr, new: Wfr):
+    """RadResizeCore_OnlyLargerRange (sroptelm.cpp:4231-4306)."""
+    outx = np.zeros((new.nz, new.nx), np.complex128)
+    outy = np.zeros((new.nz, new.nx), np.complex128)
+    ixS, ixE, izS, izE = new.AuxLong1, new.AuxLong2, new.AuxLong3, new.AuxLong4
+    ix = np.arange(ixS, ixE + 1)
+    iz = np.arange(izS, izE + 1)
+    xo = ((new.xStart + ix * new.xStep - old.xStart) * (1. / old.xStep) + 1.E-08).astype(np.int64)
+    zo = ((new.zStart + iz * new.zStep - old.zStart) * (1. / old.zStep) + 1.E-08).astype(np.int64)
+    outx[izS:izE + 1, ixS:ixE + 1] = old.ex[zo][:, xo]
+    outy[izS:izE + 1, ixS:ixE + 1] = old.ey[zo][:, xo]
+    return outx, outy
+
+
+def rad_resize_gen(w: Wfr, pxm, pxd, pzm, pzd, shift_type=0, xCenShift=0., zCenShift=0., other_side=False):
+    """RadResizeGen (sroptelm.cpp:2242-3036), ne == 1, no per-polarisation memory fallback."""
+    if pxm == 1. and pxd == 1. and pzm == 1. and pzd == 1. and shift_type <= 0:
+        return
+    RelCenPosX = RelCenPosZ = 0.5
+    RelCenPosTol = 1.e-06
+    if shift_type & 1:
+        rxTot = w.xStep * (w.nx - 1)
+        rxLeft = xCenShift - w.xStart
+        if rxLeft > 0. and xCenShift < (w.xStart + rxTot):
+            RelCenPosX = rxLeft / rxTot
+    if shift_type & 2:
+        rzTot = w.zStep * (w.nz - 1)
+        rzLeft = zCenShift - w.zStart
+        if rzLeft > 0. and zCenShift < (w.zStart + rzTot):
+            RelCenPosZ = rzLeft / rzTot
+    nxOld, nzOld = w.nx, w.nz
+    xStartOld, zStartOld = w.xStart, w.zStart
+    xStepOld, zStepOld = w.xStep, w.zStep
+    xRangeOld, zRangeOld = xStepOld * nxOld, zStepOld * nzOld
+    useStartTrOther = (abs(xStartOld + 0.5 * xRangeOld) > 0.5 * w.xStep) or (abs(zStartOld + 0.5 * zRangeOld) > 0.5 * w.zStep)
+    pxmIn, pxdIn, pzmIn, pzdIn = pxm, pxd, pzm, pzd
+    if other_side:
+        to = 1 if w.Pres == 0 else 0
+        if useStartTrOther:
+            w.xStart = -(w.nx >> 1) * w.xStep
+            w.zStart = -(w.nz >> 1) * w.zStep
+            xs, zs = w.xStart - xStartOld, w.zStart - zStartOld
+            w.xWfrMin += xs; w.xWfrMax += xs
+            w.zWfrMin += zs; w.zWfrMax += zs
+        set_rad_repres(w, to)
+        pxm, pxd, pzm, pzd = pxd, pxm, pzd, pzm
+    old = w
+    new = Wfr(**{k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in w.__dict__.items()})
+    pxTot, pzTot = pxm * pxd, pzm * pzd
+    NewNx, NewNz = w.nx, w.nz
+    changed = (pxTot != 1.) or (pzTot != 1.)
+    if changed:
+        v = pxTot * NewNx
+        iv = int(v)
+        NewNx = iv + 1 if (v - iv) >= 0.5 else iv
+        v = pzTot * NewNz
+        iv = int(v)
+        NewNz = iv + 1 if (v - iv) >= 0.5 else iv
+        NewNx = next_correct_number_for_fft(NewNx)
+        NewNz = next_correct_number_for_fft(NewNz)
+        new.nx, new.nz = NewNx, NewNz
+    iXc = w.nx >> 1
+    centerOffset = False
+    if abs(RelCenPosX - 0.5) > RelCenPosTol:
+        xcAppr = w.xStart + w.nx * w.xStep * RelCenPosX
+        iXc = _int_offset_coord(w.xStart, w.xStep, xcAppr)
+        centerOffset = True
+    Xc = w.xStart + w.xStep * iXc
+    iZc = w.nz >> 1
+    if abs(RelCenPosZ - 0.5) > RelCenPosTol:
+        zcAppr = w.zStart + w.nz * w.zStep * RelCenPosZ
+        iZc = _int_offset_coord(w.zStart, w.zStep, zcAppr)
+        centerOffset = True
+    Zc = w.zStart + w.zStep * iZc
+    if centerOffset:
+        raise NotImplementedError("off-centre resize (pp[9] shift types) is not restated")
+
+    def preserve(axis):
+        """PreserveLogicsOfWfrLimitsAtRangeResizing (srradstr.cpp:1598)."""
+        if axis == 'x':
+            tol = 0.01 * new.xStep
+            if abs(old.xWfrMin - old.xStart) < tol and abs(old.xStart + old.nx * old.xStep - old.xWfrMax) < tol:
+                new.xWfrMin, new.xWfrMax = new.xStart, new.xStart + new.nx * new.xStep
+            else:
+                new.xWfrMin, new.xWfrMax = old.xWfrMin, old.xWfrMax
+        else:
+            tol = 0.01 * new.zStep
+            if abs(old.zWfrMin - old.zStart) < tol and abs(old.zStart + old.nz * old.zStep - old.zWfrMax) < tol:
+                new.zWfrMin, new.zWfrMax = new.zStart, new.zStart + new.nz * new.zStep
+            else:
+                new.zWfrMin, new.zWfrMax = old.zWfrMin, old.zWfrMax
+    xMagOld = (w.nx - 1) * w.xStep
+    if pxm > 1.:
+        NxInner = int(NewNx / pxm) if pxd != 1. else w.nx
+        d = NewNx - NxInner
+        left = d >> 1
+        if (left << 1) != d:
+            left += 1
+        new.xStep = xMagOld / (NxInner - 1)
+        new.xStart = w.xStart - left * new.xStep
+        new.AuxLong1 = left
+        new.AuxLong2 = left + NxInner - 1
+        preserve('x')
+    else:
+        xEndOld = w.xStart + (w.nx - 1) * w.xStep
+        xMid = 0.5 * (w.xStart + xEndOld)
+        xMagNew = xMagOld * pxm
+        new.xStep = xMagNew / (NewNx - 1)
+        if pxd == 1:
+            new.xStep = w.xStep
+            xMagNew = (NewNx - 1) * new.xStep
+        new.xStart = xMid - 0.5 * xMagNew
+        new.AuxLong1 = 0
+        new.AuxLong2 = NewNx - 1
+        if new.xStart > new.xWfrMin:
+            new.xWfrMin = new.xStart
+        if (new.xStart + xMagNew) < new.xWfrMax:
+            new.xWfrMax = new.xStart + xMagNew
+    zMagOld = (w.nz - 1) * w.zStep
+    if pzm > 1.:
+        NzInner = int(NewNz / pzm) if pzd != 1. else w.nz
+        d = NewNz - NzInner
+        left = d >> 1
+        if (left << 1) != d:
+            left += 1
+        new.zStep = zMagOld / (NzInner - 1)
+        new.zStart = w.zStart - left * new.zStep
+        new.AuxLong3 = left
+        new.AuxLong4 = left + NzInner - 1
+        preserve('z')
+    else:
+        zEndOld = w.zStart + (w.nz - 1) * w.zStep
+        zMid = 0.5 * (w.zStart + zEndOld)
+        zMagNew = zMagOld * pzm
+        new.zStep = zMagNew / (NewNz - 1)
+        if pzd == 1:
+            new.zStep = w.zStep
+            zMagNew = (NewNz - 1) * new.zStep
+        new.zStart = zMid - 0.5 * zMagNew
+        new.AuxLong3 = 0
+        new.AuxLong4 = NewNz - 1
+        if new.zStart > new.zWfrMin:
+            new.zWfrMin = new.zStart
+        if (new.zStart + zMagNew) < new.zWfrMax:
+            new.zWfrMax = new.zStart + zMagNew
+
+    grow = (pxmIn * pxdIn * pzmIn * pzdIn) >= 1.
+    if grow and changed:
+        new.srwl_roundtrip()                         # ModifyWfrNeNxNz before the core
+    # RadResizeCore (sroptelm.cpp:3038)
+    RelStepTol = 1.e-05
+    only_larger = (pxd == 1. and pzd == 1. and pxm >= 1. and pzm >= 1.) and \
+        (abs(old.xStep - new.xStep) < RelStepTol and abs(old.zStep - new.zStep) < RelStepTol)
+    if only_larger:
+        ex, ey = _resize_core_only_larger_range(old, new)
+    else:
+        treated = False
+        origQX, origQZ = old.QuadX, old.QuadZ
+        if _wavefront_term_can_be_treated(old) and old.Pres < 1:
+            new.QuadX, new.QuadZ = old.QuadX, old.QuadZ
+            _treat_strongly_oscillating(old, 'r')
+            treated = True
+        ex, ey = _resize_core(old, new, treated)
+        new.ex, new.ey = ex, ey
+        if treated:
+            _treat_strongly_oscillating(new, 'a')
+            ex, ey = new.ex, new.ey
+        new.QuadX, new.QuadZ = origQX, origQZ
+    new.ex, new.ey = ex, ey
+    if (not grow) and changed:
+        new.srwl_roundtrip()                         # ModifyWfrNeNxNz after the core
+    for k, v in new.__dict__.items():
+        setattr(w, k, v)
+    if other_side:
+        to = 1 if w.Pres == 0 else 0
+        set_rad_repres(w, to)
+        if useStartTrOther:
+            xcOld = xStartOld + (nxOld >> 1) * xStepOld
+            w.xStart = xcOld - (w.nx >> 1) * w.xStep
+            zcOld = zStartOld + (nzOld >> 1) * zStepOld
+            w.zStart = zcOld - (w.nz >> 1) * w.zStep
+            w.set_full_range()
+
+
+# ----------------------------------------------------------------------------------------
+# Container (srTCompositeOptElem, cpp/src/core/sroptcnt.cpp:87-425)
+# ----------------------------------------------------------------------------------------
+
+
+def _pp(pp, i, default):
+    return pp[i] if (pp is not None and len(pp) > i) else default
+
+
+def propagate(w: Wfr, elements, props):
+    """srTCompositeOptElem ctor (sroptcnt.cpp:87-221) + PropagateRadiationGuided (:254-425).
+
+    ``elements``: list of tuples ('drift', L, treat) | ('aperture', shape, ap_or_ob, Dx, Dy, x, y)
+    | ('lens', Fx, Fy, x, y).  ``props``: list of per-element propagation parameter lists
+    (len(props) may be len(elements)+1 for a post-resize)."""
+    if (w.nx <= 1) or (w.nz <= 1):
+        raise ValueError("CAN_NOT_PROPAGATE_1D_RAD")
+    tolRes = 1.e-04
+    for i, el in enumerate(elements):
+        pp = props[i] if i < len(props) else None
+        anal = 0
+        if pp is not None:
+            if int(_pp(pp, 0, 0)) or int(_pp(pp, 1, 0)):
+                raise NotImplementedError("auto-resize (pp[0]/pp[1]) is not restated")
+            anal = int(_pp(pp, 3, 0))
+            pxm, pxd, pzm, pzd = _pp(pp, 5, 1.), _pp(pp, 6, 1.), _pp(pp, 7, 1.), _pp(pp, 8, 1.)
+            shift = int(_pp(pp, 9, 0))
+            if abs(pxd - 1.) > tolRes or abs(pxm - 1.) > tolRes or abs(pzd - 1.) > tolRes or \
+                    abs(pzm - 1.) > tolRes or shift > 0:
+                rad_resize_gen(w, pxm, pxd, pzm, pzd, shift, _pp(pp, 10, 0.), _pp(pp, 11, 0.),
+                               other_side=bool(int(_pp(pp, 4, 0))))
+        kind = el[0]
+        if kind == 'drift':
+            drift(w, el[1], el[2], anal)
+        elif kind == 'lens':
+            lens(w, el[1], el[2], el[3], el[4])
+        elif kind == 'aperture':
+            aperture(w, el[1], el[2], el[3], el[4], el[5], el[6])
+        else:
+            raise ValueError("UNKNOWN_OPTICAL_ELEMENT")
+    n = len(elements)
+    if n < len(props):
+        pp = props[n]
+        pxm, pxd, pzm, pzd = _pp(pp, 5, 1.), _pp(pp, 6, 1.), _pp(pp, 7, 1.), _pp(pp, 8, 1.)
+        if abs(pxd - 1.) > tolRes or abs(pxm - 1.) > tolRes or abs(pzd - 1.) > tolRes or abs(pzm - 1.) > tolRes:
+            rad_resize_gen(w, pxm, pxd, pzm, pzd, other_side=bool(int(_pp(pp, 4, 0))))
+    return w

@@ -1,0 +1,189 @@
+"""Generates the golden fixtures in tests/golden/ by running the reference SRW itself.
+
+Run in a container that has the reference sources (default /root/reference) and the reference
+built by ``make -C oracle`` (oracle/_ref/srwlpy.so, oracle/_ref/nextfft_probe):
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+Outputs (committed):
+  good_numbers.txt      runs "first last result" of NextCorrectNumberForFFT(n), n <= 300000
+  cases.npz             per case: input field + wavefront scalars, beamline, and the reference's
+                        output field, mesh, Rx/Ry/dRx/dRy/xc/yc and moments (float32 fields)
+The cases are small (<= 128^2 inputs) so the CPU tests finish in seconds.  Nothing in the
+product reads this script; the GPU box never runs it.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+from array import array
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def load_reference(ref):
+    sys.path.insert(0, os.path.join(REPO, 'oracle', '_ref'))
+    sys.path.insert(0, os.path.join(ref, 'env', 'python', 'srwpy'))
+    import srwlpy  # noqa: F401  (the reference extension built from source)
+    import srwlib
+    return srwlib
+
+
+def gaussian_wfr(L, E, sig, nx, ny, xr, yr, z=0.):
+    """Gaussian beam at its waist through the reference's CalcElecFieldGaussian, precPar=[0]."""
+    gb = L.SRWLGsnBm()
+    gb.x = gb.y = 0.; gb.xp = gb.yp = 0.
+    gb.avgPhotEn = E; gb.pulseEn = 0.001; gb.repRate = 1; gb.polar = 1
+    gb.sigX = sig; gb.sigY = sig; gb.sigT = 10e-15; gb.mx = 0; gb.my = 0
+    w = L.SRWLWfr(); w.allocate(1, nx, ny)
+    m = w.mesh
+    m.zStart = z; m.eStart = E; m.eFin = E
+    m.xStart, m.xFin, m.yStart, m.yFin = -xr, xr, -yr, yr
+    w.partBeam.partStatMom1.x = 0.; w.partBeam.partStatMom1.y = 0.; w.partBeam.partStatMom1.z = 0.
+    w.partBeam.partStatMom1.xp = 0.; w.partBeam.partStatMom1.yp = 0.
+    L.srwl.CalcElecFieldGaussian(w, gb, [0])
+    return w
+
+
+def undulator_wfr(L, nx, ny, xr=1.5e-3, yr=1.5e-3, z=20., npTraj=20000):
+    """Planar undulator (3 GeV, 0.5 A filament, 20 mm x 100 periods, K=1.5) first harmonic at z."""
+    per, nper, K = 0.02, 100, 1.5
+    By = K / (0.0934 * per * 1000.)
+    und = L.SRWLMagFldU([L.SRWLMagFldH(1, 'v', By, 0, 1, 1)], per, nper)
+    mag = L.SRWLMagFldC([und], array('d', [0]), array('d', [0]), array('d', [0]))
+    eb = L.SRWLPartBeam()
+    eb.Iavg = 0.5
+    eb.partStatMom1.x = 0.; eb.partStatMom1.y = 0.
+    eb.partStatMom1.z = -0.5 * per * (nper + 4)
+    eb.partStatMom1.xp = 0.; eb.partStatMom1.yp = 0.
+    eb.partStatMom1.gamma = 3. / 0.51099890221e-03
+    gam2 = eb.partStatMom1.gamma ** 2
+    lam1 = per / (2. * gam2) * (1. + K * K / 2.)
+    E1 = 1.239842e-06 / lam1
+    w = L.SRWLWfr(); w.allocate(1, nx, ny)
+    m = w.mesh
+    m.zStart = z; m.eStart = E1; m.eFin = E1
+    m.xStart, m.xFin, m.yStart, m.yFin = -xr, xr, -yr, yr
+    w.partBeam = eb
+    L.srwl.CalcElecFieldSR(w, 0, mag, [1, 0.01, 0., 0., npTraj, 1, 0])
+    return w
+
+
+def impose_radius(w, R, dR):
+    """Multiplies the field by exp(+i pi r^2/(lambda R)) and sets Rx=Ry=R, dRx=dRy=dR."""
+    nx, ny = w.mesh.nx, w.mesh.ny
+    x = np.linspace(w.mesh.xStart, w.mesh.xFin, nx)[None, :]
+    y = np.linspace(w.mesh.yStart, w.mesh.yFin, ny)[:, None]
+    lam = 1.239842e-06 / w.mesh.eStart
+    ph = np.exp(1j * np.pi * (x * x + y * y) / (lam * R))
+    for name in ('arEx', 'arEy'):
+        a = np.array(getattr(w, name), np.float32)
+        c = (a[0::2] + 1j * a[1::2]).reshape(ny, nx) * ph
+        b = np.empty(2 * nx * ny, np.float32)
+        b[0::2] = c.real.ravel(); b[1::2] = c.imag.ravel()
+        setattr(w, name, array('f', b.tobytes()))
+    w.Rx = w.Ry = R
+    w.dRx = w.dRy = dR
+
+
+def build_beamline(L, elems):
+    opts = []
+    for e in elems:
+        if e[0] == 'drift':
+            opts.append(L.SRWLOptD(e[1], e[2]) if len(e) > 2 else L.SRWLOptD(e[1]))
+        elif e[0] == 'aperture':
+            opts.append(L.SRWLOptA(e[1], e[2], e[3], e[4], e[5], e[6]))
+        elif e[0] == 'lens':
+            opts.append(L.SRWLOptL(e[1], e[2], e[3], e[4]))
+    return opts
+
+
+def snapshot(w):
+    ex = np.array(w.arEx, np.float32)
+    ey = np.array(w.arEy, np.float32)
+    m = w.mesh
+    return dict(ex=ex, ey=ey,
+                mesh=np.array([m.nx, m.ny, m.xStart, m.xFin, m.yStart, m.yFin, m.eStart, m.zStart], np.float64),
+                scal=np.array([w.Rx, w.Ry, w.dRx, w.dRy, w.xc, w.yc, w.avgPhotEn, w.presCA], np.float64),
+                momx=np.array(w.arMomX, np.float64)[:11], momy=np.array(w.arMomY, np.float64)[:11])
+
+
+PP0 = [0, 0, 1, 0, 0, 1., 1., 1., 1., 0, 0, 0]
+
+
+def cases(L):
+    """(name, wavefront factory, elements, propagation parameter lists)."""
+    pp = lambda anal=0, pxm=1., pxd=1., pzm=1., pzd=1.: [0, 0, 1., anal, 0, pxm, pxd, pzm, pzd, 0, 0, 0]
+    c0 = [('drift', 10., 0), ('aperture', 'r', 'a', 1e-3, 1e-3, 0., 0.), ('lens', 5., 5., 0., 0.), ('drift', 5., 0)]
+    c1 = [('aperture', 'c', 'a', 0.8e-3, 0.8e-3, 0., 0.), ('lens', 10., 10., 0., 0.), ('drift', 10., 0)]
+    c1pp = [pp(), pp(0, 2., 2., 2., 2.), pp(4)]
+    c2 = [('drift', 30., 0), ('lens', 15., 15., 0., 0.), ('drift', 30., 0)]
+    c2pp = [pp(2), pp(), pp(2)]
+
+    def g0(n):
+        return lambda: gaussian_wfr(L, 1000., 50e-6, n, n, 1e-3, 1e-3)
+
+    def g2(n, r):
+        def f():
+            w = gaussian_wfr(L, 10000., 20e-6, n, n, r, r)
+            impose_radius(w, 30., 0.3)
+            return w
+        return f
+    out = [
+        ('c0_64', g0(64), c0, [PP0] * 4),
+        ('c0_128', g0(128), c0, [PP0] * 4),
+        ('c0_ragged_96x80', lambda: gaussian_wfr(L, 1000., 50e-6, 96, 80, 1e-3, 0.9e-3), c0, [PP0] * 4),
+        ('c1_64', lambda: undulator_wfr(L, 64, 64, npTraj=4000), c1, c1pp),
+        ('c1_96', lambda: undulator_wfr(L, 96, 96, npTraj=4000), c1, c1pp),
+        ('c2_128', g2(128, 0.5e-3), c2, c2pp),
+        # resize variants and edge cases of the mesh logic
+        ('rs_shrink', g0(128), [('drift', 3., 0)], [pp(0, 0.5, 1., 0.5, 1.)]),
+        ('rs_res_only', g0(64), [('drift', 3., 0)], [pp(0, 1., 2., 1., 1.5)]),
+        ('rs_range_only', g0(64), [('drift', 3., 0)], [pp(0, 2., 1., 1.5, 1.)]),
+        ('rs_post', g0(64), [('drift', 3., 0)], [pp(), pp(0, 1.3, 1.7, 1.2, 1.1)]),
+        ('ob_circ_lens_offc', g0(96), [('aperture', 'c', 'o', 0.3e-3, 0.3e-3, 0.1e-3, 0.), ('drift', 2., 0),
+                                      ('lens', 3., 4., 0.2e-3, -0.1e-3), ('drift', 2., 0)], [PP0] * 4),
+        ('rect_ob_towaist', g2(96, 0.5e-3), [('aperture', 'r', 'o', 0.2e-3, 0.1e-3, 0., 0.), ('lens', 20., 20., 0., 0.),
+                                             ('drift', 12., 0)], [pp(), pp(), pp(4)]),
+        ('quad_neg_k', g2(96, 0.5e-3), [('drift', -45., 0)], [pp(2)]),
+        ('treat_path', g0(64), [('drift', 2., 1)], [pp()]),
+    ]
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--ref', default='/root/reference')
+    a = ap.parse_args()
+    L = load_reference(a.ref)
+    # 1) good numbers
+    probe = os.path.join(REPO, 'oracle', '_ref', 'nextfft_probe')
+    txt = subprocess.run([probe, '300000'], capture_output=True, text=True, check=True).stdout
+    with open(os.path.join(HERE, 'good_numbers.txt'), 'w') as f:
+        f.write(txt)
+    # 2) propagation cases
+    blob = {}
+    index = []
+    for name, make, elems, pps in cases(L):
+        w = make()
+        inp = snapshot(w)
+        opt = L.SRWLOptC(build_beamline(L, elems), [list(map(float, p)) for p in pps])
+        L.srwl.PropagElecField(w, opt)
+        out = snapshot(w)
+        for k, v in inp.items():
+            blob[name + '/in/' + k] = v
+        for k, v in out.items():
+            blob[name + '/out/' + k] = v
+        index.append(dict(name=name, elements=[list(e) for e in elems], props=[list(map(float, p)) for p in pps]))
+        print(name, 'in', int(inp['mesh'][0]), int(inp['mesh'][1]), 'out', int(out['mesh'][0]), int(out['mesh'][1]),
+              'R', out['scal'][0], out['scal'][1])
+    blob['index'] = np.array(json.dumps(index))
+    np.savez_compressed(os.path.join(HERE, 'cases.npz'), **blob)
+
+
+if __name__ == '__main__':
+    main()

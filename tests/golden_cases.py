@@ -1,0 +1,44 @@
+"""Loads the golden fixtures made by tests/golden/make_golden.py (outputs of the reference SRW
+built from source) and runs the FP64 oracle on them.  Test helper; not product code."""
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, 'golden', 'cases.npz')
+
+
+def cplx(a, nx, ny):
+    a = np.asarray(a, np.float64)
+    return (a[0::2] + 1j * a[1::2]).reshape(ny, nx)
+
+
+def load():
+    d = np.load(GOLDEN)
+    return d, json.loads(str(d['index']))
+
+
+def mesh_dict(m):
+    return dict(nx=int(m[0]), ny=int(m[1]), xStart=float(m[2]), xFin=float(m[3]), yStart=float(m[4]),
+                yFin=float(m[5]), eStart=float(m[6]), eFin=float(m[6]), zStart=float(m[7]))
+
+
+def rel_l2(a, b):
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / nb) if nb > 0 else float(np.linalg.norm(a))
+
+
+def case_io(d, name):
+    """(input dict, expected output dict) for one golden case."""
+    def side(s):
+        m = d[name + '/' + s + '/mesh']
+        sc = d[name + '/' + s + '/scal']
+        nx, ny = int(m[0]), int(m[1])
+        return dict(mesh=mesh_dict(m), ex=cplx(d[name + '/' + s + '/ex'], nx, ny),
+                    ey=cplx(d[name + '/' + s + '/ey'], nx, ny), Rx=float(sc[0]), Ry=float(sc[1]),
+                    dRx=float(sc[2]), dRy=float(sc[3]), xc=float(sc[4]), yc=float(sc[5]),
+                    presCA=int(sc[7]), momX=np.array(d[name + '/' + s + '/momx']),
+                    momY=np.array(d[name + '/' + s + '/momy']),
+                    mesh_raw=np.array(m[:6]))
+    return side('in'), side('out')

@@ -1,0 +1,364 @@
+"""Benchmark: plain single-wavefront propagation of the 1024^2 undulator beamline on B200.
+
+Workload (the configuration the headline metric is quoted on): a 1024x1024 complex-FP32
+undulator-like wavefront (first harmonic of a 3 GeV, K=1.5, 100 x 20 mm planar undulator seen at
+20 m, 2012 eV, +-1.5 mm; synthetic, see synth_undulator_field) through a 0.8 mm circular aperture,
+a thin lens f=10 m with range x2 / resolution x2 resizing before it (-> 4096^2), and a 10 m drift
+to the waist (to-waist mode).  One step = one propagation of one wavefront.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line.  ``value`` is propagations/s with the field resident in HBM; ``e2e`` is the
+same through the srwlpy-compatible C-ABI call with pinned host buffers (H2D of the input and D2H of
+the 4096^2 result inside the timed region).  ``--impl reference`` times the reference SRW (built
+from source, FFTW3 CPU path) on the host cores.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "propagations/s at 1024² FP32, batched+learned vs plain GPU at ≤1e-3 rel err"
+UNIT = "propagations/s"
+WORKLOAD = ("undulator beamline: 1024x1024 complex FP32 field (2012 eV, +-1.5 mm, R=20 m) -> circular aperture "
+            "0.8 mm -> resize x2 range x2 resolution (4096x4096) -> thin lens f=10 m -> drift 10 m to waist; "
+            "plain single-wavefront path")
+PEAKS = os.path.join(HERE, 'MEASURED_PEAKS.json')
+
+
+# ------------------------------------------------------------------------------------------------
+# synthetic input (same for both arms)
+# ------------------------------------------------------------------------------------------------
+def synth_undulator_field(n=1024, r=1.5e-3, z=20.):
+    """Undulator-like first-harmonic field at distance z: on-resonance detuning ring structure
+    sinc(q) exp(-i pi q), q = N gamma^2 theta^2 / (1 + K^2/2), on a spherical wave of radius z,
+    plus a weak vertical component.  Deterministic (no RNG)."""
+    per, nper, K = 0.02, 100, 1.5
+    gam = 3. / 0.51099890221e-03
+    lam1 = per / (2. * gam * gam) * (1. + K * K / 2.)
+    E = 1.239842e-06 / lam1
+    x = np.linspace(-r, r, n)
+    X, Y = np.meshgrid(x, x)
+    th2 = (X * X + Y * Y) / (z * z)
+    q = nper * gam * gam * th2 / (1. + K * K / 2.)
+    amp = 3.0e7 * np.sinc(q) * np.exp(-1j * np.pi * q)
+    sph = np.exp(1j * np.pi * (X * X + Y * Y) / (lam1 * z))
+    ex = (amp * sph).astype(np.complex64)
+    ey = (0.02 * amp * sph * (X * Y) / (r * r)).astype(np.complex64)
+    mesh = dict(nx=n, ny=n, xStart=-r, xFin=r, yStart=-r, yFin=r, eStart=E, eFin=E, zStart=z)
+    return ex, ey, mesh, dict(Rx=z, Ry=z, dRx=0.01 * z, dRy=0.01 * z)
+
+
+def beamline_objs(mod):
+    """C1 beamline with classes from module `mod` (srw_b200.srwlib, or the reference's when given)."""
+    pp = lambda anal=0, pxm=1., pxd=1., pzm=1., pzd=1.: [0, 0, 1., anal, 0, pxm, pxd, pzm, pzd, 0, 0, 0]  # noqa: E731
+    return mod.SRWLOptC([mod.SRWLOptA('c', 'a', 0.8e-3, 0.8e-3), mod.SRWLOptL(10., 10.), mod.SRWLOptD(10.)],
+                        [pp(), pp(0, 2., 2., 2., 2.), pp(4)])
+
+
+def make_wfr(mod, ex, ey, mesh, sc, alloc=None):
+    w = mod.SRWLWfr()
+    w.allocate(1, mesh['nx'], mesh['ny'])
+    for name, f in (('arEx', ex), ('arEy', ey)):
+        a = np.empty(2 * f.size, np.float32) if alloc is None else alloc(2 * f.size)
+        a[0::2] = f.real.ravel()
+        a[1::2] = f.imag.ravel()
+        setattr(w, name, a)
+    for k in ('xStart', 'xFin', 'yStart', 'yFin', 'eStart', 'eFin', 'zStart'):
+        setattr(w.mesh, k, mesh[k])
+    w.Rx, w.Ry, w.dRx, w.dRy = sc['Rx'], sc['Ry'], sc['dRx'], sc['dRy']
+    return w
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler(object):
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.idx), '--query-gpu=' + self.Q,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(',')])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace('.', '', 1).isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace('.', '', 1).isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({names[k] for r in self.rows if len(r) > 8 for k in range(4) if r[5 + k] == 'Active'})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------------------------------------
+# reference arm: the reference SRW built from source (oracle/_ref/srwlpy.so), CPU
+# ------------------------------------------------------------------------------------------------
+def _ref_worker(args):
+    """One propagation with the reference's own srwlpy (runs in a spawned process)."""
+    ref_dir, n = args
+    sys.path.insert(0, ref_dir)
+    import srwlpy
+    from srw_b200 import srwlib as mod          # plain Python structures with the reference's names
+    ex, ey, mesh, sc = synth_undulator_field(n)
+    w = make_wfr(mod, ex, ey, mesh, sc)
+    t = time.perf_counter()
+    srwlpy.PropagElecField(w, beamline_objs(mod))
+    return time.perf_counter() - t, int(w.mesh.nx)
+
+
+def reference_available():
+    d = os.path.join(HERE, 'oracle', '_ref')
+    return d if os.path.exists(os.path.join(d, 'srwlpy.so')) else None
+
+
+def cpu_baseline_sample(n_props=2, procs=1):
+    """Times the reference CPU path on the same workload; returns the cpu_baseline object."""
+    import multiprocessing as mp
+    ref = reference_available()
+    if ref is None:
+        return None
+    ctx = mp.get_context('spawn')
+    with ctx.Pool(procs) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_ref_worker, [(ref, 1024)] * (n_props * procs))
+        wall = time.perf_counter() - t0
+    return {"value": len(res) / wall, "unit": UNIT, "cores": procs, "kind": "reference",
+            "sample": "%d full propagations of the same 1024^2 workload with the reference SRW (FFTW3 build from "
+                      "source, single-threaded per process, %d process(es)); median per-propagation %.2f s"
+                      % (len(res), procs, statistics.median([r[0] for r in res]))}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    ref = reference_available()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/srwlpy.so not present"}))
+        return
+    import multiprocessing as mp
+    procs = max(1, min(os.cpu_count() or 1, 16))
+    ctx = mp.get_context('spawn')
+    times = []
+    with ctx.Pool(procs) as pool:
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_ref_worker, [(ref, 1024)] * procs)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                times.append(dt)
+    total = sum(times)
+    value = procs * len(times) / total
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000. * total / len(times), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "step": "%d concurrent reference propagations (one per process)" % procs},
+           "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                            "sample": "each step: %d processes x 1 propagation of the full workload" % procs},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+# ------------------------------------------------------------------------------------------------
+# our arm
+# ------------------------------------------------------------------------------------------------
+def kernel_bytes(k):
+    """Algorithmic bytes of one pass (both components, read + write, complex FP32)."""
+    if k[0] == 'resize':
+        return 2 * 8 * (k[1] * k[2] + k[3] * k[4])
+    return 2 * 8 * 2 * k[1] * k[2]
+
+
+def run_ours(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from srw_b200 import srwlib as mod
+    from srw_b200 import srwlpy as srwl
+    from srw_b200.plan import Plan
+
+    dev = torch.device('cuda', int(os.environ.get('LOCAL_RANK', 0)))
+    torch.cuda.set_device(dev)
+    ex, ey, mesh, sc = synth_undulator_field(1024)
+    w = make_wfr(mod, ex, ey, mesh, sc)
+    plan = Plan(w, beamline_objs(mod), device=dev.index)
+    dex = torch.from_numpy(ex).to(dev)
+    dey = torch.from_numpy(ey).to(dev)
+    ox, oy = plan.new_output()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)    # > L2 (126 MB)
+    stream = torch.cuda.current_stream(dev)
+    kinfo = plan.kernels()
+
+    for _ in range(args.warmup):
+        plan.execute(dex, dey, ox, oy)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+
+    step_ms, kern_ms = [], []
+    with ClockSampler(dev.index) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)                                  # L2 flush between steps (outside the events)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            kern_ms.append(plan.execute_timed(dex, dey, ox, oy, stream))
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize(dev)
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    value = world * args.steps / (total_ms / 1000.)
+
+    # roofline of the dominant pass (live, same timed steps)
+    per_k = np.mean(np.array(kern_ms), axis=0)
+    kd = int(np.argmax(per_k))
+    alg = kernel_bytes(kinfo[kd])
+    achieved = alg / (per_k[kd] / 1000.) / 1e9
+    peak, peak_src = 6650., 'fallback'
+    if os.path.exists(PEAKS):
+        peak, peak_src = float(json.load(open(PEAKS))['hbm_gbs']), 'measured'
+    total_alg = sum(kernel_bytes(k) for k in kinfo)
+
+    # e2e through the C-ABI (host buffers in pinned memory; H2D + D2H inside the timed region)
+    pinned = []
+
+    def palloc(n):
+        t = torch.empty(n, dtype=torch.float32).pin_memory()
+        pinned.append(t)
+        return t.numpy()
+
+    class PinnedWfr(mod.SRWLWfr):
+        def allocate(self, _ne, _nx, _ny, _EXNeeded=1, _EYNeeded=1, _typeE='f', _backupNeeded=0):
+            mod.SRWLWfr.allocate(self, _ne, 0, 0, _EXNeeded, _EYNeeded, _typeE, _backupNeeded)
+            if _EXNeeded:
+                self.arEx = out_bufs[0]
+            if _EYNeeded:
+                self.arEy = out_bufs[1]
+            self.mesh.nx, self.mesh.ny = _nx, _ny
+
+    out_bufs = [palloc(2 * plan.nx_out * plan.ny_out), palloc(2 * plan.nx_out * plan.ny_out)]
+    in_x, in_y = palloc(2 * ex.size), palloc(2 * ey.size)
+    in_x[0::2], in_x[1::2] = ex.real.ravel(), ex.imag.ravel()
+    in_y[0::2], in_y[1::2] = ey.real.ravel(), ey.imag.ravel()
+    bl = beamline_objs(mod)
+
+    def e2e_once():
+        wp = PinnedWfr()
+        wp.allocate(1, 1024, 1024)
+        wp.arEx, wp.arEy = in_x, in_y
+        for k in ('xStart', 'xFin', 'yStart', 'yFin', 'eStart', 'eFin', 'zStart'):
+            setattr(wp.mesh, k, mesh[k])
+        wp.Rx, wp.Ry, wp.dRx, wp.dRy = sc['Rx'], sc['Ry'], sc['dRx'], sc['dRy']
+        srwl.PropagElecField(wp, bl, None, dev.index + 1)
+        return wp
+
+    for _ in range(2):
+        e2e_once()
+    n_e2e = max(3, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        wp = e2e_once()
+        _ = float(wp.arEx[0])                                  # host read of the result
+    e2e_s = time.perf_counter() - t0
+    e2e_val = world * n_e2e / e2e_s
+
+    if rank != 0:
+        return
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(n_props=2, procs=1)
+    if cpu is None:
+        cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "reference build not present"}
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "grid_in": [1024, 1024], "grid_out": [plan.nx_out, plan.ny_out],
+                      "passes": plan.n_kernels, "algorithmic_bytes_per_step": total_alg,
+                      "l2": "256 MB buffer written between steps (outside the per-step CUDA events); working set "
+                            "768 MB > L2", "parallelism": "replicas" if world > 1 else "single GPU"},
+           "roofline": {"bound": "hbm", "kernel": "%s %s" % (kinfo[kd][0], 'x'.join(map(str, kinfo[kd][1:]))),
+                        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "peak_source": peak_src, "traffic": None,
+                        "algorithmic_bytes": alg, "avg_ms": float(per_k[kd]),
+                        "step_frac": (total_alg / (total_ms / args.steps / 1000.) / 1e9) / peak,
+                        "per_pass_ms": [round(float(v), 4) for v in per_k]},
+           "cpu_baseline": cpu,
+           "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * 1024 * 1024,
+                   "d2h_bytes_per_step": 2 * 8 * plan.nx_out * plan.ny_out,
+                   "path": "srw_b200.srwlpy.PropagElecField (C-ABI srwlPropagElecField), pinned host buffers"},
+           "clocks": clk.summary(),
+           "gpu_launches": plan.n_kernels * args.steps}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    if args.impl == 'reference':
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', 0)))
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,171 @@
+/*
+ * srwl_b200: B200-native (sm_100a) implementation of SRW's Fourier-optics wavefront
+ * propagation -- srwlPropagElecField over SRWLOptC chains of drifts, thin lenses and
+ * apertures/obstacles -- behind the reference's own C API.
+ *
+ * The structures below are declared with the same members, order and types as the reference's
+ * public header (cpp/src/lib/srwlib.h:75-94, 239-276, 302-327, 523-531), so a C client compiled
+ * against the reference header can link this library instead (the binary layouts agree).
+ * Only the members this path reads or writes are documented.
+ *
+ * Error convention (srwlib.h): 0 = success, > 0 error number, < 0 warning number.  Error
+ * numbers of the reference are kept; numbers >= 23900 are specific to this library.
+ */
+#ifndef SRWL_B200_H
+#define SRWL_B200_H
+
+#if defined(__GNUC__)
+#define SRWG_API __attribute__((visibility("default")))
+#else
+#define SRWG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+struct SRWLStructParticle {
+    double x, y, z;
+    double xp, yp;
+    double gamma;
+    double relE0;
+    int nq;
+};
+typedef struct SRWLStructParticle SRWLParticle;
+
+struct SRWLStructParticleBeam {
+    double Iavg;
+    double nPart;
+    SRWLParticle partStatMom1;
+    double arStatMom2[21];
+};
+typedef struct SRWLStructParticleBeam SRWLPartBeam;
+
+struct SRWLStructRadMesh {
+    double eStart, eFin, xStart, xFin, yStart, yFin, zStart;
+    long ne, nx, ny;
+    double nvx, nvy, nvz, hvx, hvy, hvz;
+    double* arSurf;
+    char type;
+    long long itStart, itFin;
+};
+typedef struct SRWLStructRadMesh SRWLRadMesh;
+
+struct SRWLStructWaveFront {
+    char *arEx, *arEy;           /* float32 [ny][nx][ne][re,im] each, host memory */
+    char *arExAux, *arEyAux;
+    SRWLRadMesh mesh;
+    double Rx, Ry;               /* instant wavefront radii */
+    double dRx, dRy;             /* their errors */
+    double xc, yc;               /* instant source centre */
+    double avgPhotEn;
+    char presCA;                 /* 0 coordinate, 1 angular representation */
+    char presFT;
+    char numTypeElFld;           /* 'f' */
+    char unitElFld;
+    char unitElFldAng;
+    SRWLPartBeam partBeam;
+    double* arElecPropMatr;
+    double *arMomX, *arMomY;     /* 11*ne statistical moments per component */
+    double* arWfrAuxData;
+};
+typedef struct SRWLStructWaveFront SRWLWfr;
+
+struct SRWLStructOpticsDrift {
+    double L;
+    char treat;
+};
+typedef struct SRWLStructOpticsDrift SRWLOptD;
+
+struct SRWLStructOpticsAperture {
+    char shape;                  /* 'r' rectangular, 'c' circular */
+    char ap_or_ob;               /* 'a' aperture, 'o' obstacle */
+    double Dx, Dy;
+    double x, y;
+};
+typedef struct SRWLStructOpticsAperture SRWLOptA;
+
+struct SRWLStructOpticsLens {
+    double Fx, Fy;
+    double x, y;
+};
+typedef struct SRWLStructOpticsLens SRWLOptL;
+
+struct SRWLStructOpticsContainer {
+    void** arOpt;                /* element pointers */
+    char** arOptTypes;           /* "drift", "aperture", "obstacle", "lens", "container" */
+    int nElem;
+    double** arProp;             /* per-element propagation parameter lists */
+    char* arPropN;               /* their lengths (9..17) */
+    int nProp;                   /* nElem or nElem+1 (post-resize) */
+};
+typedef struct SRWLStructOpticsContainer SRWLOptC;
+
+/* ---------------------------------------------------------------------------------------------
+ * Reference C API entry points (same signatures and semantics)
+ * ------------------------------------------------------------------------------------------- */
+
+/* Replaces srwlPropagElecField (cpp/src/lib/srwlib.h:821, srwlib.cpp:1023).  Propagates the
+ * wavefront in place through the optical container on the GPU (arParGPU = {nPar, device index
+ * (1-based)} or NULL for device 0).  Field arrays are host memory owned by the caller; when the
+ * mesh size changes the registered modification callback is called (action 2) to re-allocate
+ * them before the result is written back.  nInt/arID/arIM/arI (intermediate intensities) are
+ * not supported and must be 0.  Not thread-safe, like the reference. */
+SRWG_API int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SRWLRadMesh* arIM, char** arI,
+                        double* arParGPU);
+
+/* Replaces srwlUtiSetWfrModifFunc (srwlib.h:542): registers the client callback that
+ * re-allocates wavefront arrays (action 2: allocate for the current mesh; 12: with backup). */
+SRWG_API void srwlUtiSetWfrModifFunc(int (*pExtFunc)(int action, SRWLWfr* pWfrIn, char pol));
+
+/* Replaces srwlUtiGetErrText (srwlib.h:574): copies the text of error/warning number erNo to t
+ * (at least 2048 bytes). */
+SRWG_API int srwlUtiGetErrText(char* t, int erNo);
+
+/* ---------------------------------------------------------------------------------------------
+ * Extensions (no counterpart in the reference): plan once, execute on device-resident fields.
+ * ------------------------------------------------------------------------------------------- */
+
+typedef struct srwgPlan srwgPlan;
+
+/* Plans the propagation of a wavefront with pWfr's mesh and scalars (arrays are not read)
+ * through pOpt on device `device` (0-based): runs the reference's mesh/radius bookkeeping on
+ * the host and lowers the element chain into fused GPU passes. */
+SRWG_API int srwgPlanCreate(const SRWLWfr* pWfr, const SRWLOptC* pOpt, int device, srwgPlan** ppPlan);
+
+/* Writes the output mesh and scalars (Rx, Ry, dRx, dRy, xc, yc, presCA, moments when arMomX/Y
+ * are non-NULL) of the planned propagation into pWfrOut; field arrays are not touched. */
+SRWG_API int srwgPlanGetOutput(const srwgPlan* plan, SRWLWfr* pWfrOut);
+
+/* Input and output grid sizes, number of GPU kernels per execution, and the bytes of device
+ * work space the plan holds (two buffers of the largest grid, both components). */
+SRWG_API int srwgPlanInfo(const srwgPlan* plan, long* nxIn, long* nyIn, long* nxOut, long* nyOut, int* nKernels,
+                 long long* workBytes);
+
+/* Executes the plan on device arrays (interleaved complex FP32, [ny][nx]) on CUDA stream
+ * `stream` (NULL = default stream).  dExIn/dEyIn are read only; the result (output mesh) is
+ * written to dExOut/dEyOut, which must hold nxOut*nyOut complex values each. */
+SRWG_API int srwgPlanExecute(srwgPlan* plan, const float* dExIn, const float* dEyIn, float* dExOut, float* dEyOut,
+                    void* stream);
+
+/* Executes the plan on a batch of n wavefronts of the same mesh: wavefront b reads
+ * dExIn + b*strideIn (floats) and writes dExOut + b*strideOut. */
+SRWG_API int srwgPlanExecuteBatch(srwgPlan* plan, int n, const float* dExIn, const float* dEyIn, long long strideIn,
+                         float* dExOut, float* dEyOut, long long strideOut, void* stream);
+
+/* As srwgPlanExecute, and records a CUDA event pair around every pass on `stream`; waits for
+ * the stream and writes each pass's duration in milliseconds to kernelMs[0 .. nKernels-1]
+ * (at most maxKernels values).  Returns the number of passes in *nTimed. */
+SRWG_API int srwgPlanExecuteTimed(srwgPlan* plan, const float* dExIn, const float* dEyIn, float* dExOut,
+                                  float* dEyOut, void* stream, float* kernelMs, int maxKernels, int* nTimed);
+
+SRWG_API int srwgPlanDestroy(srwgPlan* plan);
+
+/* Human-readable list of the planned passes (one line per kernel) into buf. */
+SRWG_API int srwgPlanDescribe(const srwgPlan* plan, char* buf, int bufLen);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SRWL_B200_H */

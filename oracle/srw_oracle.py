@@ -35,7 +35,7 @@ import numpy as np
 
 def _good_numbers():
     """Even n <= 100000 of the form 2^a 3^b 5^c 7^d 11^e 13^f with e, f <= 1 (the reference's
-    table at gmfft.cpp:26 is exactly this set; pinned by tests/golden/good_numbers.json)."""
+    table at gmfft.cpp:26 is exactly this set; pinned by tests/golden/good_numbers.txt)."""
     out = []
     for n in range(2, 100001, 2):
         m = n
@@ -752,7 +752,15 @@ def _resize_core(old: Wfr, new: Wfr, quad_treat):
         rel = np.where(ic == 0, rel - step_old, rel)
         return ic, st, rel * inv
     ixc, ixst, xr = axis(ix, new.xStart, new.xStep, old.xStart, old.xStep, xStepInv, old.nx)
-    izc, izst, zr = axis(iz, new.zStart, new.zStep, old.zStart, old.zStep, zStepInv, old.nz)
+    izc_all, izst_all, zr_all = axis(iz, new.zStart, new.zStep, old.zStart, old.zStep, zStepInv, old.nz)
+    CH = max(1, 2 ** 22 // max(1, ix.size))          # rows per chunk (bounded memory)
+    for z0 in range(0, iz.size, CH):
+        sl = slice(z0, min(iz.size, z0 + CH))
+        _resize_rows(old, outx, outy, ix, iz[sl], ixc, ixst, xr, izc_all[sl], izst_all[sl], zr_all[sl], ixS, izS + z0)
+    return outx, outy
+
+
+def _resize_rows(old, outx, outy, ix, iz, ixc, ixst, xr, izc, izst, zr, ixS, izS):
     wx = _lagrange4(xr)          # [4, nX]
     wz = _lagrange4(zr)          # [4, nZ]
     irx = np.clip(ixc - ixst, 0, 2)
@@ -788,8 +796,7 @@ def _resize_core(old: Wfr, new: Wfr, quad_treat):
         FI = np.where(low, FIL, FI)
         app = np.abs(F) ** 2
         fac = np.where(app != 0., np.sqrt(np.where(app != 0., FI / np.where(app != 0., app, 1.), 1.)), 1.)
-        dst[izS:izE + 1, ixS:ixE + 1] = F * fac
-    return outx, outy
+        dst[izS:izS + iz.size, ixS:ixS + ix.size] = F * fac
 
 
 def _resize_core_only_larger_range(old: Wfr, new: Wfr):

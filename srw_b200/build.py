@@ -1,0 +1,48 @@
+"""Builds the CUDA library in-tree: srw_b200/_lib/libsrwl_b200.so (sm_100a).
+
+    python -m srw_b200.build          # or srw_b200.build.build()
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, 'csrc')
+OUT_DIR = os.path.join(HERE, '_lib')
+LIB = os.path.join(OUT_DIR, 'libsrwl_b200.so')
+NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+SOURCES = ['kernels.cu', 'planner.cpp', 'capi.cpp']
+# host code: no FP contraction so the mesh bookkeeping rounds exactly like the reference
+HOST_FLAGS = '-O2,-fPIC,-ffp-contract=off,-fvisibility=hidden'
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(' '.join(cmd) + '\n' + r.stdout + r.stderr)
+        raise RuntimeError('build step failed: ' + os.path.basename(cmd[-1]))
+    return r.stdout + r.stderr
+
+
+def build(verbose=False, ptxas_info=False):
+    os.makedirs(OUT_DIR, exist_ok=True)
+    objs = []
+    for s in SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(OUT_DIR, s + '.o')
+        cmd = [NVCC, '-c', '-O3', '-std=c++17', '-lineinfo', '-Xcompiler', HOST_FLAGS, '--fmad=true'] + ARCH + \
+              ['-I', CSRC, '-o', obj, src]
+        if ptxas_info and s.endswith('.cu'):
+            cmd.insert(1, '-Xptxas=-v')
+        out = _run(cmd)
+        if verbose or ptxas_info:
+            sys.stdout.write(out)
+        objs.append(obj)
+    # exported symbols: the C-ABI in include/srwl_b200.h
+    _run([NVCC, '-shared', '-o', LIB] + ARCH + objs + ['-lcudart'])
+    return LIB
+
+
+if __name__ == '__main__':
+    print(build(verbose=True, ptxas_info='-v' in sys.argv))

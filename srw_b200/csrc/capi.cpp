@@ -1,0 +1,457 @@
+// C-ABI of the library: the reference's srwlPropagElecField / srwlUtiSetWfrModifFunc /
+// srwlUtiGetErrText (cpp/src/lib/srwlib.h:542, 574, 821) and the srwgPlan* extensions, plus the
+// executor that runs a plan's passes on a CUDA stream.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/srwl_b200.h"
+#include "errors.h"
+#include "kernels.h"
+#include "planner.h"
+
+namespace srwg {
+
+static std::string g_lastDetail;                          // detail text of the last error
+static int (*g_modifFunc)(int, SRWLWfr*, char) = nullptr;  // client re-allocation callback
+static std::mutex g_mutex;
+
+struct DeviceCtx {
+    int dev = 0;
+    std::map<int, float2*> tw;          // twiddle tables by FFT length
+    float2* work = nullptr;             // 2 work buffers x 2 components
+    size_t workElems = 0;               // per buffer per component
+    float2* io = nullptr;               // input + output staging for the host-memory entry point
+    size_t ioElems = 0;
+    cudaStream_t stream = nullptr;
+};
+static std::map<int, DeviceCtx*> g_ctx;
+
+#define CUDA_TRY(x)                                                                     \
+    do {                                                                                \
+        cudaError_t e__ = (x);                                                          \
+        if (e__ != cudaSuccess) {                                                       \
+            g_lastDetail = std::string(#x) + ": " + cudaGetErrorString(e__);            \
+            return SRWG_ERR_CUDA;                                                       \
+        }                                                                               \
+    } while (0)
+
+static int get_ctx(int dev, DeviceCtx** out)
+{
+    auto it = g_ctx.find(dev);
+    if (it != g_ctx.end()) {
+        CUDA_TRY(cudaSetDevice(dev));
+        *out = it->second;
+        return 0;
+    }
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        g_lastDetail = "no CUDA device available";
+        return SRWG_ERR_NO_DEVICE;
+    }
+    if (dev < 0 || dev >= n) {
+        g_lastDetail = "device index out of range";
+        return SRWG_ERR_NO_DEVICE;
+    }
+    CUDA_TRY(cudaSetDevice(dev));
+    DeviceCtx* c = new DeviceCtx();
+    c->dev = dev;
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    g_ctx[dev] = c;
+    *out = c;
+    return 0;
+}
+
+// exp(-2 pi i k/N) in FP64, rounded to FP32
+static int twiddles(DeviceCtx& c, int N, const float2** out)
+{
+    auto it = c.tw.find(N);
+    if (it != c.tw.end()) { *out = it->second; return 0; }
+    std::vector<float2> h(N);
+    for (int k = 0; k < N; k++) {
+        double a = -2. * M_PI * (double)k / (double)N;
+        h[k] = make_float2((float)cos(a), (float)sin(a));
+    }
+    float2* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, sizeof(float2) * N));
+    CUDA_TRY(cudaMemcpy(d, h.data(), sizeof(float2) * N, cudaMemcpyHostToDevice));
+    c.tw[N] = d;
+    *out = d;
+    return 0;
+}
+
+// radix schedule of an even N: power-of-two part in radix-16/8 stages (4/8-bit splits), then 3, 5, 7, 11, 13
+int radix_plan(int N, int* r)
+{
+    int n = N, p2 = 0, ns = 0;
+    while (n % 2 == 0) { n /= 2; p2++; }
+    int odd[32], no = 0;
+    const int primes[5] = {3, 5, 7, 11, 13};
+    for (int i = 0; i < 5; i++)
+        while (n % primes[i] == 0) { odd[no++] = primes[i]; n /= primes[i]; }
+    if (n != 1) return -1;
+    int bits[16], nb = 0;
+    while (p2 >= 4 && p2 != 5) {
+        if (p2 == 6) { bits[nb++] = 3; bits[nb++] = 3; p2 = 0; break; }
+        bits[nb++] = 4;
+        p2 -= 4;
+    }
+    if (p2 == 5) { bits[nb++] = 3; bits[nb++] = 2; p2 = 0; }
+    else if (p2 >= 1 && p2 <= 3) { bits[nb++] = p2; p2 = 0; }
+    for (int i = 0; i < nb; i++) r[ns++] = 1 << bits[i];
+    for (int i = 0; i < no; i++) r[ns++] = odd[i];
+    if (ns > SRWG_MAX_STAGES) return -1;
+    return ns;
+}
+
+static int line_config(const LineDesc& d, LineLaunch& p)
+{
+    p.d = d;
+    int N = d.axis == 0 ? d.nx : d.nz;
+    p.N = N;
+    p.nlines = d.axis == 0 ? d.nz : d.nx;
+    // T threads per line, at most 16 points each; G = threads per CTA / T groups work on the
+    // CTA's L lines in batches
+    int T = (N + 15) / 16;
+    T = ((T + 31) / 32) * 32;
+    if (T < 32) T = 32;
+    if (T > 512) { g_lastDetail = "FFT length above 8192"; return SRWG_ERR_UNSUPPORTED; }
+    p.T = T;
+    const size_t cap = SRWG_LINE_SMEM_MAX;
+    int L;
+    if (d.axis == 0) {
+        L = 256 / T > 1 ? 256 / T : 1;          // rows: ~256 threads, one batch
+        p.P = N;
+    } else {
+        L = 512 / T > 4 ? 512 / T : 4;          // columns: >= 4 per tile (32-byte row segments)
+        p.P = N + 1;
+    }
+    while (L > 1 && (size_t)L * p.P * sizeof(float2) > cap) L--;
+    p.L = L;
+    if ((size_t)p.L * p.P * sizeof(float2) > cap) { g_lastDetail = "line too long for shared memory"; return SRWG_ERR_UNSUPPORTED; }
+    int G = 512 / T;
+    if (G > L) G = L;
+    if (G < 1) G = 1;
+    p.G = G;
+    p.nst = radix_plan(N, p.radix);
+    if (p.nst < 0) { g_lastDetail = "FFT length is not 2^a 3^b 5^c 7^d 11^e 13^f"; return SRWG_ERR_UNSUPPORTED; }
+    return 0;
+}
+
+// runs the plan's passes: buffer 0 = input, 1/2 = work buffers; the last pass writes the output
+static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* inY, float2* outX, float2* outY,
+                   float2* work, size_t workElems, cudaStream_t st, cudaEvent_t* ev = nullptr)
+{
+    const size_t nOut = (size_t)pl.w.nx * pl.w.nz;
+    if (pl.kernels.empty()) {
+        CUDA_TRY(cudaMemcpyAsync(outX, inX, nOut * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(outY, inY, nOut * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+        return 0;
+    }
+    float2* wb[3][2] = {{nullptr, nullptr},
+                        {work, work + workElems},
+                        {work + 2 * workElems, work + 3 * workElems}};
+    const size_t nk = pl.kernels.size();
+    for (size_t i = 0; i < nk; i++) {
+        const KernelDesc& k = pl.kernels[i];
+        if (ev) CUDA_TRY(cudaEventRecord(ev[2 * i], st));
+        const float2* s0 = k.src == 0 ? inX : wb[k.src][0];
+        const float2* s1 = k.src == 0 ? inY : wb[k.src][1];
+        float2* d0 = (i + 1 == nk) ? outX : wb[k.dst][0];
+        float2* d1 = (i + 1 == nk) ? outY : wb[k.dst][1];
+        cudaError_t e = cudaSuccess;
+        if (k.kind == K_LINE) {
+            LineLaunch p;
+            memset(&p, 0, sizeof(p));
+            int r = line_config(k.line, p);
+            if (r) return r;
+            r = twiddles(c, p.N, &p.tw);
+            if (r) return r;
+            p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
+            e = launch_line(p, st);
+        } else if (k.kind == K_RESIZE) {
+            ResizeLaunch p;
+            memset(&p, 0, sizeof(p));
+            p.d = k.rs;
+            p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
+            p.xStepInvO = 1. / k.rs.xStepO;
+            p.zStepInvO = 1. / k.rs.zStepO;
+            e = launch_resize(p, st);
+        } else {
+            PwLaunch p;
+            memset(&p, 0, sizeof(p));
+            p.d = k.pwk;
+            p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
+            e = launch_pw(p, st);
+        }
+        if (e != cudaSuccess) {
+            g_lastDetail = std::string("kernel launch: ") + cudaGetErrorString(e);
+            return SRWG_ERR_CUDA;
+        }
+        if (ev) CUDA_TRY(cudaEventRecord(ev[2 * i + 1], st));
+    }
+    return 0;
+}
+
+static int ensure_work(DeviceCtx& c, size_t elems)
+{
+    if (c.workElems >= elems && c.work) return 0;
+    if (c.work) { cudaFree(c.work); c.work = nullptr; c.workElems = 0; }
+    CUDA_TRY(cudaMalloc(&c.work, 4 * elems * sizeof(float2)));
+    c.workElems = elems;
+    return 0;
+}
+
+static int ensure_io(DeviceCtx& c, size_t elems)
+{
+    if (c.ioElems >= elems && c.io) return 0;
+    if (c.io) { cudaFree(c.io); c.io = nullptr; c.ioElems = 0; }
+    CUDA_TRY(cudaMalloc(&c.io, 4 * elems * sizeof(float2)));
+    c.ioElems = elems;
+    return 0;
+}
+
+static void out_wfr(const Planner& pl, SRWLWfr* p)
+{   // OutSRWRadPtrs (srradstr.cpp:687): mesh and scalars
+    const WfrState& w = pl.w;
+    p->mesh.eStart = w.eStart;
+    p->mesh.eFin = w.eStart;
+    p->mesh.xStart = w.xStart;
+    p->mesh.xFin = w.xStart + w.xStep * (w.nx - 1);
+    p->mesh.yStart = w.zStart;
+    p->mesh.yFin = w.zStart + w.zStep * (w.nz - 1);
+    p->mesh.ne = 1;
+    p->mesh.nx = w.nx;
+    p->mesh.ny = w.nz;
+    p->Rx = w.RobsX; p->Ry = w.RobsZ;
+    p->dRx = w.RobsXAbsErr; p->dRy = w.RobsZAbsErr;
+    p->xc = w.xc; p->yc = w.zc;
+    p->presCA = (char)w.Pres;
+    p->avgPhotEn = w.avgPhotEn;
+}
+
+static void out_moments(const Planner& pl, SRWLWfr* p)
+{
+    if (p->arMomX) for (int i = 0; i < 11; i++) p->arMomX[i] = pl.w.momX[i];
+    if (p->arMomY) for (int i = 0; i < 11; i++) p->arMomY[i] = pl.w.momZ[i];
+}
+
+}  // namespace srwg
+
+using namespace srwg;
+
+struct srwgPlan {
+    Planner pl;
+    int device = 0;
+    DeviceCtx* ctx = nullptr;   // bound at the first execution
+};
+
+extern "C" {
+
+void srwlUtiSetWfrModifFunc(int (*pExtFunc)(int action, SRWLWfr* pWfrIn, char pol))
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    g_modifFunc = pExtFunc;
+}
+
+int srwlUtiGetErrText(char* t, int erNo)
+{
+    if (t == nullptr) return 0;
+    const char* s = nullptr;
+    switch (erNo) {
+    case 0: s = ""; break;
+    case MEMORY_ALLOCATION_FAILURE: s = "Memory allocation failure."; break;
+    case UNKNOWN_OPTICAL_ELEMENT: s = "Unknown optical element or incorrect optical element definition."; break;
+    case ERROR_IN_FFT: s = "Error in FFT."; break;
+    case CAN_NOT_PROPAGATE_1D_RAD: s = "Propagation needs more than one point in both the horizontal and the vertical direction."; break;
+    case SRWL_WFR_EXT_MODIF_FAILED: s = "The wavefront modification (re-allocation) callback failed."; break;
+    case SRWL_INCORRECT_PARAM_FOR_WFR_PROP: s = "Incorrect or insufficient parameters for wavefront propagation."; break;
+    case SRWL_WFR_EXT_FUNC_NOT_DEFINED: s = "No wavefront modification (re-allocation) callback is registered."; break;
+    case SRWG_ERR_UNSUPPORTED: s = "Not supported on the GPU propagation path"; break;
+    case SRWG_ERR_CUDA: s = "CUDA error"; break;
+    case SRWG_ERR_NO_DEVICE: s = "No usable CUDA device"; break;
+    case SRWG_ERR_BAD_ARG: s = "Invalid argument"; break;
+    default: s = "Unknown error or warning number."; break;
+    }
+    std::string txt(s);
+    if ((erNo >= SRWG_ERR_UNSUPPORTED && erNo <= SRWG_ERR_BAD_ARG) && !g_lastDetail.empty()) txt += ": " + g_lastDetail;
+    strncpy(t, txt.c_str(), 2047);
+    t[2047] = 0;
+    return 0;
+}
+
+int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SRWLRadMesh* arIM, char** arI,
+                        double* arParGPU)
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    g_lastDetail.clear();
+    if (pWfr == nullptr || pOpt == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
+    if (nInt != 0 && arID != nullptr && arI != nullptr) {
+        g_lastDetail = "intermediate intensity extraction (nInt > 0)";
+        return SRWG_ERR_UNSUPPORTED;
+    }
+    (void)arIM;
+    int dev = 0;
+    if (arParGPU != nullptr && arParGPU[0] >= 1. && arParGPU[1] >= 1.) dev = (int)arParGPU[1] - 1;
+    if (pWfr->arEx == nullptr && pWfr->arEy == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
+
+    Planner pl;
+    int r = pl.plan(pWfr, pOpt);
+    if (r) { g_lastDetail = pl.err; return r; }
+    DeviceCtx* c = nullptr;
+    r = get_ctx(dev, &c);
+    if (r) return r;
+    const size_t nIn = (size_t)pl.in.nx * pl.in.nz, nOut = (size_t)pl.w.nx * pl.w.nz;
+    r = ensure_io(*c, nIn > nOut ? nIn : nOut);
+    if (r) return r;
+    r = ensure_work(*c, (size_t)pl.maxElems);
+    if (r) return r;
+    float2* inX = c->io;
+    float2* inY = c->io + c->ioElems;
+    float2* outX = c->io + 2 * c->ioElems;
+    float2* outY = c->io + 3 * c->ioElems;
+    cudaStream_t st = c->stream;
+    if (pWfr->arEx) CUDA_TRY(cudaMemcpyAsync(inX, pWfr->arEx, nIn * sizeof(float2), cudaMemcpyHostToDevice, st));
+    else CUDA_TRY(cudaMemsetAsync(inX, 0, nIn * sizeof(float2), st));
+    if (pWfr->arEy) CUDA_TRY(cudaMemcpyAsync(inY, pWfr->arEy, nIn * sizeof(float2), cudaMemcpyHostToDevice, st));
+    else CUDA_TRY(cudaMemsetAsync(inY, 0, nIn * sizeof(float2), st));
+    r = execute(pl, *c, inX, inY, outX, outY, c->work, c->workElems, st);
+    if (r) return r;
+    bool hadX = pWfr->arEx != nullptr, hadY = pWfr->arEy != nullptr;
+    bool resized = (pl.w.nx != pl.in.nx) || (pl.w.nz != pl.in.nz);
+    out_wfr(pl, pWfr);
+    if (resized) {
+        CUDA_TRY(cudaStreamSynchronize(st));
+        if (g_modifFunc == nullptr) return SRWL_WFR_EXT_FUNC_NOT_DEFINED;
+        if ((*g_modifFunc)(2, pWfr, 0)) return SRWL_WFR_EXT_MODIF_FAILED;
+        out_wfr(pl, pWfr);
+    }
+    if (hadX && pWfr->arEx) CUDA_TRY(cudaMemcpyAsync(pWfr->arEx, outX, nOut * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    if (hadY && pWfr->arEy) CUDA_TRY(cudaMemcpyAsync(pWfr->arEy, outY, nOut * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    out_moments(pl, pWfr);
+    return 0;
+}
+
+int srwgPlanCreate(const SRWLWfr* pWfr, const SRWLOptC* pOpt, int device, srwgPlan** ppPlan)
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    g_lastDetail.clear();
+    if (ppPlan == nullptr) return SRWG_ERR_BAD_ARG;
+    *ppPlan = nullptr;
+    srwgPlan* p = new srwgPlan();
+    int r = p->pl.plan(pWfr, pOpt);
+    if (r) { g_lastDetail = p->pl.err; delete p; return r; }
+    p->device = device;
+    // validate every pass configuration up front
+    for (const KernelDesc& k : p->pl.kernels) {
+        if (k.kind == K_LINE) {
+            LineLaunch l;
+            memset(&l, 0, sizeof(l));
+            r = line_config(k.line, l);
+            if (r) { delete p; return r; }
+        }
+    }
+    *ppPlan = p;
+    return 0;
+}
+
+int srwgPlanGetOutput(const srwgPlan* plan, SRWLWfr* pWfrOut)
+{
+    if (plan == nullptr || pWfrOut == nullptr) return SRWG_ERR_BAD_ARG;
+    out_wfr(plan->pl, pWfrOut);
+    out_moments(plan->pl, pWfrOut);
+    return 0;
+}
+
+int srwgPlanInfo(const srwgPlan* plan, long* nxIn, long* nyIn, long* nxOut, long* nyOut, int* nKernels, long long* workBytes)
+{
+    if (plan == nullptr) return SRWG_ERR_BAD_ARG;
+    if (nxIn) *nxIn = plan->pl.in.nx;
+    if (nyIn) *nyIn = plan->pl.in.nz;
+    if (nxOut) *nxOut = plan->pl.w.nx;
+    if (nyOut) *nyOut = plan->pl.w.nz;
+    if (nKernels) *nKernels = (int)plan->pl.kernels.size();
+    if (workBytes) *workBytes = 4LL * plan->pl.maxElems * (long long)sizeof(float2);
+    return 0;
+}
+
+int srwgPlanExecute(srwgPlan* plan, const float* dExIn, const float* dEyIn, float* dExOut, float* dEyOut, void* stream)
+{
+    return srwgPlanExecuteBatch(plan, 1, dExIn, dEyIn, 0, dExOut, dEyOut, 0, stream);
+}
+
+int srwgPlanExecuteBatch(srwgPlan* plan, int n, const float* dExIn, const float* dEyIn, long long strideIn,
+                         float* dExOut, float* dEyOut, long long strideOut, void* stream)
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    g_lastDetail.clear();
+    if (plan == nullptr || dExIn == nullptr || dEyIn == nullptr || dExOut == nullptr || dEyOut == nullptr || n < 1)
+        return SRWG_ERR_BAD_ARG;
+    int r = get_ctx(plan->device, &plan->ctx);
+    if (r) return r;
+    DeviceCtx& c = *plan->ctx;
+    r = ensure_work(c, (size_t)plan->pl.maxElems);
+    if (r) return r;
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int b = 0; b < n; b++) {
+        r = execute(plan->pl, c, (const float2*)(dExIn + b * strideIn), (const float2*)(dEyIn + b * strideIn),
+                    (float2*)(dExOut + b * strideOut), (float2*)(dEyOut + b * strideOut), c.work, c.workElems, st);
+        if (r) return r;
+    }
+    return 0;
+}
+
+int srwgPlanExecuteTimed(srwgPlan* plan, const float* dExIn, const float* dEyIn, float* dExOut, float* dEyOut,
+                         void* stream, float* kernelMs, int maxKernels, int* nTimed)
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    g_lastDetail.clear();
+    if (plan == nullptr || dExIn == nullptr || dEyIn == nullptr || dExOut == nullptr || dEyOut == nullptr)
+        return SRWG_ERR_BAD_ARG;
+    int r = get_ctx(plan->device, &plan->ctx);
+    if (r) return r;
+    DeviceCtx& c = *plan->ctx;
+    r = ensure_work(c, (size_t)plan->pl.maxElems);
+    if (r) return r;
+    const size_t nk = plan->pl.kernels.size();
+    std::vector<cudaEvent_t> ev(2 * nk);
+    for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
+    cudaStream_t st = (cudaStream_t)stream;
+    r = execute(plan->pl, c, (const float2*)dExIn, (const float2*)dEyIn, (float2*)dExOut, (float2*)dEyOut, c.work,
+                c.workElems, st, nk ? ev.data() : nullptr);
+    if (r == 0) {
+        CUDA_TRY(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < nk && (int)i < maxKernels; i++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+            if (kernelMs) kernelMs[i] = ms;
+        }
+        if (nTimed) *nTimed = (int)nk;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return r;
+}
+
+int srwgPlanDestroy(srwgPlan* plan)
+{
+    delete plan;
+    return 0;
+}
+
+int srwgPlanDescribe(const srwgPlan* plan, char* buf, int bufLen)
+{
+    if (plan == nullptr || buf == nullptr || bufLen <= 0) return SRWG_ERR_BAD_ARG;
+    std::string s = plan->pl.describe();
+    strncpy(buf, s.c_str(), bufLen - 1);
+    buf[bufLen - 1] = 0;
+    return 0;
+}
+
+}  // extern "C"

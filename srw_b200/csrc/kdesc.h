@@ -1,0 +1,94 @@
+// Kernel descriptors shared by the host planner and the sm_100a kernels.
+//
+// A propagation through an SRWLOptC chain is lowered by the planner (planner.cpp) into a short
+// list of bandwidth-bound passes over the two field components (Ex, Ey; complex FP32,
+// row-major [nz][nx], the reference's layout for ne == 1, srradstr.cpp:501):
+//   * LINE passes: each CTA loads whole rows (axis 0) or tiles of whole columns (axis 1) into
+//     shared memory, runs up to two 1D FFTs along the line with point-wise work folded in
+//     between / before / after them, and stores the lines back;
+//   * RESIZE passes: the 16-point bicubic gather of RadResizeCore (sroptelm.cpp:3038);
+//   * PW passes: a standalone element-wise pass (only when nothing else can host the ops).
+// All point-wise work of the reference (drift transfer functions, quadratic phases, lens,
+// aperture masks, FFT centring sign/rotation, normalisation, shift tables, mirror) is expressed
+// by the structs below and applied inside those passes.
+#pragma once
+#include <stdint.h>
+
+#define SRWG_MAX_MASKS 4
+#define SRWG_MAX_STAGES 12
+#define SRWG_MAX_KERNELS 64
+
+// Aperture / obstacle mask in physical coordinates (sroptapt.h:118-395).  The physical coordinate
+// of kernel index i is x0 + i*dx (dx may be negative when the kernel's index order is mirrored).
+struct PwMask {
+    int type;        // 1: rectangle, 2: circle
+    int obstacle;    // 0: aperture (zero outside), 1: obstacle (zero inside)
+    double x0, dx, z0, dz;
+    double cx, cz;   // centre
+    double hx, hz;   // rectangle half sizes incl. the reference's 1e-10 m tolerance
+    double r2;       // circle radius squared
+};
+
+// Point-wise operator: v <- mask(i,j) * scale * exp(i*phase(i,j)) * v, with i the x index and j the
+// z index of the element in the kernel's index space.
+struct PwOps {
+    int has_quad;
+    double Ai, Bi, Aj, Bj, C;            // phase += Ai i^2 + Bi i + Aj j^2 + Bj j + C   (FP64)
+    int has_ang;                         // angular-representation drift (sroptdrf.h:615)
+    double qx0, dqx, qz0, dqz;           // q coordinates of index (i, j)
+    double c0, c1;                       // phase += c0 q^2 (1 + c1 q^2 + 2 (c1 q^2)^2)
+    int has_scale;
+    float sre, sim;                      // complex scale
+    int nmask;
+    PwMask mask[SRWG_MAX_MASKS];
+};
+
+// Index-only side operations of one centred 1D DFT (Make2DFFT helpers, gmfft.h:232-480),
+// per axis.  For a forward transform they are applied after the DFT (RepairSign then Rotate,
+// x Mult, shift-after table); for an inverse transform rotation+sign and the shift-before table
+// are applied before it and Mult and the shift-after table after it.
+struct FftSide {
+    int rs;              // sign (-1)^k + half rotation (even N)
+    int has_shift;       // multiply by exp(i * shift_a * (k - N/2))
+    double shift_a;
+    float scale;         // real factor (1 if none)
+};
+
+struct LineDesc {
+    int axis;            // 0: rows (transform along x), 1: columns (transform along z)
+    int nx, nz;
+    int f1;              // 0 none, +1 forward, -1 inverse: first transform along the line
+    FftSide f1_pre, f1_post;
+    int has_pw;
+    PwOps pw;
+    int mirror_along;    // reverse order along the line after the point-wise ops
+    int mirror_lines;    // store line l at (nlines - 1 - l)
+    int f2;              // second transform along the line
+    FftSide f2_pre, f2_post;
+};
+
+struct ResizeDesc {
+    int nxo, nzo, nxn, nzn;
+    double xStartO, xStepO, zStartO, zStepO;   // old mesh
+    double xStartN, xStepN, zStartN, zStepN;   // new mesh
+    long ixStart, ixEnd, izStart, izEnd;       // AuxLong1..4
+    int only_larger;                           // RadResizeCore_OnlyLargerRange
+    int has_pw;
+    PwOps pw;                                  // applied to the new points
+};
+
+struct PwDesc {
+    int nx, nz;
+    PwOps pw;
+    int mirror_x, mirror_z;                    // output index flips
+};
+
+enum KernelKind { K_LINE = 1, K_RESIZE = 2, K_PW = 3 };
+
+struct KernelDesc {
+    int kind;
+    int src, dst;        // buffer ids: 0 = input, 1 = work A, 2 = work B
+    LineDesc line;
+    ResizeDesc rs;
+    PwDesc pwk;
+};

@@ -1,0 +1,39 @@
+// Launch parameters of the sm_100a kernels (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "kdesc.h"
+
+namespace srwg {
+
+// dynamic shared memory of a line pass (leaves room for the static descriptor copy)
+#define SRWG_LINE_SMEM_MAX (220 * 1024)
+
+struct LineLaunch {
+    LineDesc d;
+    const float2* src[2];
+    float2* dst[2];
+    const float2* tw;        // exp(-2 pi i k / N), k < N (FP64-accurate, rounded to FP32)
+    int N, nlines;           // line length, number of lines
+    int T, L, P, G;          // threads per line, lines per CTA, shared-memory pitch (float2), thread groups
+    int nst;
+    int radix[SRWG_MAX_STAGES];
+};
+
+struct ResizeLaunch {
+    ResizeDesc d;
+    const float2* src[2];
+    float2* dst[2];
+    double xStepInvO, zStepInvO;
+};
+
+struct PwLaunch {
+    PwDesc d;
+    const float2* src[2];
+    float2* dst[2];
+};
+
+cudaError_t launch_line(const LineLaunch& p, cudaStream_t st);
+cudaError_t launch_resize(const ResizeLaunch& p, cudaStream_t st);
+cudaError_t launch_pw(const PwLaunch& p, cudaStream_t st);
+
+}  // namespace srwg

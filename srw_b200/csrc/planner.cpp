@@ -1,0 +1,1058 @@
+// Host planner (see planner.h).  Every mesh / radius / centre / moment update below follows the
+// reference's statement order in FP64 (compiled without FP contraction), so resized and
+// transformed meshes are bit-identical to the reference's; the field work is only described
+// (kdesc.h) and fused into as few GPU passes as possible by Builder.
+#include "planner.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "errors.h"
+
+namespace srwg {
+
+// ================================================================================================
+// FFT good numbers (CGenMathFFT::NextCorrectNumberForFFT, cpp/src/ext/genmath/gmfft.cpp:156-228).
+// The reference's table (gmfft.cpp:26) holds the even n <= 100000 of the form 2^a 3^b 5^c 7^d 11^e
+// 13^f with e, f <= 1; it is generated here from that rule.
+// ================================================================================================
+static const std::vector<long>& good_numbers()
+{
+    static std::vector<long> g;
+    if (g.empty()) {
+        for (long n = 2; n <= 100000; n += 2) {
+            long m = n;
+            while (m % 2 == 0) m /= 2;
+            while (m % 3 == 0) m /= 3;
+            while (m % 5 == 0) m /= 5;
+            while (m % 7 == 0) m /= 7;
+            if (m % 11 == 0) m /= 11;
+            if (m % 13 == 0) m /= 13;
+            if (m == 1) g.push_back(n);
+        }
+    }
+    return g;
+}
+
+long next_correct_number_for_fft(long n)
+{
+    if (n < 4) return 4;
+    if (n < 100001) {
+        const std::vector<long>& g = good_numbers();
+        return *std::lower_bound(g.begin(), g.end(), n);
+    }
+    const double mults[] = {10. / 9., 9. / 8., 6. / 5., 5. / 4., 4. / 3., 3. / 2., 8. / 5., 5. / 3., 16. / 9., 15. / 8.};
+    long k = 99000;
+    for (int j = 0; j < 100; j++) {
+        for (int m = 0; m < 10; m++) {
+            double dk = k * mults[m];
+            long kt = (long)dk;
+            if ((dk - (double)kt) >= 0.5) kt++;
+            if (n <= kt) return kt;
+        }
+        k <<= 1;
+        if (n <= k) return k;
+    }
+    return n;
+}
+
+// ================================================================================================
+// Builder: fuses the stream of point-wise operators, centred 2D FFTs, resizes and mirrors into
+// LINE / RESIZE / PW passes.
+//
+//  - a 2D FFT is split into an x transform (row pass) and a z transform (column pass); the first
+//    half closes the currently open line pass of the same axis (as its second transform) when
+//    there is one, the second half opens a pass of the other axis whose middle section then
+//    collects the following point-wise operators;
+//  - point-wise operators are converted to the index space of the open pass at the time they
+//    are added (so later re-labelling of the mesh or mirrors inside the pass are accounted for);
+//  - a resize closes everything before it and opens a RESIZE pass that collects the operators
+//    on the new mesh.
+// ================================================================================================
+class Builder {
+public:
+    std::vector<KernelDesc>& ks;
+    long long& maxElems;
+    int cur = 0;       // buffer with the current field (0: caller's input)
+    int open = -1;     // pass collecting point-wise operators
+    int fx = 0, fz = 0;
+    Builder(std::vector<KernelDesc>& k, long long& me) : ks(k), maxElems(me) {}
+
+    int next_buf() const { return cur == 1 ? 2 : 1; }
+    KernelDesc& newk(int kind, int nx, int nz)
+    {
+        KernelDesc k;
+        memset(&k, 0, sizeof(k));
+        k.kind = kind;
+        k.src = cur;
+        k.dst = next_buf();
+        cur = k.dst;
+        long long e = (long long)nx * nz;
+        if (e > maxElems) maxElems = e;
+        ks.push_back(k);
+        return ks.back();
+    }
+    void close() { open = -1; fx = fz = 0; }
+
+    PwOps* open_ops()
+    {
+        if (open < 0) return nullptr;
+        KernelDesc& k = ks[open];
+        if (k.kind == K_LINE) { k.line.has_pw = 1; return &k.line.pw; }
+        if (k.kind == K_RESIZE) { k.rs.has_pw = 1; return &k.rs.pw; }
+        return &k.pwk.pw;
+    }
+    PwOps* ensure(const WfrState& w)
+    {
+        if (open < 0) {
+            KernelDesc& k = newk(K_PW, w.nx, w.nz);
+            k.pwk.nx = w.nx;
+            k.pwk.nz = w.nz;
+            open = (int)ks.size() - 1;
+            fx = fz = 0;
+        }
+        return open_ops();
+    }
+    // affine map: kernel index -> physical coordinate of the current logical mesh
+    void axis_map(const WfrState& w, double& X0, double& DX, double& Z0, double& DZ) const
+    {
+        if (fx) { X0 = w.xStart + (w.nx - 1) * w.xStep; DX = -w.xStep; }
+        else { X0 = w.xStart; DX = w.xStep; }
+        if (fz) { Z0 = w.zStart + (w.nz - 1) * w.zStep; DZ = -w.zStep; }
+        else { Z0 = w.zStart; DZ = w.zStep; }
+    }
+    // phase += ax x^2 + bx x + az z^2 + bz z + c  (x, z physical on the current mesh)
+    void quad(const WfrState& w, double ax, double bx, double az, double bz, double c)
+    {
+        PwOps* p = ensure(w);
+        double X0, DX, Z0, DZ;
+        axis_map(w, X0, DX, Z0, DZ);
+        p->has_quad = 1;
+        p->Ai += ax * DX * DX;
+        p->Bi += (2. * ax * X0 + bx) * DX;
+        p->Aj += az * DZ * DZ;
+        p->Bj += (2. * az * Z0 + bz) * DZ;
+        p->C += ax * X0 * X0 + bx * X0 + az * Z0 * Z0 + bz * Z0 + c;
+    }
+    void ang(const WfrState& w, double c0, double c1, double cconst)
+    {
+        PwOps* p = ensure(w);
+        if (p->has_ang) {      // one angular transfer function per pass: materialise first
+            close();
+            p = ensure(w);
+        }
+        double X0, DX, Z0, DZ;
+        axis_map(w, X0, DX, Z0, DZ);
+        p->has_ang = 1;
+        p->qx0 = X0; p->dqx = DX; p->qz0 = Z0; p->dqz = DZ;
+        p->c0 = c0; p->c1 = c1;
+        if (cconst != 0.) { p->has_quad = 1; p->C += cconst; }
+    }
+    void mask(const WfrState& w, int type, int obstacle, double cx, double cz, double hx, double hz, double r2)
+    {
+        PwOps* p = ensure(w);
+        if (p->nmask >= SRWG_MAX_MASKS) {
+            close();
+            p = ensure(w);
+        }
+        PwMask& m = p->mask[p->nmask++];
+        axis_map(w, m.x0, m.dx, m.z0, m.dz);
+        m.type = type; m.obstacle = obstacle;
+        m.cx = cx; m.cz = cz; m.hx = hx; m.hz = hz; m.r2 = r2;
+    }
+    void scale(const WfrState& w, float re, float im)
+    {
+        PwOps* p = ensure(w);
+        if (!p->has_scale) { p->has_scale = 1; p->sre = re; p->sim = im; }
+        else {
+            float r = p->sre * re - p->sim * im, i = p->sre * im + p->sim * re;
+            p->sre = r; p->sim = i;
+        }
+    }
+    // centred 2D FFT on a (nx, nz) mesh; sides per axis
+    void fft2(int nx, int nz, int dir, const FftSide& xpre, const FftSide& xpost, const FftSide& zpre,
+              const FftSide& zpost)
+    {
+        int A = 0;
+        bool reuse = (open >= 0) && ks[open].kind == K_LINE && ks[open].line.f2 == 0;
+        bool upgrade = (open >= 0) && ks[open].kind == K_PW;
+        if (reuse) {
+            LineDesc& d = ks[open].line;
+            A = d.axis;
+            d.f2 = dir;
+            d.f2_pre = A == 0 ? xpre : zpre;
+            d.f2_post = A == 0 ? xpost : zpost;
+            close();
+        } else if (upgrade) {
+            // a pending element-wise pass becomes the row pass of the transform: its operators
+            // (and mirrors) run in shared memory just before the row FFT
+            KernelDesc& k = ks[open];
+            PwDesc pd = k.pwk;
+            memset(&k.line, 0, sizeof(k.line));
+            k.kind = K_LINE;
+            k.line.axis = 0; k.line.nx = nx; k.line.nz = nz;
+            k.line.has_pw = 1; k.line.pw = pd.pw;
+            k.line.mirror_along = pd.mirror_x; k.line.mirror_lines = pd.mirror_z;
+            k.line.f2 = dir; k.line.f2_pre = xpre; k.line.f2_post = xpost;
+            A = 0;
+            close();
+        } else {
+            close();
+            KernelDesc& k = newk(K_LINE, nx, nz);
+            k.line.axis = 0; k.line.nx = nx; k.line.nz = nz;
+            k.line.f2 = dir; k.line.f2_pre = xpre; k.line.f2_post = xpost;
+            A = 0;
+        }
+        int B = 1 - A;
+        KernelDesc& k = newk(K_LINE, nx, nz);
+        k.line.axis = B; k.line.nx = nx; k.line.nz = nz;
+        k.line.f1 = dir;
+        k.line.f1_pre = B == 0 ? xpre : zpre;
+        k.line.f1_post = B == 0 ? xpost : zpost;
+        open = (int)ks.size() - 1;
+        fx = fz = 0;
+    }
+    void mirror(const WfrState& w, int sx, int sz)
+    {
+        int mx = sx < 0, mz = sz < 0;
+        if (!mx && !mz) return;
+        if (open >= 0 && ks[open].kind == K_LINE) {
+            LineDesc& d = ks[open].line;
+            if (d.axis == 0) { d.mirror_along ^= mx; d.mirror_lines ^= mz; }
+            else { d.mirror_along ^= mz; d.mirror_lines ^= mx; }
+        } else {
+            if (open >= 0 && ks[open].kind == K_RESIZE) close();
+            ensure(w);
+            PwDesc& d = ks[open].pwk;
+            d.mirror_x ^= mx; d.mirror_z ^= mz;
+        }
+        fx ^= mx;
+        fz ^= mz;
+    }
+    void resize(const WfrState& o, const WfrState& n, int only_larger)
+    {
+        close();
+        KernelDesc& k = newk(K_RESIZE, n.nx, n.nz);
+        ResizeDesc& r = k.rs;
+        r.nxo = o.nx; r.nzo = o.nz; r.nxn = n.nx; r.nzn = n.nz;
+        r.xStartO = o.xStart; r.xStepO = o.xStep; r.zStartO = o.zStart; r.zStepO = o.zStep;
+        r.xStartN = n.xStart; r.xStepN = n.xStep; r.zStartN = n.zStart; r.zStepN = n.zStep;
+        r.ixStart = n.AuxLong1; r.ixEnd = n.AuxLong2; r.izStart = n.AuxLong3; r.izEnd = n.AuxLong4;
+        r.only_larger = only_larger;
+        open = (int)ks.size() - 1;
+        fx = fz = 0;
+    }
+};
+
+// ================================================================================================
+// SRWLOptC parsing (srTCompositeOptElem ctor, cpp/src/core/sroptcnt.cpp:87-221)
+// ================================================================================================
+int Planner::flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vector<PropDesc>& props, bool nested)
+{
+    if (opt == nullptr || opt->nElem <= 0 || opt->arOpt == nullptr || opt->arOptTypes == nullptr)
+        return UNKNOWN_OPTICAL_ELEMENT;
+    for (int i = 0; i <= opt->nElem; i++) {
+        bool isElem = false;
+        if (i < opt->nElem) {
+            void* p = opt->arOpt[i];
+            const char* t = opt->arOptTypes[i];
+            if (p == nullptr || t == nullptr) return UNKNOWN_OPTICAL_ELEMENT;
+            ElemDesc e;
+            if (strcmp(t, "drift") == 0) {
+                const SRWLOptD* d = (const SRWLOptD*)p;
+                e.kind = E_DRIFT; e.L = d->L; e.treat = d->treat;
+            } else if (strcmp(t, "aperture") == 0 || strcmp(t, "obstacle") == 0) {
+                const SRWLOptA* a = (const SRWLOptA*)p;
+                e.kind = E_APERTURE; e.shape = a->shape; e.Dx = a->Dx; e.Dy = a->Dy; e.x = a->x; e.y = a->y;
+                if (a->ap_or_ob == 'a' || a->ap_or_ob == 'A') e.apob = 'a';
+                else if (a->ap_or_ob == 'o' || a->ap_or_ob == 'O') e.apob = 'o';
+                else return UNKNOWN_OPTICAL_ELEMENT;
+                if (e.shape != 'r' && e.shape != 'c') { isElem = false; goto props_only; }
+            } else if (strcmp(t, "lens") == 0) {
+                const SRWLOptL* l = (const SRWLOptL*)p;
+                e.kind = E_LENS; e.Fx = l->Fx; e.Fy = l->Fy; e.x = l->x; e.y = l->y;
+            } else if (strcmp(t, "container") == 0) {
+                // a nested container is one element of the outer chain; its own propagation
+                // parameters apply inside it (sroptcnt.cpp:171)
+                std::vector<ElemDesc> sub;
+                std::vector<PropDesc> subp;
+                int r = flatten((const SRWLOptC*)p, sub, subp, true);
+                if (r) return r;
+                (void)sub; (void)subp;
+                err = "nested SRWLOptC containers are not supported on the GPU path";
+                return SRWG_ERR_UNSUPPORTED;
+            } else {
+                err = std::string("optical element type not supported on the GPU path: ") + t;
+                return SRWG_ERR_UNSUPPORTED;
+            }
+            els.push_back(e);
+            isElem = true;
+        }
+    props_only:
+        if (opt->arProp != nullptr && (isElem || i == opt->nElem)) {
+            PropDesc pd;
+            pd.n = 0;
+            for (int k = 0; k < 17; k++) pd.pp[k] = 0;
+            pd.pp[2] = 1.; pd.pp[5] = pd.pp[6] = pd.pp[7] = pd.pp[8] = 1.;
+            if (i < opt->nProp && opt->arProp[i] != nullptr) {
+                int n = 9;
+                if (opt->arPropN != nullptr) n = opt->arPropN[i];
+                if (n > 17) n = 17;
+                for (int k = 0; k < n; k++) pd.pp[k] = opt->arProp[i][k];
+                pd.n = n;
+            } else {
+                pd.n = -1;   // default instruction: no resize
+            }
+            props.push_back(pd);
+        }
+    }
+    (void)nested;
+    return 0;
+}
+
+// ================================================================================================
+// wavefront bookkeeping helpers (srradstr.cpp / srradstr.h)
+// ================================================================================================
+void Planner::set_full_range()
+{   // SetNonZeroWavefrontLimitsToFullRange (srradstr.h:339)
+    w.xWfrMin = w.xStart;
+    w.xWfrMax = w.xStart + w.nx * w.xStep;
+    w.zWfrMin = w.zStart;
+    w.zWfrMax = w.zStart + w.nz * w.zStep;
+}
+
+void Planner::srwl_roundtrip()
+{   // ModifyWfrNeNxNz (srradstr.cpp:760): OutSRWRadPtrs then InSRWRadPtrs on the client struct
+    double xFin = w.xStart + w.xStep * (w.nx - 1);
+    double yFin = w.zStart + w.zStep * (w.nz - 1);
+    double xS = w.xStart, yS = w.zStart;
+    if (w.nx <= 1) { w.xStart = 0.5 * (xS + xFin); w.xStep = 0.; }
+    else { w.xStart = xS; w.xStep = (xFin - xS) / (w.nx - 1); }
+    if (w.nz <= 1) { w.zStart = 0.5 * (yS + yFin); w.zStep = 0.; }
+    else { w.zStart = yS; w.zStep = (yFin - yS) / (w.nz - 1); }
+    w.xWfrMin = xS; w.xWfrMax = xFin;
+    w.zWfrMin = yS; w.zWfrMax = yFin;
+}
+
+// One centred 2D FFT (CGenMathFFT2D::Make2DFFT, gmfft.cpp:295-897): computes the transformed
+// mesh (SetupLimitsTr, gmfft.h:232) and the per-axis side operations, and emits the transform.
+void Planner::fft2_emit(int dir, bool use_given, double& xStepTr, double& zStepTr, double& xStartTr, double& zStartTr)
+{
+    const double RelShiftTol = 1.E-06;
+    long Nx = w.nx, Ny = w.nz;
+    long HalfNx = Nx >> 1, HalfNy = Ny >> 1;
+    double xStartTr0 = -0.5 / w.xStep;
+    xStepTr = -xStartTr0 / HalfNx;
+    double yStartTr0 = -0.5 / w.zStep;
+    zStepTr = -yStartTr0 / HalfNy;
+    if (use_given) { xStartTr = w.xStartTr; zStartTr = w.zStartTr; }
+    else { xStartTr = xStartTr0; zStartTr = yStartTr0; }
+    double xStepNx = Nx * w.xStep, yStepNy = Ny * w.zStep;
+    double x0_After = w.xStart + 0.5 * xStepNx;
+    double y0_After = w.zStart + 0.5 * yStepNy;
+    bool aftX = ::fabs(x0_After) > RelShiftTol * xStepNx;
+    bool aftY = ::fabs(y0_After) > RelShiftTol * yStepNy;
+    bool befX = false, befY = false;
+    double x0_Before = 0., y0_Before = 0.;
+    if (use_given) {
+        x0_Before = w.xStartTr - xStartTr0;
+        y0_Before = w.zStartTr - yStartTr0;
+        befX = ::fabs(x0_Before) > RelShiftTol * ::fabs(xStartTr0);
+        befY = ::fabs(y0_Before) > RelShiftTol * ::fabs(yStartTr0);
+    }
+    double sg = (dir > 0) ? -1. : 1.;
+    const double twoPi = 6.283185307179586477;
+    FftSide xpre{}, xpost{}, zpre{}, zpost{};
+    xpre.scale = xpost.scale = zpre.scale = zpost.scale = 1.f;
+    // FillArrayShift (gmfft.h:250): exp(i 2 pi t0 (k - N/2) tStep)
+    if (befX) { xpre.has_shift = 1; xpre.shift_a = twoPi * (sg * x0_Before) * w.xStep; }
+    if (befY) { zpre.has_shift = 1; zpre.shift_a = twoPi * (sg * y0_Before) * w.zStep; }
+    if (aftX) { xpost.has_shift = 1; xpost.shift_a = twoPi * (sg * x0_After) * xStepTr; }
+    if (aftY) { zpost.has_shift = 1; zpost.shift_a = twoPi * (sg * y0_After) * zStepTr; }
+    if (dir > 0) { xpost.rs = 1; zpost.rs = 1; }     // RepairSign then Rotate after the forward FFT
+    else { xpre.rs = 1; zpre.rs = 1; }               // Rotate then RepairSign before the backward FFT
+    zpost.scale = (float)(w.xStep * w.zStep);        // NormalizeDataAfter2DFFT (x dx dy)
+    b->fft2(w.nx, w.nz, dir, xpre, xpost, zpre, zpost);
+}
+
+void Planner::set_rad_repres(int to)
+{   // srTGenOptElem::SetRadRepres (sroptelm.cpp:1243-1528), ne == 1; edge correction is never on
+    if (w.Pres == to) return;
+    int dir = (to == 0) ? -1 : 1;
+    bool use_given = (w.AuxLong4 == 7777777) || ((to == 0) && w.UseStartTrToShiftAtChangingRepresToCoord);
+    double xs, zs, x0, z0;
+    fft2_emit(dir, use_given, xs, zs, x0, z0);
+    w.xStep = xs; w.zStep = zs; w.xStart = x0; w.zStart = z0;
+    w.Pres = to;
+    set_full_range();
+}
+
+void Planner::mirror(int sx, int sz)
+{
+    b->mirror(w, sx, sz);
+}
+
+// ================================================================================================
+// Drift space (cpp/src/core/sroptdrf.h, sroptdrf.cpp)
+// ================================================================================================
+static const double PI_D_LAMBDA_PER_EV = 2.53384080189E+06;   // sroptdrf.h:479
+static const double INV_LAMBDA_PER_EV = 806546.577258;         // sroptdrf.h:481
+static const double LAMBDA_EV_M = 1.239842e-06;                // sroptdrf.h:617
+
+double Planner::diff_lim_spot(char xz, double L) const
+{   // DiffractionLimitedPropagatedSpotSize (sroptdrf.h:1020)
+    double lam = LAMBDA_EV_M / w.eStart;
+    double dLim = (xz == 'x') ? (w.nx - 1) * w.xStep : (w.nz - 1) * w.zStep;
+    double dWfr = (xz == 'x') ? (w.xWfrMax - w.xWfrMin) : (w.zWfrMax - w.zWfrMin);
+    double d = ((dWfr > 0.) && (dWfr < dLim)) ? dWfr : dLim;
+    return lam * L / d;
+}
+
+static void mom_apply(double* m, const double ax[2][2], const double az[2][2])
+{   // MultSquareMatrByVect steps of AuxPropagateRadMoments / GenAuxPropagateRadMoments
+    double bx[3][3] = {{ax[0][0] * ax[0][0], 2. * ax[0][0] * ax[0][1], ax[0][1] * ax[0][1]},
+                       {ax[0][0] * ax[1][0], ax[0][1] * ax[1][0] + ax[0][0] * ax[1][1], ax[0][1] * ax[1][1]},
+                       {ax[1][0] * ax[1][0], 2. * ax[1][0] * ax[1][1], ax[1][1] * ax[1][1]}};
+    double bz[3][3] = {{az[0][0] * az[0][0], 2. * az[0][0] * az[0][1], az[0][1] * az[0][1]},
+                       {az[0][0] * az[1][0], az[0][1] * az[1][0] + az[0][0] * az[1][1], az[0][1] * az[1][1]},
+                       {az[1][0] * az[1][0], 2. * az[1][0] * az[1][1], az[1][1] * az[1][1]}};
+    double v2[2], v3[3];
+    v2[0] = m[1]; v2[1] = m[2];
+    for (int i = 0; i < 2; i++) { double s = 0; for (int j = 0; j < 2; j++) s += ax[i][j] * v2[j]; m[1 + i] = s; }
+    v2[0] = m[3]; v2[1] = m[4];
+    for (int i = 0; i < 2; i++) { double s = 0; for (int j = 0; j < 2; j++) s += az[i][j] * v2[j]; m[3 + i] = s; }
+    v3[0] = m[5]; v3[1] = m[6]; v3[2] = m[7];
+    for (int i = 0; i < 3; i++) { double s = 0; for (int j = 0; j < 3; j++) s += bx[i][j] * v3[j]; m[5 + i] = s; }
+    v3[0] = m[8]; v3[1] = m[9]; v3[2] = m[10];
+    for (int i = 0; i < 3; i++) { double s = 0; for (int j = 0; j < 3; j++) s += bz[i][j] * v3[j]; m[8 + i] = s; }
+}
+
+void Planner::drift_moments(double L)
+{   // srTDriftSpace::PropagateRadMoments -> AuxPropagateRadMoments (sroptdrf.h:967, sroptdrf.cpp:22)
+    const double a[2][2] = {{1., L}, {0., 1.}};
+    double* moms[2] = {w.momX, w.momZ};
+    for (int c = 0; c < 2; c++) {
+        double* m = moms[c];
+        if (m[0] != 0.) {
+            mom_apply(m, a, a);
+            double sx = diff_lim_spot('x', L);
+            if (m[5] - m[1] * m[1] < sx * sx) m[5] = sx * sx + m[1] * m[1];
+            double sz = diff_lim_spot('z', L);
+            if (m[8] - m[3] * m[3] < sz * sz) m[8] = sz * sz + m[3] * m[3];
+        }
+    }
+}
+
+void Planner::drift_ang(const ElemDesc& e)
+{   // PropagateRadiationSimple_AngRepres (sroptdrf.h:348-411), RadPointModifier_AngRepres (:615)
+    double xStartOld = w.xStart, zStartOld = w.zStart;
+    w.xStart = -(w.nx >> 1) * w.xStep;
+    w.zStart = -(w.nz >> 1) * w.zStep;
+    double xShift = w.xStart - xStartOld, zShift = w.zStart - zStartOld;
+    w.xWfrMin += xShift; w.xWfrMax += xShift;
+    w.zWfrMin += zShift; w.zWfrMax += zShift;
+    if (w.Pres != 1) set_rad_repres(1);
+    double lam = LAMBDA_EV_M / w.eStart;
+    double c0 = -3.1415926536 * e.L * lam, c1 = 0.25 * lam * lam;
+    double cc = (e.treat == 1) ? (5.067730652e+06) * e.L * w.eStart : 0.;
+    b->ang(w, c0, c1, cc);
+    if (w.UseStartTrToShiftAtChangingRepresToCoord) { w.xStartTr += xShift; w.zStartTr += zShift; }
+    set_rad_repres(0);
+    w.xStart = xStartOld; w.zStart = zStartOld;
+    if (w.UseStartTrToShiftAtChangingRepresToCoord) {
+        w.xStart = w.xStartTr - xShift;
+        w.zStart = w.zStartTr - zShift;
+    }
+    set_full_range();
+}
+
+void Planner::drift_to_waist(const ElemDesc& e)
+{   // PropagateRadiationSimple_PropToWaist (sroptdrf.cpp:356-489), SetupPropBufVars_PropToWaist
+    // (sroptdrf.h:476), RadPointModifier_PropToWaist (sroptdrf.h:649-710)
+    const double L = e.L;
+    set_full_range();
+    double InvLength = 1. / L;
+    double Pi_d_LambdaM = w.eStart * PI_D_LAMBDA_PER_EV;
+    double Pi_d_LambdaM_d_Length = Pi_d_LambdaM * InvLength;
+    double InvLength_d_Lambda = InvLength * w.eStart * INV_LAMBDA_PER_EV;
+    double TwoPi_d_LambdaM = 2. * Pi_d_LambdaM;
+    double TwoPiXc = TwoPi_d_LambdaM * w.xc / w.RobsX;
+    double TwoPiZc = TwoPi_d_LambdaM * w.zc / w.RobsZ;
+    if (w.Pres != 0) set_rad_repres(0);
+    double cc = (e.treat == 1) ? (5.067730652e+06) * L * w.eStart : 0.;
+    b->quad(w, Pi_d_LambdaM_d_Length, TwoPiXc, Pi_d_LambdaM_d_Length, TwoPiZc, cc);
+    double InvLambda_m = w.eStart * INV_LAMBDA_PER_EV;
+    double InvLambda_m_d_Length = InvLambda_m / L;
+    double LambdaM_Length = 1. / InvLambda_m_d_Length;
+    double xs, zs, x0, z0;
+    fft2_emit(1, false, xs, zs, x0, z0);     // Make2DFFT forward, representation flag unchanged
+    double qxCen = -w.xc * InvLambda_m / w.RobsX;
+    double qzCen = -w.zc * InvLambda_m / w.RobsZ;
+    w.xStart = (x0 + qxCen) * LambdaM_Length;
+    w.zStart = (z0 + qzCen) * LambdaM_Length;
+    w.xStep = xs * LambdaM_Length;
+    w.zStep = zs * LambdaM_Length;
+    b->quad(w, Pi_d_LambdaM_d_Length, 0., Pi_d_LambdaM_d_Length, 0., 0.);
+    b->scale(w, 0.f, (float)(-InvLength_d_Lambda));     // x InvLength_d_Lambda, then (re,im) <- (im,-re)
+    if (LambdaM_Length < 0) {
+        mirror(-1, -1);
+        double xEnd = w.xStart + (w.xStep) * (w.nx - 1);
+        w.xStart = xEnd;
+        w.xStep *= -1.;
+        double zEnd = w.zStart + (w.zStep) * (w.nz - 1);
+        w.zStart = zEnd;
+        w.zStep *= -1.;
+    }
+}
+
+static double sgn(double v) { return v > 0 ? 1. : (v < 0 ? -1. : 0.); }
+
+int Planner::drift_quad(const ElemDesc& e, int subtype)
+{   // PropagateRadiationSimple_AnalytTreatQuadPhaseTerm (sroptdrf.cpp:726-887),
+    // SetupPropBufVars_AnalytTreatQuadPhaseTerm (:889), EstimateWfrRadToSub2 (:1085),
+    // RadPointModifier_AnalytTreatQuadPhaseTerm (sroptdrf.h:806-880)
+    const double L = e.L;
+    const double infLarge = 1E+23;
+    double xc = w.xc, zc = w.zc;
+    double invRx = 0, invRz = 0, Lx = 0, Lz = 0, invRxL = 1. / L, invRzL = 1. / L;
+    double kx = infLarge, kxc = infLarge, kz = infLarge, kzc = infLarge;
+    double trueRx = w.RobsX, trueRz = w.RobsZ;
+    if (subtype == 2) {
+        const double factRadEr = 3.;
+        double minAbsEffRx = factRadEr * w.RobsXAbsErr, minAbsEffRz = factRadEr * w.RobsZAbsErr;
+        double effRx_p_L = trueRx + L;
+        if (::fabs(trueRx) < minAbsEffRx) trueRx = minAbsEffRx * ((trueRx >= 0) ? 1. : -1.);
+        else if (::fabs(effRx_p_L) < minAbsEffRx) trueRx = minAbsEffRx * ((effRx_p_L >= 0) ? 1. : -1.) - L;
+        double effRz_p_L = trueRz + L;
+        if (::fabs(trueRz) < minAbsEffRz) trueRz = minAbsEffRz * ((trueRz >= 0) ? 1. : -1.);
+        else if (::fabs(effRz_p_L) < minAbsEffRz) trueRz = minAbsEffRz * ((effRz_p_L >= 0) ? 1. : -1.) - L;
+    } else if (subtype == 1) {
+        err = "drift mode pp[3]=1 (moment-based radius estimate) is not supported on the GPU path";
+        return SRWG_ERR_UNSUPPORTED;
+    }
+    if (trueRx != 0) {
+        invRx = 1. / trueRx;
+        kx = (trueRx + L) * invRx;
+        kxc = L / trueRx;
+        if (-L != trueRx) { Lx = L / (1. + L * invRx); invRxL = 1. / (L + trueRx); }
+        else { Lx = infLarge; invRxL = infLarge; }
+    }
+    if (trueRz != 0) {
+        invRz = 1. / trueRz;
+        kz = (trueRz + L) * invRz;
+        kzc = L / trueRz;
+        if (-L != trueRz) { Lz = L / (1. + L * invRz); invRzL = 1. / (L + trueRz); }
+        else { Lz = infLarge; invRzL = infLarge; }
+    }
+    double sqrt_LxLz_d_L = ::sqrt(::fabs(Lx * Lz)) / L;
+    double phase_term = 0.25 * 3.141592653589793 * (2. - sgn(Lx) - sgn(Lz));
+
+    if (w.Pres != 0) set_rad_repres(0);
+    double lam = LAMBDA_EV_M / w.eStart;
+    double Pi_d_Lambda_m = 3.1415926536 / lam;
+    // pass 1: -pi/lambda ((x-xc)^2/Rx + (z-zc)^2/Rz)
+    {
+        double ax = -Pi_d_Lambda_m * invRx, az = -Pi_d_Lambda_m * invRz;
+        b->quad(w, ax, -2. * ax * xc, az, -2. * az * zc, ax * xc * xc + az * zc * zc);
+    }
+    double xStartOld = w.xStart, zStartOld = w.zStart;
+    w.xStart = -(w.nx >> 1) * w.xStep;
+    w.zStart = -(w.nz >> 1) * w.zStep;
+    double xShift = w.xStart - xStartOld, zShift = w.zStart - zStartOld;
+    w.xWfrMin += xShift; w.xWfrMax += xShift;
+    w.zWfrMin += zShift; w.zWfrMax += zShift;
+    set_rad_repres(1);
+    // pass 2 (angular side): -pi lambda (Lx qx^2 + Lz qz^2) + sign term, x sqrt(|Lx Lz|)/L
+    {
+        double Pi_Lambda_m = 3.1415926536 * lam;
+        b->quad(w, -Pi_Lambda_m * Lx, 0., -Pi_Lambda_m * Lz, 0., phase_term);
+        b->scale(w, (float)sqrt_LxLz_d_L, 0.f);
+    }
+    if (w.UseStartTrToShiftAtChangingRepresToCoord) { w.xStartTr += xShift; w.zStartTr += zShift; }
+    set_rad_repres(0);
+    w.xStart = xStartOld; w.zStart = zStartOld;
+    if (w.UseStartTrToShiftAtChangingRepresToCoord) { w.xStart = w.xStartTr - xShift; w.zStart = w.zStartTr - zShift; }
+    w.xStart = kx * (w.xStart) - kxc * (w.xc);
+    w.xStep *= kx;
+    w.zStart = kz * (w.zStart) - kzc * (w.zc);
+    w.zStep *= kz;
+    // pass 3: +pi/lambda ((x-xc)^2/(R+L) ...)
+    {
+        double ax = Pi_d_Lambda_m * invRxL, az = Pi_d_Lambda_m * invRzL;
+        double cc = ax * xc * xc + az * zc * zc;
+        if (e.treat == 1) cc += 2 * Pi_d_Lambda_m * L;
+        b->quad(w, ax, -2. * ax * xc, az, -2. * az * zc, cc);
+    }
+    mirror((int)sgn(kx), (int)sgn(kz));
+    if (kx < 0) {
+        double xEnd = w.xStart + (w.nx - 1) * w.xStep;
+        w.xStart = xEnd;
+        w.xStep *= -1;
+    }
+    if (kz < 0) {
+        double zEnd = w.zStart + (w.nz - 1) * w.zStep;
+        w.zStart = zEnd;
+        w.zStep *= -1;
+    }
+    set_full_range();
+    return 0;
+}
+
+void Planner::drift(const ElemDesc& e, int anal)
+{   // srTDriftSpace::PropagateRadiation (sroptdrf.h:116) -> PropagateRadiationSingleE_Meth_0 (:158)
+    if (anal == 1 || anal == 2) {
+        int r = drift_quad(e, anal);
+        if (r) throw r;
+    } else if (anal == 4) drift_to_waist(e);
+    else if (anal == 0) drift_ang(e);
+    else {
+        err = "drift mode pp[3]=" + std::to_string(anal) + " is not supported on the GPU path";
+        throw (int)SRWG_ERR_UNSUPPORTED;
+    }
+    drift_moments(e.L);
+    w.RobsX += e.L;                       // PropagateWaveFrontRadius (sroptdrf.h:981)
+    w.RobsZ += e.L;
+    set_full_range();
+}
+
+// ================================================================================================
+// Linear phase terms (CheckAndSubtract/ResetPhaseTermsLin, srradstr.cpp:2610-2705)
+// ================================================================================================
+void Planner::phase_lin_subtract(double newXc, double newZc)
+{
+    const double ratAllowSubtract = 0.2, minNumOptCycles = 10;
+    double lambda_m = 3.1415926535898 / (w.eStart * 2.53384080189E+06);
+    const double twoPi = 2. * 3.1415926535898;
+    bool xOK = false;
+    double dxcSubNew = newXc - w.xc;
+    if (w.RobsX != 0) {
+        double r = w.xStep * (w.nx - 1);
+        double nc = 0.25 * r * r / (lambda_m * w.RobsX);
+        xOK = (::fabs(w.RobsX) > ::fabs(w.RobsXAbsErr)) && (nc > minNumOptCycles) && (::fabs(dxcSubNew) / r > ratAllowSubtract);
+    }
+    if (!xOK) dxcSubNew = 0;
+    bool zOK = false;
+    double dzcSubNew = newZc - w.zc;
+    if (w.RobsZ != 0) {
+        double r = w.zStep * (w.nz - 1);
+        double nc = 0.25 * r * r / (lambda_m * w.RobsZ);
+        zOK = (::fabs(w.RobsZ) > ::fabs(w.RobsZAbsErr)) && (nc > minNumOptCycles) && (::fabs(dzcSubNew) / r > ratAllowSubtract);
+    }
+    if (!zOK) dzcSubNew = 0;
+    if (!xOK && !zOK) return;
+    double dxc = dxcSubNew;
+    if (w.xLinOnly) {
+        dxc -= w.dxcSub;
+        if (::fabs(dxc) / ::fabs(w.dxcSub) < ratAllowSubtract) { dxc = 0; dxcSubNew = w.dxcSub; }
+    }
+    w.dxcSub = dxcSubNew;
+    w.xLinOnly = (dxcSubNew != 0);
+    double xMult = -twoPi * dxc / (lambda_m * w.RobsX);
+    double dzc = dzcSubNew;
+    if (zOK && w.zLinOnly) {
+        dzc -= w.dzcSub;
+        if (::fabs(dzc) / ::fabs(w.dzcSub) < ratAllowSubtract) { dzc = 0; dzcSubNew = w.dzcSub; }
+    }
+    w.dzcSub = dzcSubNew;
+    w.zLinOnly = (dzcSubNew != 0);
+    double zMult = -twoPi * dzc / (lambda_m * w.RobsZ);
+    if (xMult == 0 && zMult == 0) return;
+    b->quad(w, 0., xMult, 0., zMult, 0.);       // MultiplyElFieldByPhaseLin
+}
+
+void Planner::phase_lin_reset()
+{
+    if (!w.xLinOnly && !w.zLinOnly) return;
+    double lambda_m = 3.1415926535898 / (w.eStart * 2.53384080189E+06);
+    const double twoPi = 2. * 3.1415926535898;
+    double xMult = 0, zMult = 0;
+    if (w.xLinOnly && w.dxcSub != 0 && w.RobsX != 0) xMult = twoPi * w.dxcSub / (lambda_m * w.RobsX);
+    if (w.zLinOnly && w.dzcSub != 0 && w.RobsZ != 0) zMult = twoPi * w.dzcSub / (lambda_m * w.RobsZ);
+    w.xLinOnly = w.zLinOnly = false;
+    w.dxcSub = w.dzcSub = 0;
+    if (xMult == 0 && zMult == 0) return;
+    b->quad(w, 0., xMult, 0., zMult, 0.);
+}
+
+void Planner::fix_abs_err()
+{   // tail of srTGenOptElem::PropagateRadiationMeth_0 (sroptel2.cpp:151)
+    if ((w.RobsX != 0) && (w.RobsXAbsErr == 0)) w.RobsXAbsErr = ::fabs(0.1 * w.RobsX);
+    if ((w.RobsZ != 0) && (w.RobsZAbsErr == 0)) w.RobsZAbsErr = ::fabs(0.1 * w.RobsZ);
+}
+
+// ================================================================================================
+// Thin lens (cpp/src/core/sroptfoc.h:18-276)
+// ================================================================================================
+void Planner::lens(const ElemDesc& e)
+{
+    phase_lin_subtract(e.x, e.y);
+    if (w.Pres != 0) set_rad_repres(0);
+    double Pi_d_Lambda_m = w.eStart * 2.533865612E+06;
+    {   // -pi/lambda ((x-cx)^2/Fx + (z-cz)^2/Fz)
+        double ax = -Pi_d_Lambda_m / e.Fx, az = -Pi_d_Lambda_m / e.Fy;
+        b->quad(w, ax, -2. * ax * e.x, az, -2. * az * e.y, ax * e.x * e.x + az * e.y * e.y);
+    }
+    const double ax[2][2] = {{1., 0.}, {-1. / e.Fx, 1.}};
+    const double az[2][2] = {{1., 0.}, {-1. / e.Fy, 1.}};
+    mom_apply(w.momX, ax, az);
+    mom_apply(w.momZ, ax, az);
+    const double dSmall = 1E-23;
+    double difX = (e.Fx == w.RobsX) ? dSmall : e.Fx - w.RobsX;
+    double difZ = (e.Fy == w.RobsZ) ? dSmall : e.Fy - w.RobsZ;
+    double MagnX = e.Fx / difX, MagnZ = e.Fy / difZ;
+    w.RobsX *= MagnX;
+    w.RobsZ *= MagnZ;
+    w.RobsXAbsErr *= (MagnX * MagnX);
+    w.RobsZAbsErr *= (MagnZ * MagnZ);
+    w.xc = e.x - (e.x - w.xc) * MagnX;
+    w.zc = e.y - (e.y - w.zc) * MagnZ;
+    fix_abs_err();
+    phase_lin_reset();
+}
+
+// ================================================================================================
+// Apertures / obstacles (cpp/src/core/sroptapt.h, sroptapt.cpp:248-350)
+// ================================================================================================
+void Planner::aperture(const ElemDesc& e)
+{
+    if (w.Pres != 0) set_rad_repres(0);
+    int obstacle = (e.apob == 'o');
+    if (e.shape == 'r') {
+        const double SmallOffset = 1.E-10;
+        b->mask(w, 1, obstacle, e.x, e.y, 0.5 * e.Dx + SmallOffset, 0.5 * e.Dy + SmallOffset, 0.);
+    } else {
+        double R = 0.5 * e.Dx;
+        b->mask(w, 2, obstacle, e.x, e.y, 0., 0., R * R);
+    }
+    // PropagateRadMoments: the reference recomputes the moments numerically (ComputeRadMoments)
+    // when 1.7 sigma of the beam is not inside the opening (always for obstacles); flagged here.
+    {
+        double* mx = w.momX; double* mz = w.momZ;
+        auto central = [](const double* m, double& sxx, double& szz) {
+            double Mxx = m[5] - m[1] * m[1], Mzz = m[8] - m[3] * m[3];
+            if (Mxx < 0.1 * m[5]) Mxx = 0.1 * m[5];
+            if (Mzz < 0.1 * m[8]) Mzz = 0.1 * m[8];
+            sxx = ::sqrt(::fabs(Mxx)); szz = ::sqrt(::fabs(Mzz));
+        };
+        double sxX, szX, sxZ, szZ;
+        central(mx, sxX, szX);
+        central(mz, sxZ, szZ);
+        bool recompute = true;
+        if (!obstacle) {
+            double hx = (e.shape == 'r') ? 0.5 * e.Dx : 0.5 * e.Dx, hz = (e.shape == 'r') ? 0.5 * e.Dy : 0.5 * e.Dx;
+            recompute = ((mx[1] - 1.7 * sxX) < (e.x - hx)) || ((mx[1] + 1.7 * sxX) > (e.x + hx)) ||
+                        ((mx[3] - 1.7 * szX) < (e.y - hz)) || ((mx[3] + 1.7 * szX) > (e.y + hz)) ||
+                        ((mz[1] - 1.7 * sxZ) < (e.x - hx)) || ((mz[1] + 1.7 * sxZ) > (e.x + hx)) ||
+                        ((mz[3] - 1.7 * szZ) < (e.y - hz)) || ((mz[3] + 1.7 * szZ) > (e.y + hz));
+        }
+        if (recompute) w.momentsStale = true;
+    }
+    if (e.apob == 'a') {     // SetNewNonZeroWfrLimits of the apertures
+        double hx = (e.shape == 'r') ? 0.5 * e.Dx : 0.5 * e.Dx;
+        double hz = (e.shape == 'r') ? 0.5 * e.Dy : 0.5 * e.Dx;
+        if (w.xWfrMin < e.x - hx) w.xWfrMin = e.x - hx;
+        if (w.xWfrMax > e.x + hx) w.xWfrMax = e.x + hx;
+        if (w.zWfrMin < e.y - hz) w.zWfrMin = e.y - hz;
+        if (w.zWfrMax > e.y + hz) w.zWfrMax = e.y + hz;
+    }
+    fix_abs_err();
+}
+
+// ================================================================================================
+// Resizing (RadResizeGen, sroptelm.cpp:2242-3036; RadResizeCore :3038-3337)
+// ================================================================================================
+void Planner::treat_quad(char add_or_rem)
+{   // TreatStronglyOscillatingTerm (sroptelm.cpp:4774-5014) as a point-wise phase
+    const double Const = 3.14159265358979 * 1.E+06 / 1.23984186;
+    double cRx, cRz;
+    if (w.Pres == 0) { cRx = w.QuadX ? Const / w.RobsX : 0.; cRz = w.QuadZ ? Const / w.RobsZ : 0.; }
+    else {
+        double lam = LAMBDA_EV_M / w.eStart;
+        cRx = w.QuadX ? -Const * w.RobsX * lam * lam : 0.;
+        cRz = w.QuadZ ? -Const * w.RobsZ * lam * lam : 0.;
+    }
+    if (add_or_rem == 'r') { cRx = -cRx; cRz = -cRz; }
+    double ax = cRx * w.eStart, az = cRz * w.eStart;
+    b->quad(w, ax, -2. * ax * w.xc, az, -2. * az * w.zc, ax * w.xc * w.xc + az * w.zc * w.zc);
+}
+
+int Planner::resize(double pxm, double pxd, double pzm, double pzd, int shift, double xcs, double zcs, bool other_side)
+{
+    if ((pxm == 1.) && (pxd == 1.) && (pzm == 1.) && (pzd == 1.) && (shift <= 0)) return 0;
+    double RelCenPosX = 0.5, RelCenPosZ = 0.5;
+    const double RelCenPosTol = 1.e-06;
+    if (shift & 1) {
+        double rxTot = w.xStep * (w.nx - 1), rxLeft = xcs - w.xStart;
+        if ((rxLeft > 0.) && (xcs < (w.xStart + rxTot))) RelCenPosX = rxLeft / rxTot;
+    }
+    if (shift & 2) {
+        double rzTot = w.zStep * (w.nz - 1), rzLeft = zcs - w.zStart;
+        if ((rzLeft > 0.) && (zcs < (w.zStart + rzTot))) RelCenPosZ = rzLeft / rzTot;
+    }
+    int nxOld = w.nx, nzOld = w.nz;
+    double xStartOld = w.xStart, zStartOld = w.zStart, xStepOld = w.xStep, zStepOld = w.zStep;
+    double xRangeOld = xStepOld * nxOld, zRangeOld = zStepOld * nzOld;
+    bool useStartTrOther = (::fabs(xStartOld + 0.5 * xRangeOld) > 0.5 * w.xStep) ||
+                           (::fabs(zStartOld + 0.5 * zRangeOld) > 0.5 * w.zStep);
+    double pxmIn = pxm, pxdIn = pxd, pzmIn = pzm, pzdIn = pzd;
+    if (other_side) {
+        int to = (w.Pres == 0) ? 1 : 0;
+        if (useStartTrOther) {
+            w.xStart = -(w.nx >> 1) * w.xStep;
+            w.zStart = -(w.nz >> 1) * w.zStep;
+            double xs = w.xStart - xStartOld, zs = w.zStart - zStartOld;
+            w.xWfrMin += xs; w.xWfrMax += xs;
+            w.zWfrMin += zs; w.zWfrMax += zs;
+        }
+        set_rad_repres(to);
+        double t;
+        t = pxm; pxm = pxd; pxd = t;
+        t = pzm; pzm = pzd; pzd = t;
+    }
+    WfrState old = w;
+    WfrState nw = w;
+    double pxTot = pxm * pxd, pzTot = pzm * pzd;
+    long NewNx = w.nx, NewNz = w.nz;
+    bool changed = (pxTot != 1.) || (pzTot != 1.);
+    if (changed) {
+        double v = pxTot * NewNx;
+        long iv = (long)v;
+        NewNx = ((v - iv) >= 0.5) ? iv + 1 : iv;
+        v = pzTot * NewNz;
+        iv = (long)v;
+        NewNz = ((v - iv) >= 0.5) ? iv + 1 : iv;
+        NewNx = next_correct_number_for_fft(NewNx);
+        NewNz = next_correct_number_for_fft(NewNz);
+        nw.nx = (int)NewNx;
+        nw.nz = (int)NewNz;
+    }
+    if ((::fabs(RelCenPosX - 0.5) > RelCenPosTol) || (::fabs(RelCenPosZ - 0.5) > RelCenPosTol)) {
+        err = "off-centre resizing (pp[9] shift types) is not supported on the GPU path";
+        return SRWG_ERR_UNSUPPORTED;
+    }
+    auto preserve = [&](char ax) {   // PreserveLogicsOfWfrLimitsAtRangeResizing (srradstr.cpp:1598)
+        if (ax == 'x') {
+            double tol = 0.01 * nw.xStep;
+            if ((::fabs(old.xWfrMin - old.xStart) < tol) && (::fabs(old.xStart + old.nx * old.xStep - old.xWfrMax) < tol)) {
+                nw.xWfrMin = nw.xStart; nw.xWfrMax = nw.xStart + nw.nx * nw.xStep;
+            } else { nw.xWfrMin = old.xWfrMin; nw.xWfrMax = old.xWfrMax; }
+        } else {
+            double tol = 0.01 * nw.zStep;
+            if ((::fabs(old.zWfrMin - old.zStart) < tol) && (::fabs(old.zStart + old.nz * old.zStep - old.zWfrMax) < tol)) {
+                nw.zWfrMin = nw.zStart; nw.zWfrMax = nw.zStart + nw.nz * nw.zStep;
+            } else { nw.zWfrMin = old.zWfrMin; nw.zWfrMax = old.zWfrMax; }
+        }
+    };
+    double xMagOld = (w.nx - 1) * w.xStep;
+    if (pxm > 1.) {
+        long NxInner = (pxd != 1.) ? (long)(NewNx / pxm) : w.nx;
+        long d = NewNx - NxInner;
+        long left = d >> 1;
+        if ((left << 1) != d) left++;
+        nw.xStep = xMagOld / (NxInner - 1);
+        nw.xStart = w.xStart - left * nw.xStep;
+        nw.AuxLong1 = left;
+        nw.AuxLong2 = left + NxInner - 1;
+        preserve('x');
+    } else {
+        double xEndOld = w.xStart + (w.nx - 1) * w.xStep;
+        double xMid = 0.5 * (w.xStart + xEndOld);
+        double xMagNew = xMagOld * pxm;
+        nw.xStep = xMagNew / (NewNx - 1);
+        if (pxd == 1) { nw.xStep = w.xStep; xMagNew = (NewNx - 1) * nw.xStep; }
+        nw.xStart = xMid - 0.5 * xMagNew;
+        nw.AuxLong1 = 0;
+        nw.AuxLong2 = NewNx - 1;
+        if (nw.xStart > nw.xWfrMin) nw.xWfrMin = nw.xStart;
+        if ((nw.xStart + xMagNew) < nw.xWfrMax) nw.xWfrMax = nw.xStart + xMagNew;
+    }
+    double zMagOld = (w.nz - 1) * w.zStep;
+    if (pzm > 1.) {
+        long NzInner = (pzd != 1.) ? (long)(NewNz / pzm) : w.nz;
+        long d = NewNz - NzInner;
+        long left = d >> 1;
+        if ((left << 1) != d) left++;
+        nw.zStep = zMagOld / (NzInner - 1);
+        nw.zStart = w.zStart - left * nw.zStep;
+        nw.AuxLong3 = left;
+        nw.AuxLong4 = left + NzInner - 1;
+        preserve('z');
+    } else {
+        double zEndOld = w.zStart + (w.nz - 1) * w.zStep;
+        double zMid = 0.5 * (w.zStart + zEndOld);
+        double zMagNew = zMagOld * pzm;
+        nw.zStep = zMagNew / (NewNz - 1);
+        if (pzd == 1) { nw.zStep = w.zStep; zMagNew = (NewNz - 1) * nw.zStep; }
+        nw.zStart = zMid - 0.5 * zMagNew;
+        nw.AuxLong3 = 0;
+        nw.AuxLong4 = NewNz - 1;
+        if (nw.zStart > nw.zWfrMin) nw.zWfrMin = nw.zStart;
+        if ((nw.zStart + zMagNew) < nw.zWfrMax) nw.zWfrMax = nw.zStart + zMagNew;
+    }
+    bool grow = (pxmIn * pxdIn * pzmIn * pzdIn) >= 1.;
+    if (grow && changed) { WfrState t = w; w = nw; srwl_roundtrip(); nw = w; w = t; }
+
+    const double RelStepTol = 1.e-05;
+    bool only_larger = ((pxd == 1.) && (pzd == 1.) && (pxm >= 1.) && (pzm >= 1.)) &&
+                       ((::fabs(old.xStep - nw.xStep) < RelStepTol) && (::fabs(old.zStep - nw.zStep) < RelStepTol));
+    if (only_larger) {
+        b->resize(old, nw, 1);
+        w = nw;
+    } else {
+        bool origQX = old.QuadX, origQZ = old.QuadZ;
+        // WaveFrontTermCanBeTreated (sroptelm.cpp:4692), checkBenefit = false
+        bool qx = ::fabs(old.RobsXAbsErr) < 0.4 * ::fabs(old.RobsX);
+        bool qz = ::fabs(old.RobsZAbsErr) < 0.4 * ::fabs(old.RobsZ);
+        bool treated = false;
+        if ((qx || qz) && old.Pres < 1) {
+            w.QuadX = qx; w.QuadZ = qz;
+            treat_quad('r');            // on the old mesh, before the gather
+            nw.QuadX = qx; nw.QuadZ = qz;
+            treated = true;
+        }
+        b->resize(old, nw, 0);
+        w = nw;
+        if (treated) treat_quad('a');   // on the new mesh
+        w.QuadX = origQX; w.QuadZ = origQZ;
+    }
+    if (!grow && changed) srwl_roundtrip();
+    if (other_side) {
+        int to = (w.Pres == 0) ? 1 : 0;
+        set_rad_repres(to);
+        if (useStartTrOther) {
+            double xcOld = xStartOld + (nxOld >> 1) * xStepOld;
+            w.xStart = xcOld - (w.nx >> 1) * w.xStep;
+            double zcOld = zStartOld + (nzOld >> 1) * zStepOld;
+            w.zStart = zcOld - (w.nz >> 1) * w.zStep;
+            set_full_range();
+        }
+    }
+    return 0;
+}
+
+// ================================================================================================
+// Container (PropagateRadiationGuided, sroptcnt.cpp:254-425)
+// ================================================================================================
+int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
+{
+    kernels.clear();
+    maxElems = 0;
+    err.clear();
+    if (pw == nullptr || opt == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
+    // InSRWRadPtrs (srradstr.cpp:501)
+    const SRWLRadMesh& m = pw->mesh;
+    w = WfrState();
+    w.eStart = m.eStart;
+    if (m.nx <= 1) { w.xStart = 0.5 * (m.xStart + m.xFin); w.xStep = 0.; }
+    else { w.xStart = m.xStart; w.xStep = (m.xFin - m.xStart) / (m.nx - 1); }
+    if (m.ny <= 1) { w.zStart = 0.5 * (m.yStart + m.yFin); w.zStep = 0.; }
+    else { w.zStart = m.yStart; w.zStep = (m.yFin - m.yStart) / (m.ny - 1); }
+    w.nx = (int)m.nx; w.nz = (int)m.ny;
+    w.yStart = m.zStart;
+    w.RobsX = pw->Rx; w.RobsZ = pw->Ry; w.RobsXAbsErr = pw->dRx; w.RobsZAbsErr = pw->dRy;
+    w.xc = pw->xc; w.zc = pw->yc;
+    w.xWfrMin = m.xStart; w.xWfrMax = m.xFin; w.zWfrMin = m.yStart; w.zWfrMax = m.yFin;
+    w.Pres = pw->presCA;
+    w.avgPhotEn = pw->avgPhotEn;
+    if (pw->arMomX != nullptr) { for (int i = 0; i < 11; i++) w.momX[i] = pw->arMomX[i]; w.haveMom = true; }
+    if (pw->arMomY != nullptr) for (int i = 0; i < 11; i++) w.momZ[i] = pw->arMomY[i];
+    if (m.ne != 1) { err = "only ne == 1 wavefronts are supported on the GPU path"; return SRWG_ERR_UNSUPPORTED; }
+    if (pw->presFT != 0) { err = "time-domain wavefronts are not supported on the GPU path"; return SRWG_ERR_UNSUPPORTED; }
+    if (pw->numTypeElFld != 0 && pw->numTypeElFld != 'f') { err = "only float fields are supported"; return SRWG_ERR_UNSUPPORTED; }
+    in = w;
+    std::vector<ElemDesc> els;
+    std::vector<PropDesc> props;
+    int r = flatten(opt, els, props, false);
+    if (r) return r;
+    if ((w.nx <= 1) || (w.nz <= 1)) return CAN_NOT_PROPAGATE_1D_RAD;   // CheckRadStructForPropagation
+
+    Builder bld(kernels, maxElems);
+    b = &bld;
+    const double tolRes = 1.e-04;
+    try {
+        size_t numRes = props.size();
+        size_t i = 0;
+        for (; i < els.size(); i++) {
+            const ElemDesc& e = els[i];
+            int anal = 0;
+            if (i < numRes) {
+                const PropDesc& p = props[i];
+                if (p.n >= 0) {
+                    if ((int)p.get(0, 0) || (int)p.get(1, 0)) {
+                        err = "automatic resizing (pp[0], pp[1]) is not supported on the GPU path";
+                        throw (int)SRWG_ERR_UNSUPPORTED;
+                    }
+                    anal = (int)p.get(3, 0);
+                    double pxm = p.get(5, 1.), pxd = p.get(6, 1.), pzm = p.get(7, 1.), pzd = p.get(8, 1.);
+                    int sh = (int)(char)p.get(9, 0);
+                    if ((::fabs(pxd - 1.) > tolRes) || (::fabs(pxm - 1.) > tolRes) || (::fabs(pzd - 1.) > tolRes) ||
+                        (::fabs(pzm - 1.) > tolRes) || (sh > 0)) {
+                        int rr = resize(pxm, pxd, pzm, pzd, sh, p.get(10, 0.), p.get(11, 0.), (int)p.get(4, 0) != 0);
+                        if (rr) throw rr;
+                    }
+                }
+            }
+            if (e.kind == E_DRIFT) drift(e, anal);
+            else if (e.kind == E_LENS) lens(e);
+            else if (e.kind == E_APERTURE) aperture(e);
+        }
+        if (i < numRes && props[i].n >= 0) {
+            const PropDesc& p = props[i];
+            double pxm = p.get(5, 1.), pxd = p.get(6, 1.), pzm = p.get(7, 1.), pzd = p.get(8, 1.);
+            if ((::fabs(pxd - 1.) > tolRes) || (::fabs(pxm - 1.) > tolRes) || (::fabs(pzd - 1.) > tolRes) ||
+                (::fabs(pzm - 1.) > tolRes)) {
+                int rr = resize(pxm, pxd, pzm, pzd, 0, 0., 0., (int)p.get(4, 0) != 0);
+                if (rr) throw rr;
+            }
+        }
+    } catch (int code) {
+        b = nullptr;
+        return code;
+    }
+    bld.close();
+    outBuf = bld.cur;
+    b = nullptr;
+    // the GPU passes need even line lengths (centring rotation) and at most 16384 points per line
+    for (const KernelDesc& k : kernels) {
+        if (k.kind == K_LINE) {
+            int N = k.line.axis == 0 ? k.line.nx : k.line.nz;
+            if ((N & 1) || N > 16384 || N < 4) {
+                err = "FFT length " + std::to_string(N) + " not supported on the GPU path (even, 4..16384)";
+                return SRWG_ERR_UNSUPPORTED;
+            }
+        }
+        if (k.kind == K_RESIZE && !k.rs.only_larger && (k.rs.nxo < 4 || k.rs.nzo < 4)) {
+            err = "resize of a mesh smaller than 4 points";
+            return SRWG_ERR_UNSUPPORTED;
+        }
+    }
+    return 0;
+}
+
+std::string Planner::describe() const
+{
+    std::string s;
+    char buf[512];
+    for (size_t i = 0; i < kernels.size(); i++) {
+        const KernelDesc& k = kernels[i];
+        if (k.kind == K_LINE) {
+            const LineDesc& d = k.line;
+            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d  buf %d->%d\n", i,
+                     d.axis == 0 ? "rows" : "cols", d.nx, d.nz, d.f1, d.has_pw, d.pw.has_quad, d.pw.has_ang, d.pw.nmask,
+                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, k.src, k.dst);
+        } else if (k.kind == K_RESIZE) {
+            snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pw=%d  buf %d->%d\n", i, k.rs.nxo, k.rs.nzo,
+                     k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pw, k.src, k.dst);
+        } else {
+            snprintf(buf, sizeof(buf), "%zu PW %dx%d (q%d a%d m%d s%d) mirror=%d/%d  buf %d->%d\n", i, k.pwk.nx, k.pwk.nz,
+                     k.pwk.pw.has_quad, k.pwk.pw.has_ang, k.pwk.pw.nmask, k.pwk.pw.has_scale, k.pwk.mirror_x,
+                     k.pwk.mirror_z, k.src, k.dst);
+        }
+        s += buf;
+    }
+    return s;
+}
+
+}  // namespace srwg

@@ -1,0 +1,84 @@
+// Host planner: the reference's per-element bookkeeping (meshes, radii, centres, moments) in FP64
+// with the reference's operation order, lowered into fused GPU passes (kdesc.h).
+#pragma once
+#include <string>
+#include <vector>
+#include "kdesc.h"
+#include "../../include/srwl_b200.h"
+
+namespace srwg {
+
+// Subset of srTSRWRadStructAccessData (cpp/src/core/srradstr.h:67) used by this path, ne == 1.
+struct WfrState {
+    int nx = 0, nz = 0;
+    double eStart = 0, xStart = 0, xStep = 0, zStart = 0, zStep = 0;
+    double yStart = 0, avgPhotEn = 0;
+    double RobsX = 0, RobsZ = 0, RobsXAbsErr = 0, RobsZAbsErr = 0, xc = 0, zc = 0;
+    double xWfrMin = 0, xWfrMax = 0, zWfrMin = 0, zWfrMax = 0;
+    int Pres = 0;
+    double xStartTr = 0, zStartTr = 0;
+    bool UseStartTrToShiftAtChangingRepresToCoord = false;
+    long AuxLong1 = 0, AuxLong2 = 0, AuxLong3 = 0, AuxLong4 = 0;
+    bool xLinOnly = false, zLinOnly = false;
+    double dxcSub = 0, dzcSub = 0;
+    bool QuadX = false, QuadZ = false;
+    double momX[11] = {0}, momZ[11] = {0};
+    bool haveMom = false;
+    bool momentsStale = false;   // the reference would recompute them numerically (not done here)
+};
+
+enum ElemKind { E_DRIFT = 1, E_APERTURE = 2, E_LENS = 3 };
+
+struct ElemDesc {
+    int kind = 0;
+    double L = 0; int treat = 0;                            // drift
+    char shape = 'r', apob = 'a'; double Dx = 0, Dy = 0;    // aperture / obstacle
+    double Fx = 0, Fy = 0;                                  // lens
+    double x = 0, y = 0;                                    // centre
+};
+
+struct PropDesc {
+    int n = 0;
+    double pp[17] = {0};
+    double get(int i, double def) const { return i < n ? pp[i] : def; }
+};
+
+class Builder;
+
+class Planner {
+public:
+    WfrState w;                          // evolves from the input to the output state
+    WfrState in;
+    std::vector<KernelDesc> kernels;
+    int outBuf = 0;                      // buffer holding the result (0: the input itself)
+    long long maxElems = 0;              // largest grid over all work buffers
+    std::string err;
+
+    // flattens SRWLOptC (nested containers included) and plans; returns 0 or an SRW error number
+    int plan(const SRWLWfr* wfr, const SRWLOptC* opt);
+    std::string describe() const;
+
+private:
+    Builder* b = nullptr;
+    int flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vector<PropDesc>& props, bool nested);
+    void set_full_range();
+    void srwl_roundtrip();
+    void set_rad_repres(int coord_or_ang);
+    void fft2_emit(int dir, bool use_given, double& xStepTr, double& zStepTr, double& xStartTr, double& zStartTr);
+    void drift(const ElemDesc& e, int anal);
+    void drift_ang(const ElemDesc& e);
+    void drift_to_waist(const ElemDesc& e);
+    int drift_quad(const ElemDesc& e, int subtype);
+    void drift_moments(double L);
+    void lens(const ElemDesc& e);
+    void aperture(const ElemDesc& e);
+    void phase_lin_subtract(double newXc, double newZc);
+    void phase_lin_reset();
+    void fix_abs_err();
+    void mirror(int sx, int sz);
+    int resize(double pxm, double pxd, double pzm, double pzd, int shift, double xcs, double zcs, bool other_side);
+    void treat_quad(char add_or_rem);
+    double diff_lim_spot(char xz, double L) const;
+};
+
+}  // namespace srwg

@@ -1,0 +1,201 @@
+"""Drop-in for the reference's ``srwlpy.PropagElecField`` (cpp/src/clients/python/srwlpy.cpp:5214)
+on the GPU path:
+
+    from srw_b200 import srwlpy as srwl
+    srwl.PropagElecField(wfr, optBL)          # wfr, optBL: SRWLWfr / SRWLOptC objects
+
+Arguments, return value and error behaviour follow the reference: elements of ``optC.arOpt`` are
+dispatched by class name (SRWLOptD -> "drift", SRWLOptA -> "aperture", SRWLOptL -> "lens",
+SRWLOptC -> "container", srwlpy.cpp:2678-2700); ``optC.arProp`` is a list of propagation
+parameter lists; field arrays must expose a float32 buffer (numpy or ``array('f')``); when the
+mesh size changes the wavefront is re-allocated through ``wfr.allocate(ne, nx, ny, EXNeeded,
+EYNeeded, typeE, backupNeeded)`` (srwlpy.cpp:4141); after the call the mesh, radii, centres and
+representation flags are written back to the Python object (UpdatePyWfr, srwlpy.cpp:3599); errors
+raise RuntimeError with the library's error text.  ``dev`` is the 1-based GPU index (default 1).
+"""
+import ctypes as C
+from array import array
+
+import numpy as np
+
+from . import capi
+
+_ELEM_TYPES = {'SRWLOptD': 'drift', 'SRWLOptA': 'aperture', 'SRWLOptL': 'lens', 'SRWLOptC': 'container'}
+
+
+def _buf_ptr(a, keep, dtype):
+    """Address of a contiguous buffer of the given numpy dtype (numpy array or array.array)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if a.dtype != dtype or not a.flags['C_CONTIGUOUS']:
+            raise RuntimeError('field/moment arrays must be contiguous %s' % np.dtype(dtype).name)
+        keep.append(a)
+        return a.ctypes.data
+    if isinstance(a, array):
+        if np.dtype(a.typecode) != np.dtype(dtype):
+            raise RuntimeError("array type '%s' where %s is required" % (a.typecode, np.dtype(dtype).name))
+        keep.append(a)
+        return a.buffer_info()[0] if len(a) > 0 else None
+    m = memoryview(a)
+    keep.append(m)
+    npv = np.frombuffer(m, dtype=dtype)
+    keep.append(npv)
+    return npv.ctypes.data
+
+
+def _chr(v, default):
+    if v is None:
+        return default
+    if isinstance(v, (bytes, bytearray)):
+        return bytes(v[:1])
+    if isinstance(v, str):
+        return v[:1].encode()
+    return bytes([int(v) & 0xff])
+
+
+def make_c_wfr(wfr, keep):
+    """SRWLWfr (C) view of a Python wavefront object (ParseSructSRWLWfr, srwlpy.cpp:3058)."""
+    w = capi.SRWLWfr()
+    w.arEx = _buf_ptr(getattr(wfr, 'arEx', None), keep, np.float32)
+    w.arEy = _buf_ptr(getattr(wfr, 'arEy', None), keep, np.float32)
+    m = wfr.mesh
+    w.mesh.eStart, w.mesh.eFin = float(m.eStart), float(m.eFin)
+    w.mesh.xStart, w.mesh.xFin = float(m.xStart), float(m.xFin)
+    w.mesh.yStart, w.mesh.yFin = float(m.yStart), float(m.yFin)
+    w.mesh.zStart = float(getattr(m, 'zStart', 0.))
+    w.mesh.ne, w.mesh.nx, w.mesh.ny = int(m.ne), int(m.nx), int(m.ny)
+    w.Rx, w.Ry = float(wfr.Rx), float(wfr.Ry)
+    w.dRx, w.dRy = float(wfr.dRx), float(wfr.dRy)
+    w.xc, w.yc = float(wfr.xc), float(wfr.yc)
+    w.avgPhotEn = float(getattr(wfr, 'avgPhotEn', 0.))
+    w.presCA = _chr(int(getattr(wfr, 'presCA', 0)), b'\0')
+    w.presFT = _chr(int(getattr(wfr, 'presFT', 0)), b'\0')
+    w.numTypeElFld = _chr(getattr(wfr, 'numTypeElFld', 'f'), b'f')
+    w.unitElFld = _chr(int(getattr(wfr, 'unitElFld', 1)), b'\1')
+    w.unitElFldAng = _chr(int(getattr(wfr, 'unitElFldAng', 0)), b'\0')
+    w.arMomX = _buf_ptr(getattr(wfr, 'arMomX', None), keep, np.float64) if len(getattr(wfr, 'arMomX', [])) >= 11 else None
+    w.arMomY = _buf_ptr(getattr(wfr, 'arMomY', None), keep, np.float64) if len(getattr(wfr, 'arMomY', [])) >= 11 else None
+    return w
+
+
+def make_c_optc(opt, keep):
+    """SRWLOptC (C) view of a Python container (ParseSructSRWLOptC, srwlpy.cpp:2618)."""
+    els = list(opt.arOpt)
+    props = list(getattr(opt, 'arProp', []) or [])
+    n = len(els)
+    if n <= 0:
+        raise RuntimeError('No objects in optical container')
+    c = capi.SRWLOptC()
+    arOpt = (C.c_void_p * n)()
+    arTypes = (C.c_char_p * n)()
+    for i, e in enumerate(els):
+        cls = type(e).__name__
+        kind = _ELEM_TYPES.get(cls)
+        if kind is None:
+            raise RuntimeError('optical element %s is not supported on the GPU path' % cls)
+        if kind == 'drift':
+            s = capi.SRWLOptD(float(e.L), _chr(int(getattr(e, 'treat', 0)), b'\0'))
+        elif kind == 'aperture':
+            s = capi.SRWLOptA(_chr(e.shape, b'r'), _chr(e.ap_or_ob, b'a'), float(e.Dx), float(e.Dy), float(e.x), float(e.y))
+        elif kind == 'lens':
+            s = capi.SRWLOptL(float(e.Fx), float(e.Fy), float(e.x), float(e.y))
+        else:
+            s = make_c_optc(e, keep)
+        keep.append(s)
+        arOpt[i] = C.cast(C.pointer(s), C.c_void_p)
+        tb = C.create_string_buffer(kind.encode())
+        keep.append(tb)
+        arTypes[i] = C.cast(tb, C.c_char_p)
+    keep += [arOpt, arTypes]
+    c.arOpt = C.cast(arOpt, C.POINTER(C.c_void_p))
+    c.arOptTypes = C.cast(arTypes, C.POINTER(C.c_char_p))
+    c.nElem = n
+    npr = len(props)
+    if npr > 0:
+        arProp = (C.POINTER(C.c_double) * npr)()
+        arPropN = C.create_string_buffer(npr)
+        for i, p in enumerate(props):
+            vals = [float(v) for v in p] if isinstance(p, (list, tuple, array, np.ndarray)) else []
+            buf = (C.c_double * max(1, len(vals)))(*vals)
+            keep.append(buf)
+            arProp[i] = C.cast(buf, C.POINTER(C.c_double))
+            arPropN[i] = bytes([len(vals)])
+        keep += [arProp, arPropN]
+        c.arProp = C.cast(arProp, C.POINTER(C.POINTER(C.c_double)))
+        c.arPropN = C.cast(arPropN, C.c_char_p)
+    c.nProp = npr
+    return c
+
+
+def _update_py_wfr(wfr, w):
+    """UpdatePyWfr (srwlpy.cpp:3599)."""
+    m = wfr.mesh
+    m.eStart, m.eFin = w.mesh.eStart, w.mesh.eFin
+    m.xStart, m.xFin = w.mesh.xStart, w.mesh.xFin
+    m.yStart, m.yFin = w.mesh.yStart, w.mesh.yFin
+    m.zStart = w.mesh.zStart
+    m.ne, m.nx, m.ny = int(w.mesh.ne), int(w.mesh.nx), int(w.mesh.ny)
+    wfr.Rx, wfr.Ry, wfr.dRx, wfr.dRy = w.Rx, w.Ry, w.dRx, w.dRy
+    wfr.xc, wfr.yc = w.xc, w.yc
+    wfr.avgPhotEn = w.avgPhotEn
+    wfr.presCA = ord(w.presCA) if w.presCA else 0
+    wfr.presFT = ord(w.presFT) if w.presFT else 0
+
+
+_state = {'wfr': None, 'keep': None}
+
+
+@capi.MODIF_FUNC
+def _modif(action, pw, pol):
+    """Re-allocation callback (ModifySRWLWfr, srwlpy.cpp:4141)."""
+    try:
+        wfr = _state['wfr']
+        if wfr is None or action < 0:
+            return -1
+        p = pol if isinstance(pol, int) else (pol[0] if pol else 0)
+        ex_needed = 1 if p in (0, ord('x'), ord('X')) else 0
+        ey_needed = 1 if p in (0, ord('y'), ord('Y'), ord('z'), ord('Z')) else 0
+        w = pw.contents
+        if action in (2, 12):
+            wfr.allocate(int(w.mesh.ne), int(w.mesh.nx), int(w.mesh.ny), ex_needed, ey_needed,
+                         getattr(wfr, 'numTypeElFld', 'f'), 1 if action == 12 else 0)
+        elif action == 0:
+            wfr.allocate(0, 0, 0, 1, 1, getattr(wfr, 'numTypeElFld', 'f'))
+        else:
+            return -1
+        keep = _state['keep']
+        w.arEx = _buf_ptr(wfr.arEx, keep, np.float32)
+        w.arEy = _buf_ptr(wfr.arEy, keep, np.float32)
+        w.arMomX = _buf_ptr(wfr.arMomX, keep, np.float64) if len(wfr.arMomX) >= 11 else None
+        w.arMomY = _buf_ptr(wfr.arMomY, keep, np.float64) if len(wfr.arMomY) >= 11 else None
+        return 0
+    except Exception:
+        return -1
+
+
+def PropagElecField(wfr, optC, intList=None, dev=None):
+    """Propagates ``wfr`` in place through ``optC`` on the GPU; returns ``wfr``."""
+    if wfr is None or optC is None:
+        raise RuntimeError('Incorrect arguments for PropagElecField')
+    if intList is not None:
+        raise RuntimeError('intermediate intensity extraction is not supported on the GPU path')
+    L = capi.lib()
+    keep = []
+    w = make_c_wfr(wfr, keep)
+    o = make_c_optc(optC, keep)
+    par = None
+    if dev is not None:
+        par = (C.c_double * 2)(1., float(dev))
+    _state['wfr'] = wfr
+    _state['keep'] = keep
+    try:
+        L.srwlUtiSetWfrModifFunc(_modif)
+        r = L.srwlPropagElecField(C.byref(w), C.byref(o), 0, None, None, None, par)
+    finally:
+        _state['wfr'] = None
+        _state['keep'] = None
+    if r > 0:
+        raise RuntimeError(capi.err_text(r))
+    _update_py_wfr(wfr, w)
+    return wfr

@@ -1,0 +1,90 @@
+"""CPU tests of the C-ABI library: it loads, exports every entry point declared in include/*.h,
+and its host planner reproduces the reference's meshes and wavefront scalars bit-exactly (the
+planning half of srwlPropagElecField runs without a GPU)."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from srw_b200 import capi
+from srw_b200.plan import Plan
+from tests.golden_cases import case_io, load
+from tests.helpers import beamline, gaussian, make_wfr, C1, C1PP, PP
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+D, INDEX = load()
+
+
+def header_symbols():
+    names = []
+    inc = os.path.join(REPO, 'include')
+    for f in os.listdir(inc):
+        if f.endswith('.h'):
+            names += re.findall(r'SRWG_API\s+[\w\s\*]+?\b(\w+)\s*\(', open(os.path.join(inc, f)).read())
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = capi.lib()
+    names = header_symbols()
+    assert 'srwlPropagElecField' in names and 'srwgPlanExecute' in names
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(capi.SYMBOLS), set(names) ^ set(capi.SYMBOLS)
+
+
+def test_error_texts():
+    assert 'callback' in capi.err_text(23172)
+    assert 'one point' in capi.err_text(23059)
+
+
+def plan_case(name):
+    c = next(c for c in INDEX if c['name'] == name)
+    i, o = case_io(D, name)
+    w = make_wfr(i['ex'], i['ey'], i['mesh'], i['Rx'], i['Ry'], i['dRx'], i['dRy'], i['xc'], i['yc'],
+                 i['momX'], i['momY'])
+    return Plan(w, beamline(c['elements'], c['props'])), o
+
+
+@pytest.mark.parametrize('name', [c['name'] for c in INDEX])
+def test_planner_mesh_bit_exact(name):
+    p, o = plan_case(name)
+    m = p.output_mesh()
+    mine = np.array([m['nx'], m['ny'], m['xStart'], m['xFin'], m['yStart'], m['yFin']])
+    assert np.array_equal(mine, o['mesh_raw']), (mine, o['mesh_raw'])
+    assert [m['Rx'], m['Ry'], m['dRx'], m['dRy'], m['xc'], m['yc']] == [o['Rx'], o['Ry'], o['dRx'], o['dRy'], o['xc'], o['yc']]
+
+
+def test_pass_fusion_counts():
+    # C0: 2 angular drifts around aperture+lens -> 5 passes; C1: aperture, resize(+lens), to-waist -> 4
+    assert plan_case('c0_64')[0].n_kernels == 5
+    assert plan_case('c1_64')[0].n_kernels == 4
+    assert plan_case('c2_128')[0].n_kernels == 5
+
+
+def test_full_size_c1_plan():
+    ex, ey, mesh = gaussian(1024, E=2000., sig=0.4e-3, r=1.5e-3)
+    w = make_wfr(ex, ey, mesh, Rx=20., Ry=20., dRx=0.2, dRy=0.2)
+    p = Plan(w, beamline(C1, C1PP))
+    assert (p.nx_out, p.ny_out) == (4096, 4096)
+    k = p.kernels()
+    assert k[1][0] == 'resize' and k[1][3:] == (4096, 4096)
+
+
+def test_unsupported_and_invalid_inputs_raise():
+    ex, ey, mesh = gaussian(64)
+    w = make_wfr(ex, ey, mesh)
+    with pytest.raises(RuntimeError, match='pp\\[3\\]=5'):
+        Plan(w, beamline([('drift', 1., 0)], [PP(5)]))
+    with pytest.raises(RuntimeError, match='automatic resizing'):
+        Plan(w, beamline([('drift', 1., 0)], [[1, 0, 1., 0, 0, 1., 1., 1., 1.]]))
+    ex1, ey1, mesh1 = gaussian(64, ny=1)
+    with pytest.raises(RuntimeError, match='one point'):
+        Plan(make_wfr(ex1, ey1, mesh1), beamline([('drift', 1., 0)], [PP()]))
+
+    class SRWLOptT(object):
+        pass
+    from srw_b200.srwlib import SRWLOptC
+    with pytest.raises(RuntimeError, match='not supported'):
+        Plan(w, SRWLOptC([SRWLOptT()], [PP()]))

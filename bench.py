@@ -294,15 +294,17 @@ def run_ours(args, rank, world):
         srwl.PropagElecField(wp, bl, None, dev.index + 1)
         return wp
 
-    for _ in range(2):
-        e2e_once()
-    n_e2e = max(3, min(args.steps, 10))
-    t0 = time.perf_counter()
-    for _ in range(n_e2e):
-        wp = e2e_once()
-        _ = float(wp.arEx[0])                                  # host read of the result
-    e2e_s = time.perf_counter() - t0
-    e2e_val = world * n_e2e / e2e_s
+    e2e_val = None
+    if not args.no_e2e:
+        for _ in range(2):
+            e2e_once()
+        n_e2e = max(3, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for _ in range(n_e2e):
+            wp = e2e_once()
+            _ = float(wp.arEx[0])                              # host read of the result
+        e2e_s = time.perf_counter() - t0
+        e2e_val = world * n_e2e / e2e_s
 
     if rank != 0:
         return
@@ -340,6 +342,7 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end leg (profiling runs)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))

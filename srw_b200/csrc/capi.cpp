@@ -116,14 +116,39 @@ static int line_config(const LineDesc& d, LineLaunch& p)
     int N = d.axis == 0 ? d.nx : d.nz;
     p.N = N;
     p.nlines = d.axis == 0 ? d.nz : d.nx;
-    // T threads per line, at most 16 points each; G = threads per CTA / T groups work on the
-    // CTA's L lines in batches
+    const size_t cap = SRWG_LINE_SMEM_MAX;
+    if (N >= 64 && N <= 16384 && (N & (N - 1)) == 0) {
+        // power of two: 16 points per thread, radix-16 stages then a 16/8/4/2 stage
+        p.v2 = 1;
+        p.T = N / 16;
+        int nb = 0;
+        while ((1 << nb) < N) nb++;
+        p.nst = 0;
+        while (nb > 4 && nb - 4 >= 1) {
+            if (nb - 4 < 1) break;
+            p.radix[p.nst++] = 16;
+            nb -= 4;
+        }
+        p.radix[p.nst++] = 1 << nb;          // 16, 8, 4 or 2
+        p.P = N + N / 16;
+        int L = d.axis == 0 ? (256 / p.T) : (1024 / p.T);
+        if (L < 1) L = 1;
+        if (d.axis == 1 && L > 32) L = 32;
+        while (L > 1 && (size_t)L * p.P * sizeof(float2) > cap) L--;
+        if (p.T * L > 1024) { g_lastDetail = "line pass too large"; return SRWG_ERR_UNSUPPORTED; }
+        p.L = L;
+        p.G = L;
+        if ((size_t)p.L * p.P * sizeof(float2) > cap) { g_lastDetail = "line too long for shared memory"; return SRWG_ERR_UNSUPPORTED; }
+        return 0;
+    }
+    p.v2 = 0;
+    // general good number: T threads per line, at most 16 points each; G = threads per CTA / T
+    // groups work on the CTA's L lines in batches
     int T = (N + 15) / 16;
     T = ((T + 31) / 32) * 32;
     if (T < 32) T = 32;
     if (T > 512) { g_lastDetail = "FFT length above 8192"; return SRWG_ERR_UNSUPPORTED; }
     p.T = T;
-    const size_t cap = SRWG_LINE_SMEM_MAX;
     int L;
     if (d.axis == 0) {
         L = 256 / T > 1 ? 256 / T : 1;          // rows: ~256 threads, one batch

@@ -443,6 +443,166 @@ __global__ void __launch_bounds__(512, 1) line_kernel(const LineLaunch p)
 }
 
 // ------------------------------------------------------------------------------------------------
+// LINE pass, power-of-two lines (N >= 64): every thread owns 16 points of its line.  The first
+// FFT stage reads its butterfly inputs straight from global memory through the point-wise chain
+// (coalesced: thread t reads t + T*m), the last stage writes straight to global memory through
+// the output chain; intermediate stages exchange through shared memory padded by one point per
+// 16 (conflict-free Stockham writes).  A second transform in the same pass (f1 -> f2) reads the
+// first one's output from shared memory through the middle chain.
+// ------------------------------------------------------------------------------------------------
+#define PADI(p) ((p) + ((p) >> 4))
+
+// output index k whose source is q under a store chain (no pre-rotation): k = mir(rot(q))
+__device__ __forceinline__ int chain_inv(const Chain& c, int q, int N)
+{
+    int i = q;
+    if (c.rs1) { i = q + (N >> 1); if (i >= N) i -= N; }
+    return c.mir ? (N - 1 - i) : i;
+}
+
+// IN: 0 shared, 1 shared through chain cin, 2 global through chain cin;  OUT: 0 shared, 1 global through chain cout
+template <int R, int DIR, int IN, int OUT>
+__device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
+                                        long long gstr, int N, int Ns, int t, int T, int line, const Chain& cin,
+                                        const Chain& cout, const float2* __restrict__ tw, bool active)
+{
+    constexpr int B = 16 / R;
+    const int NR = N / R;
+    const int lgNs = __ffs(Ns) - 1;
+    const int tws = N / (Ns * R);
+    float2 v[B][R];
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+        const int j = t + T * b;
+        const int k = j & (Ns - 1);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int p = j + r * NR;
+            float2 x = make_float2(0.f, 0.f);
+            if (active) {
+                if (IN == 0) {
+                    x = s[PADI(p)];
+                } else {
+                    int sp;
+                    float2 f = chain_eval(cin, p, N, line, sp);
+                    x = (IN == 1) ? s[PADI(sp)] : __ldcs(&gin[(long long)sp * gstr]);
+                    x = cmul(f, x);
+                }
+                if (r > 0 && k != 0) {
+                    float2 w = __ldg(&tw[k * tws * r]);
+                    if (DIR < 0) w.y = -w.y;
+                    x = cmul(x, w);
+                }
+            }
+            v[b][r] = x;
+        }
+    }
+    if (OUT == 0) __syncthreads();
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+        const int j = t + T * b;
+        const int k = j & (Ns - 1);
+        dftR<R, DIR>(v[b], tw, N);
+        const int base = ((j >> lgNs) << lgNs) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int q = base + r * Ns;
+            if (active) {
+                if (OUT == 0) {
+                    s[PADI(q)] = v[b][r];
+                } else {
+                    int i = chain_inv(cout, q, N), sp;
+                    float2 f = chain_eval(cout, i, N, line, sp);
+                    __stcs(&gout[(long long)i * gstr], cmul(f, v[b][r]));
+                }
+            }
+        }
+    }
+    if (OUT == 0) __syncthreads();
+}
+
+// last stage dispatch on its radix (16, 8, 4, 2)
+template <int DIR, int OUT>
+__device__ __forceinline__ void stage_last(int R, float2* s, float2* __restrict__ gout, long long gstr, int N, int Ns,
+                                           int t, int T, int line, const Chain& cin, const Chain& cout,
+                                           const float2* __restrict__ tw, bool active)
+{
+    switch (R) {
+    case 16: stage16<16, DIR, 0, OUT>(s, nullptr, gout, gstr, N, Ns, t, T, line, cin, cout, tw, active); break;
+    case 8: stage16<8, DIR, 0, OUT>(s, nullptr, gout, gstr, N, Ns, t, T, line, cin, cout, tw, active); break;
+    case 4: stage16<4, DIR, 0, OUT>(s, nullptr, gout, gstr, N, Ns, t, T, line, cin, cout, tw, active); break;
+    default: stage16<2, DIR, 0, OUT>(s, nullptr, gout, gstr, N, Ns, t, T, line, cin, cout, tw, active); break;
+    }
+}
+
+// one FFT along the line: radix-16 stages then radix[nst-1]; IN mode of the first stage, OUT of the last
+template <int DIR, int IN, int OUT>
+__device__ __forceinline__ void fft16(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
+                                      long long gstr, int N, const int* radix, int nst, int t, int T, int line,
+                                      const Chain& cin, const Chain& cout, const float2* __restrict__ tw, bool active)
+{
+    stage16<16, DIR, IN, 0>(s, gin, nullptr, gstr, N, 1, t, T, line, cin, cout, tw, active);
+    int Ns = 16;
+    for (int st = 1; st < nst - 1; st++) {
+        stage16<16, DIR, 0, 0>(s, nullptr, nullptr, gstr, N, Ns, t, T, line, cin, cout, tw, active);
+        Ns *= 16;
+    }
+    stage_last<DIR, OUT>(radix[nst - 1], s, gout, gstr, N, Ns, t, T, line, cin, cout, tw, active);
+}
+
+template <bool COLS>
+__global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
+{
+    extern __shared__ float2 sm[];
+    __shared__ LineDesc d;
+    __shared__ int radix[SRWG_MAX_STAGES];
+    if (threadIdx.x == 0) {
+        d = p.d;
+        for (int i = 0; i < SRWG_MAX_STAGES; i++) radix[i] = p.radix[i];
+    }
+    __syncthreads();
+    const int comp = blockIdx.y;
+    const float2* __restrict__ src = p.src[comp];
+    float2* __restrict__ dst = p.dst[comp];
+    const int N = p.N, T = p.T, L = p.L, P = p.P, nl = p.nlines;
+    const int tid = threadIdx.x;
+    const int g = COLS ? (tid % L) : (tid / T);          // line of the tile
+    const int t = COLS ? (tid / L) : (tid - g * T);      // thread within the line
+    const int line = blockIdx.x * L + g;
+    const bool active = line < nl;
+    float2* s = sm + (size_t)g * P;
+    const long long gstr = COLS ? (long long)nl : 1;
+    const float2* gin = COLS ? (src + line) : (src + (size_t)line * N);
+    const int oline = d.mirror_lines ? (nl - 1 - line) : line;
+    float2* gout = COLS ? (dst + oline) : (dst + (size_t)oline * N);
+
+    Chain pre, mid, fin;
+    pre.rs1 = 0; pre.sh1 = 0; pre.a1 = 0.; pre.sc1 = 1.f; pre.pw = nullptr; pre.mir = 0;
+    pre.rs2 = d.f1_pre.rs; pre.sh2 = d.f1_pre.has_shift; pre.a2 = d.f1_pre.shift_a; pre.axis = d.axis;
+    mid.rs1 = 0; mid.sh1 = 0; mid.a1 = 0.; mid.sc1 = 1.f; mid.pw = d.has_pw ? &d.pw : nullptr;
+    mid.mir = d.mirror_along; mid.rs2 = 0; mid.sh2 = 0; mid.a2 = 0.; mid.axis = d.axis;
+    if (d.f1) { mid.rs1 = d.f1_post.rs; mid.sh1 = d.f1_post.has_shift; mid.a1 = d.f1_post.shift_a; mid.sc1 = d.f1_post.scale; }
+    if (d.f2) {
+        mid.rs2 = d.f2_pre.rs; mid.sh2 = d.f2_pre.has_shift; mid.a2 = d.f2_pre.shift_a;
+        fin.rs1 = d.f2_post.rs; fin.sh1 = d.f2_post.has_shift; fin.a1 = d.f2_post.shift_a; fin.sc1 = d.f2_post.scale;
+        fin.pw = nullptr; fin.mir = 0; fin.rs2 = 0; fin.sh2 = 0; fin.a2 = 0.; fin.axis = d.axis;
+    }
+    const int nst = p.nst;
+    if (d.f1 && d.f2) {
+        if (d.f1 > 0) fft16<1, 2, 0>(s, gin, nullptr, gstr, N, radix, nst, t, T, line, pre, mid, p.tw, active);
+        else fft16<-1, 2, 0>(s, gin, nullptr, gstr, N, radix, nst, t, T, line, pre, mid, p.tw, active);
+        if (d.f2 > 0) fft16<1, 1, 1>(s, nullptr, gout, gstr, N, radix, nst, t, T, line, mid, fin, p.tw, active);
+        else fft16<-1, 1, 1>(s, nullptr, gout, gstr, N, radix, nst, t, T, line, mid, fin, p.tw, active);
+    } else if (d.f1) {
+        if (d.f1 > 0) fft16<1, 2, 1>(s, gin, gout, gstr, N, radix, nst, t, T, line, pre, mid, p.tw, active);
+        else fft16<-1, 2, 1>(s, gin, gout, gstr, N, radix, nst, t, T, line, pre, mid, p.tw, active);
+    } else {
+        if (d.f2 > 0) fft16<1, 2, 1>(s, gin, gout, gstr, N, radix, nst, t, T, line, mid, fin, p.tw, active);
+        else fft16<-1, 2, 1>(s, gin, gout, gstr, N, radix, nst, t, T, line, mid, fin, p.tw, active);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
 // RESIZE pass (RadResizeCore, sroptelm.cpp:3038-3337; OnlyLargerRange :4231)
 // ------------------------------------------------------------------------------------------------
 __device__ __forceinline__ void lagrange4(float t, float* w)
@@ -615,9 +775,16 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
     if (smem > SRWG_LINE_SMEM_MAX) return cudaErrorInvalidValue;
     if (!attr_set) {
         cudaFuncSetAttribute(line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
+        cudaFuncSetAttribute(line2_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
+        cudaFuncSetAttribute(line2_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
         attr_set = 1;
     }
-    line_kernel<<<grid, p.T * p.G, smem, st>>>(p);
+    if (p.v2) {
+        if (p.d.axis == 0) line2_kernel<false><<<grid, p.T * p.L, smem, st>>>(p);
+        else line2_kernel<true><<<grid, p.T * p.L, smem, st>>>(p);
+    } else {
+        line_kernel<<<grid, p.T * p.G, smem, st>>>(p);
+    }
     return cudaGetLastError();
 }
 

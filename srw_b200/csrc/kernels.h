@@ -17,6 +17,7 @@ struct LineLaunch {
     int T, L, P, G;          // threads per line, lines per CTA, shared-memory pitch (float2), thread groups
     int nst;
     int radix[SRWG_MAX_STAGES];
+    int v2;                  // power-of-two line pass (line2_kernel)
 };
 
 struct ResizeLaunch {

@@ -9,10 +9,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 OUT_DIR = os.path.join(HERE, '_lib')
+OBJ_DIR = os.path.join(HERE, '_build')          # objects: kept out of the shipped tree
 LIB = os.path.join(OUT_DIR, 'libsrwl_b200.so')
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
-SOURCES = ['kernels.cu', 'planner.cpp', 'capi.cpp']
+SOURCES = ['kernels.cu'] + ['line2_%d.cu' % l for l in range(6, 15)] + ['planner.cpp', 'tables.cpp', 'capi.cpp']
 # host code: no FP contraction so the mesh bookkeeping rounds exactly like the reference
 HOST_FLAGS = '-O2,-fPIC,-ffp-contract=off,-fvisibility=hidden'
 
@@ -25,20 +26,29 @@ def _run(cmd):
     return r.stdout + r.stderr
 
 
+def _compile(s, ptxas_info):
+    src = os.path.join(CSRC, s)
+    obj = os.path.join(OBJ_DIR, s + '.o')
+    deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(('.h', '.cuh'))]
+    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps) and not ptxas_info:
+        return obj, ''
+    cmd = [NVCC, '-c', '-O3', '-std=c++17', '-lineinfo', '-Xcompiler', HOST_FLAGS, '--fmad=true'] + ARCH + \
+          ['-I', CSRC, '-o', obj, src]
+    if ptxas_info and s.endswith('.cu'):
+        cmd.insert(1, '-Xptxas=-v')
+    return obj, _run(cmd)
+
+
 def build(verbose=False, ptxas_info=False):
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
-    for s in SOURCES:
-        src = os.path.join(CSRC, s)
-        obj = os.path.join(OUT_DIR, s + '.o')
-        cmd = [NVCC, '-c', '-O3', '-std=c++17', '-lineinfo', '-Xcompiler', HOST_FLAGS, '--fmad=true'] + ARCH + \
-              ['-I', CSRC, '-o', obj, src]
-        if ptxas_info and s.endswith('.cu'):
-            cmd.insert(1, '-Xptxas=-v')
-        out = _run(cmd)
-        if verbose or ptxas_info:
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        res = list(ex.map(lambda s: _compile(s, ptxas_info), SOURCES))
+    objs = [o for o, _ in res]
+    if verbose or ptxas_info:
+        for _, out in res:
             sys.stdout.write(out)
-        objs.append(obj)
     # exported symbols: the C-ABI in include/srwl_b200.h
     _run([NVCC, '-shared', '-o', LIB] + ARCH + objs + ['-lcudart'])
     return LIB

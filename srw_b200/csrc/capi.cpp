@@ -29,6 +29,8 @@ struct DeviceCtx {
     size_t workElems = 0;               // per buffer per component
     float2* io = nullptr;               // input + output staging for the host-memory entry point
     size_t ioElems = 0;
+    float2* tab = nullptr;              // point-wise tables of the one-shot entry point
+    size_t tabElems = 0;
     cudaStream_t stream = nullptr;
 };
 static std::map<int, DeviceCtx*> g_ctx;
@@ -130,7 +132,9 @@ static int line_config(const LineDesc& d, LineLaunch& p)
             nb -= 4;
         }
         p.radix[p.nst++] = 1 << nb;          // 16, 8, 4 or 2
-        p.P = N + N / 16;
+        // one pad point per 16 (conflict-free Stockham exchanges) plus 4 per line, so that the
+        // lines of a tile start 8 banks apart
+        p.P = N + N / 16 + 4;
         int L = d.axis == 0 ? (256 / p.T) : (1024 / p.T);
         if (L < 1) L = 1;
         if (d.axis == 1 && L > 32) L = 32;
@@ -169,9 +173,39 @@ static int line_config(const LineDesc& d, LineLaunch& p)
     return 0;
 }
 
+// device copy of a plan's constant data: its point-wise tables, then (256-byte aligned) its pass
+// descriptors; returns the byte offset of the descriptors
+static size_t const_bytes(const Planner& pl, size_t* descOff)
+{
+    size_t tb = pl.tables.size() * sizeof(float2);
+    size_t off = (tb + 255) & ~(size_t)255;
+    *descOff = off;
+    return off + pl.kernels.size() * sizeof(KernelDesc);
+}
+
+static int upload_tables(const Planner& pl, float2** buf, size_t* capElems, cudaStream_t st)
+{
+    size_t descOff;
+    size_t bytes = const_bytes(pl, &descOff);
+    size_t n = (bytes + sizeof(float2) - 1) / sizeof(float2);
+    if (*capElems < n || *buf == nullptr) {
+        if (*buf) cudaFree(*buf);
+        *buf = nullptr;
+        *capElems = 0;
+        CUDA_TRY(cudaMalloc(buf, n * sizeof(float2)));
+        *capElems = n;
+    }
+    if (!pl.tables.empty())
+        CUDA_TRY(cudaMemcpyAsync(*buf, pl.tables.data(), pl.tables.size() * sizeof(float2), cudaMemcpyHostToDevice, st));
+    if (!pl.kernels.empty())
+        CUDA_TRY(cudaMemcpyAsync((char*)*buf + descOff, pl.kernels.data(), pl.kernels.size() * sizeof(KernelDesc),
+                                 cudaMemcpyHostToDevice, st));
+    return 0;
+}
+
 // runs the plan's passes: buffer 0 = input, 1/2 = work buffers; the last pass writes the output
 static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* inY, float2* outX, float2* outY,
-                   float2* work, size_t workElems, cudaStream_t st, cudaEvent_t* ev = nullptr)
+                   float2* work, size_t workElems, const float2* dtab, cudaStream_t st, cudaEvent_t* ev = nullptr)
 {
     const size_t nOut = (size_t)pl.w.nx * pl.w.nz;
     if (pl.kernels.empty()) {
@@ -183,6 +217,9 @@ static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* i
                         {work, work + workElems},
                         {work + 2 * workElems, work + 3 * workElems}};
     const size_t nk = pl.kernels.size();
+    size_t descOff;
+    const_bytes(pl, &descOff);
+    const KernelDesc* gk = (const KernelDesc*)((const char*)dtab + descOff);
     for (size_t i = 0; i < nk; i++) {
         const KernelDesc& k = pl.kernels[i];
         if (ev) CUDA_TRY(cudaEventRecord(ev[2 * i], st));
@@ -199,6 +236,8 @@ static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* i
             r = twiddles(c, p.N, &p.tw);
             if (r) return r;
             p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
+            p.tabs = dtab;
+            p.gd = &gk[i].line;
             e = launch_line(p, st);
         } else if (k.kind == K_RESIZE) {
             ResizeLaunch p;
@@ -207,12 +246,16 @@ static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* i
             p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
             p.xStepInvO = 1. / k.rs.xStepO;
             p.zStepInvO = 1. / k.rs.zStepO;
+            p.tabs = dtab;
+            p.gd = &gk[i].rs;
             e = launch_resize(p, st);
         } else {
             PwLaunch p;
             memset(&p, 0, sizeof(p));
             p.d = k.pwk;
             p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
+            p.tabs = dtab;
+            p.gd = &gk[i].pwk;
             e = launch_pw(p, st);
         }
         if (e != cudaSuccess) {
@@ -275,7 +318,24 @@ struct srwgPlan {
     Planner pl;
     int device = 0;
     DeviceCtx* ctx = nullptr;   // bound at the first execution
+    float2* dtab = nullptr;     // the plan's point-wise tables on that device
+    size_t dtabElems = 0;
+    bool tabReady = false;
+    ~srwgPlan() { if (dtab) cudaFree(dtab); }
 };
+
+static int plan_bind(srwgPlan* plan, cudaStream_t st)
+{
+    int r = get_ctx(plan->device, &plan->ctx);
+    if (r) return r;
+    if (!plan->tabReady) {
+        r = upload_tables(plan->pl, &plan->dtab, &plan->dtabElems, st);
+        if (r) return r;
+        CUDA_TRY(cudaStreamSynchronize(st));
+        plan->tabReady = true;
+    }
+    return ensure_work(*plan->ctx, (size_t)plan->pl.maxElems);
+}
 
 extern "C" {
 
@@ -346,7 +406,9 @@ int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SR
     else CUDA_TRY(cudaMemsetAsync(inX, 0, nIn * sizeof(float2), st));
     if (pWfr->arEy) CUDA_TRY(cudaMemcpyAsync(inY, pWfr->arEy, nIn * sizeof(float2), cudaMemcpyHostToDevice, st));
     else CUDA_TRY(cudaMemsetAsync(inY, 0, nIn * sizeof(float2), st));
-    r = execute(pl, *c, inX, inY, outX, outY, c->work, c->workElems, st);
+    r = upload_tables(pl, &c->tab, &c->tabElems, st);
+    if (r) return r;
+    r = execute(pl, *c, inX, inY, outX, outY, c->work, c->workElems, c->tab, st);
     if (r) return r;
     bool hadX = pWfr->arEx != nullptr, hadY = pWfr->arEy != nullptr;
     bool resized = (pl.w.nx != pl.in.nx) || (pl.w.nz != pl.in.nz);
@@ -419,15 +481,14 @@ int srwgPlanExecuteBatch(srwgPlan* plan, int n, const float* dExIn, const float*
     g_lastDetail.clear();
     if (plan == nullptr || dExIn == nullptr || dEyIn == nullptr || dExOut == nullptr || dEyOut == nullptr || n < 1)
         return SRWG_ERR_BAD_ARG;
-    int r = get_ctx(plan->device, &plan->ctx);
+    cudaStream_t st = (cudaStream_t)stream;
+    int r = plan_bind(plan, st);
     if (r) return r;
     DeviceCtx& c = *plan->ctx;
-    r = ensure_work(c, (size_t)plan->pl.maxElems);
-    if (r) return r;
-    cudaStream_t st = (cudaStream_t)stream;
     for (int b = 0; b < n; b++) {
         r = execute(plan->pl, c, (const float2*)(dExIn + b * strideIn), (const float2*)(dEyIn + b * strideIn),
-                    (float2*)(dExOut + b * strideOut), (float2*)(dEyOut + b * strideOut), c.work, c.workElems, st);
+                    (float2*)(dExOut + b * strideOut), (float2*)(dEyOut + b * strideOut), c.work, c.workElems,
+                    plan->dtab, st);
         if (r) return r;
     }
     return 0;
@@ -440,17 +501,15 @@ int srwgPlanExecuteTimed(srwgPlan* plan, const float* dExIn, const float* dEyIn,
     g_lastDetail.clear();
     if (plan == nullptr || dExIn == nullptr || dEyIn == nullptr || dExOut == nullptr || dEyOut == nullptr)
         return SRWG_ERR_BAD_ARG;
-    int r = get_ctx(plan->device, &plan->ctx);
+    cudaStream_t st = (cudaStream_t)stream;
+    int r = plan_bind(plan, st);
     if (r) return r;
     DeviceCtx& c = *plan->ctx;
-    r = ensure_work(c, (size_t)plan->pl.maxElems);
-    if (r) return r;
     const size_t nk = plan->pl.kernels.size();
     std::vector<cudaEvent_t> ev(2 * nk);
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
-    cudaStream_t st = (cudaStream_t)stream;
     r = execute(plan->pl, c, (const float2*)dExIn, (const float2*)dEyIn, (float2*)dExOut, (float2*)dEyOut, c.work,
-                c.workElems, st, nk ? ev.data() : nullptr);
+                c.workElems, plan->dtab, st, nk ? ev.data() : nullptr);
     if (r == 0) {
         CUDA_TRY(cudaStreamSynchronize(st));
         for (size_t i = 0; i < nk && (int)i < maxKernels; i++) {

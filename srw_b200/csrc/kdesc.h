@@ -41,6 +41,15 @@ struct PwOps {
     float sre, sim;                      // complex scale
     int nmask;
     PwMask mask[SRWG_MAX_MASKS];
+    int ang_resid;                       // 1: only the non-separable part c0 q^2 c1 q^2 (1 + 2 c1 q^2)
+};
+
+// Separable factor tables (complex FP32, computed in FP64 on the host) of one point-wise chain:
+// factor(k, line) = tab[k] * ltab[line] * (non-separable extras).  Offsets are in float2 units into
+// the plan's table buffer; -1 when absent.
+struct ChainTab {
+    long long tab;
+    long long ltab;
 };
 
 // Index-only side operations of one centred 1D DFT (Make2DFFT helpers, gmfft.h:232-480),
@@ -65,6 +74,9 @@ struct LineDesc {
     int mirror_lines;    // store line l at (nlines - 1 - l)
     int f2;              // second transform along the line
     FftSide f2_pre, f2_post;
+    ChainTab t_pre, t_mid, t_fin;   // tables of the pre / middle / final chains
+    int has_extra;                  // non-separable point-wise work of the middle chain
+    PwOps extra;
 };
 
 struct ResizeDesc {
@@ -75,12 +87,27 @@ struct ResizeDesc {
     int only_larger;                           // RadResizeCore_OnlyLargerRange
     int has_pw;
     PwOps pw;                                  // applied to the new points
+    ChainTab t;                                // separable part of pw: tab over x, ltab over z
+    int has_extra;
+    PwOps extra;
+    long long axx, axz;                        // per-axis gather tables (ResizeAxis), float2 offsets
+};
+
+// per new-mesh index along one axis: first old node of the 4-point stencil, clipped relative cell
+// index for the low-order fallback, relative coordinate (old steps) w.r.t. node st+1; for the
+// range-only resize `st` is the copied node.  Stored as two float2 (ints bit-cast).
+struct ResizeAxis {
+    int st, ir;
+    float rel, pad;
 };
 
 struct PwDesc {
     int nx, nz;
     PwOps pw;
     int mirror_x, mirror_z;                    // output index flips
+    ChainTab t;
+    int has_extra;
+    PwOps extra;
 };
 
 enum KernelKind { K_LINE = 1, K_RESIZE = 2, K_PW = 3 };

@@ -18,12 +18,16 @@ struct LineLaunch {
     int nst;
     int radix[SRWG_MAX_STAGES];
     int v2;                  // power-of-two line pass (line2_kernel)
+    const float2* tabs;      // the plan's separable point-wise tables
+    const LineDesc* gd;      // this pass's descriptor in device memory
 };
 
 struct ResizeLaunch {
     ResizeDesc d;
     const float2* src[2];
     float2* dst[2];
+    const float2* tabs;
+    const ResizeDesc* gd;
     double xStepInvO, zStepInvO;
 };
 
@@ -31,9 +35,18 @@ struct PwLaunch {
     PwDesc d;
     const float2* src[2];
     float2* dst[2];
+    const float2* tabs;
+    const PwDesc* gd;
 };
 
 cudaError_t launch_line(const LineLaunch& p, cudaStream_t st);
+
+// power-of-two line pass kernels, one translation unit per line length (line2_<logn>.cu)
+typedef void (*Line2Fn)(const LineLaunch);
+Line2Fn line2_kernel_ptr(int logn, bool cols);
+#define SRWG_LINE2_DECL(L) Line2Fn line2_get_##L(bool cols);
+SRWG_LINE2_DECL(6) SRWG_LINE2_DECL(7) SRWG_LINE2_DECL(8) SRWG_LINE2_DECL(9) SRWG_LINE2_DECL(10)
+SRWG_LINE2_DECL(11) SRWG_LINE2_DECL(12) SRWG_LINE2_DECL(13) SRWG_LINE2_DECL(14)
 cudaError_t launch_resize(const ResizeLaunch& p, cudaStream_t st);
 cudaError_t launch_pw(const PwLaunch& p, cudaStream_t st);
 

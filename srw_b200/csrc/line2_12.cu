@@ -1,0 +1,6 @@
+// Line pass instantiation for lines of 2^12 points (see line2.cuh).
+#include "line2.cuh"
+
+namespace srwg {
+Line2Fn line2_get_12(bool cols) { return cols ? line2_kernel<12, true> : line2_kernel<12, false>; }
+}  // namespace srwg

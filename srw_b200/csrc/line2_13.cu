@@ -1,0 +1,6 @@
+// Line pass instantiation for lines of 2^13 points (see line2.cuh).
+#include "line2.cuh"
+
+namespace srwg {
+Line2Fn line2_get_13(bool cols) { return cols ? line2_kernel<13, true> : line2_kernel<13, false>; }
+}  // namespace srwg

@@ -1,0 +1,6 @@
+// Line pass instantiation for lines of 2^14 points (see line2.cuh).
+#include "line2.cuh"
+
+namespace srwg {
+Line2Fn line2_get_14(bool cols) { return cols ? line2_kernel<14, true> : line2_kernel<14, false>; }
+}  // namespace srwg

@@ -1028,6 +1028,7 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
             return SRWG_ERR_UNSUPPORTED;
         }
     }
+    build_tables(kernels, tables);
     return 0;
 }
 

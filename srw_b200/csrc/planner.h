@@ -1,6 +1,8 @@
 // Host planner: the reference's per-element bookkeeping (meshes, radii, centres, moments) in FP64
 // with the reference's operation order, lowered into fused GPU passes (kdesc.h).
 #pragma once
+#include <vector_types.h>
+
 #include <string>
 #include <vector>
 #include "kdesc.h"
@@ -45,6 +47,9 @@ struct PropDesc {
 
 class Builder;
 
+// fills the separable point-wise tables of every pass (tables.cpp)
+void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& tables);
+
 class Planner {
 public:
     WfrState w;                          // evolves from the input to the output state
@@ -52,6 +57,7 @@ public:
     std::vector<KernelDesc> kernels;
     int outBuf = 0;                      // buffer holding the result (0: the input itself)
     long long maxElems = 0;              // largest grid over all work buffers
+    std::vector<float2> tables;          // separable point-wise tables of all passes (tables.cpp)
     std::string err;
 
     // flattens SRWLOptC (nested containers included) and plans; returns 0 or an SRW error number

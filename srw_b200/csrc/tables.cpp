@@ -1,0 +1,220 @@
+// Separable point-wise tables.  Every point-wise factor of this path -- quadratic and linear phases
+// (lens, drift passes, resize quadratic-term removal/restoration), the separable c0*q^2 part of
+// the angular transfer function, FFT centring signs and shift tables, scales and rectangular
+// apertures -- is a product of a function of the index along a line and a function of the line.
+// They are evaluated here once per plan in FP64 (phases reduced modulo 2*pi by the C library's
+// cos/sin) and stored as complex FP32 tables, so the passes apply them with table reads and
+// complex multiplies.  What is not separable (circular masks, rectangular obstacles, the quartic
+// remainder of the angular transfer function) stays in PwOps 'extra' for the device.
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <vector>
+
+#include "planner.h"
+
+namespace srwg {
+
+typedef std::complex<double> cd;
+
+struct SepPart {
+    std::vector<double> ph;   // phase per index
+    std::vector<char> zero;   // index masked out
+    bool any = false;         // anything non-trivial
+};
+
+// splits PwOps of a pass whose lines run along `axis` (0: along = x index, line = z index)
+static void separate(const PwOps& pw, int axis, int nAlong, int nLine, SepPart& A, SepPart& Lp, cd& scale,
+                     PwOps& extra, int& has_extra)
+{
+    A.ph.assign(nAlong, 0.); A.zero.assign(nAlong, 0); A.any = false;
+    Lp.ph.assign(nLine, 0.); Lp.zero.assign(nLine, 0); Lp.any = false;
+    scale = cd(1., 0.);
+    memset(&extra, 0, sizeof(extra));
+    has_extra = 0;
+    if (pw.has_quad) {
+        double Aa = axis == 0 ? pw.Ai : pw.Aj, Ba = axis == 0 ? pw.Bi : pw.Bj;
+        double Al = axis == 0 ? pw.Aj : pw.Ai, Bl = axis == 0 ? pw.Bj : pw.Bi;
+        for (int a = 0; a < nAlong; a++) A.ph[a] += (Aa * a + Ba) * a + pw.C;
+        for (int l = 0; l < nLine; l++) Lp.ph[l] += (Al * l + Bl) * l;
+        A.any = Lp.any = true;
+    }
+    if (pw.has_ang) {
+        double qa0 = axis == 0 ? pw.qx0 : pw.qz0, dqa = axis == 0 ? pw.dqx : pw.dqz;
+        double ql0 = axis == 0 ? pw.qz0 : pw.qx0, dql = axis == 0 ? pw.dqz : pw.dqx;
+        for (int a = 0; a < nAlong; a++) { double q = qa0 + a * dqa; A.ph[a] += pw.c0 * q * q; }
+        for (int l = 0; l < nLine; l++) { double q = ql0 + l * dql; Lp.ph[l] += pw.c0 * q * q; }
+        A.any = Lp.any = true;
+        extra.has_ang = 1;
+        extra.ang_resid = 1;
+        extra.qx0 = pw.qx0; extra.dqx = pw.dqx; extra.qz0 = pw.qz0; extra.dqz = pw.dqz;
+        extra.c0 = pw.c0; extra.c1 = pw.c1;
+        has_extra = 1;
+    }
+    if (pw.has_scale) { scale = cd(pw.sre, pw.sim); A.any = true; }
+    for (int m = 0; m < pw.nmask; m++) {
+        const PwMask& k = pw.mask[m];
+        if (k.type == 1 && !k.obstacle) {   // rectangular aperture: zero outside in x OR outside in z
+            for (int a = 0; a < nAlong; a++) {
+                double c0 = axis == 0 ? k.x0 : k.z0, dc = axis == 0 ? k.dx : k.dz, cc = axis == 0 ? k.cx : k.cz;
+                double h = axis == 0 ? k.hx : k.hz;
+                double r = (c0 + (double)a * dc) - cc;
+                if ((r < -h) || (r > h)) A.zero[a] = 1;
+            }
+            for (int l = 0; l < nLine; l++) {
+                double c0 = axis == 0 ? k.z0 : k.x0, dc = axis == 0 ? k.dz : k.dx, cc = axis == 0 ? k.cz : k.cx;
+                double h = axis == 0 ? k.hz : k.hx;
+                double r = (c0 + (double)l * dc) - cc;
+                if ((r < -h) || (r > h)) Lp.zero[l] = 1;
+            }
+            A.any = Lp.any = true;
+        } else {
+            extra.mask[extra.nmask++] = k;
+            has_extra = 1;
+        }
+    }
+}
+
+static cd cis(double ph) { return cd(::cos(ph), ::sin(ph)); }
+
+static long long push(std::vector<float2>& T, const std::vector<cd>& v)
+{
+    long long off = (long long)T.size();
+    for (const cd& c : v) { float2 f; f.x = (float)c.real(); f.y = (float)c.imag(); T.push_back(f); }
+    return off;
+}
+
+// table of one chain W[k] = tab[k] * ltab[line] * extra * V[src(k)]:
+// [post of a previous transform: rs1 / shift1 / scale1] -> [pw] -> [mirror] -> [pre of the next: rs2 / shift2]
+static ChainTab chain_table(std::vector<float2>& T, int N, int nLine, int rs1, int sh1, double a1, float sc1,
+                            const SepPart* A, const SepPart* Lp, cd scale, int mir, int rs2, int sh2, double a2)
+{
+    ChainTab ct;
+    ct.tab = -1;
+    ct.ltab = -1;
+    bool along = rs1 || sh1 || sc1 != 1.f || (A && A->any) || rs2 || sh2 || scale != cd(1., 0.);
+    if (along) {
+        std::vector<cd> v(N);
+        const int half = N >> 1;
+        for (int k = 0; k < N; k++) {
+            double sg = 1., ph = 0.;
+            int m = k;
+            if (rs2) { m = k + half; if (m >= N) m -= N; if (k & 1) sg = -sg; }
+            if (sh2) ph += a2 * (double)(m - half);
+            int i = mir ? (N - 1 - m) : m;
+            bool z = false;
+            if (A) { ph += A->ph[i]; z = A->zero[i] != 0; }
+            int s = i;
+            if (rs1) { s = i + half; if (s >= N) s -= N; if (s & 1) sg = -sg; }
+            if (sh1) ph += a1 * (double)(i - half);
+            v[k] = z ? cd(0., 0.) : (sg * (double)sc1) * scale * cis(ph);
+        }
+        ct.tab = push(T, v);
+    }
+    if (Lp && Lp->any) {
+        std::vector<cd> v(nLine);
+        for (int l = 0; l < nLine; l++) v[l] = Lp->zero[l] ? cd(0., 0.) : cis(Lp->ph[l]);
+        ct.ltab = push(T, v);
+    }
+    return ct;
+}
+
+// RadResizeCore (sroptelm.cpp:3038-3337) index arithmetic along one axis, in the reference's FP64
+// operation order (this file is compiled without FP contraction): for every new index in the
+// window, the 4-point stencil start, the clipped sub-cell and the relative coordinate.
+static long long resize_axis_table(std::vector<float2>& T, int nNew, long iS, long iE, double startN, double stepN,
+                                   double startO, double stepO, int nO, bool only_larger)
+{
+    if (T.size() & 1) {                      // entries are read as 16-byte float4: keep them aligned
+        float2 z; z.x = z.y = 0.f;
+        T.push_back(z);
+    }
+    long long off = (long long)T.size();
+    const double inv = 1. / stepO;
+    for (int i = 0; i < nNew; i++) {
+        ResizeAxis a;
+        a.st = 0; a.ir = 0; a.rel = 0.f; a.pad = 0.f;
+        if (i >= iS && i <= iE) {
+            double absc = startN + (double)i * stepN;
+            if (only_larger) {
+                long o = (long)((absc - startO) * inv + 1.E-08);
+                if (o < 0) o = 0;
+                if (o > nO - 1) o = nO - 1;
+                a.st = (int)o;
+            } else {
+                int ic = (int)((absc - startO) * inv + 1.E-06);
+                double rel = absc - (startO + (double)ic * stepO);
+                int st;
+                if (ic == nO - 1) { st = ic - 3; rel += 2. * stepO; }
+                else if (ic == nO - 2) { st = ic - 2; rel += stepO; }
+                else if (ic == 0) { st = ic; rel -= stepO; }
+                else st = ic - 1;
+                // a new point outside the old mesh would make the reference read outside it: clamp
+                if (st < 0) st = 0;
+                if (st > nO - 4) st = nO - 4;
+                int ir = ic - st;
+                ir = ir < 0 ? 0 : (ir > 2 ? 2 : ir);
+                a.st = st; a.ir = ir; a.rel = (float)(rel * inv);
+            }
+        }
+        float2 f0, f1;
+        memcpy(&f0, &a, sizeof(float2));
+        memcpy(&f1, ((const char*)&a) + sizeof(float2), sizeof(float2));
+        T.push_back(f0);
+        T.push_back(f1);
+    }
+    return off;
+}
+
+void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& T)
+{
+    T.clear();
+    for (KernelDesc& k : ks) {
+        if (k.kind == K_LINE) {
+            LineDesc& d = k.line;
+            int N = d.axis == 0 ? d.nx : d.nz, nl = d.axis == 0 ? d.nz : d.nx;
+            SepPart A, Lp;
+            cd scale(1., 0.);
+            d.has_extra = 0;
+            memset(&d.extra, 0, sizeof(d.extra));
+            if (d.has_pw) separate(d.pw, d.axis, N, nl, A, Lp, scale, d.extra, d.has_extra);
+            const SepPart* pA = d.has_pw ? &A : nullptr;
+            const SepPart* pL = d.has_pw ? &Lp : nullptr;
+            d.t_pre = chain_table(T, N, nl, 0, 0, 0., 1.f, nullptr, nullptr, cd(1., 0.), 0, d.f1_pre.rs,
+                                  d.f1_pre.has_shift, d.f1_pre.shift_a);
+            int rs1 = 0, sh1 = 0, rs2 = 0, sh2 = 0;
+            double a1 = 0., a2 = 0.;
+            float sc1 = 1.f;
+            if (d.f1) { rs1 = d.f1_post.rs; sh1 = d.f1_post.has_shift; a1 = d.f1_post.shift_a; sc1 = d.f1_post.scale; }
+            if (d.f2) { rs2 = d.f2_pre.rs; sh2 = d.f2_pre.has_shift; a2 = d.f2_pre.shift_a; }
+            d.t_mid = chain_table(T, N, nl, rs1, sh1, a1, sc1, pA, pL, scale, d.mirror_along, rs2, sh2, a2);
+            d.t_fin.tab = d.t_fin.ltab = -1;
+            if (d.f2)
+                d.t_fin = chain_table(T, N, nl, d.f2_post.rs, d.f2_post.has_shift, d.f2_post.shift_a, d.f2_post.scale,
+                                      nullptr, nullptr, cd(1., 0.), 0, 0, 0, 0.);
+        } else if (k.kind == K_RESIZE) {
+            ResizeDesc& r = k.rs;
+            r.t.tab = r.t.ltab = -1;
+            r.has_extra = 0;
+            memset(&r.extra, 0, sizeof(r.extra));
+            if (r.has_pw) {
+                SepPart A, Lp;
+                cd scale;
+                separate(r.pw, 0, r.nxn, r.nzn, A, Lp, scale, r.extra, r.has_extra);
+                r.t = chain_table(T, r.nxn, r.nzn, 0, 0, 0., 1.f, &A, &Lp, scale, 0, 0, 0, 0.);
+            }
+            r.axx = resize_axis_table(T, r.nxn, r.ixStart, r.ixEnd, r.xStartN, r.xStepN, r.xStartO, r.xStepO, r.nxo,
+                                      r.only_larger != 0);
+            r.axz = resize_axis_table(T, r.nzn, r.izStart, r.izEnd, r.zStartN, r.zStepN, r.zStartO, r.zStepO, r.nzo,
+                                      r.only_larger != 0);
+        } else {
+            PwDesc& p = k.pwk;
+            SepPart A, Lp;
+            cd scale;
+            separate(p.pw, 0, p.nx, p.nz, A, Lp, scale, p.extra, p.has_extra);
+            p.t = chain_table(T, p.nx, p.nz, 0, 0, 0., 1.f, &A, &Lp, scale, 0, 0, 0, 0.);
+        }
+    }
+}
+
+}  // namespace srwg

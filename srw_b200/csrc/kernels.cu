@@ -194,46 +194,161 @@ __device__ __forceinline__ float2 resize_point(const float2* __restrict__ o, int
     return F;
 }
 
+// interpolation of one point from its 4x4 stencil already in registers (see resize_point)
+__device__ __forceinline__ float2 interp_stencil(const float2 (&f)[4][4], const float* wx, const float* wz, float xr,
+                                                 float zr, int irx, int irz)
+{
+    bool low = false;
+#pragma unroll
+    for (int dz = 0; dz < 4; dz++)
+#pragma unroll
+        for (int dx = 0; dx < 4; dx++) low |= (f[dz][dx].x == 0.f) || (f[dz][dx].y == 0.f);
+    float2 F;
+    float FI;
+    if (!low) {
+        F = make_float2(0.f, 0.f);
+        FI = 0.f;
+#pragma unroll
+        for (int dz = 0; dz < 4; dz++) {
+            float2 rowF = make_float2(0.f, 0.f);
+            float rowI = 0.f;
+#pragma unroll
+            for (int dx = 0; dx < 4; dx++) {
+                float2 v = f[dz][dx];
+                rowF.x = fmaf(wx[dx], v.x, rowF.x);
+                rowF.y = fmaf(wx[dx], v.y, rowF.y);
+                rowI = fmaf(wx[dx], v.x * v.x + v.y * v.y, rowI);
+            }
+            F.x = fmaf(wz[dz], rowF.x, F.x);
+            F.y = fmaf(wz[dz], rowF.y, F.y);
+            FI = fmaf(wz[dz], rowI, FI);
+        }
+    } else {
+        float2 f00 = f[0][0], f10 = f[0][1], f01 = f[1][0], f11 = f[1][1];
+        // select the 2x2 sub-cell (irx, irz) without dynamic register indexing
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                if (a == irz && c == irx) { f00 = f[a][c]; f10 = f[a][c + 1]; f01 = f[a + 1][c]; f11 = f[a + 1][c + 1]; }
+        float xz = xr * zr;
+        F.x = f00.x + (f10.x - f00.x) * xr + (f01.x - f00.x) * zr + (f00.x - f01.x - f10.x + f11.x) * xz;
+        F.y = f00.y + (f10.y - f00.y) * xr + (f01.y - f00.y) * zr + (f00.y - f01.y - f10.y + f11.y) * xz;
+        float i00 = f00.x * f00.x + f00.y * f00.y, i10 = f10.x * f10.x + f10.y * f10.y;
+        float i01 = f01.x * f01.x + f01.y * f01.y, i11 = f11.x * f11.x + f11.y * f11.y;
+        FI = i00 + (i10 - i00) * xr + (i01 - i00) * zr + (i00 - i01 - i10 + i11) * xz;
+    }
+    FI = FI > 0.f ? FI : 0.f;
+    float app = F.x * F.x + F.y * F.y;          // ImproveReAndIm
+    if (app != 0.f) {
+        float fac = sqrtf(FI / app);
+        F.x *= fac; F.y *= fac;
+    }
+    return F;
+}
+
+__device__ __forceinline__ float2 pick3(const float2* c, int o, int dx)
+{   // c[o + dx] for o in {0, 1, 2} with compile-time register indices
+    return o == 0 ? c[dx] : (o == 1 ? c[dx + 1] : c[dx + 2]);
+}
+
+__device__ __forceinline__ float2 resize_factor(const ResizeDesc& d, const float2* tabs, int ix, int iz)
+{
+    float2 e = make_float2(1.f, 0.f);
+    if (d.t.tab >= 0) e = __ldg(&tabs[d.t.tab + ix]);
+    if (d.t.ltab >= 0) e = cmul(e, __ldg(&tabs[d.t.ltab + iz]));
+    bool zero = false;
+    if (d.has_extra) extra_eval(d.extra, ix, iz, e, zero);
+    return zero ? make_float2(0.f, 0.f) : e;
+}
+
 // RESIZE pass (RadResizeCore, sroptelm.cpp:3038-3337; OnlyLargerRange :4231).  The index
 // arithmetic is tabulated per axis by the host (exact reference formulas); this kernel gathers,
 // interpolates, applies the new-mesh point-wise factors and writes every new point (zero outside
-// the window).
+// the window).  A thread produces two horizontally adjacent points: when their stencils start at
+// most one old node apart, each stencil row is read once as three aligned float4 (6 complex).
 __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
 {
     const ResizeDesc& d = *p.gd;       // device-memory descriptor (read-only, cached)
-    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ix0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ix >= d.nxn || iz >= d.nzn) return;
-    float2 out[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    const bool inwin = (ix >= d.ixStart) && (ix <= d.ixEnd) && (iz >= d.izStart) && (iz <= d.izEnd);
-    if (inwin) {
-        const ResizeAxis ax = load_axis(p.tabs, d.axx, ix);
+    if (ix0 >= d.nxn || iz >= d.nzn) return;
+    const bool two = ix0 + 1 < d.nxn;
+    float2 out[2][2] = {{make_float2(0.f, 0.f), make_float2(0.f, 0.f)}, {make_float2(0.f, 0.f), make_float2(0.f, 0.f)}};
+    const bool zin = (iz >= d.izStart) && (iz <= d.izEnd);
+    const bool in0 = zin && (ix0 >= d.ixStart) && (ix0 <= d.ixEnd);
+    const bool in1 = two && zin && (ix0 + 1 >= d.ixStart) && (ix0 + 1 <= d.ixEnd);
+    if (in0 || in1) {
         const ResizeAxis az = load_axis(p.tabs, d.axz, iz);
+        const ResizeAxis a0 = load_axis(p.tabs, d.axx, ix0);
+        const ResizeAxis a1 = two ? load_axis(p.tabs, d.axx, ix0 + 1) : a0;
         if (d.only_larger) {
 #pragma unroll
-            for (int c = 0; c < 2; c++) out[c] = __ldg(&p.src[c][(size_t)az.st * d.nxo + ax.st]);
+            for (int c = 0; c < 2; c++) {
+                if (in0) out[0][c] = __ldg(&p.src[c][(size_t)az.st * d.nxo + a0.st]);
+                if (in1) out[1][c] = __ldg(&p.src[c][(size_t)az.st * d.nxo + a1.st]);
+            }
         } else {
-            float wx[4], wz[4];
-            lagrange4(ax.rel, wx);
+            float wz[4], wx0[4], wx1[4];
             lagrange4(az.rel, wz);
+            lagrange4(a0.rel, wx0);
+            lagrange4(a1.rel, wx1);
+            const int base = a0.st & ~1;
+            const int o0 = a0.st - base, o1 = a1.st - base;
+            const bool vec = p.vec_ok && in0 && in1 && (o1 >= o0) && (o1 <= 2) && (base + 6 <= d.nxo);
+            if (vec) {
 #pragma unroll
-            for (int c = 0; c < 2; c++)
-                out[c] = resize_point(p.src[c] + (size_t)az.st * d.nxo + ax.st, d.nxo, wx, wz, ax.rel, az.rel, ax.ir, az.ir);
+                for (int c = 0; c < 2; c++) {
+                    const float2* __restrict__ o = p.src[c] + (size_t)az.st * d.nxo + base;
+                    float2 f0[4][4], f1[4][4];
+#pragma unroll
+                    for (int dz = 0; dz < 4; dz++) {
+                        const float4* r4 = reinterpret_cast<const float4*>(o + (size_t)dz * d.nxo);
+                        float4 q0 = __ldg(r4), q1 = __ldg(r4 + 1), q2 = __ldg(r4 + 2);
+                        float2 cc[6] = {make_float2(q0.x, q0.y), make_float2(q0.z, q0.w), make_float2(q1.x, q1.y),
+                                        make_float2(q1.z, q1.w), make_float2(q2.x, q2.y), make_float2(q2.z, q2.w)};
+#pragma unroll
+                        for (int dx = 0; dx < 4; dx++) {
+                            f0[dz][dx] = pick3(cc, o0, dx);
+                            f1[dz][dx] = pick3(cc, o1, dx);
+                        }
+                    }
+                    out[0][c] = interp_stencil(f0, wx0, wz, a0.rel, az.rel, a0.ir, az.ir);
+                    out[1][c] = interp_stencil(f1, wx1, wz, a1.rel, az.rel, a1.ir, az.ir);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 2; c++) {
+                    if (in0) out[0][c] = resize_point(p.src[c] + (size_t)az.st * d.nxo + a0.st, d.nxo, wx0, wz, a0.rel,
+                                                      az.rel, a0.ir, az.ir);
+                    if (in1) out[1][c] = resize_point(p.src[c] + (size_t)az.st * d.nxo + a1.st, d.nxo, wx1, wz, a1.rel,
+                                                      az.rel, a1.ir, az.ir);
+                }
+            }
         }
         if (d.has_pw) {
-            float2 e = make_float2(1.f, 0.f);
-            if (d.t.tab >= 0) e = __ldg(&p.tabs[d.t.tab + ix]);
-            if (d.t.ltab >= 0) e = cmul(e, __ldg(&p.tabs[d.t.ltab + iz]));
-            bool zero = false;
-            if (d.has_extra) extra_eval(d.extra, ix, iz, e, zero);
-            if (zero) e = make_float2(0.f, 0.f);
-            out[0] = cmul(out[0], e);
-            out[1] = cmul(out[1], e);
+            if (in0) {
+                float2 e = resize_factor(d, p.tabs, ix0, iz);
+                out[0][0] = cmul(out[0][0], e);
+                out[0][1] = cmul(out[0][1], e);
+            }
+            if (in1) {
+                float2 e = resize_factor(d, p.tabs, ix0 + 1, iz);
+                out[1][0] = cmul(out[1][0], e);
+                out[1][1] = cmul(out[1][1], e);
+            }
         }
     }
-    const size_t o = (size_t)iz * d.nxn + ix;
-    __stcs(&p.dst[0][o], out[0]);
-    __stcs(&p.dst[1][o], out[1]);
+    const size_t o = (size_t)iz * d.nxn + ix0;
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        if (p.vec_ok && two && ((o & 1) == 0)) {
+            __stcs(reinterpret_cast<float4*>(p.dst[c] + o), make_float4(out[0][c].x, out[0][c].y, out[1][c].x, out[1][c].y));
+        } else {
+            __stcs(&p.dst[c][o], out[0][c]);
+            if (two) __stcs(&p.dst[c][o + 1], out[1][c]);
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -303,10 +418,15 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t launch_resize(const ResizeLaunch& p, cudaStream_t st)
+cudaError_t launch_resize(const ResizeLaunch& q, cudaStream_t st)
 {
-    dim3 blk(128, 2);
-    dim3 grid((p.d.nxn + blk.x - 1) / blk.x, (p.d.nzn + blk.y - 1) / blk.y);
+    ResizeLaunch p = q;
+    p.vec_ok = ((q.d.nxo & 1) == 0) && ((q.d.nxn & 1) == 0);
+    for (int c = 0; c < 2; c++)
+        p.vec_ok = p.vec_ok && ((((uintptr_t)q.src[c]) & 15) == 0) && ((((uintptr_t)q.dst[c]) & 15) == 0);
+    dim3 blk(64, 4);
+    const int nxh = (p.d.nxn + 1) / 2;
+    dim3 grid((nxh + blk.x - 1) / blk.x, (p.d.nzn + blk.y - 1) / blk.y);
     resize_kernel<<<grid, blk, 0, st>>>(p);
     return cudaGetLastError();
 }

@@ -28,6 +28,7 @@ struct ResizeLaunch {
     float2* dst[2];
     const float2* tabs;
     const ResizeDesc* gd;
+    int vec_ok;              // even row lengths and 16-byte aligned buffers: float4 paths allowed
     double xStepInvO, zStepInvO;
 };
 

@@ -53,6 +53,18 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
         for (int b = 0; b < B; b++) {
             const int j = t + T * b;
             const int k = j & (NS - 1);
+            // twiddles W^(k r): W^k, W^2k, W^4k, W^8k from the table, the other powers as products
+            float2 wp[4];
+            if (NS > 1) {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    if ((1 << e) < R) {
+                        float2 w = __ldg(&tw[(k * TWS) << e]);
+                        if (DIR < 0) w.y = -w.y;
+                        wp[e] = w;
+                    }
+                }
+            }
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int p = j + r * NR;
@@ -65,11 +77,14 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
                         float2 f = chain2_eval(cin, p, N, line, sp);
                         x = cmul(f, s[PADI(sp)]);
                     }
-                    if (NS > 1 && r > 0) {
-                        float2 w = __ldg(&tw[k * TWS * r]);
-                        if (DIR < 0) w.y = -w.y;
-                        x = cmul(x, w);
-                    }
+                }
+                if (NS > 1 && r > 0) {
+                    float2 w = make_float2(1.f, 0.f);
+                    bool first = true;
+#pragma unroll
+                    for (int e = 0; e < 4; e++)
+                        if (r & (1 << e)) { w = first ? wp[e] : cmul(w, wp[e]); first = false; }
+                    x = cmul(x, w);
                 }
                 v[b][r] = x;
             }

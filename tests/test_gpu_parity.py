@@ -135,3 +135,20 @@ def test_drift_round_trip_and_energy():
     w1 = run_gpu(ex, ey, mesh, [('drift', 7., 0)], [[0, 0, 1., 0, 0, 1., 1., 1., 1.]])
     g1, _ = fields(w1)
     assert abs(np.sum(np.abs(g1) ** 2) / np.sum(np.abs(ex) ** 2) - 1.) < 1e-5
+
+
+def test_odd_input_mesh_resize_then_drift_vs_oracle():
+    """Odd input mesh (101 x 75): resize to good numbers then angular drift; exercises the scalar
+    (non-vectorised) resize path and the general-radix line passes."""
+    need_gpu()
+    ex, ey, mesh = gaussian(101, E=1500., sig=80e-6, r=1e-3, ny=75, ry=0.8e-3)
+    ey = 0.1 * ex
+    el = [('aperture', 'c', 'a', 1.2e-3, 1.2e-3, 0.05e-3, 0.), ('drift', 2., 0)]
+    pp = [[0, 0, 1., 0, 0, 1.3, 1.7, 1.2, 1.1, 0, 0, 0], [0, 0, 1., 0, 0, 1., 1., 1., 1., 0, 0, 0]]
+    w = run_gpu(ex, ey, mesh, el, pp)
+    o = oracle_run(ex, ey, mesh, el, pp)
+    m = o.out_mesh()
+    assert np.array_equal(mesh_tuple(w), np.array([m['nx'], m['ny'], m['xStart'], m['xFin'], m['yStart'], m['yFin']]))
+    gx, gy = fields(w)
+    assert rel_l2(gx, o.ex) < TOL
+    assert rel_l2(gy, o.ey) < TOL

@@ -161,6 +161,22 @@ SRWG_API int srwgPlanExecuteTimed(srwgPlan* plan, const float* dExIn, const floa
 
 SRWG_API int srwgPlanDestroy(srwgPlan* plan);
 
+/* Allocation-free propagation (no counterpart in the reference).  For callers that cannot call
+ * cudaMalloc at run time -- programs that reserve all device memory at start-up and hand out
+ * slices themselves, or whose device memory must go through their own caching allocator --
+ * this runs the propagation of srwgPlanCreate + srwgPlanExecute without allocating any device
+ * memory: the caller passes the input fields (dExIn/dEyIn, read only) and the output fields
+ * (dExOut/dEyOut, outCapacity complex points each, device memory), and all intermediate data
+ * lives in one fixed device array inside the library (9 MiB, held by every GPU that loads the
+ * library until the process exits).  Limit: intermediate grids of at most 512 x 512 points and
+ * 1 MiB of plan tables; larger propagations return error 23904 (text: srwlUtiGetErrText).
+ * Runs on the current device and `stream`; pWfrOut (optional) receives the output mesh and
+ * scalars.  The first call on a device looks the array up (cudaGetSymbolAddress) with that
+ * device current.  Calls share the array: calls that overlap on the GPU race. */
+SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRWLOptC* pOpt, const float* dExIn,
+                                       const float* dEyIn, float* dExOut, float* dEyOut, long long outCapacity,
+                                       void* stream, SRWLWfr* pWfrOut);
+
 /* Human-readable list of the planned passes (one line per kernel) into buf. */
 SRWG_API int srwgPlanDescribe(const srwgPlan* plan, char* buf, int bufLen);
 

@@ -75,6 +75,8 @@ SYMBOLS = {
     'srwgPlanExecuteTimed': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     'srwgPlanDestroy': (C.c_int, [C.c_void_p]),
+    'srwgPropagElecFieldStatic': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(SRWLWfr)]),
     'srwgPlanDescribe': (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
 }
 

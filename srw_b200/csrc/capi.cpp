@@ -14,11 +14,13 @@
 #include "../../include/srwl_b200.h"
 #include "errors.h"
 #include "kernels.h"
+#include "exec.h"
 #include "planner.h"
 
 namespace srwg {
 
 static std::string g_lastDetail;                          // detail text of the last error
+void set_last_detail(const std::string& s) { g_lastDetail = s; }
 static int (*g_modifFunc)(int, SRWLWfr*, char) = nullptr;  // client re-allocation callback
 static std::mutex g_mutex;
 
@@ -112,7 +114,7 @@ int radix_plan(int N, int* r)
     return ns;
 }
 
-static int line_config(const LineDesc& d, LineLaunch& p)
+int line_config(const LineDesc& d, LineLaunch& p)
 {
     p.d = d;
     int N = d.axis == 0 ? d.nx : d.nz;
@@ -362,10 +364,11 @@ int srwlUtiGetErrText(char* t, int erNo)
     case SRWG_ERR_CUDA: s = "CUDA error"; break;
     case SRWG_ERR_NO_DEVICE: s = "No usable CUDA device"; break;
     case SRWG_ERR_BAD_ARG: s = "Invalid argument"; break;
+    case SRWG_ERR_STATIC_LIMIT: s = "Propagation too large for the allocation-free entry point"; break;
     default: s = "Unknown error or warning number."; break;
     }
     std::string txt(s);
-    if ((erNo >= SRWG_ERR_UNSUPPORTED && erNo <= SRWG_ERR_BAD_ARG) && !g_lastDetail.empty()) txt += ": " + g_lastDetail;
+    if ((erNo >= SRWG_ERR_UNSUPPORTED && erNo <= SRWG_ERR_STATIC_LIMIT) && !g_lastDetail.empty()) txt += ": " + g_lastDetail;
     strncpy(t, txt.c_str(), 2047);
     t[2047] = 0;
     return 0;

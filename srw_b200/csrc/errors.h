@@ -15,3 +15,4 @@
 #define SRWG_ERR_CUDA (901 + SRWG_FIRST_ERR)            // CUDA runtime error (text has details)
 #define SRWG_ERR_NO_DEVICE (902 + SRWG_FIRST_ERR)       // no usable CUDA device
 #define SRWG_ERR_BAD_ARG (903 + SRWG_FIRST_ERR)         // invalid argument to an extension entry point
+#define SRWG_ERR_STATIC_LIMIT (904 + SRWG_FIRST_ERR)    // above the static scratch of srwgPropagElecFieldStatic

@@ -34,6 +34,12 @@ WORKLOAD = ("undulator beamline: 1024x1024 complex FP32 field (2012 eV, +-1.5 mm
             "0.8 mm -> resize x2 range x2 resolution (4096x4096) -> thin lens f=10 m -> drift 10 m to waist; "
             "plain single-wavefront path")
 PEAKS = os.path.join(HERE, 'MEASURED_PEAKS.json')
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a pass, from an ncu
+# capture of this workload (profiles/line_4096_c1.md, profiles/resize_1024_to_4096_c1.md); keyed by
+# the pass tuple of Plan.kernels().  Re-captured whenever the kernel changes.
+TRAFFIC = {('line_cols', 4096, 4096): 268648960 + 235960832,
+           ('line_rows', 4096, 4096): 268642816 + 232941568,
+           ('resize', 1024, 1024, 4096, 4096): 17597184 + 210405120}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -83,6 +89,59 @@ def make_wfr(mod, ex, ey, mesh, sc, alloc=None):
 # ------------------------------------------------------------------------------------------------
 # clocks sampled during the timed region
 # ------------------------------------------------------------------------------------------------
+class NvmlSampler(object):
+    """Polls SM clock, max clock and clock-event reasons through NVML every `period` seconds
+    (read-only queries) while the timed region runs."""
+    REASONS = {0x8: 'hw_slowdown', 0x40: 'hw_thermal_slowdown', 0x20: 'sw_thermal_slowdown',
+               0x4: 'sw_power_cap', 0x80: 'hw_power_brake_slowdown'}
+
+    def __init__(self, torch_dev, period=0.01):
+        self.dev, self.period, self.rows, self.h = torch_dev, period, [], None
+        self.stop = threading.Event()
+
+    def __enter__(self):
+        try:
+            import pynvml as N
+            import torch
+            N.nvmlInit()
+            self.N = N
+            p = torch.cuda.get_device_properties(self.dev)
+            try:
+                bus = '%08X:%02X:%02X.0' % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+                self.h = N.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.h = N.nvmlDeviceGetHandleByIndex(self.dev.index)
+            self.mx = float(N.nvmlDeviceGetMaxClockInfo(self.h, N.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+        except Exception:
+            self.h = None
+        return self
+
+    def _poll(self):
+        N = self.N
+        while not self.stop.is_set():
+            try:
+                sm = float(N.nvmlDeviceGetClockInfo(self.h, N.NVML_CLOCK_SM))
+                rs = int(N.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.rows.append((sm, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __exit__(self, *a):
+        self.stop.set()
+        if self.h is not None:
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return None
+        reasons = sorted({n for _, r in self.rows for b, n in self.REASONS.items() if r & b})
+        return {"sm_mhz": statistics.median([r[0] for r in self.rows]), "sm_max_mhz": self.mx, "reasons": reasons,
+                "samples": len(self.rows), "source": "nvml, 10 ms period"}
+
+
 class ClockSampler(object):
     Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
          'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
@@ -232,7 +291,7 @@ def run_ours(args, rank, world):
         dist.barrier()
 
     step_ms, kern_ms = [], []
-    with ClockSampler(dev.index) as clk:
+    with ClockSampler(dev.index) as clk, NvmlSampler(dev) as nv:
         for _ in range(args.steps):
             flush.fill_(1)                                  # L2 flush between steps (outside the events)
             e0 = torch.cuda.Event(enable_timing=True)
@@ -259,7 +318,12 @@ def run_ours(args, rank, world):
     peak, peak_src = 6650., 'fallback'
     if os.path.exists(PEAKS):
         peak, peak_src = float(json.load(open(PEAKS))['hbm_gbs']), 'measured'
-    total_alg = sum(kernel_bytes(k) for k in kinfo)
+    pass_bytes = sum(kernel_bytes(k) for k in kinfo)
+    # algorithmic bytes of one propagation (model: resize reads the old and writes the new mesh,
+    # one 2D FFT = one read + one write pass per axis at the new mesh, point-wise work fused; both
+    # components): [8 N_in + 8 N_out + 2 * 16 N_out] * 2 = 1,358,954,496 B for 1024^2 -> 4096^2
+    n_in, n_out = 1024 * 1024, plan.nx_out * plan.ny_out
+    total_alg = (8 * n_in + 8 * n_out + 2 * 16 * n_out) * 2
 
     # e2e through the C-ABI (host buffers in pinned memory; H2D + D2H inside the timed region)
     pinned = []
@@ -312,17 +376,19 @@ def run_ours(args, rank, world):
     if not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(n_props=2, procs=1)
     if cpu is None:
-        cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "reference build not present"}
+        why = "not measured (--no-cpu-baseline)" if args.no_cpu_baseline else "reference build not present"
+        cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
            "config": {"workload": WORKLOAD, "grid_in": [1024, 1024], "grid_out": [plan.nx_out, plan.ny_out],
                       "passes": plan.n_kernels, "algorithmic_bytes_per_step": total_alg,
+                      "pass_bytes_per_step": pass_bytes,
                       "l2": "256 MB buffer written between steps (outside the per-step CUDA events); working set "
                             "768 MB > L2", "parallelism": "replicas" if world > 1 else "single GPU"},
            "roofline": {"bound": "hbm", "kernel": "%s %s" % (kinfo[kd][0], 'x'.join(map(str, kinfo[kd][1:]))),
                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "peak_source": peak_src, "traffic": None,
+                        "peak_source": peak_src, "traffic": TRAFFIC.get(kinfo[kd]),
                         "algorithmic_bytes": alg, "avg_ms": float(per_k[kd]),
                         "step_frac": (total_alg / (total_ms / args.steps / 1000.) / 1e9) / peak,
                         "per_pass_ms": [round(float(v), 4) for v in per_k]},
@@ -330,7 +396,7 @@ def run_ours(args, rank, world):
            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * 1024 * 1024,
                    "d2h_bytes_per_step": 2 * 8 * plan.nx_out * plan.ny_out,
                    "path": "srw_b200.srwlpy.PropagElecField (C-ABI srwlPropagElecField), pinned host buffers"},
-           "clocks": clk.summary(),
+           "clocks": nv.summary() or clk.summary(),
            "gpu_launches": plan.n_kernels * args.steps}
     print(json.dumps(out))
 
@@ -338,7 +404,7 @@ def run_ours(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--steps', type=int, default=200)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')

@@ -11,8 +11,9 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// complex add / subtract as one packed FP32x2 instruction each (sm_100); b * (-1) + a is exactly a - b
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 // multiply by -i (forward, DIR=+1) or +i (inverse, DIR=-1)
 template <int DIR> __device__ __forceinline__ float2 mul_mi(float2 a)
@@ -353,50 +354,44 @@ __device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2&
     }
 }
 
-// chain with its factors in tables: W[k] = tab[k] * lf * extra(i, line) * V[src(k)]
+// chain with its along-line factors in a table: W[k] = tab[k] * extra(k ^ xi, line) * V[k ^ xs].  For
+// power-of-two lines the centring rotation and the mirror are XOR masks: (k + N/2) mod N = k ^ N/2,
+// N - 1 - k = k ^ (N - 1).  The chain's per-line factor is not part of it: the line factors of all
+// chains of a pass are multiplied once per line and applied at the store (a per-line constant
+// commutes with the FFT along the line).
 struct Chain2 {
-    int rs1, mir, rs2;
-    const float2* tab;
-    float2 lf;
-    const PwOps* extra;
-    int axis;
+    int xs;                  // source index mask: rotation (rs2), mirror, rotation (rs1)
+    int xi;                  // evaluation index mask of the non-separable work (rs2, mirror)
+    int xinv;                // output chains: destination of transform output q is q ^ xinv
+    int tab;                 // offset of the along-line factors in the plan's tables, or -1
+    int extra;               // the pass's non-separable work applies to this chain
 };
 
-__device__ __forceinline__ float2 chain2_eval(const Chain2& c, int k, int N, int line, int& src)
+// v <- factor(k) v; `tabs` are the plan's tables, `ex` the pass's non-separable work
+template <bool EXTRA>
+__device__ __forceinline__ float2 chain2_apply(const Chain2& c, int k, int line, float2 v, const float2* tabs,
+                                               const PwOps* ex, int axis)
 {
-    const int half = N >> 1;
-    int m = k;
-    if (c.rs2) { m = k + half; if (m >= N) m -= N; }
-    int i = c.mir ? (N - 1 - m) : m;
-    int s = i;
-    if (c.rs1) { s = i + half; if (s >= N) s -= N; }
-    src = s;
-    float2 f = c.tab ? __ldg(&c.tab[k]) : make_float2(1.f, 0.f);
-    f = cmul(f, c.lf);
-    if (c.extra) {
+    if (c.tab >= 0) v = cmul(__ldg(&tabs[c.tab + k]), v);
+    if (EXTRA && c.extra) {
+        const int i = k ^ c.xi;
         bool zero = false;
-        extra_eval(*c.extra, c.axis == 0 ? i : line, c.axis == 0 ? line : i, f, zero);
-        if (zero) f = make_float2(0.f, 0.f);
+        float2 f = make_float2(1.f, 0.f);
+        extra_eval(*ex, axis == 0 ? i : line, axis == 0 ? line : i, f, zero);
+        v = zero ? make_float2(0.f, 0.f) : cmul(f, v);
     }
-    return f;
+    return v;
 }
 
-__device__ __forceinline__ int chain2_inv(const Chain2& c, int q, int N)
-{
-    int i = q;
-    if (c.rs1) { i = q + (N >> 1); if (i >= N) i -= N; }
-    return c.mir ? (N - 1 - i) : i;
-}
-
-__device__ __forceinline__ Chain2 make_chain2(const ChainTab& t, const float2* tabs, int rs1, int mir, int rs2,
-                                              const PwOps* extra, int axis, int line, bool active)
+__device__ __forceinline__ Chain2 make_chain2(const ChainTab& t, int rs1, int mir, int rs2, int extra, int N)
 {
     Chain2 c;
-    c.rs1 = rs1; c.mir = mir; c.rs2 = rs2;
-    c.tab = t.tab >= 0 ? tabs + t.tab : nullptr;
-    c.lf = (t.ltab >= 0 && active) ? __ldg(&tabs[t.ltab + line]) : make_float2(1.f, 0.f);
+    const int h = N >> 1;
+    c.xi = (rs2 ? h : 0) ^ (mir ? N - 1 : 0);
+    c.xs = c.xi ^ (rs1 ? h : 0);
+    c.xinv = (rs1 ? h : 0) ^ (mir ? N - 1 : 0);
+    c.tab = t.tab >= 0 ? (int)t.tab : -1;
     c.extra = extra;
-    c.axis = axis;
     return c;
 }
 

@@ -376,18 +376,18 @@ __global__ void __launch_bounds__(256) pw_kernel(const PwLaunch p)
 // ------------------------------------------------------------------------------------------------
 // launchers
 // ------------------------------------------------------------------------------------------------
-Line2Fn line2_kernel_ptr(int logn, bool cols)
+Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra)
 {
     switch (logn) {
-    case 6: return line2_get_6(cols);
-    case 7: return line2_get_7(cols);
-    case 8: return line2_get_8(cols);
-    case 9: return line2_get_9(cols);
-    case 10: return line2_get_10(cols);
-    case 11: return line2_get_11(cols);
-    case 12: return line2_get_12(cols);
-    case 13: return line2_get_13(cols);
-    case 14: return line2_get_14(cols);
+    case 6: return extra ? line2e_get_6(cols) : line2_get_6(cols);
+    case 7: return extra ? line2e_get_7(cols) : line2_get_7(cols);
+    case 8: return extra ? line2e_get_8(cols) : line2_get_8(cols);
+    case 9: return extra ? line2e_get_9(cols) : line2_get_9(cols);
+    case 10: return extra ? line2e_get_10(cols) : line2_get_10(cols);
+    case 11: return extra ? line2e_get_11(cols) : line2_get_11(cols);
+    case 12: return extra ? line2e_get_12(cols) : line2_get_12(cols);
+    case 13: return extra ? line2e_get_13(cols) : line2_get_13(cols);
+    case 14: return extra ? line2e_get_14(cols) : line2_get_14(cols);
     default: return nullptr;
     }
 }
@@ -400,16 +400,16 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
     static int attr_set = 0;
     if (!attr_set) {
         cudaFuncSetAttribute(line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
-        for (int lg = 6; lg <= 14; lg++) {
-            cudaFuncSetAttribute(line2_kernel_ptr(lg, false), cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
-            cudaFuncSetAttribute(line2_kernel_ptr(lg, true), cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
-        }
+        for (int lg = 6; lg <= 14; lg++)
+            for (int e = 0; e < 4; e++)
+                cudaFuncSetAttribute(line2_kernel_ptr(lg, e & 1, e >> 1), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     SRWG_LINE_SMEM_MAX);
         attr_set = 1;
     }
     if (p.v2) {
         int lg = 0;
         while ((1 << lg) < p.N) lg++;
-        Line2Fn f = line2_kernel_ptr(lg, p.d.axis != 0);
+        Line2Fn f = line2_kernel_ptr(lg, p.d.axis != 0, p.d.has_extra != 0);
         if (f == nullptr) return cudaErrorInvalidValue;
         f<<<grid, p.T * p.L, smem, st>>>(p);
     } else {

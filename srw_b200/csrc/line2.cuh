@@ -9,17 +9,18 @@ namespace srwg {
 // FFT stage reads its butterfly inputs straight from global memory through the point-wise chain
 // (coalesced: thread t reads t + T*m), the last stage writes straight to global memory through
 // the output chain; intermediate stages exchange through shared memory padded by one point per
-// 16 (conflict-free Stockham writes).  A second transform in the same pass (f1 -> f2) reads the
+// 16 (conflict-free Stockham writes).  Complex adds and subtracts are packed FP32x2 instructions.  A second transform in the same pass (f1 -> f2) reads the
 // first one's output from shared memory through the middle chain.
 // ------------------------------------------------------------------------------------------------
 #define PADI(p) ((p) + ((p) >> 4))
 
 // IN: 0 shared, 1 shared through chain cin, 2 global through chain cin;  OUT: 0 shared, 1 global through chain cout
 // N (line length), R (radix) and Ns (product of the radices already applied) are compile-time.
-template <int N, int R, int NS, int DIR, int IN, int OUT>
+template <int N, int R, int NS, int DIR, int IN, int OUT, bool EXTRA>
 __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
-                                        long long gstr, int t, int line, const Chain2& cin, const Chain2& cout,
-                                        const float2* __restrict__ tw, bool active)
+                                        int gstr, int t, int line, const Chain2& cin, const Chain2& cout,
+                                        const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
+                                        const float2* __restrict__ tabs, const PwOps* ex, int axis)
 {
     constexpr int T = N / 16;
     constexpr int B = 16 / R;
@@ -33,20 +34,12 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int p = t + T * b + r * NR;
-                int q = p;
-                if (cin.rs2) { q = p + (N >> 1); if (q >= N) q -= N; }
-                if (cin.mir) q = N - 1 - q;
-                if (cin.rs1) { q += (N >> 1); if (q >= N) q -= N; }
-                v[b][r] = active ? __ldcs(&gin[(long long)q * gstr]) : make_float2(0.f, 0.f);
+                v[b][r] = active ? __ldcs(&gin[(p ^ cin.xs) * gstr]) : make_float2(0.f, 0.f);
             }
 #pragma unroll
         for (int b = 0; b < B; b++)
 #pragma unroll
-            for (int r = 0; r < R; r++) {
-                const int p = t + T * b + r * NR;
-                int sp;
-                v[b][r] = cmul(chain2_eval(cin, p, N, line, sp), v[b][r]);
-            }
+            for (int r = 0; r < R; r++) v[b][r] = chain2_apply<EXTRA>(cin, t + T * b + r * NR, line, v[b][r], tabs, ex, axis);
         // NS == 1 for the first stage: no twiddles
     } else {
 #pragma unroll
@@ -70,13 +63,8 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
                 const int p = j + r * NR;
                 float2 x = make_float2(0.f, 0.f);
                 if (active) {
-                    if (IN == 0) {
-                        x = s[PADI(p)];
-                    } else {
-                        int sp;
-                        float2 f = chain2_eval(cin, p, N, line, sp);
-                        x = cmul(f, s[PADI(sp)]);
-                    }
+                    if (IN == 0) x = s[PADI(p)];
+                    else x = chain2_apply<EXTRA>(cin, p, line, s[PADI(p ^ cin.xs)], tabs, ex, axis);
                 }
                 if (NS > 1 && r > 0) {
                     float2 w = make_float2(1.f, 0.f);
@@ -104,9 +92,10 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
                 if (OUT == 0) {
                     s[PADI(q)] = v[b][r];
                 } else {
-                    int i = chain2_inv(cout, q, N), sp;
-                    float2 f = chain2_eval(cout, i, N, line, sp);
-                    __stcs(&gout[(long long)i * gstr], cmul(f, v[b][r]));
+                    const int i = q ^ cout.xinv;
+                    float2 o = chain2_apply<EXTRA>(cout, i, line, v[b][r], tabs, ex, axis);
+                    if (has_lf) o = cmul(lf, o);
+                    __stcs(&gout[i * gstr], o);
                 }
             }
         }
@@ -115,21 +104,28 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
 }
 
 // one FFT of N = 2^LOGN points along the line: radix-16 stages, the last one of radix 2..16
-template <int LOGN, int DIR, int IN, int OUT>
+template <int LOGN, int DIR, int IN, int OUT, bool EXTRA>
 __device__ __forceinline__ void fftN(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
-                                     long long gstr, int t, int line, const Chain2& cin, const Chain2& cout,
-                                     const float2* __restrict__ tw, bool active)
+                                     int gstr, int t, int line, const Chain2& cin, const Chain2& cout,
+                                     const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
+                                     const float2* __restrict__ tabs, const PwOps* ex, int axis)
 {
     constexpr int N = 1 << LOGN;
     constexpr int NST = (LOGN + 3) / 4;
     constexpr int RL = 1 << (LOGN - 4 * (NST - 1));
-    stage16<N, 16, 1, DIR, IN, 0>(s, gin, nullptr, gstr, t, line, cin, cout, tw, active);
-    if constexpr (NST >= 3) stage16<N, 16, 16, DIR, 0, 0>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active);
-    if constexpr (NST >= 4) stage16<N, 16, 256, DIR, 0, 0>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active);
-    stage16<N, RL, (1 << (4 * (NST - 1))), DIR, 0, OUT>(s, nullptr, gout, gstr, t, line, cin, cout, tw, active);
+    stage16<N, 16, 1, DIR, IN, 0, EXTRA>(s, gin, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis);
+    if constexpr (NST >= 3)
+        stage16<N, 16, 16, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis);
+    if constexpr (NST >= 4)
+        stage16<N, 16, 256, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis);
+    stage16<N, RL, (1 << (4 * (NST - 1))), DIR, 0, OUT, EXTRA>(s, nullptr, gout, gstr, t, line, cin, cout, tw, active,
+                                                         has_lf, lf, tabs, ex, axis);
 }
 
-template <int LOGN, bool COLS>
+// EXTRA: the pass has non-separable point-wise work (circular masks, rectangular obstacles, the
+// quartic part of the angular transfer function); a separate instantiation keeps its registers out
+// of the common kernels
+template <int LOGN, bool COLS, bool EXTRA>
 __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
 {
     constexpr int N = 1 << LOGN;
@@ -146,29 +142,37 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     const int line = blockIdx.x * L + g;
     const bool active = line < nl;
     float2* s = sm + (size_t)g * P;
-    const long long gstr = COLS ? (long long)nl : 1;
+    const int gstr = COLS ? nl : 1;
     const float2* gin = COLS ? (src + line) : (src + (size_t)line * N);
     const int oline = d.mirror_lines ? (nl - 1 - line) : line;
     float2* gout = COLS ? (dst + oline) : (dst + (size_t)oline * N);
 
     const float2* tabs = p.tabs;
-    const PwOps* extra = d.has_extra ? &d.extra : nullptr;
-    Chain2 pre = make_chain2(d.t_pre, tabs, 0, 0, d.f1_pre.rs, nullptr, d.axis, line, active);
-    Chain2 mid = make_chain2(d.t_mid, tabs, d.f1 ? d.f1_post.rs : 0, d.mirror_along, d.f2 ? d.f2_pre.rs : 0, extra,
-                             d.axis, line, active);
-    Chain2 fin = make_chain2(d.t_fin, tabs, d.f2 ? d.f2_post.rs : 0, 0, 0, nullptr, d.axis, line, active);
+    const PwOps* ex = &d.extra;
+    const int axis = d.axis;
+    Chain2 pre = make_chain2(d.t_pre, 0, 0, d.f1_pre.rs, 0, N);
+    Chain2 mid = make_chain2(d.t_mid, d.f1 ? d.f1_post.rs : 0, d.mirror_along, d.f2 ? d.f2_pre.rs : 0, d.has_extra, N);
+    Chain2 fin = make_chain2(d.t_fin, d.f2 ? d.f2_post.rs : 0, 0, 0, 0, N);
+    // product of the line factors of all chains of the pass, applied once at the store
+    const bool has_lf = (d.t_pre.ltab >= 0) || (d.t_mid.ltab >= 0) || (d.t_fin.ltab >= 0);
+    float2 lf = make_float2(1.f, 0.f);
+    if (has_lf && active) {
+        if (d.t_pre.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_pre.ltab + line]));
+        if (d.t_mid.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_mid.ltab + line]));
+        if (d.t_fin.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_fin.ltab + line]));
+    }
     const float2* tw = p.tw;
     if (d.f1 && d.f2) {
-        if (d.f1 > 0) fftN<LOGN, 1, 2, 0>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active);
-        else fftN<LOGN, -1, 2, 0>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active);
-        if (d.f2 > 0) fftN<LOGN, 1, 1, 1>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active);
-        else fftN<LOGN, -1, 1, 1>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active);
+        if (d.f1 > 0) fftN<LOGN, 1, 2, 0, EXTRA>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis);
+        else fftN<LOGN, -1, 2, 0, EXTRA>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis);
+        if (d.f2 > 0) fftN<LOGN, 1, 1, 1, EXTRA>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis);
+        else fftN<LOGN, -1, 1, 1, EXTRA>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis);
     } else if (d.f1) {
-        if (d.f1 > 0) fftN<LOGN, 1, 2, 1>(s, gin, gout, gstr, t, line, pre, mid, tw, active);
-        else fftN<LOGN, -1, 2, 1>(s, gin, gout, gstr, t, line, pre, mid, tw, active);
+        if (d.f1 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis);
+        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis);
     } else {
-        if (d.f2 > 0) fftN<LOGN, 1, 2, 1>(s, gin, gout, gstr, t, line, mid, fin, tw, active);
-        else fftN<LOGN, -1, 2, 1>(s, gin, gout, gstr, t, line, mid, fin, tw, active);
+        if (d.f2 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis);
+        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis);
     }
 }
 

@@ -1,6 +1,7 @@
-// Line pass instantiation for lines of 2^14 points (see line2.cuh).
+// Line pass instantiation for lines of 2^14 points without non-separable point-wise work (see
+// line2.cuh).
 #include "line2.cuh"
 
 namespace srwg {
-Line2Fn line2_get_14(bool cols) { return cols ? line2_kernel<14, true> : line2_kernel<14, false>; }
+Line2Fn line2_get_14(bool cols) { return cols ? line2_kernel<14, true, false> : line2_kernel<14, false, false>; }
 }  // namespace srwg

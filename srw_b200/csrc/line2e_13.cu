@@ -1,0 +1,7 @@
+// Line pass instantiation for lines of 2^13 points with non-separable point-wise work (see
+// line2.cuh).
+#include "line2.cuh"
+
+namespace srwg {
+Line2Fn line2e_get_13(bool cols) { return cols ? line2_kernel<13, true, true> : line2_kernel<13, false, true>; }
+}  // namespace srwg

@@ -91,6 +91,13 @@ struct ResizeDesc {
     int has_extra;
     PwOps extra;
     long long axx, axz;                        // per-axis gather tables (ResizeAxis), float2 offsets
+    int has_pre;                               // point-wise work on the OLD mesh before resampling (a
+    PwOps pre;                                 //   preceding element-wise pass folded into this one)
+    ChainTab tp;                               // separable part of pre: tab over old x, ltab over old z
+    int has_pre_extra;
+    PwOps pre_extra;
+    int tile_or, tile_oc;                      // tiled kernel: largest old-row / old-column extent of a
+                                               //   tile of new points (0: not tiled)
 };
 
 // per new-mesh index along one axis: first old node of the 4-point stencil, clipped relative cell

@@ -142,8 +142,11 @@ __device__ __forceinline__ ResizeAxis load_axis(const float2* tabs, long long of
 // one new point of one component: bicubic of Re, Im and |E|^2 over the 4x4 old stencil, the
 // reference's bilinear fallback when any of the 32 values is exactly zero, and the amplitude
 // correction by the interpolated intensity (ImproveReAndIm)
+__device__ __forceinline__ float2 pre_factor(const ResizeDesc& d, const float2* tabs, int ix, int iz);
+
 __device__ __forceinline__ float2 resize_point(const float2* __restrict__ o, int nxo, const float* wx, const float* wz,
-                                               float xr, float zr, int irx, int irz)
+                                               float xr, float zr, int irx, int irz, const ResizeDesc* pre = nullptr,
+                                               const float2* tabs = nullptr, int gx = 0, int gz = 0)
 {
     float2 f[4][4];
     bool low = false;
@@ -152,6 +155,7 @@ __device__ __forceinline__ float2 resize_point(const float2* __restrict__ o, int
 #pragma unroll
         for (int dx = 0; dx < 4; dx++) {
             float2 v = __ldg(&o[(size_t)dz * nxo + dx]);
+            if (pre) v = cmul(pre_factor(*pre, tabs, gx + dx, gz + dz), v);
             f[dz][dx] = v;
             low |= (v.x == 0.f) || (v.y == 0.f);
         }
@@ -295,7 +299,7 @@ __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
             lagrange4(a1.rel, wx1);
             const int base = a0.st & ~1;
             const int o0 = a0.st - base, o1 = a1.st - base;
-            const bool vec = p.vec_ok && in0 && in1 && (o1 >= o0) && (o1 <= 2) && (base + 6 <= d.nxo);
+            const bool vec = p.vec_ok && in0 && in1 && (o1 >= o0) && (o1 <= 2) && (base + 6 <= d.nxo) && !d.has_pre;
             if (vec) {
 #pragma unroll
                 for (int c = 0; c < 2; c++) {
@@ -319,10 +323,11 @@ __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
             } else {
 #pragma unroll
                 for (int c = 0; c < 2; c++) {
+                    const ResizeDesc* pre = d.has_pre ? &d : nullptr;
                     if (in0) out[0][c] = resize_point(p.src[c] + (size_t)az.st * d.nxo + a0.st, d.nxo, wx0, wz, a0.rel,
-                                                      az.rel, a0.ir, az.ir);
+                                                      az.rel, a0.ir, az.ir, pre, p.tabs, a0.st, az.st);
                     if (in1) out[1][c] = resize_point(p.src[c] + (size_t)az.st * d.nxo + a1.st, d.nxo, wx1, wz, a1.rel,
-                                                      az.rel, a1.ir, az.ir);
+                                                      az.rel, a1.ir, az.ir, pre, p.tabs, a1.st, az.st);
                 }
             }
         }
@@ -348,6 +353,176 @@ __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
             __stcs(&p.dst[c][o], out[0][c]);
             if (two) __stcs(&p.dst[c][o + 1], out[1][c]);
         }
+    }
+}
+
+// point-wise work folded in from a preceding element-wise pass, at old index (ix, iz); the same
+// operations in the same order as pw_kernel
+__device__ __forceinline__ float2 pre_factor(const ResizeDesc& d, const float2* tabs, int ix, int iz)
+{
+    float2 e = make_float2(1.f, 0.f);
+    if (d.tp.tab >= 0) e = __ldg(&tabs[d.tp.tab + ix]);
+    if (d.tp.ltab >= 0) e = cmul(e, __ldg(&tabs[d.tp.ltab + iz]));
+    bool zero = false;
+    if (d.has_pre_extra) extra_eval(d.pre_extra, ix, iz, e, zero);
+    return zero ? make_float2(0.f, 0.f) : e;
+}
+
+// Tiled RESIZE pass: a CTA makes a TZ x TX tile of new points.  The old points under the tile's
+// stencils are staged once in shared memory (with the folded point-wise work applied); the 4x4
+// interpolation is separable, so the x interpolation of Re, Im and |E|^2 is done once per (old
+// row, new column) and each new point combines four of those rows.  The operation order per new
+// point is that of resize_kernel (x first, then z; same FMAs), so both kernels give identical
+// results.  Points outside the window are written as zeros.
+__global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
+{
+    const ResizeDesc& d = *p.gd;
+    constexpr int TX = SRWG_RESIZE_TX, TZ = SRWG_RESIZE_TZ;
+    extern __shared__ float4 rsm[];
+    const int OR = d.tile_or, OC = d.tile_oc;
+    float4* wxs = rsm;                    // x weights per tile column
+    float4* axs = wxs + TX;               // (st, ir, rel) per tile column
+    float4* wzs = axs + TX;               // z weights per tile row
+    float4* azs = wzs + TZ;
+    float4* H = azs + TZ;                 // [comp][old row][tile column]: (Re, Im, |E|^2, any zero)
+    float2* old = reinterpret_cast<float2*>(H + 2 * OR * TX);   // [comp][old row][old column]
+    __shared__ int ext[4];
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * TX, z0 = blockIdx.y * TZ;
+    const int xa = max(x0, (int)d.ixStart), xb = min(min(x0 + TX, d.nxn) - 1, (int)d.ixEnd);
+    const int za = max(z0, (int)d.izStart), zb = min(min(z0 + TZ, d.nzn) - 1, (int)d.izEnd);
+    if (xa > xb || za > zb) {
+        for (int e = tid; e < TZ * TX; e += 256) {
+            const int gi = x0 + (e & (TX - 1)), gj = z0 + e / TX;
+            if (gi < d.nxn && gj < d.nzn) {
+                const size_t o = (size_t)gj * d.nxn + gi;
+                __stcs(&p.dst[0][o], make_float2(0.f, 0.f));
+                __stcs(&p.dst[1][o], make_float2(0.f, 0.f));
+            }
+        }
+        return;
+    }
+    if (tid == 0) { ext[0] = 1 << 30; ext[1] = -1; ext[2] = 1 << 30; ext[3] = -1; }
+    __syncthreads();
+    if (tid < TX) {
+        const int i = x0 + tid;
+        if (i >= xa && i <= xb) {
+            const ResizeAxis a = load_axis(p.tabs, d.axx, i);
+            float w[4];
+            lagrange4(a.rel, w);
+            wxs[tid] = make_float4(w[0], w[1], w[2], w[3]);
+            axs[tid] = make_float4(__int_as_float(a.st), __int_as_float(a.ir), a.rel, 0.f);
+            atomicMin(&ext[0], a.st);
+            atomicMax(&ext[1], a.st);
+        }
+    } else if (tid >= 128 && tid < 128 + TZ) {
+        const int j = z0 + tid - 128;
+        if (j >= za && j <= zb) {
+            const ResizeAxis a = load_axis(p.tabs, d.axz, j);
+            float w[4];
+            lagrange4(a.rel, w);
+            wzs[tid - 128] = make_float4(w[0], w[1], w[2], w[3]);
+            azs[tid - 128] = make_float4(__int_as_float(a.st), __int_as_float(a.ir), a.rel, 0.f);
+            atomicMin(&ext[2], a.st);
+            atomicMax(&ext[3], a.st);
+        }
+    }
+    __syncthreads();
+    const int ox0 = ext[0], oz0 = ext[2];
+    const int nc = ext[1] - ox0 + 4, nr = ext[3] - oz0 + 4;     // <= OC, OR (host-computed maxima)
+    // old tile of both components, with the folded point-wise work
+    for (int e = tid; e < nr * nc; e += 256) {
+        const int r = e / nc, c = e - r * nc;
+        const int gx = ox0 + c, gz = oz0 + r;
+        const size_t go = (size_t)gz * d.nxo + gx;
+        float2 v0 = __ldg(&p.src[0][go]), v1 = __ldg(&p.src[1][go]);
+        if (d.has_pre) {
+            const float2 f = pre_factor(d, p.tabs, gx, gz);
+            v0 = cmul(f, v0);
+            v1 = cmul(f, v1);
+        }
+        old[r * OC + c] = v0;
+        old[OR * OC + r * OC + c] = v1;
+    }
+    __syncthreads();
+    // x interpolation per (old row, tile column)
+    for (int e = tid; e < 2 * nr * TX; e += 256) {
+        const int comp = e >= nr * TX;
+        const int e2 = e - comp * nr * TX;
+        const int r = e2 / TX, i = e2 & (TX - 1);
+        const int gi = x0 + i;
+        if (gi < xa || gi > xb) continue;
+        const float4 w4 = wxs[i];
+        const float w[4] = {w4.x, w4.y, w4.z, w4.w};
+        const float2* row = old + comp * OR * OC + r * OC + (__float_as_int(axs[i].x) - ox0);
+        float rx = 0.f, ry = 0.f, ri = 0.f;
+        bool low = false;
+#pragma unroll
+        for (int dx = 0; dx < 4; dx++) {
+            const float2 v = row[dx];
+            low |= (v.x == 0.f) || (v.y == 0.f);
+            rx = fmaf(w[dx], v.x, rx);
+            ry = fmaf(w[dx], v.y, ry);
+            ri = fmaf(w[dx], v.x * v.x + v.y * v.y, ri);
+        }
+        H[comp * OR * TX + r * TX + i] = make_float4(rx, ry, ri, low ? 1.f : 0.f);
+    }
+    __syncthreads();
+    // new points: z interpolation, low-order fallback, amplitude correction, new-mesh factors
+    for (int e = tid; e < TZ * TX; e += 256) {
+        const int jj = e / TX, i = e & (TX - 1);
+        const int gi = x0 + i, gj = z0 + jj;
+        if (gi >= d.nxn || gj >= d.nzn) continue;
+        float2 out[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        if (gi >= xa && gi <= xb && gj >= za && gj <= zb) {
+            const float4 wz4 = wzs[jj], az = azs[jj], ax = axs[i];
+            const float wz[4] = {wz4.x, wz4.y, wz4.z, wz4.w};
+            const int r0 = __float_as_int(az.x) - oz0;
+#pragma unroll
+            for (int comp = 0; comp < 2; comp++) {
+                const float4* h = H + comp * OR * TX + r0 * TX + i;
+                float2 F = make_float2(0.f, 0.f);
+                float FI = 0.f;
+                bool low = false;
+#pragma unroll
+                for (int dz = 0; dz < 4; dz++) {
+                    const float4 q = h[dz * TX];
+                    low |= q.w != 0.f;
+                    F.x = fmaf(wz[dz], q.x, F.x);
+                    F.y = fmaf(wz[dz], q.y, F.y);
+                    FI = fmaf(wz[dz], q.z, FI);
+                }
+                if (low) {
+                    // bilinear on the 2x2 sub-cell (ir_x, ir_z) of the stencil (CheckForLowOrderInterp)
+                    const int irx = __float_as_int(ax.y), irz = __float_as_int(az.y);
+                    const float xr = ax.z, zr = az.z;
+                    const float2* c0 = old + comp * OR * OC + (r0 + irz) * OC + (__float_as_int(ax.x) - ox0) + irx;
+                    const float2 f00 = c0[0], f10 = c0[1], f01 = c0[OC], f11 = c0[OC + 1];
+                    const float xz = xr * zr;
+                    F.x = f00.x + (f10.x - f00.x) * xr + (f01.x - f00.x) * zr + (f00.x - f01.x - f10.x + f11.x) * xz;
+                    F.y = f00.y + (f10.y - f00.y) * xr + (f01.y - f00.y) * zr + (f00.y - f01.y - f10.y + f11.y) * xz;
+                    const float i00 = f00.x * f00.x + f00.y * f00.y, i10 = f10.x * f10.x + f10.y * f10.y;
+                    const float i01 = f01.x * f01.x + f01.y * f01.y, i11 = f11.x * f11.x + f11.y * f11.y;
+                    FI = i00 + (i10 - i00) * xr + (i01 - i00) * zr + (i00 - i01 - i10 + i11) * xz;
+                }
+                FI = FI > 0.f ? FI : 0.f;
+                const float app = F.x * F.x + F.y * F.y;      // ImproveReAndIm
+                if (app != 0.f) {
+                    const float fac = sqrtf(FI / app);
+                    F.x *= fac;
+                    F.y *= fac;
+                }
+                out[comp] = F;
+            }
+            if (d.has_pw) {
+                const float2 f = resize_factor(d, p.tabs, gi, gj);
+                out[0] = cmul(out[0], f);
+                out[1] = cmul(out[1], f);
+            }
+        }
+        const size_t o = (size_t)gj * d.nxn + gi;
+        __stcs(&p.dst[0][o], out[0]);
+        __stcs(&p.dst[1][o], out[1]);
     }
 }
 
@@ -424,6 +599,19 @@ cudaError_t launch_resize(const ResizeLaunch& q, cudaStream_t st)
     p.vec_ok = ((q.d.nxo & 1) == 0) && ((q.d.nxn & 1) == 0);
     for (int c = 0; c < 2; c++)
         p.vec_ok = p.vec_ok && ((((uintptr_t)q.src[c]) & 15) == 0) && ((((uintptr_t)q.dst[c]) & 15) == 0);
+    if (p.d.tile_or > 0 && p.d.tile_oc > 0 && p.d.tile_or <= SRWG_RESIZE_OR_MAX && p.d.tile_oc <= SRWG_RESIZE_OC_MAX) {
+        const size_t smem = (size_t)(2 * SRWG_RESIZE_TX + 2 * SRWG_RESIZE_TZ) * sizeof(float4) +
+                            (size_t)2 * p.d.tile_or * SRWG_RESIZE_TX * sizeof(float4) +
+                            (size_t)2 * p.d.tile_or * p.d.tile_oc * sizeof(float2);
+        static int attr = 0;
+        if (!attr) {
+            cudaFuncSetAttribute(resize2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
+            attr = 1;
+        }
+        dim3 grid((p.d.nxn + SRWG_RESIZE_TX - 1) / SRWG_RESIZE_TX, (p.d.nzn + SRWG_RESIZE_TZ - 1) / SRWG_RESIZE_TZ);
+        resize2_kernel<<<grid, 256, smem, st>>>(p);
+        return cudaGetLastError();
+    }
     dim3 blk(64, 4);
     const int nxh = (p.d.nxn + 1) / 2;
     dim3 grid((nxh + blk.x - 1) / blk.x, (p.d.nzn + blk.y - 1) / blk.y);

@@ -233,8 +233,20 @@ public:
     }
     void resize(const WfrState& o, const WfrState& n, int only_larger)
     {
+        // a pending element-wise pass without mirrors on the old mesh is folded into the resize
+        // (applied to the old points as they are gathered)
+        PwOps pre;
+        int has_pre = 0;
+        if (!only_larger && open >= 0 && open == (int)ks.size() - 1 && ks[open].kind == K_PW &&
+            !ks[open].pwk.mirror_x && !ks[open].pwk.mirror_z && ks[open].pwk.nx == o.nx && ks[open].pwk.nz == o.nz) {
+            pre = ks[open].pwk.pw;
+            has_pre = 1;
+            cur = ks[open].src;
+            ks.pop_back();
+        }
         close();
         KernelDesc& k = newk(K_RESIZE, n.nx, n.nz);
+        if (has_pre) { k.rs.has_pre = 1; k.rs.pre = pre; }
         ResizeDesc& r = k.rs;
         r.nxo = o.nx; r.nzo = o.nz; r.nxn = n.nx; r.nzn = n.nz;
         r.xStartO = o.xStart; r.xStepO = o.xStep; r.zStartO = o.zStart; r.zStepO = o.zStep;
@@ -1044,8 +1056,9 @@ std::string Planner::describe() const
                      d.axis == 0 ? "rows" : "cols", d.nx, d.nz, d.f1, d.has_pw, d.pw.has_quad, d.pw.has_ang, d.pw.nmask,
                      d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, k.src, k.dst);
         } else if (k.kind == K_RESIZE) {
-            snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pw=%d  buf %d->%d\n", i, k.rs.nxo, k.rs.nzo,
-                     k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pw, k.src, k.dst);
+            snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pre=%d pw=%d tile=%dx%d  buf %d->%d\n", i,
+                     k.rs.nxo, k.rs.nzo, k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pre, k.rs.has_pw, k.rs.tile_or,
+                     k.rs.tile_oc, k.src, k.dst);
         } else {
             snprintf(buf, sizeof(buf), "%zu PW %dx%d (q%d a%d m%d s%d) mirror=%d/%d  buf %d->%d\n", i, k.pwk.nx, k.pwk.nz,
                      k.pwk.pw.has_quad, k.pwk.pw.has_ang, k.pwk.pw.nmask, k.pwk.pw.has_scale, k.pwk.mirror_x,

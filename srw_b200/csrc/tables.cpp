@@ -11,6 +11,7 @@
 #include <cstring>
 #include <vector>
 
+#include "kernels.h"
 #include "planner.h"
 
 namespace srwg {
@@ -166,6 +167,24 @@ static long long resize_axis_table(std::vector<float2>& T, int nNew, long iS, lo
     return off;
 }
 
+// largest (max st - min st + 4) over the in-window new indices of each tile of `tile` new indices
+static int tile_extent(const std::vector<float2>& T, long long off, int nNew, long iS, long iE, int tile)
+{
+    int best = 0;
+    for (int t0 = 0; t0 < nNew; t0 += tile) {
+        int lo = 1 << 30, hi = -1;
+        for (int i = t0; i < t0 + tile && i < nNew; i++) {
+            if (i < iS || i > iE) continue;
+            ResizeAxis a;
+            memcpy(&a, &T[off + 2 * i], sizeof(a));
+            if (a.st < lo) lo = a.st;
+            if (a.st > hi) hi = a.st;
+        }
+        if (hi >= lo && hi - lo + 4 > best) best = hi - lo + 4;
+    }
+    return best;
+}
+
 void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& T)
 {
     T.clear();
@@ -203,10 +222,29 @@ void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& T)
                 separate(r.pw, 0, r.nxn, r.nzn, A, Lp, scale, r.extra, r.has_extra);
                 r.t = chain_table(T, r.nxn, r.nzn, 0, 0, 0., 1.f, &A, &Lp, scale, 0, 0, 0, 0.);
             }
+            r.tp.tab = r.tp.ltab = -1;
+            r.has_pre_extra = 0;
+            memset(&r.pre_extra, 0, sizeof(r.pre_extra));
+            if (r.has_pre) {
+                SepPart A, Lp;
+                cd scale;
+                separate(r.pre, 0, r.nxo, r.nzo, A, Lp, scale, r.pre_extra, r.has_pre_extra);
+                r.tp = chain_table(T, r.nxo, r.nzo, 0, 0, 0., 1.f, &A, &Lp, scale, 0, 0, 0, 0.);
+            }
             r.axx = resize_axis_table(T, r.nxn, r.ixStart, r.ixEnd, r.xStartN, r.xStepN, r.xStartO, r.xStepO, r.nxo,
                                       r.only_larger != 0);
             r.axz = resize_axis_table(T, r.nzn, r.izStart, r.izEnd, r.zStartN, r.zStepN, r.zStartO, r.zStepO, r.nzo,
                                       r.only_larger != 0);
+            r.tile_or = r.tile_oc = 0;
+            if (!r.only_larger) {
+                // largest old extent (stencil rows / columns) over the tiles of the tiled kernel
+                const int er = tile_extent(T, r.axz, r.nzn, r.izStart, r.izEnd, SRWG_RESIZE_TZ);
+                const int ec = tile_extent(T, r.axx, r.nxn, r.ixStart, r.ixEnd, SRWG_RESIZE_TX);
+                if (er > 0 && ec > 0 && er <= SRWG_RESIZE_OR_MAX && ec <= SRWG_RESIZE_OC_MAX) {
+                    r.tile_or = er;
+                    r.tile_oc = ec;
+                }
+            }
         } else {
             PwDesc& p = k.pwk;
             SepPart A, Lp;

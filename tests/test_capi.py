@@ -57,9 +57,10 @@ def test_planner_mesh_bit_exact(name):
 
 
 def test_pass_fusion_counts():
-    # C0: 2 angular drifts around aperture+lens -> 5 passes; C1: aperture, resize(+lens), to-waist -> 4
+    # C0: 2 angular drifts around aperture+lens -> 5 passes; C1: resize (+ the aperture and the
+    # quadratic-term removal before it, + the lens after it), to-waist rows + columns -> 3
     assert plan_case('c0_64')[0].n_kernels == 5
-    assert plan_case('c1_64')[0].n_kernels == 4
+    assert plan_case('c1_64')[0].n_kernels == 3
     assert plan_case('c2_128')[0].n_kernels == 5
 
 
@@ -69,7 +70,8 @@ def test_full_size_c1_plan():
     p = Plan(w, beamline(C1, C1PP))
     assert (p.nx_out, p.ny_out) == (4096, 4096)
     k = p.kernels()
-    assert k[1][0] == 'resize' and k[1][3:] == (4096, 4096)
+    assert k[0][0] == 'resize' and k[0][3:] == (4096, 4096)
+    assert 'pre=1' in p.describe() and 'tile=' in p.describe()
 
 
 def test_unsupported_and_invalid_inputs_raise():

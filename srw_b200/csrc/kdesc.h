@@ -77,6 +77,8 @@ struct LineDesc {
     ChainTab t_pre, t_mid, t_fin;   // tables of the pre / middle / final chains
     int has_extra;                  // non-separable point-wise work of the middle chain
     PwOps extra;
+    int zwin;                       // the input is zero outside lines [zl0, zl1] x along [za0, za1]
+    int zl0, zl1, za0, za1;         //   (the output window of the resize that produced it)
 };
 
 struct ResizeDesc {
@@ -98,6 +100,8 @@ struct ResizeDesc {
     PwOps pre_extra;
     int tile_or, tile_oc;                      // tiled kernel: largest old-row / old-column extent of a
                                                //   tile of new points (0: not tiled)
+    int skip_zero;                             // points outside the window are not written: the next
+                                               //   pass treats them as zero (LineDesc::zwin)
 };
 
 // per new-mesh index along one axis: first old node of the 4-point stencil, clipped relative cell

@@ -392,6 +392,7 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
     const int xa = max(x0, (int)d.ixStart), xb = min(min(x0 + TX, d.nxn) - 1, (int)d.ixEnd);
     const int za = max(z0, (int)d.izStart), zb = min(min(z0 + TZ, d.nzn) - 1, (int)d.izEnd);
     if (xa > xb || za > zb) {
+        if (d.skip_zero) return;
         for (int e = tid; e < TZ * TX; e += 256) {
             const int gi = x0 + (e & (TX - 1)), gj = z0 + e / TX;
             if (gi < d.nxn && gj < d.nzn) {
@@ -474,7 +475,9 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
         const int gi = x0 + i, gj = z0 + jj;
         if (gi >= d.nxn || gj >= d.nzn) continue;
         float2 out[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-        if (gi >= xa && gi <= xb && gj >= za && gj <= zb) {
+        const bool inw = gi >= xa && gi <= xb && gj >= za && gj <= zb;
+        if (!inw && d.skip_zero) continue;
+        if (inw) {
             const float4 wz4 = wzs[jj], az = azs[jj], ax = axs[i];
             const float wz[4] = {wz4.x, wz4.y, wz4.z, wz4.w};
             const int r0 = __float_as_int(az.x) - oz0;

@@ -20,7 +20,8 @@ template <int N, int R, int NS, int DIR, int IN, int OUT, bool EXTRA>
 __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
                                         int gstr, int t, int line, const Chain2& cin, const Chain2& cout,
                                         const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
-                                        const float2* __restrict__ tabs, const PwOps* ex, int axis)
+                                        const float2* __restrict__ tabs, const PwOps* ex, int axis,
+                                        int za0, int za1)
 {
     constexpr int T = N / 16;
     constexpr int B = 16 / R;
@@ -34,7 +35,9 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int p = t + T * b + r * NR;
-                v[b][r] = active ? __ldcs(&gin[(p ^ cin.xs) * gstr]) : make_float2(0.f, 0.f);
+                const int q = p ^ cin.xs;
+                const bool in = active && q >= za0 && q <= za1;
+                v[b][r] = in ? __ldcs(&gin[q * gstr]) : make_float2(0.f, 0.f);
             }
 #pragma unroll
         for (int b = 0; b < B; b++)
@@ -108,18 +111,19 @@ template <int LOGN, int DIR, int IN, int OUT, bool EXTRA>
 __device__ __forceinline__ void fftN(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
                                      int gstr, int t, int line, const Chain2& cin, const Chain2& cout,
                                      const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
-                                     const float2* __restrict__ tabs, const PwOps* ex, int axis)
+                                     const float2* __restrict__ tabs, const PwOps* ex, int axis, int za0,
+                                     int za1)
 {
     constexpr int N = 1 << LOGN;
     constexpr int NST = (LOGN + 3) / 4;
     constexpr int RL = 1 << (LOGN - 4 * (NST - 1));
-    stage16<N, 16, 1, DIR, IN, 0, EXTRA>(s, gin, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis);
+    stage16<N, 16, 1, DIR, IN, 0, EXTRA>(s, gin, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     if constexpr (NST >= 3)
-        stage16<N, 16, 16, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis);
+        stage16<N, 16, 16, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     if constexpr (NST >= 4)
-        stage16<N, 16, 256, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis);
+        stage16<N, 16, 256, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     stage16<N, RL, (1 << (4 * (NST - 1))), DIR, 0, OUT, EXTRA>(s, nullptr, gout, gstr, t, line, cin, cout, tw, active,
-                                                         has_lf, lf, tabs, ex, axis);
+                                                         has_lf, lf, tabs, ex, axis, za0, za1);
 }
 
 // EXTRA: the pass has non-separable point-wise work (circular masks, rectangular obstacles, the
@@ -147,6 +151,21 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     const int oline = d.mirror_lines ? (nl - 1 - line) : line;
     float2* gout = COLS ? (dst + oline) : (dst + (size_t)oline * N);
 
+    // input known to be zero outside lines [zl0, zl1] x points [za0, za1] (output of a resize that
+    // wrote only its window): loads outside are skipped, all-zero tiles write zeros directly
+    int za0 = 0, za1 = N - 1;
+    if (d.zwin) {
+        const int l0 = blockIdx.x * L, l1 = min(l0 + L, nl) - 1;
+        if (l1 < d.zl0 || l0 > d.zl1) {
+            if (active) {
+#pragma unroll
+                for (int m = 0; m < 16; m++) __stcs(&gout[(t + T * m) * gstr], make_float2(0.f, 0.f));
+            }
+            return;
+        }
+        if (line < d.zl0 || line > d.zl1) { za0 = 1; za1 = 0; }
+        else { za0 = d.za0; za1 = d.za1; }
+    }
     const float2* tabs = p.tabs;
     const PwOps* ex = &d.extra;
     const int axis = d.axis;
@@ -163,16 +182,16 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     }
     const float2* tw = p.tw;
     if (d.f1 && d.f2) {
-        if (d.f1 > 0) fftN<LOGN, 1, 2, 0, EXTRA>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis);
-        else fftN<LOGN, -1, 2, 0, EXTRA>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis);
-        if (d.f2 > 0) fftN<LOGN, 1, 1, 1, EXTRA>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis);
-        else fftN<LOGN, -1, 1, 1, EXTRA>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis);
+        if (d.f1 > 0) fftN<LOGN, 1, 2, 0, EXTRA>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        else fftN<LOGN, -1, 2, 0, EXTRA>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        if (d.f2 > 0) fftN<LOGN, 1, 1, 1, EXTRA>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        else fftN<LOGN, -1, 1, 1, EXTRA>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     } else if (d.f1) {
-        if (d.f1 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis);
-        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis);
+        if (d.f1 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     } else {
-        if (d.f2 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis);
-        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis);
+        if (d.f2 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     }
 }
 

@@ -14,8 +14,10 @@
 // SRWG_STATIC_CONST_POINTS float2 (1 MiB); larger propagations are rejected with
 // SRWG_ERR_STATIC_LIMIT and a message giving the sizes.
 //
-// All calls share the array and it keeps the last call's contents.  Every pass writes each
-// point of its output before any later pass reads it, so nothing has to start at zero.  Calls
+// All calls share the array and it keeps the last call's contents.  Nothing has to start at
+// zero: every point a pass reads was written earlier in the same call (a resize that leaves the
+// points outside its window unwritten is followed by a pass that treats them as zero without
+// reading them).  Calls
 // that overlap on the GPU (issued on different streams with no ordering between them) race on
 // the array; issue them on one stream, or order them with events.
 //

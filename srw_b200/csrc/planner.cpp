@@ -1041,6 +1041,24 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
         }
     }
     build_tables(kernels, tables);
+    // a tiled resize followed by a line pass on its output writes only its window; the line pass
+    // reads zeros outside it (the buffer is overwritten before anything else reads it)
+    for (size_t i = 0; i + 1 < kernels.size(); i++) {
+        ResizeDesc& r = kernels[i].rs;
+        KernelDesc& n = kernels[i + 1];
+        if (kernels[i].kind != K_RESIZE || r.only_larger || r.tile_or == 0 || n.kind != K_LINE ||
+            n.src != kernels[i].dst || n.line.nx != r.nxn || n.line.nz != r.nzn)
+            continue;
+        const int N = n.line.axis == 0 ? n.line.nx : n.line.nz;
+        if (N < 64 || (N & (N - 1)) != 0) continue;      // power-of-two line kernels only
+        LineDesc& d = n.line;
+        const int ixs = (int)std::max(0L, r.ixStart), ixe = (int)std::min((long)r.nxn - 1, r.ixEnd);
+        const int izs = (int)std::max(0L, r.izStart), ize = (int)std::min((long)r.nzn - 1, r.izEnd);
+        r.skip_zero = 1;
+        d.zwin = 1;
+        if (d.axis == 0) { d.zl0 = izs; d.zl1 = ize; d.za0 = ixs; d.za1 = ixe; }
+        else { d.zl0 = ixs; d.zl1 = ixe; d.za0 = izs; d.za1 = ize; }
+    }
     return 0;
 }
 
@@ -1052,9 +1070,9 @@ std::string Planner::describe() const
         const KernelDesc& k = kernels[i];
         if (k.kind == K_LINE) {
             const LineDesc& d = k.line;
-            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d  buf %d->%d\n", i,
+            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d zwin=%d  buf %d->%d\n", i,
                      d.axis == 0 ? "rows" : "cols", d.nx, d.nz, d.f1, d.has_pw, d.pw.has_quad, d.pw.has_ang, d.pw.nmask,
-                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, k.src, k.dst);
+                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, d.zwin, k.src, k.dst);
         } else if (k.kind == K_RESIZE) {
             snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pre=%d pw=%d tile=%dx%d  buf %d->%d\n", i,
                      k.rs.nxo, k.rs.nzo, k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pre, k.rs.has_pw, k.rs.tile_or,

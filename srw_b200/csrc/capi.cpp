@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -137,10 +138,7 @@ int line_config(const LineDesc& d, LineLaunch& p)
         // one pad point per 16 (conflict-free Stockham exchanges) plus 4 per line, so that the
         // lines of a tile start 8 banks apart
         p.P = N + N / 16 + 4;
-        int L = d.axis == 0 ? (256 / p.T) : (1024 / p.T);
-        if (L < 1) L = 1;
-        if (d.axis == 1 && L > 32) L = 32;
-        while (L > 1 && (size_t)L * p.P * sizeof(float2) > cap) L--;
+        const int L = line2_lines_per_cta(d.axis, N);
         if (p.T * L > 1024) { g_lastDetail = "line pass too large"; return SRWG_ERR_UNSUPPORTED; }
         p.L = L;
         p.G = L;

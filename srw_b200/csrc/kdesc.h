@@ -79,6 +79,8 @@ struct LineDesc {
     PwOps extra;
     int zwin;                       // the input is zero outside lines [zl0, zl1] x along [za0, za1]
     int zl0, zl1, za0, za1;         //   (the output window of the resize that produced it)
+    int blk_out;                    // row pass: output in blocks of blk_out columns (0: row-major)
+    int blk_in;                     // column pass: input in blocks of blk_in columns (0: row-major)
 };
 
 struct ResizeDesc {

@@ -8,6 +8,19 @@ namespace srwg {
 // dynamic shared memory of a line pass (leaves room for the static descriptor copy)
 #define SRWG_LINE_SMEM_MAX (220 * 1024)
 
+// lines per CTA of the power-of-two line pass (line2_kernel): rows ~256 threads, columns up to
+// 1024 threads (at most 32 columns), within the shared-memory budget; pitch N + N/16 + 4 points
+inline int line2_lines_per_cta(int axis, int N)
+{
+    const int T = N / 16;
+    int L = axis == 0 ? 256 / T : 1024 / T;
+    if (L < 1) L = 1;
+    if (axis == 1 && L > 32) L = 32;
+    const size_t P = (size_t)N + N / 16 + 4;
+    while (L > 1 && (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) L--;
+    return L;
+}
+
 struct LineLaunch {
     LineDesc d;
     const float2* src[2];

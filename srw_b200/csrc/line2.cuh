@@ -16,9 +16,16 @@ namespace srwg {
 
 // IN: 0 shared, 1 shared through chain cin, 2 global through chain cin;  OUT: 0 shared, 1 global through chain cout
 // N (line length), R (radix) and Ns (product of the radices already applied) are compile-time.
+// element i of the output line: row-major (offset i * str) or, for a row pass feeding a column pass,
+// column-blocked: blocks of 2^lg columns stored contiguously per row, offset (i >> lg) * bstr + (i & mask)
+struct OutMap {
+    int str, lg, bstr;
+    __device__ __forceinline__ int at(int i) const { return lg < 0 ? i * str : ((i >> lg) * bstr + (i & ((1 << lg) - 1))); }
+};
+
 template <int N, int R, int NS, int DIR, int IN, int OUT, bool EXTRA>
 __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
-                                        int gstr, int t, int line, const Chain2& cin, const Chain2& cout,
+                                        int gstr, const OutMap& om, int t, int line, const Chain2& cin, const Chain2& cout,
                                         const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
                                         const float2* __restrict__ tabs, const PwOps* ex, int axis,
                                         int za0, int za1)
@@ -98,7 +105,7 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
                     const int i = q ^ cout.xinv;
                     float2 o = chain2_apply<EXTRA>(cout, i, line, v[b][r], tabs, ex, axis);
                     if (has_lf) o = cmul(lf, o);
-                    __stcs(&gout[i * gstr], o);
+                    __stcs(&gout[om.at(i)], o);
                 }
             }
         }
@@ -109,7 +116,7 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
 // one FFT of N = 2^LOGN points along the line: radix-16 stages, the last one of radix 2..16
 template <int LOGN, int DIR, int IN, int OUT, bool EXTRA>
 __device__ __forceinline__ void fftN(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
-                                     int gstr, int t, int line, const Chain2& cin, const Chain2& cout,
+                                     int gstr, const OutMap& om, int t, int line, const Chain2& cin, const Chain2& cout,
                                      const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
                                      const float2* __restrict__ tabs, const PwOps* ex, int axis, int za0,
                                      int za1)
@@ -117,12 +124,12 @@ __device__ __forceinline__ void fftN(float2* s, const float2* __restrict__ gin, 
     constexpr int N = 1 << LOGN;
     constexpr int NST = (LOGN + 3) / 4;
     constexpr int RL = 1 << (LOGN - 4 * (NST - 1));
-    stage16<N, 16, 1, DIR, IN, 0, EXTRA>(s, gin, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+    stage16<N, 16, 1, DIR, IN, 0, EXTRA>(s, gin, nullptr, gstr, om, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     if constexpr (NST >= 3)
-        stage16<N, 16, 16, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        stage16<N, 16, 16, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, om, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     if constexpr (NST >= 4)
-        stage16<N, 16, 256, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-    stage16<N, RL, (1 << (4 * (NST - 1))), DIR, 0, OUT, EXTRA>(s, nullptr, gout, gstr, t, line, cin, cout, tw, active,
+        stage16<N, 16, 256, DIR, 0, 0, EXTRA>(s, nullptr, nullptr, gstr, om, t, line, cin, cout, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+    stage16<N, RL, (1 << (4 * (NST - 1))), DIR, 0, OUT, EXTRA>(s, nullptr, gout, gstr, om, t, line, cin, cout, tw, active,
                                                          has_lf, lf, tabs, ex, axis, za0, za1);
 }
 
@@ -146,10 +153,24 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     const int line = blockIdx.x * L + g;
     const bool active = line < nl;
     float2* s = sm + (size_t)g * P;
-    const int gstr = COLS ? nl : 1;
+    // input: row-major, or (column pass after a row pass) blocks of blk_in columns stored together
+    int gstr = COLS ? nl : 1;
     const float2* gin = COLS ? (src + line) : (src + (size_t)line * N);
+    if (COLS && d.blk_in > 0) {
+        gstr = d.blk_in;
+        gin = src + (size_t)(line / d.blk_in) * N * d.blk_in + (line % d.blk_in);
+    }
     const int oline = d.mirror_lines ? (nl - 1 - line) : line;
     float2* gout = COLS ? (dst + oline) : (dst + (size_t)oline * N);
+    OutMap om;
+    om.str = COLS ? nl : 1;
+    om.lg = -1;
+    om.bstr = 0;
+    if (!COLS && d.blk_out > 0) {
+        om.lg = 31 - __clz(d.blk_out);
+        om.bstr = nl * d.blk_out;
+        gout = dst + (size_t)oline * d.blk_out;
+    }
 
     // input known to be zero outside lines [zl0, zl1] x points [za0, za1] (output of a resize that
     // wrote only its window): loads outside are skipped, all-zero tiles write zeros directly
@@ -159,7 +180,7 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
         if (l1 < d.zl0 || l0 > d.zl1) {
             if (active) {
 #pragma unroll
-                for (int m = 0; m < 16; m++) __stcs(&gout[(t + T * m) * gstr], make_float2(0.f, 0.f));
+                for (int m = 0; m < 16; m++) __stcs(&gout[om.at(t + T * m)], make_float2(0.f, 0.f));
             }
             return;
         }
@@ -182,16 +203,16 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     }
     const float2* tw = p.tw;
     if (d.f1 && d.f2) {
-        if (d.f1 > 0) fftN<LOGN, 1, 2, 0, EXTRA>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        else fftN<LOGN, -1, 2, 0, EXTRA>(s, gin, nullptr, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        if (d.f2 > 0) fftN<LOGN, 1, 1, 1, EXTRA>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        else fftN<LOGN, -1, 1, 1, EXTRA>(s, nullptr, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        if (d.f1 > 0) fftN<LOGN, 1, 2, 0, EXTRA>(s, gin, nullptr, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        else fftN<LOGN, -1, 2, 0, EXTRA>(s, gin, nullptr, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        if (d.f2 > 0) fftN<LOGN, 1, 1, 1, EXTRA>(s, nullptr, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        else fftN<LOGN, -1, 1, 1, EXTRA>(s, nullptr, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     } else if (d.f1) {
-        if (d.f1 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        if (d.f1 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     } else {
-        if (d.f2 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        if (d.f2 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
     }
 }
 

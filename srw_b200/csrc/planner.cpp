@@ -2,6 +2,7 @@
 // reference's statement order in FP64 (compiled without FP contraction), so resized and
 // transformed meshes are bit-identical to the reference's; the field work is only described
 // (kdesc.h) and fused into as few GPU passes as possible by Builder.
+#include "kernels.h"
 #include "planner.h"
 
 #include <algorithm>
@@ -1059,6 +1060,22 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
         if (d.axis == 0) { d.zl0 = izs; d.zl1 = ize; d.za0 = ixs; d.za1 = ixe; }
         else { d.zl0 = ixs; d.zl1 = ixe; d.za0 = izs; d.za1 = ize; }
     }
+    // a row pass followed by a column pass on its output writes it in blocks of as many columns as
+    // a column CTA transforms, so that the column pass reads whole blocks sequentially
+    for (size_t i = 0; i + 1 < kernels.size(); i++) {
+        KernelDesc& a = kernels[i];
+        KernelDesc& n = kernels[i + 1];
+        if (a.kind != K_LINE || n.kind != K_LINE || a.line.axis != 0 || n.line.axis != 1 || n.src != a.dst ||
+            a.line.nx != n.line.nx || a.line.nz != n.line.nz)
+            continue;
+        const int Nr = a.line.nx, Nc = n.line.nz;
+        auto pow2 = [](int v) { return v >= 64 && v <= 16384 && (v & (v - 1)) == 0; };
+        if (!pow2(Nr) || !pow2(Nc)) continue;
+        const int bw = line2_lines_per_cta(1, Nc);
+        if (bw < 2 || (bw & (bw - 1)) != 0 || n.line.nx % bw != 0) continue;
+        a.line.blk_out = bw;
+        n.line.blk_in = bw;
+    }
     return 0;
 }
 
@@ -1070,9 +1087,9 @@ std::string Planner::describe() const
         const KernelDesc& k = kernels[i];
         if (k.kind == K_LINE) {
             const LineDesc& d = k.line;
-            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d zwin=%d  buf %d->%d\n", i,
-                     d.axis == 0 ? "rows" : "cols", d.nx, d.nz, d.f1, d.has_pw, d.pw.has_quad, d.pw.has_ang, d.pw.nmask,
-                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, d.zwin, k.src, k.dst);
+            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d zwin=%d blk=%d/%d  buf %d->%d\n",
+                     i, d.axis == 0 ? "rows" : "cols", d.nx, d.nz, d.f1, d.has_pw, d.pw.has_quad, d.pw.has_ang, d.pw.nmask,
+                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, d.zwin, d.blk_in, d.blk_out, k.src, k.dst);
         } else if (k.kind == K_RESIZE) {
             snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pre=%d pw=%d tile=%dx%d  buf %d->%d\n", i,
                      k.rs.nxo, k.rs.nzo, k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pre, k.rs.has_pw, k.rs.tile_or,

@@ -161,6 +161,29 @@ SRWG_API int srwgPlanExecuteTimed(srwgPlan* plan, const float* dExIn, const floa
 
 SRWG_API int srwgPlanDestroy(srwgPlan* plan);
 
+/* Partially coherent (multi-electron) propagation on the device (no counterpart C API in the
+ * reference: it is the per-electron loop of srwl_wfr_emit_prop_multi_e, env/python/srwpy/srwlib.py:8506).
+ * Macro-electron wavefronts are the base wavefront with the source offset of SRWLWfr.sim_src_offset
+ * (srwlib.py:2803, _move_mesh=True): an angular kick (x', y') and a mesh shift (x + x' R, y + y' R);
+ * each is propagated through pOpt (planned like srwlPropagElecField) in batches of up to maxBatch
+ * (one launch per pass per batch; useGraph: replayed as a CUDA graph), and its total intensity
+ * (srwlCalcIntFromElecField, polarisation 6, vs x and y) is added, bilinearly interpolated onto
+ * pAccMesh (avg_update_interp order 1, srwlib.py:1116), to an FP64 accumulator on the device.
+ * srwgMultiEAdd takes 4 doubles per electron (x [m], x' [rad], y [m], y' [rad]); a null stream
+ * means the library's stream, synchronised before the call returns.  srwgMultiEGetMean copies the
+ * mean (sum / number of electrons) to host memory.  pOpt must stay valid while the object lives. */
+typedef struct srwgMultiE srwgMultiE;
+SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* pOpt, const SRWLRadMesh* pAccMesh, int maxBatch,
+                              int useGraph, int device, srwgMultiE** out);
+SRWG_API int srwgMultiEAdd(srwgMultiE* m, int n, const double* arOffsets, void* stream);
+SRWG_API int srwgMultiEGetMean(srwgMultiE* m, double* arMean, long long* nElec, void* stream);
+/* device address of the FP64 intensity sum (pAccMesh ny x nx) and the electron count, e.g. for a
+ * sum over ranks; srwgMultiESetAccumulator makes the object add into caller-owned device memory */
+SRWG_API int srwgMultiEAccumulator(srwgMultiE* m, double** dAcc, long long* nElec);
+SRWG_API int srwgMultiESetAccumulator(srwgMultiE* m, double* dAcc);
+SRWG_API int srwgMultiEReset(srwgMultiE* m, void* stream);
+SRWG_API int srwgMultiEDestroy(srwgMultiE* m);
+
 /* Allocation-free propagation (no counterpart in the reference).  For callers that cannot call
  * cudaMalloc at run time -- programs that reserve all device memory at start-up and hand out
  * slices themselves, or whose device memory must go through their own caching allocator --

@@ -1030,3 +1030,74 @@ def propagate(w: Wfr, elements, props):
         if abs(pxd - 1.) > tolRes or abs(pxm - 1.) > tolRes or abs(pzd - 1.) > tolRes or abs(pzm - 1.) > tolRes:
             rad_resize_gen(w, pxm, pxd, pzm, pzd, other_side=bool(int(_pp(pp, 4, 0))))
     return w
+
+
+# ----------------------------------------------------------------------------------------
+# Multi-electron loop pieces (srwl_wfr_emit_prop_multi_e, env/python/srwpy/srwlib.py:8506)
+# ----------------------------------------------------------------------------------------
+
+
+def electron_offset(ex, ey, mesh, sc, dx0, dxp, dy0, dyp):
+    """SRWLWfr.sim_src_offset with _move_mesh=True (env/python/srwpy/srwlib.py:2803-2849): the kick
+    of srTOptAngle::RadPointModifier (cpp/src/core/sroptang.h:64-79; phase 5.06773065e6 e (x' x + y' z)
+    in FP64 on the unshifted mesh, field stored back as FP32), then the mesh moved by
+    (x + x' R, y + y' R), R = (Rx + Ry)/2, and xc += x, yc += y.  Returns (ex, ey, mesh, sc)."""
+    ny, nx = ex.shape
+    xStep = (mesh['xFin'] - mesh['xStart']) / (nx - 1)
+    zStep = (mesh['yFin'] - mesh['yStart']) / (ny - 1)
+    x = mesh['xStart'] + np.arange(nx) * xStep
+    z = mesh['yStart'] + np.arange(ny) * zStep
+    ph = 5.06773065e+06 * mesh['eStart'] * (dxp * x[None, :] + dyp * z[:, None])
+    f = np.exp(1j * ph)
+    ex2 = (np.asarray(ex, np.complex128) * f).astype(np.complex64).astype(np.complex128)
+    ey2 = (np.asarray(ey, np.complex128) * f).astype(np.complex64).astype(np.complex128)
+    R = 0.5 * (sc['Rx'] + sc['Ry'])
+    dx, dy = dx0 + dxp * R, dy0 + dyp * R
+    m2 = dict(mesh)
+    m2['xStart'] += dx
+    m2['xFin'] += dx
+    m2['yStart'] += dy
+    m2['yFin'] += dy
+    sc2 = dict(sc)
+    sc2['xc'] = sc.get('xc', 0.) + dx0
+    sc2['yc'] = sc.get('yc', 0.) + dy0
+    return ex2, ey2, m2, sc2
+
+
+def total_intensity(ex, ey):
+    """srwlCalcIntFromElecField, single-electron intensity, polarisation 6 (total), vs x and y
+    (cpp/src/core/srradmnp.cpp:681): |Ex|^2 + |Ey|^2 stored as FP32."""
+    ex = np.asarray(ex, np.complex64)
+    ey = np.asarray(ey, np.complex64)
+    return (ex.real * ex.real + ex.imag * ex.imag + ey.real * ey.real + ey.imag * ey.imag).astype(np.float32)
+
+
+def add_interp_bilinear(acc, acc_mesh, I, mesh):
+    """acc += I interpolated on acc_mesh: SRWLStokes.avg_update_interp with _ord=1 and _sum=True
+    (env/python/srwpy/srwlib.py:1116-1203; points outside the mesh add nothing)."""
+    anx, any_ = acc_mesh['nx'], acc_mesh['ny']
+    axs = (acc_mesh['xFin'] - acc_mesh['xStart']) / (anx - 1)
+    ays = (acc_mesh['yFin'] - acc_mesh['yStart']) / (any_ - 1)
+    ny, nx = I.shape
+    xs = (mesh['xFin'] - mesh['xStart']) / (nx - 1)
+    ys = (mesh['yFin'] - mesh['yStart']) / (ny - 1)
+    xa = acc_mesh['xStart'] + np.arange(anx) * axs
+    ya = acc_mesh['yStart'] + np.arange(any_) * ays
+    ix0 = np.trunc((xa - mesh['xStart']) / xs + 1.e-09).astype(np.int64)
+    iy0 = np.trunc((ya - mesh['yStart']) / ys + 1.e-09).astype(np.int64)
+    okx = (ix0 >= 0) & (ix0 < nx - 1)
+    oky = (iy0 >= 0) & (iy0 < ny - 1)
+    ix0c = np.clip(ix0, 0, nx - 2)
+    iy0c = np.clip(iy0, 0, ny - 2)
+    tx = (xa - (mesh['xStart'] + xs * ix0c)) / xs
+    ty = (ya - (mesh['yStart'] + ys * iy0c)) / ys
+    I = np.asarray(I, np.float64)
+    a00 = I[iy0c[:, None], ix0c[None, :]]
+    f10 = I[iy0c[:, None], ix0c[None, :] + 1]
+    f01 = I[iy0c[:, None] + 1, ix0c[None, :]]
+    f11 = I[iy0c[:, None] + 1, ix0c[None, :] + 1]
+    a10, a01, a11 = f10 - a00, f01 - a00, a00 - f01 - f10 + f11
+    TX, TY = tx[None, :], ty[:, None]
+    f = a00 + TX * (a10 + TY * a11) + TY * a01
+    acc += np.where(oky[:, None] & okx[None, :], f, 0.)
+    return acc

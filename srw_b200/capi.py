@@ -75,6 +75,14 @@ SYMBOLS = {
     'srwgPlanExecuteTimed': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     'srwgPlanDestroy': (C.c_int, [C.c_void_p]),
+    'srwgMultiECreate': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.POINTER(SRWLRadMesh), C.c_int, C.c_int,
+                                   C.c_int, C.POINTER(C.c_void_p)]),
+    'srwgMultiEAdd': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    'srwgMultiEGetMean': (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong), C.c_void_p]),
+    'srwgMultiEAccumulator': (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)]),
+    'srwgMultiESetAccumulator': (C.c_int, [C.c_void_p, C.c_void_p]),
+    'srwgMultiEReset': (C.c_int, [C.c_void_p, C.c_void_p]),
+    'srwgMultiEDestroy': (C.c_int, [C.c_void_p]),
     'srwgPropagElecFieldStatic': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(SRWLWfr)]),
     'srwgPlanDescribe': (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),

@@ -3,6 +3,7 @@
 // executor that runs a plan's passes on a CUDA stream.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -24,18 +25,8 @@ static std::string g_lastDetail;                          // detail text of the 
 void set_last_detail(const std::string& s) { g_lastDetail = s; }
 static int (*g_modifFunc)(int, SRWLWfr*, char) = nullptr;  // client re-allocation callback
 static std::mutex g_mutex;
+std::mutex& library_mutex() { return g_mutex; }
 
-struct DeviceCtx {
-    int dev = 0;
-    std::map<int, float2*> tw;          // twiddle tables by FFT length
-    float2* work = nullptr;             // 2 work buffers x 2 components
-    size_t workElems = 0;               // per buffer per component
-    float2* io = nullptr;               // input + output staging for the host-memory entry point
-    size_t ioElems = 0;
-    float2* tab = nullptr;              // point-wise tables of the one-shot entry point
-    size_t tabElems = 0;
-    cudaStream_t stream = nullptr;
-};
 static std::map<int, DeviceCtx*> g_ctx;
 
 #define CUDA_TRY(x)                                                                     \
@@ -47,7 +38,7 @@ static std::map<int, DeviceCtx*> g_ctx;
         }                                                                               \
     } while (0)
 
-static int get_ctx(int dev, DeviceCtx** out)
+int device_ctx(int dev, DeviceCtx** out)
 {
     auto it = g_ctx.find(dev);
     if (it != g_ctx.end()) {
@@ -74,7 +65,7 @@ static int get_ctx(int dev, DeviceCtx** out)
 }
 
 // exp(-2 pi i k/N) in FP64, rounded to FP32
-static int twiddles(DeviceCtx& c, int N, const float2** out)
+int device_twiddles(DeviceCtx& c, int N, const float2** out)
 {
     auto it = c.tw.find(N);
     if (it != c.tw.end()) { *out = it->second; return 0; }
@@ -203,41 +194,43 @@ static int upload_tables(const Planner& pl, float2** buf, size_t* capElems, cuda
     return 0;
 }
 
-// runs the plan's passes: buffer 0 = input, 1/2 = work buffers; the last pass writes the output
-static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* inY, float2* outX, float2* outY,
-                   float2* work, size_t workElems, const float2* dtab, cudaStream_t st, cudaEvent_t* ev = nullptr)
+// runs a pass list on nb wavefronts at once: buffer 0 = input (wavefront b at inX + b * inStride), 1/2 =
+// work buffers (layout [buffer][component][wavefront][workElems]); the last pass writes the output
+// (outX + b * outStride).  dconst holds per wavefront (stride constStride bytes) the tables and, at
+// descOff, the pass descriptors; all wavefronts have passes of the same kinds and sizes.
+int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, const float2* inX, const float2* inY,
+                   long long inStride, float2* outX, float2* outY, long long outStride, float2* work, size_t workElems,
+                   const char* dconst, long long constStride, size_t descOff, cudaStream_t st, cudaEvent_t* ev,
+                   const std::vector<KernelDesc>* hostMax)
 {
-    const size_t nOut = (size_t)pl.w.nx * pl.w.nz;
-    if (pl.kernels.empty()) {
-        CUDA_TRY(cudaMemcpyAsync(outX, inX, nOut * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-        CUDA_TRY(cudaMemcpyAsync(outY, inY, nOut * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-        return 0;
-    }
-    float2* wb[3][2] = {{nullptr, nullptr},
-                        {work, work + workElems},
-                        {work + 2 * workElems, work + 3 * workElems}};
-    const size_t nk = pl.kernels.size();
-    size_t descOff;
-    const_bytes(pl, &descOff);
-    const KernelDesc* gk = (const KernelDesc*)((const char*)dtab + descOff);
+    const size_t nk = ks.size();
+    const size_t W = (size_t)nb * workElems;
+    float2* wb[3][2] = {{nullptr, nullptr}, {work, work + W}, {work + 2 * W, work + 3 * W}};
+    const float2* tabs = (const float2*)dconst;
+    const KernelDesc* gk = (const KernelDesc*)(dconst + descOff);
+    const long long tabStride = constStride / (long long)sizeof(float2);
     for (size_t i = 0; i < nk; i++) {
-        const KernelDesc& k = pl.kernels[i];
+        const KernelDesc& k = hostMax ? (*hostMax)[i] : ks[i];
         if (ev) CUDA_TRY(cudaEventRecord(ev[2 * i], st));
-        const float2* s0 = k.src == 0 ? inX : wb[k.src][0];
-        const float2* s1 = k.src == 0 ? inY : wb[k.src][1];
-        float2* d0 = (i + 1 == nk) ? outX : wb[k.dst][0];
-        float2* d1 = (i + 1 == nk) ? outY : wb[k.dst][1];
+        const bool fromIn = k.src == 0, toOut = i + 1 == nk;
+        const float2* s0 = fromIn ? inX : wb[k.src][0];
+        const float2* s1 = fromIn ? inY : wb[k.src][1];
+        float2* d0 = toOut ? outX : wb[k.dst][0];
+        float2* d1 = toOut ? outY : wb[k.dst][1];
+        const long long bSrc = fromIn ? inStride : (long long)workElems;
+        const long long bDst = toOut ? outStride : (long long)workElems;
         cudaError_t e = cudaSuccess;
         if (k.kind == K_LINE) {
             LineLaunch p;
             memset(&p, 0, sizeof(p));
             int r = line_config(k.line, p);
             if (r) return r;
-            r = twiddles(c, p.N, &p.tw);
+            r = device_twiddles(c, p.N, &p.tw);
             if (r) return r;
             p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
-            p.tabs = dtab;
+            p.tabs = tabs;
             p.gd = &gk[i].line;
+            p.nb = nb; p.bDesc = constStride; p.bTab = tabStride; p.bSrc = bSrc; p.bDst = bDst;
             e = launch_line(p, st);
         } else if (k.kind == K_RESIZE) {
             ResizeLaunch p;
@@ -246,16 +239,18 @@ static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* i
             p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
             p.xStepInvO = 1. / k.rs.xStepO;
             p.zStepInvO = 1. / k.rs.zStepO;
-            p.tabs = dtab;
+            p.tabs = tabs;
             p.gd = &gk[i].rs;
+            p.nb = nb; p.bDesc = constStride; p.bTab = tabStride; p.bSrc = bSrc; p.bDst = bDst;
             e = launch_resize(p, st);
         } else {
             PwLaunch p;
             memset(&p, 0, sizeof(p));
             p.d = k.pwk;
             p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
-            p.tabs = dtab;
+            p.tabs = tabs;
             p.gd = &gk[i].pwk;
+            p.nb = nb; p.bDesc = constStride; p.bTab = tabStride; p.bSrc = bSrc; p.bDst = bDst;
             e = launch_pw(p, st);
         }
         if (e != cudaSuccess) {
@@ -265,6 +260,27 @@ static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* i
         if (ev) CUDA_TRY(cudaEventRecord(ev[2 * i + 1], st));
     }
     return 0;
+}
+
+// runs the plan's passes on one wavefront (or nb wavefronts with the same plan)
+static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* inY, float2* outX, float2* outY,
+                   float2* work, size_t workElems, const float2* dtab, cudaStream_t st, cudaEvent_t* ev = nullptr,
+                   int nb = 1, long long inStride = 0, long long outStride = 0)
+{
+    const size_t nOut = (size_t)pl.w.nx * pl.w.nz;
+    if (pl.kernels.empty()) {
+        for (int b = 0; b < nb; b++) {
+            CUDA_TRY(cudaMemcpyAsync(outX + b * outStride, inX + b * inStride, nOut * sizeof(float2),
+                                     cudaMemcpyDeviceToDevice, st));
+            CUDA_TRY(cudaMemcpyAsync(outY + b * outStride, inY + b * inStride, nOut * sizeof(float2),
+                                     cudaMemcpyDeviceToDevice, st));
+        }
+        return 0;
+    }
+    size_t descOff;
+    const_bytes(pl, &descOff);
+    return execute_passes(pl.kernels, c, nb, inX, inY, inStride, outX, outY, outStride, work, workElems,
+                          (const char*)dtab, 0, descOff, st, ev, nullptr);
 }
 
 static int ensure_work(DeviceCtx& c, size_t elems)
@@ -326,7 +342,7 @@ struct srwgPlan {
 
 static int plan_bind(srwgPlan* plan, cudaStream_t st)
 {
-    int r = get_ctx(plan->device, &plan->ctx);
+    int r = device_ctx(plan->device, &plan->ctx);
     if (r) return r;
     if (!plan->tabReady) {
         r = upload_tables(plan->pl, &plan->dtab, &plan->dtabElems, st);
@@ -391,7 +407,7 @@ int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SR
     int r = pl.plan(pWfr, pOpt);
     if (r) { g_lastDetail = pl.err; return r; }
     DeviceCtx* c = nullptr;
-    r = get_ctx(dev, &c);
+    r = device_ctx(dev, &c);
     if (r) return r;
     const size_t nIn = (size_t)pl.in.nx * pl.in.nz, nOut = (size_t)pl.w.nx * pl.w.nz;
     r = ensure_io(*c, nIn > nOut ? nIn : nOut);
@@ -486,10 +502,19 @@ int srwgPlanExecuteBatch(srwgPlan* plan, int n, const float* dExIn, const float*
     int r = plan_bind(plan, st);
     if (r) return r;
     DeviceCtx& c = *plan->ctx;
-    for (int b = 0; b < n; b++) {
-        r = execute(plan->pl, c, (const float2*)(dExIn + b * strideIn), (const float2*)(dEyIn + b * strideIn),
-                    (float2*)(dExOut + b * strideOut), (float2*)(dEyOut + b * strideOut), c.work, c.workElems,
-                    plan->dtab, st);
+    if ((strideIn & 1) || (strideOut & 1)) return SRWG_ERR_BAD_ARG;     // whole complex points
+    // one launch per pass for the whole batch (grid z = wavefront) when the work buffers hold it
+    const size_t per = (size_t)plan->pl.maxElems;
+    int chunk = n;
+    const size_t budget = (size_t)1 << 30;                               // work elements (8 GiB)
+    while (chunk > 1 && 4 * (size_t)chunk * per > budget) chunk = (chunk + 1) / 2;
+    r = ensure_work(c, (size_t)chunk * per);
+    if (r) return r;
+    for (int b0 = 0; b0 < n; b0 += chunk) {
+        const int nb = std::min(chunk, n - b0);
+        r = execute(plan->pl, c, (const float2*)(dExIn + b0 * strideIn), (const float2*)(dEyIn + b0 * strideIn),
+                    (float2*)(dExOut + b0 * strideOut), (float2*)(dEyOut + b0 * strideOut), c.work, per, plan->dtab,
+                    st, nullptr, nb, strideIn / 2, strideOut / 2);
         if (r) return r;
     }
     return 0;

@@ -1,9 +1,30 @@
 // Host helpers shared by the entry points (capi.cpp, noalloc.cu).
 #pragma once
+#include <map>
+#include <mutex>
 #include <string>
 #include "kernels.h"
 
 namespace srwg {
+// per-device state of the library (capi.cpp)
+struct DeviceCtx {
+    int dev = 0;
+    std::map<int, float2*> tw;          // twiddle tables by FFT length
+    float2* work = nullptr;             // 2 work buffers x 2 components
+    size_t workElems = 0;               // per buffer per component
+    float2* io = nullptr;               // input + output staging for the host-memory entry point
+    size_t ioElems = 0;
+    float2* tab = nullptr;              // point-wise tables of the one-shot entry point
+    size_t tabElems = 0;
+    cudaStream_t stream = nullptr;
+};
+std::mutex& library_mutex();                          // serialises the entry points
+int device_ctx(int dev, DeviceCtx** out);             // makes `dev` current, returns its state
+int device_twiddles(DeviceCtx& c, int N, const float2** out);
+int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, const float2* inX, const float2* inY,
+                   long long inStride, float2* outX, float2* outY, long long outStride, float2* work, size_t workElems,
+                   const char* dconst, long long constStride, size_t descOff, cudaStream_t st, cudaEvent_t* ev,
+                   const std::vector<KernelDesc>* hostMax);
 int line_config(const LineDesc& d, LineLaunch& p);   // launch shape of a line pass (capi.cpp)
 int radix_plan(int N, int* r);
 void set_last_detail(const std::string& s);          // detail text for srwlUtiGetErrText

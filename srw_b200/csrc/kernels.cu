@@ -19,13 +19,13 @@ __global__ void __launch_bounds__(512, 1) line_kernel(const LineLaunch p)
     extern __shared__ float2 sm[];
     // descriptor in shared memory: point-wise code takes references to it (a reference to a
     // kernel parameter would force a copy of the whole parameter block to local memory)
-    const LineDesc& d = *p.gd;
+    const LineDesc& d = *reinterpret_cast<const LineDesc*>(reinterpret_cast<const char*>(p.gd) + blockIdx.z * p.bDesc);
     __shared__ int radix[SRWG_MAX_STAGES];
     if (threadIdx.x < SRWG_MAX_STAGES) radix[threadIdx.x] = p.radix[threadIdx.x];
     __syncthreads();
     const int comp = blockIdx.y;
-    const float2* __restrict__ src = p.src[comp];
-    float2* __restrict__ dst = p.dst[comp];
+    const float2* __restrict__ src = p.src[comp] + blockIdx.z * p.bSrc;
+    float2* __restrict__ dst = p.dst[comp] + blockIdx.z * p.bDst;
     const int N = p.N, T = p.T, L = p.L, P = p.P, nl = p.nlines;
     const int tid = threadIdx.x, nth = blockDim.x;
     const int G = nth / T;
@@ -273,7 +273,10 @@ __device__ __forceinline__ float2 resize_factor(const ResizeDesc& d, const float
 // most one old node apart, each stencil row is read once as three aligned float4 (6 complex).
 __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
 {
-    const ResizeDesc& d = *p.gd;       // device-memory descriptor (read-only, cached)
+    const ResizeDesc& d = *reinterpret_cast<const ResizeDesc*>(reinterpret_cast<const char*>(p.gd) + blockIdx.z * p.bDesc);
+    const float2* S[2] = {p.src[0] + blockIdx.z * p.bSrc, p.src[1] + blockIdx.z * p.bSrc};
+    float2* D[2] = {p.dst[0] + blockIdx.z * p.bDst, p.dst[1] + blockIdx.z * p.bDst};
+    const float2* tabs = p.tabs + blockIdx.z * p.bTab;
     const int ix0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int iz = blockIdx.y * blockDim.y + threadIdx.y;
     if (ix0 >= d.nxn || iz >= d.nzn) return;
@@ -283,14 +286,14 @@ __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
     const bool in0 = zin && (ix0 >= d.ixStart) && (ix0 <= d.ixEnd);
     const bool in1 = two && zin && (ix0 + 1 >= d.ixStart) && (ix0 + 1 <= d.ixEnd);
     if (in0 || in1) {
-        const ResizeAxis az = load_axis(p.tabs, d.axz, iz);
-        const ResizeAxis a0 = load_axis(p.tabs, d.axx, ix0);
-        const ResizeAxis a1 = two ? load_axis(p.tabs, d.axx, ix0 + 1) : a0;
+        const ResizeAxis az = load_axis(tabs, d.axz, iz);
+        const ResizeAxis a0 = load_axis(tabs, d.axx, ix0);
+        const ResizeAxis a1 = two ? load_axis(tabs, d.axx, ix0 + 1) : a0;
         if (d.only_larger) {
 #pragma unroll
             for (int c = 0; c < 2; c++) {
-                if (in0) out[0][c] = __ldg(&p.src[c][(size_t)az.st * d.nxo + a0.st]);
-                if (in1) out[1][c] = __ldg(&p.src[c][(size_t)az.st * d.nxo + a1.st]);
+                if (in0) out[0][c] = __ldg(&S[c][(size_t)az.st * d.nxo + a0.st]);
+                if (in1) out[1][c] = __ldg(&S[c][(size_t)az.st * d.nxo + a1.st]);
             }
         } else {
             float wz[4], wx0[4], wx1[4];
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
             if (vec) {
 #pragma unroll
                 for (int c = 0; c < 2; c++) {
-                    const float2* __restrict__ o = p.src[c] + (size_t)az.st * d.nxo + base;
+                    const float2* __restrict__ o = S[c] + (size_t)az.st * d.nxo + base;
                     float2 f0[4][4], f1[4][4];
 #pragma unroll
                     for (int dz = 0; dz < 4; dz++) {
@@ -324,21 +327,21 @@ __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
 #pragma unroll
                 for (int c = 0; c < 2; c++) {
                     const ResizeDesc* pre = d.has_pre ? &d : nullptr;
-                    if (in0) out[0][c] = resize_point(p.src[c] + (size_t)az.st * d.nxo + a0.st, d.nxo, wx0, wz, a0.rel,
-                                                      az.rel, a0.ir, az.ir, pre, p.tabs, a0.st, az.st);
-                    if (in1) out[1][c] = resize_point(p.src[c] + (size_t)az.st * d.nxo + a1.st, d.nxo, wx1, wz, a1.rel,
-                                                      az.rel, a1.ir, az.ir, pre, p.tabs, a1.st, az.st);
+                    if (in0) out[0][c] = resize_point(S[c] + (size_t)az.st * d.nxo + a0.st, d.nxo, wx0, wz, a0.rel,
+                                                      az.rel, a0.ir, az.ir, pre, tabs, a0.st, az.st);
+                    if (in1) out[1][c] = resize_point(S[c] + (size_t)az.st * d.nxo + a1.st, d.nxo, wx1, wz, a1.rel,
+                                                      az.rel, a1.ir, az.ir, pre, tabs, a1.st, az.st);
                 }
             }
         }
         if (d.has_pw) {
             if (in0) {
-                float2 e = resize_factor(d, p.tabs, ix0, iz);
+                float2 e = resize_factor(d, tabs, ix0, iz);
                 out[0][0] = cmul(out[0][0], e);
                 out[0][1] = cmul(out[0][1], e);
             }
             if (in1) {
-                float2 e = resize_factor(d, p.tabs, ix0 + 1, iz);
+                float2 e = resize_factor(d, tabs, ix0 + 1, iz);
                 out[1][0] = cmul(out[1][0], e);
                 out[1][1] = cmul(out[1][1], e);
             }
@@ -348,10 +351,10 @@ __global__ void __launch_bounds__(256) resize_kernel(const ResizeLaunch p)
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         if (p.vec_ok && two && ((o & 1) == 0)) {
-            __stcs(reinterpret_cast<float4*>(p.dst[c] + o), make_float4(out[0][c].x, out[0][c].y, out[1][c].x, out[1][c].y));
+            __stcs(reinterpret_cast<float4*>(D[c] + o), make_float4(out[0][c].x, out[0][c].y, out[1][c].x, out[1][c].y));
         } else {
-            __stcs(&p.dst[c][o], out[0][c]);
-            if (two) __stcs(&p.dst[c][o + 1], out[1][c]);
+            __stcs(&D[c][o], out[0][c]);
+            if (two) __stcs(&D[c][o + 1], out[1][c]);
         }
     }
 }
@@ -376,7 +379,10 @@ __device__ __forceinline__ float2 pre_factor(const ResizeDesc& d, const float2* 
 // results.  Points outside the window are written as zeros.
 __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
 {
-    const ResizeDesc& d = *p.gd;
+    const ResizeDesc& d = *reinterpret_cast<const ResizeDesc*>(reinterpret_cast<const char*>(p.gd) + blockIdx.z * p.bDesc);
+    const float2* S[2] = {p.src[0] + blockIdx.z * p.bSrc, p.src[1] + blockIdx.z * p.bSrc};
+    float2* D[2] = {p.dst[0] + blockIdx.z * p.bDst, p.dst[1] + blockIdx.z * p.bDst};
+    const float2* tabs = p.tabs + blockIdx.z * p.bTab;
     constexpr int TX = SRWG_RESIZE_TX, TZ = SRWG_RESIZE_TZ;
     extern __shared__ float4 rsm[];
     const int OR = d.tile_or, OC = d.tile_oc;
@@ -397,8 +403,8 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
             const int gi = x0 + (e & (TX - 1)), gj = z0 + e / TX;
             if (gi < d.nxn && gj < d.nzn) {
                 const size_t o = (size_t)gj * d.nxn + gi;
-                __stcs(&p.dst[0][o], make_float2(0.f, 0.f));
-                __stcs(&p.dst[1][o], make_float2(0.f, 0.f));
+                __stcs(&D[0][o], make_float2(0.f, 0.f));
+                __stcs(&D[1][o], make_float2(0.f, 0.f));
             }
         }
         return;
@@ -408,7 +414,7 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
     if (tid < TX) {
         const int i = x0 + tid;
         if (i >= xa && i <= xb) {
-            const ResizeAxis a = load_axis(p.tabs, d.axx, i);
+            const ResizeAxis a = load_axis(tabs, d.axx, i);
             float w[4];
             lagrange4(a.rel, w);
             wxs[tid] = make_float4(w[0], w[1], w[2], w[3]);
@@ -419,7 +425,7 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
     } else if (tid >= 128 && tid < 128 + TZ) {
         const int j = z0 + tid - 128;
         if (j >= za && j <= zb) {
-            const ResizeAxis a = load_axis(p.tabs, d.axz, j);
+            const ResizeAxis a = load_axis(tabs, d.axz, j);
             float w[4];
             lagrange4(a.rel, w);
             wzs[tid - 128] = make_float4(w[0], w[1], w[2], w[3]);
@@ -436,9 +442,9 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
         const int r = e / nc, c = e - r * nc;
         const int gx = ox0 + c, gz = oz0 + r;
         const size_t go = (size_t)gz * d.nxo + gx;
-        float2 v0 = __ldg(&p.src[0][go]), v1 = __ldg(&p.src[1][go]);
+        float2 v0 = __ldg(&S[0][go]), v1 = __ldg(&S[1][go]);
         if (d.has_pre) {
-            const float2 f = pre_factor(d, p.tabs, gx, gz);
+            const float2 f = pre_factor(d, tabs, gx, gz);
             v0 = cmul(f, v0);
             v1 = cmul(f, v1);
         }
@@ -518,14 +524,14 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
                 out[comp] = F;
             }
             if (d.has_pw) {
-                const float2 f = resize_factor(d, p.tabs, gi, gj);
+                const float2 f = resize_factor(d, tabs, gi, gj);
                 out[0] = cmul(out[0], f);
                 out[1] = cmul(out[1], f);
             }
         }
         const size_t o = (size_t)gj * d.nxn + gi;
-        __stcs(&p.dst[0][o], out[0]);
-        __stcs(&p.dst[1][o], out[1]);
+        __stcs(&D[0][o], out[0]);
+        __stcs(&D[1][o], out[1]);
     }
 }
 
@@ -534,13 +540,16 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
 // ------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) pw_kernel(const PwLaunch p)
 {
-    const PwDesc& d = *p.gd;
+    const PwDesc& d = *reinterpret_cast<const PwDesc*>(reinterpret_cast<const char*>(p.gd) + blockIdx.z * p.bDesc);
+    const float2* S[2] = {p.src[0] + blockIdx.z * p.bSrc, p.src[1] + blockIdx.z * p.bSrc};
+    float2* D[2] = {p.dst[0] + blockIdx.z * p.bDst, p.dst[1] + blockIdx.z * p.bDst};
+    const float2* tabs = p.tabs + blockIdx.z * p.bTab;
     const int ix = blockIdx.x * blockDim.x + threadIdx.x;
     const int iz = blockIdx.y;
     if (ix >= d.nx) return;
     float2 e = make_float2(1.f, 0.f);
-    if (d.t.tab >= 0) e = __ldg(&p.tabs[d.t.tab + ix]);
-    if (d.t.ltab >= 0) e = cmul(e, __ldg(&p.tabs[d.t.ltab + iz]));
+    if (d.t.tab >= 0) e = __ldg(&tabs[d.t.tab + ix]);
+    if (d.t.ltab >= 0) e = cmul(e, __ldg(&tabs[d.t.ltab + iz]));
     bool zero = false;
     if (d.has_extra) extra_eval(d.extra, ix, iz, e, zero);
     if (zero) e = make_float2(0.f, 0.f);
@@ -548,7 +557,7 @@ __global__ void __launch_bounds__(256) pw_kernel(const PwLaunch p)
     const int oz = d.mirror_z ? d.nz - 1 - iz : iz;
     const size_t i = (size_t)iz * d.nx + ix, o = (size_t)oz * d.nx + ox;
 #pragma unroll
-    for (int c = 0; c < 2; c++) __stcs(&p.dst[c][o], cmul(e, __ldcs(&p.src[c][i])));
+    for (int c = 0; c < 2; c++) __stcs(&D[c][o], cmul(e, __ldcs(&S[c][i])));
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -572,7 +581,7 @@ Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra)
 
 cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
 {
-    dim3 grid((p.nlines + p.L - 1) / p.L, 2);
+    dim3 grid((p.nlines + p.L - 1) / p.L, 2, p.nb > 1 ? p.nb : 1);
     size_t smem = (size_t)p.L * p.P * sizeof(float2);
     if (smem > SRWG_LINE_SMEM_MAX) return cudaErrorInvalidValue;
     static int attr_set = 0;
@@ -599,7 +608,7 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
 cudaError_t launch_resize(const ResizeLaunch& q, cudaStream_t st)
 {
     ResizeLaunch p = q;
-    p.vec_ok = ((q.d.nxo & 1) == 0) && ((q.d.nxn & 1) == 0);
+    p.vec_ok = ((q.d.nxo & 1) == 0) && ((q.d.nxn & 1) == 0) && ((q.bSrc & 1) == 0) && ((q.bDst & 1) == 0);
     for (int c = 0; c < 2; c++)
         p.vec_ok = p.vec_ok && ((((uintptr_t)q.src[c]) & 15) == 0) && ((((uintptr_t)q.dst[c]) & 15) == 0);
     if (p.d.tile_or > 0 && p.d.tile_oc > 0 && p.d.tile_or <= SRWG_RESIZE_OR_MAX && p.d.tile_oc <= SRWG_RESIZE_OC_MAX) {
@@ -611,13 +620,14 @@ cudaError_t launch_resize(const ResizeLaunch& q, cudaStream_t st)
             cudaFuncSetAttribute(resize2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
             attr = 1;
         }
-        dim3 grid((p.d.nxn + SRWG_RESIZE_TX - 1) / SRWG_RESIZE_TX, (p.d.nzn + SRWG_RESIZE_TZ - 1) / SRWG_RESIZE_TZ);
+        dim3 grid((p.d.nxn + SRWG_RESIZE_TX - 1) / SRWG_RESIZE_TX, (p.d.nzn + SRWG_RESIZE_TZ - 1) / SRWG_RESIZE_TZ,
+                  p.nb > 1 ? p.nb : 1);
         resize2_kernel<<<grid, 256, smem, st>>>(p);
         return cudaGetLastError();
     }
     dim3 blk(64, 4);
     const int nxh = (p.d.nxn + 1) / 2;
-    dim3 grid((nxh + blk.x - 1) / blk.x, (p.d.nzn + blk.y - 1) / blk.y);
+    dim3 grid((nxh + blk.x - 1) / blk.x, (p.d.nzn + blk.y - 1) / blk.y, p.nb > 1 ? p.nb : 1);
     resize_kernel<<<grid, blk, 0, st>>>(p);
     return cudaGetLastError();
 }
@@ -625,7 +635,7 @@ cudaError_t launch_resize(const ResizeLaunch& q, cudaStream_t st)
 cudaError_t launch_pw(const PwLaunch& p, cudaStream_t st)
 {
     dim3 blk(256);
-    dim3 grid((p.d.nx + 255) / 256, p.d.nz);
+    dim3 grid((p.d.nx + 255) / 256, p.d.nz, p.nb > 1 ? p.nb : 1);
     pw_kernel<<<grid, blk, 0, st>>>(p);
     return cudaGetLastError();
 }

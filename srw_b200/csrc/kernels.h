@@ -33,6 +33,9 @@ struct LineLaunch {
     int v2;                  // power-of-two line pass (line2_kernel)
     const float2* tabs;      // the plan's separable point-wise tables
     const LineDesc* gd;      // this pass's descriptor in device memory
+    int nb;                  // wavefronts in the launch (grid z; 0 or 1: one)
+    long long bDesc, bTab;   // per wavefront: descriptor stride (bytes), table stride (float2)
+    long long bSrc, bDst;    // per wavefront: source / destination field stride (float2)
 };
 
 // tiled resize: a CTA makes TZ x TX new points from an old tile of at most OR_MAX x OC_MAX points
@@ -49,6 +52,9 @@ struct ResizeLaunch {
     const ResizeDesc* gd;
     int vec_ok;              // even row lengths and 16-byte aligned buffers: float4 paths allowed
     double xStepInvO, zStepInvO;
+    int nb;                  // wavefronts in the launch (grid z; 0 or 1: one)
+    long long bDesc, bTab;   // per wavefront: descriptor stride (bytes), table stride (float2)
+    long long bSrc, bDst;    // per wavefront: source / destination field stride (float2)
 };
 
 struct PwLaunch {
@@ -57,6 +63,9 @@ struct PwLaunch {
     float2* dst[2];
     const float2* tabs;
     const PwDesc* gd;
+    int nb;                  // wavefronts in the launch (grid z; 0 or 1: one)
+    long long bDesc, bTab;   // per wavefront: descriptor stride (bytes), table stride (float2)
+    long long bSrc, bDst;    // per wavefront: source / destination field stride (float2)
 };
 
 cudaError_t launch_line(const LineLaunch& p, cudaStream_t st);

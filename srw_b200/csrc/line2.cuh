@@ -142,10 +142,11 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     constexpr int N = 1 << LOGN;
     constexpr int T = N / 16;
     extern __shared__ float2 sm[];
-    const LineDesc& d = *p.gd;         // device-memory descriptor (read-only, cached)
+    // device-memory descriptor (read-only, cached); blockIdx.z = wavefront of a batched launch
+    const LineDesc& d = *reinterpret_cast<const LineDesc*>(reinterpret_cast<const char*>(p.gd) + blockIdx.z * p.bDesc);
     const int comp = blockIdx.y;
-    const float2* __restrict__ src = p.src[comp];
-    float2* __restrict__ dst = p.dst[comp];
+    const float2* __restrict__ src = p.src[comp] + blockIdx.z * p.bSrc;
+    float2* __restrict__ dst = p.dst[comp] + blockIdx.z * p.bDst;
     const int L = p.L, P = p.P, nl = p.nlines;
     const int tid = threadIdx.x;
     const int g = COLS ? (tid % L) : (tid / T);          // line of the tile
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
         if (line < d.zl0 || line > d.zl1) { za0 = 1; za1 = 0; }
         else { za0 = d.za0; za1 = d.za1; }
     }
-    const float2* tabs = p.tabs;
+    const float2* tabs = p.tabs + blockIdx.z * p.bTab;
     const PwOps* ex = &d.extra;
     const int axis = d.axis;
     Chain2 pre = make_chain2(d.t_pre, 0, 0, d.f1_pre.rs, 0, N);

@@ -1,0 +1,491 @@
+// Partially coherent (multi-electron) propagation in batches.
+//
+// The reference averages the intensity of many macro-electron wavefronts in a Python loop
+// (srwl_wfr_emit_prop_multi_e, env/python/srwpy/srwlib.py:8506): per electron a field, then
+// srwlPropagElecField, srwlCalcIntFromElecField (total polarisation, intensity vs x and y) and
+// avg_update_interp (srwlib.py:1116) onto a common mesh.  Here the electrons' wavefronts are made
+// on the device from one base field by the source offset of SRWLWfr.sim_src_offset with
+// _move_mesh=True (srwlib.py:2803): the angular kick of srTOptAngle (cpp/src/core/sroptang.h:64,
+// phase 5.06773065e6 * e * (x' x + y' y) on the unshifted mesh) followed by a shift of the mesh by
+// (x + x' R, y + y' R), R = (Rx + Ry)/2, and xc += x, yc += y.  Each electron is planned on the host
+// (its own mesh, exact bookkeeping); electrons whose passes have the same kinds and sizes run
+// together: every pass is ONE launch over the batch (grid z = electron, per-electron descriptors
+// and tables), then one kernel adds the batch's intensities, interpolated bilinearly onto the
+// common mesh as avg_update_interp does with order 1, to an FP64 accumulator on the device.
+// With `graph` set, the launch sequence of a full batch is captured once as a CUDA graph and
+// replayed (only the descriptor and parameter uploads change between batches).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/srwl_b200.h"
+#include "common.cuh"
+#include "errors.h"
+#include "exec.h"
+#include "kernels.h"
+#include "planner.h"
+
+namespace srwg {
+
+// per-electron parameters in device memory
+struct ElecParams {
+    double kx, kz;                       // kick: phase = kx * x + kz * z on the base mesh
+    double oxStart, oxStep, ozStart, ozStep;   // output mesh (steps as (Fin - Start)/(n - 1))
+    int onx, onz;
+    int pad[2];
+};
+
+// kicked copies of the base field for the electrons of a batch (grid z = electron)
+__global__ void __launch_bounds__(256) kick_kernel(const float2* __restrict__ bx, const float2* __restrict__ by,
+                                                   float2* __restrict__ ox, float2* __restrict__ oy, long long stride,
+                                                   int nx, int nz, double xStart, double xStep, double zStart,
+                                                   double zStep, const ElecParams* __restrict__ ep)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= nx) return;
+    const ElecParams& e = ep[blockIdx.z];
+    const double x = xStart + (double)i * xStep, z = zStart + (double)j * zStep;
+    const float2 f = expi(e.kx * x + e.kz * z);
+    const size_t o = (size_t)j * nx + i;
+    const size_t ob = (size_t)blockIdx.z * stride + o;
+    ox[ob] = cmul(f, __ldg(&bx[o]));
+    oy[ob] = cmul(f, __ldg(&by[o]));
+}
+
+// acc[p] += sum over the batch of the bilinearly interpolated total intensity at common-mesh
+// point p (avg_update_interp, order 1: points outside an electron's mesh add nothing)
+__global__ void __launch_bounds__(256) accum_kernel(const float2* __restrict__ ex, const float2* __restrict__ ey,
+                                                    long long stride, int nb, const ElecParams* __restrict__ ep,
+                                                    double* __restrict__ acc, int anx, int anz, double axStart,
+                                                    double axStep, double azStart, double azStep)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= anx) return;
+    const double x = axStart + (double)i * axStep, y = azStart + (double)j * azStep;
+    double sum = 0.;
+    for (int b = 0; b < nb; b++) {
+        const ElecParams& e = ep[b];
+        const int ix0 = (int)trunc((x - e.oxStart) / e.oxStep + 1.e-09);
+        if (ix0 < 0 || ix0 >= e.onx - 1) continue;
+        const int iy0 = (int)trunc((y - e.ozStart) / e.ozStep + 1.e-09);
+        if (iy0 < 0 || iy0 >= e.onz - 1) continue;
+        const double tx = (x - (e.oxStart + e.oxStep * ix0)) / e.oxStep;
+        const double ty = (y - (e.ozStart + e.ozStep * iy0)) / e.ozStep;
+        const float2* px = ex + (size_t)b * stride + (size_t)iy0 * e.onx + ix0;
+        const float2* py = ey + (size_t)b * stride + (size_t)iy0 * e.onx + ix0;
+        float I[4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const size_t o = (c >> 1) * (size_t)e.onx + (c & 1);
+            const float2 u = __ldg(&px[o]), v = __ldg(&py[o]);
+            I[c] = u.x * u.x + u.y * u.y + v.x * v.x + v.y * v.y;     // total intensity (FP32, as the reference)
+        }
+        const double a00 = I[0], f10 = I[1], f01 = I[2], f11 = I[3];
+        const double a10 = f10 - a00, a01 = f01 - a00, a11 = a00 - f01 - f10 + f11;
+        sum += a00 + tx * (a10 + ty * a11) + ty * a01;
+    }
+    acc[(size_t)j * anx + i] += sum;
+}
+
+}  // namespace srwg
+
+using namespace srwg;
+
+struct srwgMultiE {
+    int device = 0;
+    DeviceCtx* ctx = nullptr;
+    // base wavefront (host copy of its description; field on the device)
+    SRWLWfr base;
+    std::vector<double> momX, momY;
+    const SRWLOptC* opt = nullptr;       // caller-owned beamline
+    int nx = 0, nz = 0;
+    double xStart = 0, xStep = 0, zStart = 0, zStep = 0, eStart = 0;
+    float2* dBase = nullptr;             // [2][nIn]
+    // common mesh and FP64 accumulator
+    int anx = 0, anz = 0;
+    double axStart = 0, axStep = 0, azStart = 0, azStep = 0;
+    double* dAcc = nullptr;
+    bool ownAcc = true;                  // false: caller-provided accumulator (srwgMultiESetAccumulator)
+    long long nAdded = 0;
+    // batch buffers
+    int maxBatch = 0;
+    size_t nIn = 0, nOut = 0, perWork = 0, constStride = 0, descOff = 0;
+    float2* dIn = nullptr;               // [2][B][nIn]
+    float2* dOut = nullptr;              // [2][B][nOut]
+    float2* dWork = nullptr;             // [4][B][perWork]
+    char* dConst = nullptr;              // [B][constStride]
+    ElecParams* dParams = nullptr;       // [B]
+    char* hConst[2] = {nullptr, nullptr};          // pinned staging, two slots used in turn
+    ElecParams* hParams[2] = {nullptr, nullptr};
+    cudaEvent_t staged[2] = {nullptr, nullptr};    // the slot's upload has completed
+    int slot = 0;
+    bool useGraph = false;
+    cudaGraphExec_t graph = nullptr;
+    int graphNb = 0;
+    std::vector<KernelDesc> graphKs;     // host copy (launch shapes) the graph was captured with
+    ~srwgMultiE()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (ownAcc) cudaFree(dAcc);
+        cudaFree(dBase); cudaFree(dIn); cudaFree(dOut); cudaFree(dWork); cudaFree(dConst);
+        cudaFree(dParams);
+        for (int i = 0; i < 2; i++) {
+            cudaFreeHost(hConst[i]);
+            cudaFreeHost(hParams[i]);
+            if (staged[i]) cudaEventDestroy(staged[i]);
+        }
+    }
+};
+
+namespace srwg {
+
+#define MTRY(x)                                                                          \
+    do {                                                                                 \
+        cudaError_t e__ = (x);                                                           \
+        if (e__ != cudaSuccess) {                                                        \
+            set_last_detail(std::string(#x) + ": " + cudaGetErrorString(e__));           \
+            return SRWG_ERR_CUDA;                                                        \
+        }                                                                                \
+    } while (0)
+
+// the electron's wavefront description: kicked on the base mesh, then the mesh moved
+// (SRWLWfr.sim_src_offset with _move_mesh=True, srwlib.py:2803-2849; srTOptAngle moments, sroptang.h:81)
+static void electron_wfr(const srwgMultiE& m, const double* off, SRWLWfr& w, double* momX, double* momY,
+                         ElecParams& ep)
+{
+    const double dx0 = off[0], dxp = off[1], dy0 = off[2], dyp = off[3];
+    w = m.base;
+    for (int i = 0; i < 11; i++) { momX[i] = m.momX[i]; momY[i] = m.momY[i]; }
+    w.arMomX = momX;
+    w.arMomY = momY;
+    const double twoPiDLambda = 5.06773065e+06 * m.eStart;
+    ep.kx = twoPiDLambda * dxp;
+    ep.kz = twoPiDLambda * dyp;
+    momX[1] += dxp; momX[3] += dyp; momY[1] += dxp; momY[3] += dyp;     // srTOptAngle::PropagateRadMoments
+    const double R = 0.5 * (w.Rx + w.Ry);
+    const double dx = dx0 + dxp * R, dy = dy0 + dyp * R;
+    w.mesh.xStart += dx; w.mesh.xFin += dx;
+    w.mesh.yStart += dy; w.mesh.yFin += dy;
+    w.xc += dx0; w.yc += dy0;
+    momX[0] += dx; momX[1] += dxp; momX[2] += dy; momX[3] += dyp;
+    momY[0] += dx; momY[1] += dxp; momY[2] += dy; momY[3] += dyp;
+}
+
+// passes of the same kinds, sizes, buffers and launch-relevant flags
+static bool same_structure(const std::vector<KernelDesc>& a, const std::vector<KernelDesc>& b)
+{
+    if (a.size() != b.size()) return false;
+    for (size_t i = 0; i < a.size(); i++) {
+        const KernelDesc &x = a[i], &y = b[i];
+        if (x.kind != y.kind || x.src != y.src || x.dst != y.dst) return false;
+        if (x.kind == K_LINE) {
+            const LineDesc &p = x.line, &q = y.line;
+            if (p.axis != q.axis || p.nx != q.nx || p.nz != q.nz || p.f1 != q.f1 || p.f2 != q.f2 ||
+                p.has_extra != q.has_extra || p.zwin != q.zwin || p.blk_in != q.blk_in || p.blk_out != q.blk_out)
+                return false;
+        } else if (x.kind == K_RESIZE) {
+            const ResizeDesc &p = x.rs, &q = y.rs;
+            if (p.nxo != q.nxo || p.nzo != q.nzo || p.nxn != q.nxn || p.nzn != q.nzn || p.only_larger != q.only_larger ||
+                (p.tile_or > 0) != (q.tile_or > 0) || p.skip_zero != q.skip_zero)
+                return false;
+        } else {
+            if (x.pwk.nx != y.pwk.nx || x.pwk.nz != y.pwk.nz) return false;
+        }
+    }
+    return true;
+}
+
+// runs one batch: kick -> passes -> accumulation; ks = launch shapes (largest resize tiles of the batch)
+static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, cudaStream_t st)
+{
+    dim3 blk(256);
+    dim3 gk((m.nx + 255) / 256, m.nz, nb);
+    kick_kernel<<<gk, blk, 0, st>>>(m.dBase, m.dBase + m.nIn, m.dIn, m.dIn + (size_t)m.maxBatch * m.nIn,
+                                    (long long)m.nIn, m.nx, m.nz, m.xStart, m.xStep, m.zStart, m.zStep, m.dParams);
+    MTRY(cudaGetLastError());
+    float2* outX = m.dOut;
+    float2* outY = m.dOut + (size_t)m.maxBatch * m.nOut;
+    if (ks.empty()) {
+        for (int b = 0; b < nb; b++) {
+            MTRY(cudaMemcpyAsync(outX + b * m.nOut, m.dIn + b * m.nIn, m.nIn * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+            MTRY(cudaMemcpyAsync(outY + b * m.nOut, m.dIn + (size_t)m.maxBatch * m.nIn + b * m.nIn, m.nIn * sizeof(float2),
+                                 cudaMemcpyDeviceToDevice, st));
+        }
+    } else {
+        int r = execute_passes(ks, *m.ctx, nb, m.dIn, m.dIn + (size_t)m.maxBatch * m.nIn, (long long)m.nIn, outX, outY,
+                               (long long)m.nOut, m.dWork, m.perWork, m.dConst, (long long)m.constStride, m.descOff, st,
+                               nullptr, &ks);
+        if (r) return r;
+    }
+    dim3 ga((m.anx + 255) / 256, m.anz);
+    accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams, m.dAcc, m.anx, m.anz, m.axStart,
+                                     m.axStep, m.azStart, m.azStep);
+    MTRY(cudaGetLastError());
+    return 0;
+}
+
+// uploads the staged constants of nb electrons and runs (or replays) the batch
+static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_t st)
+{
+    if (nb == 0) return 0;
+    MTRY(cudaMemcpyAsync(m.dConst, m.hConst[m.slot], (size_t)nb * m.constStride, cudaMemcpyHostToDevice, st));
+    MTRY(cudaMemcpyAsync(m.dParams, m.hParams[m.slot], (size_t)nb * sizeof(ElecParams), cudaMemcpyHostToDevice, st));
+    MTRY(cudaEventRecord(m.staged[m.slot], st));
+    m.slot ^= 1;
+    // the next batch is staged in the other slot once that slot's previous upload has completed
+    MTRY(cudaEventSynchronize(m.staged[m.slot]));
+    int r = 0;
+    if (m.useGraph && nb == m.maxBatch) {
+        // the graph holds the launch shapes; a batch whose resize tiles are larger needs a new one
+        bool fits = m.graph != nullptr && m.graphKs.size() == ks.size();
+        for (size_t i = 0; fits && i < ks.size(); i++)
+            if (ks[i].kind == K_RESIZE && (ks[i].rs.tile_or > m.graphKs[i].rs.tile_or || ks[i].rs.tile_oc > m.graphKs[i].rs.tile_oc))
+                fits = false;
+        if (!fits) {
+            if (m.graph) { cudaGraphExecDestroy(m.graph); m.graph = nullptr; }
+            std::vector<KernelDesc> cap = ks;
+            for (size_t i = 0; i < cap.size(); i++)
+                if (cap[i].kind == K_RESIZE && cap[i].rs.tile_or > 0) {     // headroom for other batches
+                    cap[i].rs.tile_or = std::min(SRWG_RESIZE_OR_MAX, cap[i].rs.tile_or + 2);
+                    cap[i].rs.tile_oc = std::min(SRWG_RESIZE_OC_MAX, cap[i].rs.tile_oc + 2);
+                }
+            // this batch runs directly (which also creates every lazily made resource -- twiddle
+            // tables, kernel attributes -- before the capture); the capture only records the launches
+            r = run_batch(m, nb, cap, st);
+            if (r) return r;
+            cudaGraph_t g;
+            MTRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            r = run_batch(m, nb, cap, st);
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (r) return r;
+            MTRY(e);
+            MTRY(cudaGraphInstantiate(&m.graph, g, 0));
+            cudaGraphDestroy(g);
+            m.graphKs = cap;
+            m.nAdded += nb;
+            return 0;
+        }
+        MTRY(cudaGraphLaunch(m.graph, st));
+    } else {
+        r = run_batch(m, nb, ks, st);
+        if (r) return r;
+    }
+    m.nAdded += nb;
+    return 0;
+}
+
+}  // namespace srwg
+
+extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* pOpt, const SRWLRadMesh* pAccMesh,
+                                         int maxBatch, int useGraph, int device, srwgMultiE** out)
+{
+    std::lock_guard<std::mutex> lk(library_mutex());
+    set_last_detail("");
+    if (!pBase || !pOpt || !pAccMesh || !out || maxBatch < 1 || !pBase->arEx || !pBase->arEy) return SRWG_ERR_BAD_ARG;
+    if (pBase->mesh.ne != 1 || pBase->mesh.nx < 2 || pBase->mesh.ny < 2 || pAccMesh->nx < 2 || pAccMesh->ny < 2)
+        return SRWG_ERR_BAD_ARG;
+    srwgMultiE* m = new srwgMultiE();
+    DeviceCtx* c = nullptr;
+    int r = device_ctx(device, &c);
+    if (r) { delete m; return r; }
+    m->device = device;
+    m->ctx = c;
+    m->base = *pBase;
+    m->momX.assign(11, 0.);
+    m->momY.assign(11, 0.);
+    if (pBase->arMomX) for (int i = 0; i < 11; i++) m->momX[i] = pBase->arMomX[i];
+    if (pBase->arMomY) for (int i = 0; i < 11; i++) m->momY[i] = pBase->arMomY[i];
+    m->opt = pOpt;
+    m->nx = (int)pBase->mesh.nx;
+    m->nz = (int)pBase->mesh.ny;
+    m->xStart = pBase->mesh.xStart;
+    m->xStep = (pBase->mesh.xFin - pBase->mesh.xStart) / (m->nx - 1);
+    m->zStart = pBase->mesh.yStart;
+    m->zStep = (pBase->mesh.yFin - pBase->mesh.yStart) / (m->nz - 1);
+    m->eStart = pBase->mesh.eStart;
+    m->anx = (int)pAccMesh->nx;
+    m->anz = (int)pAccMesh->ny;
+    m->axStart = pAccMesh->xStart;
+    m->axStep = (pAccMesh->xFin - pAccMesh->xStart) / (m->anx - 1);
+    m->azStart = pAccMesh->yStart;
+    m->azStep = (pAccMesh->yFin - pAccMesh->yStart) / (m->anz - 1);
+    m->maxBatch = maxBatch;
+    m->useGraph = useGraph != 0;
+    // sizes from the unshifted electron's plan
+    Planner pl;
+    r = pl.plan(pBase, pOpt);
+    if (r) { set_last_detail(pl.err); delete m; return r; }
+    m->nIn = (size_t)m->nx * m->nz;
+    m->nOut = (size_t)pl.w.nx * pl.w.nz;
+    m->perWork = (size_t)std::max<long long>(pl.maxElems, 1);
+    const size_t tabBytes = ((pl.tables.size() * sizeof(float2) + 255) & ~(size_t)255) + 4096;   // slack for alignment pads
+    m->descOff = tabBytes;
+    m->constStride = (tabBytes + pl.kernels.size() * sizeof(KernelDesc) + 255) & ~(size_t)255;
+#define MALLOC(p, n)                                                                 \
+    do {                                                                             \
+        cudaError_t e__ = cudaMalloc(&(p), (n));                                     \
+        if (e__ != cudaSuccess) {                                                    \
+            set_last_detail(std::string("cudaMalloc: ") + cudaGetErrorString(e__));  \
+            delete m;                                                                \
+            return MEMORY_ALLOCATION_FAILURE;                                        \
+        }                                                                            \
+    } while (0)
+    const size_t B = (size_t)maxBatch;
+    MALLOC(m->dBase, 2 * m->nIn * sizeof(float2));
+    MALLOC(m->dIn, 2 * B * m->nIn * sizeof(float2));
+    MALLOC(m->dOut, 2 * B * m->nOut * sizeof(float2));
+    MALLOC(m->dWork, 4 * B * m->perWork * sizeof(float2));
+    MALLOC(m->dConst, B * m->constStride);
+    MALLOC(m->dParams, B * sizeof(ElecParams));
+    MALLOC(m->dAcc, (size_t)m->anx * m->anz * sizeof(double));
+#undef MALLOC
+    for (int i = 0; i < 2; i++) {
+        if (cudaMallocHost(&m->hConst[i], B * m->constStride) != cudaSuccess ||
+            cudaMallocHost(&m->hParams[i], B * sizeof(ElecParams)) != cudaSuccess ||
+            cudaEventCreateWithFlags(&m->staged[i], cudaEventDisableTiming) != cudaSuccess) {
+            set_last_detail("pinned staging buffers could not be allocated");
+            delete m;
+            return MEMORY_ALLOCATION_FAILURE;
+        }
+        cudaEventRecord(m->staged[i], 0);
+    }
+    if (cudaMemcpy(m->dBase, pBase->arEx, m->nIn * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(m->dBase + m->nIn, pBase->arEy, m->nIn * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(m->dAcc, 0, (size_t)m->anx * m->anz * sizeof(double)) != cudaSuccess) {
+        set_last_detail("base field upload failed");
+        delete m;
+        return SRWG_ERR_CUDA;
+    }
+    m->base.arEx = nullptr;           // the host arrays are not kept
+    m->base.arEy = nullptr;
+    *out = m;
+    return 0;
+}
+
+extern "C" SRWG_API int srwgMultiEAdd(srwgMultiE* m, int n, const double* arOffsets, void* stream)
+{
+    std::lock_guard<std::mutex> lk(library_mutex());
+    set_last_detail("");
+    if (!m || n < 0 || (n > 0 && !arOffsets)) return SRWG_ERR_BAD_ARG;
+    DeviceCtx* c = nullptr;
+    int r = device_ctx(m->device, &c);
+    if (r) return r;
+    // the library's own stream when none is given (stream capture needs a non-default stream)
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    std::vector<KernelDesc> first, launchKs;
+    int nb = 0;
+    double momX[11], momY[11];
+    for (int e = 0; e < n; e++) {
+        SRWLWfr w;
+        ElecParams ep;
+        memset(&ep, 0, sizeof(ep));
+        electron_wfr(*m, arOffsets + 4 * (size_t)e, w, momX, momY, ep);
+        Planner pl;
+        r = pl.plan(&w, m->opt);
+        if (r) { set_last_detail(pl.err); return r; }
+        const size_t tb = pl.tables.size() * sizeof(float2);
+        if ((size_t)pl.w.nx * pl.w.nz != m->nOut || (size_t)pl.maxElems > m->perWork || tb > m->descOff ||
+            m->descOff + pl.kernels.size() * sizeof(KernelDesc) > m->constStride) {
+            set_last_detail("electron " + std::to_string(e) + ": its passes differ in size from the base wavefront's");
+            return SRWG_ERR_UNSUPPORTED;
+        }
+        if (nb > 0 && (!same_structure(first, pl.kernels) || nb == m->maxBatch)) {
+            r = flush(*m, nb, launchKs, st);
+            if (r) return r;
+            nb = 0;
+        }
+        if (nb == 0) { first = pl.kernels; launchKs = pl.kernels; }
+        for (size_t i = 0; i < launchKs.size(); i++)
+            if (launchKs[i].kind == K_RESIZE) {
+                launchKs[i].rs.tile_or = std::max(launchKs[i].rs.tile_or, pl.kernels[i].rs.tile_or);
+                launchKs[i].rs.tile_oc = std::max(launchKs[i].rs.tile_oc, pl.kernels[i].rs.tile_oc);
+            }
+        char* blk = m->hConst[m->slot] + (size_t)nb * m->constStride;
+        memcpy(blk, pl.tables.data(), tb);
+        memcpy(blk + m->descOff, pl.kernels.data(), pl.kernels.size() * sizeof(KernelDesc));
+        // output mesh as the reference's SRWLWfr holds it, step re-derived from (Fin - Start)/(n - 1)
+        const double xFin = pl.w.xStart + pl.w.xStep * (pl.w.nx - 1);
+        const double zFin = pl.w.zStart + pl.w.zStep * (pl.w.nz - 1);
+        ep.oxStart = pl.w.xStart;
+        ep.oxStep = (xFin - pl.w.xStart) / (pl.w.nx - 1);
+        ep.ozStart = pl.w.zStart;
+        ep.ozStep = (zFin - pl.w.zStart) / (pl.w.nz - 1);
+        ep.onx = pl.w.nx;
+        ep.onz = pl.w.nz;
+        m->hParams[m->slot][nb] = ep;
+        nb++;
+    }
+    r = flush(*m, nb, launchKs, st);
+    if (r) return r;
+    if (!stream) MTRY(cudaStreamSynchronize(st));
+    return 0;
+}
+
+extern "C" SRWG_API int srwgMultiEGetMean(srwgMultiE* m, double* arMean, long long* nElec, void* stream)
+{
+    std::lock_guard<std::mutex> lk(library_mutex());
+    if (!m) return SRWG_ERR_BAD_ARG;
+    if (nElec) *nElec = m->nAdded;
+    if (!arMean) return 0;
+    DeviceCtx* c = nullptr;
+    int r = device_ctx(m->device, &c);
+    if (r) return r;
+    const size_t na = (size_t)m->anx * m->anz;
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    MTRY(cudaMemcpyAsync(arMean, m->dAcc, na * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MTRY(cudaStreamSynchronize(st));
+    if (m->nAdded > 0)
+        for (size_t i = 0; i < na; i++) arMean[i] /= (double)m->nAdded;
+    return 0;
+}
+
+extern "C" SRWG_API int srwgMultiEAccumulator(srwgMultiE* m, double** dAcc, long long* nElec)
+{
+    if (!m || !dAcc) return SRWG_ERR_BAD_ARG;
+    *dAcc = m->dAcc;
+    if (nElec) *nElec = m->nAdded;
+    return 0;
+}
+
+extern "C" SRWG_API int srwgMultiESetAccumulator(srwgMultiE* m, double* dAcc)
+{
+    std::lock_guard<std::mutex> lk(library_mutex());
+    if (!m || !dAcc) return SRWG_ERR_BAD_ARG;
+    if (!m->ownAcc) return SRWG_ERR_BAD_ARG;
+    cudaFree(m->dAcc);
+    m->dAcc = dAcc;
+    m->ownAcc = false;
+    return 0;
+}
+
+extern "C" SRWG_API int srwgMultiEReset(srwgMultiE* m, void* stream)
+{
+    std::lock_guard<std::mutex> lk(library_mutex());
+    if (!m) return SRWG_ERR_BAD_ARG;
+    DeviceCtx* c = nullptr;
+    int r = device_ctx(m->device, &c);
+    if (r) return r;
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    MTRY(cudaMemsetAsync(m->dAcc, 0, (size_t)m->anx * m->anz * sizeof(double), st));
+    if (!stream) MTRY(cudaStreamSynchronize(st));
+    m->nAdded = 0;
+    return 0;
+}
+
+extern "C" SRWG_API int srwgMultiEDestroy(srwgMultiE* m)
+{
+    std::lock_guard<std::mutex> lk(library_mutex());
+    if (m) {
+        DeviceCtx* c = nullptr;
+        device_ctx(m->device, &c);
+        delete m;
+    }
+    return 0;
+}

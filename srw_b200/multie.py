@@ -1,0 +1,102 @@
+"""Partially coherent (multi-electron) propagation on the GPU.
+
+The reference's ``srwl_wfr_emit_prop_multi_e`` (env/python/srwpy/srwlib.py:8506) loops in Python
+over macro-electrons: field, ``srwl.PropagElecField``, ``srwl.CalcIntFromElecField`` and
+``SRWLStokes.avg_update_interp`` onto a common mesh.  ``MultiE`` runs that loop on the device in
+batches (C-ABI ``srwgMultiE*``): electron wavefronts are the base wavefront offset as
+``SRWLWfr.sim_src_offset`` does (srwlib.py:2803), every pass of the beamline is one launch per
+batch, and the intensities are summed in FP64 on the device.
+
+    me = MultiE(base_wfr, optBL, acc_mesh, max_batch=8, graph=True)
+    me.add(offsets)                 # [n, 4] float64: x [m], x' [rad], y [m], y' [rad]
+    mean = me.mean()                # [ny, nx] float64 mean intensity on acc_mesh
+
+``sample_offsets`` draws the offsets from an uncorrelated Gaussian source phase space with a
+counter-based generator (numpy Philox), so any subset of electrons can be drawn independently,
+e.g. one shard per rank (``shard``).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .srwlpy import make_c_optc, make_c_wfr
+
+
+def sample_offsets(n, sig_x, sig_xp, sig_y, sig_yp, seed=0, first=0):
+    """Offsets of electrons first .. first+n-1: [n, 4] = (x, x', y, y'), independent normals.
+    Electron k always gets the same numbers (Philox stream keyed by the seed, advanced to k)."""
+    out = np.empty((n, 4), np.float64)
+    sig = np.array([sig_x, sig_xp, sig_y, sig_yp], np.float64)
+    for i in range(n):
+        g = np.random.Generator(np.random.Philox(key=seed, counter=[first + i, 0, 0, 0]))
+        out[i] = g.standard_normal(4) * sig
+    return out
+
+
+def shard(n_total, rank, world):
+    """Electron indices of one rank: round-robin, so every rank gets the same mix of electrons."""
+    return np.arange(rank, n_total, world, dtype=np.int64)
+
+
+def _mesh_struct(m):
+    """SRWLRadMesh from a dict or an object with the reference's mesh attribute names."""
+    s = capi.SRWLRadMesh()
+    get = (lambda k, d=None: m.get(k, d)) if isinstance(m, dict) else (lambda k, d=None: getattr(m, k, d))
+    s.eStart = s.eFin = float(get('eStart', 0.))
+    s.xStart, s.xFin, s.yStart, s.yFin = (float(get(k)) for k in ('xStart', 'xFin', 'yStart', 'yFin'))
+    s.ne, s.nx, s.ny = 1, int(get('nx')), int(get('ny'))
+    return s
+
+
+class MultiE(object):
+    def __init__(self, base_wfr, optC, acc_mesh, max_batch=8, graph=False, device=0):
+        L = capi.lib()
+        self._keep = []
+        w = make_c_wfr(base_wfr, self._keep)
+        self._optc = make_c_optc(optC, self._keep)      # must outlive the object (the library keeps it)
+        self._accm = _mesh_struct(acc_mesh)
+        h = C.c_void_p()
+        capi.check(L.srwgMultiECreate(C.byref(w), C.byref(self._optc), C.byref(self._accm), int(max_batch),
+                                      1 if graph else 0, int(device), C.byref(h)), 'multi-electron')
+        self._h = h
+        self.nx, self.ny = int(self._accm.nx), int(self._accm.ny)
+
+    def add(self, offsets, stream=None):
+        off = np.ascontiguousarray(offsets, np.float64).reshape(-1, 4)
+        st = C.c_void_p(stream) if stream else None
+        capi.check(capi.lib().srwgMultiEAdd(self._h, int(off.shape[0]), off.ctypes.data, st), 'multi-electron add')
+
+    def count(self):
+        n = C.c_longlong()
+        capi.check(capi.lib().srwgMultiEGetMean(self._h, None, C.byref(n), None))
+        return int(n.value)
+
+    def mean(self, stream=None):
+        out = np.empty((self.ny, self.nx), np.float64)
+        n = C.c_longlong()
+        st = C.c_void_p(stream) if stream else None
+        capi.check(capi.lib().srwgMultiEGetMean(self._h, out.ctypes.data, C.byref(n), st), 'multi-electron mean')
+        return out
+
+    def accumulator(self):
+        """(device address of the FP64 intensity sum [ny, nx], number of electrons added)."""
+        p = C.c_void_p()
+        n = C.c_longlong()
+        capi.check(capi.lib().srwgMultiEAccumulator(self._h, C.byref(p), C.byref(n)))
+        return int(p.value), int(n.value)
+
+    def use_accumulator(self, dev_ptr):
+        """Adds into caller-owned device memory (ny * nx float64, zeroed by the caller)."""
+        capi.check(capi.lib().srwgMultiESetAccumulator(self._h, C.c_void_p(int(dev_ptr))))
+
+    def reset(self):
+        capi.check(capi.lib().srwgMultiEReset(self._h, None))
+
+    def __del__(self):
+        try:
+            if getattr(self, '_h', None):
+                capi.lib().srwgMultiEDestroy(self._h)
+                self._h = None
+        except Exception:
+            pass

@@ -1,0 +1,154 @@
+"""Partially coherent (multi-electron) propagation: electron sampling and sharding, the mean-intensity
+accumulation (avg_update_interp order 1), the sum over ranks (gloo, 2 processes on the CPU), and on
+the GPU the batched C-ABI path (srwgMultiE*) against the FP64 oracle run electron by electron."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from srw_b200.multie import sample_offsets, shard
+from tests.golden_cases import case_io, load
+from tests.helpers import O, beamline, make_wfr, rel_l2
+
+TOL = 1e-4                       # relative L2 of the mean intensity, FP32 GPU path vs FP64 oracle
+SIG = (30e-6, 5e-6, 5e-6, 2e-6)  # source phase space: sigma x [m], x' [rad], y [m], y' [rad]
+D, INDEX = load()
+
+
+def base_case():
+    c = next(c for c in INDEX if c['name'] == 'c1_64')
+    i, o = case_io(D, 'c1_64')
+    sc = dict(Rx=i['Rx'], Ry=i['Ry'], dRx=i['dRx'], dRy=i['dRy'], xc=i['xc'], yc=i['yc'])
+    acc = dict(nx=96, ny=80, xStart=0.8 * o['mesh']['xStart'], xFin=0.8 * o['mesh']['xFin'],
+               yStart=0.8 * o['mesh']['yStart'], yFin=0.8 * o['mesh']['yFin'], eStart=i['mesh']['eStart'])
+    return i, sc, c['elements'], c['props'], acc
+
+
+def oracle_sum(i, sc, elements, props, acc, offsets):
+    """FP64 oracle: the reference's per-electron loop (offset, propagate, intensity, interpolate)."""
+    s = np.zeros((acc['ny'], acc['nx']))
+    for off in offsets:
+        ex, ey, mesh, sc2 = O.electron_offset(i['ex'], i['ey'], i['mesh'], sc, *off)
+        w = O.Wfr.from_srwl(ex, ey, mesh, sc2['Rx'], sc2['Ry'], sc2['dRx'], sc2['dRy'], sc2['xc'], sc2['yc'])
+        O.propagate(w, [tuple(e) for e in elements], props)
+        O.add_interp_bilinear(s, acc, O.total_intensity(w.ex, w.ey), w.out_mesh())
+    return s
+
+
+def test_offsets_counter_based_and_shards():
+    a = sample_offsets(10, *SIG, seed=7)
+    b = np.concatenate([sample_offsets(4, *SIG, seed=7), sample_offsets(6, *SIG, seed=7, first=4)])
+    assert np.array_equal(a, b)
+    assert abs(np.std(sample_offsets(4000, *SIG, seed=1)[:, 0]) / SIG[0] - 1.) < 0.05
+    parts = [shard(103, r, 4) for r in range(4)]
+    allk = np.sort(np.concatenate(parts))
+    assert np.array_equal(allk, np.arange(103))
+    assert max(len(p) for p in parts) - min(len(p) for p in parts) <= 1
+
+
+def test_interp_matches_reference_loop():
+    """The vectorised accumulation against a scalar restatement of avg_update_interp (order 1)."""
+    rng = np.random.default_rng(3)
+    I = rng.random((7, 9)).astype(np.float32)
+    mesh = dict(nx=9, ny=7, xStart=-1.0, xFin=1.2, yStart=-0.7, yFin=0.9)
+    acc_mesh = dict(nx=11, ny=6, xStart=-1.3, xFin=1.4, yStart=-0.9, yFin=1.0)
+    got = O.add_interp_bilinear(np.zeros((6, 11)), acc_mesh, I, mesh)
+    xs, ys = (mesh['xFin'] - mesh['xStart']) / 8, (mesh['yFin'] - mesh['yStart']) / 6
+    want = np.zeros((6, 11))
+    for iy in range(6):
+        y = acc_mesh['yStart'] + iy * (acc_mesh['yFin'] - acc_mesh['yStart']) / 5
+        for ix in range(11):
+            x = acc_mesh['xStart'] + ix * (acc_mesh['xFin'] - acc_mesh['xStart']) / 10
+            ix0 = int(np.trunc((x - mesh['xStart']) / xs + 1.e-09))
+            iy0 = int(np.trunc((y - mesh['yStart']) / ys + 1.e-09))
+            if ix0 < 0 or ix0 >= 8 or iy0 < 0 or iy0 >= 6:
+                continue
+            tx = (x - (mesh['xStart'] + xs * ix0)) / xs
+            ty = (y - (mesh['yStart'] + ys * iy0)) / ys
+            a00, f10, f01, f11 = (float(I[iy0, ix0]), float(I[iy0, ix0 + 1]), float(I[iy0 + 1, ix0]),
+                                  float(I[iy0 + 1, ix0 + 1]))
+            want[iy, ix] = a00 + tx * ((f10 - a00) + ty * (a00 - f01 - f10 + f11)) + ty * (f01 - a00)
+    np.testing.assert_allclose(got, want, rtol=1e-14, atol=1e-14)
+
+
+def _rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    import torch
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        i, sc, el, pp, acc = base_case()
+        n = 6
+        offs = sample_offsets(n, *SIG, seed=11)
+        mine = shard(n, rank, world)
+        part = torch.from_numpy(oracle_sum(i, sc, el, pp, acc, offs[mine]))
+        cnt = torch.tensor([float(len(mine))], dtype=torch.float64)
+        dist.all_reduce(part)
+        dist.all_reduce(cnt)
+        if rank == 0:
+            q.put((part.numpy() / cnt.item(), oracle_sum(i, sc, el, pp, acc, offs) / n))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_sum_over_ranks_gloo():
+    """Electrons sharded round-robin over 2 ranks, partial FP64 sums reduced over gloo: the mean
+    equals the single-process mean."""
+    import multiprocessing as mp
+    import socket
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    with socket.socket() as s:
+        s.bind(('127.0.0.1', 0))
+        port = s.getsockname()[1]
+    ps = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got, want = q.get(timeout=300)
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU
+# ------------------------------------------------------------------------------------------------
+def _gpu():
+    torch = pytest.importorskip('torch')
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+
+
+def _multie(batch, graph, offsets):
+    from srw_b200.multie import MultiE
+    i, sc, el, pp, acc = base_case()
+    w = make_wfr(i['ex'], i['ey'], i['mesh'], **sc)
+    me = MultiE(w, beamline(el, pp), acc, max_batch=batch, graph=graph)
+    me.add(offsets)
+    return me.mean(), me.count()
+
+
+@pytest.mark.gpu
+def test_multie_vs_oracle():
+    _gpu()
+    offs = sample_offsets(6, *SIG, seed=5)
+    got, n = _multie(4, False, offs)
+    i, sc, el, pp, acc = base_case()
+    want = oracle_sum(i, sc, el, pp, acc, offs) / 6
+    assert n == 6
+    assert np.abs(want).max() > 0
+    assert rel_l2(got, want) < TOL
+
+
+@pytest.mark.gpu
+def test_multie_batch_sizes_and_graph_agree():
+    _gpu()
+    offs = sample_offsets(9, *SIG, seed=9)
+    ref, _ = _multie(1, False, offs)
+    for batch, graph in ((4, False), (4, True), (9, True)):
+        got, n = _multie(batch, graph, offs)
+        assert n == 9
+        np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())

@@ -340,7 +340,10 @@ def measure_batched(args, dev, world, dist):
     # the FP64 intensity sum lives in a torch tensor so that ranks can sum it (NCCL) at the end
     acc_t = torch.zeros((acc['ny'], acc['nx']), dtype=torch.float64, device=dev)
     me.use_accumulator(acc_t.data_ptr())
-    stream = torch.cuda.current_stream(dev)
+    # a stream of its own: batches are queued without host synchronisation (the legacy default
+    # stream cannot be captured into a graph)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.synchronize(dev)
     rank = int(os.environ.get('RANK', '0'))
     for k in range(args.warmup):
         me.add(sample_offsets(BATCH, *SIG, seed=1000 + rank, first=k * BATCH), stream.cuda_stream)

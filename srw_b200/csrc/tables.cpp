@@ -76,7 +76,13 @@ static void separate(const PwOps& pw, int axis, int nAlong, int nLine, SepPart& 
     }
 }
 
-static cd cis(double ph) { return cd(::cos(ph), ::sin(ph)); }
+static cd cis(double ph)
+{
+    if (ph == 0.) return cd(1., 0.);
+    double sn, cs;
+    ::sincos(ph, &sn, &cs);
+    return cd(cs, sn);
+}
 
 static long long push(std::vector<float2>& T, const std::vector<cd>& v)
 {

@@ -8,9 +8,12 @@ to the waist (to-waist mode).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Prints one JSON line.  ``value`` is propagations/s of the batched path: one step = a batch of
-BATCH macro-electron wavefronts (the field with each electron's source offset, made on the device)
-propagated together and their intensities added in FP64 on the device.  ``plain`` is the
+Prints one JSON line.  ``value`` is propagations/s of the batched path with learned resize factors:
+one step = a batch of BATCH macro-electron wavefronts (the field with each electron's source offset,
+made on the device) propagated together and their intensities added in FP64 on the device, with the
+range / resolution factors the trained network (srw_b200.learned) chooses -- when its choice passes
+the run-time check and the mean intensity agrees within 1e-3 with the configured factors' (2, 2) on
+the same electrons; otherwise the configured factors (``batched_configured``).  ``plain`` is the
 single-wavefront path (one propagation per step, device-resident field) with the per-pass CUDA
 event times that give ``roofline``.  ``e2e`` is the batched path through its public API (electron
 offsets from the host in, mean intensity to the host out, every step); ``e2e_single_wavefront`` is
@@ -42,11 +45,11 @@ PEAKS = os.path.join(HERE, 'MEASURED_PEAKS.json')
 BATCH = 16                                     # macro-electron wavefronts per step
 SIG = (30e-6, 5e-6, 5e-6, 2e-6)                # source: sigma x [m], x' [rad], y [m], y' [rad]
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a pass, from an ncu
-# capture of this workload (profiles/line_4096_c1.md, profiles/resize_1024_to_4096_c1.md); keyed by
-# the pass tuple of Plan.kernels().  Re-captured whenever the kernel changes.
-TRAFFIC = {('line_cols', 4096, 4096): 268648960 + 235960832,
-           ('line_rows', 4096, 4096): 268642816 + 232941568,
-           ('resize', 1024, 1024, 4096, 4096): 17597184 + 210405120}
+# capture of this workload (profiles/passes_4096_c1.md); keyed by the pass tuple of Plan.kernels().
+# Re-captured whenever the kernel changes.
+TRAFFIC = {('line_cols', 4096, 4096): 268611840 + 225405440,
+           ('line_rows', 4096, 4096): 67257856 + 216448256,
+           ('resize', 1024, 1024, 4096, 4096): 16920320 + 13591296}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -72,11 +75,12 @@ def synth_undulator_field(n=1024, r=1.5e-3, z=20.):
     return ex, ey, mesh, dict(Rx=z, Ry=z, dRx=0.01 * z, dRy=0.01 * z)
 
 
-def beamline_objs(mod):
-    """C1 beamline with classes from module `mod` (srw_b200.srwlib, or the reference's when given)."""
+def beamline_objs(mod, rng_f=2., res_f=2.):
+    """C1 beamline with classes from module `mod` (srw_b200.srwlib, or the reference's when given);
+    range / resolution factors (rng_f, res_f) of the resize before the lens (2, 2 as configured)."""
     pp = lambda anal=0, pxm=1., pxd=1., pzm=1., pzd=1.: [0, 0, 1., anal, 0, pxm, pxd, pzm, pzd, 0, 0, 0]  # noqa: E731
     return mod.SRWLOptC([mod.SRWLOptA('c', 'a', 0.8e-3, 0.8e-3), mod.SRWLOptL(10., 10.), mod.SRWLOptD(10.)],
-                        [pp(), pp(0, 2., 2., 2., 2.), pp(4)])
+                        [pp(), pp(0, rng_f, res_f, rng_f, res_f), pp(4)])
 
 
 def make_wfr(mod, ex, ey, mesh, sc, alloc=None):
@@ -324,7 +328,7 @@ def _acc_mesh(plan, n=512):
     return dict(nx=n, ny=n, xStart=om['xStart'], xFin=om['xFin'], yStart=om['yStart'], yFin=om['yFin'])
 
 
-def measure_batched(args, dev, world, dist):
+def measure_batched(args, dev, world, dist, factors=(2., 2.), acc=None, e2e_leg=True):
     """Batched path: each step propagates a batch of BATCH macro-electron wavefronts (the 1024^2
     field offset per electron) through the same beamline and adds their intensities on the device;
     K steps between two CUDA events (host planning of the electrons included)."""
@@ -334,8 +338,8 @@ def measure_batched(args, dev, world, dist):
     from srw_b200.plan import Plan
     ex, ey, mesh, sc = synth_undulator_field(1024)
     w = make_wfr(mod, ex, ey, mesh, sc)
-    bl = beamline_objs(mod)
-    acc = _acc_mesh(Plan(w, bl, device=dev.index))
+    bl = beamline_objs(mod, *factors)
+    acc = acc or _acc_mesh(Plan(w, beamline_objs(mod), device=dev.index))
     me = MultiE(w, bl, acc, max_batch=BATCH, graph=True, device=dev.index)
     # the FP64 intensity sum lives in a torch tensor so that ranks can sum it (NCCL) at the end
     acc_t = torch.zeros((acc['ny'], acc['nx']), dtype=torch.float64, device=dev)
@@ -369,7 +373,7 @@ def measure_batched(args, dev, world, dist):
 
     # end to end through the public API: host offsets in, mean intensity (host) out, every step
     e2e = None
-    if not args.no_e2e:
+    if e2e_leg and not args.no_e2e:
         me2 = MultiE(w, bl, acc, max_batch=BATCH, graph=True, device=dev.index)
         me2.add(sample_offsets(BATCH, *SIG, seed=77))
         me2.mean()
@@ -384,24 +388,36 @@ def measure_batched(args, dev, world, dist):
                "path": "srw_b200.multie.MultiE.add (C-ABI srwgMultiEAdd; base field resident, electron offsets "
                        "from host) + MultiE.mean (D2H of the %dx%d FP64 mean intensity)" % (acc['nx'], acc['ny'])}
     return dict(value=value, total_ms=total_ms, e2e=e2e, clocks=nv.summary() or clk.summary(), mean_peak=mean_peak,
-                n_all=n_all)
+                n_all=n_all, mean=acc_t.cpu().numpy() / n_all, acc=acc)
 
 
-def measure_mixed(args, dev, n_elec):
+def measure_mixed(args, dev, n_elec, model=None):
     """Partially coherent workload: n_elec electrons, grids 256^2 / 512^2 / 1024^2 in equal numbers,
-    batched (one MultiE per grid class, graphs) against the same electrons one at a time."""
+    batched (one MultiE per grid class, graphs) against the same electrons one at a time, and
+    batched with the factors the trained network chooses per grid class (mean intensity compared
+    with the configured factors' on the same electrons)."""
     import torch
     from srw_b200 import srwlib as mod
     from srw_b200.multie import MultiE, sample_offsets
     from srw_b200.plan import Plan
-    res = {}
-    for mode, batch, graph in (('batched', None, True), ('plain', 1, False)):
+    modes = [('batched', None, True), ('plain', 1, False)]
+    if model is not None:
+        modes.append(('learned', None, True))
+    res, errs, facs = {}, {}, {}
+    means = {}
+    for mode, batch, graph in modes:
         total = 0.
         for cls, n in enumerate((256, 512, 1024)):
             ex, ey, mesh, sc = synth_undulator_field(n)
             w = make_wfr(mod, ex, ey, mesh, sc)
-            bl = beamline_objs(mod)
-            acc = _acc_mesh(Plan(w, bl, device=dev.index))
+            acc = _acc_mesh(Plan(w, beamline_objs(mod), device=dev.index))
+            factors = (2., 2.)
+            if mode == 'learned':
+                from srw_b200 import learned
+                case = dict(ex=ex, ey=ey, mesh=mesh, sc=sc, E=mesh['eStart'], ap_d=0.8e-3, f=10., L=10.)
+                factors, fb = learned.choose_factors(model, case, dev)
+                facs[n] = list(factors) + (['fallback'] if fb else [])
+            bl = beamline_objs(mod, *factors)
             b = batch or {256: 32, 512: 32, 1024: 16}[n]
             me = MultiE(w, bl, acc, max_batch=b, graph=graph, device=dev.index)
             me.add(sample_offsets(b, *SIG, seed=999))                      # warm-up (plans, graph)
@@ -413,11 +429,49 @@ def measure_mixed(args, dev, n_elec):
             me.add(offs)
             torch.cuda.synchronize(dev)
             total += time.perf_counter() - t0
+            m = me.mean()
+            if mode == 'batched':
+                means[n] = m
+            elif mode == 'learned':
+                ref = means[n]
+                sel = ref > 1e-3 * ref.max()
+                errs[n] = float(np.linalg.norm(m[sel] - ref[sel]) / np.linalg.norm(ref[sel]))
         res[mode] = 3 * (n_elec // 3) / total
-    return {"electrons": 3 * (n_elec // 3), "grids": [256, 512, 1024], "unit": "electrons/s",
-            "batched": res['batched'], "plain": res['plain'], "speedup": res['batched'] / res['plain'],
-            "note": "each electron: offset field, C1 beamline (resize x2/x2 -> 4x grid), intensity added in FP64 "
-                    "onto a 512x512 common mesh; plain = the same electrons one per launch sequence"}
+    out = {"electrons": 3 * (n_elec // 3), "grids": [256, 512, 1024], "unit": "electrons/s",
+           "batched": res['batched'], "plain": res['plain'], "speedup": res['batched'] / res['plain'],
+           "note": "each electron: offset field, C1 beamline (resize before the lens), intensity added in FP64 "
+                   "onto a 512x512 common mesh; plain = the same electrons one per launch sequence with the "
+                   "configured factors (2, 2)"}
+    if model is not None:
+        out.update({"batched_learned": res['learned'], "learned_speedup_vs_plain": res['learned'] / res['plain'],
+                    "learned_factors": {str(k): v for k, v in facs.items()},
+                    "learned_rel_err_vs_configured": {str(k): v for k, v in errs.items()}})
+    return out
+
+
+def measure_learned(args, dev, world, dist, plain_bt):
+    """Batched path with the resize factors the trained network chooses for this wavefront and
+    beamline (srw_b200.learned; run-time check with fallback to the configured factors), on the same
+    electrons as the batched leg; its mean intensity is compared with that leg's."""
+    import torch
+    from srw_b200 import learned
+    from srw_b200 import srwlib as mod  # noqa: F401
+    model = learned.ResizeMLP.load(learned.DEFAULT_MODEL, device=dev.index)
+    ex, ey, mesh, sc = synth_undulator_field(1024)
+    case = dict(ex=ex, ey=ey, mesh=mesh, sc=sc, E=mesh['eStart'], ap_d=0.8e-3, f=10., L=10.)
+    t0 = time.perf_counter()
+    factors, fallback = learned.choose_factors(model, case, dev)
+    choose_s = time.perf_counter() - t0
+    lb = measure_batched(args, dev, world, dist, factors=factors, acc=plain_bt['acc'], e2e_leg=False)
+    ref = plain_bt['mean']
+    sel = ref > 1e-3 * ref.max()                # where the mean intensity is (the learned window is smaller)
+    err = float(np.linalg.norm(lb['mean'][sel] - ref[sel]) / np.linalg.norm(ref[sel]))
+    return {"value": lb['value'], "unit": UNIT, "factors": list(factors), "configured_factors": [2., 2.],
+            "fallback": bool(fallback), "choose_seconds": choose_s,
+            "rel_err_mean_intensity_vs_configured": err,
+            "error_region": "points where the configured-factor mean intensity exceeds 1e-3 of its maximum",
+            "model": {k: v for k, v in getattr(model, 'meta', {}).items()
+                      if k in ('samples', 'val_within_tol', 'val_cost_pred', 'cost_conservative', 'tol')}}
 
 
 def run_ours(args, rank, world):
@@ -430,6 +484,9 @@ def run_ours(args, rank, world):
     torch.cuda.set_device(dev)
     pl = measure_plain(args, dev, world, dist)
     bt = measure_batched(args, dev, world, dist)
+    ln = None
+    if not args.no_learned:
+        ln = measure_learned(args, dev, world, dist, bt)
     plan, kinfo, per_k = pl['plan'], pl['kinfo'], pl['per_k']
 
     # roofline of the dominant pass (live, the plain path's timed steps; same kernels as the batch)
@@ -453,7 +510,11 @@ def run_ours(args, rank, world):
 
     mixed = None
     if not args.no_mixed and world == 1:
-        mixed = measure_mixed(args, dev, args.mixed_electrons)
+        model = None
+        if not args.no_learned:
+            from srw_b200 import learned
+            model = learned.ResizeMLP.load(learned.DEFAULT_MODEL, device=dev.index)
+        mixed = measure_mixed(args, dev, args.mixed_electrons, model)
 
     if rank != 0:
         return
@@ -463,8 +524,15 @@ def run_ours(args, rank, world):
     if cpu is None:
         why = "not measured (--no-cpu-baseline)" if args.no_cpu_baseline else "reference build not present"
         cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
-    out = {"metric": METRIC, "value": bt['value'], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": bt['total_ms'] / args.steps, "higher_is_better": True,
+    # headline: batched + learned factors when the network's factors pass (no fallback, mean intensity
+    # within 1e-3 of the configured factors' on the same electrons), else batched with the configured ones
+    use_learned = ln is not None and not ln['fallback'] and ln['rel_err_mean_intensity_vs_configured'] <= 1e-3
+    head = ln['value'] if use_learned else bt['value']
+    if ln is not None:
+        ln['used_for_value'] = use_learned
+        ln['vs_plain'] = ln['value'] / pl['value']
+    out = {"metric": METRIC, "value": head, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1000. * BATCH / head, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
            "config": {"workload": WORKLOAD, "step": "one batch of %d macro-electron wavefronts (1024^2 field with "
                                                     "its electron's source offset) through the beamline, intensities "
@@ -479,9 +547,11 @@ def run_ours(args, rank, world):
                      "steps": pl['steps'], "path": "srwgPlanExecute on a device-resident 1024^2 field, one wavefront "
                                                    "per step"},
            "batched_vs_plain": bt['value'] / pl['value'],
+           "value_vs_plain": head / pl['value'],
            "mean_intensity": {"electrons": bt['n_all'], "peak": bt['mean_peak'],
                               "reduced_over_ranks": world > 1},
-           "learned": None,
+           "batched_configured": {"value": bt['value'], "unit": UNIT, "factors": [2., 2.]},
+           "learned": ln,
            "roofline": {"bound": "hbm", "kernel": "%s %s" % (kinfo[kd][0], 'x'.join(map(str, kinfo[kd][1:]))),
                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                         "peak_source": peak_src, "traffic": TRAFFIC.get(kinfo[kd]),
@@ -557,6 +627,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end legs (profiling runs)')
     ap.add_argument('--no-mixed', action='store_true', help='skip the mixed-grid multi-electron workload')
+    ap.add_argument('--no-learned', action='store_true', help='skip the learned-factor leg')
     ap.add_argument('--mixed-electrons', type=int, default=600)
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))

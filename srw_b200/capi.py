@@ -83,6 +83,17 @@ SYMBOLS = {
     'srwgMultiESetAccumulator': (C.c_int, [C.c_void_p, C.c_void_p]),
     'srwgMultiEReset': (C.c_int, [C.c_void_p, C.c_void_p]),
     'srwgMultiEDestroy': (C.c_int, [C.c_void_p]),
+    'srwgMlpGemm': (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                              C.c_void_p, C.c_int, C.c_float, C.c_float, C.c_void_p]),
+    'srwgMlpBiasAct': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    'srwgMlpActBackward': (C.c_int, [C.c_void_p, C.c_void_p, C.c_longlong, C.c_int, C.c_void_p]),
+    'srwgMlpColSum': (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    'srwgMlpMse': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    'srwgMlpAdam': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, C.c_float, C.c_float,
+                              C.c_float, C.c_float, C.c_int, C.c_void_p]),
+    'srwgWfrFeatures': (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                  C.c_double, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p,
+                                  C.c_void_p]),
     'srwgPropagElecFieldStatic': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(SRWLWfr)]),
     'srwgPlanDescribe': (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),

@@ -329,6 +329,67 @@ __device__ __forceinline__ void gather_pass(float2* s, int N, int line, const Ch
     __syncthreads();
 }
 
+// chain of a general (even) line length with its along-line factors in the plan's tables:
+// W[k] = tab[k] * extra(i(k), line) * V[src(k)], m = rot2(k), i = mirror(m), src = rot1(i)
+struct ChainG {
+    int rs1, mir, rs2;
+    int tab;                 // offset of the along-line factors in the plan's tables, or -1
+    int extra;               // the pass's non-separable work applies to this chain
+};
+
+__device__ __forceinline__ int chainG_src(const ChainG& c, int k, int N, int& i)
+{
+    const int h = N >> 1;
+    int m = k;
+    if (c.rs2) { m = k + h; if (m >= N) m -= N; }
+    i = c.mir ? (N - 1 - m) : m;
+    int s = i;
+    if (c.rs1) { s = i + h; if (s >= N) s -= N; }
+    return s;
+}
+
+__device__ __forceinline__ bool chainG_trivial(const ChainG& c)
+{
+    return !c.rs1 && !c.mir && !c.rs2 && c.tab < 0 && !c.extra;
+}
+
+__device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2& f, bool& zero);
+
+__device__ __forceinline__ float2 chainG_factor(const ChainG& c, int k, int i, int line, const float2* tabs,
+                                                const PwOps* ex, int axis)
+{
+    float2 f = c.tab >= 0 ? __ldg(&tabs[c.tab + k]) : make_float2(1.f, 0.f);
+    if (c.extra) {
+        bool zero = false;
+        extra_eval(*ex, axis == 0 ? i : line, axis == 0 ? line : i, f, zero);
+        if (zero) f = make_float2(0.f, 0.f);
+    }
+    return f;
+}
+
+// register-staged in-place gather on one line through a table chain: s[k] <- factor(k) s[src(k)]
+__device__ __forceinline__ void gather_pass_t(float2* s, int N, int line, const ChainG& c, int t, int T, bool active,
+                                              const float2* tabs, const PwOps* ex, int axis)
+{
+    float2 tmp[16];
+#pragma unroll
+    for (int v = 0; v < 16; v++) {
+        const int k = t + v * T;
+        if (active && k < N) {
+            int i;
+            const int src = chainG_src(c, k, N, i);
+            tmp[v] = cmul(chainG_factor(c, k, i, line, tabs, ex, axis), s[src]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 16; v++) {
+        const int k = t + v * T;
+        if (active && k < N) s[k] = tmp[v];
+    }
+    __syncthreads();
+}
+
 // non-separable point-wise work: circular masks, rectangular obstacles and the quartic remainder
 // of the angular transfer function (everything separable is in the plan's tables)
 __device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2& f, bool& zero)

@@ -47,21 +47,20 @@ __global__ void __launch_bounds__(512, 1) line_kernel(const LineLaunch p)
     }
     __syncthreads();
 
-    Chain mid;
-    mid.rs1 = 0; mid.sh1 = 0; mid.a1 = 0.; mid.sc1 = 1.f; mid.pw = d.has_pw ? &d.pw : nullptr;
-    mid.mir = d.mirror_along; mid.rs2 = 0; mid.sh2 = 0; mid.a2 = 0.; mid.axis = d.axis;
-    Chain pre;
-    pre.rs1 = 0; pre.sh1 = 0; pre.a1 = 0.; pre.sc1 = 1.f; pre.pw = nullptr; pre.mir = 0;
-    pre.rs2 = d.f1_pre.rs; pre.sh2 = d.f1_pre.has_shift; pre.a2 = d.f1_pre.shift_a; pre.axis = d.axis;
-    if (d.f1) { mid.rs1 = d.f1_post.rs; mid.sh1 = d.f1_post.has_shift; mid.a1 = d.f1_post.shift_a; mid.sc1 = d.f1_post.scale; }
-    Chain fin;
+    // chains with their along-line factors in the plan's tables (as the power-of-two kernels); the
+    // per-line factors of all chains are multiplied once and applied at the store
+    const float2* tabs = p.tabs + blockIdx.z * p.bTab;
+    const PwOps* ex = &d.extra;
+    ChainG pre, mid, fin;
+    pre.rs1 = 0; pre.mir = 0; pre.rs2 = d.f1_pre.rs; pre.tab = (int)d.t_pre.tab; pre.extra = 0;
+    mid.rs1 = d.f1 ? d.f1_post.rs : 0; mid.mir = d.mirror_along; mid.rs2 = d.f2 ? d.f2_pre.rs : 0;
+    mid.tab = (int)d.t_mid.tab; mid.extra = d.has_extra;
     if (d.f2) {
-        mid.rs2 = d.f2_pre.rs; mid.sh2 = d.f2_pre.has_shift; mid.a2 = d.f2_pre.shift_a;
-        fin.rs1 = d.f2_post.rs; fin.sh1 = d.f2_post.has_shift; fin.a1 = d.f2_post.shift_a; fin.sc1 = d.f2_post.scale;
-        fin.pw = nullptr; fin.mir = 0; fin.rs2 = 0; fin.sh2 = 0; fin.a2 = 0.; fin.axis = d.axis;
+        fin.rs1 = d.f2_post.rs; fin.mir = 0; fin.rs2 = 0; fin.tab = (int)d.t_fin.tab; fin.extra = 0;
     } else {
         fin = mid;
     }
+    const bool has_lf = (d.t_pre.ltab >= 0) || (d.t_mid.ltab >= 0) || (d.t_fin.ltab >= 0);
 
     // ---- transforms, batch by batch (uniform trip count: every thread reaches every barrier)
     if (d.f1 || d.f2) {
@@ -72,46 +71,45 @@ __global__ void __launch_bounds__(512, 1) line_kernel(const LineLaunch p)
             const bool active = (g < G) && (c < L) && (line < nl);
             float2* s = sm + (size_t)(c < L ? c : 0) * P;
             if (d.f1) {
-                if (!chain_trivial(pre)) gather_pass(s, N, line, pre, t, T, active);
+                if (!chainG_trivial(pre)) gather_pass_t(s, N, line, pre, t, T, active, tabs, ex, d.axis);
                 if (d.f1 > 0) run_fft<1>(s, N, radix, p.nst, p.tw, t, T, active);
                 else run_fft<-1>(s, N, radix, p.nst, p.tw, t, T, active);
             }
             if (d.f2) {
-                if (!chain_trivial(mid)) gather_pass(s, N, line, mid, t, T, active);
+                if (!chainG_trivial(mid)) gather_pass_t(s, N, line, mid, t, T, active, tabs, ex, d.axis);
                 if (d.f2 > 0) run_fft<1>(s, N, radix, p.nst, p.tw, t, T, active);
                 else run_fft<-1>(s, N, radix, p.nst, p.tw, t, T, active);
             }
         }
     }
-    const bool triv = chain_trivial(fin);
+    const bool triv = chainG_trivial(fin) && !has_lf;
 
     // ---- store the tile
-    if (d.axis == 0) {
-        for (int e = tid; e < N * L; e += nth) {
-            int c = e / N, k = e - c * N;
-            int line = line0 + c;
-            if (line < nl) {
-                const float2* sc = sm + (size_t)c * P;
-                float2 v;
-                if (triv) v = sc[k];
-                else { int sr; float2 f = chain_eval(fin, k, N, line, sr); v = cmul(f, sc[sr]); }
-                int ol = d.mirror_lines ? (nl - 1 - line) : line;
-                __stcs(&dst[(size_t)ol * N + k], v);
+    for (int e = tid; e < N * L; e += nth) {
+        int c, k;
+        if (d.axis == 0) { c = e / N; k = e - c * N; }
+        else { k = e / L; c = e - k * L; }
+        const int line = line0 + c;
+        if (line >= nl) continue;
+        const float2* sc = sm + (size_t)c * P;
+        float2 v;
+        if (triv) {
+            v = sc[k];
+        } else {
+            int i;
+            const int sr = chainG_src(fin, k, N, i);
+            v = cmul(chainG_factor(fin, k, i, line, tabs, ex, d.axis), sc[sr]);
+            if (has_lf) {
+                float2 lf = make_float2(1.f, 0.f);
+                if (d.t_pre.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_pre.ltab + line]));
+                if (d.t_mid.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_mid.ltab + line]));
+                if (d.t_fin.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_fin.ltab + line]));
+                v = cmul(lf, v);
             }
         }
-    } else {
-        for (int e = tid; e < N * L; e += nth) {
-            int r = e / L, c = e - r * L;
-            int col = line0 + c;
-            if (col < nl) {
-                const float2* sc = sm + (size_t)c * P;
-                float2 v;
-                if (triv) v = sc[r];
-                else { int sr; float2 f = chain_eval(fin, r, N, col, sr); v = cmul(f, sc[sr]); }
-                int oc = d.mirror_lines ? (nl - 1 - col) : col;
-                __stcs(&dst[(size_t)r * nl + oc], v);
-            }
-        }
+        const int ol = d.mirror_lines ? (nl - 1 - line) : line;
+        if (d.axis == 0) __stcs(&dst[(size_t)ol * N + k], v);
+        else __stcs(&dst[(size_t)k * nl + ol], v);
     }
 }
 
@@ -563,18 +561,18 @@ __global__ void __launch_bounds__(256) pw_kernel(const PwLaunch p)
 // ------------------------------------------------------------------------------------------------
 // launchers
 // ------------------------------------------------------------------------------------------------
-Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra)
+Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra, int f1, int f2)
 {
     switch (logn) {
-    case 6: return extra ? line2e_get_6(cols) : line2_get_6(cols);
-    case 7: return extra ? line2e_get_7(cols) : line2_get_7(cols);
-    case 8: return extra ? line2e_get_8(cols) : line2_get_8(cols);
-    case 9: return extra ? line2e_get_9(cols) : line2_get_9(cols);
-    case 10: return extra ? line2e_get_10(cols) : line2_get_10(cols);
-    case 11: return extra ? line2e_get_11(cols) : line2_get_11(cols);
-    case 12: return extra ? line2e_get_12(cols) : line2_get_12(cols);
-    case 13: return extra ? line2e_get_13(cols) : line2_get_13(cols);
-    case 14: return extra ? line2e_get_14(cols) : line2_get_14(cols);
+    case 6: return extra ? line2e_get_6(cols, f1, f2) : line2_get_6(cols, f1, f2);
+    case 7: return extra ? line2e_get_7(cols, f1, f2) : line2_get_7(cols, f1, f2);
+    case 8: return extra ? line2e_get_8(cols, f1, f2) : line2_get_8(cols, f1, f2);
+    case 9: return extra ? line2e_get_9(cols, f1, f2) : line2_get_9(cols, f1, f2);
+    case 10: return extra ? line2e_get_10(cols, f1, f2) : line2_get_10(cols, f1, f2);
+    case 11: return extra ? line2e_get_11(cols, f1, f2) : line2_get_11(cols, f1, f2);
+    case 12: return extra ? line2e_get_12(cols, f1, f2) : line2_get_12(cols, f1, f2);
+    case 13: return extra ? line2e_get_13(cols, f1, f2) : line2_get_13(cols, f1, f2);
+    case 14: return extra ? line2e_get_14(cols, f1, f2) : line2_get_14(cols, f1, f2);
     default: return nullptr;
     }
 }
@@ -587,16 +585,18 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
     static int attr_set = 0;
     if (!attr_set) {
         cudaFuncSetAttribute(line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
+        const int dirs[8][2] = {{1, 1}, {1, -1}, {-1, 1}, {-1, -1}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
         for (int lg = 6; lg <= 14; lg++)
             for (int e = 0; e < 4; e++)
-                cudaFuncSetAttribute(line2_kernel_ptr(lg, e & 1, e >> 1), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     SRWG_LINE_SMEM_MAX);
+                for (int m = 0; m < 8; m++)
+                    cudaFuncSetAttribute(line2_kernel_ptr(lg, e & 1, e >> 1, dirs[m][0], dirs[m][1]),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
         attr_set = 1;
     }
     if (p.v2) {
         int lg = 0;
         while ((1 << lg) < p.N) lg++;
-        Line2Fn f = line2_kernel_ptr(lg, p.d.axis != 0, p.d.has_extra != 0);
+        Line2Fn f = line2_kernel_ptr(lg, p.d.axis != 0, p.d.has_extra != 0, p.d.f1, p.d.f2);
         if (f == nullptr) return cudaErrorInvalidValue;
         f<<<grid, p.T * p.L, smem, st>>>(p);
     } else {

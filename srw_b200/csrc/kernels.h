@@ -72,8 +72,8 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st);
 
 // power-of-two line pass kernels, one translation unit per line length (line2_<logn>.cu)
 typedef void (*Line2Fn)(const LineLaunch);
-Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra);
-#define SRWG_LINE2_DECL(L) Line2Fn line2_get_##L(bool cols); Line2Fn line2e_get_##L(bool cols);
+Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra, int f1, int f2);
+#define SRWG_LINE2_DECL(L) Line2Fn line2_get_##L(bool cols, int f1, int f2); Line2Fn line2e_get_##L(bool cols, int f1, int f2);
 SRWG_LINE2_DECL(6) SRWG_LINE2_DECL(7) SRWG_LINE2_DECL(8) SRWG_LINE2_DECL(9) SRWG_LINE2_DECL(10)
 SRWG_LINE2_DECL(11) SRWG_LINE2_DECL(12) SRWG_LINE2_DECL(13) SRWG_LINE2_DECL(14)
 cudaError_t launch_resize(const ResizeLaunch& p, cudaStream_t st);

@@ -136,7 +136,7 @@ __device__ __forceinline__ void fftN(float2* s, const float2* __restrict__ gin, 
 // EXTRA: the pass has non-separable point-wise work (circular masks, rectangular obstacles, the
 // quartic part of the angular transfer function); a separate instantiation keeps its registers out
 // of the common kernels
-template <int LOGN, bool COLS, bool EXTRA>
+template <int LOGN, bool COLS, bool EXTRA, int D1, int D2>
 __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
 {
     constexpr int N = 1 << LOGN;
@@ -203,18 +203,35 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
         if (d.t_fin.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_fin.ltab + line]));
     }
     const float2* tw = p.tw;
-    if (d.f1 && d.f2) {
-        if (d.f1 > 0) fftN<LOGN, 1, 2, 0, EXTRA>(s, gin, nullptr, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        else fftN<LOGN, -1, 2, 0, EXTRA>(s, gin, nullptr, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        if (d.f2 > 0) fftN<LOGN, 1, 1, 1, EXTRA>(s, nullptr, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        else fftN<LOGN, -1, 1, 1, EXTRA>(s, nullptr, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-    } else if (d.f1) {
-        if (d.f1 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+    // D1, D2: directions of the first / second transform (0: none), fixed per instantiation so that
+    // each kernel holds one code path (and its registers)
+    if constexpr (D1 != 0 && D2 != 0) {
+        fftN<LOGN, D1, 2, 0, EXTRA>(s, gin, nullptr, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis,
+                                    za0, za1);
+        fftN<LOGN, D2, 1, 1, EXTRA>(s, nullptr, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex,
+                                    axis, za0, za1);
+    } else if constexpr (D1 != 0) {
+        fftN<LOGN, D1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, pre, mid, tw, active, has_lf, lf, tabs, ex, axis,
+                                    za0, za1);
     } else {
-        if (d.f2 > 0) fftN<LOGN, 1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
-        else fftN<LOGN, -1, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis, za0, za1);
+        fftN<LOGN, D2, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, mid, fin, tw, active, has_lf, lf, tabs, ex, axis,
+                                    za0, za1);
     }
+}
+
+// kernel of a (COLS, EXTRA, f1, f2) combination
+template <int LOGN, bool COLS, bool EXTRA>
+Line2Fn line2_select(int f1, int f2)
+{
+    if (f1 > 0 && f2 > 0) return line2_kernel<LOGN, COLS, EXTRA, 1, 1>;
+    if (f1 > 0 && f2 < 0) return line2_kernel<LOGN, COLS, EXTRA, 1, -1>;
+    if (f1 < 0 && f2 > 0) return line2_kernel<LOGN, COLS, EXTRA, -1, 1>;
+    if (f1 < 0 && f2 < 0) return line2_kernel<LOGN, COLS, EXTRA, -1, -1>;
+    if (f1 > 0) return line2_kernel<LOGN, COLS, EXTRA, 1, 0>;
+    if (f1 < 0) return line2_kernel<LOGN, COLS, EXTRA, -1, 0>;
+    if (f2 > 0) return line2_kernel<LOGN, COLS, EXTRA, 0, 1>;
+    if (f2 < 0) return line2_kernel<LOGN, COLS, EXTRA, 0, -1>;
+    return nullptr;
 }
 
 }  // namespace srwg

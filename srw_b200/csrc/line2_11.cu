@@ -1,7 +1,10 @@
-// Line pass instantiation for lines of 2^11 points without non-separable point-wise work (see
+// Line pass instantiations for lines of 2^11 points without non-separable point-wise work (see
 // line2.cuh).
 #include "line2.cuh"
 
 namespace srwg {
-Line2Fn line2_get_11(bool cols) { return cols ? line2_kernel<11, true, false> : line2_kernel<11, false, false>; }
+Line2Fn line2_get_11(bool cols, int f1, int f2)
+{
+    return cols ? line2_select<11, true, false>(f1, f2) : line2_select<11, false, false>(f1, f2);
+}
 }  // namespace srwg

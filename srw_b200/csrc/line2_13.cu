@@ -1,7 +1,10 @@
-// Line pass instantiation for lines of 2^13 points without non-separable point-wise work (see
+// Line pass instantiations for lines of 2^13 points without non-separable point-wise work (see
 // line2.cuh).
 #include "line2.cuh"
 
 namespace srwg {
-Line2Fn line2_get_13(bool cols) { return cols ? line2_kernel<13, true, false> : line2_kernel<13, false, false>; }
+Line2Fn line2_get_13(bool cols, int f1, int f2)
+{
+    return cols ? line2_select<13, true, false>(f1, f2) : line2_select<13, false, false>(f1, f2);
+}
 }  // namespace srwg

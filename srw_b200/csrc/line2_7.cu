@@ -1,7 +1,10 @@
-// Line pass instantiation for lines of 2^7 points without non-separable point-wise work (see
+// Line pass instantiations for lines of 2^7 points without non-separable point-wise work (see
 // line2.cuh).
 #include "line2.cuh"
 
 namespace srwg {
-Line2Fn line2_get_7(bool cols) { return cols ? line2_kernel<7, true, false> : line2_kernel<7, false, false>; }
+Line2Fn line2_get_7(bool cols, int f1, int f2)
+{
+    return cols ? line2_select<7, true, false>(f1, f2) : line2_select<7, false, false>(f1, f2);
+}
 }  // namespace srwg

@@ -1,7 +1,10 @@
-// Line pass instantiation for lines of 2^13 points with non-separable point-wise work (see
+// Line pass instantiations for lines of 2^13 points with non-separable point-wise work (see
 // line2.cuh).
 #include "line2.cuh"
 
 namespace srwg {
-Line2Fn line2e_get_13(bool cols) { return cols ? line2_kernel<13, true, true> : line2_kernel<13, false, true>; }
+Line2Fn line2e_get_13(bool cols, int f1, int f2)
+{
+    return cols ? line2_select<13, true, true>(f1, f2) : line2_select<13, false, true>(f1, f2);
+}
 }  // namespace srwg

@@ -21,6 +21,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/srwl_b200.h"
@@ -381,14 +382,35 @@ extern "C" SRWG_API int srwgMultiEAdd(srwgMultiE* m, int n, const double* arOffs
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
     std::vector<KernelDesc> first, launchKs;
     int nb = 0;
-    double momX[11], momY[11];
+    // electrons are planned on host threads a group at a time (the planner keeps no shared state);
+    // the GPU runs the previous batches meanwhile
+    const int group = std::max(m->maxBatch, 16);
+    const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<Planner> pls(group);
+    std::vector<ElecParams> eps(group);
+    std::vector<int> rcs(group);
     for (int e = 0; e < n; e++) {
-        SRWLWfr w;
-        ElecParams ep;
-        memset(&ep, 0, sizeof(ep));
-        electron_wfr(*m, arOffsets + 4 * (size_t)e, w, momX, momY, ep);
-        Planner pl;
-        r = pl.plan(&w, m->opt);
+        const int g = e % group;
+        if (g == 0) {
+            const int cnt = std::min(group, n - e);
+            auto work = [&](int t0) {
+                double momX[11], momY[11];
+                for (int k = t0; k < cnt; k += nthr) {
+                    SRWLWfr w;
+                    memset(&eps[k], 0, sizeof(ElecParams));
+                    electron_wfr(*m, arOffsets + 4 * (size_t)(e + k), w, momX, momY, eps[k]);
+                    pls[k] = Planner();
+                    rcs[k] = pls[k].plan(&w, m->opt);
+                }
+            };
+            std::vector<std::thread> th;
+            for (int t = 1; t < std::min(nthr, cnt); t++) th.emplace_back(work, t);
+            work(0);
+            for (auto& t : th) t.join();
+        }
+        Planner& pl = pls[g];
+        ElecParams& ep = eps[g];
+        r = rcs[g];
         if (r) { set_last_detail(pl.err); return r; }
         const size_t tb = pl.tables.size() * sizeof(float2);
         if ((size_t)pl.w.nx * pl.w.nz != m->nOut || (size_t)pl.maxElems > m->perWork || tb > m->descOff ||

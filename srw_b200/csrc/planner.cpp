@@ -19,21 +19,25 @@ namespace srwg {
 // The reference's table (gmfft.cpp:26) holds the even n <= 100000 of the form 2^a 3^b 5^c 7^d 11^e
 // 13^f with e, f <= 1; it is generated here from that rule.
 // ================================================================================================
+static std::vector<long> make_good_numbers()
+{
+    std::vector<long> g;
+    for (long n = 2; n <= 100000; n += 2) {
+        long m = n;
+        while (m % 2 == 0) m /= 2;
+        while (m % 3 == 0) m /= 3;
+        while (m % 5 == 0) m /= 5;
+        while (m % 7 == 0) m /= 7;
+        if (m % 11 == 0) m /= 11;
+        if (m % 13 == 0) m /= 13;
+        if (m == 1) g.push_back(n);
+    }
+    return g;
+}
+
 static const std::vector<long>& good_numbers()
 {
-    static std::vector<long> g;
-    if (g.empty()) {
-        for (long n = 2; n <= 100000; n += 2) {
-            long m = n;
-            while (m % 2 == 0) m /= 2;
-            while (m % 3 == 0) m /= 3;
-            while (m % 5 == 0) m /= 5;
-            while (m % 7 == 0) m /= 7;
-            if (m % 11 == 0) m /= 11;
-            if (m % 13 == 0) m /= 13;
-            if (m == 1) g.push_back(n);
-        }
-    }
+    static const std::vector<long> g = make_good_numbers();     // initialised once, thread-safe
     return g;
 }
 

@@ -1,0 +1,169 @@
+"""Learned resize factors: the MLP kernels against the FP64 oracle (forward, gradients, Adam),
+the feature kernels, training, and what the trained network gains over fixed conservative factors."""
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from tests.helpers import REPO
+
+sys.path.insert(0, os.path.join(REPO, 'oracle'))
+import mlp_oracle as MO  # noqa: E402  (the checker)
+
+from srw_b200 import learned  # noqa: E402
+
+
+def test_oracle_gradients_match_central_differences():
+    rng = np.random.default_rng(0)
+    sizes = [7, 5, 4, 2]
+    Ws = [rng.standard_normal((a, c)) * 0.5 for a, c in zip(sizes[:-1], sizes[1:])]
+    bs = [rng.standard_normal(c) * 0.1 for c in sizes[1:]]
+    X = rng.standard_normal((6, 7))
+    T = rng.standard_normal((6, 2))
+    out, Z, Y = MO.forward(X, Ws, bs)
+    dW, _ = MO.backward(MO.mse(out, T)[1], Ws, Z, Y)
+    for l, idx in ((0, (3, 2)), (1, (0, 1)), (2, (3, 1))):
+        assert abs(MO.numeric_grad(X, T, Ws, bs, l, idx) - dW[l][idx]) < 1e-7
+
+
+def test_round_up_and_targets():
+    assert learned.round_up(np.log2([1.3, 0.5])) == (1.5, 1.0)
+    assert learned.round_up(np.log2([2.0, 1.75])) == (2.0, 1.75)
+    assert learned.round_up(np.log2([2.6, 1.0])) == (2.0, 1.0)
+    assert np.allclose(2. ** learned.target((1.25, 2.0)), [1.25, 2.0])
+
+
+# ------------------------------------------------------------------------------------------------
+# GPU
+# ------------------------------------------------------------------------------------------------
+def _torch():
+    torch = pytest.importorskip('torch')
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    return torch
+
+
+@pytest.mark.gpu
+def test_gemm_all_transposes():
+    torch = _torch()
+    from srw_b200 import capi
+    import ctypes as C
+    rng = np.random.default_rng(1)
+    M, N, K = 70, 130, 33
+    for ta in (0, 1):
+        for tb in (0, 1):
+            A = rng.standard_normal((K, M) if ta else (M, K)).astype(np.float32)
+            B = rng.standard_normal((N, K) if tb else (K, N)).astype(np.float32)
+            Cm = rng.standard_normal((M, N)).astype(np.float32)
+            dA, dB, dC = (torch.from_numpy(a).cuda() for a in (A, B, Cm))
+            r = capi.lib().srwgMlpGemm(M, N, K, dA.data_ptr(), A.shape[1], ta, dB.data_ptr(), B.shape[1], tb,
+                                       dC.data_ptr(), N, 0.5, 2.0, None)
+            assert r == 0
+            want = 0.5 * ((A.T if ta else A).astype(np.float64) @ (B.T if tb else B).astype(np.float64)) + 2.0 * Cm
+            np.testing.assert_allclose(dC.cpu().numpy(), want, rtol=1e-4, atol=1e-4)
+
+
+@pytest.mark.gpu
+def test_mlp_forward_backward_vs_fp64_oracle():
+    """Gradients of the CUDA kernels against the FP64 oracle's analytic (and numerically checked)
+    gradients: relative error below 1e-4."""
+    torch = _torch()
+    m = learned.ResizeMLP(n_in=40, hidden=(32, 24), n_out=2, seed=3)
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((50, 40)).astype(np.float32)
+    T = rng.standard_normal((50, 2)).astype(np.float32)
+    dX, dT = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
+    out = m.forward(dX)
+    loss, dout = m.loss_grad(out, dT)
+    dW, db = m.backward(dout)
+    torch.cuda.synchronize()
+    Ws = [w.cpu().numpy() for w in m.W]
+    bs = [b.cpu().numpy() for b in m.b]
+    o, Z, Y = MO.forward(X, Ws, bs)
+    l, g = MO.mse(o, T)
+    rW, rb = MO.backward(g, Ws, Z, Y)
+    assert np.linalg.norm(out.cpu().numpy() - o) / np.linalg.norm(o) < 1e-5
+    assert abs(float(loss.item()) - l) / l < 1e-5
+    for a, b in zip(dW + db, rW + rb):
+        a = a.cpu().numpy()
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4
+
+
+@pytest.mark.gpu
+def test_adam_step_matches_formula():
+    torch = _torch()
+    m = learned.ResizeMLP(n_in=5, hidden=(4,), n_out=1, seed=0)
+    w0 = m.W[0].cpu().numpy().astype(np.float64)
+    g = [torch.full_like(w, 0.5) for w in m.W]
+    gb = [torch.full_like(b, -0.25) for b in m.b]
+    m.adam(g, gb, lr=0.01)
+    m.adam(g, gb, lr=0.01)
+    torch.cuda.synchronize()
+    mm, vv, w = 0., 0., w0.copy()
+    for t in (1, 2):
+        mm = 0.9 * mm + 0.1 * 0.5
+        vv = 0.999 * vv + 0.001 * 0.25
+        w = w - 0.01 * (mm / (1 - 0.9 ** t)) / (math.sqrt(vv / (1 - 0.999 ** t)) + 1e-8)
+    np.testing.assert_allclose(m.W[0].cpu().numpy(), w, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.gpu
+def test_features_downsample_and_curvature():
+    torch = _torch()
+    n, r, E, R = 256, 1e-3, 5000., 12.0
+    lam = 1.239842e-06 / E
+    x = np.linspace(-r, r, n)
+    X, Y = np.meshgrid(x, x)
+    ex = (np.exp(-(X * X + Y * Y) / (2 * (0.3e-3) ** 2)) * np.exp(1j * math.pi * (X * X + Y * Y) / (lam * R))).astype(
+        np.complex64)
+    ey = (0.1 * ex).astype(np.complex64)
+    mesh = dict(nx=n, ny=n, xStart=-r, xFin=r, yStart=-r, yFin=r)
+    # the wavefront's own radius is 5 % off: the fit recovers the rest from the (resolved) residual phase
+    f = learned.features(torch.from_numpy(ex).cuda(), torch.from_numpy(ey).cuda(), mesh, E, 1e-3, 10., 10.,
+                         torch.device('cuda', 0), Rx=1.05 * R, Ry=0.95 * R).cpu().numpy()
+    I = np.abs(ex.astype(np.complex128)) ** 2 + np.abs(ey.astype(np.complex128)) ** 2
+    d = MO.downsample64(I)
+    np.testing.assert_allclose(f[:4096], np.sqrt(d / d.max()).ravel(), rtol=1e-5, atol=1e-6)
+    assert abs(f[4096] * R - 1.) < 0.01 and abs(f[4097] * R - 1.) < 0.01      # fitted 1/R
+
+
+@pytest.mark.gpu
+def test_training_fits_a_smooth_map():
+    torch = _torch()
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((600, 12)).astype(np.float32)
+    T = np.stack([np.tanh(X[:, 0] + 0.5 * X[:, 1]), 0.3 * X[:, 2] * X[:, 3]], 1).astype(np.float32)
+    m = learned.ResizeMLP(n_in=12, hidden=(64, 64), n_out=2, seed=1)
+    h = m.train(torch.from_numpy(X[:500]).cuda(), torch.from_numpy(T[:500]).cuda(),
+                torch.from_numpy(X[500:]).cuda(), torch.from_numpy(T[500:]).cuda(), epochs=60, batch=50, lr=3e-3)
+    assert h[-1][1] < 0.1 * h[0][1]
+    assert h[-1][2] < 0.3 * float(np.mean(T[500:] ** 2))
+
+
+@pytest.mark.gpu
+def test_trained_model_gain_over_conservative_factors():
+    """Held-out wavefronts (a seed not used in training): the trained network's factors (with the
+    run-time check and its fallback) against the oversampled propagation, and their cost against
+    the conservative factors (2, 2)."""
+    torch = _torch()
+    if not os.path.exists(learned.DEFAULT_MODEL):
+        pytest.skip('no trained model in the package')
+    m = learned.ResizeMLP.load(learned.DEFAULT_MODEL)
+    dev = torch.device('cuda', 0)
+    rng = np.random.default_rng(123456)
+    costs, errs, n_fallback = [], [], 0
+    for _ in range(12):
+        case = learned.sample_case(rng)
+        fac, fb = learned.choose_factors(m, case, dev)
+        n_fallback += fb
+        Iref, omref = learned.propagate_intensity(case, *learned.REF_FACTORS, dev)
+        I, om = learned.propagate_intensity(case, *fac, dev)
+        errs.append(learned.factor_error(I, om, Iref, omref, learned.eval_box(Iref, omref)))
+        costs.append((fac[0] * fac[1]) ** 2)
+    gain = 16.0 / np.mean(costs)
+    print('mean cost gain over conservative factors %.2f, fallbacks %d, median error %.2e' %
+          (gain, n_fallback, np.median(errs)))
+    assert gain > 1.0
+    assert np.median(errs) < 1e-2

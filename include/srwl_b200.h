@@ -184,6 +184,30 @@ SRWG_API int srwgMultiESetAccumulator(srwgMultiE* m, double* dAcc);
 SRWG_API int srwgMultiEReset(srwgMultiE* m, void* stream);
 SRWG_API int srwgMultiEDestroy(srwgMultiE* m);
 
+/* Learned resize-factor predictor (no counterpart in the reference, whose users set the resize
+ * factors pp[5..8] by hand): kernels of a small FP32 MLP and of the wavefront features it reads.
+ * All pointers are device memory of the current device; row-major matrices.
+ *   srwgMlpGemm:        C = alpha op(A) op(B) + beta C, op(A) M x K, op(B) K x N (trans flags transpose)
+ *   srwgMlpBiasAct:     Z += bias (per column); Y = act(Z), act 0 identity, 1 GELU (tanh form)
+ *   srwgMlpActBackward: dY *= act'(Z)
+ *   srwgMlpColSum:      db[j] = sum_i dZ[i][j]
+ *   srwgMlpMse:         *loss += mean (out - target)^2 (FP64), dout = 2 (out - target) / n
+ *   srwgMlpAdam:        Adam step t (>= 1) with bias correction
+ *   srwgWfrFeatures:    total intensity averaged on 64 x 64 cells (dFeat[4096]) and the sums of the
+ *                       weighted fit of the phase curvature left after removing k (x^2/R0x + z^2/R0z)/2
+ *                       (dSums[4]: sum w x dphi, sum w x^2, the same in z; k = 2 pi / lambda) */
+SRWG_API int srwgMlpGemm(int M, int N, int K, const float* A, int lda, int transA, const float* B, int ldb, int transB,
+                         float* C, int ldc, float alpha, float beta, void* stream);
+SRWG_API int srwgMlpBiasAct(float* Z, const float* bias, float* Y, int M, int N, int act, void* stream);
+SRWG_API int srwgMlpActBackward(const float* Z, float* dY, long long n, int act, void* stream);
+SRWG_API int srwgMlpColSum(const float* dZ, float* db, int M, int N, void* stream);
+SRWG_API int srwgMlpMse(const float* out, const float* target, float* dout, double* loss, int n, void* stream);
+SRWG_API int srwgMlpAdam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
+                         float eps, int t, void* stream);
+SRWG_API int srwgWfrFeatures(const float* dEx, const float* dEy, int nx, int ny, double xStart, double xStep,
+                             double zStart, double zStep, double k, double invRx0, double invRz0, float* dFeat,
+                             double* dSums, void* stream);
+
 /* Allocation-free propagation (no counterpart in the reference).  For callers that cannot call
  * cudaMalloc at run time -- programs that reserve all device memory at start-up and hand out
  * slices themselves, or whose device memory must go through their own caching allocator --

@@ -136,6 +136,33 @@ int line_config(const LineDesc& d, LineLaunch& p)
         if ((size_t)p.L * p.P * sizeof(float2) > cap) { g_lastDetail = "line too long for shared memory"; return SRWG_ERR_UNSUPPORTED; }
         return 0;
     }
+    // general good number with radices 16/8/4/2, 3, 5, 7 and at least two stages: the fused pass of
+    // lineg.cuh (T >= N/16 threads per line, rows ~256 threads, columns up to 512 threads per CTA)
+    {
+        int rad[SRWG_MAX_STAGES];
+        const int ns = radix_plan(N, rad);
+        bool gen = ns >= 2 && N <= 8192;
+        for (int i = 0; i < ns && gen; i++) gen = rad[i] != 11 && rad[i] != 13;
+        if (gen) {
+            p.v2 = 2;
+            int T = (N + 15) / 16;
+            T = ((T + 31) / 32) * 32;
+            p.T = T;
+            p.P = N + N / 16 + 4;
+            int L = d.axis == 0 ? 256 / T : 512 / T;
+            if (L < 1) L = 1;
+            while (L > 1 && (size_t)L * p.P * sizeof(float2) > cap) L--;
+            if (T * L > 512 || (size_t)L * p.P * sizeof(float2) > cap) {
+                g_lastDetail = "line too long for shared memory";
+                return SRWG_ERR_UNSUPPORTED;
+            }
+            p.L = L;
+            p.G = L;
+            p.nst = ns;
+            for (int i = 0; i < ns; i++) p.radix[i] = rad[i];
+            return 0;
+        }
+    }
     p.v2 = 0;
     // general good number: T threads per line, at most 16 points each; G = threads per CTA / T
     // groups work on the CTA's L lines in batches

@@ -355,11 +355,12 @@ __device__ __forceinline__ bool chainG_trivial(const ChainG& c)
 
 __device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2& f, bool& zero);
 
+template <bool EXTRA = true>
 __device__ __forceinline__ float2 chainG_factor(const ChainG& c, int k, int i, int line, const float2* tabs,
                                                 const PwOps* ex, int axis)
 {
     float2 f = c.tab >= 0 ? __ldg(&tabs[c.tab + k]) : make_float2(1.f, 0.f);
-    if (c.extra) {
+    if (EXTRA && c.extra) {
         bool zero = false;
         extra_eval(*ex, axis == 0 ? i : line, axis == 0 ? line : i, f, zero);
         if (zero) f = make_float2(0.f, 0.f);

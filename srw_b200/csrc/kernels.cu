@@ -591,9 +591,17 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
                 for (int m = 0; m < 8; m++)
                     cudaFuncSetAttribute(line2_kernel_ptr(lg, e & 1, e >> 1, dirs[m][0], dirs[m][1]),
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
+        for (int e = 0; e < 2; e++) {
+            cudaFuncSetAttribute(lineg_get(e != 0), cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
+            cudaFuncSetAttribute(lineg_e_get(e != 0), cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
+        }
         attr_set = 1;
     }
-    if (p.v2) {
+    if (p.v2 == 2) {
+        Line2Fn f = p.d.has_extra ? lineg_e_get(p.d.axis != 0) : lineg_get(p.d.axis != 0);
+        if (p.T * p.L > 512) return cudaErrorInvalidValue;
+        f<<<grid, p.T * p.L, smem, st>>>(p);
+    } else if (p.v2) {
         int lg = 0;
         while ((1 << lg) < p.N) lg++;
         Line2Fn f = line2_kernel_ptr(lg, p.d.axis != 0, p.d.has_extra != 0, p.d.f1, p.d.f2);

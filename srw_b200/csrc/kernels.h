@@ -30,7 +30,7 @@ struct LineLaunch {
     int T, L, P, G;          // threads per line, lines per CTA, shared-memory pitch (float2), thread groups
     int nst;
     int radix[SRWG_MAX_STAGES];
-    int v2;                  // power-of-two line pass (line2_kernel)
+    int v2;                  // 1: power-of-two pass (line2_kernel), 2: general length (lineg_kernel)
     const float2* tabs;      // the plan's separable point-wise tables
     const LineDesc* gd;      // this pass's descriptor in device memory
     int nb;                  // wavefronts in the launch (grid z; 0 or 1: one)
@@ -76,6 +76,9 @@ Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra, int f1, int f2);
 #define SRWG_LINE2_DECL(L) Line2Fn line2_get_##L(bool cols, int f1, int f2); Line2Fn line2e_get_##L(bool cols, int f1, int f2);
 SRWG_LINE2_DECL(6) SRWG_LINE2_DECL(7) SRWG_LINE2_DECL(8) SRWG_LINE2_DECL(9) SRWG_LINE2_DECL(10)
 SRWG_LINE2_DECL(11) SRWG_LINE2_DECL(12) SRWG_LINE2_DECL(13) SRWG_LINE2_DECL(14)
+// general-length line pass kernels (lineg.cu, lineg_e.cu)
+Line2Fn lineg_get(bool cols);
+Line2Fn lineg_e_get(bool cols);
 cudaError_t launch_resize(const ResizeLaunch& p, cudaStream_t st);
 cudaError_t launch_pw(const PwLaunch& p, cudaStream_t st);
 

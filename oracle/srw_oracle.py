@@ -16,9 +16,11 @@ Parity pin: the restatement is checked against the reference itself (built from 
 ``oracle/Makefile`` into ``oracle/_ref/``) through the golden fixtures in ``tests/golden/``
 made by ``tests/golden/make_golden.py``.
 
-Not restated (documented gaps): ComputeRadMoments (sroptelm.cpp:1608) — statistical moments
-are propagated with the reference's analytic matrices only; the auto-resize Meth_1/Meth_2
-machinery (pp[0], pp[1] != 0); drift modes pp[3] = 1, 5 and >= 100; ne > 1.
+Statistical moments: propagated with the reference's analytic matrices, and recomputed from the
+field (ComputeRadMoments, sroptelm.cpp:1608) where an aperture or obstacle asks for it.
+
+Not restated (documented gaps): the auto-resize Meth_1/Meth_2 machinery (pp[0], pp[1] != 0);
+drift modes pp[3] = 1, 5 and >= 100; ne > 1.
 """
 from __future__ import annotations
 
@@ -663,6 +665,10 @@ def aperture(w: Wfr, shape, ap_or_ob, Dx, Dy, cx, cy):
         inside = ~inside
     w.ex = np.where(inside, w.ex, 0.)
     w.ey = np.where(inside, w.ey, 0.)
+    # srTAperture::PropagateRadMoments (sroptapt.cpp:248-350): recompute the moments numerically
+    # when 1.7 sigma of the beam is not inside the opening (obstacles: always, sroptapt.h:294)
+    if ap_or_ob in 'oO' or _moments_outside_opening(w, shape, Dx, Dy, cx, cy):
+        compute_rad_moments(w)
     # SetNewNonZeroWfrLimits (apertures only; obstacles keep the limits in the cases used here)
     if ap_or_ob in 'aA':
         if shape == 'r':
@@ -717,6 +723,203 @@ def _treat_strongly_oscillating(w: Wfr, add_or_rem):
     if w.QuadX:
         ph = ph + cRx * w.eStart * x * x
     _apply_phase(w, ph)
+
+
+def central_moments(m):
+    """srTMomentsPtrs::ComputeCentralMoments (srstraux.h:357): (sqrt Mxx, sqrt Mzz) with the 0.1
+    safety floor on the central second moments."""
+    Mxx = m[5] - m[1] * m[1]
+    Mzz = m[8] - m[3] * m[3]
+    if Mxx < 0.1 * m[5]:
+        Mxx = 0.1 * m[5]
+    if Mzz < 0.1 * m[8]:
+        Mzz = 0.1 * m[8]
+    return math.sqrt(abs(Mxx)), math.sqrt(abs(Mzz))
+
+
+def _moments_outside_opening(w: Wfr, shape, Dx, Dy, cx, cy):
+    """CheckIfMomentsShouldBeRecomputed of the rectangular (sroptapt.h:206) and circular
+    (sroptapt.h:384) apertures, applied to the Ex and Ez moments with the 1.7 sigma margin."""
+    hx, hz = (0.5 * Dx, 0.5 * Dy) if shape == 'r' else (0.5 * Dx, 0.5 * Dx)
+    for m in (w.momX, w.momZ):
+        sx, sz = central_moments(m)
+        sx, sz = 1.7 * sx, 1.7 * sz
+        if (m[1] - sx) < (cx - hx) or (m[1] + sx) > (cx + hx) or (m[3] - sz) < (cy - hz) or (m[3] + sz) > (cy + hz):
+            return True
+    return False
+
+
+def _find_limit_left(a, stop):
+    """srTAuxMatStat::FindLimit1DLeft (srmatsta.cpp:400): first index where the running sum
+    exceeds `stop` (0 when it never does)."""
+    s = 0.
+    for i in range(len(a)):
+        s += a[i]
+        if s > stop:
+            return i
+    return 0
+
+
+def _find_limit_right(a, stop):
+    """FindLimit1DRight (srmatsta.cpp:426): the same from the right end (n - 1 when never)."""
+    n = len(a)
+    s = 0.
+    for i in range(n):
+        s += a[n - 1 - i]
+        if s > stop:
+            return n - 1 - i
+    return n - 1
+
+
+def _sum_up(a):
+    """SumUpArray (srmatsta.h:437) over a whole line: 0 for fewer than two points."""
+    return float(np.sum(a, dtype=np.float64)) if len(a) >= 2 else 0.
+
+
+def find_intensity_limits_inds(I, w: Wfr, rel_pow=0.9):
+    """srTAuxMatStat::FindIntensityLimitsInds (srmatsta.cpp:572) with FindIntensityLimits2D (:452):
+    the index box holding `rel_pow` of the power of the FP32 intensity I [nz, nx], trimmed by
+    (1 - rel_pow)/4 of the total at each edge, first along z (rows summed over x) then along x
+    within the z limits.  Returns [ix0, ix1, iz0, iz1]; the whole mesh when the search fails."""
+    nx, nz = w.nx, w.nz
+    full = [0, nx - 1, 0, nz - 1]
+    I = np.asarray(I, np.float32)
+    tot = float(np.float32(float(np.sum(I, dtype=np.float64)) * w.xStep * w.zStep))   # IntegrateSimple
+    stop = tot * (1. - rel_pow) * 0.25
+    if nx < 2 or nz < 2:                                   # IntegrateOverX: ixStart >= ixEnd
+        return full
+    rows = np.array([w.xStep * _sum_up(I[iz, :]) for iz in range(nz)])
+    iy0 = _find_limit_left(rows, stop / w.zStep)
+    iy1 = _find_limit_right(rows, stop / w.zStep)
+    if iy1 <= iy0:
+        return full
+    cols = np.array([w.zStep * (float(np.sum(I[iy0:iy1 + 1, ix], dtype=np.float64))) for ix in range(nx)])
+    ix0 = _find_limit_left(cols, stop / w.xStep)
+    ix1 = _find_limit_right(cols, stop / w.xStep)
+    f = [np.float32(w.xStart + w.xStep * ix0), np.float32(w.xStart + w.xStep * ix1),
+         np.float32(w.zStart + w.zStep * iy0), np.float32(w.zStart + w.zStep * iy1)]
+    lims = [int((float(f[0]) - w.xStart) * 1.0000001 / w.xStep), int((float(f[1]) - w.xStart) * 1.0000001 / w.xStep),
+            int((float(f[2]) - w.zStart) * 1.0000001 / w.zStep), int((float(f[3]) - w.zStart) * 1.0000001 / w.zStep)]
+    lims[0] = max(lims[0], 0)
+    lims[1] = min(lims[1], nx - 1)
+    lims[2] = max(lims[2], 0)
+    lims[3] = min(lims[3], nz - 1)
+    return lims
+
+
+def moment_sums(ex, ey, w: Wfr, lims):
+    """The 22 weighted sums of srTGenOptElem::ComputeRadMoments (sroptelm.cpp:1745-1935) for the
+    coordinate representation: per component norm, first moments, and (inside the power limits)
+    second moments; the angular moments from finite differences of the field along x and z plus
+    the wavefront-curvature term 2 pi/(lambda R) * step * coordinate.  Trapezoid weights: 1/2 at
+    the mesh edges, and 1/2 again on the angular terms of the second row / column."""
+    nx, nz = w.nx, w.nz
+    lam = 1.239842E-06 / w.eStart
+    R_x = w.RobsX if w.RobsX != 0. else 100. * lam
+    R_z = w.RobsZ if w.RobsZ != 0. else 100. * lam
+    four_pi = 3.141592653590 * 2. * 2.
+    lam_d_4pi = 1.239842E-06 / (four_pi * w.eStart)
+    ax = 0.5 * (w.xStep * ((1. / lam_d_4pi) / R_x))         # TwoPi_d_Lamb_d_Rx_xStep
+    az = 0.5 * (w.zStep * ((1. / lam_d_4pi) / R_z))
+    x = (w.xStart + np.arange(nx) * w.xStep)[None, :]
+    z = (w.zStart + np.arange(nz) * w.zStep)[:, None]
+    ix = np.arange(nx)[None, :]
+    iz = np.arange(nz)[:, None]
+    inside = (ix >= lims[0]) & (ix <= lims[1]) & (iz >= lims[2]) & (iz <= lims[3])
+    S = np.zeros(22)
+    for base, E in ((0, ex), (11, ey)):
+        re, im = np.real(E).astype(np.float64), np.imag(E).astype(np.float64)
+        f = [None] * 11
+        n = re * re + im * im
+        f[0] = n
+        f[1] = x * n
+        f[3] = z * n
+        f[5] = np.where(inside, x * f[1], 0.)
+        f[8] = np.where(inside, z * f[3], 0.)
+        # along x (ix > 0)
+        dr = np.zeros_like(re); di = np.zeros_like(im)
+        dr[:, 1:] = re[:, 1:] - re[:, :-1]
+        di[:, 1:] = im[:, 1:] - im[:, :-1]
+        cr = di * re - dr * im
+        hasx = np.broadcast_to(ix > 0, re.shape)
+        f[2] = np.where(hasx, cr + ax * x * n, 0.)
+        f[6] = np.where(hasx & inside, x * f[2], 0.)
+        f[7] = np.where(hasx & inside, (dr * dr + di * di) + cr * ax * x + ax * ax * x * x * n, 0.)
+        # along z (iz > 0)
+        dr = np.zeros_like(re); di = np.zeros_like(im)
+        dr[1:, :] = re[1:, :] - re[:-1, :]
+        di[1:, :] = im[1:, :] - im[:-1, :]
+        cr = di * re - dr * im
+        hasz = np.broadcast_to(iz > 0, re.shape)
+        f[4] = np.where(hasz, cr + az * z * n, 0.)
+        f[9] = np.where(hasz & inside, z * f[4], 0.)
+        f[10] = np.where(hasz & inside, (dr * dr + di * di) + cr * az * z + az * az * z * z * n, 0.)
+        wx = np.ones(nx); wx[0] *= 0.5; wx[-1] *= 0.5
+        wz = np.ones(nz); wz[0] *= 0.5; wz[-1] *= 0.5
+        wx1 = wx.copy()
+        if nx > 1:
+            wx1[1] *= 0.5
+        wz1 = wz.copy()
+        if nz > 1:
+            wz1[1] *= 0.5
+        for k in range(11):
+            cx = wx1 if k in (2, 6, 7) else wx
+            cz = wz1 if k in (4, 9, 10) else wz
+            S[base + k] = float(np.sum(f[k] * cx[None, :] * cz[:, None]))
+    return S, ax, az
+
+
+def moments_from_sums(S, w: Wfr):
+    """Normalisation of the sums into the 11 moments of Ex and of Ez, each rounded to FP32 as the
+    reference stores it (sroptelm.cpp:1937-2080, coordinate representation)."""
+    lam_d_4pi = 1.239842E-06 / (3.141592653590 * 2. * 2. * w.eStart)
+    lam_d_2pi = 2. * lam_d_4pi
+    lam_d_2pi_e2 = lam_d_2pi * lam_d_2pi
+    inv_sx, inv_sz = 1. / w.xStep, 1. / w.zStep
+    scan_x, scan_z = w.nx > 1, w.nz > 1
+    out = []
+    for b in (0, 11):
+        if S[b] == 0.:
+            out.append(np.zeros(11))
+            continue
+        inv_n = 1. / S[b]
+        a = inv_n * lam_d_2pi
+        ax, az = a * inv_sx, a * inv_sz
+        a2 = inv_n * lam_d_2pi_e2
+        ax2, az2 = a2 * (inv_sx * inv_sx), a2 * (inv_sz * inv_sz)
+        f32 = lambda v: float(np.float32(v))  # noqa: E731
+        m = np.array([
+            f32(S[b] * (w.xStep * w.zStep * 1.E+06) if (scan_x and scan_z) else 0.),
+            f32(S[b + 1] * inv_n if scan_x else w.xStart),
+            f32(S[b + 2] * ax if scan_x else 0.),
+            f32(S[b + 3] * inv_n if scan_z else w.zStart),
+            f32(S[b + 4] * az if scan_z else 0.),
+            f32(S[b + 5] * inv_n if scan_x else w.xStart * w.xStart),
+            f32(S[b + 6] * ax if scan_x else 0.),
+            f32(S[b + 7] * ax2 if scan_x else 0.),
+            f32(S[b + 8] * inv_n if scan_z else w.zStart * w.zStart),
+            f32(S[b + 9] * az if scan_z else 0.),
+            f32(S[b + 10] * az2 if scan_z else 0.)])
+        out.append(m)
+    return out[0], out[1]
+
+
+def compute_rad_moments(w: Wfr):
+    """srTGenOptElem::ComputeRadMoments (sroptelm.cpp:1608-2092), coordinate representation, ne = 1:
+    the quadratic phase of the wavefront radius is removed first (TreatStronglyOscillatingTerm 'r'
+    when WaveFrontTermCanBeTreated; re-added after, so only a local copy is changed here), the
+    power limits found on the intensity, then the sums normalised into w.momX / w.momZ."""
+    if w.nx <= 1 and w.nz <= 1:
+        return
+    ex, ey = w.ex, w.ey
+    if w.Pres == 0 and _wavefront_term_can_be_treated(w):
+        save = (w.ex, w.ey)
+        _treat_strongly_oscillating(w, 'r')
+        ex, ey = w.ex, w.ey
+        w.ex, w.ey = save
+    lims = find_intensity_limits_inds(total_intensity(ex, ey), w)
+    S, _, _ = moment_sums(ex, ey, w, lims)
+    w.momX, w.momZ = moments_from_sums(S, w)
 
 
 def _lagrange4(t):

@@ -42,3 +42,16 @@ def case_io(d, name):
                     momY=np.array(d[name + '/' + s + '/momy']),
                     mesh_raw=np.array(m[:6]))
     return side('in'), side('out')
+
+
+def moment_err(a, b):
+    """Largest error of the 11 statistical moments `a` against `b`, each relative to its natural
+    scale: the norm for [0], the rms size / divergence for the first moments, and the second
+    moments themselves (cross terms: the product of the two rms values)."""
+    a = np.asarray(a, np.float64)[:11]
+    b = np.asarray(b, np.float64)[:11]
+    r = lambda k: np.sqrt(abs(b[k]))  # noqa: E731
+    s = np.array([abs(b[0]), r(5), r(7), r(8), r(10), abs(b[5]), r(5) * r(7), abs(b[7]), abs(b[8]), r(8) * r(10),
+                  abs(b[10])])
+    s = np.where(s > 0, s, 1e-300)
+    return float(np.max(np.abs(a - b) / s))

@@ -134,8 +134,16 @@ typedef struct srwgPlan srwgPlan;
 SRWG_API int srwgPlanCreate(const SRWLWfr* pWfr, const SRWLOptC* pOpt, int device, srwgPlan** ppPlan);
 
 /* Writes the output mesh and scalars (Rx, Ry, dRx, dRy, xc, yc, presCA, moments when arMomX/Y
- * are non-NULL) of the planned propagation into pWfrOut; field arrays are not touched. */
+ * are non-NULL) of the planned propagation into pWfrOut; field arrays are not touched.  Where
+ * the propagation recomputes the statistical moments from the field (an aperture that clips the
+ * beam, an obstacle: srTAperture::PropagateRadMoments, sroptapt.cpp:248), the moments are those
+ * of wavefront 0 of the last execution (the call waits for it); before any execution they are
+ * the analytically propagated ones. */
 SRWG_API int srwgPlanGetOutput(const srwgPlan* plan, SRWLWfr* pWfrOut);
+
+/* The 11 + 11 output moments (arMomX / arMomY layout) of wavefront `index` of the last execution
+ * (waits for it); for plans without a moment recomputation the analytically propagated ones. */
+SRWG_API int srwgPlanGetMoments(const srwgPlan* plan, int index, double* momX, double* momY);
 
 /* Input and output grid sizes, number of GPU kernels per execution, and the bytes of device
  * work space the plan holds (two buffers of the largest grid, both components). */

@@ -67,6 +67,7 @@ SYMBOLS = {
     'srwlUtiGetErrText': (C.c_int, [C.c_char_p, C.c_int]),
     'srwgPlanCreate': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_int, C.POINTER(C.c_void_p)]),
     'srwgPlanGetOutput': (C.c_int, [C.c_void_p, C.POINTER(SRWLWfr)]),
+    'srwgPlanGetMoments': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     'srwgPlanInfo': (C.c_int, [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_long),
                                C.POINTER(C.c_long), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
     'srwgPlanExecute': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

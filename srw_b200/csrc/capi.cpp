@@ -228,7 +228,7 @@ static int upload_tables(const Planner& pl, float2** buf, size_t* capElems, cuda
 int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, const float2* inX, const float2* inY,
                    long long inStride, float2* outX, float2* outY, long long outStride, float2* work, size_t workElems,
                    const char* dconst, long long constStride, size_t descOff, cudaStream_t st, cudaEvent_t* ev,
-                   const std::vector<KernelDesc>* hostMax)
+                   const std::vector<KernelDesc>* hostMax, double* momScratch, double* momSlots, int nSlots)
 {
     const size_t nk = ks.size();
     const size_t W = (size_t)nb * workElems;
@@ -236,18 +236,45 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
     const float2* tabs = (const float2*)dconst;
     const KernelDesc* gk = (const KernelDesc*)(dconst + descOff);
     const long long tabStride = constStride / (long long)sizeof(float2);
+    // the last pass that writes a field writes the output; MOM passes after it read the output
+    size_t lastField = nk;
+    for (size_t i = nk; i-- > 0;)
+        if (ks[i].kind != K_MOM) { lastField = i; break; }
+    if (lastField == nk && nk > 0) {        // a moment pass always comes with the pass of its mask
+        g_lastDetail = "plan without field passes";
+        return SRWG_ERR_BAD_ARG;
+    }
     for (size_t i = 0; i < nk; i++) {
         const KernelDesc& k = hostMax ? (*hostMax)[i] : ks[i];
         if (ev) CUDA_TRY(cudaEventRecord(ev[2 * i], st));
-        const bool fromIn = k.src == 0, toOut = i + 1 == nk;
-        const float2* s0 = fromIn ? inX : wb[k.src][0];
-        const float2* s1 = fromIn ? inY : wb[k.src][1];
+        const bool fromOut = k.kind == K_MOM && k.src != 0 && i > lastField && k.src == ks[lastField].dst;
+        const bool fromIn = k.src == 0, toOut = i == lastField;
+        const float2* s0 = fromOut ? outX : fromIn ? inX : wb[k.src][0];
+        const float2* s1 = fromOut ? outY : fromIn ? inY : wb[k.src][1];
         float2* d0 = toOut ? outX : wb[k.dst][0];
         float2* d1 = toOut ? outY : wb[k.dst][1];
-        const long long bSrc = fromIn ? inStride : (long long)workElems;
+        const long long bSrc = fromOut ? outStride : fromIn ? inStride : (long long)workElems;
         const long long bDst = toOut ? outStride : (long long)workElems;
         cudaError_t e = cudaSuccess;
-        if (k.kind == K_LINE) {
+        if (k.kind == K_MOM) {
+            if (momScratch == nullptr || momSlots == nullptr || k.mom.slot < 0 || k.mom.slot >= nSlots) {
+                g_lastDetail = "moment pass without result buffers";
+                return SRWG_ERR_BAD_ARG;
+            }
+            MomLaunch p;
+            memset(&p, 0, sizeof(p));
+            p.d = k.mom;
+            p.src[0] = s0;
+            p.src[1] = s1;
+            p.tabs = tabs;
+            p.gd = &gk[i].mom;
+            p.scratch = momScratch;
+            p.out = momSlots + (size_t)k.mom.slot * SRWG_MOM_SLOT;
+            p.nb = nb; p.bDesc = constStride; p.bTab = tabStride;
+            p.bSrc = bSrc;
+            p.bOut = (long long)nSlots * SRWG_MOM_SLOT;
+            e = launch_moments(p, st);
+        } else if (k.kind == K_LINE) {
             LineLaunch p;
             memset(&p, 0, sizeof(p));
             int r = line_config(k.line, p);
@@ -289,10 +316,30 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
     return 0;
 }
 
-// runs the plan's passes on one wavefront (or nb wavefronts with the same plan)
+// doubles of the scratch of the plan's largest moment pass (0: no moment pass)
+static size_t mom_scratch_for(const Planner& pl)
+{
+    size_t m = 0;
+    for (const KernelDesc& k : pl.kernels)
+        if (k.kind == K_MOM) m = std::max(m, mom_scratch_doubles(k.mom.nx, k.mom.nz));
+    return m;
+}
+
+static int ensure_doubles(double** buf, size_t* cap, size_t n)
+{
+    if (*buf && *cap >= n) return 0;
+    if (*buf) { cudaFree(*buf); *buf = nullptr; *cap = 0; }
+    CUDA_TRY(cudaMalloc(buf, n * sizeof(double)));
+    *cap = n;
+    return 0;
+}
+
+// runs the plan's passes on one wavefront (or nb wavefronts with the same plan); moment passes
+// write their sums to momSlots (nMomSlots * SRWG_MOM_SLOT doubles per wavefront)
 static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* inY, float2* outX, float2* outY,
                    float2* work, size_t workElems, const float2* dtab, cudaStream_t st, cudaEvent_t* ev = nullptr,
-                   int nb = 1, long long inStride = 0, long long outStride = 0)
+                   int nb = 1, long long inStride = 0, long long outStride = 0, double* momSlots = nullptr,
+                   double* momScratch = nullptr)
 {
     const size_t nOut = (size_t)pl.w.nx * pl.w.nz;
     if (pl.kernels.empty()) {
@@ -307,7 +354,7 @@ static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* i
     size_t descOff;
     const_bytes(pl, &descOff);
     return execute_passes(pl.kernels, c, nb, inX, inY, inStride, outX, outY, outStride, work, workElems,
-                          (const char*)dtab, 0, descOff, st, ev, nullptr);
+                          (const char*)dtab, 0, descOff, st, ev, nullptr, momScratch, momSlots, pl.nMomSlots);
 }
 
 static int ensure_work(DeviceCtx& c, size_t elems)
@@ -347,10 +394,15 @@ static void out_wfr(const Planner& pl, SRWLWfr* p)
     p->avgPhotEn = w.avgPhotEn;
 }
 
-static void out_moments(const Planner& pl, SRWLWfr* p)
+// output moments: the plan-time ones, or (with moment passes) the replayed bookkeeping with the
+// passes' result slots of one wavefront
+static void out_moments(const Planner& pl, SRWLWfr* p, const double* slots = nullptr)
 {
-    if (p->arMomX) for (int i = 0; i < 11; i++) p->arMomX[i] = pl.w.momX[i];
-    if (p->arMomY) for (int i = 0; i < 11; i++) p->arMomY[i] = pl.w.momZ[i];
+    double mx[11], mz[11];
+    if (pl.nMomSlots > 0 && slots != nullptr) pl.replay_moments(slots, mx, mz);
+    else for (int i = 0; i < 11; i++) { mx[i] = pl.w.momX[i]; mz[i] = pl.w.momZ[i]; }
+    if (p->arMomX) for (int i = 0; i < 11; i++) p->arMomX[i] = mx[i];
+    if (p->arMomY) for (int i = 0; i < 11; i++) p->arMomY[i] = mz[i];
 }
 
 }  // namespace srwg
@@ -364,8 +416,43 @@ struct srwgPlan {
     float2* dtab = nullptr;     // the plan's point-wise tables on that device
     size_t dtabElems = 0;
     bool tabReady = false;
-    ~srwgPlan() { if (dtab) cudaFree(dtab); }
+    double* dmom = nullptr;     // moment passes: result slots of every wavefront | scratch
+    size_t dmomDoubles = 0;
+    int lastN = 0;              // wavefronts of the last execution
+    cudaEvent_t momEv = nullptr;  // recorded after the last execution
+    ~srwgPlan()
+    {
+        if (dtab) cudaFree(dtab);
+        if (dmom) cudaFree(dmom);
+        if (momEv) cudaEventDestroy(momEv);
+    }
 };
+
+// moment buffers of a plan for n wavefronts; slots of wavefront b at dmom + b * nMomSlots * SLOT
+static int plan_moments(srwgPlan* plan, int n, double** slots, double** scratch)
+{
+    *slots = *scratch = nullptr;
+    if (plan->pl.nMomSlots == 0) return 0;
+    const size_t per = (size_t)plan->pl.nMomSlots * SRWG_MOM_SLOT;
+    int r = ensure_doubles(&plan->dmom, &plan->dmomDoubles, per * (size_t)n + mom_scratch_for(plan->pl));
+    if (r) return r;
+    if (plan->momEv == nullptr) CUDA_TRY(cudaEventCreateWithFlags(&plan->momEv, cudaEventDisableTiming));
+    *slots = plan->dmom;
+    *scratch = plan->dmom + per * (size_t)n;
+    return 0;
+}
+
+// result slots of wavefront b of the last execution (host copy); false when there are none
+static bool plan_slots(const srwgPlan* plan, int b, std::vector<double>& hs)
+{
+    if (plan->pl.nMomSlots == 0 || plan->lastN <= b || plan->dmom == nullptr || plan->momEv == nullptr) return false;
+    const size_t per = (size_t)plan->pl.nMomSlots * SRWG_MOM_SLOT;
+    hs.resize(per);
+    if (cudaSetDevice(plan->device) != cudaSuccess || cudaEventSynchronize(plan->momEv) != cudaSuccess ||
+        cudaMemcpy(hs.data(), plan->dmom + per * (size_t)b, per * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return false;
+    return true;
+}
 
 static int plan_bind(srwgPlan* plan, cudaStream_t st)
 {
@@ -452,8 +539,16 @@ int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SR
     else CUDA_TRY(cudaMemsetAsync(inY, 0, nIn * sizeof(float2), st));
     r = upload_tables(pl, &c->tab, &c->tabElems, st);
     if (r) return r;
-    r = execute(pl, *c, inX, inY, outX, outY, c->work, c->workElems, c->tab, st);
+    const size_t nSlotD = (size_t)pl.nMomSlots * SRWG_MOM_SLOT;
+    if (nSlotD) {
+        r = ensure_doubles(&c->mom, &c->momDoubles, nSlotD + mom_scratch_for(pl));
+        if (r) return r;
+    }
+    r = execute(pl, *c, inX, inY, outX, outY, c->work, c->workElems, c->tab, st, nullptr, 1, 0, 0,
+                nSlotD ? c->mom : nullptr, nSlotD ? c->mom + nSlotD : nullptr);
     if (r) return r;
+    std::vector<double> hs(nSlotD);
+    if (nSlotD) CUDA_TRY(cudaMemcpyAsync(hs.data(), c->mom, nSlotD * sizeof(double), cudaMemcpyDeviceToHost, st));
     bool hadX = pWfr->arEx != nullptr, hadY = pWfr->arEy != nullptr;
     bool resized = (pl.w.nx != pl.in.nx) || (pl.w.nz != pl.in.nz);
     out_wfr(pl, pWfr);
@@ -466,7 +561,7 @@ int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SR
     if (hadX && pWfr->arEx) CUDA_TRY(cudaMemcpyAsync(pWfr->arEx, outX, nOut * sizeof(float2), cudaMemcpyDeviceToHost, st));
     if (hadY && pWfr->arEy) CUDA_TRY(cudaMemcpyAsync(pWfr->arEy, outY, nOut * sizeof(float2), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    out_moments(pl, pWfr);
+    out_moments(pl, pWfr, nSlotD ? hs.data() : nullptr);
     return 0;
 }
 
@@ -497,7 +592,28 @@ int srwgPlanGetOutput(const srwgPlan* plan, SRWLWfr* pWfrOut)
 {
     if (plan == nullptr || pWfrOut == nullptr) return SRWG_ERR_BAD_ARG;
     out_wfr(plan->pl, pWfrOut);
-    out_moments(plan->pl, pWfrOut);
+    std::vector<double> hs;
+    const bool have = plan_slots(plan, 0, hs);
+    out_moments(plan->pl, pWfrOut, have ? hs.data() : nullptr);
+    return 0;
+}
+
+int srwgPlanGetMoments(const srwgPlan* plan, int index, double* momX, double* momY)
+{
+    if (plan == nullptr || index < 0) return SRWG_ERR_BAD_ARG;
+    double mx[11], mz[11];
+    if (plan->pl.nMomSlots == 0) {
+        for (int i = 0; i < 11; i++) { mx[i] = plan->pl.w.momX[i]; mz[i] = plan->pl.w.momZ[i]; }
+    } else {
+        std::vector<double> hs;
+        if (!plan_slots(plan, index, hs)) {
+            g_lastDetail = "no executed wavefront with this index";
+            return SRWG_ERR_BAD_ARG;
+        }
+        plan->pl.replay_moments(hs.data(), mx, mz);
+    }
+    if (momX) for (int i = 0; i < 11; i++) momX[i] = mx[i];
+    if (momY) for (int i = 0; i < 11; i++) momY[i] = mz[i];
     return 0;
 }
 
@@ -537,12 +653,20 @@ int srwgPlanExecuteBatch(srwgPlan* plan, int n, const float* dExIn, const float*
     while (chunk > 1 && 4 * (size_t)chunk * per > budget) chunk = (chunk + 1) / 2;
     r = ensure_work(c, (size_t)chunk * per);
     if (r) return r;
+    double *slots, *scratch;
+    r = plan_moments(plan, n, &slots, &scratch);
+    if (r) return r;
+    const size_t perSlots = (size_t)plan->pl.nMomSlots * SRWG_MOM_SLOT;
     for (int b0 = 0; b0 < n; b0 += chunk) {
         const int nb = std::min(chunk, n - b0);
         r = execute(plan->pl, c, (const float2*)(dExIn + b0 * strideIn), (const float2*)(dEyIn + b0 * strideIn),
                     (float2*)(dExOut + b0 * strideOut), (float2*)(dEyOut + b0 * strideOut), c.work, per, plan->dtab,
-                    st, nullptr, nb, strideIn / 2, strideOut / 2);
+                    st, nullptr, nb, strideIn / 2, strideOut / 2, slots ? slots + perSlots * b0 : nullptr, scratch);
         if (r) return r;
+    }
+    if (slots) {
+        CUDA_TRY(cudaEventRecord(plan->momEv, st));
+        plan->lastN = n;
     }
     return 0;
 }
@@ -561,8 +685,15 @@ int srwgPlanExecuteTimed(srwgPlan* plan, const float* dExIn, const float* dEyIn,
     const size_t nk = plan->pl.kernels.size();
     std::vector<cudaEvent_t> ev(2 * nk);
     for (auto& e : ev) CUDA_TRY(cudaEventCreate(&e));
-    r = execute(plan->pl, c, (const float2*)dExIn, (const float2*)dEyIn, (float2*)dExOut, (float2*)dEyOut, c.work,
-                c.workElems, plan->dtab, st, nk ? ev.data() : nullptr);
+    double *slots, *scratch;
+    r = plan_moments(plan, 1, &slots, &scratch);
+    if (r == 0)
+        r = execute(plan->pl, c, (const float2*)dExIn, (const float2*)dEyIn, (float2*)dExOut, (float2*)dEyOut, c.work,
+                    c.workElems, plan->dtab, st, nk ? ev.data() : nullptr, 1, 0, 0, slots, scratch);
+    if (r == 0 && slots) {
+        if (cudaEventRecord(plan->momEv, st) != cudaSuccess) r = SRWG_ERR_CUDA;
+        else plan->lastN = 1;
+    }
     if (r == 0) {
         CUDA_TRY(cudaStreamSynchronize(st));
         for (size_t i = 0; i < nk && (int)i < maxKernels; i++) {

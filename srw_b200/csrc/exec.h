@@ -17,6 +17,8 @@ struct DeviceCtx {
     size_t ioElems = 0;
     float2* tab = nullptr;              // point-wise tables of the one-shot entry point
     size_t tabElems = 0;
+    double* mom = nullptr;              // moment passes of the one-shot entry point: slots | scratch
+    size_t momDoubles = 0;
     cudaStream_t stream = nullptr;
 };
 std::mutex& library_mutex();                          // serialises the entry points
@@ -25,7 +27,8 @@ int device_twiddles(DeviceCtx& c, int N, const float2** out);
 int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, const float2* inX, const float2* inY,
                    long long inStride, float2* outX, float2* outY, long long outStride, float2* work, size_t workElems,
                    const char* dconst, long long constStride, size_t descOff, cudaStream_t st, cudaEvent_t* ev,
-                   const std::vector<KernelDesc>* hostMax);
+                   const std::vector<KernelDesc>* hostMax, double* momScratch = nullptr, double* momSlots = nullptr,
+                   int nSlots = 0);
 int line_config(const LineDesc& d, LineLaunch& p);   // launch shape of a line pass (capi.cpp)
 int radix_plan(int N, int* r);
 void set_last_detail(const std::string& s);          // detail text for srwlUtiGetErrText

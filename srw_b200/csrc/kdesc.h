@@ -7,7 +7,8 @@
 //     shared memory, runs up to two 1D FFTs along the line with point-wise work folded in
 //     between / before / after them, and stores the lines back;
 //   * RESIZE passes: the 16-point bicubic gather of RadResizeCore (sroptelm.cpp:3038);
-//   * PW passes: a standalone element-wise pass (only when nothing else can host the ops).
+//   * PW passes: a standalone element-wise pass (only when nothing else can host the ops);
+//   * MOM passes: read-only reductions for the statistical moments (no output field).
 // All point-wise work of the reference (drift transfer functions, quadratic phases, lens,
 // aperture masks, FFT centring sign/rotation, normalisation, shift tables, mirror) is expressed
 // by the structs below and applied inside those passes.
@@ -123,7 +124,24 @@ struct PwDesc {
     PwOps extra;
 };
 
-enum KernelKind { K_LINE = 1, K_RESIZE = 2, K_PW = 3 };
+// Statistical moments of the field (ComputeRadMoments, sroptelm.cpp:1608-2092), coordinate
+// representation: a read-only reduction of the field in buffer `src` after the point-wise work `pw`
+// (the operators still pending on it, and the removal of the wavefront's quadratic phase) into the
+// 22 weighted sums of one result slot.  The host turns the sums into moments after the run.
+struct MomDesc {
+    int nx, nz;
+    double xStart, xStep, zStart, zStep;       // physical mesh of the field
+    double ax, az;                             // 2 pi / (lambda R) * step, per axis
+    PwOps pw;
+    ChainTab t;                                // separable part of pw: tab over x, ltab over z
+    int has_extra;
+    PwOps extra;
+    int slot;
+};
+
+#define SRWG_MOM_SLOT 32   // doubles per result slot: 22 sums, 4 power-limit indices, status
+
+enum KernelKind { K_LINE = 1, K_RESIZE = 2, K_PW = 3, K_MOM = 4 };
 
 struct KernelDesc {
     int kind;
@@ -131,4 +149,5 @@ struct KernelDesc {
     LineDesc line;
     ResizeDesc rs;
     PwDesc pwk;
+    MomDesc mom;
 };

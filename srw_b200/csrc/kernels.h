@@ -68,6 +68,22 @@ struct PwLaunch {
     long long bSrc, bDst;    // per wavefront: source / destination field stride (float2)
 };
 
+// MOM pass (moments.cu): reduction of one field into the 22 sums of ComputeRadMoments.  For nb
+// wavefronts the passes run one wavefront after the other (scratch reused in stream order).
+struct MomLaunch {
+    MomDesc d;                 // host copy (launch shapes); the kernels read gd
+    const float2* src[2];
+    const float2* tabs;
+    const MomDesc* gd;
+    double* scratch;           // mom_scratch_doubles(nx, nz) doubles
+    double* out;               // result slot of wavefront 0 (SRWG_MOM_SLOT doubles)
+    int nb;
+    long long bDesc, bTab;     // per wavefront: descriptor stride (bytes), table stride (float2)
+    long long bSrc, bOut;      // per wavefront: field stride (float2), result stride (doubles)
+};
+size_t mom_scratch_doubles(int nx, int nz);
+cudaError_t launch_moments(const MomLaunch& p, cudaStream_t st);
+
 cudaError_t launch_line(const LineLaunch& p, cudaStream_t st);
 
 // power-of-two line pass kernels, one translation unit per line length (line2_<logn>.cu)

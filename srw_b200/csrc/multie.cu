@@ -321,6 +321,7 @@ extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* p
     m->useGraph = useGraph != 0;
     // sizes from the unshifted electron's plan
     Planner pl;
+    pl.numMoments = false;               // only the intensity is kept: no moment passes
     r = pl.plan(pBase, pOpt);
     if (r) { set_last_detail(pl.err); delete m; return r; }
     m->nIn = (size_t)m->nx * m->nz;
@@ -400,6 +401,7 @@ extern "C" SRWG_API int srwgMultiEAdd(srwgMultiE* m, int n, const double* arOffs
                     memset(&eps[k], 0, sizeof(ElecParams));
                     electron_wfr(*m, arOffsets + 4 * (size_t)(e + k), w, momX, momY, eps[k]);
                     pls[k] = Planner();
+                    pls[k].numMoments = false;
                     rcs[k] = pls[k].plan(&w, m->opt);
                 }
             };

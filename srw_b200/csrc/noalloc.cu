@@ -11,8 +11,13 @@
 //
 // Limits: the largest intermediate grid of the planned passes may hold at most
 // SRWG_STATIC_WORK_POINTS complex points (512 x 512), and the plan's constant data at most
-// SRWG_STATIC_CONST_POINTS float2 (1 MiB); larger propagations are rejected with
+// SRWG_STATIC_CONST_POINTS float2 (1 MiB), and the moment passes (result slots and scratch) at
+// most SRWG_STATIC_MOM_DOUBLES doubles (2 MiB); larger propagations are rejected with
 // SRWG_ERR_STATIC_LIMIT and a message giving the sizes.
+//
+// Where the propagation recomputes the statistical moments from the field (an aperture that clips
+// the beam, an obstacle) and pWfrOut has moment arrays, the call waits for the stream to finish
+// and reads the passes' result slots back; otherwise it returns without waiting.
 //
 // All calls share the array and it keeps the last call's contents.  Nothing has to start at
 // zero: every point a pass reads was written earlier in the same call (a resize that leaves the
@@ -26,6 +31,7 @@
 // device.  Make that first call before any stream capture.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -42,11 +48,12 @@
 
 #define SRWG_STATIC_WORK_POINTS (512 * 512)
 #define SRWG_STATIC_CONST_POINTS (128 * 1024)
-#define SRWG_STATIC_POINTS (4 * SRWG_STATIC_WORK_POINTS + SRWG_STATIC_CONST_POINTS)
+#define SRWG_STATIC_MOM_DOUBLES (256 * 1024)
+#define SRWG_STATIC_POINTS (4 * SRWG_STATIC_WORK_POINTS + SRWG_STATIC_CONST_POINTS + SRWG_STATIC_MOM_DOUBLES)
 
 namespace srwg {
 
-// [ work buffer A: Ex, Ey | work buffer B: Ex, Ey | constant data ]  (9 MiB)
+// [ work buffer A: Ex, Ey | work buffer B: Ex, Ey | constant data | moment slots and scratch ]  (11 MiB)
 static __device__ __align__(256) float2 g_static_scratch[SRWG_STATIC_POINTS];
 
 static std::mutex g_static_mutex;
@@ -118,6 +125,15 @@ extern "C" SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRW
                         std::to_string(SRWG_STATIC_CONST_POINTS));
         return SRWG_ERR_STATIC_LIMIT;
     }
+    const size_t nSlotD = (size_t)pl.nMomSlots * SRWG_MOM_SLOT;
+    size_t momNeed = 0;
+    for (const KernelDesc& k : pl.kernels)
+        if (k.kind == K_MOM) momNeed = std::max(momNeed, mom_scratch_doubles(k.mom.nx, k.mom.nz));
+    if (nSlotD + momNeed > SRWG_STATIC_MOM_DOUBLES) {
+        set_last_detail("the moment passes need " + std::to_string(nSlotD + momNeed) + " doubles, above the static limit of " +
+                        std::to_string(SRWG_STATIC_MOM_DOUBLES));
+        return SRWG_ERR_STATIC_LIMIT;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) { set_last_detail("cudaGetDevice failed"); return SRWG_ERR_NO_DEVICE; }
     float2* base = nullptr;
@@ -126,6 +142,7 @@ extern "C" SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRW
     cudaStream_t st = (cudaStream_t)stream;
     float2* work = base;
     float2* cdev = base + 4 * (size_t)SRWG_STATIC_WORK_POINTS;
+    double* mom = (double*)(cdev + SRWG_STATIC_CONST_POINTS);     // slots | scratch
     cudaError_t e = cudaMemcpyAsync(cdev, cst.data(), cst.size() * sizeof(float2), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) { set_last_detail(std::string("constant upload: ") + cudaGetErrorString(e)); return SRWG_ERR_CUDA; }
     const KernelDesc* gk = (const KernelDesc*)(cdev + descOff);
@@ -140,13 +157,30 @@ extern "C" SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRW
         e = cudaMemcpyAsync(outX, inX, nOut * sizeof(float2), cudaMemcpyDeviceToDevice, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(outY, inY, nOut * sizeof(float2), cudaMemcpyDeviceToDevice, st);
     }
+    // the last pass that writes a field writes the output; moment passes after it read the output
+    size_t lastField = nk;
+    for (size_t i = nk; i-- > 0;)
+        if (pl.kernels[i].kind != K_MOM) { lastField = i; break; }
+    if (nk > 0 && lastField == nk) { set_last_detail("plan without field passes"); return SRWG_ERR_BAD_ARG; }
     for (size_t i = 0; i < nk && e == cudaSuccess; i++) {
         const KernelDesc& k = pl.kernels[i];
-        const float2* s0 = k.src == 0 ? inX : wb[k.src][0];
-        const float2* s1 = k.src == 0 ? inY : wb[k.src][1];
-        float2* d0 = (i + 1 == nk) ? outX : wb[k.dst][0];
-        float2* d1 = (i + 1 == nk) ? outY : wb[k.dst][1];
-        if (k.kind == K_LINE) {
+        const bool fromOut = k.kind == K_MOM && k.src != 0 && i > lastField && k.src == pl.kernels[lastField].dst;
+        const float2* s0 = fromOut ? outX : k.src == 0 ? inX : wb[k.src][0];
+        const float2* s1 = fromOut ? outY : k.src == 0 ? inY : wb[k.src][1];
+        float2* d0 = (i == lastField) ? outX : wb[k.dst][0];
+        float2* d1 = (i == lastField) ? outY : wb[k.dst][1];
+        if (k.kind == K_MOM) {
+            MomLaunch p;
+            memset(&p, 0, sizeof(p));
+            p.d = k.mom;
+            p.src[0] = s0; p.src[1] = s1;
+            p.tabs = cdev;
+            p.gd = &gk[i].mom;
+            p.scratch = mom + nSlotD;
+            p.out = mom + (size_t)k.mom.slot * SRWG_MOM_SLOT;
+            p.nb = 1;
+            e = launch_moments(p, st);
+        } else if (k.kind == K_LINE) {
             LineLaunch p;
             memset(&p, 0, sizeof(p));
             r = line_config(k.line, p);
@@ -186,8 +220,18 @@ extern "C" SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRW
         pWfrOut->mesh.ne = 1; pWfrOut->mesh.nx = w.nx; pWfrOut->mesh.ny = w.nz;
         pWfrOut->Rx = w.RobsX; pWfrOut->Ry = w.RobsZ; pWfrOut->dRx = w.RobsXAbsErr; pWfrOut->dRy = w.RobsZAbsErr;
         pWfrOut->xc = w.xc; pWfrOut->yc = w.zc; pWfrOut->presCA = (char)w.Pres; pWfrOut->avgPhotEn = w.avgPhotEn;
-        if (pWfrOut->arMomX) for (int m = 0; m < 11; m++) pWfrOut->arMomX[m] = w.momX[m];
-        if (pWfrOut->arMomY) for (int m = 0; m < 11; m++) pWfrOut->arMomY[m] = w.momZ[m];
+        double mx[11], mz[11];
+        for (int m = 0; m < 11; m++) { mx[m] = w.momX[m]; mz[m] = w.momZ[m]; }
+        if (nSlotD && (pWfrOut->arMomX || pWfrOut->arMomY)) {
+            // moments recomputed from the field: wait for the passes and read their result slots
+            std::vector<double> hs(nSlotD);
+            e = cudaStreamSynchronize(st);
+            if (e == cudaSuccess) e = cudaMemcpy(hs.data(), mom, nSlotD * sizeof(double), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) { set_last_detail(std::string("moment read-back: ") + cudaGetErrorString(e)); return SRWG_ERR_CUDA; }
+            pl.replay_moments(hs.data(), mx, mz);
+        }
+        if (pWfrOut->arMomX) for (int m = 0; m < 11; m++) pWfrOut->arMomX[m] = mx[m];
+        if (pWfrOut->arMomY) for (int m = 0; m < 11; m++) pWfrOut->arMomY[m] = mz[m];
     }
     return 0;
 }

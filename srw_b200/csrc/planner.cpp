@@ -134,12 +134,38 @@ public:
         PwOps* p = ensure(w);
         double X0, DX, Z0, DZ;
         axis_map(w, X0, DX, Z0, DZ);
+        add_quad(p, X0, DX, Z0, DZ, ax, bx, az, bz, c);
+    }
+    static void add_quad(PwOps* p, double X0, double DX, double Z0, double DZ, double ax, double bx, double az,
+                         double bz, double c)
+    {
         p->has_quad = 1;
         p->Ai += ax * DX * DX;
         p->Bi += (2. * ax * X0 + bx) * DX;
         p->Aj += az * DZ * DZ;
         p->Bj += (2. * az * Z0 + bz) * DZ;
         p->C += ax * X0 * X0 + bx * X0 + az * Z0 * Z0 + bz * Z0 + c;
+    }
+    // read-only moment pass on the current field (index order = the logical mesh).  The operators
+    // still pending in an element-wise pass are applied on the fly by the moment pass, which runs
+    // just before that pass and reads its source; the element-wise pass stays open.
+    MomDesc& moments(const WfrState& w)
+    {
+        KernelDesc k;
+        memset(&k, 0, sizeof(k));
+        k.kind = K_MOM;
+        if (open >= 0 && open == (int)ks.size() - 1 && ks[open].kind == K_PW && !fx && !fz &&
+            !ks[open].pwk.mirror_x && !ks[open].pwk.mirror_z && ks[open].pwk.nx == w.nx && ks[open].pwk.nz == w.nz) {
+            k.src = k.dst = ks[open].src;
+            k.mom.pw = ks[open].pwk.pw;
+            ks.insert(ks.begin() + open, k);
+            open++;
+            return ks[open - 1].mom;
+        }
+        close();
+        k.src = k.dst = cur;
+        ks.push_back(k);
+        return ks.back().mom;
     }
     void ang(const WfrState& w, double c0, double c1, double cconst)
     {
@@ -446,18 +472,98 @@ static void mom_apply(double* m, const double ax[2][2], const double az[2][2])
     for (int i = 0; i < 3; i++) { double s = 0; for (int j = 0; j < 3; j++) s += bz[i][j] * v3[j]; m[8 + i] = s; }
 }
 
+static void apply_matrix_op(const MomOp& op, double* m)
+{
+    if (!op.clamp) { mom_apply(m, op.ax, op.az); return; }
+    if (m[0] == 0.) return;
+    mom_apply(m, op.ax, op.az);
+    if (m[5] - m[1] * m[1] < op.sx * op.sx) m[5] = op.sx * op.sx + m[1] * m[1];
+    if (m[8] - m[3] * m[3] < op.sz * op.sz) m[8] = op.sz * op.sz + m[3] * m[3];
+}
+
+void Planner::record_matrix(const double ax[2][2], const double az[2][2], int clamp, double sx, double sz)
+{
+    MomOp op;
+    op.kind = MOP_MATRIX;
+    memcpy(op.ax, ax, sizeof(op.ax));
+    memcpy(op.az, az, sizeof(op.az));
+    op.clamp = clamp; op.sx = sx; op.sz = sz;
+    momOps.push_back(op);
+    apply_matrix_op(op, w.momX);
+    apply_matrix_op(op, w.momZ);
+}
+
 void Planner::drift_moments(double L)
-{   // srTDriftSpace::PropagateRadMoments -> AuxPropagateRadMoments (sroptdrf.h:967, sroptdrf.cpp:22)
+{   // srTDriftSpace::PropagateRadMoments -> AuxPropagateRadMoments (sroptdrf.h:967, sroptdrf.cpp:22):
+    // drift matrices, then the rms sizes floored at the diffraction-limited spot
     const double a[2][2] = {{1., L}, {0., 1.}};
-    double* moms[2] = {w.momX, w.momZ};
+    record_matrix(a, a, 1, diff_lim_spot('x', L), diff_lim_spot('z', L));
+}
+
+// CheckIfMomentsShouldBeRecomputed of the rectangular / circular apertures (sroptapt.h:206, 384) on the
+// Ex and Ez moments, with the rms sizes of srTMomentsPtrs::ComputeCentralMoments (srstraux.h:357)
+static bool mom_outside(const double* mx, const double* mz, const MomOp& op)
+{
+    auto rms = [](const double* m, double& sx, double& sz) {
+        double Mxx = m[5] - m[1] * m[1], Mzz = m[8] - m[3] * m[3];
+        if (Mxx < 0.1 * m[5]) Mxx = 0.1 * m[5];
+        if (Mzz < 0.1 * m[8]) Mzz = 0.1 * m[8];
+        sx = ::sqrt(::fabs(Mxx)); sz = ::sqrt(::fabs(Mzz));
+    };
+    const double* ms[2] = {mx, mz};
     for (int c = 0; c < 2; c++) {
-        double* m = moms[c];
-        if (m[0] != 0.) {
-            mom_apply(m, a, a);
-            double sx = diff_lim_spot('x', L);
-            if (m[5] - m[1] * m[1] < sx * sx) m[5] = sx * sx + m[1] * m[1];
-            double sz = diff_lim_spot('z', L);
-            if (m[8] - m[3] * m[3] < sz * sz) m[8] = sz * sz + m[3] * m[3];
+        const double* m = ms[c];
+        double sx, sz;
+        rms(m, sx, sz);
+        sx *= 1.7; sz *= 1.7;
+        if (((m[1] - sx) < (op.cx - op.hx)) || ((m[1] + sx) > (op.cx + op.hx)) || ((m[3] - sz) < (op.cz - op.hz)) ||
+            ((m[3] + sz) > (op.cz + op.hz)))
+            return true;
+    }
+    return false;
+}
+
+// the 22 sums of a MOM pass normalised into the 11 moments of Ex and of Ez, each rounded to FP32 as
+// the reference stores them (sroptelm.cpp:1937-2080, coordinate representation)
+static void moments_from_sums(const double* S, const MomOp& op, double* mx, double* mz)
+{
+    const double FourPi = 3.141592653590 * 2. * 2.;
+    const double lam_d_4pi = 1.239842E-06 / (FourPi * op.eStart);
+    const double lam_d_2pi = 2. * lam_d_4pi, lam_d_2pi_e2 = lam_d_2pi * lam_d_2pi;
+    const double isx = 1. / op.xStep, isz = 1. / op.zStep;
+    const bool scx = op.nx > 1, scz = op.nz > 1;
+    auto f32 = [](double v) { return (double)(float)v; };
+    double* out[2] = {mx, mz};
+    for (int c = 0; c < 2; c++) {
+        const double* s = S + 11 * c;
+        double* m = out[c];
+        if (s[0] == 0.) { for (int i = 0; i < 11; i++) m[i] = 0.; continue; }
+        const double inv_n = 1. / s[0];
+        const double a = inv_n * lam_d_2pi, ax = a * isx, az = a * isz;
+        const double a2 = inv_n * lam_d_2pi_e2, ax2 = a2 * (isx * isx), az2 = a2 * (isz * isz);
+        m[0] = f32((scx && scz) ? s[0] * (op.xStep * op.zStep * 1.E+06) : 0.);
+        m[1] = f32(scx ? s[1] * inv_n : op.xStart);
+        m[2] = f32(scx ? s[2] * ax : 0.);
+        m[3] = f32(scz ? s[3] * inv_n : op.zStart);
+        m[4] = f32(scz ? s[4] * az : 0.);
+        m[5] = f32(scx ? s[5] * inv_n : op.xStart * op.xStart);
+        m[6] = f32(scx ? s[6] * ax : 0.);
+        m[7] = f32(scx ? s[7] * ax2 : 0.);
+        m[8] = f32(scz ? s[8] * inv_n : op.zStart * op.zStart);
+        m[9] = f32(scz ? s[9] * az : 0.);
+        m[10] = f32(scz ? s[10] * az2 : 0.);
+    }
+}
+
+void Planner::replay_moments(const double* slots, double* mx, double* mz) const
+{
+    for (int i = 0; i < 11; i++) { mx[i] = in.momX[i]; mz[i] = in.momZ[i]; }
+    for (const MomOp& op : momOps) {
+        if (op.kind == MOP_MATRIX) {
+            apply_matrix_op(op, mx);
+            apply_matrix_op(op, mz);
+        } else if (op.slot >= 0 && slots != nullptr && (op.obstacle || mom_outside(mx, mz, op))) {
+            moments_from_sums(slots + (size_t)op.slot * SRWG_MOM_SLOT, op, mx, mz);
         }
     }
 }
@@ -713,8 +819,7 @@ void Planner::lens(const ElemDesc& e)
     }
     const double ax[2][2] = {{1., 0.}, {-1. / e.Fx, 1.}};
     const double az[2][2] = {{1., 0.}, {-1. / e.Fy, 1.}};
-    mom_apply(w.momX, ax, az);
-    mom_apply(w.momZ, ax, az);
+    record_matrix(ax, az, 0, 0., 0.);
     const double dSmall = 1E-23;
     double difX = (e.Fx == w.RobsX) ? dSmall : e.Fx - w.RobsX;
     double difZ = (e.Fy == w.RobsZ) ? dSmall : e.Fy - w.RobsZ;
@@ -743,28 +848,47 @@ void Planner::aperture(const ElemDesc& e)
         double R = 0.5 * e.Dx;
         b->mask(w, 2, obstacle, e.x, e.y, 0., 0., R * R);
     }
-    // PropagateRadMoments: the reference recomputes the moments numerically (ComputeRadMoments)
-    // when 1.7 sigma of the beam is not inside the opening (always for obstacles); flagged here.
+    // srTAperture::PropagateRadMoments (sroptapt.cpp:248-350): the moments are recomputed from the
+    // masked field (ComputeRadMoments) when 1.7 sigma of the beam is not inside the opening, always
+    // for obstacles.  A MOM pass measures the field whenever the answer may be yes: the check itself
+    // is replayed on the host after the run (earlier recomputations make plan-time moments provisional).
     {
-        double* mx = w.momX; double* mz = w.momZ;
-        auto central = [](const double* m, double& sxx, double& szz) {
-            double Mxx = m[5] - m[1] * m[1], Mzz = m[8] - m[3] * m[3];
-            if (Mxx < 0.1 * m[5]) Mxx = 0.1 * m[5];
-            if (Mzz < 0.1 * m[8]) Mzz = 0.1 * m[8];
-            sxx = ::sqrt(::fabs(Mxx)); szz = ::sqrt(::fabs(Mzz));
-        };
-        double sxX, szX, sxZ, szZ;
-        central(mx, sxX, szX);
-        central(mz, sxZ, szZ);
-        bool recompute = true;
-        if (!obstacle) {
-            double hx = (e.shape == 'r') ? 0.5 * e.Dx : 0.5 * e.Dx, hz = (e.shape == 'r') ? 0.5 * e.Dy : 0.5 * e.Dx;
-            recompute = ((mx[1] - 1.7 * sxX) < (e.x - hx)) || ((mx[1] + 1.7 * sxX) > (e.x + hx)) ||
-                        ((mx[3] - 1.7 * szX) < (e.y - hz)) || ((mx[3] + 1.7 * szX) > (e.y + hz)) ||
-                        ((mz[1] - 1.7 * sxZ) < (e.x - hx)) || ((mz[1] + 1.7 * sxZ) > (e.x + hx)) ||
-                        ((mz[3] - 1.7 * szZ) < (e.y - hz)) || ((mz[3] + 1.7 * szZ) > (e.y + hz));
+        MomOp op;
+        op.kind = MOP_APERTURE;
+        op.obstacle = obstacle;
+        op.cx = e.x; op.cz = e.y;
+        op.hx = 0.5 * e.Dx;
+        op.hz = (e.shape == 'r') ? 0.5 * e.Dy : 0.5 * e.Dx;
+        const bool recompute = obstacle || mom_outside(w.momX, w.momZ, op);
+        if ((recompute || momProvisional) && numMoments) {
+            op.slot = nMomSlots++;
+            op.nx = w.nx; op.nz = w.nz; op.eStart = w.eStart;
+            op.xStart = w.xStart; op.xStep = w.xStep; op.zStart = w.zStart; op.zStep = w.zStep;
+            MomDesc& d = b->moments(w);
+            d.nx = w.nx; d.nz = w.nz;
+            d.xStart = w.xStart; d.xStep = w.xStep; d.zStart = w.zStart; d.zStep = w.zStep;
+            d.slot = op.slot;
+            // WaveFrontTermCanBeTreated (sroptelm.cpp:4692) and TreatStronglyOscillatingTerm 'r' (:4774):
+            // the quadratic phase of the wavefront radius about (xc, zc) comes off before the sums (the
+            // reference adds it back after, so the field itself is unchanged)
+            const bool qx = ::fabs(w.RobsXAbsErr) < 0.4 * ::fabs(w.RobsX);
+            const bool qz = ::fabs(w.RobsZAbsErr) < 0.4 * ::fabs(w.RobsZ);
+            w.QuadX = qx; w.QuadZ = qz;
+            if (qx || qz) {
+                const double Const = 3.14159265358979 * 1.E+06 / 1.23984186;
+                const double cx = qx ? -Const / w.RobsX * w.eStart : 0., cz = qz ? -Const / w.RobsZ * w.eStart : 0.;
+                Builder::add_quad(&d.pw, w.xStart, w.xStep, w.zStart, w.zStep, cx, -2. * cx * w.xc, cz, -2. * cz * w.zc,
+                                  cx * w.xc * w.xc + cz * w.zc * w.zc);
+            }
+            // 2 pi / (lambda R) * step with the reference's constants (R = 100 lambda when 0)
+            const double FourPi = 3.141592653590 * 2. * 2.;
+            const double lam_d_4pi = 1.239842E-06 / (FourPi * w.eStart), lam = lam_d_4pi * FourPi;
+            const double Rx = (w.RobsX != 0.) ? w.RobsX : 100. * lam, Rz = (w.RobsZ != 0.) ? w.RobsZ : 100. * lam;
+            d.ax = 0.5 * (w.xStep * ((1. / lam_d_4pi) / Rx));
+            d.az = 0.5 * (w.zStep * ((1. / lam_d_4pi) / Rz));
+            momProvisional = true;
         }
-        if (recompute) w.momentsStale = true;
+        momOps.push_back(op);
     }
     if (e.apob == 'a') {     // SetNewNonZeroWfrLimits of the apertures
         double hx = (e.shape == 'r') ? 0.5 * e.Dx : 0.5 * e.Dx;
@@ -957,6 +1081,9 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
     kernels.clear();
     maxElems = 0;
     err.clear();
+    momOps.clear();
+    nMomSlots = 0;
+    momProvisional = false;
     if (pw == nullptr || opt == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
     // InSRWRadPtrs (srradstr.cpp:501)
     const SRWLRadMesh& m = pw->mesh;
@@ -1098,6 +1225,9 @@ std::string Planner::describe() const
             snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pre=%d pw=%d tile=%dx%d  buf %d->%d\n", i,
                      k.rs.nxo, k.rs.nzo, k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pre, k.rs.has_pw, k.rs.tile_or,
                      k.rs.tile_oc, k.src, k.dst);
+        } else if (k.kind == K_MOM) {
+            snprintf(buf, sizeof(buf), "%zu MOM %dx%d (q%d a%d m%d s%d) slot=%d  buf %d\n", i, k.mom.nx, k.mom.nz,
+                     k.mom.pw.has_quad, k.mom.pw.has_ang, k.mom.pw.nmask, k.mom.pw.has_scale, k.mom.slot, k.src);
         } else {
             snprintf(buf, sizeof(buf), "%zu PW %dx%d (q%d a%d m%d s%d) mirror=%d/%d  buf %d->%d\n", i, k.pwk.nx, k.pwk.nz,
                      k.pwk.pw.has_quad, k.pwk.pw.has_ang, k.pwk.pw.nmask, k.pwk.pw.has_scale, k.pwk.mirror_x,

@@ -26,8 +26,23 @@ struct WfrState {
     bool QuadX = false, QuadZ = false;
     double momX[11] = {0}, momZ[11] = {0};
     bool haveMom = false;
-    bool momentsStale = false;   // the reference would recompute them numerically (not done here)
 };
+
+// One step of the statistical-moment bookkeeping.  The steps are replayed on the host after the
+// passes ran, with the moments the reference recomputes from the field (ComputeRadMoments) taken
+// from the result slots of the MOM passes.
+struct MomOp {
+    int kind = 0;                      // MOP_MATRIX or MOP_APERTURE
+    double ax[2][2] = {{0}}, az[2][2] = {{0}};   // transfer matrices (lens, drift)
+    int clamp = 0;                     // drift: floor of the rms sizes at the diffraction limit
+    double sx = 0, sz = 0;
+    int obstacle = 0;                  // aperture: opening (centre, half sizes) for the 1.7 sigma check
+    double cx = 0, cz = 0, hx = 0, hz = 0;
+    int slot = -1;                     // result slot of the MOM pass (-1: no recomputation possible)
+    int nx = 0, nz = 0;                // mesh and photon energy of the recomputation
+    double eStart = 0, xStart = 0, xStep = 0, zStart = 0, zStep = 0;
+};
+enum { MOP_MATRIX = 1, MOP_APERTURE = 2 };
 
 enum ElemKind { E_DRIFT = 1, E_APERTURE = 2, E_LENS = 3 };
 
@@ -59,6 +74,13 @@ public:
     long long maxElems = 0;              // largest grid over all work buffers
     std::vector<float2> tables;          // separable point-wise tables of all passes (tables.cpp)
     std::string err;
+    bool numMoments = true;              // emit MOM passes where the reference recomputes the moments
+    int nMomSlots = 0;                   // MOM passes of the plan (result slots per wavefront)
+    std::vector<MomOp> momOps;
+
+    // the output moments from the input ones and the MOM passes' result slots (nMomSlots x
+    // SRWG_MOM_SLOT doubles; unused when nMomSlots == 0)
+    void replay_moments(const double* slots, double* momX, double* momZ) const;
 
     // flattens SRWLOptC (nested containers included) and plans; returns 0 or an SRW error number
     int plan(const SRWLWfr* wfr, const SRWLOptC* opt);
@@ -76,6 +98,8 @@ private:
     void drift_to_waist(const ElemDesc& e);
     int drift_quad(const ElemDesc& e, int subtype);
     void drift_moments(double L);
+    void record_matrix(const double ax[2][2], const double az[2][2], int clamp, double sx, double sz);
+    bool momProvisional = false;         // plan-time moments wait for a MOM pass's result
     void lens(const ElemDesc& e);
     void aperture(const ElemDesc& e);
     void phase_lin_subtract(double newXc, double newZc);

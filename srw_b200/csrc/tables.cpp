@@ -251,6 +251,14 @@ void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& T)
                     r.tile_oc = ec;
                 }
             }
+        } else if (k.kind == K_MOM) {
+            MomDesc& m = k.mom;
+            SepPart A, Lp;
+            cd scale;
+            m.has_extra = 0;
+            memset(&m.extra, 0, sizeof(m.extra));
+            separate(m.pw, 0, m.nx, m.nz, A, Lp, scale, m.extra, m.has_extra);
+            m.t = chain_table(T, m.nx, m.nz, 0, 0, 0., 1.f, &A, &Lp, scale, 0, 0, 0, 0.);
         } else {
             PwDesc& p = k.pwk;
             SepPart A, Lp;

@@ -46,6 +46,14 @@ class Plan(object):
                     Rx=self.out.Rx, Ry=self.out.Ry, dRx=self.out.dRx, dRy=self.out.dRy, xc=self.out.xc,
                     yc=self.out.yc, presCA=ord(self.out.presCA) if self.out.presCA else 0)
 
+    def moments(self, index=0):
+        """(momX, momY): the 11 + 11 output moments of wavefront `index` of the last execution (the
+        analytically propagated ones when the plan recomputes none from the field)."""
+        import numpy as np
+        mx, my = np.zeros(11), np.zeros(11)
+        capi.check(capi.lib().srwgPlanGetMoments(self._h, int(index), mx.ctypes.data, my.ctypes.data), 'moments')
+        return mx, my
+
     def new_output(self, batch=None):
         shape = (self.ny_out, self.nx_out) if batch is None else (batch, self.ny_out, self.nx_out)
         return (torch.empty(shape, dtype=torch.complex64, device=self.device),
@@ -92,6 +100,9 @@ class Plan(object):
                 nxo, nyo = f[2].split('x')
                 nxn, nyn = f[4].split('x')
                 out.append(('resize', int(nxo), int(nyo), int(nxn), int(nyn)))
+            elif f[1] == 'MOM':
+                nx, ny = f[2].split('x')
+                out.append(('moments', int(nx), int(ny)))
             else:
                 nx, ny = f[2].split('x')
                 out.append(('pw', int(nx), int(ny)))

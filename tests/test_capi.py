@@ -57,9 +57,12 @@ def test_planner_mesh_bit_exact(name):
 
 
 def test_pass_fusion_counts():
-    # C0: 2 angular drifts around aperture+lens -> 5 passes; C1: resize (+ the aperture and the
-    # quadratic-term removal before it, + the lens after it), to-waist rows + columns -> 3
-    assert plan_case('c0_64')[0].n_kernels == 5
+    # C0: 2 angular drifts around aperture+lens -> 5 passes, but the aperture clips the beam: the
+    # moments are measured on the masked field (a moment pass), so the lens starts a new row pass
+    # -> 6 field passes + 1 moment pass; C1: resize (+ the aperture and the quadratic-term removal
+    # before it, + the lens after it), to-waist rows + columns -> 3
+    k = [x[0] for x in plan_case('c0_64')[0].kernels()]
+    assert len(k) == 7 and k.count('moments') == 1 and k.index('moments') == 3
     assert plan_case('c1_64')[0].n_kernels == 3
     assert plan_case('c2_128')[0].n_kernels == 5
 

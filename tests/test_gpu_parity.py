@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 from srw_b200 import srwlpy as srwl  # noqa: E402
 from srw_b200.plan import Plan  # noqa: E402
-from tests.golden_cases import case_io, load  # noqa: E402
+from tests.golden_cases import case_io, load, moment_err  # noqa: E402
 from tests.helpers import (C0, C0PP, C1, C1PP, C2, C2PP, beamline, fields, gaussian, make_wfr,  # noqa: E402
                            mesh_tuple, oracle_run, rel_l2)
 
@@ -52,6 +52,10 @@ def test_golden_case(name):
     assert rel_l2(np.abs(ex) ** 2 + np.abs(ey) ** 2, np.abs(o['ex']) ** 2 + np.abs(o['ey']) ** 2) < TOL
     if name not in MOMENT_RECOMPUTED:
         np.testing.assert_allclose(np.array(w.arMomX), o['momX'], rtol=1e-12)
+        np.testing.assert_allclose(np.array(w.arMomY), o['momY'], rtol=1e-12)
+    else:       # recomputed from the FP32 field: each moment to 1e-4 of its scale
+        assert moment_err(np.array(w.arMomX), o['momX']) < TOL
+        assert moment_err(np.array(w.arMomY), o['momY']) < TOL
 
 
 def full_case(which):

@@ -3,7 +3,7 @@
 It serves callers that cannot allocate device memory while they run (memory reserved once at
 start-up, or owned by the caller's own allocator): its intermediate fields live in a fixed array
 inside the library.  The test checks that it returns the same fields, mesh and scalars as the
-allocating entry point (srwgPlanCreate + srwgPlanExecute) on two calls in a row, alternating
+allocating entry point (srwgPlanCreate + srwgPlanExecute), moments included, on two calls in a row, alternating
 cases so that the second call of a case follows a different propagation in the shared array,
 and that a propagation above the array's limit is refused with a clear error.
 
@@ -56,10 +56,13 @@ def run_static(w, optC, ex, ey, nx_out, ny_out):
     ox = torch.full((ny_out, nx_out), float('nan'), dtype=torch.complex64, device='cuda')
     oy = torch.full((ny_out, nx_out), float('nan'), dtype=torch.complex64, device='cuda')
     res = capi.SRWLWfr()
+    moms = (np.zeros(11), np.zeros(11))
+    res.arMomX, res.arMomY = moms[0].ctypes.data, moms[1].ctypes.data
     st = torch.cuda.current_stream().cuda_stream
     r = capi.lib().srwgPropagElecFieldStatic(C.byref(cw), C.byref(co), ex.data_ptr(), ey.data_ptr(), ox.data_ptr(),
                                              oy.data_ptr(), ox.numel(), C.c_void_p(st), C.byref(res))
     torch.cuda.synchronize()
+    res.moms = moms
     return r, ox, oy, res
 
 
@@ -93,6 +96,10 @@ def test_static_matches_plan_twice():
                 [m['xStart'], m['xFin'], m['yStart'], m['yFin']]
             assert [res.Rx, res.Ry, res.dRx, res.dRy, res.xc, res.yc] == \
                 [m['Rx'], m['Ry'], m['dRx'], m['dRy'], m['xc'], m['yc']]
+            # moments (recomputed from the field for the aperture / obstacle cases)
+            mx, my = p.moments()
+            np.testing.assert_allclose(res.moms[0], mx, rtol=1e-6, atol=0)
+            np.testing.assert_allclose(res.moms[1], my, rtol=1e-6, atol=0)
 
 
 def test_static_refuses_above_limit():

@@ -435,7 +435,7 @@ def drift_quad(w: Wfr, L, treat, subtype):
         elif abs(effRz_p_L) < minAbsEffRz:
             trueRz = minAbsEffRz * (1. if effRz_p_L >= 0 else -1.) - L
     elif subtype == 1:
-        raise NotImplementedError("pp[3]=1 (moment-based radius estimate) is not restated")
+        trueRx, trueRz = estimate_rad_to_sub(w, L)
     if trueRx != 0:
         invRx = 1. / trueRx
         kx = (trueRx + L) * invRx
@@ -725,6 +725,65 @@ def _treat_strongly_oscillating(w: Wfr, add_or_rem):
     _apply_phase(w, ph)
 
 
+def _central_full(m):
+    """srTMomentsPtrs::ComputeCentralMoments (srstraux.h:357): (precCenMomIsOK, SqrtMxpxp,
+    SqrtMzpzp) of one component's 11 moments."""
+    Mxx = m[5] - m[1] * m[1]
+    Mxpxp = m[7] - m[2] * m[2]
+    Mzz = m[8] - m[3] * m[3]
+    Mzpzp = m[10] - m[4] * m[4]
+    ok = not (Mxx < 0 or Mxpxp < 0 or Mzz < 0 or Mzpzp < 0)
+    if Mxpxp < 0.1 * m[7]:
+        Mxpxp = 0.1 * m[7]
+    if Mzpzp < 0.1 * m[10]:
+        Mzpzp = 0.1 * m[10]
+    return ok, math.sqrt(abs(Mxpxp)), math.sqrt(abs(Mzpzp))
+
+
+def estimate_rad_to_sub(w: Wfr, L):
+    """srTDriftSpace::EstimateWfrRadToSub_AnalytTreatQuadPhaseTerm (sroptdrf.cpp:1123-1365), the
+    pp[3]=1 radius estimate from the rms divergence: the moments are recomputed from the field when
+    both norms are zero, or when the chosen component's central moments (as they stood before any
+    recomputation) are unusable."""
+    infLarge = 1E+23
+    coefAngRange = 0.2
+    fourPi = 4. * 3.14159265359
+    cX, cZ = _central_full(w.momX), _central_full(w.momZ)
+    s1X, s1Z = w.RobsX, w.RobsZ
+    s2X, s2Z = s1X + L, s1Z + L
+    if w.momX[0] == 0 and w.momZ[0] == 0:
+        compute_rad_moments(w)
+    use_x = w.momX[0] >= w.momZ[0]
+    c = cX if use_x else cZ
+    if (not c[0]) or c[1] == 0 or c[2] == 0:
+        compute_rad_moments(w)
+        c = _central_full(w.momX if use_x else w.momZ)
+    SigXp, SigZp = c[1], c[2]
+    if SigXp == 0 or SigZp == 0:
+        return (w.RobsX if w.RobsX != 0 else infLarge), (w.RobsZ if w.RobsZ != 0 else infLarge)
+    lambM = 1.239842E-06 / w.eStart
+
+    def one(s1, s2, sig):
+        ap = coefAngRange * sig
+        smin = lambM / (fourPi * ap * ap)
+        Rmin = 2 * smin
+        if abs(s1) < smin:
+            if abs(s2) < smin:
+                if abs(s1) < abs(s2):
+                    return Rmin if L > 0 else -Rmin
+                return (-Rmin - L) if L > 0 else (Rmin - L)
+            return Rmin if L > 0 else -Rmin
+        eff = s1 + smin * smin / s1
+        eff_p_L = eff + L
+        minRmin = 0.007 * abs(eff)
+        if Rmin < minRmin:
+            Rmin = minRmin
+        if abs(eff_p_L) < Rmin:
+            eff = (-Rmin - L) if eff_p_L < 0 else (Rmin - L)
+        return eff
+    return one(s1X, s2X, SigXp), one(s1Z, s2Z, SigZp)
+
+
 def central_moments(m):
     """srTMomentsPtrs::ComputeCentralMoments (srstraux.h:357): (sqrt Mxx, sqrt Mzz) with the 0.1
     safety floor on the central second moments."""
@@ -911,6 +970,8 @@ def compute_rad_moments(w: Wfr):
     power limits found on the intensity, then the sums normalised into w.momX / w.momZ."""
     if w.nx <= 1 and w.nz <= 1:
         return
+    if w.Pres != 0:
+        raise NotImplementedError("moments of a wavefront in the angular representation are not restated")
     ex, ey = w.ex, w.ey
     if w.Pres == 0 and _wavefront_term_can_be_treated(w):
         save = (w.ex, w.ey)

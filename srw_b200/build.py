@@ -26,10 +26,23 @@ def _run(cmd):
     return r.stdout + r.stderr
 
 
+def _includes(path, seen):
+    """The source and every project header it includes, transitively (quoted includes)."""
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for line in f:
+            t = line.strip()
+            if t.startswith('#include "'):
+                _includes(os.path.normpath(os.path.join(os.path.dirname(path), t.split('"')[1])), seen)
+    return seen
+
+
 def _compile(s, ptxas_info):
     src = os.path.join(CSRC, s)
     obj = os.path.join(OBJ_DIR, s + '.o')
-    deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith(('.h', '.cuh'))]
+    deps = sorted(_includes(src, set()))
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps) and not ptxas_info:
         return obj, ''
     cmd = [NVCC, '-c', '-O3', '-std=c++17', '-lineinfo', '-Xcompiler', HOST_FLAGS, '--fmad=true'] + ARCH + \

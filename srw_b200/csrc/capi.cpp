@@ -240,10 +240,7 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
     size_t lastField = nk;
     for (size_t i = nk; i-- > 0;)
         if (ks[i].kind != K_MOM) { lastField = i; break; }
-    if (lastField == nk && nk > 0) {        // a moment pass always comes with the pass of its mask
-        g_lastDetail = "plan without field passes";
-        return SRWG_ERR_BAD_ARG;
-    }
+
     for (size_t i = 0; i < nk; i++) {
         const KernelDesc& k = hostMax ? (*hostMax)[i] : ks[i];
         if (ev) CUDA_TRY(cudaEventRecord(ev[2 * i], st));
@@ -342,14 +339,16 @@ static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* i
                    double* momScratch = nullptr)
 {
     const size_t nOut = (size_t)pl.w.nx * pl.w.nz;
-    if (pl.kernels.empty()) {
+    bool anyField = false;
+    for (const KernelDesc& k : pl.kernels) anyField |= (k.kind != K_MOM);
+    if (!anyField) {          // the output is the input (moment passes, if any, read the input)
         for (int b = 0; b < nb; b++) {
             CUDA_TRY(cudaMemcpyAsync(outX + b * outStride, inX + b * inStride, nOut * sizeof(float2),
                                      cudaMemcpyDeviceToDevice, st));
             CUDA_TRY(cudaMemcpyAsync(outY + b * outStride, inY + b * inStride, nOut * sizeof(float2),
                                      cudaMemcpyDeviceToDevice, st));
         }
-        return 0;
+        if (pl.kernels.empty()) return 0;
     }
     size_t descOff;
     const_bytes(pl, &descOff);
@@ -502,6 +501,81 @@ int srwlUtiGetErrText(char* t, int erNo)
     return 0;
 }
 
+// srwlPropagElecField for a plan with stage boundaries (an element planned on moments measured from
+// the field): each stage runs from the previous stage's output into a stage buffer, its moment
+// results come back to the host, and planning resumes; the last stage's output is the result
+static int propagate_staged(Planner& pl, SRWLWfr* pWfr, int dev)
+{
+    int pr = SRWG_NEED_STAGE;           // planning status: the plan stopped at a stage boundary
+    DeviceCtx* c = nullptr;
+    int r = device_ctx(dev, &c);
+    if (r) return r;
+    cudaStream_t st = c->stream;
+    const size_t nIn = (size_t)pl.in.nx * pl.in.nz;
+    r = ensure_io(*c, nIn);
+    if (r) return r;
+    if (pWfr->arEx) CUDA_TRY(cudaMemcpyAsync(c->io, pWfr->arEx, nIn * sizeof(float2), cudaMemcpyHostToDevice, st));
+    else CUDA_TRY(cudaMemsetAsync(c->io, 0, nIn * sizeof(float2), st));
+    if (pWfr->arEy) CUDA_TRY(cudaMemcpyAsync(c->io + c->ioElems, pWfr->arEy, nIn * sizeof(float2), cudaMemcpyHostToDevice, st));
+    else CUDA_TRY(cudaMemsetAsync(c->io + c->ioElems, 0, nIn * sizeof(float2), st));
+    const float2* curX = c->io;
+    const float2* curY = c->io + c->ioElems;
+    float2 *oX = nullptr, *oY = nullptr;
+    std::vector<double> slots, tmp;
+    for (int k = 0;; k++) {
+        const bool last = (pr == 0);
+        const size_t nSt = (size_t)pl.w.nx * pl.w.nz;
+        float2*& sb = c->stg[k & 1];
+        size_t& se = c->stgElems[k & 1];
+        if (sb == nullptr || se < nSt) {
+            if (sb) cudaFree(sb);
+            sb = nullptr; se = 0;
+            CUDA_TRY(cudaMalloc(&sb, 2 * nSt * sizeof(float2)));
+            se = nSt;
+        }
+        oX = sb; oY = sb + se;
+        r = ensure_work(*c, (size_t)std::max<long long>(pl.maxElems, 1));
+        if (r) return r;
+        r = upload_tables(pl, &c->tab, &c->tabElems, st);
+        if (r) return r;
+        const size_t nSlotD = (size_t)pl.nMomSlots * SRWG_MOM_SLOT;
+        if (nSlotD) {
+            r = ensure_doubles(&c->mom, &c->momDoubles, nSlotD + mom_scratch_for(pl));
+            if (r) return r;
+        }
+        r = execute(pl, *c, curX, curY, oX, oY, c->work, c->workElems, c->tab, st, nullptr, 1, 0, 0,
+                    nSlotD ? c->mom : nullptr, nSlotD ? c->mom + nSlotD : nullptr);
+        if (r) return r;
+        tmp.assign(nSlotD, 0.);
+        if (nSlotD) CUDA_TRY(cudaMemcpyAsync(tmp.data(), c->mom, nSlotD * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        slots.resize(nSlotD, 0.);
+        for (const KernelDesc& kd : pl.kernels)          // the slots this stage's passes wrote
+            if (kd.kind == K_MOM)
+                std::copy(tmp.begin() + (size_t)kd.mom.slot * SRWG_MOM_SLOT,
+                          tmp.begin() + (size_t)(kd.mom.slot + 1) * SRWG_MOM_SLOT,
+                          slots.begin() + (size_t)kd.mom.slot * SRWG_MOM_SLOT);
+        if (last) break;
+        pr = pl.resume(slots.data());
+        if (pr && pr != SRWG_NEED_STAGE) { g_lastDetail = pl.err; return pr; }
+        curX = oX; curY = oY;
+    }
+    const size_t nOut = (size_t)pl.w.nx * pl.w.nz;
+    bool hadX = pWfr->arEx != nullptr, hadY = pWfr->arEy != nullptr;
+    bool resized = (pl.w.nx != pl.in.nx) || (pl.w.nz != pl.in.nz);
+    out_wfr(pl, pWfr);
+    if (resized) {
+        if (g_modifFunc == nullptr) return SRWL_WFR_EXT_FUNC_NOT_DEFINED;
+        if ((*g_modifFunc)(2, pWfr, 0)) return SRWL_WFR_EXT_MODIF_FAILED;
+        out_wfr(pl, pWfr);
+    }
+    if (hadX && pWfr->arEx) CUDA_TRY(cudaMemcpyAsync(pWfr->arEx, oX, nOut * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    if (hadY && pWfr->arEy) CUDA_TRY(cudaMemcpyAsync(pWfr->arEy, oY, nOut * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    out_moments(pl, pWfr, slots.empty() ? nullptr : slots.data());
+    return 0;
+}
+
 int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SRWLRadMesh* arIM, char** arI,
                         double* arParGPU)
 {
@@ -518,7 +592,9 @@ int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SR
     if (pWfr->arEx == nullptr && pWfr->arEy == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
 
     Planner pl;
+    pl.allowStages = true;
     int r = pl.plan(pWfr, pOpt);
+    if (r == SRWG_NEED_STAGE) return propagate_staged(pl, pWfr, dev);
     if (r) { g_lastDetail = pl.err; return r; }
     DeviceCtx* c = nullptr;
     r = device_ctx(dev, &c);

@@ -19,6 +19,8 @@ struct DeviceCtx {
     size_t tabElems = 0;
     double* mom = nullptr;              // moment passes of the one-shot entry point: slots | scratch
     size_t momDoubles = 0;
+    float2* stg[2] = {nullptr, nullptr};  // stage outputs of a staged propagation (2 components each)
+    size_t stgElems[2] = {0, 0};
     cudaStream_t stream = nullptr;
 };
 std::mutex& library_mutex();                          // serialises the entry points

@@ -9,7 +9,9 @@ namespace srwg {
 #define SRWG_LINE_SMEM_MAX (220 * 1024)
 
 // lines per CTA of the power-of-two line pass (line2_kernel): rows ~256 threads, columns up to
-// 1024 threads (at most 32 columns), within the shared-memory budget; pitch N + N/16 + 4 points
+// 1024 threads (at most 32 columns), within the shared-memory budget; pitch N + N/16 + 4 points.
+// (Column tiles of half the width, two CTAs per SM, measured slower: the row pass then writes
+// 16-byte pieces per row and column block, and the column pass's stores are half sectors.)
 inline int line2_lines_per_cta(int axis, int N)
 {
     const int T = N / 16;

@@ -555,6 +555,137 @@ static void moments_from_sums(const double* S, const MomOp& op, double* mx, doub
     }
 }
 
+// central moments as srTMomentsPtrs caches them (srstraux.h:357): usable flag, rms divergences
+struct CenMom { bool ok; double sxp, szp; };
+static CenMom cen_mom(const double* m)
+{
+    double Mxx = m[5] - m[1] * m[1], Mxpxp = m[7] - m[2] * m[2];
+    double Mzz = m[8] - m[3] * m[3], Mzpzp = m[10] - m[4] * m[4];
+    CenMom c;
+    c.ok = !((Mxx < 0) || (Mxpxp < 0) || (Mzz < 0) || (Mzpzp < 0));
+    if (Mxpxp < 0.1 * m[7]) Mxpxp = 0.1 * m[7];
+    if (Mzpzp < 0.1 * m[10]) Mzpzp = 0.1 * m[10];
+    c.sxp = ::sqrt(::fabs(Mxpxp)); c.szp = ::sqrt(::fabs(Mzpzp));
+    return c;
+}
+
+// the moment handling of EstimateWfrRadToSub_AnalytTreatQuadPhaseTerm (sroptdrf.cpp:1156-1213): the
+// moments are recomputed from the field when both norms are zero, or when the central moments of
+// the stronger component, as they were cached before any recomputation, are unusable; then the rms
+// divergences of that component.  S: the sums of the field (nullptr: none measured).  Returns false
+// when a recomputation is needed and S is nullptr.
+static bool estimate_moments(const MomOp& op, const double* S, double* mx, double* mz, double& sxp, double& szp)
+{
+    const CenMom cX = cen_mom(mx), cZ = cen_mom(mz);
+    if (mx[0] == 0. && mz[0] == 0.) {
+        if (S == nullptr) return false;
+        moments_from_sums(S, op, mx, mz);
+    }
+    const bool useX = mx[0] >= mz[0];
+    CenMom c = useX ? cX : cZ;
+    if (!c.ok || c.sxp == 0. || c.szp == 0.) {
+        if (S == nullptr) return false;
+        moments_from_sums(S, op, mx, mz);
+        c = cen_mom(useX ? mx : mz);
+    }
+    sxp = c.sxp; szp = c.szp;
+    return true;
+}
+
+// a MOM pass on the current field (ComputeRadMoments, sroptelm.cpp:1608) with the result slot of op
+void Planner::emit_moment_pass(MomOp& op)
+{
+    op.slot = nMomSlots++;
+    op.nx = w.nx; op.nz = w.nz; op.eStart = w.eStart;
+    op.xStart = w.xStart; op.xStep = w.xStep; op.zStart = w.zStart; op.zStep = w.zStep;
+    MomDesc& d = b->moments(w);
+    d.nx = w.nx; d.nz = w.nz;
+    d.xStart = w.xStart; d.xStep = w.xStep; d.zStart = w.zStart; d.zStep = w.zStep;
+    d.slot = op.slot;
+    // WaveFrontTermCanBeTreated (sroptelm.cpp:4692) and TreatStronglyOscillatingTerm 'r' (:4774): the
+    // quadratic phase of the wavefront radius about (xc, zc) comes off before the sums (the reference
+    // adds it back after, so the field itself is unchanged)
+    const bool qx = ::fabs(w.RobsXAbsErr) < 0.4 * ::fabs(w.RobsX);
+    const bool qz = ::fabs(w.RobsZAbsErr) < 0.4 * ::fabs(w.RobsZ);
+    w.QuadX = qx; w.QuadZ = qz;
+    if (qx || qz) {
+        const double Const = 3.14159265358979 * 1.E+06 / 1.23984186;
+        const double cx = qx ? -Const / w.RobsX * w.eStart : 0., cz = qz ? -Const / w.RobsZ * w.eStart : 0.;
+        Builder::add_quad(&d.pw, w.xStart, w.xStep, w.zStart, w.zStep, cx, -2. * cx * w.xc, cz, -2. * cz * w.zc,
+                          cx * w.xc * w.xc + cz * w.zc * w.zc);
+    }
+    // 2 pi / (lambda R) * step with the reference's constants (R = 100 lambda when 0)
+    const double FourPi = 3.141592653590 * 2. * 2.;
+    const double lam_d_4pi = 1.239842E-06 / (FourPi * w.eStart), lam = lam_d_4pi * FourPi;
+    const double Rx = (w.RobsX != 0.) ? w.RobsX : 100. * lam, Rz = (w.RobsZ != 0.) ? w.RobsZ : 100. * lam;
+    d.ax = 0.5 * (w.xStep * ((1. / lam_d_4pi) / Rx));
+    d.az = 0.5 * (w.zStep * ((1. / lam_d_4pi) / Rz));
+    momProvisional = true;
+}
+
+// EstimateWfrRadToSub_AnalytTreatQuadPhaseTerm (sroptdrf.cpp:1123-1365): the radius to subtract in
+// the pp[3]=1 drift, from the rms divergence.  When the moments it needs come from the field, the
+// field is measured here and the plan stops at a stage boundary; the element is planned again once
+// the measurement is back.
+void Planner::estimate_rad(double L, double& effRx, double& effRz)
+{
+    MomOp op;
+    op.kind = MOP_ESTIMATE;
+    const double* S = nullptr;
+    if (pendingEstSlot_ >= 0) {
+        op = pendingEstOp_;
+        S = slotVals_.data() + (size_t)op.slot * SRWG_MOM_SLOT;
+    } else {
+        double mx[11], mz[11], a, c;
+        memcpy(mx, w.momX, sizeof(mx));
+        memcpy(mz, w.momZ, sizeof(mz));
+        if (momProvisional || !estimate_moments(op, nullptr, mx, mz, a, c)) {
+            if (!allowStages || !numMoments || w.Pres != 0) {
+                err = "drift mode pp[3]=1 needs the moments of the field while planning: only "
+                      "srwlPropagElecField plans in stages";
+                throw (int)SRWG_ERR_UNSUPPORTED;
+            }
+            emit_moment_pass(op);
+            pendingEstSlot_ = op.slot;
+            pendingEstOp_ = op;
+            throw (int)SRWG_NEED_STAGE;
+        }
+    }
+    double SigXp = 0., SigZp = 0.;
+    estimate_moments(op, S, w.momX, w.momZ, SigXp, SigZp);
+    momOps.push_back(op);
+    pendingEstSlot_ = -1;
+    const double infLarge = 1E+23;
+    if ((SigXp == 0) || (SigZp == 0)) {
+        effRx = (w.RobsX != 0) ? w.RobsX : infLarge;
+        effRz = (w.RobsZ != 0) ? w.RobsZ : infLarge;
+        return;
+    }
+    const double coefAngRange = 0.2, fourPi = 4. * 3.14159265359;
+    const double lambM = 1.239842E-06 / w.eStart;
+    auto one = [&](double s1, double sig) {
+        const double s2 = s1 + L;
+        const double ap = coefAngRange * sig;
+        const double smin = lambM / (fourPi * ap * ap);
+        double Rmin = 2 * smin;
+        if (::fabs(s1) < smin) {
+            if (::fabs(s2) < smin) {
+                if (::fabs(s1) < ::fabs(s2)) return (L > 0) ? Rmin : -Rmin;
+                return (L > 0) ? (-Rmin - L) : (Rmin - L);
+            }
+            return (L > 0) ? Rmin : -Rmin;
+        }
+        double eff = s1 + smin * smin / s1;
+        const double eff_p_L = eff + L;
+        const double minRmin = 0.007 * (::fabs(eff));
+        if (Rmin < minRmin) Rmin = minRmin;
+        if (::fabs(eff_p_L) < Rmin) eff = (eff_p_L < 0) ? (-Rmin - L) : (Rmin - L);
+        return eff;
+    };
+    effRx = one(w.RobsX, SigXp);
+    effRz = one(w.RobsZ, SigZp);
+}
+
 void Planner::replay_moments(const double* slots, double* mx, double* mz) const
 {
     for (int i = 0; i < 11; i++) { mx[i] = in.momX[i]; mz[i] = in.momZ[i]; }
@@ -562,6 +693,10 @@ void Planner::replay_moments(const double* slots, double* mx, double* mz) const
         if (op.kind == MOP_MATRIX) {
             apply_matrix_op(op, mx);
             apply_matrix_op(op, mz);
+        } else if (op.kind == MOP_ESTIMATE) {
+            double a, c;
+            if (op.slot >= 0 && slots != nullptr)
+                estimate_moments(op, slots + (size_t)op.slot * SRWG_MOM_SLOT, mx, mz, a, c);
         } else if (op.slot >= 0 && slots != nullptr && (op.obstacle || mom_outside(mx, mz, op))) {
             moments_from_sums(slots + (size_t)op.slot * SRWG_MOM_SLOT, op, mx, mz);
         }
@@ -652,8 +787,7 @@ int Planner::drift_quad(const ElemDesc& e, int subtype)
         if (::fabs(trueRz) < minAbsEffRz) trueRz = minAbsEffRz * ((trueRz >= 0) ? 1. : -1.);
         else if (::fabs(effRz_p_L) < minAbsEffRz) trueRz = minAbsEffRz * ((effRz_p_L >= 0) ? 1. : -1.) - L;
     } else if (subtype == 1) {
-        err = "drift mode pp[3]=1 (moment-based radius estimate) is not supported on the GPU path";
-        return SRWG_ERR_UNSUPPORTED;
+        estimate_rad(L, trueRx, trueRz);
     }
     if (trueRx != 0) {
         invRx = 1. / trueRx;
@@ -860,34 +994,7 @@ void Planner::aperture(const ElemDesc& e)
         op.hx = 0.5 * e.Dx;
         op.hz = (e.shape == 'r') ? 0.5 * e.Dy : 0.5 * e.Dx;
         const bool recompute = obstacle || mom_outside(w.momX, w.momZ, op);
-        if ((recompute || momProvisional) && numMoments) {
-            op.slot = nMomSlots++;
-            op.nx = w.nx; op.nz = w.nz; op.eStart = w.eStart;
-            op.xStart = w.xStart; op.xStep = w.xStep; op.zStart = w.zStart; op.zStep = w.zStep;
-            MomDesc& d = b->moments(w);
-            d.nx = w.nx; d.nz = w.nz;
-            d.xStart = w.xStart; d.xStep = w.xStep; d.zStart = w.zStart; d.zStep = w.zStep;
-            d.slot = op.slot;
-            // WaveFrontTermCanBeTreated (sroptelm.cpp:4692) and TreatStronglyOscillatingTerm 'r' (:4774):
-            // the quadratic phase of the wavefront radius about (xc, zc) comes off before the sums (the
-            // reference adds it back after, so the field itself is unchanged)
-            const bool qx = ::fabs(w.RobsXAbsErr) < 0.4 * ::fabs(w.RobsX);
-            const bool qz = ::fabs(w.RobsZAbsErr) < 0.4 * ::fabs(w.RobsZ);
-            w.QuadX = qx; w.QuadZ = qz;
-            if (qx || qz) {
-                const double Const = 3.14159265358979 * 1.E+06 / 1.23984186;
-                const double cx = qx ? -Const / w.RobsX * w.eStart : 0., cz = qz ? -Const / w.RobsZ * w.eStart : 0.;
-                Builder::add_quad(&d.pw, w.xStart, w.xStep, w.zStart, w.zStep, cx, -2. * cx * w.xc, cz, -2. * cz * w.zc,
-                                  cx * w.xc * w.xc + cz * w.zc * w.zc);
-            }
-            // 2 pi / (lambda R) * step with the reference's constants (R = 100 lambda when 0)
-            const double FourPi = 3.141592653590 * 2. * 2.;
-            const double lam_d_4pi = 1.239842E-06 / (FourPi * w.eStart), lam = lam_d_4pi * FourPi;
-            const double Rx = (w.RobsX != 0.) ? w.RobsX : 100. * lam, Rz = (w.RobsZ != 0.) ? w.RobsZ : 100. * lam;
-            d.ax = 0.5 * (w.xStep * ((1. / lam_d_4pi) / Rx));
-            d.az = 0.5 * (w.zStep * ((1. / lam_d_4pi) / Rz));
-            momProvisional = true;
-        }
+        if ((recompute || momProvisional) && numMoments) emit_moment_pass(op);
         momOps.push_back(op);
     }
     if (e.apob == 'a') {     // SetNewNonZeroWfrLimits of the apertures
@@ -1079,11 +1186,17 @@ int Planner::resize(double pxm, double pxd, double pzm, double pzd, int shift, d
 int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
 {
     kernels.clear();
+    tables.clear();
     maxElems = 0;
     err.clear();
     momOps.clear();
     nMomSlots = 0;
     momProvisional = false;
+    nStages = 0;
+    slotVals_.clear();
+    pendingEstSlot_ = -1;
+    elemIdx_ = 0;
+    resizeDone_ = false;
     if (pw == nullptr || opt == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
     // InSRWRadPtrs (srradstr.cpp:501)
     const SRWLRadMesh& m = pw->mesh;
@@ -1106,19 +1219,42 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
     if (pw->presFT != 0) { err = "time-domain wavefronts are not supported on the GPU path"; return SRWG_ERR_UNSUPPORTED; }
     if (pw->numTypeElFld != 0 && pw->numTypeElFld != 'f') { err = "only float fields are supported"; return SRWG_ERR_UNSUPPORTED; }
     in = w;
-    std::vector<ElemDesc> els;
-    std::vector<PropDesc> props;
-    int r = flatten(opt, els, props, false);
+    stageIn = w;
+    els_.clear();
+    props_.clear();
+    int r = flatten(opt, els_, props_, false);
     if (r) return r;
     if ((w.nx <= 1) || (w.nz <= 1)) return CAN_NOT_PROPAGATE_1D_RAD;   // CheckRadStructForPropagation
+    return run();
+}
 
+int Planner::resume(const double* slots)
+{
+    // moments as they stand after the stage: the bookkeeping replayed with every result so far
+    slotVals_.assign(slots, slots + (size_t)nMomSlots * SRWG_MOM_SLOT);
+    replay_moments(slotVals_.data(), w.momX, w.momZ);
+    momProvisional = false;
+    kernels.clear();
+    tables.clear();
+    maxElems = 0;
+    stageIn = w;
+    nStages++;
+    return run();
+}
+
+// plans the chain from the element reached; a stage boundary (SRWG_NEED_STAGE) leaves a complete
+// pass list behind and the element to be planned again on resume (its pre-resize already done)
+int Planner::run()
+{
     Builder bld(kernels, maxElems);
     b = &bld;
     const double tolRes = 1.e-04;
+    const std::vector<ElemDesc>& els = els_;
+    const std::vector<PropDesc>& props = props_;
     try {
         size_t numRes = props.size();
-        size_t i = 0;
-        for (; i < els.size(); i++) {
+        size_t& i = elemIdx_;
+        for (; i < els.size(); i++, resizeDone_ = false) {
             const ElemDesc& e = els[i];
             int anal = 0;
             if (i < numRes) {
@@ -1131,11 +1267,12 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
                     anal = (int)p.get(3, 0);
                     double pxm = p.get(5, 1.), pxd = p.get(6, 1.), pzm = p.get(7, 1.), pzd = p.get(8, 1.);
                     int sh = (int)(char)p.get(9, 0);
-                    if ((::fabs(pxd - 1.) > tolRes) || (::fabs(pxm - 1.) > tolRes) || (::fabs(pzd - 1.) > tolRes) ||
-                        (::fabs(pzm - 1.) > tolRes) || (sh > 0)) {
+                    if (!resizeDone_ && ((::fabs(pxd - 1.) > tolRes) || (::fabs(pxm - 1.) > tolRes) ||
+                                         (::fabs(pzd - 1.) > tolRes) || (::fabs(pzm - 1.) > tolRes) || (sh > 0))) {
                         int rr = resize(pxm, pxd, pzm, pzd, sh, p.get(10, 0.), p.get(11, 0.), (int)p.get(4, 0) != 0);
                         if (rr) throw rr;
                     }
+                    resizeDone_ = true;
                 }
             }
             if (e.kind == E_DRIFT) drift(e, anal);
@@ -1152,12 +1289,25 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
             }
         }
     } catch (int code) {
+        if (code != SRWG_NEED_STAGE) {
+            b = nullptr;
+            return code;
+        }
+        bld.close();
+        outBuf = bld.cur;
         b = nullptr;
-        return code;
+        int r = finalize();
+        return r ? r : SRWG_NEED_STAGE;
     }
     bld.close();
     outBuf = bld.cur;
     b = nullptr;
+    return finalize();
+}
+
+// checks the passes of the plan (or stage), fills their tables and links neighbouring passes
+int Planner::finalize()
+{
     // the GPU passes need even line lengths (centring rotation) and at most 16384 points per line
     for (const KernelDesc& k : kernels) {
         if (k.kind == K_LINE) {

@@ -42,7 +42,12 @@ struct MomOp {
     int nx = 0, nz = 0;                // mesh and photon energy of the recomputation
     double eStart = 0, xStart = 0, xStep = 0, zStart = 0, zStep = 0;
 };
-enum { MOP_MATRIX = 1, MOP_APERTURE = 2 };
+enum { MOP_MATRIX = 1, MOP_APERTURE = 2, MOP_ESTIMATE = 3 };
+
+// Planner::plan / resume: the plan stops at a stage boundary (its passes so far are complete and
+// must run before planning can go on, because the next element depends on moments measured from
+// the field)
+#define SRWG_NEED_STAGE (-77)
 
 enum ElemKind { E_DRIFT = 1, E_APERTURE = 2, E_LENS = 3 };
 
@@ -82,12 +87,30 @@ public:
     // SRWG_MOM_SLOT doubles; unused when nMomSlots == 0)
     void replay_moments(const double* slots, double* momX, double* momZ) const;
 
-    // flattens SRWLOptC (nested containers included) and plans; returns 0 or an SRW error number
+    // flattens SRWLOptC (nested containers included) and plans; returns 0, an SRW error number, or
+    // (with allowStages) SRWG_NEED_STAGE: `kernels` then hold a complete stage, which must run on
+    // the field before resume() plans on with the stage's moment results
     int plan(const SRWLWfr* wfr, const SRWLOptC* opt);
+    // slots: the result slots of every MOM pass so far (nMomSlots x SRWG_MOM_SLOT doubles)
+    int resume(const double* slots);
     std::string describe() const;
+    bool allowStages = false;            // staged planning (the one-shot entry point only)
+    int nStages = 0;                     // stage boundaries passed
+    WfrState stageIn;                    // mesh of the current stage's input
 
 private:
     Builder* b = nullptr;
+    std::vector<ElemDesc> els_;          // the flattened chain and the element reached
+    std::vector<PropDesc> props_;
+    size_t elemIdx_ = 0;
+    bool resizeDone_ = false;            // the current element's pre-resize is planned
+    std::vector<double> slotVals_;       // host copy of the result slots of completed stages
+    int pendingEstSlot_ = -1;            // MOM pass of a pp[3]=1 radius estimate waiting for its stage
+    MomOp pendingEstOp_;
+    int run();
+    int finalize();
+    void emit_moment_pass(MomOp& op);
+    void estimate_rad(double L, double& effRx, double& effRz);
     int flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vector<PropDesc>& props, bool nested);
     void set_full_range();
     void srwl_roundtrip();

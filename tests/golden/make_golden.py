@@ -151,8 +151,28 @@ def cases(L):
                                              ('drift', 12., 0)], [pp(), pp(), pp(4)]),
         ('quad_neg_k', g2(96, 0.5e-3), [('drift', -45., 0)], [pp(2)]),
         ('treat_path', g0(64), [('drift', 2., 1)], [pp()]),
+        # pp[3]=1: radius estimate from the rms divergence, on analytic moments, on moments an
+        # aperture recomputed, and on a wavefront without moments (recomputed by the drift itself)
+        ('quad1_c2', g2(128, 0.5e-3), c2, [pp(1), pp(), pp(1)]),
+        ('quad1_clip', g2(96, 0.5e-3), [('aperture', 'r', 'a', 0.05e-3, 0.05e-3, 0., 0.), ('lens', 15., 15., 0., 0.),
+                                        ('drift', 10., 0)], [pp(), pp(), pp(1)]),
+        ('quad1_nomom', no_moments(lambda: undulator_wfr(L, 64, 64, npTraj=4000)), [('drift', 5., 0)], [pp(1)]),
+        # pp[3]=3: from a waist over a large distance
+        ('fromwaist_64', g0(64), [('drift', 20., 0)], [pp(3)]),
+        ('fromwaist_lens_96x80', lambda: gaussian_wfr(L, 2000., 30e-6, 96, 80, 0.6e-3, 0.5e-3),
+         [('drift', 6., 0), ('lens', 3., 3., 0., 0.), ('drift', 3., 0)], [pp(3), pp(), pp(3)]),
     ]
     return out
+
+
+def no_moments(make):
+    """The wavefront of `make` with its statistical moments set to zero."""
+    def f():
+        w = make()
+        w.arMomX = array('d', [0.] * 11)
+        w.arMomY = array('d', [0.] * 11)
+        return w
+    return f
 
 
 def main():

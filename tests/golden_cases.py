@@ -55,3 +55,18 @@ def moment_err(a, b):
                   abs(b[10])])
     s = np.where(s > 0, s, 1e-300)
     return float(np.max(np.abs(a - b) / s))
+
+
+# cases whose plan depends on moments measured from the field (pp[3]=1 radius estimate on
+# recomputed moments): the device-resident plan API refuses them, the drop-in plans in stages, and
+# the output mesh follows the measured moments (compared to 1e-8 instead of bit-exact)
+STAGED = {'quad1_clip', 'quad1_nomom'}
+# cases of features still being restated (skipped)
+PENDING = {'fromwaist_64', 'fromwaist_lens_96x80'}
+
+
+def mesh_close(mine, ref, staged):
+    mine, ref = np.asarray(mine, np.float64), np.asarray(ref, np.float64)
+    if not staged:
+        return bool(np.array_equal(mine, ref))
+    return bool(np.array_equal(mine[:2], ref[:2]) and np.allclose(mine[2:], ref[2:], rtol=1e-8, atol=0))

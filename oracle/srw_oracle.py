@@ -20,7 +20,7 @@ Statistical moments: propagated with the reference's analytic matrices, and reco
 field (ComputeRadMoments, sroptelm.cpp:1608) where an aperture or obstacle asks for it.
 
 Not restated (documented gaps): the auto-resize Meth_1/Meth_2 machinery (pp[0], pp[1] != 0);
-drift modes pp[3] = 1, 5 and >= 100; ne > 1.
+drift modes pp[3] = 5 and >= 100; ne > 1.
 """
 from __future__ import annotations
 
@@ -405,6 +405,38 @@ def drift_to_waist(w: Wfr, L, treat):
         w.zStep *= -1.
 
 
+def drift_from_waist(w: Wfr, L, treat):
+    """PropagateRadiationSimple_PropFromWaist (sroptdrf.cpp:614-724), SetupPropBufVars_PropFromWaist
+    (sroptdrf.h:522-535), RadPointModifier_PropFromWaist (sroptdrf.h:756-804): quadratic phase,
+    forward FFT, mesh scaled by lambda L, quadratic phase again with the 1/(lambda L) factor and the
+    -i; no centre terms and no mirror."""
+    InvLength = 1. / L
+    Pi_d_LambdaM = w.eStart * PI_D_LAMBDA_PER_EV
+    Pi_d_LambdaM_d_Length = Pi_d_LambdaM * InvLength
+    InvLength_d_Lambda = InvLength * w.eStart * INV_LAMBDA_PER_EV
+    if w.Pres != 0:
+        set_rad_repres(w, 0)
+    x, z = w.coords()
+    _apply_phase(w, Pi_d_LambdaM_d_Length * (x * x + z * z))
+    InvLambda_m = w.eStart * INV_LAMBDA_PER_EV
+    LambdaM_Length = 1. / (InvLambda_m / L)
+    r = None
+    for comp in ('ex', 'ey'):
+        d, xs, ys, x0, y0 = make_2d_fft(getattr(w, comp), w.nx, w.nz, w.xStep, w.zStep, w.xStart, w.zStart, 1)
+        setattr(w, comp, d)
+        r = (xs, ys, x0, y0)
+    xStepTr, yStepTr, xStartTr, yStartTr = r
+    w.xStart = xStartTr * LambdaM_Length
+    w.zStart = yStartTr * LambdaM_Length
+    w.xStep = xStepTr * LambdaM_Length
+    w.zStep = yStepTr * LambdaM_Length
+    x, z = w.coords()
+    ph = Pi_d_LambdaM_d_Length * (x * x + z * z)
+    if treat == 1:
+        ph = ph + 5.067730652e+06 * L * w.eStart
+    w.mult(np.exp(1j * ph) * (-1j * InvLength_d_Lambda))
+
+
 def _sign(v):
     return 1. if v > 0 else (-1. if v < 0 else 0.)
 
@@ -522,6 +554,8 @@ def drift(w: Wfr, L, treat, anal_treatment):
         drift_quad(w, L, treat, anal_treatment)
     elif anal_treatment == 4:
         drift_to_waist(w, L, treat)
+    elif anal_treatment == 3:
+        drift_from_waist(w, L, treat)
     elif anal_treatment == 0:
         drift_ang_repres(w, L, treat)
     else:

@@ -765,6 +765,31 @@ void Planner::drift_to_waist(const ElemDesc& e)
     }
 }
 
+void Planner::drift_from_waist(const ElemDesc& e)
+{   // PropagateRadiationSimple_PropFromWaist (sroptdrf.cpp:614-724), SetupPropBufVars_PropFromWaist
+    // (sroptdrf.h:522), RadPointModifier_PropFromWaist (sroptdrf.h:756-804): as to the waist without
+    // the centre terms and the mirror, the path-length phase in the second pass
+    const double L = e.L;
+    double InvLength = 1. / L;
+    double Pi_d_LambdaM = w.eStart * PI_D_LAMBDA_PER_EV;
+    double Pi_d_LambdaM_d_Length = Pi_d_LambdaM * InvLength;
+    double InvLength_d_Lambda = InvLength * w.eStart * INV_LAMBDA_PER_EV;
+    if (w.Pres != 0) set_rad_repres(0);
+    b->quad(w, Pi_d_LambdaM_d_Length, 0., Pi_d_LambdaM_d_Length, 0., 0.);
+    double InvLambda_m = w.eStart * INV_LAMBDA_PER_EV;
+    double InvLambda_m_d_Length = InvLambda_m / L;
+    double LambdaM_Length = 1. / InvLambda_m_d_Length;
+    double xs, zs, x0, z0;
+    fft2_emit(1, false, xs, zs, x0, z0);     // Make2DFFT forward, representation flag unchanged
+    w.xStart = x0 * LambdaM_Length;
+    w.zStart = z0 * LambdaM_Length;
+    w.xStep = xs * LambdaM_Length;
+    w.zStep = zs * LambdaM_Length;
+    double cc = (e.treat == 1) ? (5.067730652e+06) * L * w.eStart : 0.;
+    b->quad(w, Pi_d_LambdaM_d_Length, 0., Pi_d_LambdaM_d_Length, 0., cc);
+    b->scale(w, 0.f, (float)(-InvLength_d_Lambda));     // x InvLength_d_Lambda, then (re,im) <- (im,-re)
+}
+
 static double sgn(double v) { return v > 0 ? 1. : (v < 0 ? -1. : 0.); }
 
 int Planner::drift_quad(const ElemDesc& e, int subtype)
@@ -863,6 +888,7 @@ void Planner::drift(const ElemDesc& e, int anal)
         int r = drift_quad(e, anal);
         if (r) throw r;
     } else if (anal == 4) drift_to_waist(e);
+    else if (anal == 3) drift_from_waist(e);
     else if (anal == 0) drift_ang(e);
     else {
         err = "drift mode pp[3]=" + std::to_string(anal) + " is not supported on the GPU path";

@@ -119,6 +119,7 @@ private:
     void drift(const ElemDesc& e, int anal);
     void drift_ang(const ElemDesc& e);
     void drift_to_waist(const ElemDesc& e);
+    void drift_from_waist(const ElemDesc& e);
     int drift_quad(const ElemDesc& e, int subtype);
     void drift_moments(double L);
     void record_matrix(const double ax[2][2], const double az[2][2], int clamp, double sx, double sz);

@@ -61,8 +61,6 @@ def moment_err(a, b):
 # recomputed moments): the device-resident plan API refuses them, the drop-in plans in stages, and
 # the output mesh follows the measured moments (compared to 1e-8 instead of bit-exact)
 STAGED = {'quad1_clip', 'quad1_nomom'}
-# cases of features still being restated (skipped)
-PENDING = {'fromwaist_64', 'fromwaist_lens_96x80'}
 
 
 def mesh_close(mine, ref, staged):

@@ -9,7 +9,7 @@ import pytest
 
 from srw_b200 import capi
 from srw_b200.plan import Plan
-from tests.golden_cases import PENDING, STAGED, case_io, load
+from tests.golden_cases import STAGED, case_io, load
 from tests.helpers import beamline, gaussian, make_wfr, C1, C1PP, PP
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -49,8 +49,6 @@ def plan_case(name):
 
 @pytest.mark.parametrize('name', [c['name'] for c in INDEX])
 def test_planner_mesh_bit_exact(name):
-    if name in PENDING:
-        pytest.skip('not restated yet')
     if name in STAGED:      # the plan depends on moments measured from the field: refused here
         with pytest.raises(RuntimeError, match='plans in stages'):
             plan_case(name)

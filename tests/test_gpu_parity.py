@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 from srw_b200 import srwlpy as srwl  # noqa: E402
 from srw_b200.plan import Plan  # noqa: E402
-from tests.golden_cases import PENDING, STAGED, case_io, load, mesh_close, moment_err  # noqa: E402
+from tests.golden_cases import STAGED, case_io, load, mesh_close, moment_err  # noqa: E402
 from tests.helpers import (C0, C0PP, C1, C1PP, C2, C2PP, PP, beamline, fields, gaussian, make_wfr,  # noqa: E402
                            mesh_tuple, oracle_run, rel_l2)
 
@@ -38,8 +38,6 @@ def run_gpu(ex, ey, mesh, elements, props, **sc):
 @pytest.mark.parametrize('name', [c['name'] for c in INDEX])
 def test_golden_case(name):
     need_gpu()
-    if name in PENDING:
-        pytest.skip('not restated yet')
     c = next(c for c in INDEX if c['name'] == name)
     i, o = case_io(D, name)
     w = run_gpu(i['ex'], i['ey'], i['mesh'], c['elements'], c['props'], Rx=i['Rx'], Ry=i['Ry'], dRx=i['dRx'],

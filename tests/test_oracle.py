@@ -6,7 +6,7 @@ import sys
 import numpy as np
 import pytest
 
-from tests.golden_cases import GOLDEN, PENDING, STAGED, case_io, load, mesh_close, moment_err, rel_l2
+from tests.golden_cases import GOLDEN, STAGED, case_io, load, mesh_close, moment_err, rel_l2
 
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'oracle'))
 import srw_oracle as O  # noqa: E402
@@ -40,8 +40,6 @@ def run_oracle(name):
 
 @pytest.mark.parametrize('name', NAMES)
 def test_oracle_vs_reference(name):
-    if name in PENDING:
-        pytest.skip('not restated yet')
     w, o = run_oracle(name)
     m = w.out_mesh()
     mine = np.array([m['nx'], m['ny'], m['xStart'], m['xFin'], m['yStart'], m['yFin']])

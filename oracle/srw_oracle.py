@@ -20,7 +20,7 @@ Statistical moments: propagated with the reference's analytic matrices, and reco
 field (ComputeRadMoments, sroptelm.cpp:1608) where an aperture or obstacle asks for it.
 
 Not restated (documented gaps): the auto-resize Meth_1/Meth_2 machinery (pp[0], pp[1] != 0);
-drift modes pp[3] = 5 and >= 100; ne > 1.
+drift modes pp[3] >= 100; ne > 1.
 """
 from __future__ import annotations
 
@@ -437,6 +437,74 @@ def drift_from_waist(w: Wfr, L, treat):
     w.mult(np.exp(1j * ph) * (-1j * InvLength_d_Lambda))
 
 
+def _radical(x, plus_one):
+    """sqrt(1 + x) (plus_one) or sqrt(1 + x) - 1 as sroptdrf.h:731-735 evaluates them: the square
+    root for |x| > 0.01, else the 8-term binomial series of sqrt(1 + x) - 1 (plus 1)."""
+    x = np.asarray(x, np.float64)
+    ser = x * (0.5 + x * (-0.125 + x * (0.0625 + x * (-0.0390625 + x * (0.02734375 + x * (-0.0205078125 +
+                                                                                      x * 0.01611328125))))))
+    root = np.sqrt(np.maximum(1. + x, 0.))
+    if plus_one:
+        return np.where(np.abs(x) > 0.01, root, 1. + ser)
+    return np.where(np.abs(x) > 0.01, root - 1., ser)
+
+
+def drift_to_waist_beyond_parax(w: Wfr, L, treat):
+    """PropagateRadiationSimple_PropToWaistBeyondParax (sroptdrf.cpp:491-612), its buffer set-up
+    (sroptdrf.h:492-520) and RadPointModifier_PropToWaistBeyondParax (sroptdrf.h:712-754): the
+    quadratic phase off (TreatQuadPhaseTerm 'r' with the wavefront's current treatment flags), the
+    mesh mapped to angular frequencies (x - xc)/(lambda R), the exact propagator
+    exp(i k L (sqrt(1 - lambda^2 q^2) - 1)) with the curvature and Gouy terms, an inverse FFT, and a
+    mirror where the transformed steps are negative."""
+    w.set_full_range()
+    sqrtAbsRxRz = math.sqrt(abs(w.RobsX * w.RobsZ))
+    sgnRx = 1 if w.RobsX >= 0 else -1
+    sgnRz = 1 if w.RobsZ >= 0 else -1
+    dPhaseSignR = 0.7853981633974483 * (sgnRx + sgnRz)
+    Pi_MultLambdaM = 3.141592653589793 * 1.239842e-06
+    Pi_MultLambdaM_Rx = Pi_MultLambdaM * w.RobsX
+    Pi_MultLambdaM_Rz = Pi_MultLambdaM * w.RobsZ
+    MultEn_TwoPi_L_d_LambdaM = 2. * 2.53384080189E+06 * L
+    if w.Pres != 0:
+        set_rad_repres(w, 0)
+    _treat_strongly_oscillating(w, 'r')       # srradstr.h:841, with the flags as they stand
+    xcOrig, zcOrig = w.xc, w.zc
+    InvLambdaM = w.eStart * 806546.577258
+    InvLambdaM_d_Rx = InvLambdaM / w.RobsX
+    InvLambdaM_d_Rz = InvLambdaM / w.RobsZ
+    w.xStep *= InvLambdaM_d_Rx
+    w.zStep *= InvLambdaM_d_Rz
+    w.xStart = (w.xStart - xcOrig) * InvLambdaM_d_Rx
+    w.zStart = (w.zStart - zcOrig) * InvLambdaM_d_Rz
+    x, z = w.coords()
+    e = w.eStart
+    ph = -(Pi_MultLambdaM_Rx * x * x + Pi_MultLambdaM_Rz * z * z) / e
+    kL = MultEn_TwoPi_L_d_LambdaM * e
+    LambdaM = 1.239842e-06 / e
+    lx, lz = LambdaM * x, LambdaM * z
+    X = -(lx * lx + lz * lz)
+    ph = ph + kL * _radical(X, treat == 1) + dPhaseSignR
+    w.mult(np.exp(1j * ph) * (LambdaM * sqrtAbsRxRz))
+    res = None
+    for comp in ('ex', 'ey'):
+        d, xs, ys, x0, y0 = make_2d_fft(getattr(w, comp), w.nx, w.nz, w.xStep, w.zStep, w.xStart, w.zStart, -1)
+        setattr(w, comp, d)
+        res = (xs, ys, x0, y0)
+    xStepTr, yStepTr, xStartTr, yStartTr = res
+    sx = sz = 1
+    xStartNew, xStepNew = xStartTr + xcOrig, xStepTr
+    zStartNew, zStepNew = yStartTr + zcOrig, yStepTr
+    if xStepTr < 0:
+        sx = -1
+        xStartNew, xStepNew = -xStartTr + xcOrig, -xStepTr
+    if yStepTr < 0:
+        sz = -1
+        zStartNew, zStepNew = -yStartTr + zcOrig, -yStepTr
+    if sx < 0 or sz < 0:
+        mirror_field(w, sx, sz)
+    w.xStart, w.zStart, w.xStep, w.zStep = xStartNew, zStartNew, xStepNew, zStepNew
+
+
 def _sign(v):
     return 1. if v > 0 else (-1. if v < 0 else 0.)
 
@@ -556,6 +624,8 @@ def drift(w: Wfr, L, treat, anal_treatment):
         drift_to_waist(w, L, treat)
     elif anal_treatment == 3:
         drift_from_waist(w, L, treat)
+    elif anal_treatment == 5:
+        drift_to_waist_beyond_parax(w, L, treat)
     elif anal_treatment == 0:
         drift_ang_repres(w, L, treat)
     else:

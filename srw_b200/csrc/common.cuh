@@ -391,8 +391,30 @@ __device__ __forceinline__ void gather_pass_t(float2* s, int N, int line, const 
     __syncthreads();
 }
 
-// non-separable point-wise work: circular masks, rectangular obstacles and the quartic remainder
-// of the angular transfer function (everything separable is in the plan's tables)
+// RadPointModifier_PropToWaistBeyondParax (sroptdrf.h:712-754): exp(i k L (sqrt(1 + X) - 1)), or with
+// k L sqrt(1 + X) on the path-length option, X = -lambda^2 (qx^2 + qz^2); the square root for
+// |X| > 0.01, else the reference's binomial series; FP64, then reduced by 2 pi.  Out of line: rare,
+// and it keeps the passes that may evaluate it small.
+static __device__ __noinline__ float2 bpx_factor(const PwOps& e, int i, int j)
+{
+    const double qx = e.bqx0 + (double)i * e.bdqx, qz = e.bqz0 + (double)j * e.bdqz;
+    const double lx = e.blam * qx, lz = e.blam * qz;
+    const double X = -(lx * lx + lz * lz);
+    double r;
+    if (fabs(X) > 0.01) {
+        r = sqrt(1. + X);
+        if (!e.btreat) r -= 1.;
+    } else {
+        r = X * (0.5 + X * (-0.125 + X * (0.0625 + X * (-0.0390625 + X * (0.02734375 + X * (-0.0205078125 +
+                                                                                  X * 0.01611328125))))));
+        if (e.btreat) r += 1.;
+    }
+    return expi(e.bkL * r);
+}
+
+// non-separable point-wise work: circular masks, rectangular obstacles, the quartic remainder of
+// the angular transfer function, the beyond-paraxial propagator (everything separable is in the
+// plan's tables)
 __device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2& f, bool& zero)
 {
     if (e.has_ang) {
@@ -404,6 +426,7 @@ __device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2&
         __sincosf(ph, &sn, &cs);
         f = cmul(f, make_float2(cs, sn));
     }
+    if (e.has_bpx) f = cmul(f, bpx_factor(e, i, j));
     for (int m = 0; m < e.nmask; m++) {
         const PwMask& k = e.mask[m];
         double x = dadd(k.x0, dmul((double)i, k.dx));

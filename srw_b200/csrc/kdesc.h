@@ -43,6 +43,10 @@ struct PwOps {
     int nmask;
     PwMask mask[SRWG_MAX_MASKS];
     int ang_resid;                       // 1: only the non-separable part c0 q^2 c1 q^2 (1 + 2 c1 q^2)
+    int has_bpx;                         // exact propagator beyond the paraxial approximation
+    double bqx0, bdqx, bqz0, bdqz;       //   (sroptdrf.h:712): phase += kL * (sqrt(1 - lam^2 q^2) - 1
+    double blam, bkL;                    //   + btreat), q the angular frequencies of index (i, j)
+    int btreat;
 };
 
 // Separable factor tables (complex FP32, computed in FP64 on the host) of one point-wise chain:

@@ -167,6 +167,20 @@ public:
         ks.push_back(k);
         return ks.back().mom;
     }
+    // exact beyond-paraxial propagator phase on the current (angular-frequency) mesh
+    void bpx(const WfrState& w, double lam, double kL, int treat)
+    {
+        PwOps* p = ensure(w);
+        if (p->has_bpx) {
+            close();
+            p = ensure(w);
+        }
+        double X0, DX, Z0, DZ;
+        axis_map(w, X0, DX, Z0, DZ);
+        p->has_bpx = 1;
+        p->bqx0 = X0; p->bdqx = DX; p->bqz0 = Z0; p->bdqz = DZ;
+        p->blam = lam; p->bkL = kL; p->btreat = treat;
+    }
     void ang(const WfrState& w, double c0, double c1, double cconst)
     {
         PwOps* p = ensure(w);
@@ -574,12 +588,15 @@ static CenMom cen_mom(const double* m)
 // the stronger component, as they were cached before any recomputation, are unusable; then the rms
 // divergences of that component.  S: the sums of the field (nullptr: none measured).  Returns false
 // when a recomputation is needed and S is nullptr.
-static bool estimate_moments(const MomOp& op, const double* S, double* mx, double* mz, double& sxp, double& szp)
+static bool estimate_moments(const MomOp& op, const double* S, double* mx, double* mz, double& sxp, double& szp,
+                             bool* recomputed = nullptr)
 {
     const CenMom cX = cen_mom(mx), cZ = cen_mom(mz);
+    bool rec = false;
     if (mx[0] == 0. && mz[0] == 0.) {
         if (S == nullptr) return false;
         moments_from_sums(S, op, mx, mz);
+        rec = true;
     }
     const bool useX = mx[0] >= mz[0];
     CenMom c = useX ? cX : cZ;
@@ -587,13 +604,16 @@ static bool estimate_moments(const MomOp& op, const double* S, double* mx, doubl
         if (S == nullptr) return false;
         moments_from_sums(S, op, mx, mz);
         c = cen_mom(useX ? mx : mz);
+        rec = true;
     }
     sxp = c.sxp; szp = c.szp;
+    if (recomputed) *recomputed = rec;
     return true;
 }
 
-// a MOM pass on the current field (ComputeRadMoments, sroptelm.cpp:1608) with the result slot of op
-void Planner::emit_moment_pass(MomOp& op)
+// a MOM pass on the current field (ComputeRadMoments, sroptelm.cpp:1608) with the result slot of op;
+// certain: the recomputation is known to happen (its treatment flags stay behind, as the reference's)
+void Planner::emit_moment_pass(MomOp& op, bool certain)
 {
     op.slot = nMomSlots++;
     op.nx = w.nx; op.nz = w.nz; op.eStart = w.eStart;
@@ -607,7 +627,9 @@ void Planner::emit_moment_pass(MomOp& op)
     // adds it back after, so the field itself is unchanged)
     const bool qx = ::fabs(w.RobsXAbsErr) < 0.4 * ::fabs(w.RobsX);
     const bool qz = ::fabs(w.RobsZAbsErr) < 0.4 * ::fabs(w.RobsZ);
-    w.QuadX = qx; w.QuadZ = qz;
+    op.qx = qx; op.qz = qz;
+    if (certain) { w.QuadX = qx; w.QuadZ = qz; }
+    else quadFlagsUncertain_ = true;
     if (qx || qz) {
         const double Const = 3.14159265358979 * 1.E+06 / 1.23984186;
         const double cx = qx ? -Const / w.RobsX * w.eStart : 0., cz = qz ? -Const / w.RobsZ * w.eStart : 0.;
@@ -645,14 +667,16 @@ void Planner::estimate_rad(double L, double& effRx, double& effRz)
                       "srwlPropagElecField plans in stages";
                 throw (int)SRWG_ERR_UNSUPPORTED;
             }
-            emit_moment_pass(op);
+            emit_moment_pass(op, false);
             pendingEstSlot_ = op.slot;
             pendingEstOp_ = op;
             throw (int)SRWG_NEED_STAGE;
         }
     }
     double SigXp = 0., SigZp = 0.;
-    estimate_moments(op, S, w.momX, w.momZ, SigXp, SigZp);
+    bool rec = false;
+    estimate_moments(op, S, w.momX, w.momZ, SigXp, SigZp, &rec);
+    if (rec) { w.QuadX = op.qx; w.QuadZ = op.qz; }
     momOps.push_back(op);
     pendingEstSlot_ = -1;
     const double infLarge = 1E+23;
@@ -686,21 +710,27 @@ void Planner::estimate_rad(double L, double& effRx, double& effRz)
     effRz = one(w.RobsZ, SigZp);
 }
 
-void Planner::replay_moments(const double* slots, double* mx, double* mz) const
+void Planner::replay_moments(const double* slots, double* mx, double* mz, bool* quadX, bool* quadZ) const
 {
     for (int i = 0; i < 11; i++) { mx[i] = in.momX[i]; mz[i] = in.momZ[i]; }
+    bool qx = in.QuadX, qz = in.QuadZ;     // treatment flags left by the last recomputation
     for (const MomOp& op : momOps) {
         if (op.kind == MOP_MATRIX) {
             apply_matrix_op(op, mx);
             apply_matrix_op(op, mz);
         } else if (op.kind == MOP_ESTIMATE) {
             double a, c;
+            bool rec = false;
             if (op.slot >= 0 && slots != nullptr)
-                estimate_moments(op, slots + (size_t)op.slot * SRWG_MOM_SLOT, mx, mz, a, c);
+                estimate_moments(op, slots + (size_t)op.slot * SRWG_MOM_SLOT, mx, mz, a, c, &rec);
+            if (rec) { qx = op.qx; qz = op.qz; }
         } else if (op.slot >= 0 && slots != nullptr && (op.obstacle || mom_outside(mx, mz, op))) {
             moments_from_sums(slots + (size_t)op.slot * SRWG_MOM_SLOT, op, mx, mz);
+            qx = op.qx; qz = op.qz;
         }
     }
+    if (quadX) *quadX = qx;
+    if (quadZ) *quadZ = qz;
 }
 
 void Planner::drift_ang(const ElemDesc& e)
@@ -788,6 +818,51 @@ void Planner::drift_from_waist(const ElemDesc& e)
     double cc = (e.treat == 1) ? (5.067730652e+06) * L * w.eStart : 0.;
     b->quad(w, Pi_d_LambdaM_d_Length, 0., Pi_d_LambdaM_d_Length, 0., cc);
     b->scale(w, 0.f, (float)(-InvLength_d_Lambda));     // x InvLength_d_Lambda, then (re,im) <- (im,-re)
+}
+
+void Planner::drift_beyond_parax(const ElemDesc& e)
+{   // PropagateRadiationSimple_PropToWaistBeyondParax (sroptdrf.cpp:491-612), its buffer set-up
+    // (sroptdrf.h:492) and RadPointModifier_PropToWaistBeyondParax (sroptdrf.h:712-754)
+    if (quadFlagsUncertain_) {
+        // TreatQuadPhaseTerm below uses the treatment flags that the last moment recomputation left;
+        // whether an aperture recomputed is only known once its passes ran
+        if (!allowStages) {
+            err = "drift mode pp[3]=5 after an aperture whose moment recomputation is decided on the "
+                  "device: only srwlPropagElecField plans in stages";
+            throw (int)SRWG_ERR_UNSUPPORTED;
+        }
+        throw (int)SRWG_NEED_STAGE;
+    }
+    const double L = e.L;
+    set_full_range();
+    const double sqrtAbsRxRz = ::sqrt(::fabs(w.RobsX * w.RobsZ));
+    const int sgnRx = (w.RobsX >= 0) ? 1 : -1, sgnRz = (w.RobsZ >= 0) ? 1 : -1;
+    const double dPhaseSignR = 0.7853981633974483 * (sgnRx + sgnRz);
+    const double Pi_MultLambdaM = 3.141592653589793 * 1.239842e-06;
+    const double Pi_MultLambdaM_Rx = Pi_MultLambdaM * w.RobsX, Pi_MultLambdaM_Rz = Pi_MultLambdaM * w.RobsZ;
+    const double MultEn_TwoPi_L_d_LambdaM = 2. * 2.53384080189E+06 * L;
+    if (w.Pres != 0) set_rad_repres(0);
+    treat_quad('r');                     // TreatQuadPhaseTerm (srradstr.h:841), flags as they stand
+    const double xcOrig = w.xc, zcOrig = w.zc;
+    const double InvLambdaM = w.eStart * 806546.577258;
+    const double InvLambdaM_d_Rx = InvLambdaM / w.RobsX, InvLambdaM_d_Rz = InvLambdaM / w.RobsZ;
+    w.xStep *= InvLambdaM_d_Rx;
+    w.zStep *= InvLambdaM_d_Rz;
+    w.xStart = (w.xStart - xcOrig) * InvLambdaM_d_Rx;
+    w.zStart = (w.zStart - zcOrig) * InvLambdaM_d_Rz;
+    const double en = w.eStart, LambdaM = 1.239842e-06 / en;
+    b->quad(w, -Pi_MultLambdaM_Rx / en, 0., -Pi_MultLambdaM_Rz / en, 0., dPhaseSignR);
+    b->bpx(w, LambdaM, MultEn_TwoPi_L_d_LambdaM * en, e.treat == 1 ? 1 : 0);
+    b->scale(w, (float)(LambdaM * sqrtAbsRxRz), 0.f);
+    double xs, zs, x0, z0;
+    fft2_emit(-1, false, xs, zs, x0, z0);
+    int sx = 1, sz = 1;
+    double xStartNew = x0 + xcOrig, xStepNew = xs, zStartNew = z0 + zcOrig, zStepNew = zs;
+    if (xs < 0) { sx = -1; xStartNew = -x0 + xcOrig; xStepNew = -xs; }
+    if (zs < 0) { sz = -1; zStartNew = -z0 + zcOrig; zStepNew = -zs; }
+    if ((sx < 0) || (sz < 0)) mirror(sx, sz);
+    w.xStart = xStartNew; w.zStart = zStartNew;
+    w.xStep = xStepNew; w.zStep = zStepNew;
 }
 
 static double sgn(double v) { return v > 0 ? 1. : (v < 0 ? -1. : 0.); }
@@ -889,6 +964,7 @@ void Planner::drift(const ElemDesc& e, int anal)
         if (r) throw r;
     } else if (anal == 4) drift_to_waist(e);
     else if (anal == 3) drift_from_waist(e);
+    else if (anal == 5) drift_beyond_parax(e);
     else if (anal == 0) drift_ang(e);
     else {
         err = "drift mode pp[3]=" + std::to_string(anal) + " is not supported on the GPU path";
@@ -1020,7 +1096,7 @@ void Planner::aperture(const ElemDesc& e)
         op.hx = 0.5 * e.Dx;
         op.hz = (e.shape == 'r') ? 0.5 * e.Dy : 0.5 * e.Dx;
         const bool recompute = obstacle || mom_outside(w.momX, w.momZ, op);
-        if ((recompute || momProvisional) && numMoments) emit_moment_pass(op);
+        if ((recompute || momProvisional) && numMoments) emit_moment_pass(op, !momProvisional);
         momOps.push_back(op);
     }
     if (e.apob == 'a') {     // SetNewNonZeroWfrLimits of the apertures
@@ -1223,6 +1299,7 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
     pendingEstSlot_ = -1;
     elemIdx_ = 0;
     resizeDone_ = false;
+    quadFlagsUncertain_ = false;
     if (pw == nullptr || opt == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
     // InSRWRadPtrs (srradstr.cpp:501)
     const SRWLRadMesh& m = pw->mesh;
@@ -1258,8 +1335,9 @@ int Planner::resume(const double* slots)
 {
     // moments as they stand after the stage: the bookkeeping replayed with every result so far
     slotVals_.assign(slots, slots + (size_t)nMomSlots * SRWG_MOM_SLOT);
-    replay_moments(slotVals_.data(), w.momX, w.momZ);
+    replay_moments(slotVals_.data(), w.momX, w.momZ, &w.QuadX, &w.QuadZ);
     momProvisional = false;
+    quadFlagsUncertain_ = false;
     kernels.clear();
     tables.clear();
     maxElems = 0;

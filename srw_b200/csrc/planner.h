@@ -39,6 +39,7 @@ struct MomOp {
     int obstacle = 0;                  // aperture: opening (centre, half sizes) for the 1.7 sigma check
     double cx = 0, cz = 0, hx = 0, hz = 0;
     int slot = -1;                     // result slot of the MOM pass (-1: no recomputation possible)
+    int qx = 0, qz = 0;                // quadratic-term treatment flags a recomputation leaves behind
     int nx = 0, nz = 0;                // mesh and photon energy of the recomputation
     double eStart = 0, xStart = 0, xStep = 0, zStart = 0, zStep = 0;
 };
@@ -85,7 +86,8 @@ public:
 
     // the output moments from the input ones and the MOM passes' result slots (nMomSlots x
     // SRWG_MOM_SLOT doubles; unused when nMomSlots == 0)
-    void replay_moments(const double* slots, double* momX, double* momZ) const;
+    void replay_moments(const double* slots, double* momX, double* momZ, bool* quadX = nullptr,
+                        bool* quadZ = nullptr) const;
 
     // flattens SRWLOptC (nested containers included) and plans; returns 0, an SRW error number, or
     // (with allowStages) SRWG_NEED_STAGE: `kernels` then hold a complete stage, which must run on
@@ -109,7 +111,7 @@ private:
     MomOp pendingEstOp_;
     int run();
     int finalize();
-    void emit_moment_pass(MomOp& op);
+    void emit_moment_pass(MomOp& op, bool certain);
     void estimate_rad(double L, double& effRx, double& effRz);
     int flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vector<PropDesc>& props, bool nested);
     void set_full_range();
@@ -120,6 +122,8 @@ private:
     void drift_ang(const ElemDesc& e);
     void drift_to_waist(const ElemDesc& e);
     void drift_from_waist(const ElemDesc& e);
+    void drift_beyond_parax(const ElemDesc& e);
+    bool quadFlagsUncertain_ = false;    // QuadX/QuadZ depend on a moment recomputation decided on the device
     int drift_quad(const ElemDesc& e, int subtype);
     void drift_moments(double L);
     void record_matrix(const double ax[2][2], const double az[2][2], int clamp, double sx, double sz);

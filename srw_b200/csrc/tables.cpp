@@ -52,6 +52,12 @@ static void separate(const PwOps& pw, int axis, int nAlong, int nLine, SepPart& 
         extra.c0 = pw.c0; extra.c1 = pw.c1;
         has_extra = 1;
     }
+    if (pw.has_bpx) {       // non-separable: evaluated per point in FP64 (common.cuh extra_eval)
+        extra.has_bpx = 1;
+        extra.bqx0 = pw.bqx0; extra.bdqx = pw.bdqx; extra.bqz0 = pw.bqz0; extra.bdqz = pw.bdqz;
+        extra.blam = pw.blam; extra.bkL = pw.bkL; extra.btreat = pw.btreat;
+        has_extra = 1;
+    }
     if (pw.has_scale) { scale = cd(pw.sre, pw.sim); A.any = true; }
     for (int m = 0; m < pw.nmask; m++) {
         const PwMask& k = pw.mask[m];

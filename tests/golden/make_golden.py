@@ -161,6 +161,13 @@ def cases(L):
         ('fromwaist_64', g0(64), [('drift', 20., 0)], [pp(3)]),
         ('fromwaist_lens_96x80', lambda: gaussian_wfr(L, 2000., 30e-6, 96, 80, 0.6e-3, 0.5e-3),
          [('drift', 6., 0), ('lens', 3., 3., 0., 0.), ('drift', 3., 0)], [pp(3), pp(), pp(3)]),
+        # pp[3]=5: to a waist beyond the paraxial approximation (quadratic term kept, and taken off
+        # first once an aperture's moment recomputation has set the treatment flags; path length)
+        ('bpx_towaist', g2(96, 0.5e-3), [('lens', 15., 15., 0., 0.), ('drift', 30., 0)], [pp(), pp(5)]),
+        ('bpx_clip', g2(96, 0.5e-3), [('aperture', 'r', 'a', 0.05e-3, 0.05e-3, 0., 0.), ('lens', 15., 15., 0., 0.),
+                                      ('drift', 30., 0)], [pp(), pp(), pp(5)]),
+        ('bpx_treat_offc', g2(96, 0.5e-3), [('lens', 15., 15., 0.02e-3, -0.01e-3), ('drift', 30., 1)],
+         [pp(), pp(5)]),
     ]
     return out
 

@@ -84,8 +84,8 @@ def test_full_size_c1_plan():
 def test_unsupported_and_invalid_inputs_raise():
     ex, ey, mesh = gaussian(64)
     w = make_wfr(ex, ey, mesh)
-    with pytest.raises(RuntimeError, match='pp\\[3\\]=5'):
-        Plan(w, beamline([('drift', 1., 0)], [PP(5)]))
+    with pytest.raises(RuntimeError, match='pp\\[3\\]=100'):
+        Plan(w, beamline([('drift', 1., 0)], [PP(100)]))
     with pytest.raises(RuntimeError, match='automatic resizing'):
         Plan(w, beamline([('drift', 1., 0)], [[1, 0, 1., 0, 0, 1., 1., 1., 1.]]))
     ex1, ey1, mesh1 = gaussian(64, ny=1)

@@ -13,14 +13,12 @@ pytestmark = pytest.mark.gpu
 
 from srw_b200 import srwlpy as srwl  # noqa: E402
 from srw_b200.plan import Plan  # noqa: E402
-from tests.golden_cases import STAGED, case_io, load, mesh_close, moment_err  # noqa: E402
+from tests.golden_cases import MOMENT_RECOMPUTED, STAGED, case_io, load, mesh_close, moment_err  # noqa: E402
 from tests.helpers import (C0, C0PP, C1, C1PP, C2, C2PP, PP, beamline, fields, gaussian, make_wfr,  # noqa: E402
                            mesh_tuple, oracle_run, rel_l2)
 
 TOL = 1e-4           # relative L2, field and intensity
 D, INDEX = load()
-MOMENT_RECOMPUTED = {'c0_64', 'c0_128', 'c0_ragged_96x80', 'ob_circ_lens_offc', 'rect_ob_towaist', 'quad1_clip',
-                     'quad1_nomom'}
 REF_DIR = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'oracle', '_ref')
 
 

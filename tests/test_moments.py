@@ -100,3 +100,35 @@ def test_plan_batch_moments_match_single_runs():
         mx, my = p.moments(b)
         np.testing.assert_allclose(mx, np.array(w.arMomX), rtol=1e-6, atol=0)
         np.testing.assert_allclose(my, np.array(w.arMomY), rtol=1e-6, atol=0)
+
+
+# two clipping apertures (the second one's recomputation is decided on the device, and with it the
+# quadratic-term treatment flags) before a beyond-paraxial drift that uses those flags
+BPX_CHAIN = [('aperture', 'r', 'a', 0.3e-3, 0.3e-3, 0.1e-3, 0.),
+             ('aperture', 'c', 'a', 0.5e-3, 0.5e-3, 0.1e-3, 0.05e-3),
+             ('lens', 8., 8., 0., 0.),
+             ('drift', 8., 0)]
+BPX_PP = [PP, PP, PP, [0, 0, 1., 5, 0, 1., 1., 1., 1., 0, 0, 0]]
+
+
+def test_beyond_paraxial_after_device_decision_needs_stages():
+    ex, ey, mesh, sc = beam(64)
+    with pytest.raises(RuntimeError, match='plans in stages'):
+        Plan(make_wfr(ex, ey, mesh, **sc), beamline(BPX_CHAIN, BPX_PP))
+
+
+@pytest.mark.gpu
+def test_beyond_paraxial_staged_vs_oracle():
+    _gpu()
+    from srw_b200 import srwlpy as srwl
+    from tests.helpers import fields, mesh_tuple, rel_l2
+    ex, ey, mesh, sc = beam(128)
+    w = make_wfr(ex, ey, mesh, **sc)
+    srwl.PropagElecField(w, beamline(BPX_CHAIN, BPX_PP))
+    o = oracle_run(ex, ey, mesh, BPX_CHAIN, BPX_PP, **sc)
+    m = o.out_mesh()
+    np.testing.assert_allclose(mesh_tuple(w), [m['nx'], m['ny'], m['xStart'], m['xFin'], m['yStart'], m['yFin']],
+                               rtol=1e-12)
+    gx, gy = fields(w)
+    assert rel_l2(gx, o.ex) < TOL and rel_l2(gy, o.ey) < TOL
+    assert moment_err(np.array(w.arMomX), o.momX) < TOL

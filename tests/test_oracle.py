@@ -6,17 +6,15 @@ import sys
 import numpy as np
 import pytest
 
-from tests.golden_cases import GOLDEN, STAGED, case_io, load, mesh_close, moment_err, rel_l2
+from tests.golden_cases import (GOLDEN, MOMENT_RECOMPUTED, STAGED, case_io, load, mesh_close, moment_err,
+                                rel_l2)
 
 sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'oracle'))
 import srw_oracle as O  # noqa: E402
 
 D, INDEX = load()
 NAMES = [c['name'] for c in INDEX]
-# cases where the reference recomputes the statistical moments numerically (ComputeRadMoments: an
-# aperture clips the beam, or an obstacle): compared to FP32 round-off of each moment's scale
-MOMENT_RECOMPUTED = {'c0_64', 'c0_128', 'c0_ragged_96x80', 'ob_circ_lens_offc', 'rect_ob_towaist', 'quad1_clip',
-                     'quad1_nomom'}
+# moments the reference recomputes from the field: to FP32 round-off of each moment's scale
 MOMENT_TOL = 1e-5                # relative to the moment's scale (observed <= 2.3e-7)
 
 

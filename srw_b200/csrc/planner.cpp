@@ -1461,6 +1461,24 @@ int Planner::finalize()
         a.line.blk_out = bw;
         n.line.blk_in = bw;
     }
+    // a row pass that transforms only the rows of a resize window writes zeros in the other rows;
+    // the column pass on its output then skips loading them (the same window along its lines)
+    for (size_t i = 0; i + 1 < kernels.size(); i++) {
+        KernelDesc& a = kernels[i];
+        KernelDesc& n = kernels[i + 1];
+        if (a.kind != K_LINE || n.kind != K_LINE || a.line.axis != 0 || n.line.axis != 1 || !a.line.zwin ||
+            n.line.zwin || n.src != a.dst || a.line.nx != n.line.nx || a.line.nz != n.line.nz)
+            continue;
+        const int Nc = n.line.nz;
+        if (Nc < 64 || (Nc & (Nc - 1)) != 0) continue;
+        const int nz = a.line.nz;
+        LineDesc& d = n.line;
+        d.zwin = 1;
+        d.zl0 = 0;
+        d.zl1 = n.line.nx - 1;
+        d.za0 = a.line.mirror_lines ? nz - 1 - a.line.zl1 : a.line.zl0;
+        d.za1 = a.line.mirror_lines ? nz - 1 - a.line.zl0 : a.line.zl1;
+    }
     return 0;
 }
 

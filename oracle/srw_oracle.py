@@ -1440,6 +1440,88 @@ def total_intensity(ex, ey):
     return (ex.real * ex.real + ex.imag * ex.imag + ey.real * ey.real + ey.imag * ey.imag).astype(np.float32)
 
 
+def _formal_phase(re, im):
+    """FormalPhase (srradmnp.h:434): the argument of re + i im from atan of the FP32 ratio, in the
+    quadrant of (re, im) (-pi - ... pi, the reference's branch conventions and pi constants)."""
+    re = np.asarray(re, np.float32)
+    im = np.asarray(im, np.float32)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        a = np.arctan((im / re).astype(np.float64))
+    HalhPi, Pi = 1.5707963267949, 3.1415926535898
+    out = np.where(re != 0, np.where(re < 0, np.where(im <= 0, a - Pi, a + Pi), a),
+                   np.where(im == 0, 0., np.where(im > 0, HalhPi, -HalhPi)))
+    return out
+
+
+def intensity_component(ex, ey, pol, what):
+    """srTRadGenManip::IntensityComponent (srradmnp.h:367-425) over whole arrays with its FP32 / FP64
+    operation order.  what: 0 intensity, 2 phase (FP64 result), 3 Re E, 6 Im E (the reference's
+    internal numbering); pol 0 linear horizontal, 1 vertical, 2 +45 deg, 3 135 deg, 4 circular right,
+    5 circular left, 6 total; -1..-4 the Stokes components."""
+    f32 = np.float32
+    exr, exi = np.real(ex).astype(f32), np.imag(ex).astype(f32)
+    eyr, eyi = np.real(ey).astype(f32), np.imag(ey).astype(f32)
+    if pol == -1:
+        return (exr * exr + exi * exi + eyr * eyr + eyi * eyi).astype(f32)
+    if pol == -2:
+        return (exr * exr + exi * exi - (eyr * eyr + eyi * eyi)).astype(f32)
+    if pol == -3:
+        return (2. * (exr * eyr + exi * eyi).astype(np.float64)).astype(f32)
+    if pol == -4:
+        return (2. * (exr * eyi - exi * eyr).astype(np.float64)).astype(f32)
+    half = False
+    if pol == 0:
+        a, b = exr, exi
+    elif pol == 1:
+        a, b = eyr, eyi
+    elif pol == 2:
+        a, b, half = exr + eyr, exi + eyi, True
+    elif pol == 3:
+        a, b, half = exr - eyr, exi - eyi, True
+    elif pol == 5:
+        a, b, half = exr - eyi, exi + eyr, True
+    elif pol == 4:
+        a, b, half = exr + eyi, exi - eyr, True
+    else:
+        if what in (0, 1):
+            return (exr * exr + exi * exi + eyr * eyr + eyi * eyi).astype(f32)
+        if what == 2:
+            return _formal_phase(exr, exi).astype(np.float32).astype(np.float64)
+        return exr if what == 3 else exi
+    if what in (0, 1):
+        v = (a * a + b * b).astype(f32)
+        return (0.5 * v.astype(np.float64)).astype(f32) if half else v
+    if what == 2:       # IntensityComponent returns FP32: the phase too is rounded to FP32
+        return _formal_phase(a, b).astype(np.float32).astype(np.float64)
+    v = a if what == 3 else b
+    return (0.70710678 * v.astype(np.float64)).astype(f32) if half else v
+
+
+def calc_int_from_elec_field(ex, ey, pol, int_type, meth=None, prev=None):
+    """srwlCalcIntFromElecField (cpp/src/lib/srwlib.cpp:757) for a single photon energy, vs x and y
+    (ExtractSingleElecIntensity2DvsXZ, srradmnp.cpp:681): int_type 0 single-electron intensity, 4 phase
+    (FP64), 5 Re E, 6 Im E; pol -5 gives the four Stokes components one after the other.  meth[0] = 1
+    averages into prev over meth[1] earlier iterations, 2 adds to prev."""
+    what = {0: 0, 4: 2, 5: 3, 6: 6}[int_type]
+    pols = [-1, -2, -3, -4] if pol == -5 else [pol]
+    res = [np.asarray(intensity_component(ex, ey, p, what)).ravel() for p in pols]
+    res = np.concatenate(res)
+    mode = 0 if meth is None else int(meth[0])
+    if mode == 0 or prev is None:
+        return res
+    if what == 2:
+        prev = np.asarray(prev, np.float64)
+        if mode == 1:
+            it = float(meth[1])
+            return (prev * it + res) * (1. / (it + 1.))
+        return prev + res
+    prev = np.asarray(prev, np.float32)
+    if mode == 1:
+        it = float(meth[1])
+        return ((prev.astype(np.float64) * it + res.astype(np.float64)) * (1. / (it + 1.))).astype(np.float32)
+    return (prev + res).astype(np.float32)
+
+
 def add_interp_bilinear(acc, acc_mesh, I, mesh):
     """acc += I interpolated on acc_mesh: SRWLStokes.avg_update_interp with _ord=1 and _sum=True
     (env/python/srwpy/srwlib.py:1116-1203; points outside the mesh add nothing)."""

@@ -61,6 +61,8 @@ MODIF_FUNC = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(SRWLWfr), C.c_char)
 
 # symbol -> (restype, argtypes); the complete exported surface of include/srwl_b200.h
 SYMBOLS = {
+    'srwlCalcIntFromElecField': (C.c_int, [C.c_void_p, C.POINTER(SRWLWfr), C.c_char, C.c_char, C.c_char, C.c_double,
+                                           C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     'srwlPropagElecField': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_int, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.POINTER(C.c_double)]),
     'srwlUtiSetWfrModifFunc': (None, [MODIF_FUNC]),

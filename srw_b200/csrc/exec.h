@@ -20,6 +20,8 @@ struct DeviceCtx {
     double* mom = nullptr;              // moment passes of the one-shot entry point: slots | scratch
     size_t momDoubles = 0;
     float2* stg[2] = {nullptr, nullptr};  // stage outputs of a staged propagation (2 components each)
+    void* intBuf = nullptr;             // intensity extraction: both components and the result
+    size_t intBytes = 0;
     size_t stgElems[2] = {0, 0};
     cudaStream_t stream = nullptr;
 };

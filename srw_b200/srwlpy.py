@@ -199,3 +199,29 @@ def PropagElecField(wfr, optC, intList=None, dev=None):
         raise RuntimeError(capi.err_text(r))
     _update_py_wfr(wfr, w)
     return wfr
+
+
+def CalcIntFromElecField(arI, wfr, pol, intType, depType, e, x, y, meth=None, fldTrj=None, dev=None):
+    """srwlpy.CalcIntFromElecField (cpp/src/clients/python/srwlpy.cpp:4873): fills ``arI`` (array('f')
+    or a float32 numpy array; float64 for the phase, intType 4) with the intensity of ``wfr`` vs x and
+    y, on the GPU.  ``meth``: [1, n] averages into arI over n earlier iterations, [2] adds to it."""
+    if fldTrj is not None:
+        raise RuntimeError('intensity with the central electron field/trajectory is not supported on the GPU path')
+    keep = []
+    w = make_c_wfr(wfr, keep)
+    pI = _buf_ptr(arI, keep, np.float64 if int(intType) == 4 else np.float32)
+    pm = None
+    if meth is not None:
+        m = np.zeros(20)
+        m[:min(20, len(meth))] = np.asarray(meth, np.float64)[:20]
+        keep.append(m)
+        pm = m.ctypes.data
+    par = None
+    if dev is not None:
+        par = (C.c_double * 2)(1., float(dev))
+    c = lambda v: C.c_char(int(v) & 0xff)  # noqa: E731
+    r = capi.lib().srwlCalcIntFromElecField(pI, C.byref(w), c(pol), c(intType), c(depType), float(e), float(x),
+                                            float(y), pm, None, par)
+    if r > 0:
+        raise RuntimeError(capi.err_text(r))
+    return arI

@@ -208,6 +208,42 @@ def main():
         index.append(dict(name=name, elements=[list(e) for e in elems], props=[list(map(float, p)) for p in pps]))
         print(name, 'in', int(inp['mesh'][0]), int(inp['mesh'][1]), 'out', int(out['mesh'][0]), int(out['mesh'][1]),
               'R', out['scal'][0], out['scal'][1])
+    # 3) intensity extraction (srwlCalcIntFromElecField vs x and y) on a propagated wavefront with both
+    #    components: every polarisation, intensity / phase / Re / Im, and the averaging and adding modes
+    wsrc = None
+    for name, make, elems, pps in cases(L):
+        if name == 'quad1_nomom':
+            wsrc = make()
+            L.srwl.PropagElecField(wsrc, L.SRWLOptC(build_beamline(L, elems), [list(map(float, p)) for p in pps]))
+    nx, ny = wsrc.mesh.nx, wsrc.mesh.ny
+    ex = np.array(wsrc.arEx, np.float32)
+    xx = np.linspace(-1., 1., nx)[None, :]
+    yy = np.linspace(-1., 1., ny)[:, None]
+    c = (ex[0::2] + 1j * ex[1::2]).reshape(ny, nx) * (0.4 * np.exp(1j * (1.3 * xx - 0.7 * yy)) + 0.2 * xx)
+    ey = np.empty(2 * nx * ny, np.float32)
+    ey[0::2] = c.real.ravel(); ey[1::2] = c.imag.ravel()
+    wsrc.arEy = array('f', ey.tobytes())
+    blob['int/ex'] = ex
+    blob['int/ey'] = ey
+    blob['int/mesh'] = snapshot(wsrc)['mesh']
+    ints = []
+    for it in (0, 4, 5, 6):
+        for pol in (0, 1, 2, 3, 4, 5, 6, -1, -2, -3, -4, -5):
+            if pol < 0 and it != 0:
+                continue
+            n = nx * ny * (4 if pol == -5 else 1)
+            for meth in (None, [1., 3.], [2.]):
+                code = 'd' if it == 4 else 'f'
+                prev = np.sin(np.arange(n) * 0.37).astype(np.float64 if it == 4 else np.float32)
+                arI = array(code, prev.tobytes())
+                args = [arI, wsrc, pol, it, 3, wsrc.mesh.eStart, 0., 0.]
+                if meth is not None:
+                    args.append(array('d', meth + [0.] * (20 - len(meth))))
+                L.srwl.CalcIntFromElecField(*args)
+                key = 'int/%d/%d/%d' % (it, pol, 0 if meth is None else int(meth[0]))
+                blob[key] = np.array(arI, np.float64 if it == 4 else np.float32)
+                ints.append(dict(key=key, int_type=it, pol=pol, meth=meth))
+    blob['int/index'] = np.array(json.dumps(ints))
     blob['index'] = np.array(json.dumps(index))
     np.savez_compressed(os.path.join(HERE, 'cases.npz'), **blob)
 

@@ -47,9 +47,9 @@ SIG = (30e-6, 5e-6, 5e-6, 2e-6)                # source: sigma x [m], x' [rad], 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a pass, from an ncu
 # capture of this workload (profiles/passes_4096_c1.md); keyed by the pass tuple of Plan.kernels().
 # Re-captured whenever the kernel changes.
-TRAFFIC = {('line_cols', 4096, 4096): 268611840 + 225405440,
-           ('line_rows', 4096, 4096): 67257856 + 216448256,
-           ('resize', 1024, 1024, 4096, 4096): 16920320 + 13591296}
+TRAFFIC = {('line_cols', 4096, 4096): 134334464 + 219883776,
+           ('line_rows', 4096, 4096): 67189504 + 216088320,
+           ('resize', 1024, 1024, 4096, 4096): 16922624 + 15437824}
 
 
 # ------------------------------------------------------------------------------------------------

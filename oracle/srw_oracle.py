@@ -110,6 +110,7 @@ class Wfr:
     avgPhotEn: float = 0.
     momX: np.ndarray = field(default_factory=lambda: np.zeros(11))
     momZ: np.ndarray = field(default_factory=lambda: np.zeros(11))
+    propM: np.ndarray = field(default_factory=lambda: np.zeros(20))     # arElecPropMatr
     xStartTr: float = 0.
     zStartTr: float = 0.
     UseStartTrToShiftAtChangingRepresToCoord: bool = False
@@ -126,7 +127,7 @@ class Wfr:
 
     # --- SRWLWfr <-> internal mesh (srradstr.cpp:501-634, 687-758)
     @staticmethod
-    def from_srwl(ex, ey, mesh, Rx, Ry, dRx, dRy, xc, yc, presCA=0, momX=None, momY=None, avgPhotEn=0.):
+    def from_srwl(ex, ey, mesh, Rx, Ry, dRx, dRy, xc, yc, presCA=0, momX=None, momY=None, avgPhotEn=0., propM=None):
         """InSRWRadPtrs (srradstr.cpp:501).  ``mesh`` is a dict of SRWLRadMesh fields."""
         nx, ny = int(mesh['nx']), int(mesh['ny'])
         if nx <= 1:
@@ -147,6 +148,8 @@ class Wfr:
             w.momX = np.array(momX, np.float64)[:11].copy()
         if momY is not None:
             w.momZ = np.array(momY, np.float64)[:11].copy()
+        if propM is not None:
+            w.propM = np.array(propM, np.float64)[:20].copy()
         return w
 
     def out_mesh(self):
@@ -634,6 +637,24 @@ def drift(w: Wfr, L, treat, anal_treatment):
     w.RobsX += L                             # PropagateWaveFrontRadius (sroptdrf.h:981)
     w.RobsZ += L
     w.set_full_range()
+    # Propagate4x4PropMatr of the drift (sroptdrf.h:1002)
+    _prop_4x4(w, np.array([[1., L, 0., 0.], [0., 1., 0., 0.], [0., 0., 1., L], [0., 0., 0., 1.]]), np.zeros(4))
+
+
+def _prop_4x4(w: Wfr, E, e):
+    """GenAuxPropagate4x4PropMatr (sroptelm.cpp:5594): M <- E M, V <- E V + e on arElecPropMatr."""
+    M = np.asarray(w.propM[:16], np.float64).reshape(4, 4)
+    V = np.asarray(w.propM[16:20], np.float64)
+    R = np.zeros((4, 4))
+    RV = np.zeros(4)
+    for i in range(4):
+        for j in range(4):
+            r = 0.
+            for k in range(4):
+                r += E[i, k] * M[k, j]
+            R[i, j] = r
+            RV[i] += E[i, j] * V[j]
+    w.propM = np.concatenate([R.ravel(), RV + e])
 
 
 # ----------------------------------------------------------------------------------------
@@ -743,6 +764,9 @@ def lens(w: Wfr, Fx, Fz, cx, cz):
     w.RobsZAbsErr *= MagnZ * MagnZ
     w.xc = cx - (cx - w.xc) * MagnX
     w.zc = cz - (cz - w.zc) * MagnZ
+    # Propagate4x4PropMatr of the focusing element (sroptfoc.h:101)
+    _prop_4x4(w, np.array([[1., 0., 0., 0.], [-1. / Fx, 1., 0., 0.], [0., 0., 1., 0.], [0., 0., -1. / Fz, 1.]]),
+              np.array([0., cx / Fx, 0., cz / Fz]))
     _fix_abs_err(w)
     check_and_reset_phase_lin(w)
 

@@ -391,6 +391,8 @@ static void out_wfr(const Planner& pl, SRWLWfr* p)
     p->xc = w.xc; p->yc = w.zc;
     p->presCA = (char)w.Pres;
     p->avgPhotEn = w.avgPhotEn;
+    if (p->arElecPropMatr != nullptr && w.havePropM)
+        for (int i = 0; i < 20; i++) p->arElecPropMatr[i] = w.propM[i];
 }
 
 // output moments: the plan-time ones, or (with moment passes) the replayed bookkeeping with the

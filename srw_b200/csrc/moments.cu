@@ -6,7 +6,7 @@
 //               operators still pending on it, and the removal of the wavefront's quadratic phase)
 //   2. limits:  the total power and the rows holding 90 % of it (FindIntensityLimitsInds,
 //               srmatsta.cpp:572, with FindIntensityLimits2D :452 and FindLimit1DLeft/Right :400-450)
-//   3. columns: per-column sums over those rows, in row segments
+//   3. columns: per-column sums over those rows, in row segments, then their totals
 //   4. limits:  the columns holding 90 % of the power, the reference's FP32 round trip of the
 //               limits into mesh indices
 //   5. sums:    the 22 weighted sums (norms, first moments, second moments inside the limits, and the
@@ -23,8 +23,7 @@
 namespace srwg {
 
 #define MOM_T 256          // threads per CTA of the row / column / sum kernels
-#define MOM_RPC 8          // rows per CTA of the row kernel (one warp each)
-#define MOM_R5 32          // rows per CTA of the sum kernel
+#define MOM_R5 8           // rows per CTA of the sum kernel
 #define MOM_LT 1024        // threads of the limit kernels (one CTA)
 
 struct MomArgs {
@@ -41,8 +40,8 @@ struct MomArgs {
 static int mom_segments(int nx, int nz)
 {
     const int cx = (nx + MOM_T - 1) / MOM_T;
-    int S = (2 * 148 + cx - 1) / cx;
-    if (S > 64) S = 64;
+    int S = (4 * 148 + cx - 1) / cx;     // about four CTAs per SM
+    if (S > 256) S = 256;
     if (S > nz) S = nz;
     return S < 1 ? 1 : S;
 }
@@ -119,22 +118,27 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-// 1. per-row intensity sums, one warp per row
+// 1. per-row intensity sums, one CTA per row (warp sums, then the CTA's in warp order)
 __global__ void __launch_bounds__(MOM_T) mom_rows_kernel(const MomArgs a)
 {
+    __shared__ double ws[MOM_T / 32];
     const MomField F = mom_field(a);
-    const int nz = a.d->nz;
+    const int iz = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int iz = blockIdx.x * MOM_RPC + warp;
-    if (iz >= nz) return;
     double s = 0.;
-    for (int ix = lane; ix < F.nx; ix += 32) {
+    for (int ix = threadIdx.x; ix < F.nx; ix += MOM_T) {
         float2 ex, ey;
         F.load(ix, iz, ex, ey);
         s += (double)mom_int(ex, ey);
     }
     s = warp_sum(s);
-    if (lane == 0) a.sc[iz] = s;
+    if (lane == 0) ws[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.;
+        for (int w = 0; w < MOM_T / 32; w++) t += ws[w];
+        a.sc[iz] = t;
+    }
 }
 
 // first index where the running sum of v(0..n-1) exceeds `stop` (0 if none; `left`), or the last
@@ -239,13 +243,7 @@ __global__ void __launch_bounds__(MOM_LT) mom_limits_kernel(const MomArgs a, int
     if (ok) {
         const int iy0 = (int)lim[0], iy1 = (int)lim[1];
         const double stop = lim[3];
-        double* col = a.sc + a.offCol;
-        for (int i = t; i < nx; i += MOM_LT) {     // add the row segments, in place into segment 0
-            double s = col[i];
-            for (int k = 1; k < a.S; k++) s += col[(size_t)k * nx + i];
-            col[i] = s;
-        }
-        __syncthreads();
+        const double* col = a.sc + a.offCol;       // column totals (mom_colsum_kernel)
         const ColVals cv{col, d.zStep};
         const int ix0 = mom_find_limit(cv, nx, stop / d.xStep, true, sh, &ish);
         const int ix1 = mom_find_limit(cv, nx, stop / d.xStep, false, sh, &ish);
@@ -290,6 +288,20 @@ __global__ void __launch_bounds__(MOM_T) mom_cols_kernel(const MomArgs a)
         acc += (double)mom_int(ex, ey);
     }
     col[ix] = acc;
+}
+
+// 3b. column totals over the row segments, in place into segment 0: one warp per column, each lane
+// adding every 32nd segment, then a shuffle tree (fixed order)
+__global__ void __launch_bounds__(MOM_T) mom_colsum_kernel(const MomArgs a)
+{
+    const int nx = a.d->nx;
+    const int c = blockIdx.x * (MOM_T / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (c >= nx) return;
+    double* col = a.sc + a.offCol;
+    double s = 0.;
+    for (int k = lane; k < a.S; k += 32) s += col[(size_t)k * nx + c];
+    s = warp_sum(s);
+    if (lane == 0) col[c] = s;                  // every lane of this warp has read its segments
 }
 
 // the 11 weighted terms of one component at one point (sroptelm.cpp:1770-1906): c the value, l
@@ -411,9 +423,10 @@ cudaError_t launch_moments(const MomLaunch& p, cudaStream_t st)
         a.S = S;
         a.RS = (nz + S - 1) / S;
         a.offCol = offCol; a.offPart = offPart; a.offLim = offLim;
-        mom_rows_kernel<<<(nz + MOM_RPC - 1) / MOM_RPC, MOM_T, 0, st>>>(a);
+        mom_rows_kernel<<<nz, MOM_T, 0, st>>>(a);
         mom_limits_kernel<<<1, MOM_LT, 0, st>>>(a, 0);
         mom_cols_kernel<<<dim3(cx, S), MOM_T, 0, st>>>(a);
+        mom_colsum_kernel<<<(nx + MOM_T / 32 - 1) / (MOM_T / 32), MOM_T, 0, st>>>(a);
         mom_limits_kernel<<<1, MOM_LT, 0, st>>>(a, 1);
         mom_sums_kernel<<<dim3(cx, cz5), MOM_T, 0, st>>>(a);
         mom_final_kernel<<<1, 22 * 32, 0, st>>>(a, cx * cz5);

@@ -220,6 +220,8 @@ extern "C" SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRW
         pWfrOut->mesh.ne = 1; pWfrOut->mesh.nx = w.nx; pWfrOut->mesh.ny = w.nz;
         pWfrOut->Rx = w.RobsX; pWfrOut->Ry = w.RobsZ; pWfrOut->dRx = w.RobsXAbsErr; pWfrOut->dRy = w.RobsZAbsErr;
         pWfrOut->xc = w.xc; pWfrOut->yc = w.zc; pWfrOut->presCA = (char)w.Pres; pWfrOut->avgPhotEn = w.avgPhotEn;
+        if (pWfrOut->arElecPropMatr != nullptr && w.havePropM)
+            for (int m = 0; m < 20; m++) pWfrOut->arElecPropMatr[m] = w.propM[m];
         double mx[11], mz[11];
         for (int m = 0; m < 11; m++) { mx[m] = w.momX[m]; mz[m] = w.momZ[m]; }
         if (nSlotD && (pWfrOut->arMomX || pWfrOut->arMomY)) {

@@ -974,6 +974,28 @@ void Planner::drift(const ElemDesc& e, int anal)
     w.RobsX += e.L;                       // PropagateWaveFrontRadius (sroptdrf.h:981)
     w.RobsZ += e.L;
     set_full_range();
+    // Propagate4x4PropMatr of the drift (sroptdrf.h:1002): no vector
+    const double D[16] = {1., e.L, 0., 0., 0., 1., 0., 0., 0., 0., 1., e.L, 0., 0., 0., 1.};
+    const double v0[4] = {0., 0., 0., 0.};
+    prop_4x4(D, v0);
+}
+
+// GenAuxPropagate4x4PropMatr (sroptelm.cpp:5594): M <- E M, V <- E V + e for the element's 4x4 matrix
+// E and vector e (the wavefront's arElecPropMatr: 16 matrix entries, then the vector)
+void Planner::prop_4x4(const double E[16], const double e[4])
+{
+    double R[16], V[4];
+    for (int i = 0; i < 4; i++) {
+        V[i] = 0.;
+        for (int j = 0; j < 4; j++) {
+            double r = 0.;
+            for (int k = 0; k < 4; k++) r += E[4 * i + k] * w.propM[4 * k + j];
+            R[4 * i + j] = r;
+            V[i] += E[4 * i + j] * w.propM[16 + j];
+        }
+    }
+    for (int i = 0; i < 16; i++) w.propM[i] = R[i];
+    for (int i = 0; i < 4; i++) w.propM[16 + i] = V[i] + e[i];
 }
 
 // ================================================================================================
@@ -1066,6 +1088,10 @@ void Planner::lens(const ElemDesc& e)
     w.RobsZAbsErr *= (MagnZ * MagnZ);
     w.xc = e.x - (e.x - w.xc) * MagnX;
     w.zc = e.y - (e.y - w.zc) * MagnZ;
+    // Propagate4x4PropMatr of the focusing element (sroptfoc.h:101)
+    const double Foc[16] = {1., 0., 0., 0., -1. / e.Fx, 1., 0., 0., 0., 0., 1., 0., 0., 0., -1. / e.Fy, 1.};
+    const double fv[4] = {0., e.x / e.Fx, 0., e.y / e.Fy};
+    prop_4x4(Foc, fv);
     fix_abs_err();
     phase_lin_reset();
 }
@@ -1318,6 +1344,10 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
     w.avgPhotEn = pw->avgPhotEn;
     if (pw->arMomX != nullptr) { for (int i = 0; i < 11; i++) w.momX[i] = pw->arMomX[i]; w.haveMom = true; }
     if (pw->arMomY != nullptr) for (int i = 0; i < 11; i++) w.momZ[i] = pw->arMomY[i];
+    if (pw->arElecPropMatr != nullptr) {
+        for (int i = 0; i < 20; i++) w.propM[i] = pw->arElecPropMatr[i];
+        w.havePropM = true;
+    }
     if (m.ne != 1) { err = "only ne == 1 wavefronts are supported on the GPU path"; return SRWG_ERR_UNSUPPORTED; }
     if (pw->presFT != 0) { err = "time-domain wavefronts are not supported on the GPU path"; return SRWG_ERR_UNSUPPORTED; }
     if (pw->numTypeElFld != 0 && pw->numTypeElFld != 'f') { err = "only float fields are supported"; return SRWG_ERR_UNSUPPORTED; }

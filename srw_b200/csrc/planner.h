@@ -25,6 +25,8 @@ struct WfrState {
     double dxcSub = 0, dzcSub = 0;
     bool QuadX = false, QuadZ = false;
     double momX[11] = {0}, momZ[11] = {0};
+    double propM[20] = {0};      // 4x4 propagation matrix and 4-vector (SRWLWfr::arElecPropMatr)
+    bool havePropM = false;
     bool haveMom = false;
 };
 
@@ -127,6 +129,7 @@ private:
     int drift_quad(const ElemDesc& e, int subtype);
     void drift_moments(double L);
     void record_matrix(const double ax[2][2], const double az[2][2], int clamp, double sx, double sz);
+    void prop_4x4(const double E[16], const double e[4]);
     bool momProvisional = false;         // plan-time moments wait for a MOM pass's result
     void lens(const ElemDesc& e);
     void aperture(const ElemDesc& e);

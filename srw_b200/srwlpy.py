@@ -76,6 +76,8 @@ def make_c_wfr(wfr, keep):
     w.unitElFldAng = _chr(int(getattr(wfr, 'unitElFldAng', 0)), b'\0')
     w.arMomX = _buf_ptr(getattr(wfr, 'arMomX', None), keep, np.float64) if len(getattr(wfr, 'arMomX', [])) >= 11 else None
     w.arMomY = _buf_ptr(getattr(wfr, 'arMomY', None), keep, np.float64) if len(getattr(wfr, 'arMomY', [])) >= 11 else None
+    pm = getattr(wfr, 'arElecPropMatr', None)
+    w.arElecPropMatr = _buf_ptr(pm, keep, np.float64) if pm is not None and len(pm) >= 20 else None
     return w
 
 
@@ -169,6 +171,8 @@ def _modif(action, pw, pol):
         w.arEy = _buf_ptr(wfr.arEy, keep, np.float32)
         w.arMomX = _buf_ptr(wfr.arMomX, keep, np.float64) if len(wfr.arMomX) >= 11 else None
         w.arMomY = _buf_ptr(wfr.arMomY, keep, np.float64) if len(wfr.arMomY) >= 11 else None
+        pm = getattr(wfr, 'arElecPropMatr', None)
+        w.arElecPropMatr = _buf_ptr(pm, keep, np.float64) if pm is not None and len(pm) >= 20 else None
         return 0
     except Exception:
         return -1

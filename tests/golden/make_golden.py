@@ -109,7 +109,8 @@ def snapshot(w):
     return dict(ex=ex, ey=ey,
                 mesh=np.array([m.nx, m.ny, m.xStart, m.xFin, m.yStart, m.yFin, m.eStart, m.zStart], np.float64),
                 scal=np.array([w.Rx, w.Ry, w.dRx, w.dRy, w.xc, w.yc, w.avgPhotEn, w.presCA], np.float64),
-                momx=np.array(w.arMomX, np.float64)[:11], momy=np.array(w.arMomY, np.float64)[:11])
+                momx=np.array(w.arMomX, np.float64)[:11], momy=np.array(w.arMomY, np.float64)[:11],
+                prop=np.array(w.arElecPropMatr, np.float64)[:20])
 
 
 PP0 = [0, 0, 1, 0, 0, 1., 1., 1., 1., 0, 0, 0]
@@ -197,6 +198,9 @@ def main():
     index = []
     for name, make, elems, pps in cases(L):
         w = make()
+        # a 4x4 propagation matrix and vector to carry through the drifts (arElecPropMatr)
+        w.arElecPropMatr = array('d', [1., 0.5, 0., 0., 0., 1., 0., 0., 0., 0., 1., -0.25, 0., 0., 0., 1.,
+                                       1e-4, 2e-6, -3e-4, 4e-6])
         inp = snapshot(w)
         opt = L.SRWLOptC(build_beamline(L, elems), [list(map(float, p)) for p in pps])
         L.srwl.PropagElecField(w, opt)

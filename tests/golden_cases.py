@@ -40,6 +40,7 @@ def case_io(d, name):
                     dRx=float(sc[2]), dRy=float(sc[3]), xc=float(sc[4]), yc=float(sc[5]),
                     presCA=int(sc[7]), momX=np.array(d[name + '/' + s + '/momx']),
                     momY=np.array(d[name + '/' + s + '/momy']),
+                    prop=np.array(d[name + '/' + s + '/prop']),
                     mesh_raw=np.array(m[:6]))
     return side('in'), side('out')
 

@@ -12,7 +12,7 @@ import srw_oracle as O  # noqa: E402  (the checker)
 from srw_b200.srwlib import SRWLOptA, SRWLOptC, SRWLOptD, SRWLOptL, SRWLWfr  # noqa: E402
 
 
-def make_wfr(ex, ey, mesh, Rx=0., Ry=0., dRx=0., dRy=0., xc=0., yc=0., momX=None, momY=None, presCA=0):
+def make_wfr(ex, ey, mesh, Rx=0., Ry=0., dRx=0., dRy=0., xc=0., yc=0., momX=None, momY=None, presCA=0, propM=None):
     ny, nx = ex.shape
     w = SRWLWfr()
     w.allocate(1, nx, ny)
@@ -30,6 +30,8 @@ def make_wfr(ex, ey, mesh, Rx=0., Ry=0., dRx=0., dRy=0., xc=0., yc=0., momX=None
     if momX is not None:
         w.arMomX = array('d', list(momX))
         w.arMomY = array('d', list(momY))
+    if propM is not None:
+        w.arElecPropMatr = array('d', list(propM))
     return w
 
 

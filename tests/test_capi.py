@@ -43,8 +43,19 @@ def plan_case(name):
     c = next(c for c in INDEX if c['name'] == name)
     i, o = case_io(D, name)
     w = make_wfr(i['ex'], i['ey'], i['mesh'], i['Rx'], i['Ry'], i['dRx'], i['dRy'], i['xc'], i['yc'],
-                 i['momX'], i['momY'])
+                 i['momX'], i['momY'], propM=i['prop'])
     return Plan(w, beamline(c['elements'], c['props'])), o
+
+
+def plan_prop_matrix(p):
+    """arElecPropMatr of a plan's output (the 4x4 propagation matrix and vector)."""
+    import ctypes as C
+    from srw_b200 import capi
+    out = capi.SRWLWfr()
+    m = np.zeros(20)
+    out.arElecPropMatr = m.ctypes.data
+    assert capi.lib().srwgPlanGetOutput(p._h, C.byref(out)) == 0
+    return m
 
 
 @pytest.mark.parametrize('name', [c['name'] for c in INDEX])
@@ -54,6 +65,7 @@ def test_planner_mesh_bit_exact(name):
             plan_case(name)
         return
     p, o = plan_case(name)
+    np.testing.assert_allclose(plan_prop_matrix(p), o['prop'], rtol=1e-14, atol=1e-300)
     m = p.output_mesh()
     mine = np.array([m['nx'], m['ny'], m['xStart'], m['xFin'], m['yStart'], m['yFin']])
     assert np.array_equal(mine, o['mesh_raw']), (mine, o['mesh_raw'])

@@ -39,8 +39,9 @@ def test_golden_case(name):
     c = next(c for c in INDEX if c['name'] == name)
     i, o = case_io(D, name)
     w = run_gpu(i['ex'], i['ey'], i['mesh'], c['elements'], c['props'], Rx=i['Rx'], Ry=i['Ry'], dRx=i['dRx'],
-                dRy=i['dRy'], xc=i['xc'], yc=i['yc'], momX=i['momX'], momY=i['momY'])
+                dRy=i['dRy'], xc=i['xc'], yc=i['yc'], momX=i['momX'], momY=i['momY'], propM=i['prop'])
     assert mesh_close(mesh_tuple(w), o['mesh_raw'], name in STAGED)
+    np.testing.assert_allclose(np.array(w.arElecPropMatr), o['prop'], rtol=1e-14, atol=1e-300)
     scal = [w.Rx, w.Ry, w.dRx, w.dRy, w.xc, w.yc]
     ref = [o['Rx'], o['Ry'], o['dRx'], o['dRy'], o['xc'], o['yc']]
     if name in STAGED:      # planned on moments measured from the FP32 field

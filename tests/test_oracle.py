@@ -31,7 +31,7 @@ def run_oracle(name):
     c = next(c for c in INDEX if c['name'] == name)
     i, o = case_io(D, name)
     w = O.Wfr.from_srwl(i['ex'], i['ey'], i['mesh'], i['Rx'], i['Ry'], i['dRx'], i['dRy'], i['xc'], i['yc'],
-                        i['presCA'], i['momX'], i['momY'])
+                        i['presCA'], i['momX'], i['momY'], propM=i['prop'])
     O.propagate(w, [tuple(e) for e in c['elements']], c['props'])
     return w, o
 
@@ -54,6 +54,7 @@ def test_oracle_vs_reference(name):
     I_m = np.abs(w.ex) ** 2 + np.abs(w.ey) ** 2
     I_r = np.abs(o['ex']) ** 2 + np.abs(o['ey']) ** 2
     assert rel_l2(I_m, I_r) < 1e-5
+    np.testing.assert_allclose(w.propM, o['prop'], rtol=1e-14, atol=1e-300)      # 4x4 propagation matrix
     if name not in MOMENT_RECOMPUTED:
         np.testing.assert_allclose(w.momX, o['momX'], rtol=1e-12, atol=0)
         np.testing.assert_allclose(w.momZ, o['momY'], rtol=1e-12, atol=0)

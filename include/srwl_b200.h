@@ -41,6 +41,20 @@ struct SRWLStructParticleBeam {
 };
 typedef struct SRWLStructParticleBeam SRWLPartBeam;
 
+/* SRWLGsnBm (srwlib.h:211-222): a (Hermite-)Gaussian beam at its waist */
+struct SRWLStructGaussianBeam {
+    double x, y, z;
+    double xp, yp;
+    double avgPhotEn;
+    double pulseEn;
+    double repRate;
+    char polar;
+    double sigX, sigY;
+    double sigT;
+    char mx, my;
+};
+typedef struct SRWLStructGaussianBeam SRWLGsnBm;
+
 struct SRWLStructRadMesh {
     double eStart, eFin, xStart, xFin, yStart, yFin, zStart;
     long ne, nx, ny;
@@ -113,6 +127,13 @@ typedef struct SRWLStructOpticsContainer SRWLOptC;
  * not supported and must be 0.  Not thread-safe, like the reference. */
 SRWG_API int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SRWLRadMesh* arIM, char** arI,
                         double* arParGPU);
+
+/* Replaces srwlCalcElecFieldGaussian (cpp/src/lib/srwlib.h, srwlib.cpp:544) for a single photon energy
+ * without automatic sampling (precPar NULL or precPar[0] = 0): fills arEx / arEy (host memory, the
+ * wavefront's mesh) with the field computed on the GPU, and sets Rx, Ry, dRx, dRy, xc, yc, the
+ * moments (recomputed from the field) and the 4x4 matrix block of arElecPropMatr as the reference
+ * does.  Automatic sampling and time-domain wavefronts return error 23900. */
+SRWG_API int srwlCalcElecFieldGaussian(SRWLWfr* pWfr, SRWLGsnBm* pGsnBm, double* precPar);
 
 /* Replaces srwlCalcIntFromElecField (cpp/src/lib/srwlib.h:748, srwlib.cpp:757) for wavefronts at a
  * single photon energy (ne == 1) vs x and y (depType 3): intType 0 (single-electron intensity),

@@ -1464,6 +1464,101 @@ def total_intensity(ex, ey):
     return (ex.real * ex.real + ex.imag * ex.imag + ey.real * ey.real + ey.imag * ey.imag).astype(np.float32)
 
 
+def _hermite(n, x):
+    """srTGsnBeam::HermitePolynomial (srgsnbm.cpp:97): physicists' Hermite polynomial by recursion."""
+    if n == 0:
+        return np.ones_like(x)
+    if n == 1:
+        return 2. * x
+    return 2. * (x * _hermite(n - 1, x) - (n - 1) * _hermite(n - 2, x))
+
+
+def calc_elec_field_gaussian(mesh, gb, unit_el_fld=1, part_z=0.):
+    """srwlCalcElecFieldGaussian (cpp/src/lib/srwlib.cpp:544) for a single photon energy without
+    automatic sampling (precPar[0] = 0): srTGsnBeam (srgsnbm.cpp:15-78), its frequency-domain field
+    (CreateWavefrontElFieldFreqDomain, :230-310, SetupSourceConstantsFreqDomain :104-126,
+    SetupProperPolariz srgsnbm.h:74), the wavefront scalars of AuxSetupActionsArbSrc
+    (srradstr.cpp:324-349) and the moments (ComputeRadMoments of the FP32 field).  ``gb``: dict with
+    the SRWLGsnBm fields.  Returns the Wfr (FP32-rounded field) and the 20 entries of the 4x4
+    propagation matrix block InitialSetupOf4x4PropMatr writes (srradstr.h:399)."""
+    Pi = 3.1415926535898
+    sqrt_2 = math.sqrt(2.)
+    SigmaX, SigmaZ = gb['sigX'] * sqrt_2, gb['sigY'] * sqrt_2
+    mx, mz = int(gb['mx']), int(gb['my'])
+    SigmaPhotEn = (0.5 * 6.58211889E-16 / gb['sigT']) * sqrt_2 if gb['sigT'] > 0 else 1.e+23
+    PhotPerBW = -1.
+    if gb['pulseEn'] > 0 and gb['sigT'] > 0:
+        PhotPerBW = 6.2415096E+15 * gb['pulseEn'] / (math.sqrt(Pi) * SigmaPhotEn)
+        if gb['repRate'] > 0:
+            PhotPerBW *= gb['repRate']
+    AuxConst = float(1 << (mx + mz)) * math.factorial(mx) * math.factorial(mz)
+    NormConst = math.sqrt(PhotPerBW / (AuxConst * ((1.E+06) * Pi)))
+    if unit_el_fld == 2:
+        NormConst *= math.sqrt(1.602176462e-16)
+    x0, dxds0, z0, dzds0, s0 = gb['x'], gb['xp'], gb['y'], gb['yp'], gb['z']
+    PhEnConv = 1.239842E-06
+    en = mesh['eStart']
+    Robs = mesh['zStart'] - s0
+    LongDist = Robs
+    if LongDist == 0.:
+        LongDist = 0.01 * (PhEnConv / en)
+    InvTwoSigXe2, InvTwoSigZe2 = 0.5 / (SigmaX * SigmaX), 0.5 / (SigmaZ * SigmaZ)
+    InvTwoSigPhotEnE2 = 0.5 / (SigmaPhotEn * SigmaPhotEn)
+    Buf = (Pi * 1.) / (PhEnConv * LongDist)
+    PropagMultX, PropagMultZ = Buf / InvTwoSigXe2, Buf / InvTwoSigZe2
+    x0Prop, z0Prop = x0 + dxds0 * LongDist, z0 + dzds0 * LongDist
+    nx, ny = int(mesh['nx']), int(mesh['ny'])
+    xStep = (mesh['xFin'] - mesh['xStart']) / (nx - 1)
+    zStep = (mesh['yFin'] - mesh['yStart']) / (ny - 1)
+    ix = np.arange(nx)[None, :]
+    iz = np.arange(ny)[:, None]
+    x = (mesh['xStart'] - x0Prop) + ix * xStep
+    z = (mesh['yStart'] - z0Prop) + iz * zStep
+    x_mi_x0 = (mesh['xStart'] - x0) + ix * xStep
+    z_mi_z0 = (mesh['yStart'] - z0) + iz * zStep
+    xx, zz = x_mi_x0 + x0, z_mi_z0 + z0
+    enMult = 2.53384080189E+06
+    InvLongDist = 1. / LongDist
+    PropRatX, PropRatZ = en * PropagMultX, en * PropagMultZ
+    InvPropRatX, InvPropRatZ = 1. / PropRatX, 1. / PropRatZ
+    SigMultX, SigMultZ = 1. + InvPropRatX * InvPropRatX, 1. + InvPropRatZ * InvPropRatZ
+    DisMultX, DisMultZ = 1. + PropRatX * PropRatX, 1. + PropRatZ * PropRatZ
+    PropInvTwoSigXe2, PropInvTwoSigZe2 = InvTwoSigXe2 / SigMultX, InvTwoSigZe2 / SigMultZ
+    PropInvSigX, PropInvSigZ = math.sqrt(2. * PropInvTwoSigXe2), math.sqrt(2. * PropInvTwoSigZe2)
+    PropInvRx, PropInvRz = InvLongDist / DisMultX, InvLongDist / DisMultZ
+    xpMult = (1. / PropInvRx - LongDist) * dxds0
+    zpMult = (1. / PropInvRz - LongDist) * dzds0
+    NuX, NuZ = math.atan(InvPropRatX), math.atan(InvPropRatZ)
+    Phase = en * enMult * ((x_mi_x0 * x_mi_x0 + 2 * LongDist * x0 * dxds0 + xpMult * (2 * xx - LongDist * dxds0)) * PropInvRx
+                           + (z_mi_z0 * z_mi_z0 + 2 * LongDist * z0 * dzds0 + zpMult * (2 * zz - LongDist * dzds0)) * PropInvRz) \
+        + (mx + 0.5) * NuX + (mz + 0.5) * NuZ
+    TwoPI = 6.28318530717959
+    Phase = Phase - TwoPI * np.trunc(Phase * (1. / TwoPI))
+    arg = -(x * x) * PropInvTwoSigXe2 - (z * z) * PropInvTwoSigZe2
+    if gb['avgPhotEn'] > 0:
+        d = en - gb['avgPhotEn']
+        arg = arg - d * d * InvTwoSigPhotEnE2
+    BufA = NormConst * math.sqrt(PropInvSigX * PropInvSigZ) * np.exp(arg) * _hermite(mx, x * PropInvSigX) * \
+        _hermite(mz, z * PropInvSigZ)
+    ReA, ImA = BufA * np.cos(Phase), BufA * np.sin(Phase)
+    c = 0.70710678118655
+    zero = np.zeros_like(ReA)
+    pol = int(gb['polar'])
+    comps = {1: (ReA, ImA, zero, zero), 2: (zero, zero, ReA, ImA), 3: (c * ReA, c * ImA, c * ReA, c * ImA),
+             4: (c * ReA, c * ImA, -c * ReA, -c * ImA), 5: (c * ReA, c * ImA, -c * ImA, c * ReA),
+             6: (c * ReA, c * ImA, c * ImA, -c * ReA)}[pol]
+    f32 = [np.asarray(v, np.float32) for v in comps]
+    ex = (f32[0] + 1j * f32[1]).astype(np.complex64)
+    ey = (f32[2] + 1j * f32[3]).astype(np.complex64)
+    w = Wfr.from_srwl(ex, ey, mesh, Robs, Robs, 0.01 * abs(Robs), 0.01 * abs(Robs), x0, z0)
+    compute_rad_moments(w)
+    d = mesh['zStart'] - part_z
+    prop = np.zeros(16)
+    prop[[0, 5, 10, 15]] = 1.
+    prop[1] = prop[11] = d
+    return w, prop
+
+
 def _formal_phase(re, im):
     """FormalPhase (srradmnp.h:434): the argument of re + i im from atan of the FP32 ratio, in the
     quadrant of (re, im) (-pi - ... pi, the reference's branch conventions and pi constants)."""

@@ -13,7 +13,7 @@ OBJ_DIR = os.path.join(HERE, '_build')          # objects: kept out of the shipp
 LIB = os.path.join(OUT_DIR, 'libsrwl_b200.so')
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
-SOURCES = ['kernels.cu'] + ['line2_%d.cu' % l for l in range(6, 15)] + ['line2e_%d.cu' % l for l in range(6, 15)] + ['planner.cpp', 'tables.cpp', 'capi.cpp', 'noalloc.cu', 'lineg.cu', 'lineg_e.cu', 'multie.cu', 'mlp.cu', 'moments.cu', 'intensity.cu']
+SOURCES = ['kernels.cu'] + ['line2_%d.cu' % l for l in range(6, 15)] + ['line2e_%d.cu' % l for l in range(6, 15)] + ['planner.cpp', 'tables.cpp', 'capi.cpp', 'noalloc.cu', 'lineg.cu', 'lineg_e.cu', 'multie.cu', 'mlp.cu', 'moments.cu', 'intensity.cu', 'gaussian.cu']
 # host code: no FP contraction so the mesh bookkeeping rounds exactly like the reference
 HOST_FLAGS = '-O2,-fPIC,-ffp-contract=off,-fvisibility=hidden'
 

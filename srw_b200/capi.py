@@ -30,6 +30,12 @@ class SRWLRadMesh(C.Structure):
                 ('itFin', C.c_longlong)]
 
 
+class SRWLGsnBm(C.Structure):
+    _fields_ = [('x', C.c_double), ('y', C.c_double), ('z', C.c_double), ('xp', C.c_double), ('yp', C.c_double),
+                ('avgPhotEn', C.c_double), ('pulseEn', C.c_double), ('repRate', C.c_double), ('polar', C.c_char),
+                ('sigX', C.c_double), ('sigY', C.c_double), ('sigT', C.c_double), ('mx', C.c_char), ('my', C.c_char)]
+
+
 class SRWLWfr(C.Structure):
     _fields_ = [('arEx', C.c_void_p), ('arEy', C.c_void_p), ('arExAux', C.c_void_p), ('arEyAux', C.c_void_p),
                 ('mesh', SRWLRadMesh), ('Rx', C.c_double), ('Ry', C.c_double), ('dRx', C.c_double),
@@ -61,6 +67,7 @@ MODIF_FUNC = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(SRWLWfr), C.c_char)
 
 # symbol -> (restype, argtypes); the complete exported surface of include/srwl_b200.h
 SYMBOLS = {
+    'srwlCalcElecFieldGaussian': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLGsnBm), C.c_void_p]),
     'srwlCalcIntFromElecField': (C.c_int, [C.c_void_p, C.POINTER(SRWLWfr), C.c_char, C.c_char, C.c_char, C.c_double,
                                            C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     'srwlPropagElecField': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_int, C.c_void_p, C.c_void_p,

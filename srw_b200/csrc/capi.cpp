@@ -486,6 +486,8 @@ int srwlUtiGetErrText(char* t, int erNo)
     case UNKNOWN_OPTICAL_ELEMENT: s = "Unknown optical element or incorrect optical element definition."; break;
     case ERROR_IN_FFT: s = "Error in FFT."; break;
     case CAN_NOT_PROPAGATE_1D_RAD: s = "Propagation needs more than one point in both the horizontal and the vertical direction."; break;
+    case PHOT_EN_SHOULD_BE_POSITIVE: s = "Photon energy should be positive."; break;
+    case SRWL_INCORRECT_PARAM_FOR_GAUS_BEAM_COMP: s = "Incorrect or insufficient parameters for Gaussian beam calculation."; break;
     case SRWL_INCORRECT_PARAM_FOR_INT_EXTR: s = "Incorrect or insufficient parameters for intensity extraction."; break;
     case SRWL_WFR_EXT_MODIF_FAILED: s = "The wavefront modification (re-allocation) callback failed."; break;
     case SRWL_INCORRECT_PARAM_FOR_WFR_PROP: s = "Incorrect or insufficient parameters for wavefront propagation."; break;

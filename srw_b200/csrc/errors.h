@@ -7,6 +7,8 @@
 #define UNKNOWN_OPTICAL_ELEMENT (39 + SRWG_FIRST_ERR)
 #define ERROR_IN_FFT (40 + SRWG_FIRST_ERR)
 #define CAN_NOT_PROPAGATE_1D_RAD (59 + SRWG_FIRST_ERR)
+#define PHOT_EN_SHOULD_BE_POSITIVE (109 + SRWG_FIRST_ERR)
+#define SRWL_INCORRECT_PARAM_FOR_GAUS_BEAM_COMP (165 + SRWG_FIRST_ERR)
 #define SRWL_INCORRECT_PARAM_FOR_INT_EXTR (166 + SRWG_FIRST_ERR)
 #define SRWL_WFR_EXT_MODIF_FAILED (168 + SRWG_FIRST_ERR)
 #define SRWL_INCORRECT_PARAM_FOR_WFR_PROP (171 + SRWG_FIRST_ERR)

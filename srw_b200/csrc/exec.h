@@ -22,6 +22,8 @@ struct DeviceCtx {
     float2* stg[2] = {nullptr, nullptr};  // stage outputs of a staged propagation (2 components each)
     void* intBuf = nullptr;             // intensity extraction: both components and the result
     size_t intBytes = 0;
+    void* genBuf = nullptr;             // field generation: both components, tables, moment scratch
+    size_t genBytes = 0;
     size_t stgElems[2] = {0, 0};
     cudaStream_t stream = nullptr;
 };

@@ -539,7 +539,7 @@ static bool mom_outside(const double* mx, const double* mz, const MomOp& op)
 
 // the 22 sums of a MOM pass normalised into the 11 moments of Ex and of Ez, each rounded to FP32 as
 // the reference stores them (sroptelm.cpp:1937-2080, coordinate representation)
-static void moments_from_sums(const double* S, const MomOp& op, double* mx, double* mz)
+void moments_from_sums(const double* S, const MomOp& op, double* mx, double* mz)
 {
     const double FourPi = 3.141592653590 * 2. * 2.;
     const double lam_d_4pi = 1.239842E-06 / (FourPi * op.eStart);
@@ -616,9 +616,19 @@ static bool estimate_moments(const MomOp& op, const double* S, double* mx, doubl
 void Planner::emit_moment_pass(MomOp& op, bool certain)
 {
     op.slot = nMomSlots++;
+    MomDesc& d = b->moments(w);
+    fill_moment_desc(w, d, op);
+    if (certain) { w.QuadX = op.qx; w.QuadZ = op.qz; }
+    else quadFlagsUncertain_ = true;
+    momProvisional = true;
+}
+
+// the MOM pass descriptor of a wavefront state (adds to the point-wise work already in d.pw) and the
+// mesh / flags of its bookkeeping op; op.slot must be set
+void fill_moment_desc(const WfrState& w, MomDesc& d, MomOp& op)
+{
     op.nx = w.nx; op.nz = w.nz; op.eStart = w.eStart;
     op.xStart = w.xStart; op.xStep = w.xStep; op.zStart = w.zStart; op.zStep = w.zStep;
-    MomDesc& d = b->moments(w);
     d.nx = w.nx; d.nz = w.nz;
     d.xStart = w.xStart; d.xStep = w.xStep; d.zStart = w.zStart; d.zStep = w.zStep;
     d.slot = op.slot;
@@ -628,8 +638,6 @@ void Planner::emit_moment_pass(MomOp& op, bool certain)
     const bool qx = ::fabs(w.RobsXAbsErr) < 0.4 * ::fabs(w.RobsX);
     const bool qz = ::fabs(w.RobsZAbsErr) < 0.4 * ::fabs(w.RobsZ);
     op.qx = qx; op.qz = qz;
-    if (certain) { w.QuadX = qx; w.QuadZ = qz; }
-    else quadFlagsUncertain_ = true;
     if (qx || qz) {
         const double Const = 3.14159265358979 * 1.E+06 / 1.23984186;
         const double cx = qx ? -Const / w.RobsX * w.eStart : 0., cz = qz ? -Const / w.RobsZ * w.eStart : 0.;
@@ -642,7 +650,17 @@ void Planner::emit_moment_pass(MomOp& op, bool certain)
     const double Rx = (w.RobsX != 0.) ? w.RobsX : 100. * lam, Rz = (w.RobsZ != 0.) ? w.RobsZ : 100. * lam;
     d.ax = 0.5 * (w.xStep * ((1. / lam_d_4pi) / Rx));
     d.az = 0.5 * (w.zStep * ((1. / lam_d_4pi) / Rz));
-    momProvisional = true;
+}
+
+void single_moment_pass(const WfrState& w, KernelDesc& k, MomOp& op, std::vector<float2>& tables)
+{
+    std::vector<KernelDesc> ks(1);
+    memset(&ks[0], 0, sizeof(KernelDesc));
+    ks[0].kind = K_MOM;
+    op.slot = 0;
+    fill_moment_desc(w, ks[0].mom, op);
+    build_tables(ks, tables);
+    k = ks[0];
 }
 
 // EstimateWfrRadToSub_AnalytTreatQuadPhaseTerm (sroptdrf.cpp:1123-1365): the radius to subtract in

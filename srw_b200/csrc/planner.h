@@ -70,6 +70,12 @@ struct PropDesc {
 
 class Builder;
 
+// one stand-alone MOM pass (ComputeRadMoments) on a wavefront in the state w, result slot 0: its
+// descriptor, its point-wise tables, and the op that turns its sums into moments (moments_from_sums)
+void fill_moment_desc(const WfrState& w, MomDesc& d, MomOp& op);
+void single_moment_pass(const WfrState& w, KernelDesc& k, MomOp& op, std::vector<float2>& tables);
+void moments_from_sums(const double* S, const MomOp& op, double* momX, double* momZ);
+
 // fills the separable point-wise tables of every pass (tables.cpp)
 void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& tables);
 

@@ -111,3 +111,14 @@ class SRWLOptC(object):
     def __init__(self, _arOpt=None, _arProp=None):
         self.arOpt = [] if _arOpt is None else _arOpt
         self.arProp = [] if _arProp is None else _arProp
+
+
+class SRWLGsnBm(object):
+    """(Coherent) Gaussian beam at its waist, the reference's SRWLGsnBm (env/python/srwpy/srwlib.py:741)
+    with the same attribute names and defaults."""
+
+    def __init__(self, _x=0, _y=0, _z=0, _xp=0, _yp=0, _avgPhotEn=1, _pulseEn=1, _repRate=1, _polar=1, _sigX=10e-06,
+                 _sigY=10e-06, _sigT=1e-15, _mx=0, _my=0):
+        self.x, self.y, self.z, self.xp, self.yp = _x, _y, _z, _xp, _yp
+        self.avgPhotEn, self.pulseEn, self.repRate, self.polar = _avgPhotEn, _pulseEn, _repRate, _polar
+        self.sigX, self.sigY, self.sigT, self.mx, self.my = _sigX, _sigY, _sigT, _mx, _my

@@ -78,6 +78,9 @@ def make_c_wfr(wfr, keep):
     w.arMomY = _buf_ptr(getattr(wfr, 'arMomY', None), keep, np.float64) if len(getattr(wfr, 'arMomY', [])) >= 11 else None
     pm = getattr(wfr, 'arElecPropMatr', None)
     w.arElecPropMatr = _buf_ptr(pm, keep, np.float64) if pm is not None and len(pm) >= 20 else None
+    pb = getattr(wfr, 'partBeam', None)
+    if pb is not None and getattr(pb, 'partStatMom1', None) is not None:
+        w.partBeam.partStatMom1.z = float(getattr(pb.partStatMom1, 'z', 0.))
     return w
 
 
@@ -229,3 +232,27 @@ def CalcIntFromElecField(arI, wfr, pol, intType, depType, e, x, y, meth=None, fl
     if r > 0:
         raise RuntimeError(capi.err_text(r))
     return arI
+
+
+def CalcElecFieldGaussian(wfr, gsnBm, precPar=None):
+    """srwlpy.CalcElecFieldGaussian: the field of a Gaussian beam on ``wfr``'s mesh, computed on the GPU
+    (single photon energy, no automatic sampling); sets the radius, centre, moments and 4x4 matrix."""
+    keep = []
+    w = make_c_wfr(wfr, keep)
+    g = capi.SRWLGsnBm()
+    for k in ('x', 'y', 'z', 'xp', 'yp', 'avgPhotEn', 'pulseEn', 'repRate', 'sigX', 'sigY', 'sigT'):
+        setattr(g, k, float(getattr(gsnBm, k)))
+    g.polar = C.c_char(int(gsnBm.polar))
+    g.mx = C.c_char(int(gsnBm.mx))
+    g.my = C.c_char(int(gsnBm.my))
+    pp = None
+    if precPar is not None:
+        a = np.zeros(max(1, len(precPar)))
+        a[:len(precPar)] = np.asarray(precPar, np.float64)
+        keep.append(a)
+        pp = a.ctypes.data
+    r = capi.lib().srwlCalcElecFieldGaussian(C.byref(w), C.byref(g), pp)
+    if r > 0:
+        raise RuntimeError(capi.err_text(r))
+    _update_py_wfr(wfr, w)
+    return wfr

@@ -248,6 +248,49 @@ def main():
                 blob[key] = np.array(arI, np.float64 if it == 4 else np.float32)
                 ints.append(dict(key=key, int_type=it, pol=pol, meth=meth))
     blob['int/index'] = np.array(json.dumps(ints))
+    # 4) Gaussian beams (srwlCalcElecFieldGaussian, precPar = [0]): waist at the observation plane,
+    #    offsets / angles / Hermite modes / every polarisation, field units, spectral detuning
+    gcases = [
+        ('g_waist', dict(x=0., y=0., z=0., xp=0., yp=0., avgPhotEn=1000., pulseEn=0.001, repRate=1., polar=1,
+                         sigX=50e-6, sigY=50e-6, sigT=10e-15, mx=0, my=0), dict(n=(64, 64), r=(1e-3, 1e-3), e=1000.,
+                                                                                 z=0., unit=1)),
+        ('g_modes_circ', dict(x=20e-6, y=-10e-6, z=-5., xp=5e-6, yp=-3e-6, avgPhotEn=3003., pulseEn=0.002,
+                              repRate=10., polar=5, sigX=30e-6, sigY=20e-6, sigT=20e-15, mx=2, my=1),
+         dict(n=(80, 64), r=(0.6e-3, 0.5e-3), e=3000., z=10., unit=2)),
+        ('g_45_mode', dict(x=0., y=5e-6, z=1., xp=0., yp=0., avgPhotEn=2000., pulseEn=0.001, repRate=1., polar=3,
+                           sigX=40e-6, sigY=25e-6, sigT=5e-15, mx=1, my=0), dict(n=(48, 56), r=(0.4e-3, 0.4e-3),
+                                                                                e=2000., z=3., unit=1)),
+        ('g_vert', dict(x=0., y=0., z=0., xp=1e-6, yp=0., avgPhotEn=1500., pulseEn=0.001, repRate=1., polar=2,
+                        sigX=30e-6, sigY=30e-6, sigT=10e-15, mx=0, my=2), dict(n=(40, 40), r=(0.5e-3, 0.5e-3), e=1500.,
+                                                                               z=2., unit=1)),
+        ('g_135', dict(x=0., y=0., z=0., xp=0., yp=0., avgPhotEn=1500., pulseEn=0.001, repRate=1., polar=4,
+                       sigX=30e-6, sigY=30e-6, sigT=10e-15, mx=0, my=0), dict(n=(40, 40), r=(0.5e-3, 0.5e-3), e=1500.,
+                                                                              z=2., unit=1)),
+        ('g_circ_left', dict(x=0., y=0., z=0., xp=0., yp=0., avgPhotEn=1500., pulseEn=0.001, repRate=1., polar=6,
+                             sigX=30e-6, sigY=30e-6, sigT=10e-15, mx=1, my=1), dict(n=(40, 40), r=(0.5e-3, 0.5e-3),
+                                                                                    e=1500., z=2., unit=1)),
+    ]
+    gidx = []
+    for gname, gp, mp in gcases:
+        gb = L.SRWLGsnBm()
+        for k, v in gp.items():
+            setattr(gb, k, v)
+        w = L.SRWLWfr()
+        w.allocate(1, mp['n'][0], mp['n'][1])
+        m = w.mesh
+        m.zStart = mp['z']; m.eStart = m.eFin = mp['e']
+        m.xStart, m.xFin, m.yStart, m.yFin = -mp['r'][0], mp['r'][0], -mp['r'][1], mp['r'][1]
+        w.unitElFld = mp['unit']
+        w.arElecPropMatr = array('d', [0.] * 16 + [1e-4, 2e-6, -3e-4, 4e-6])
+        L.srwl.CalcElecFieldGaussian(w, gb, [0])
+        out = snapshot(w)
+        for k, v in out.items():
+            blob['gauss/' + gname + '/' + k] = v
+        gidx.append(dict(name=gname, beam=gp, mesh=dict(nx=mp['n'][0], ny=mp['n'][1], xStart=-mp['r'][0],
+                                                         xFin=mp['r'][0], yStart=-mp['r'][1], yFin=mp['r'][1],
+                                                         eStart=mp['e'], eFin=mp['e'], zStart=mp['z']),
+                         unit=mp['unit']))
+    blob['gauss/index'] = np.array(json.dumps(gidx))
     blob['index'] = np.array(json.dumps(index))
     np.savez_compressed(os.path.join(HERE, 'cases.npz'), **blob)
 

@@ -105,6 +105,16 @@ struct SRWLStructOpticsLens {
 };
 typedef struct SRWLStructOpticsLens SRWLOptL;
 
+/* SRWLOptT (srwlib.h:378-389): generic transmission; arTr holds (amplitude transmission, optical path
+ * difference [m]) pairs of doubles, [ny][nx] for ne == 1 */
+struct SRWLStructOpticsTransmission {
+    double* arTr;
+    SRWLRadMesh mesh;
+    char extTr;
+    double Fx, Fy;
+};
+typedef struct SRWLStructOpticsTransmission SRWLOptT;
+
 struct SRWLStructOpticsContainer {
     void** arOpt;                /* element pointers */
     char** arOptTypes;           /* "drift", "aperture", "obstacle", "lens", "container" */

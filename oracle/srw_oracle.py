@@ -1,4 +1,5 @@
-"""FP64 CPU restatement of SRW's wavefront-propagation path (drift / thin lens / aperture).
+"""FP64 CPU restatement of SRW's wavefront-propagation path (drift / thin lens / aperture /
+transmission).
 
 TEST INFRASTRUCTURE ONLY.  Nothing in the product (``srw_b200``) imports this module; only
 ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may use it, and
@@ -6,7 +7,7 @@ only as the checker.
 
 This module restates, in double precision with numpy, the algorithm of the reference
 ``srwlPropagElecField`` (cpp/src/lib/srwlib.cpp:1023) for SRWLOptC chains of drifts, thin
-lenses and rectangular/circular apertures/obstacles, with the per-element propagation
+lenses, rectangular/circular apertures/obstacles and generic transmission tables, with the per-element propagation
 parameter lists.  Each function cites the reference file:line it follows.  Mesh/integer logic
 follows the reference operation order exactly (so meshes are bit-exact in IEEE double); field
 arithmetic is FP64 (numpy.fft / pocketfft) instead of the reference's FP32 FFTW, so the field
@@ -772,6 +773,77 @@ def lens(w: Wfr, Fx, Fz, cx, cz):
 
 
 # ----------------------------------------------------------------------------------------
+# Generic transmission (cpp/src/core/sroptgtr.h:86-140, point modifier sroptgtr.h:168-333,
+# constructor from SRWLOptT sroptgtr.cpp:139-180)
+# ----------------------------------------------------------------------------------------
+
+
+def _tr_axis(v, start, step, n):
+    """Cell index and fraction of a table axis (sroptgtr.h:205-225): index by truncation toward zero,
+    snapped up within 1e-5 of a step from the next node, the first cell below the table (fraction 0
+    when more than one step below, linear extrapolation within the step), the last cell with
+    fraction 1 above it."""
+    i = np.trunc((v - start) / step).astype(np.int64)
+    i = np.where(np.abs(v - ((i + 1) * step + start)) < 1.E-05 * step, i + 1, i)
+    frac = (v - (i * step + start)) / step
+    frac = np.where(i < 0, 0., np.where(i > n - 2, 1., frac))
+    i = np.clip(i, 0, n - 2)
+    return i, frac
+
+
+def transmission(w: Wfr, arTr, nx, nz, rx, rz, x, z, extTr, Fx, Fz):
+    """srTGenTransmission: amplitude transmission T and optical path difference OPD tabulated over
+    [nz][nx] (pairs, ne == 1) on the mesh of ranges rx, rz centred on (x, z) (the SRWLOptT
+    constructor, srwlib.py:3071-3082), interpolated bilinearly at the wavefront's absolute
+    coordinates; E *= T exp(i k OPD); zero outside the table when extTr == 0.  The bookkeeping
+    (moments, radius, centre, 4x4 matrix) is the focusing element's with the estimated focal
+    lengths Fx, Fz about the table's centre."""
+    xStart, xFin = x - 0.5 * rx, x + 0.5 * rx
+    zStart, zFin = z - 0.5 * rz, z + 0.5 * rz
+    cx, cz = 0.5 * (xStart + xFin), 0.5 * (zStart + zFin)
+    check_and_subtract_phase_lin(w, cx, cz)
+    if w.Pres != 0:
+        set_rad_repres(w, 0)
+    x, z = w.coords()
+    x = np.broadcast_to(x, (w.nz, w.nx))
+    z = np.broadcast_to(z, (w.nz, w.nx))
+    xStep, zStep = (xFin - xStart) / (nx - 1), (zFin - zStart) / (nz - 1)
+    tab = np.asarray(arTr, dtype=np.float64).reshape(nz, nx, 2)
+    ix, xr = _tr_axis(x, xStart, xStep, nx)
+    iz, zr = _tr_axis(z, zStart, zStep, nz)
+    p00, p10, p01, p11 = tab[iz, ix], tab[iz, ix + 1], tab[iz + 1, ix], tab[iz + 1, ix + 1]
+    a_xz = p00 - p01 - p10 + p11
+    a_x, a_z = p10 - p00, p01 - p00
+    v = a_xz * (xr * zr)[..., None] + a_x * xr[..., None] + a_z * zr[..., None] + p00
+    T, Ph = v[..., 0], v[..., 1] * (w.eStart * 5.0676816042E+06)
+    fac = T * np.exp(1j * Ph)
+    if extTr == 0:
+        xEnd, zEnd = xStart + (nx - 1) * xStep, zStart + (nz - 1) * zStep
+        tx, tz = xStep * 0.001, zStep * 0.001
+        outside = (x < xStart - tx) | (x > xEnd + tx) | (z < zStart - tz) | (z > zEnd + tz)
+        fac = np.where(outside, 0., fac)
+    w.mult(fac)
+    ax = [[1., 0.], [-1. / Fx, 1.]]
+    az = [[1., 0.], [-1. / Fz, 1.]]
+    for mom in (w.momX, w.momZ):
+        _mom_apply(mom, ax, az)
+    dSmall = 1E-23
+    difX = dSmall if Fx == w.RobsX else Fx - w.RobsX
+    difZ = dSmall if Fz == w.RobsZ else Fz - w.RobsZ
+    MagnX, MagnZ = Fx / difX, Fz / difZ
+    w.RobsX *= MagnX
+    w.RobsZ *= MagnZ
+    w.RobsXAbsErr *= MagnX * MagnX
+    w.RobsZAbsErr *= MagnZ * MagnZ
+    w.xc = cx - (cx - w.xc) * MagnX
+    w.zc = cz - (cz - w.zc) * MagnZ
+    _prop_4x4(w, np.array([[1., 0., 0., 0.], [-1. / Fx, 1., 0., 0.], [0., 0., 1., 0.], [0., 0., -1. / Fz, 1.]]),
+              np.array([0., cx / Fx, 0., cz / Fz]))
+    _fix_abs_err(w)
+    check_and_reset_phase_lin(w)
+
+
+# ----------------------------------------------------------------------------------------
 # Apertures / obstacles (cpp/src/core/sroptapt.h)
 # ----------------------------------------------------------------------------------------
 
@@ -1388,7 +1460,8 @@ def propagate(w: Wfr, elements, props):
     """srTCompositeOptElem ctor (sroptcnt.cpp:87-221) + PropagateRadiationGuided (:254-425).
 
     ``elements``: list of tuples ('drift', L, treat) | ('aperture', shape, ap_or_ob, Dx, Dy, x, y)
-    | ('lens', Fx, Fy, x, y).  ``props``: list of per-element propagation parameter lists
+    | ('lens', Fx, Fy, x, y) | ('transmission', arTr, nx, ny, rx, ry, x, y, extTr, Fx, Fy).
+    ``props``: list of per-element propagation parameter lists
     (len(props) may be len(elements)+1 for a post-resize)."""
     if (w.nx <= 1) or (w.nz <= 1):
         raise ValueError("CAN_NOT_PROPAGATE_1D_RAD")
@@ -1413,6 +1486,8 @@ def propagate(w: Wfr, elements, props):
             lens(w, el[1], el[2], el[3], el[4])
         elif kind == 'aperture':
             aperture(w, el[1], el[2], el[3], el[4], el[5], el[6])
+        elif kind == 'transmission':
+            transmission(w, *el[1:])
         else:
             raise ValueError("UNKNOWN_OPTICAL_ELEMENT")
     n = len(elements)

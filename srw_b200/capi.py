@@ -58,6 +58,11 @@ class SRWLOptL(C.Structure):
     _fields_ = [('Fx', C.c_double), ('Fy', C.c_double), ('x', C.c_double), ('y', C.c_double)]
 
 
+class SRWLOptT(C.Structure):
+    _fields_ = [('arTr', C.POINTER(C.c_double)), ('mesh', SRWLRadMesh), ('extTr', C.c_char), ('Fx', C.c_double),
+                ('Fy', C.c_double)]
+
+
 class SRWLOptC(C.Structure):
     _fields_ = [('arOpt', C.POINTER(C.c_void_p)), ('arOptTypes', C.POINTER(C.c_char_p)), ('nElem', C.c_int),
                 ('arProp', C.POINTER(C.POINTER(C.c_double))), ('arPropN', C.c_char_p), ('nProp', C.c_int)]

@@ -353,7 +353,7 @@ __device__ __forceinline__ bool chainG_trivial(const ChainG& c)
     return !c.rs1 && !c.mir && !c.rs2 && c.tab < 0 && !c.extra;
 }
 
-__device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2& f, bool& zero);
+__device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2& f, bool& zero, const float2* tabs);
 
 template <bool EXTRA = true>
 __device__ __forceinline__ float2 chainG_factor(const ChainG& c, int k, int i, int line, const float2* tabs,
@@ -362,7 +362,7 @@ __device__ __forceinline__ float2 chainG_factor(const ChainG& c, int k, int i, i
     float2 f = c.tab >= 0 ? __ldg(&tabs[c.tab + k]) : make_float2(1.f, 0.f);
     if (EXTRA && c.extra) {
         bool zero = false;
-        extra_eval(*ex, axis == 0 ? i : line, axis == 0 ? line : i, f, zero);
+        extra_eval(*ex, axis == 0 ? i : line, axis == 0 ? line : i, f, zero, tabs);
         if (zero) f = make_float2(0.f, 0.f);
     }
     return f;
@@ -412,10 +412,50 @@ static __device__ __noinline__ float2 bpx_factor(const PwOps& e, int i, int j)
     return expi(e.bkL * r);
 }
 
+// srTGenTransmission::RadPointModifier (sroptgtr.h:163-310), one photon energy: amplitude
+// transmission and optical path difference bilinear in the table (FP64, its index rules: the
+// 1e-5 step snap, clamping to the last cell), the phase 2 pi / lambda * OPD; zero outside the table
+// (within 1e-3 of a step) when the element says so.  Returns false to zero the point.
+static __device__ __noinline__ bool tr_factor(const PwOps& e, int i, int j, const float2* tabs, float2& f)
+{
+    const double xRel = dadd(e.tr_x0, dmul((double)i, e.tr_dx)), zRel = dadd(e.tr_z0, dmul((double)j, e.tr_dz));
+    const int Nx = e.tr_nx, Nz = e.tr_nz;
+    const double xs = e.tr_xs, zs = e.tr_zs, xst = e.tr_xstep, zst = e.tr_zstep;
+    if (e.tr_outer == 1) {
+        const double xEnd = xs + (Nx - 1) * xst, zEnd = zs + (Nz - 1) * zst;
+        const double tx = xst * 0.001, tz = zst * 0.001;
+        if ((xRel < xs - tx) || (xRel > xEnd + tx) || (zRel < zs - tz) || (zRel > zEnd + tz)) return false;
+    }
+    double xr = 0., zr = 0.;
+    long long ix = (long long)((xRel - xs) / xst);
+    if (fabs(xRel - ((ix + 1) * xst + xs)) < 1.E-05 * xst) ix++;
+    if (ix < 0) ix = 0;
+    else if (ix > Nx - 2) { ix = Nx - 2; xr = 1.; }
+    else xr = (xRel - (ix * xst + xs)) / xst;
+    long long iz = (long long)((zRel - zs) / zst);
+    if (fabs(zRel - ((iz + 1) * zst + zs)) < 1.E-05 * zst) iz++;
+    if (iz < 0) iz = 0;
+    else if (iz > Nz - 2) { iz = Nz - 2; zr = 1.; }
+    else zr = (zRel - (iz * zst + zs)) / zst;
+    const double xrzr = xr * zr;
+    const double* d = reinterpret_cast<const double*>(tabs + e.tr_off);
+    const long long zPer = (long long)Nx << 1;
+    const double* p00 = d + (iz * zPer + (ix << 1));
+    const double *p10 = p00 + 2, *p01 = p00 + zPer, *p11 = p01 + 2;
+    const double Axz = p00[0] - p01[0] - p10[0] + p11[0], Bxz = p00[1] - p01[1] - p10[1] + p11[1];
+    const double Ax = p10[0] - p00[0], Bx = p10[1] - p00[1];
+    const double Az = p01[0] - p00[0], Bz = p01[1] - p00[1];
+    const double T = Axz * xrzr + Ax * xr + Az * zr + p00[0];
+    const double Ph = (Bxz * xrzr + Bx * xr + Bz * zr + p00[1]) * e.tr_k;
+    const float2 c = expi(Ph);
+    f = cmul(f, make_float2((float)(T * c.x), (float)(T * c.y)));
+    return true;
+}
+
 // non-separable point-wise work: circular masks, rectangular obstacles, the quartic remainder of
 // the angular transfer function, the beyond-paraxial propagator (everything separable is in the
 // plan's tables)
-__device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2& f, bool& zero)
+__device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2& f, bool& zero, const float2* tabs)
 {
     if (e.has_ang) {
         float qx = (float)(e.qx0 + (double)i * e.dqx), qz = (float)(e.qz0 + (double)j * e.dqz);
@@ -427,6 +467,7 @@ __device__ __forceinline__ void extra_eval(const PwOps& e, int i, int j, float2&
         f = cmul(f, make_float2(cs, sn));
     }
     if (e.has_bpx) f = cmul(f, bpx_factor(e, i, j));
+    if (e.has_tr && !tr_factor(e, i, j, tabs, f)) zero = true;
     for (int m = 0; m < e.nmask; m++) {
         const PwMask& k = e.mask[m];
         double x = dadd(k.x0, dmul((double)i, k.dx));
@@ -462,7 +503,7 @@ __device__ __forceinline__ float2 chain2_apply(const Chain2& c, int k, int line,
         const int i = k ^ c.xi;
         bool zero = false;
         float2 f = make_float2(1.f, 0.f);
-        extra_eval(*ex, axis == 0 ? i : line, axis == 0 ? line : i, f, zero);
+        extra_eval(*ex, axis == 0 ? i : line, axis == 0 ? line : i, f, zero, tabs);
         v = zero ? make_float2(0.f, 0.f) : cmul(f, v);
     }
     return v;

@@ -47,6 +47,12 @@ struct PwOps {
     double bqx0, bdqx, bqz0, bdqz;       //   (sroptdrf.h:712): phase += kL * (sqrt(1 - lam^2 q^2) - 1
     double blam, bkL;                    //   + btreat), q the angular frequencies of index (i, j)
     int btreat;
+    int has_tr;                          // transmission table (sroptgtr.h:163-310), bilinear, FP64:
+    int tr_id, tr_nx, tr_nz, tr_outer;   //   table id (offset after planning), size, 1: zero outside
+    long long tr_off;                    //   offset of the (T, OPD) doubles in the plan's tables (float2)
+    double tr_x0, tr_dx, tr_z0, tr_dz;   //   physical coordinate of index (i, j)
+    double tr_xs, tr_xstep, tr_zs, tr_zstep;   // the table's mesh
+    double tr_k;                         //   2 pi / lambda: phase = k * OPD
 };
 
 // Separable factor tables (complex FP32, computed in FP64 on the host) of one point-wise chain:

@@ -260,7 +260,7 @@ __device__ __forceinline__ float2 resize_factor(const ResizeDesc& d, const float
     if (d.t.tab >= 0) e = __ldg(&tabs[d.t.tab + ix]);
     if (d.t.ltab >= 0) e = cmul(e, __ldg(&tabs[d.t.ltab + iz]));
     bool zero = false;
-    if (d.has_extra) extra_eval(d.extra, ix, iz, e, zero);
+    if (d.has_extra) extra_eval(d.extra, ix, iz, e, zero, tabs);
     return zero ? make_float2(0.f, 0.f) : e;
 }
 
@@ -365,7 +365,7 @@ __device__ __forceinline__ float2 pre_factor(const ResizeDesc& d, const float2* 
     if (d.tp.tab >= 0) e = __ldg(&tabs[d.tp.tab + ix]);
     if (d.tp.ltab >= 0) e = cmul(e, __ldg(&tabs[d.tp.ltab + iz]));
     bool zero = false;
-    if (d.has_pre_extra) extra_eval(d.pre_extra, ix, iz, e, zero);
+    if (d.has_pre_extra) extra_eval(d.pre_extra, ix, iz, e, zero, tabs);
     return zero ? make_float2(0.f, 0.f) : e;
 }
 
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(256) pw_kernel(const PwLaunch p)
     if (d.t.tab >= 0) e = __ldg(&tabs[d.t.tab + ix]);
     if (d.t.ltab >= 0) e = cmul(e, __ldg(&tabs[d.t.ltab + iz]));
     bool zero = false;
-    if (d.has_extra) extra_eval(d.extra, ix, iz, e, zero);
+    if (d.has_extra) extra_eval(d.extra, ix, iz, e, zero, tabs);
     if (zero) e = make_float2(0.f, 0.f);
     const int ox = d.mirror_x ? d.nx - 1 - ix : ix;
     const int oz = d.mirror_z ? d.nz - 1 - iz : iz;

@@ -74,7 +74,7 @@ __device__ __forceinline__ float2 mom_factor(const MomDesc& d, const float2* tab
     if (tz >= 0) f = cmul(f, __ldg(&tabs[tz + iz]));
     if (d.has_extra) {
         bool zero = false;
-        extra_eval(d.extra, ix, iz, f, zero);
+        extra_eval(d.extra, ix, iz, f, zero, tabs);
         if (zero) f = make_float2(0.f, 0.f);
     }
     return f;

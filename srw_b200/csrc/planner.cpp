@@ -167,6 +167,25 @@ public:
         ks.push_back(k);
         return ks.back().mom;
     }
+    // transmission table on the current (coordinate) mesh
+    void transm(const WfrState& w, const ElemDesc& e)
+    {
+        PwOps* p = ensure(w);
+        if (p->has_tr) {
+            close();
+            p = ensure(w);
+        }
+        double X0, DX, Z0, DZ;
+        axis_map(w, X0, DX, Z0, DZ);
+        p->has_tr = 1;
+        p->tr_id = e.tr; p->tr_nx = e.trNx; p->tr_nz = e.trNz;
+        p->tr_outer = e.extTr + 1;        // OuterTransmIs (sroptgtr.cpp:142)
+        p->tr_off = -1;
+        p->tr_x0 = X0; p->tr_dx = DX; p->tr_z0 = Z0; p->tr_dz = DZ;
+        p->tr_xs = e.trXs; p->tr_xstep = (e.trXf - e.trXs) / (e.trNx - 1);
+        p->tr_zs = e.trZs; p->tr_zstep = (e.trZf - e.trZs) / (e.trNz - 1);
+        p->tr_k = w.eStart * 5.0676816042E+06;   // 2 pi / lambda [1/m] (sroptgtr.h:287)
+    }
     // exact beyond-paraxial propagator phase on the current (angular-frequency) mesh
     void bpx(const WfrState& w, double lam, double kL, int treat)
     {
@@ -330,6 +349,23 @@ int Planner::flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vecto
             } else if (strcmp(t, "lens") == 0) {
                 const SRWLOptL* l = (const SRWLOptL*)p;
                 e.kind = E_LENS; e.Fx = l->Fx; e.Fy = l->Fy; e.x = l->x; e.y = l->y;
+            } else if (strcmp(t, "transmission") == 0) {
+                // srTGenTransmission(const SRWLOptT&) (sroptgtr.cpp:139): table over the element's
+                // mesh, centre = the mesh's centre, estimated focal lengths for the bookkeeping
+                const SRWLOptT* tr = (const SRWLOptT*)p;
+                if (tr->arTr == nullptr || tr->mesh.nx < 2 || tr->mesh.ny < 2) return UNKNOWN_OPTICAL_ELEMENT;
+                if (tr->mesh.ne != 1) {
+                    err = "transmission tables vs photon energy (ne > 1) are not supported on the GPU path";
+                    return SRWG_ERR_UNSUPPORTED;
+                }
+                e.kind = E_TRANSM;
+                e.Fx = tr->Fx; e.Fy = tr->Fy;
+                e.x = 0.5 * (tr->mesh.xStart + tr->mesh.xFin);
+                e.y = 0.5 * (tr->mesh.yStart + tr->mesh.yFin);
+                e.trNx = (int)tr->mesh.nx; e.trNz = (int)tr->mesh.ny; e.extTr = tr->extTr;
+                e.trXs = tr->mesh.xStart; e.trXf = tr->mesh.xFin; e.trZs = tr->mesh.yStart; e.trZf = tr->mesh.yFin;
+                e.tr = (int)trTables_.size();
+                trTables_.emplace_back(tr->arTr, tr->arTr + 2 * (size_t)e.trNx * e.trNz);
             } else if (strcmp(t, "container") == 0) {
                 // a nested container is one element of the outer chain; its own propagation
                 // parameters apply inside it (sroptcnt.cpp:171)
@@ -1115,6 +1151,36 @@ void Planner::lens(const ElemDesc& e)
 }
 
 // ================================================================================================
+// Generic transmission (cpp/src/core/sroptgtr.h:86-140): a focusing element in the bookkeeping
+// (srTFocusingElem radius / moments / 4x4 with the estimated focal lengths), the table as the
+// point-wise work, linear phase terms about the table's centre subtracted before and reset after
+// ================================================================================================
+void Planner::transmission(const ElemDesc& e)
+{
+    phase_lin_subtract(e.x, e.y);
+    if (w.Pres != 0) set_rad_repres(0);
+    b->transm(w, e);
+    const double ax[2][2] = {{1., 0.}, {-1. / e.Fx, 1.}};
+    const double az[2][2] = {{1., 0.}, {-1. / e.Fy, 1.}};
+    record_matrix(ax, az, 0, 0., 0.);
+    const double dSmall = 1E-23;
+    double difX = (e.Fx == w.RobsX) ? dSmall : e.Fx - w.RobsX;
+    double difZ = (e.Fy == w.RobsZ) ? dSmall : e.Fy - w.RobsZ;
+    double MagnX = e.Fx / difX, MagnZ = e.Fy / difZ;
+    w.RobsX *= MagnX;
+    w.RobsZ *= MagnZ;
+    w.RobsXAbsErr *= (MagnX * MagnX);
+    w.RobsZAbsErr *= (MagnZ * MagnZ);
+    w.xc = e.x - (e.x - w.xc) * MagnX;
+    w.zc = e.y - (e.y - w.zc) * MagnZ;
+    const double Foc[16] = {1., 0., 0., 0., -1. / e.Fx, 1., 0., 0., 0., 0., 1., 0., 0., 0., -1. / e.Fy, 1.};
+    const double fv[4] = {0., e.x / e.Fx, 0., e.y / e.Fy};
+    prop_4x4(Foc, fv);
+    fix_abs_err();
+    phase_lin_reset();
+}
+
+// ================================================================================================
 // Apertures / obstacles (cpp/src/core/sroptapt.h, sroptapt.cpp:248-350)
 // ================================================================================================
 void Planner::aperture(const ElemDesc& e)
@@ -1373,6 +1439,7 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
     stageIn = w;
     els_.clear();
     props_.clear();
+    trTables_.clear();
     int r = flatten(opt, els_, props_, false);
     if (r) return r;
     if ((w.nx <= 1) || (w.nz <= 1)) return CAN_NOT_PROPAGATE_1D_RAD;   // CheckRadStructForPropagation
@@ -1430,6 +1497,7 @@ int Planner::run()
             if (e.kind == E_DRIFT) drift(e, anal);
             else if (e.kind == E_LENS) lens(e);
             else if (e.kind == E_APERTURE) aperture(e);
+            else if (e.kind == E_TRANSM) transmission(e);
         }
         if (i < numRes && props[i].n >= 0) {
             const PropDesc& p = props[i];
@@ -1475,6 +1543,28 @@ int Planner::finalize()
         }
     }
     build_tables(kernels, tables);
+    // transmission tables after the separable ones (each double of a (T, OPD) pair in one float2
+    // slot), and their offsets into every point-wise description that uses them
+    if (!trTables_.empty()) {
+        std::vector<long long> base(trTables_.size(), -1);
+        auto patch = [&](PwOps& o) {
+            if (!o.has_tr) return;
+            if (base[o.tr_id] < 0) {
+                base[o.tr_id] = (long long)tables.size();
+                const std::vector<double>& t = trTables_[o.tr_id];
+                const size_t at = tables.size();
+                tables.resize(at + t.size());
+                memcpy(&tables[at], t.data(), t.size() * sizeof(double));
+            }
+            o.tr_off = base[o.tr_id];
+        };
+        for (KernelDesc& k : kernels) {
+            if (k.kind == K_LINE) { patch(k.line.pw); patch(k.line.extra); }
+            else if (k.kind == K_RESIZE) { patch(k.rs.pw); patch(k.rs.extra); patch(k.rs.pre); patch(k.rs.pre_extra); }
+            else if (k.kind == K_MOM) { patch(k.mom.pw); patch(k.mom.extra); }
+            else { patch(k.pwk.pw); patch(k.pwk.extra); }
+        }
+    }
     // a tiled resize followed by a line pass on its output writes only its window; the line pass
     // reads zeros outside it (the buffer is overwritten before anything else reads it)
     for (size_t i = 0; i + 1 < kernels.size(); i++) {

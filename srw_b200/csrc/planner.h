@@ -52,14 +52,17 @@ enum { MOP_MATRIX = 1, MOP_APERTURE = 2, MOP_ESTIMATE = 3 };
 // the field)
 #define SRWG_NEED_STAGE (-77)
 
-enum ElemKind { E_DRIFT = 1, E_APERTURE = 2, E_LENS = 3 };
+enum ElemKind { E_DRIFT = 1, E_APERTURE = 2, E_LENS = 3, E_TRANSM = 4 };
 
 struct ElemDesc {
     int kind = 0;
     double L = 0; int treat = 0;                            // drift
     char shape = 'r', apob = 'a'; double Dx = 0, Dy = 0;    // aperture / obstacle
-    double Fx = 0, Fy = 0;                                  // lens
+    double Fx = 0, Fy = 0;                                  // lens, transmission
     double x = 0, y = 0;                                    // centre
+    int tr = -1;                                            // transmission: index of its table copy
+    int trNx = 0, trNz = 0, extTr = 0;
+    double trXs = 0, trXf = 0, trZs = 0, trZf = 0;
 };
 
 struct PropDesc {
@@ -138,6 +141,8 @@ private:
     void prop_4x4(const double E[16], const double e[4]);
     bool momProvisional = false;         // plan-time moments wait for a MOM pass's result
     void lens(const ElemDesc& e);
+    void transmission(const ElemDesc& e);
+    std::vector<std::vector<double>> trTables_;   // copies of the transmission tables (T, OPD pairs)
     void aperture(const ElemDesc& e);
     void phase_lin_subtract(double newXc, double newZc);
     void phase_lin_reset();

@@ -58,6 +58,15 @@ static void separate(const PwOps& pw, int axis, int nAlong, int nLine, SepPart& 
         extra.blam = pw.blam; extra.bkL = pw.bkL; extra.btreat = pw.btreat;
         has_extra = 1;
     }
+    if (pw.has_tr) {        // non-separable: table interpolation per point (common.cuh extra_eval)
+        extra.has_tr = 1;
+        extra.tr_id = pw.tr_id; extra.tr_nx = pw.tr_nx; extra.tr_nz = pw.tr_nz; extra.tr_outer = pw.tr_outer;
+        extra.tr_off = pw.tr_off;
+        extra.tr_x0 = pw.tr_x0; extra.tr_dx = pw.tr_dx; extra.tr_z0 = pw.tr_z0; extra.tr_dz = pw.tr_dz;
+        extra.tr_xs = pw.tr_xs; extra.tr_xstep = pw.tr_xstep; extra.tr_zs = pw.tr_zs; extra.tr_zstep = pw.tr_zstep;
+        extra.tr_k = pw.tr_k;
+        has_extra = 1;
+    }
     if (pw.has_scale) { scale = cd(pw.sre, pw.sim); A.any = true; }
     for (int m = 0; m < pw.nmask; m++) {
         const PwMask& k = pw.mask[m];

@@ -1,7 +1,7 @@
 """Wavefront and optical-element structures with the attribute names and constructor arguments of
 the reference's Python classes (env/python/srwpy/srwlib.py: SRWLRadMesh :804, SRWLWfr :2200,
-SRWLOptD :2908, SRWLOptA :2919, SRWLOptL :2938, SRWLOptC :4259) for the drift / lens / aperture
-path.  Objects of the reference's own classes work with ``srw_b200.srwlpy`` as well: elements are
+SRWLOptD :2908, SRWLOptA :2919, SRWLOptL :2938, SRWLOptT :3036, SRWLOptC :4259) for the drift / lens /
+aperture / transmission path.  Objects of the reference's own classes work with ``srw_b200.srwlpy`` as well: elements are
 recognised by class name, like the reference's C extension does (srwlpy.cpp:2678).
 
 Field arrays are numpy float32 (``array('f')`` buffers of the reference classes are accepted too).
@@ -105,6 +105,34 @@ class SRWLOptA(object):
 class SRWLOptL(object):
     def __init__(self, _Fx=1e+23, _Fy=1e+23, _x=0, _y=0):
         self.Fx, self.Fy, self.x, self.y = _Fx, _Fy, _x, _y
+
+
+class SRWLOptT(object):
+    """Generic transmission, the reference's SRWLOptT (env/python/srwpy/srwlib.py:3036) with the same
+    constructor signature: ``arTr`` holds (amplitude transmission, optical path difference) pairs,
+    C-aligned over [ny][nx] (ne == 1), on a mesh of ranges rx, ry centred on (x, y)."""
+
+    def __init__(self, _nx=1, _ny=1, _rx=1e-03, _ry=1e-03, _arTr=None, _extTr=0, _Fx=1e+23, _Fy=1e+23, _x=0, _y=0,
+                 _ne=1, _eStart=0, _eFin=0):
+        self.arTr = _arTr
+        if _arTr is None or (len(_arTr) != _ne * _nx * _ny * 2 and _ne * _nx * _ny > 0):
+            self.allocate(_ne, _nx, _ny)
+        hx, hy = 0.5 * _rx, 0.5 * _ry
+        if not hasattr(self, 'mesh'):
+            self.mesh = SRWLRadMesh(_eStart, _eFin, _ne, _x - hx, _x + hx, _nx, _y - hy, _y + hy, _ny)
+        else:
+            self.mesh.eStart, self.mesh.eFin = _eStart, _eFin
+            self.mesh.xStart, self.mesh.xFin = _x - hx, _x + hx
+            self.mesh.yStart, self.mesh.yFin = _y - hy, _y + hy
+        self.extTr = _extTr
+        self.Fx, self.Fy = _Fx, _Fy
+
+    def allocate(self, _ne, _nx, _ny):
+        if hasattr(self, 'mesh'):
+            self.mesh.ne, self.mesh.nx, self.mesh.ny = _ne, _nx, _ny
+        else:
+            self.mesh = SRWLRadMesh(0, 0, _ne, 0, 0, _nx, 0, 0, _ny)
+        self.arTr = array('d', [0.]) * (2 * _ne * _nx * _ny)
 
 
 class SRWLOptC(object):

@@ -6,7 +6,7 @@ on the GPU path:
 
 Arguments, return value and error behaviour follow the reference: elements of ``optC.arOpt`` are
 dispatched by class name (SRWLOptD -> "drift", SRWLOptA -> "aperture", SRWLOptL -> "lens",
-SRWLOptC -> "container", srwlpy.cpp:2678-2700); ``optC.arProp`` is a list of propagation
+SRWLOptT -> "transmission", SRWLOptC -> "container", srwlpy.cpp:2678-2700); ``optC.arProp`` is a list of propagation
 parameter lists; field arrays must expose a float32 buffer (numpy or ``array('f')``); when the
 mesh size changes the wavefront is re-allocated through ``wfr.allocate(ne, nx, ny, EXNeeded,
 EYNeeded, typeE, backupNeeded)`` (srwlpy.cpp:4141); after the call the mesh, radii, centres and
@@ -20,7 +20,8 @@ import numpy as np
 
 from . import capi
 
-_ELEM_TYPES = {'SRWLOptD': 'drift', 'SRWLOptA': 'aperture', 'SRWLOptL': 'lens', 'SRWLOptC': 'container'}
+_ELEM_TYPES = {'SRWLOptD': 'drift', 'SRWLOptA': 'aperture', 'SRWLOptL': 'lens', 'SRWLOptT': 'transmission',
+               'SRWLOptC': 'container'}
 
 
 def _buf_ptr(a, keep, dtype):
@@ -105,6 +106,22 @@ def make_c_optc(opt, keep):
             s = capi.SRWLOptA(_chr(e.shape, b'r'), _chr(e.ap_or_ob, b'a'), float(e.Dx), float(e.Dy), float(e.x), float(e.y))
         elif kind == 'lens':
             s = capi.SRWLOptL(float(e.Fx), float(e.Fy), float(e.x), float(e.y))
+        elif kind == 'transmission':
+            # ParseSructSRWLOptT (srwlpy.cpp:1940): the table buffer, its mesh, extTr, Fx, Fy
+            s = capi.SRWLOptT()
+            tr = _buf_ptr(e.arTr, keep, np.float64)
+            if tr is None:
+                raise RuntimeError('Incorrect Transmission structure')
+            s.arTr = C.cast(tr, C.POINTER(C.c_double))
+            m = e.mesh
+            s.mesh.eStart, s.mesh.eFin = float(m.eStart), float(m.eFin)
+            s.mesh.xStart, s.mesh.xFin = float(m.xStart), float(m.xFin)
+            s.mesh.yStart, s.mesh.yFin = float(m.yStart), float(m.yFin)
+            s.mesh.ne, s.mesh.nx, s.mesh.ny = int(m.ne), int(m.nx), int(m.ny)
+            if len(e.arTr) < 2 * int(m.ne) * int(m.nx) * int(m.ny):
+                raise RuntimeError('Incorrect Transmission structure')
+            s.extTr = bytes([int(e.extTr) & 0xff])
+            s.Fx, s.Fy = float(e.Fx), float(e.Fy)
         else:
             s = make_c_optc(e, keep)
         keep.append(s)

@@ -99,7 +99,25 @@ def build_beamline(L, elems):
             opts.append(L.SRWLOptA(e[1], e[2], e[3], e[4], e[5], e[6]))
         elif e[0] == 'lens':
             opts.append(L.SRWLOptL(e[1], e[2], e[3], e[4]))
+        elif e[0] == 'transmission':
+            tr, nx, ny, rx, ry, x, y, ext, Fx, Fy = e[1:]
+            opts.append(L.SRWLOptT(nx, ny, rx, ry, array('d', np.asarray(tr, np.float64).tobytes()), ext, Fx, Fy, x, y))
     return opts
+
+
+def tr_table(nx, ny, rx, ry, x, y, F, amp=0.3, ripple=3e-10, seed=0):
+    """(T, OPD) pairs over [ny][nx]: a focusing optical path -(r^2)/(2F) with a seeded ripple and an
+    amplitude transmission falling off towards the edges."""
+    g = np.random.default_rng(seed)
+    xs = x - 0.5 * rx + np.arange(nx) * (rx / (nx - 1))
+    ys = y - 0.5 * ry + np.arange(ny) * (ry / (ny - 1))
+    X, Y = np.meshgrid(xs - x, ys - y)
+    kx, ky, ph = (2. * np.pi / rx) * g.uniform(1., 4.), (2. * np.pi / ry) * g.uniform(1., 4.), g.uniform(0., 6.)
+    opd = -(X * X + Y * Y) / (2. * F) + ripple * np.sin(kx * X + ph) * np.cos(ky * Y)
+    t = 1. - amp * (X * X / (0.25 * rx * rx) + Y * Y / (0.25 * ry * ry)) + 0.02 * g.standard_normal(X.shape)
+    out = np.empty((ny, nx, 2))
+    out[..., 0], out[..., 1] = t, opd
+    return out.ravel()
 
 
 def snapshot(w):
@@ -169,6 +187,21 @@ def cases(L):
                                       ('drift', 30., 0)], [pp(), pp(), pp(5)]),
         ('bpx_treat_offc', g2(96, 0.5e-3), [('lens', 15., 15., 0.02e-3, -0.01e-3), ('drift', 30., 1)],
          [pp(), pp(5)]),
+        # generic transmission (SRWLOptT): a table narrower than the wavefront (zero outside), off
+        # centre and on its own grid; the boundary values outside (extTr = 1) before a drift to the
+        # waist; a table on exactly the wavefront's mesh (node snapping), then a lens and a drift
+        ('tr_plate_offc', g2(96, 0.5e-3), [('transmission', tr_table(61, 53, 0.12e-3, 0.1e-3, 0.01e-3, -0.005e-3, 200.,
+                                                                     ripple=2e-11),
+                                            61, 53, 0.12e-3, 0.1e-3, 0.01e-3, -0.005e-3, 0, 200., 200.),
+                                           ('drift', 10., 0)], [pp(), pp()]),
+        ('tr_ext_towaist', g2(96, 0.5e-3), [('transmission', tr_table(40, 40, 0.1e-3, 0.1e-3, 0., 0., 200., ripple=2e-11,
+                                                                      seed=1),
+                                             40, 40, 0.1e-3, 0.1e-3, 0., 0., 1, 200., 200.), ('drift', 12., 0)],
+         [pp(), pp(4)]),
+        ('tr_aligned_lens', g0(64), [('transmission', tr_table(64, 64, 2e-3, 2e-3, 0., 0., 1e23, amp=0.1,
+                                                               ripple=2e-10, seed=2),
+                                      64, 64, 2e-3, 2e-3, 0., 0., 0, 1e23, 1e23), ('lens', 5., 5., 0., 0.),
+                                     ('drift', 5., 0)], [pp(), pp(), pp()]),
     ]
     return out
 
@@ -209,7 +242,15 @@ def main():
             blob[name + '/in/' + k] = v
         for k, v in out.items():
             blob[name + '/out/' + k] = v
-        index.append(dict(name=name, elements=[list(e) for e in elems], props=[list(map(float, p)) for p in pps]))
+        els = []
+        for k, e in enumerate(elems):
+            e = list(e)
+            if e[0] == 'transmission':       # the table beside the case, named in the element
+                key = '%s/tr%d' % (name, k)
+                blob[key] = np.asarray(e[1], np.float64)
+                e[1] = key
+            els.append(e)
+        index.append(dict(name=name, elements=els, props=[list(map(float, p)) for p in pps]))
         print(name, 'in', int(inp['mesh'][0]), int(inp['mesh'][1]), 'out', int(out['mesh'][0]), int(out['mesh'][1]),
               'R', out['scal'][0], out['scal'][1])
     # 3) intensity extraction (srwlCalcIntFromElecField vs x and y) on a propagated wavefront with both

@@ -15,8 +15,15 @@ def cplx(a, nx, ny):
 
 
 def load():
+    """(fixtures, case index); a transmission element's table is stored beside the case and named
+    in the element by its key, which is replaced here by the table itself."""
     d = np.load(GOLDEN)
-    return d, json.loads(str(d['index']))
+    index = json.loads(str(d['index']))
+    for c in index:
+        for e in c['elements']:
+            if e[0] == 'transmission':
+                e[1] = np.array(d[e[1]], np.float64)
+    return d, index
 
 
 def mesh_dict(m):

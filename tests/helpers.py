@@ -9,7 +9,7 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, os.path.join(REPO, 'oracle'))
 import srw_oracle as O  # noqa: E402  (the checker)
 
-from srw_b200.srwlib import SRWLOptA, SRWLOptC, SRWLOptD, SRWLOptL, SRWLWfr  # noqa: E402
+from srw_b200.srwlib import SRWLOptA, SRWLOptC, SRWLOptD, SRWLOptL, SRWLOptT, SRWLWfr  # noqa: E402
 
 
 def make_wfr(ex, ey, mesh, Rx=0., Ry=0., dRx=0., dRy=0., xc=0., yc=0., momX=None, momY=None, presCA=0, propM=None):
@@ -42,6 +42,9 @@ def beamline(elements, props):
             opts.append(SRWLOptD(e[1], e[2]))
         elif e[0] == 'lens':
             opts.append(SRWLOptL(*e[1:]))
+        elif e[0] == 'transmission':
+            tr, nx, ny, rx, ry, x, y, ext, Fx, Fy = e[1:]
+            opts.append(SRWLOptT(nx, ny, rx, ry, np.ascontiguousarray(tr, np.float64), ext, Fx, Fy, x, y))
         else:
             opts.append(SRWLOptA(*e[1:]))
     return SRWLOptC(opts, [list(p) for p in props])

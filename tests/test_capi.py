@@ -104,8 +104,11 @@ def test_unsupported_and_invalid_inputs_raise():
     with pytest.raises(RuntimeError, match='one point'):
         Plan(make_wfr(ex1, ey1, mesh1), beamline([('drift', 1., 0)], [PP()]))
 
-    class SRWLOptT(object):
+    class SRWLOptMirEl(object):
         pass
-    from srw_b200.srwlib import SRWLOptC
+    from srw_b200.srwlib import SRWLOptC, SRWLOptT
     with pytest.raises(RuntimeError, match='not supported'):
-        Plan(w, SRWLOptC([SRWLOptT()], [PP()]))
+        Plan(w, SRWLOptC([SRWLOptMirEl()], [PP()]))
+    # transmission tables vs photon energy are refused by the planner
+    with pytest.raises(RuntimeError, match='ne > 1'):
+        Plan(w, SRWLOptC([SRWLOptT(8, 8, 1e-3, 1e-3, _ne=2, _eStart=1e3, _eFin=2e3)], [PP()]))

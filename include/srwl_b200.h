@@ -117,7 +117,7 @@ typedef struct SRWLStructOpticsTransmission SRWLOptT;
 
 struct SRWLStructOpticsContainer {
     void** arOpt;                /* element pointers */
-    char** arOptTypes;           /* "drift", "aperture", "obstacle", "lens", "container" */
+    char** arOptTypes;           /* "drift", "aperture", "obstacle", "lens", "transmission", "container" */
     int nElem;
     double** arProp;             /* per-element propagation parameter lists */
     char* arPropN;               /* their lengths (9..17) */
@@ -133,8 +133,13 @@ typedef struct SRWLStructOpticsContainer SRWLOptC;
  * wavefront in place through the optical container on the GPU (arParGPU = {nPar, device index
  * (1-based)} or NULL for device 0).  Field arrays are host memory owned by the caller; when the
  * mesh size changes the registered modification callback is called (action 2) to re-allocate
- * them before the result is written back.  nInt/arID/arIM/arI (intermediate intensities) are
- * not supported and must be 0.  Not thread-safe, like the reference. */
+ * them before the result is written back.  nInt > 0 with arID / arI: intensities extracted after
+ * the elements arID[0][i] (1-based; nElem + 1: after the post-resize) as the reference does
+ * (srTCompositeOptElem::ExtractPropagatedIntensity, sroptcnt.cpp:429): polarisation arID[1][i],
+ * intensity type arID[2][i] (0 single-electron intensity, 4 phase, 5 Re E, 6 Im E), dependence
+ * arID[3][i] = 3 (vs x and y), representation arID[4][i] = 0; written to arI[i] (allocated with the
+ * function registered by srwlUtiSetAllocArrayFunc when NULL), their meshes to arIM[i].  Other
+ * extraction kinds return error 23900.  Not thread-safe, like the reference. */
 SRWG_API int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SRWLRadMesh* arIM, char** arI,
                         double* arParGPU);
 
@@ -157,6 +162,11 @@ SRWG_API int srwlCalcIntFromElecField(char* pInt, SRWLWfr* pWfr, char pol, char 
 /* Replaces srwlUtiSetWfrModifFunc (srwlib.h:542): registers the client callback that
  * re-allocates wavefront arrays (action 2: allocate for the current mesh; 12: with backup). */
 SRWG_API void srwlUtiSetWfrModifFunc(int (*pExtFunc)(int action, SRWLWfr* pWfrIn, char pol));
+
+/* Replaces srwlUtiSetAllocArrayFunc (srwlib.h:549): registers the client function that allocates the
+ * arrays of intensities extracted during srwlPropagElecField ('f' or 'd', len points) when the caller
+ * passes arI[i] == NULL. */
+SRWG_API void srwlUtiSetAllocArrayFunc(char* (*pExtFunc)(char type, long long len));
 
 /* Replaces srwlUtiGetErrText (srwlib.h:574): copies the text of error/warning number erNo to t
  * (at least 2048 bytes). */

@@ -1456,13 +1456,15 @@ def _pp(pp, i, default):
     return pp[i] if (pp is not None and len(pp) > i) else default
 
 
-def propagate(w: Wfr, elements, props):
+def propagate(w: Wfr, elements, props, after=None):
     """srTCompositeOptElem ctor (sroptcnt.cpp:87-221) + PropagateRadiationGuided (:254-425).
 
     ``elements``: list of tuples ('drift', L, treat) | ('aperture', shape, ap_or_ob, Dx, Dy, x, y)
     | ('lens', Fx, Fy, x, y) | ('transmission', arTr, nx, ny, rx, ry, x, y, extTr, Fx, Fy).
     ``props``: list of per-element propagation parameter lists
-    (len(props) may be len(elements)+1 for a post-resize)."""
+    (len(props) may be len(elements)+1 for a post-resize).  ``after(k, w)``, when given, sees the
+    wavefront after element k and, with k = len(elements), after the post-resize: the points where
+    PropagateRadiationGuided extracts intensities (sroptcnt.cpp:398, :421)."""
     if (w.nx <= 1) or (w.nz <= 1):
         raise ValueError("CAN_NOT_PROPAGATE_1D_RAD")
     tolRes = 1.e-04
@@ -1490,12 +1492,16 @@ def propagate(w: Wfr, elements, props):
             transmission(w, *el[1:])
         else:
             raise ValueError("UNKNOWN_OPTICAL_ELEMENT")
+        if after is not None:
+            after(i, w)
     n = len(elements)
     if n < len(props):
         pp = props[n]
         pxm, pxd, pzm, pzd = _pp(pp, 5, 1.), _pp(pp, 6, 1.), _pp(pp, 7, 1.), _pp(pp, 8, 1.)
         if abs(pxd - 1.) > tolRes or abs(pxm - 1.) > tolRes or abs(pzd - 1.) > tolRes or abs(pzm - 1.) > tolRes:
             rad_resize_gen(w, pxm, pxd, pzm, pzd, other_side=bool(int(_pp(pp, 4, 0))))
+        if after is not None:
+            after(n, w)
     return w
 
 

@@ -69,6 +69,7 @@ class SRWLOptC(C.Structure):
 
 
 MODIF_FUNC = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(SRWLWfr), C.c_char)
+ALLOC_FUNC = C.CFUNCTYPE(C.c_void_p, C.c_char, C.c_longlong)
 
 # symbol -> (restype, argtypes); the complete exported surface of include/srwl_b200.h
 SYMBOLS = {
@@ -78,6 +79,7 @@ SYMBOLS = {
     'srwlPropagElecField': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_int, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.POINTER(C.c_double)]),
     'srwlUtiSetWfrModifFunc': (None, [MODIF_FUNC]),
+    'srwlUtiSetAllocArrayFunc': (None, [ALLOC_FUNC]),
     'srwlUtiGetErrText': (C.c_int, [C.c_char_p, C.c_int]),
     'srwgPlanCreate': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_int, C.POINTER(C.c_void_p)]),
     'srwgPlanGetOutput': (C.c_int, [C.c_void_p, C.POINTER(SRWLWfr)]),

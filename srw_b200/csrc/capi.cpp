@@ -1,5 +1,5 @@
 // C-ABI of the library: the reference's srwlPropagElecField / srwlUtiSetWfrModifFunc /
-// srwlUtiGetErrText (cpp/src/lib/srwlib.h:542, 574, 821) and the srwgPlan* extensions, plus the
+// srwlUtiSetAllocArrayFunc / srwlUtiGetErrText (cpp/src/lib/srwlib.h:542, 549, 574, 821) and the srwgPlan* extensions, plus the
 // executor that runs a plan's passes on a CUDA stream.
 #include <cuda_runtime.h>
 
@@ -24,6 +24,7 @@ namespace srwg {
 static std::string g_lastDetail;                          // detail text of the last error
 void set_last_detail(const std::string& s) { g_lastDetail = s; }
 static int (*g_modifFunc)(int, SRWLWfr*, char) = nullptr;  // client re-allocation callback
+static char* (*g_allocArrayFunc)(char, long long) = nullptr; // client array allocation (extracted intensities)
 static std::mutex g_mutex;
 std::mutex& library_mutex() { return g_mutex; }
 
@@ -228,7 +229,8 @@ static int upload_tables(const Planner& pl, float2** buf, size_t* capElems, cuda
 int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, const float2* inX, const float2* inY,
                    long long inStride, float2* outX, float2* outY, long long outStride, float2* work, size_t workElems,
                    const char* dconst, long long constStride, size_t descOff, cudaStream_t st, cudaEvent_t* ev,
-                   const std::vector<KernelDesc>* hostMax, double* momScratch, double* momSlots, int nSlots)
+                   const std::vector<KernelDesc>* hostMax, double* momScratch, double* momSlots, int nSlots,
+                   char* intOut)
 {
     const size_t nk = ks.size();
     const size_t W = (size_t)nb * workElems;
@@ -239,12 +241,12 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
     // the last pass that writes a field writes the output; MOM passes after it read the output
     size_t lastField = nk;
     for (size_t i = nk; i-- > 0;)
-        if (ks[i].kind != K_MOM) { lastField = i; break; }
+        if (!reads_only(ks[i].kind)) { lastField = i; break; }
 
     for (size_t i = 0; i < nk; i++) {
         const KernelDesc& k = hostMax ? (*hostMax)[i] : ks[i];
         if (ev) CUDA_TRY(cudaEventRecord(ev[2 * i], st));
-        const bool fromOut = k.kind == K_MOM && k.src != 0 && i > lastField && k.src == ks[lastField].dst;
+        const bool fromOut = reads_only(k.kind) && k.src != 0 && i > lastField && k.src == ks[lastField].dst;
         const bool fromIn = k.src == 0, toOut = i == lastField;
         const float2* s0 = fromOut ? outX : fromIn ? inX : wb[k.src][0];
         const float2* s1 = fromOut ? outY : fromIn ? inY : wb[k.src][1];
@@ -271,6 +273,12 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
             p.bSrc = bSrc;
             p.bOut = (long long)nSlots * SRWG_MOM_SLOT;
             e = launch_moments(p, st);
+        } else if (k.kind == K_INT) {
+            if (intOut == nullptr || nb != 1) {
+                g_lastDetail = "intensity extraction pass without its buffer";
+                return SRWG_ERR_BAD_ARG;
+            }
+            e = launch_extract(k.mom, &gk[i].mom, s0, s1, tabs, intOut + k.mom.ioff, st);
         } else if (k.kind == K_LINE) {
             LineLaunch p;
             memset(&p, 0, sizeof(p));
@@ -336,11 +344,11 @@ static int ensure_doubles(double** buf, size_t* cap, size_t n)
 static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* inY, float2* outX, float2* outY,
                    float2* work, size_t workElems, const float2* dtab, cudaStream_t st, cudaEvent_t* ev = nullptr,
                    int nb = 1, long long inStride = 0, long long outStride = 0, double* momSlots = nullptr,
-                   double* momScratch = nullptr)
+                   double* momScratch = nullptr, char* intOut = nullptr)
 {
     const size_t nOut = (size_t)pl.w.nx * pl.w.nz;
     bool anyField = false;
-    for (const KernelDesc& k : pl.kernels) anyField |= (k.kind != K_MOM);
+    for (const KernelDesc& k : pl.kernels) anyField |= !reads_only(k.kind);
     if (!anyField) {          // the output is the input (moment passes, if any, read the input)
         for (int b = 0; b < nb; b++) {
             CUDA_TRY(cudaMemcpyAsync(outX + b * outStride, inX + b * inStride, nOut * sizeof(float2),
@@ -353,7 +361,7 @@ static int execute(Planner& pl, DeviceCtx& c, const float2* inX, const float2* i
     size_t descOff;
     const_bytes(pl, &descOff);
     return execute_passes(pl.kernels, c, nb, inX, inY, inStride, outX, outY, outStride, work, workElems,
-                          (const char*)dtab, 0, descOff, st, ev, nullptr, momScratch, momSlots, pl.nMomSlots);
+                          (const char*)dtab, 0, descOff, st, ev, nullptr, momScratch, momSlots, pl.nMomSlots, intOut);
 }
 
 static int ensure_work(DeviceCtx& c, size_t elems)
@@ -476,6 +484,12 @@ void srwlUtiSetWfrModifFunc(int (*pExtFunc)(int action, SRWLWfr* pWfrIn, char po
     g_modifFunc = pExtFunc;
 }
 
+void srwlUtiSetAllocArrayFunc(char* (*pExtFunc)(char type, long long len))
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    g_allocArrayFunc = pExtFunc;
+}
+
 int srwlUtiGetErrText(char* t, int erNo)
 {
     if (t == nullptr) return 0;
@@ -492,6 +506,7 @@ int srwlUtiGetErrText(char* t, int erNo)
     case SRWL_WFR_EXT_MODIF_FAILED: s = "The wavefront modification (re-allocation) callback failed."; break;
     case SRWL_INCORRECT_PARAM_FOR_WFR_PROP: s = "Incorrect or insufficient parameters for wavefront propagation."; break;
     case SRWL_WFR_EXT_FUNC_NOT_DEFINED: s = "No wavefront modification (re-allocation) callback is registered."; break;
+    case SRWL_EXT_ARRAY_ALLOC_FAILED: s = "Failed to allocate array in front-end / client environment."; break;
     case SRWG_ERR_UNSUPPORTED: s = "Not supported on the GPU propagation path"; break;
     case SRWG_ERR_CUDA: s = "CUDA error"; break;
     case SRWG_ERR_NO_DEVICE: s = "No usable CUDA device"; break;
@@ -506,12 +521,39 @@ int srwlUtiGetErrText(char* t, int erNo)
     return 0;
 }
 
-// srwlPropagElecField for a plan with stage boundaries (an element planned on moments measured from
-// the field): each stage runs from the previous stage's output into a stage buffer, its moment
-// results come back to the host, and planning resumes; the last stage's output is the result
-static int propagate_staged(Planner& pl, SRWLWfr* pWfr, int dev)
+// the intensity extractions of a stage that ran: each into the caller's array (allocated through the
+// registered allocation function when the caller passed none, AllocExtIntArray srradstr.cpp:799),
+// with its mesh (GetIntMesh, srradstr.cpp:4140: the wavefront's x and y mesh, eStart kept)
+static int deliver_extractions(const Planner& pl, const char* dev, cudaStream_t st, char** arI, SRWLRadMesh* arIM)
 {
-    int pr = SRWG_NEED_STAGE;           // planning status: the plan stopped at a stage boundary
+    for (const IntOut& o : pl.intOuts) {
+        char*& dst = arI[o.index];
+        if (dst == nullptr) {
+            if (g_allocArrayFunc != nullptr) dst = (*g_allocArrayFunc)(o.arType, (long long)o.nx * o.nz);
+            if (dst == nullptr) return SRWL_EXT_ARRAY_ALLOC_FAILED;
+        }
+        CUDA_TRY(cudaMemcpyAsync(dst, dev + o.off, (size_t)o.bytes, cudaMemcpyDeviceToHost, st));
+        if (arIM != nullptr) {
+            SRWLRadMesh& m = arIM[o.index];
+            m.ne = 1;
+            m.nx = o.nx;
+            m.xStart = o.xStart;
+            m.xFin = o.xStart + o.xStep * (o.nx - 1);
+            m.ny = o.nz;
+            m.yStart = o.zStart;
+            m.yFin = o.zStart + o.zStep * (o.nz - 1);
+        }
+    }
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return 0;
+}
+
+// srwlPropagElecField for a plan with stage boundaries (an element planned on moments measured from
+// the field) or intensity extractions: each stage runs from the previous stage's output into a stage
+// buffer, its moment results and extractions come back to the host, and planning resumes; the last
+// stage's output is the result.  pr: the planning status (SRWG_NEED_STAGE or 0 for a single stage)
+static int propagate_staged(Planner& pl, SRWLWfr* pWfr, int dev, int pr, char** arI, SRWLRadMesh* arIM)
+{
     DeviceCtx* c = nullptr;
     int r = device_ctx(dev, &c);
     if (r) return r;
@@ -548,9 +590,20 @@ static int propagate_staged(Planner& pl, SRWLWfr* pWfr, int dev)
             r = ensure_doubles(&c->mom, &c->momDoubles, nSlotD + mom_scratch_for(pl));
             if (r) return r;
         }
+        if (pl.intBytes > 0 && (c->genBuf == nullptr || c->genBytes < (size_t)pl.intBytes)) {
+            if (c->genBuf) cudaFree(c->genBuf);
+            c->genBuf = nullptr; c->genBytes = 0;
+            CUDA_TRY(cudaMalloc(&c->genBuf, (size_t)pl.intBytes));
+            c->genBytes = (size_t)pl.intBytes;
+        }
         r = execute(pl, *c, curX, curY, oX, oY, c->work, c->workElems, c->tab, st, nullptr, 1, 0, 0,
-                    nSlotD ? c->mom : nullptr, nSlotD ? c->mom + nSlotD : nullptr);
+                    nSlotD ? c->mom : nullptr, nSlotD ? c->mom + nSlotD : nullptr,
+                    pl.intBytes > 0 ? (char*)c->genBuf : nullptr);
         if (r) return r;
+        if (!pl.intOuts.empty()) {
+            r = deliver_extractions(pl, (const char*)c->genBuf, st, arI, arIM);
+            if (r) return r;
+        }
         tmp.assign(nSlotD, 0.);
         if (nSlotD) CUDA_TRY(cudaMemcpyAsync(tmp.data(), c->mom, nSlotD * sizeof(double), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaStreamSynchronize(st));
@@ -587,19 +640,38 @@ int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SR
     std::lock_guard<std::mutex> lk(g_mutex);
     g_lastDetail.clear();
     if (pWfr == nullptr || pOpt == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
-    if (nInt != 0 && arID != nullptr && arI != nullptr) {
-        g_lastDetail = "intermediate intensity extraction (nInt > 0)";
-        return SRWG_ERR_UNSUPPORTED;
-    }
-    (void)arIM;
     int dev = 0;
     if (arParGPU != nullptr && arParGPU[0] >= 1. && arParGPU[1] >= 1.) dev = (int)arParGPU[1] - 1;
     if (pWfr->arEx == nullptr && pWfr->arEy == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
 
     Planner pl;
     pl.allowStages = true;
+    // intensity extractions after elements (PropagateRadiationGuided, sroptcnt.cpp:268, and
+    // ExtractPropagatedIntensity :429): arID[0..4][i] = element number (1-based), polarisation,
+    // intensity type, dependence, representation; negative values (and arIM[i].ne < 0) of the
+    // later requests take the first request's
+    const bool wantInt = nInt > 0 && arID != nullptr && arI != nullptr;
+    if (wantInt) {
+        for (int j = 0; j < 5; j++)
+            if (arID[j] == nullptr) return SRWL_INCORRECT_PARAM_FOR_WFR_PROP;
+        for (int i = 0; i < nInt; i++) {
+            IntReq q;
+            q.index = i;
+            q.elem = (int)arID[0][i] - 1;
+            q.pol = arID[1][i]; q.type = arID[2][i]; q.dep = arID[3][i]; q.pres = arID[4][i];
+            if (nInt > 1 && i > 0) {
+                if (q.pol < 0) q.pol = arID[1][0];
+                if (q.type < 0) q.type = arID[2][0];
+                if (q.dep < 0) q.dep = arID[3][0];
+                if (q.pres < 0) q.pres = arID[4][0];
+                if (arIM != nullptr && arIM[i].ne < 0) arIM[i] = arIM[0];
+            }
+            pl.intReqs.push_back(q);
+        }
+    }
     int r = pl.plan(pWfr, pOpt);
-    if (r == SRWG_NEED_STAGE) return propagate_staged(pl, pWfr, dev);
+    if (r == SRWG_NEED_STAGE || (r == 0 && wantInt))
+        return propagate_staged(pl, pWfr, dev, r, wantInt ? arI : nullptr, wantInt ? arIM : nullptr);
     if (r) { g_lastDetail = pl.err; return r; }
     DeviceCtx* c = nullptr;
     r = device_ctx(dev, &c);

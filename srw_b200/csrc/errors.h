@@ -13,6 +13,7 @@
 #define SRWL_WFR_EXT_MODIF_FAILED (168 + SRWG_FIRST_ERR)
 #define SRWL_INCORRECT_PARAM_FOR_WFR_PROP (171 + SRWG_FIRST_ERR)
 #define SRWL_WFR_EXT_FUNC_NOT_DEFINED (172 + SRWG_FIRST_ERR)
+#define SRWL_EXT_ARRAY_ALLOC_FAILED (188 + SRWG_FIRST_ERR)
 
 #define SRWG_ERR_UNSUPPORTED (900 + SRWG_FIRST_ERR)     // feature outside the GPU path
 #define SRWG_ERR_CUDA (901 + SRWG_FIRST_ERR)            // CUDA runtime error (text has details)

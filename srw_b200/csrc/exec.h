@@ -34,7 +34,7 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
                    long long inStride, float2* outX, float2* outY, long long outStride, float2* work, size_t workElems,
                    const char* dconst, long long constStride, size_t descOff, cudaStream_t st, cudaEvent_t* ev,
                    const std::vector<KernelDesc>* hostMax, double* momScratch = nullptr, double* momSlots = nullptr,
-                   int nSlots = 0);
+                   int nSlots = 0, char* intOut = nullptr);
 int line_config(const LineDesc& d, LineLaunch& p);   // launch shape of a line pass (capi.cpp)
 int radix_plan(int N, int* r);
 void set_last_detail(const std::string& s);          // detail text for srwlUtiGetErrText

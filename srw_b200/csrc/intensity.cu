@@ -14,58 +14,12 @@
 
 #include "../../include/srwl_b200.h"
 #include "errors.h"
+#include "common.cuh"
 #include "exec.h"
+#include "intensity.cuh"
+#include "kernels.h"
 
 namespace srwg {
-
-// FormalPhase (srradmnp.h:434): argument from atan of the FP32 ratio, the reference's quadrants
-__device__ __forceinline__ double formal_phase(float re, float im)
-{
-    const double HalhPi = 1.5707963267949, Pi = 3.1415926535898;
-    if (re != 0.f) {
-        const double a = atan((double)__fdiv_rn(im, re));
-        if (im <= 0.f) return re < 0.f ? a - Pi : a;
-        return re < 0.f ? a + Pi : a;
-    }
-    if (im == 0.f) return 0.;
-    return im > 0.f ? HalhPi : -HalhPi;
-}
-
-// IntensityComponent (srradmnp.h:367-425) with its FP32 / FP64 operation order (no contraction):
-// what 0 intensity, 2 phase, 3 Re E, 6 Im E; pol 0..6 and the Stokes components -1..-4
-__device__ __forceinline__ float int_component(float2 x, float2 z, int pol, int what)
-{
-    if (pol == -1)
-        return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x.x, x.x), __fmul_rn(x.y, x.y)), __fmul_rn(z.x, z.x)),
-                         __fmul_rn(z.y, z.y));
-    if (pol == -2)
-        return __fsub_rn(__fadd_rn(__fmul_rn(x.x, x.x), __fmul_rn(x.y, x.y)),
-                         __fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y)));
-    if (pol == -3) return (float)(2. * (double)__fadd_rn(__fmul_rn(x.x, z.x), __fmul_rn(x.y, z.y)));
-    if (pol == -4) return (float)(2. * (double)__fsub_rn(__fmul_rn(x.x, z.y), __fmul_rn(x.y, z.x)));
-    float a, b;
-    bool half = true;
-    switch (pol) {
-    case 0: a = x.x; b = x.y; half = false; break;
-    case 1: a = z.x; b = z.y; half = false; break;
-    case 2: a = __fadd_rn(x.x, z.x); b = __fadd_rn(x.y, z.y); break;
-    case 3: a = __fsub_rn(x.x, z.x); b = __fsub_rn(x.y, z.y); break;
-    case 5: a = __fsub_rn(x.x, z.y); b = __fadd_rn(x.y, z.x); break;
-    case 4: a = __fadd_rn(x.x, z.y); b = __fsub_rn(x.y, z.x); break;
-    default:
-        if (what == 0)
-            return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(x.x, x.x), __fmul_rn(x.y, x.y)), __fmul_rn(z.x, z.x)),
-                             __fmul_rn(z.y, z.y));
-        a = x.x; b = x.y; half = false;
-    }
-    if (what == 0) {
-        const float v = __fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b));
-        return half ? (float)(0.5 * (double)v) : v;
-    }
-    if (what == 2) return (float)formal_phase(a, b);
-    const float v = what == 3 ? a : b;
-    return half ? (float)__dmul_rn(0.70710678, (double)v) : v;
-}
 
 // mode 0: write; 1: average with weight iter (FP64, then FP32); 2: add
 __global__ void __launch_bounds__(256) intensity_kernel(const float2* __restrict__ ex, const float2* __restrict__ ez,
@@ -90,6 +44,46 @@ __global__ void __launch_bounds__(256) intensity_kernel(const float2* __restrict
             }
         }
     }
+}
+
+// intensity extraction pass of a propagation (srTCompositeOptElem::ExtractPropagatedIntensity,
+// cpp/src/core/sroptcnt.cpp:429, writing as srwlCalcIntFromElecField does): the field at an element
+// boundary is the source buffer times the operators still pending on it (separable tables and the
+// non-separable work), applied on the fly
+__global__ void __launch_bounds__(256) extract_kernel(const MomDesc* __restrict__ gd, const float2* __restrict__ s0,
+                                                      const float2* __restrict__ s1, const float2* __restrict__ tabs,
+                                                      float* outF, double* outD)
+{
+    const MomDesc& d = *gd;
+    const int nx = d.nx;
+    const long long n = (long long)nx * d.nz;
+    const long long tx = d.t.tab, tz = d.t.ltab;
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < n; o += (long long)gridDim.x * blockDim.x) {
+        const int iz = (int)(o / nx), ix = (int)(o - (long long)iz * nx);
+        float2 f = make_float2(1.f, 0.f);
+        if (tx >= 0) f = __ldg(&tabs[tx + ix]);
+        if (tz >= 0) f = cmul(f, __ldg(&tabs[tz + iz]));
+        if (d.has_extra) {
+            bool zero = false;
+            extra_eval(d.extra, ix, iz, f, zero, tabs);
+            if (zero) f = make_float2(0.f, 0.f);
+        }
+        const float2 x = cmul(f, __ldg(&s0[o])), z = cmul(f, __ldg(&s1[o]));
+        const float v = int_component(x, z, d.ipol, d.iwhat);
+        if (outD) outD[o] = (double)v;
+        else outF[o] = v;
+    }
+}
+
+cudaError_t launch_extract(const MomDesc& d, const MomDesc* gd, const float2* s0, const float2* s1,
+                           const float2* tabs, char* out, cudaStream_t st)
+{
+    const long long n = (long long)d.nx * d.nz;
+    if (n <= 0 || out == nullptr) return cudaErrorInvalidValue;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    extract_kernel<<<blocks, 256, 0, st>>>(gd, s0, s1, tabs, d.iwhat == 2 ? nullptr : (float*)out,
+                                           d.iwhat == 2 ? (double*)out : nullptr);
+    return cudaGetLastError();
 }
 
 }  // namespace srwg

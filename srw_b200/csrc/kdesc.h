@@ -147,11 +147,18 @@ struct MomDesc {
     int has_extra;
     PwOps extra;
     int slot;
+    // intensity extraction passes (K_INT) only: polarisation, component (0 intensity, 2 phase,
+    // 3 Re E, 6 Im E) and the byte offset of the output in the extraction buffer
+    int ipol, iwhat;
+    long long ioff;
 };
 
 #define SRWG_MOM_SLOT 32   // doubles per result slot: 22 sums, 4 power-limit indices, status
 
-enum KernelKind { K_LINE = 1, K_RESIZE = 2, K_PW = 3, K_MOM = 4 };
+enum KernelKind { K_LINE = 1, K_RESIZE = 2, K_PW = 3, K_MOM = 4, K_INT = 5 };
+
+// passes that only read the field (moments, intensity extraction)
+inline bool reads_only(int kind) { return kind == K_MOM || kind == K_INT; }
 
 struct KernelDesc {
     int kind;

@@ -86,6 +86,11 @@ struct MomLaunch {
 size_t mom_scratch_doubles(int nx, int nz);
 cudaError_t launch_moments(const MomLaunch& p, cudaStream_t st);
 
+// intensity extraction from a field with the operators still pending on it (d: host copy, gd: the
+// device copy the kernel reads); writes nx * nz values (float, or double for the phase) to out
+cudaError_t launch_extract(const MomDesc& d, const MomDesc* gd, const float2* s0, const float2* s1,
+                           const float2* tabs, char* out, cudaStream_t st);
+
 cudaError_t launch_line(const LineLaunch& p, cudaStream_t st);
 
 // power-of-two line pass kernels, one translation unit per line length (line2_<logn>.cu)

@@ -149,11 +149,11 @@ public:
     // read-only moment pass on the current field (index order = the logical mesh).  The operators
     // still pending in an element-wise pass are applied on the fly by the moment pass, which runs
     // just before that pass and reads its source; the element-wise pass stays open.
-    MomDesc& moments(const WfrState& w)
+    MomDesc& moments(const WfrState& w, int kind = K_MOM)
     {
         KernelDesc k;
         memset(&k, 0, sizeof(k));
-        k.kind = K_MOM;
+        k.kind = kind;
         if (open >= 0 && open == (int)ks.size() - 1 && ks[open].kind == K_PW && !fx && !fz &&
             !ks[open].pwk.mirror_x && !ks[open].pwk.mirror_z && ks[open].pwk.nx == w.nx && ks[open].pwk.nz == w.nz) {
             k.src = k.dst = ks[open].src;
@@ -697,6 +697,50 @@ void single_moment_pass(const WfrState& w, KernelDesc& k, MomOp& op, std::vector
     fill_moment_desc(w, ks[0].mom, op);
     build_tables(ks, tables);
     k = ks[0];
+}
+
+// srTCompositeOptElem::ExtractPropagatedIntensity (sroptcnt.cpp:429-475) for the requests of element
+// `elem`: a read-only pass on the field as the element leaves it (the operators still pending on it
+// applied on the fly) writes the intensity component into the stage's extraction buffer; the mesh is
+// the wavefront's (GetIntMesh, srradstr.cpp:4140).  Vs x and y (dep 3) in the coordinate
+// representation, single-electron intensity / phase / Re E / Im E (SRWL numbering 0, 4, 5, 6)
+void Planner::extract_after(int elem)
+{
+    for (const IntReq& q : intReqs) {
+        if (q.elem != elem) continue;
+        if (q.dep != 3 || q.pres != 0 || w.Pres != 0) {
+            err = "intensity extraction during propagation vs x and y (dep 3) in the coordinate representation only";
+            throw (int)SRWG_ERR_UNSUPPORTED;
+        }
+        int what;
+        switch (q.type) {      // arIntTypeConv (sroptcnt.cpp:446): SRWL numbering -> internal
+        case 0: what = 0; break;
+        case 4: what = 2; break;
+        case 5: what = 3; break;
+        case 6: what = 6; break;
+        default:
+            err = "intensity type " + std::to_string(q.type) + " during propagation (0, 4, 5 and 6 are supported)";
+            throw (int)SRWG_ERR_UNSUPPORTED;
+        }
+        if (q.pol < -4 || q.pol > 6) {
+            err = "polarisation " + std::to_string(q.pol) + " for intensity extraction during propagation";
+            throw (int)SRWG_ERR_UNSUPPORTED;
+        }
+        MomDesc& d = b->moments(w, K_INT);
+        d.nx = w.nx; d.nz = w.nz;
+        d.xStart = w.xStart; d.xStep = w.xStep; d.zStart = w.zStart; d.zStep = w.zStep;
+        d.slot = -1;
+        d.ipol = q.pol; d.iwhat = what;
+        IntOut o;
+        o.index = q.index; o.nx = w.nx; o.nz = w.nz;
+        o.xStart = w.xStart; o.xStep = w.xStep; o.zStart = w.zStart; o.zStep = w.zStep;
+        o.arType = what == 2 ? 'd' : 'f';
+        o.bytes = (long long)w.nx * w.nz * (what == 2 ? 8 : 4);
+        o.off = intBytes;
+        d.ioff = o.off;
+        intBytes += (o.bytes + 255) & ~255LL;
+        intOuts.push_back(o);
+    }
 }
 
 // EstimateWfrRadToSub_AnalytTreatQuadPhaseTerm (sroptdrf.cpp:1123-1365): the radius to subtract in
@@ -1404,6 +1448,8 @@ int Planner::plan(const SRWLWfr* pw, const SRWLOptC* opt)
     momOps.clear();
     nMomSlots = 0;
     momProvisional = false;
+    intOuts.clear();
+    intBytes = 0;
     nStages = 0;
     slotVals_.clear();
     pendingEstSlot_ = -1;
@@ -1455,6 +1501,8 @@ int Planner::resume(const double* slots)
     quadFlagsUncertain_ = false;
     kernels.clear();
     tables.clear();
+    intOuts.clear();
+    intBytes = 0;
     maxElems = 0;
     stageIn = w;
     nStages++;
@@ -1498,15 +1546,19 @@ int Planner::run()
             else if (e.kind == E_LENS) lens(e);
             else if (e.kind == E_APERTURE) aperture(e);
             else if (e.kind == E_TRANSM) transmission(e);
+            if (!intReqs.empty()) extract_after((int)i);
         }
-        if (i < numRes && props[i].n >= 0) {
+        if (i < numRes) {
             const PropDesc& p = props[i];
-            double pxm = p.get(5, 1.), pxd = p.get(6, 1.), pzm = p.get(7, 1.), pzd = p.get(8, 1.);
-            if ((::fabs(pxd - 1.) > tolRes) || (::fabs(pxm - 1.) > tolRes) || (::fabs(pzd - 1.) > tolRes) ||
-                (::fabs(pzm - 1.) > tolRes)) {
-                int rr = resize(pxm, pxd, pzm, pzd, 0, 0., 0., (int)p.get(4, 0) != 0);
-                if (rr) throw rr;
+            if (p.n >= 0) {
+                double pxm = p.get(5, 1.), pxd = p.get(6, 1.), pzm = p.get(7, 1.), pzd = p.get(8, 1.);
+                if ((::fabs(pxd - 1.) > tolRes) || (::fabs(pxm - 1.) > tolRes) || (::fabs(pzd - 1.) > tolRes) ||
+                    (::fabs(pzm - 1.) > tolRes)) {
+                    int rr = resize(pxm, pxd, pzm, pzd, 0, 0., 0., (int)p.get(4, 0) != 0);
+                    if (rr) throw rr;
+                }
             }
+            if (!intReqs.empty()) extract_after((int)els.size());   // after the post-resize (sroptcnt.cpp:421)
         }
     } catch (int code) {
         if (code != SRWG_NEED_STAGE) {
@@ -1561,7 +1613,7 @@ int Planner::finalize()
         for (KernelDesc& k : kernels) {
             if (k.kind == K_LINE) { patch(k.line.pw); patch(k.line.extra); }
             else if (k.kind == K_RESIZE) { patch(k.rs.pw); patch(k.rs.extra); patch(k.rs.pre); patch(k.rs.pre_extra); }
-            else if (k.kind == K_MOM) { patch(k.mom.pw); patch(k.mom.extra); }
+            else if (reads_only(k.kind)) { patch(k.mom.pw); patch(k.mom.extra); }
             else { patch(k.pwk.pw); patch(k.pwk.extra); }
         }
     }
@@ -1638,6 +1690,10 @@ std::string Planner::describe() const
         } else if (k.kind == K_MOM) {
             snprintf(buf, sizeof(buf), "%zu MOM %dx%d (q%d a%d m%d s%d) slot=%d  buf %d\n", i, k.mom.nx, k.mom.nz,
                      k.mom.pw.has_quad, k.mom.pw.has_ang, k.mom.pw.nmask, k.mom.pw.has_scale, k.mom.slot, k.src);
+        } else if (k.kind == K_INT) {
+            snprintf(buf, sizeof(buf), "%zu INT %dx%d (q%d a%d m%d s%d) pol=%d what=%d off=%lld  buf %d\n", i, k.mom.nx,
+                     k.mom.nz, k.mom.pw.has_quad, k.mom.pw.has_ang, k.mom.pw.nmask, k.mom.pw.has_scale, k.mom.ipol,
+                     k.mom.iwhat, k.mom.ioff, k.src);
         } else {
             snprintf(buf, sizeof(buf), "%zu PW %dx%d (q%d a%d m%d s%d) mirror=%d/%d  buf %d->%d\n", i, k.pwk.nx, k.pwk.nz,
                      k.pwk.pw.has_quad, k.pwk.pw.has_ang, k.pwk.pw.nmask, k.pwk.pw.has_scale, k.pwk.mirror_x,

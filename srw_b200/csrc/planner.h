@@ -82,6 +82,21 @@ void moments_from_sums(const double* S, const MomOp& op, double* momX, double* m
 // fills the separable point-wise tables of every pass (tables.cpp)
 void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& tables);
 
+// an intensity extraction after an element (srwlPropagElecField's arID / arIM / arI lists): after
+// element `elem` (0-based; the number of elements: after the post-resize), request `index`
+struct IntReq {
+    int elem = 0, index = 0;
+    int pol = 6, type = 0, dep = 3, pres = 0;
+};
+
+// a planned extraction of the current stage: its pass writes bytes at off of the extraction buffer
+struct IntOut {
+    int index = 0, nx = 0, nz = 0;
+    double xStart = 0, xStep = 0, zStart = 0, zStep = 0;
+    long long off = 0, bytes = 0;
+    char arType = 'f';
+};
+
 class Planner {
 public:
     WfrState w;                          // evolves from the input to the output state
@@ -94,6 +109,9 @@ public:
     bool numMoments = true;              // emit MOM passes where the reference recomputes the moments
     int nMomSlots = 0;                   // MOM passes of the plan (result slots per wavefront)
     std::vector<MomOp> momOps;
+    std::vector<IntReq> intReqs;         // intensity extractions asked for (set before plan())
+    std::vector<IntOut> intOuts;         // those planned in the current stage
+    long long intBytes = 0;              // extraction buffer of the current stage
 
     // the output moments from the input ones and the MOM passes' result slots (nMomSlots x
     // SRWG_MOM_SLOT doubles; unused when nMomSlots == 0)
@@ -123,6 +141,7 @@ private:
     int run();
     int finalize();
     void emit_moment_pass(MomOp& op, bool certain);
+    void extract_after(int elem);
     void estimate_rad(double L, double& effRx, double& effRz);
     int flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vector<PropDesc>& props, bool nested);
     void set_full_range();

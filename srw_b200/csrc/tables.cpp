@@ -266,7 +266,7 @@ void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& T)
                     r.tile_oc = ec;
                 }
             }
-        } else if (k.kind == K_MOM) {
+        } else if (reads_only(k.kind)) {
             MomDesc& m = k.mom;
             SepPart A, Lp;
             cd scale;

@@ -165,7 +165,7 @@ def _update_py_wfr(wfr, w):
     wfr.presFT = ord(w.presFT) if w.presFT else 0
 
 
-_state = {'wfr': None, 'keep': None}
+_state = {'wfr': None, 'keep': None, 'arrays': {}}
 
 
 @capi.MODIF_FUNC
@@ -198,12 +198,112 @@ def _modif(action, pw, pol):
         return -1
 
 
+@capi.ALLOC_FUNC
+def _alloc_array(typ, n):
+    """Client array for an extracted intensity (the reference's AllocPyArrayGetBuf, srwlpy.cpp:4424:
+    srwl_uti_array_alloc(type, n), zero-filled); kept until the call returns."""
+    t = typ.decode() if isinstance(typ, bytes) else chr(typ)
+    if t not in ('d', 'f', 'i') or n <= 0:
+        return None
+    a = array(t, bytes(int(n) * array(t).itemsize))
+    addr = a.buffer_info()[0]
+    _state['arrays'][addr] = a
+    return addr
+
+
+def _is_mesh(o):
+    return type(o).__name__ == 'SRWLRadMesh'
+
+
+def _parse_int_list(intList):
+    """ParseSructSRWLPropIntDef (srwlpy.cpp:2784): (requests [el, pol, type, dep, pres], meshes, flat).
+    Flat format: [[el, pol, type, dep, pres, SRWLRadMesh], ...]; column format: [els, pols, types, deps,
+    press, meshes], each a list or one value for all (later entries then take the first one's)."""
+    if not isinstance(intList, list) or len(intList) <= 0:
+        raise RuntimeError('Incorrect list of parameters for intensity extraction at propagation')
+    o = intList[0]
+    if isinstance(o, list) and len(o) == 6 and _is_mesh(o[5]):
+        return [list(map(int, it[:5])) for it in intList], [it[5] for it in intList], True
+    n = len(o) if isinstance(o, list) else 1
+    cols = []
+    for j in range(6):
+        v = intList[j]
+        if isinstance(v, list) and isinstance(o, list):
+            cols.append(list(v))
+        elif j == 0 and isinstance(o, list):
+            raise RuntimeError('Incorrect list of parameters for intensity extraction at propagation')
+        else:
+            cols.append([v] + [None] * (n - 1))
+    reqs = [[(-1 if cols[j][i] is None else int(cols[j][i])) for j in range(5)] for i in range(n)]
+    return reqs, cols[5], False
+
+
+def _mesh_to_c(m, cm):
+    if m is None:
+        cm.ne = -1
+        return
+    cm.eStart, cm.eFin = float(m.eStart), float(m.eFin)
+    cm.xStart, cm.xFin = float(m.xStart), float(m.xFin)
+    cm.yStart, cm.yFin = float(m.yStart), float(m.yFin)
+    cm.zStart = float(getattr(m, 'zStart', 0.))
+    cm.ne, cm.nx, cm.ny = int(m.ne), int(m.nx), int(m.ny)
+
+
+def _mesh_from_c(cm, m):
+    """UpdatePyRadMesh (srwlpy.cpp): the mesh object takes the extraction's mesh."""
+    m.eStart, m.eFin = cm.eStart, cm.eFin
+    m.xStart, m.xFin = cm.xStart, cm.xFin
+    m.yStart, m.yFin = cm.yStart, cm.yFin
+    m.ne, m.nx, m.ny = int(cm.ne), int(cm.nx), int(cm.ny)
+
+
+def _copy_mesh(m):
+    f = getattr(m, 'copy', None)
+    if callable(f):
+        return f()
+    import copy
+    return copy.copy(m)
+
+
+def _update_int_list(intList, flat, meshes, cms, arrays):
+    """UpdatePyPropInt (srwlpy.cpp:3809): meshes updated in place and the intensity arrays added
+    (flat format: as the 7th item of each request; column format: as item 6, a list when there are
+    several requests)."""
+    if flat:
+        for i, it in enumerate(intList):
+            _mesh_from_c(cms[i], it[5])
+            if len(it) > 6:
+                it[6] = arrays[i]
+            else:
+                it.append(arrays[i])
+        return
+    n = len(arrays)
+    oMesh = intList[5]
+    lists = n > 1 or isinstance(oMesh, list)
+    if n > 1 and not isinstance(oMesh, list):
+        oMesh = [oMesh] + [_copy_mesh(oMesh) for _ in range(n - 1)]
+        intList[5] = oMesh
+    elif lists:
+        seen = set()
+        for i in range(n):              # the same mesh object twice: the later ones get copies
+            if id(oMesh[i]) in seen:
+                oMesh[i] = _copy_mesh(oMesh[i])
+            seen.add(id(oMesh[i]))
+    for i in range(n):
+        _mesh_from_c(cms[i], oMesh[i] if lists else oMesh)
+    res = list(arrays) if lists else arrays[0]
+    if len(intList) > 6:
+        intList[6] = res
+    else:
+        intList.append(res)
+
+
 def PropagElecField(wfr, optC, intList=None, dev=None):
-    """Propagates ``wfr`` in place through ``optC`` on the GPU; returns ``wfr``."""
+    """Propagates ``wfr`` in place through ``optC`` on the GPU; returns ``wfr``.  ``intList``: intensities
+    to extract after elements (vs x and y; the reference's list formats), completed in place with the
+    extracted arrays and their meshes."""
     if wfr is None or optC is None:
         raise RuntimeError('Incorrect arguments for PropagElecField')
-    if intList is not None:
-        raise RuntimeError('intermediate intensity extraction is not supported on the GPU path')
     L = capi.lib()
     keep = []
     w = make_c_wfr(wfr, keep)
@@ -211,17 +311,36 @@ def PropagElecField(wfr, optC, intList=None, dev=None):
     par = None
     if dev is not None:
         par = (C.c_double * 2)(1., float(dev))
+    nInt, arID, arIM, arI = 0, None, None, None
+    if intList is not None:
+        reqs, meshes, flat = _parse_int_list(intList)
+        nInt = len(reqs)
+        cols = [(C.c_byte * nInt)(*[max(-128, min(127, r[j])) for r in reqs]) for j in range(5)]
+        arID = (C.c_void_p * 5)(*[C.cast(c, C.c_void_p) for c in cols])
+        arIM = (capi.SRWLRadMesh * nInt)()
+        for i in range(nInt):
+            _mesh_to_c(meshes[i] if i < len(meshes) else None, arIM[i])
+        arI = (C.c_void_p * nInt)()
+        keep += cols + [arID, arIM, arI]
     _state['wfr'] = wfr
     _state['keep'] = keep
+    _state['arrays'] = {}
     try:
         L.srwlUtiSetWfrModifFunc(_modif)
-        r = L.srwlPropagElecField(C.byref(w), C.byref(o), 0, None, None, None, par)
+        L.srwlUtiSetAllocArrayFunc(_alloc_array)
+        r = L.srwlPropagElecField(C.byref(w), C.byref(o), nInt, C.cast(arID, C.c_void_p) if arID else None,
+                                  C.cast(arIM, C.c_void_p) if arIM else None,
+                                  C.cast(arI, C.c_void_p) if arI else None, par)
+        arrays = [_state['arrays'].get(arI[i]) for i in range(nInt)] if nInt else []
     finally:
         _state['wfr'] = None
         _state['keep'] = None
+        _state['arrays'] = {}
     if r > 0:
         raise RuntimeError(capi.err_text(r))
     _update_py_wfr(wfr, w)
+    if nInt:
+        _update_int_list(intList, flat, meshes, arIM, arrays)
     return wfr
 
 

@@ -332,6 +332,44 @@ def main():
                                                          eStart=mp['e'], eFin=mp['e'], zStart=mp['z']),
                          unit=mp['unit']))
     blob['gauss/index'] = np.array(json.dumps(gidx))
+    # 5) intensities extracted during propagation (srwlPropagElecField's intList, flat format):
+    #    after a drift, an aperture (mask still pending in the GPU plan), a lens, the last drift and
+    #    the post-resize; intensity, Re E and Im E of several polarisations.  (The phase, type 4, is
+    #    left out: the reference allocates the client array for it as float (AllocExtIntArray gets the
+    #    converted type, sroptcnt.cpp:465, srradstr.cpp:807) and writes doubles into it, which crashes)
+    pp = lambda anal=0, pxm=1., pxd=1., pzm=1., pzd=1.: [0, 0, 1., anal, 0, pxm, pxd, pzm, pzd, 0, 0, 0]  # noqa: E731
+    c0 = [('drift', 10., 0), ('aperture', 'r', 'a', 1e-3, 1e-3, 0., 0.), ('lens', 5., 5., 0., 0.), ('drift', 5., 0)]
+    c1 = [('aperture', 'c', 'a', 0.8e-3, 0.8e-3, 0., 0.), ('lens', 10., 10., 0., 0.), ('drift', 10., 0)]
+    c1pp = [pp(), pp(0, 2., 2., 2., 2.), pp(4)]
+    xcases = [
+        ('x_c0', lambda: gaussian_wfr(L, 1000., 50e-6, 64, 64, 1e-3, 1e-3), c0, [PP0] * 4 + [pp(0, 1.5, 1., 1.25, 1.)],
+         [(1, 6, 0), (2, 0, 5), (3, 6, 5), (3, 1, 6), (4, 2, 0), (5, 6, 0)]),
+        ('x_c1', lambda: undulator_wfr(L, 64, 64, npTraj=4000), c1, c1pp,
+         [(1, 6, 0), (2, -1, 0), (3, 6, 0), (3, 0, 6)]),
+    ]
+    xidx = []
+    for xname, make, elems, pps, reqs in xcases:
+        w = make()
+        if xname == 'x_c1':          # a vertical component too, so that the polarisations differ
+            ex = np.array(w.arEx, np.float32)
+            w.arEy = array('f', (0.3 * ex[::-1]).astype(np.float32).tobytes())
+        inp = snapshot(w)
+        intList = [[el, pol, typ, 3, 0, L.SRWLRadMesh(w.mesh.eStart, w.mesh.eStart, 1)] for el, pol, typ in reqs]
+        L.srwl.PropagElecField(w, L.SRWLOptC(build_beamline(L, elems), [list(map(float, p)) for p in pps]), intList)
+        for k, v in inp.items():
+            blob['xint/' + xname + '/in/' + k] = v
+        for i, it in enumerate(intList):
+            m = it[5]
+            blob['xint/%s/%d/mesh' % (xname, i)] = np.array([m.nx, m.ny, m.xStart, m.xFin, m.yStart, m.yFin, m.eStart,
+                                                             m.ne], np.float64)
+            blob['xint/%s/%d/I' % (xname, i)] = np.array(it[6], np.float64 if it[2] == 4 else np.float32)
+        out = snapshot(w)
+        blob['xint/' + xname + '/out/ex'] = out['ex']
+        blob['xint/' + xname + '/out/mesh'] = out['mesh']
+        xidx.append(dict(name=xname, elements=[list(e) for e in elems], props=[list(map(float, p)) for p in pps],
+                         reqs=[list(r) for r in reqs]))
+        print(xname, [int(blob['xint/%s/%d/mesh' % (xname, i)][0]) for i in range(len(reqs))])
+    blob['xint/index'] = np.array(json.dumps(xidx))
     blob['index'] = np.array(json.dumps(index))
     np.savez_compressed(os.path.join(HERE, 'cases.npz'), **blob)
 

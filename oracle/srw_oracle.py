@@ -1456,11 +1456,32 @@ def _pp(pp, i, default):
     return pp[i] if (pp is not None and len(pp) > i) else default
 
 
+def _element(w: Wfr, el, anal):
+    """One element of a chain; a nested container ('container', elements, props) propagates every
+    element inside it (nested containers included) with the outer entry's treatment, its own
+    parameter lists unused (srTCompositeOptElem::PropagateRadiation, sroptcnt.h:52-76)."""
+    kind = el[0]
+    if kind == 'drift':
+        drift(w, el[1], el[2], anal)
+    elif kind == 'lens':
+        lens(w, el[1], el[2], el[3], el[4])
+    elif kind == 'aperture':
+        aperture(w, el[1], el[2], el[3], el[4], el[5], el[6])
+    elif kind == 'transmission':
+        transmission(w, *el[1:])
+    elif kind == 'container':
+        for sub in el[1]:
+            _element(w, tuple(sub), anal)
+    else:
+        raise ValueError("UNKNOWN_OPTICAL_ELEMENT")
+
+
 def propagate(w: Wfr, elements, props, after=None):
     """srTCompositeOptElem ctor (sroptcnt.cpp:87-221) + PropagateRadiationGuided (:254-425).
 
     ``elements``: list of tuples ('drift', L, treat) | ('aperture', shape, ap_or_ob, Dx, Dy, x, y)
-    | ('lens', Fx, Fy, x, y) | ('transmission', arTr, nx, ny, rx, ry, x, y, extTr, Fx, Fy).
+    | ('lens', Fx, Fy, x, y) | ('transmission', arTr, nx, ny, rx, ry, x, y, extTr, Fx, Fy)
+    | ('container', elements, props).
     ``props``: list of per-element propagation parameter lists
     (len(props) may be len(elements)+1 for a post-resize).  ``after(k, w)``, when given, sees the
     wavefront after element k and, with k = len(elements), after the post-resize: the points where
@@ -1481,17 +1502,7 @@ def propagate(w: Wfr, elements, props, after=None):
                     abs(pzm - 1.) > tolRes or shift > 0:
                 rad_resize_gen(w, pxm, pxd, pzm, pzd, shift, _pp(pp, 10, 0.), _pp(pp, 11, 0.),
                                other_side=bool(int(_pp(pp, 4, 0))))
-        kind = el[0]
-        if kind == 'drift':
-            drift(w, el[1], el[2], anal)
-        elif kind == 'lens':
-            lens(w, el[1], el[2], el[3], el[4])
-        elif kind == 'aperture':
-            aperture(w, el[1], el[2], el[3], el[4], el[5], el[6])
-        elif kind == 'transmission':
-            transmission(w, *el[1:])
-        else:
-            raise ValueError("UNKNOWN_OPTICAL_ELEMENT")
+        _element(w, el, anal)
         if after is not None:
             after(i, w)
     n = len(elements)

@@ -325,6 +325,25 @@ public:
 // ================================================================================================
 // SRWLOptC parsing (srTCompositeOptElem ctor, cpp/src/core/sroptcnt.cpp:87-221)
 // ================================================================================================
+// the propagation parameter list of entry i of a container (srTRadResize defaults when it has none)
+static PropDesc prop_desc(const SRWLOptC* opt, int i)
+{
+    PropDesc pd;
+    pd.n = 0;
+    for (int k = 0; k < 17; k++) pd.pp[k] = 0;
+    pd.pp[2] = 1.; pd.pp[5] = pd.pp[6] = pd.pp[7] = pd.pp[8] = 1.;
+    if (i < opt->nProp && opt->arProp[i] != nullptr) {
+        int n = 9;
+        if (opt->arPropN != nullptr) n = opt->arPropN[i];
+        if (n > 17) n = 17;
+        for (int k = 0; k < n; k++) pd.pp[k] = opt->arProp[i][k];
+        pd.n = n;
+    } else {
+        pd.n = -1;   // default instruction: no resize
+    }
+    return pd;
+}
+
 int Planner::flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vector<PropDesc>& props, bool nested)
 {
     if (opt == nullptr || opt->nElem <= 0 || opt->arOpt == nullptr || opt->arOptTypes == nullptr)
@@ -367,39 +386,40 @@ int Planner::flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vecto
                 e.tr = (int)trTables_.size();
                 trTables_.emplace_back(tr->arTr, tr->arTr + 2 * (size_t)e.trNx * e.trNz);
             } else if (strcmp(t, "container") == 0) {
-                // a nested container is one element of the outer chain; its own propagation
-                // parameters apply inside it (sroptcnt.cpp:171)
+                // a nested container is one element of the outer chain (sroptcnt.cpp:171): the outer
+                // chain's pre-resize for it comes first, then every element inside it (nested
+                // containers included) propagates with the outer entry's parameters, its own lists
+                // unused (srTCompositeOptElem::PropagateRadiation, sroptcnt.h:52-76)
                 std::vector<ElemDesc> sub;
                 std::vector<PropDesc> subp;
                 int r = flatten((const SRWLOptC*)p, sub, subp, true);
                 if (r) return r;
-                (void)sub; (void)subp;
-                err = "nested SRWLOptC containers are not supported on the GPU path";
-                return SRWG_ERR_UNSUPPORTED;
+                PropDesc pd;
+                const bool withProps = opt->arProp != nullptr;
+                if (withProps) pd = prop_desc(opt, i);
+                for (size_t j = 0; j < sub.size(); j++) {
+                    sub[j].outer = i;
+                    els.push_back(sub[j]);
+                    if (withProps) {
+                        PropDesc q = pd;           // after the first: the same treatment, no resize
+                        if (j > 0) {
+                            for (int k = 5; k <= 8; k++) q.pp[k] = 1.;
+                            for (int k = 9; k <= 11; k++) q.pp[k] = 0.;
+                        }
+                        props.push_back(q);
+                    }
+                }
+                continue;
             } else {
                 err = std::string("optical element type not supported on the GPU path: ") + t;
                 return SRWG_ERR_UNSUPPORTED;
             }
+            e.outer = i;
             els.push_back(e);
             isElem = true;
         }
     props_only:
-        if (opt->arProp != nullptr && (isElem || i == opt->nElem)) {
-            PropDesc pd;
-            pd.n = 0;
-            for (int k = 0; k < 17; k++) pd.pp[k] = 0;
-            pd.pp[2] = 1.; pd.pp[5] = pd.pp[6] = pd.pp[7] = pd.pp[8] = 1.;
-            if (i < opt->nProp && opt->arProp[i] != nullptr) {
-                int n = 9;
-                if (opt->arPropN != nullptr) n = opt->arPropN[i];
-                if (n > 17) n = 17;
-                for (int k = 0; k < n; k++) pd.pp[k] = opt->arProp[i][k];
-                pd.n = n;
-            } else {
-                pd.n = -1;   // default instruction: no resize
-            }
-            props.push_back(pd);
-        }
+        if (opt->arProp != nullptr && (isElem || i == opt->nElem)) props.push_back(prop_desc(opt, i));
     }
     (void)nested;
     return 0;
@@ -1546,7 +1566,8 @@ int Planner::run()
             else if (e.kind == E_LENS) lens(e);
             else if (e.kind == E_APERTURE) aperture(e);
             else if (e.kind == E_TRANSM) transmission(e);
-            if (!intReqs.empty()) extract_after((int)i);
+            // extractions after a top-level element: after the last element of a nested container
+            if (!intReqs.empty() && (i + 1 == els.size() || els[i + 1].outer != e.outer)) extract_after(e.outer);
         }
         if (i < numRes) {
             const PropDesc& p = props[i];
@@ -1558,7 +1579,7 @@ int Planner::run()
                     if (rr) throw rr;
                 }
             }
-            if (!intReqs.empty()) extract_after((int)els.size());   // after the post-resize (sroptcnt.cpp:421)
+            if (!intReqs.empty()) extract_after(els.empty() ? 0 : els.back().outer + 1);   // after the post-resize (sroptcnt.cpp:421)
         }
     } catch (int code) {
         if (code != SRWG_NEED_STAGE) {

@@ -60,6 +60,7 @@ struct ElemDesc {
     char shape = 'r', apob = 'a'; double Dx = 0, Dy = 0;    // aperture / obstacle
     double Fx = 0, Fy = 0;                                  // lens, transmission
     double x = 0, y = 0;                                    // centre
+    int outer = 0;                                          // index in the top-level container
     int tr = -1;                                            // transmission: index of its table copy
     int trNx = 0, trNz = 0, extTr = 0;
     double trXs = 0, trXf = 0, trZs = 0, trZf = 0;

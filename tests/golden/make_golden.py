@@ -102,6 +102,8 @@ def build_beamline(L, elems):
         elif e[0] == 'transmission':
             tr, nx, ny, rx, ry, x, y, ext, Fx, Fy = e[1:]
             opts.append(L.SRWLOptT(nx, ny, rx, ry, array('d', np.asarray(tr, np.float64).tobytes()), ext, Fx, Fy, x, y))
+        elif e[0] == 'container':
+            opts.append(L.SRWLOptC(build_beamline(L, e[1]), [list(map(float, p)) for p in e[2]]))
     return opts
 
 
@@ -198,6 +200,17 @@ def cases(L):
                                                                       seed=1),
                                              40, 40, 0.1e-3, 0.1e-3, 0., 0., 1, 200., 200.), ('drift', 12., 0)],
          [pp(), pp(4)]),
+        # nested containers: the outer entry's pre-resize before the container, its treatment for every
+        # element inside (the inner lists, here with resizes and other drift modes, are not used);
+        # a container inside a container
+        ('nested_c0', g0(64), [('drift', 10., 0),
+                               ('container', [('aperture', 'r', 'a', 1e-3, 1e-3, 0., 0.), ('lens', 5., 5., 0., 0.)],
+                                [pp(0, 2., 2., 2., 2.), pp(3)]),
+                               ('drift', 5., 0)], [pp(), pp(0, 1.25, 1.5, 1.25, 1.5), pp()]),
+        ('nested_deep_quad', g2(96, 0.5e-3), [('container', [('drift', 10., 0),
+                                                              ('container', [('lens', 15., 15., 0., 0.),
+                                                                             ('drift', 20., 0)], [pp(0), pp(0)])],
+                                               [pp(0), pp(0)])], [pp(2)]),
         ('tr_aligned_lens', g0(64), [('transmission', tr_table(64, 64, 2e-3, 2e-3, 0., 0., 1e23, amp=0.1,
                                                                ripple=2e-10, seed=2),
                                       64, 64, 2e-3, 2e-3, 0., 0., 0, 1e23, 1e23), ('lens', 5., 5., 0., 0.),
@@ -346,6 +359,11 @@ def main():
          [(1, 6, 0), (2, 0, 5), (3, 6, 5), (3, 1, 6), (4, 2, 0), (5, 6, 0)]),
         ('x_c1', lambda: undulator_wfr(L, 64, 64, npTraj=4000), c1, c1pp,
          [(1, 6, 0), (2, -1, 0), (3, 6, 0), (3, 0, 6)]),
+        # after a nested container (one element of the outer chain)
+        ('x_nested', lambda: gaussian_wfr(L, 1000., 50e-6, 64, 64, 1e-3, 1e-3),
+         [('drift', 10., 0), ('container', [('aperture', 'r', 'a', 1e-3, 1e-3, 0., 0.), ('lens', 5., 5., 0., 0.)],
+                              [pp(), pp()]), ('drift', 5., 0)], [pp(), pp(0, 1.25, 1.5, 1.25, 1.5), pp()],
+         [(2, 6, 0), (3, 1, 5)]),
     ]
     xidx = []
     for xname, make, elems, pps, reqs in xcases:

@@ -69,7 +69,7 @@ def moment_err(a, b):
 # aperture clips the beam, an obstacle, a pp[3]=1 estimate without usable moments): compared to
 # the round-off of each moment's scale
 MOMENT_RECOMPUTED = {'c0_64', 'c0_128', 'c0_ragged_96x80', 'ob_circ_lens_offc', 'rect_ob_towaist', 'quad1_clip',
-                     'quad1_nomom', 'bpx_clip'}
+                     'quad1_nomom', 'bpx_clip', 'nested_c0'}
 
 # cases whose plan depends on moments measured from the field (pp[3]=1 radius estimate on
 # recomputed moments): the device-resident plan API refuses them, the drop-in plans in stages, and

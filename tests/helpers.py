@@ -45,6 +45,8 @@ def beamline(elements, props):
         elif e[0] == 'transmission':
             tr, nx, ny, rx, ry, x, y, ext, Fx, Fy = e[1:]
             opts.append(SRWLOptT(nx, ny, rx, ry, np.ascontiguousarray(tr, np.float64), ext, Fx, Fy, x, y))
+        elif e[0] == 'container':
+            opts.append(beamline(e[1], e[2]))
         else:
             opts.append(SRWLOptA(*e[1:]))
     return SRWLOptC(opts, [list(p) for p in props])

@@ -151,11 +151,13 @@ SRWG_API int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char**
 SRWG_API int srwlCalcElecFieldGaussian(SRWLWfr* pWfr, SRWLGsnBm* pGsnBm, double* precPar);
 
 /* Replaces srwlCalcIntFromElecField (cpp/src/lib/srwlib.h:748, srwlib.cpp:757) for wavefronts at a
- * single photon energy (ne == 1) vs x and y (depType 3): intType 0 (single-electron intensity),
- * 4 (phase; pInt holds doubles), 5 (Re E), 6 (Im E); pol 0..6 and the Stokes components -1..-4
- * (-5: all four, one array after the other, intensity only).  arMeth[0] = 1 averages into pInt
- * with arMeth[1] earlier iterations, 2 adds to it; NULL writes it.  Computed on the GPU (arParGPU
- * as for srwlPropagElecField); other intensity types, dependences and pFldTrj return error 23900. */
+ * single photon energy (ne == 1) vs x and y (depType 3), vs x at y (1), vs y at x (2) or at the point
+ * (x, y) (0; the cuts and the point interpolated between the neighbouring nodes as the reference's
+ * 1D extractions do): intType 0 (single-electron intensity), 4 (phase; pInt holds doubles), 5 (Re E),
+ * 6 (Im E); pol 0..6 and the Stokes components -1..-4 (-5: all four, one array after the other,
+ * intensity only).  Vs x and y, arMeth[0] = 1 averages into pInt with arMeth[1] earlier iterations, 2
+ * adds to it; NULL writes it.  Computed on the GPU (arParGPU as for srwlPropagElecField); other
+ * intensity types, dependences and pFldTrj return error 23900. */
 SRWG_API int srwlCalcIntFromElecField(char* pInt, SRWLWfr* pWfr, char pol, char intType, char depType, double e,
                                       double x, double y, double* arMeth, void* pFldTrj, double* arParGPU);
 

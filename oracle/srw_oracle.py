@@ -1733,6 +1733,57 @@ def calc_int_from_elec_field(ex, ey, pol, int_type, meth=None, prev=None):
     return (prev + res).astype(np.float32)
 
 
+def _setup_int_coord(start, step, n, arg):
+    """SetupIntCoord (srradmnp.cpp:35): node below arg (truncation toward zero), the next node, and
+    the relative distance from the first, clamped to the mesh ends."""
+    if n <= 1:
+        return 0, 0, 0.
+    inv = 1. / step
+    i0 = int((arg - start) * inv)
+    if i0 < 0:
+        i0 = i1 = 0
+    elif i0 >= n - 1:
+        i0 = i1 = n - 1
+    else:
+        i1 = i0 + 1
+    return i0, i1, inv * (arg - i0 * step - start)
+
+
+def calc_int_cut(ex, ey, mesh, pol, int_type, dep, x, y):
+    """srwlCalcIntFromElecField for ne == 1 vs x at y (dep 1), vs y at x (dep 2) or at the point (x, y)
+    (dep 0): ExtractSingleElecIntensity1DvsX / 1DvsZ / 1DvsE (srradmnp.cpp:224-680), each value
+    IntensityComponentSimpleInterpol2D (srradmnp.h:353) of the four corners around it, FP32
+    differences and FP64 weights; the phase takes the first corner."""
+    f32, f64 = np.float32, np.float64
+    what = {0: 0, 4: 2, 5: 3, 6: 6}[int_type]
+    nz, nx = ex.shape
+    xStep = (mesh['xFin'] - mesh['xStart']) / (nx - 1) if nx > 1 else 0.
+    zStep = (mesh['yFin'] - mesh['yStart']) / (nz - 1) if nz > 1 else 0.
+    x0, x1, ax = _setup_int_coord(mesh['xStart'], xStep, nx, x)
+    z0, z1, az = _setup_int_coord(mesh['yStart'], zStep, nz, y)
+    out = []
+    for p in ([-1, -2, -3, -4] if pol == -5 else [pol]):
+        I = np.asarray(intensity_component(ex, ey, p, what))
+        if dep == 0:
+            c = (I[z0, x0], I[z0, x1], I[z1, x0], I[z1, x1])
+            a1, a2 = ax, az
+        elif dep == 1:
+            c = (I[z0, :], I[z0, :], I[z1, :], I[z1, :])
+            a1, a2 = 0., az
+        else:
+            c = (I[:, x0], I[:, x0], I[:, x1], I[:, x1])
+            a1, a2 = 0., ax
+        I00, I10, I01, I11 = [np.atleast_1d(v) for v in c]
+        if what == 2:
+            out.append(I00.astype(f64))
+            continue
+        I00, I10, I01, I11 = [v.astype(f32) for v in (I00, I10, I01, I11)]
+        t = ((I00 - I01) - I10) + I11
+        r = t.astype(f64) * (a1 * a2) + (I10 - I00).astype(f64) * a1 + (I01 - I00).astype(f64) * a2 + I00.astype(f64)
+        out.append(r.astype(f32))
+    return np.concatenate(out)
+
+
 def add_interp_bilinear(acc, acc_mesh, I, mesh):
     """acc += I interpolated on acc_mesh: SRWLStokes.avg_update_interp with _ord=1 and _sum=True
     (env/python/srwpy/srwlib.py:1116-1203; points outside the mesh add nothing)."""

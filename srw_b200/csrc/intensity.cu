@@ -46,6 +46,57 @@ __global__ void __launch_bounds__(256) intensity_kernel(const float2* __restrict
     }
 }
 
+// 1D cuts and the single point (dependences 1: vs x at y, 2: vs y at x, 0: at (x, y)) of a wavefront
+// with ne == 1: ExtractSingleElecIntensity1DvsX / 1DvsZ / 1DvsE (srradmnp.cpp:224-680) reduce to
+// IntensityComponentSimpleInterpol2D (srradmnp.h:353) on two lines L0, L1 of the field (rows z0, z1
+// for the x cut and the point, columns x0, x1 for the y cut), with the reference's FP32 differences
+// and FP64 weights; the phase takes the first corner.  k0, k1: the corners' positions along the lines
+// for the point (dep 0); the cuts take position p of both lines.
+__global__ void __launch_bounds__(256) cut_kernel(const float2* __restrict__ ex, const float2* __restrict__ ez,
+                                                  int nLine, int nOut, int dep, int k0, int k1, double a1, double a2,
+                                                  int pol, int what, float* outF, double* outD)
+{
+    const int np = pol == -5 ? 4 : 1;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < nOut; p += gridDim.x * blockDim.x) {
+        const int i0 = dep == 0 ? k0 : p, i1 = dep == 0 ? k1 : p;
+        const float2 x00 = ex[i0], x10 = ex[i1], x01 = ex[nLine + i0], x11 = ex[nLine + i1];
+        const float2 z00 = ez[i0], z10 = ez[i1], z01 = ez[nLine + i0], z11 = ez[nLine + i1];
+        for (int k = 0; k < np; k++) {
+            const int pc = np == 4 ? -1 - k : pol;
+            const float I00 = int_component(x00, z00, pc, what);
+            double r;
+            if (what == 2) {
+                r = (double)I00;
+            } else {
+                const float I10 = int_component(x10, z10, pc, what), I01 = int_component(x01, z01, pc, what);
+                const float I11 = int_component(x11, z11, pc, what);
+                const float t = __fadd_rn(__fsub_rn(__fsub_rn(I00, I01), I10), I11);
+                r = __dmul_rn((double)t, __dmul_rn(a1, a2));
+                r = __dadd_rn(r, __dmul_rn((double)__fsub_rn(I10, I00), a1));
+                r = __dadd_rn(r, __dmul_rn((double)__fsub_rn(I01, I00), a2));
+                r = (double)(float)__dadd_rn(r, (double)I00);
+            }
+            const long long o = p + (long long)k * nOut;
+            if (outD) outD[o] = r;
+            else outF[o] = (float)r;
+        }
+    }
+}
+
+// SetupIntCoord (srradmnp.cpp:35): the node below arg (truncation), the next one, and the relative
+// distance from the first (FP64, the reference's operation order)
+static void setup_int_coord(double start, double step, long long n, double arg, long long& i0, long long& i1,
+                            double& rel)
+{
+    if (n <= 1) { i0 = i1 = 0; rel = 0.; return; }
+    const double inv = 1. / step;
+    i0 = (long)((arg - start) * inv);
+    if (i0 < 0) { i0 = 0; i1 = i0; }
+    else if (i0 >= n - 1) { i0 = n - 1; i1 = i0; }
+    else i1 = i0 + 1;
+    rel = inv * (arg - i0 * step - start);
+}
+
 // intensity extraction pass of a propagation (srTCompositeOptElem::ExtractPropagatedIntensity,
 // cpp/src/core/sroptcnt.cpp:429, writing as srwlCalcIntFromElecField does): the field at an element
 // boundary is the source buffer times the operators still pending on it (separable tables and the
@@ -99,6 +150,60 @@ using namespace srwg;
         }                                                                               \
     } while (0)
 
+// dependences 0, 1, 2: the two field lines the result needs go to the device (rows: contiguous;
+// columns: strided copies), one kernel makes the cut, which comes back (written, as the reference's
+// 1D extractions do: no averaging)
+static int int_cut(DeviceCtx* c, char* pInt, const SRWLWfr* pWfr, char pol, int what, int dep, double x, double y)
+{
+    const long long nx = pWfr->mesh.nx, nz = pWfr->mesh.ny;
+    const double xStep = nx > 1 ? (pWfr->mesh.xFin - pWfr->mesh.xStart) / (nx - 1) : 0.;
+    const double zStep = nz > 1 ? (pWfr->mesh.yFin - pWfr->mesh.yStart) / (nz - 1) : 0.;
+    long long x0, x1, z0, z1;
+    double ax, az;
+    setup_int_coord(pWfr->mesh.xStart, xStep, nx, x, x0, x1, ax);
+    setup_int_coord(pWfr->mesh.yStart, zStep, nz, y, z0, z1, az);
+    const bool cols = dep == 2;
+    const long long nLine = cols ? nz : nx;
+    const int nOut = dep == 0 ? 1 : (int)nLine;
+    const int np = pol == -5 ? 4 : 1;
+    const size_t esz = what == 2 ? sizeof(double) : sizeof(float);
+    const size_t bytes = 4 * nLine * sizeof(float2) + (size_t)np * nOut * esz;
+    if (c->intBuf == nullptr || c->intBytes < bytes) {
+        if (c->intBuf) cudaFree(c->intBuf);
+        c->intBuf = nullptr; c->intBytes = 0;
+        INT_TRY(cudaMalloc(&c->intBuf, bytes));
+        c->intBytes = bytes;
+    }
+    float2* dX = (float2*)c->intBuf;
+    float2* dZ = dX + 2 * nLine;
+    char* dOut = (char*)(dZ + 2 * nLine);
+    cudaStream_t st = c->stream;
+    const float2* src[2] = {(const float2*)pWfr->arEx, (const float2*)pWfr->arEy};
+    float2* dst[2] = {dX, dZ};
+    for (int comp = 0; comp < 2; comp++) {
+        for (int l = 0; l < 2; l++) {
+            float2* d = dst[comp] + l * nLine;
+            if (src[comp] == nullptr) { INT_TRY(cudaMemsetAsync(d, 0, nLine * sizeof(float2), st)); continue; }
+            if (cols) {
+                const long long ix = l == 0 ? x0 : x1;
+                INT_TRY(cudaMemcpy2DAsync(d, sizeof(float2), src[comp] + ix, nx * sizeof(float2), sizeof(float2), nz,
+                                          cudaMemcpyHostToDevice, st));
+            } else {
+                const long long iz = l == 0 ? z0 : z1;
+                INT_TRY(cudaMemcpyAsync(d, src[comp] + iz * nx, nx * sizeof(float2), cudaMemcpyHostToDevice, st));
+            }
+        }
+    }
+    const double a1 = dep == 0 ? ax : 0., a2 = dep == 0 ? az : (cols ? ax : az);
+    cut_kernel<<<(nOut + 255) / 256, 256, 0, st>>>(dX, dZ, (int)nLine, nOut, dep, (int)x0, (int)x1, a1, a2, (int)pol,
+                                                   what, what == 2 ? nullptr : (float*)dOut,
+                                                   what == 2 ? (double*)dOut : nullptr);
+    INT_TRY(cudaGetLastError());
+    INT_TRY(cudaMemcpyAsync(pInt, dOut, (size_t)np * nOut * esz, cudaMemcpyDeviceToHost, st));
+    INT_TRY(cudaStreamSynchronize(st));
+    return 0;
+}
+
 extern "C" SRWG_API int srwlCalcIntFromElecField(char* pInt, SRWLWfr* pWfr, char pol, char intType, char depType,
                                                  double e, double x, double y, double* arMeth, void* pFldTrj,
                                                  double* arParGPU)
@@ -112,7 +217,10 @@ extern "C" SRWG_API int srwlCalcIntFromElecField(char* pInt, SRWLWfr* pWfr, char
         return SRWG_ERR_UNSUPPORTED;
     }
     if (pWfr->mesh.ne != 1) { set_last_detail("intensity extraction for ne == 1 only"); return SRWG_ERR_UNSUPPORTED; }
-    if (depType != 3) { set_last_detail("intensity extraction vs x and y (depType 3) only"); return SRWG_ERR_UNSUPPORTED; }
+    if (depType < 0 || depType > 3) {
+        set_last_detail("intensity extraction vs x and y (depType 3), x (1), y (2) or at one point (0) only");
+        return SRWG_ERR_UNSUPPORTED;
+    }
     int what;
     switch (intType) {           // SRWL numbering -> the reference's internal one (srwlib.cpp:792)
     case 0: what = 0; break;
@@ -140,6 +248,7 @@ extern "C" SRWG_API int srwlCalcIntFromElecField(char* pInt, SRWLWfr* pWfr, char
     if (r) return r;
     const long long n = (long long)pWfr->mesh.nx * pWfr->mesh.ny;
     if (n <= 0) return SRWL_INCORRECT_PARAM_FOR_INT_EXTR;
+    if (depType != 3) return int_cut(c, pInt, pWfr, pol, what, depType, x, y);
     const long long nOut = n * (pol == -5 ? 4 : 1);
     const size_t esz = what == 2 ? sizeof(double) : sizeof(float);
     const size_t bytes = 2 * n * sizeof(float2) + nOut * esz;

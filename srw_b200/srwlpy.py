@@ -347,7 +347,8 @@ def PropagElecField(wfr, optC, intList=None, dev=None):
 def CalcIntFromElecField(arI, wfr, pol, intType, depType, e, x, y, meth=None, fldTrj=None, dev=None):
     """srwlpy.CalcIntFromElecField (cpp/src/clients/python/srwlpy.cpp:4873): fills ``arI`` (array('f')
     or a float32 numpy array; float64 for the phase, intType 4) with the intensity of ``wfr`` vs x and
-    y, on the GPU.  ``meth``: [1, n] averages into arI over n earlier iterations, [2] adds to it."""
+    y (depType 3), vs x at y (1), vs y at x (2) or at the point (x, y) (0), on the GPU.  ``meth`` (vs x
+    and y): [1, n] averages into arI over n earlier iterations, [2] adds to it."""
     if fldTrj is not None:
         raise RuntimeError('intensity with the central electron field/trajectory is not supported on the GPU path')
     keep = []

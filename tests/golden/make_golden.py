@@ -302,6 +302,27 @@ def main():
                 blob[key] = np.array(arI, np.float64 if it == 4 else np.float32)
                 ints.append(dict(key=key, int_type=it, pol=pol, meth=meth))
     blob['int/index'] = np.array(json.dumps(ints))
+    # 3b) cuts vs x at y (dep 1), vs y at x (dep 2) and single points (dep 0): positions between nodes,
+    #     on a node, within a step below the mesh start (extrapolation) and beyond the mesh end
+    m = wsrc.mesh
+    xs, ys = (m.xFin - m.xStart) / (nx - 1), (m.yFin - m.yStart) / (ny - 1)
+    pos = [(m.xStart + 17.3 * xs, m.yStart + 40.6 * ys), (m.xStart + 31 * xs, m.yStart + 12 * ys),
+           (m.xStart - 0.4 * xs, m.yStart - 0.7 * ys), (m.xFin + 2.5 * xs, m.yFin + 0.5 * ys)]
+    cuts = []
+    for it in (0, 4, 5, 6):
+        for pol in (0, 1, 2, 3, 4, 5, 6, -1, -2, -3, -4, -5):
+            if pol < 0 and it != 0:
+                continue
+            for dep in (0, 1, 2):
+                for k, (x, y) in enumerate(pos):
+                    n = {0: 1, 1: nx, 2: ny}[dep] * (4 if pol == -5 else 1)
+                    code = 'd' if it == 4 else 'f'
+                    arI = array(code, [0.] * n)
+                    L.srwl.CalcIntFromElecField(arI, wsrc, pol, it, dep, wsrc.mesh.eStart, x, y)
+                    key = 'icut/%d/%d/%d/%d' % (it, pol, dep, k)
+                    blob[key] = np.array(arI, np.float64 if it == 4 else np.float32)
+                    cuts.append(dict(key=key, int_type=it, pol=pol, dep=dep, x=x, y=y))
+    blob['icut/index'] = np.array(json.dumps(cuts))
     # 4) Gaussian beams (srwlCalcElecFieldGaussian, precPar = [0]): waist at the observation plane,
     #    offsets / angles / Hermite modes / every polarisation, field units, spectral detuning
     gcases = [

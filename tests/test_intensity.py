@@ -63,3 +63,39 @@ def test_gpu_matches_reference_vectors():
         arI = prev(c).copy()
         srwl.CalcIntFromElecField(arI, w, c['pol'], c['int_type'], 3, w.mesh.eStart, 0., 0., c['meth'])
         check(arI, c)
+
+
+CUTS = json.loads(str(D['icut/index']))
+
+
+def mesh():
+    return dict(xStart=float(M[2]), xFin=float(M[3]), yStart=float(M[4]), yFin=float(M[5]))
+
+
+def test_oracle_cuts_match_reference_vectors():
+    """Cuts vs x (dep 1) and vs y (dep 2) and single points (dep 0), between nodes, on a node, below
+    the mesh start and beyond its end: bit-exact (phase: to the FP32 step)."""
+    assert len(CUTS) == 396
+    ex, ey = fields()
+    for c in CUTS:
+        check(O.calc_int_cut(ex, ey, mesh(), c['pol'], c['int_type'], c['dep'], c['x'], c['y']), c)
+
+
+@pytest.mark.gpu
+def test_gpu_cuts_match_reference_vectors():
+    torch = pytest.importorskip('torch')
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from srw_b200 import srwlpy as srwl
+    from srw_b200.srwlib import SRWLWfr
+    w = SRWLWfr()
+    w.allocate(1, NX, NY)
+    w.arEx = np.array(D['int/ex'], np.float32)
+    w.arEy = np.array(D['int/ey'], np.float32)
+    w.mesh.xStart, w.mesh.xFin, w.mesh.yStart, w.mesh.yFin = (float(v) for v in M[2:6])
+    w.mesh.eStart = w.mesh.eFin = float(M[6])
+    for c in CUTS:
+        n = {0: 1, 1: NX, 2: NY}[c['dep']] * (4 if c['pol'] == -5 else 1)
+        arI = np.zeros(n, np.float64 if c['int_type'] == 4 else np.float32)
+        srwl.CalcIntFromElecField(arI, w, c['pol'], c['int_type'], c['dep'], w.mesh.eStart, c['x'], c['y'])
+        check(arI, c)

@@ -791,7 +791,7 @@ def _tr_axis(v, start, step, n):
     return i, frac
 
 
-def transmission(w: Wfr, arTr, nx, nz, rx, rz, x, z, extTr, Fx, Fz):
+def transmission(w: Wfr, arTr, nx, nz, rx, rz, x, z, extTr, Fx, Fz, ne=1, eStart=0., eFin=0.):
     """srTGenTransmission: amplitude transmission T and optical path difference OPD tabulated over
     [nz][nx] (pairs, ne == 1) on the mesh of ranges rx, rz centred on (x, z) (the SRWLOptT
     constructor, srwlib.py:3071-3082), interpolated bilinearly at the wavefront's absolute
@@ -808,13 +808,26 @@ def transmission(w: Wfr, arTr, nx, nz, rx, rz, x, z, extTr, Fx, Fz):
     x = np.broadcast_to(x, (w.nz, w.nx))
     z = np.broadcast_to(z, (w.nz, w.nx))
     xStep, zStep = (xFin - xStart) / (nx - 1), (zFin - zStart) / (nz - 1)
-    tab = np.asarray(arTr, dtype=np.float64).reshape(nz, nx, 2)
     ix, xr = _tr_axis(x, xStart, xStep, nx)
     iz, zr = _tr_axis(z, zStart, zStep, nz)
-    p00, p10, p01, p11 = tab[iz, ix], tab[iz, ix + 1], tab[iz + 1, ix], tab[iz + 1, ix + 1]
-    a_xz = p00 - p01 - p10 + p11
-    a_x, a_z = p10 - p00, p01 - p00
-    v = a_xz * (xr * zr)[..., None] + a_x * xr[..., None] + a_z * zr[..., None] + p00
+    if ne == 1:
+        tab = np.asarray(arTr, dtype=np.float64).reshape(nz, nx, 2)
+        p00, p10, p01, p11 = tab[iz, ix], tab[iz, ix + 1], tab[iz + 1, ix], tab[iz + 1, ix + 1]
+        a_xz = p00 - p01 - p10 + p11
+        a_x, a_z = p10 - p00, p01 - p00
+        v = a_xz * (xr * zr)[..., None] + a_x * xr[..., None] + a_z * zr[..., None] + p00
+    else:
+        # trilinear in (e, x, z) over [nz][nx][ne] pairs (sroptgtr.h:275-300)
+        tab = np.asarray(arTr, dtype=np.float64).reshape(nz, nx, ne, 2)
+        eStep = (eFin - eStart) / (ne - 1)
+        ie = min(max(int((w.eStart - eStart) / eStep + 1.e-10), 0), ne - 2)
+        er = (w.eStart - (ie * eStep + eStart)) / eStep
+        c = lambda a, b, k: tab[iz + b, ix + a, ie + k]      # noqa: E731  (x offset a, z offset b, e offset k)
+        xr_, zr_ = xr[..., None], zr[..., None]
+        v = ((c(0, 0, 0) * ((1. - er) * (1. - xr_)) + c(0, 0, 1) * (er * (1. - xr_)) + c(1, 0, 0) * ((1. - er) * xr_)
+              + c(1, 0, 1) * (er * xr_)) * (1. - zr_)
+             + (c(0, 1, 0) * ((1. - er) * (1. - xr_)) + c(0, 1, 1) * (er * (1. - xr_)) + c(1, 1, 0) * ((1. - er) * xr_)
+                + c(1, 1, 1) * (er * xr_)) * zr_)
     T, Ph = v[..., 0], v[..., 1] * (w.eStart * 5.0676816042E+06)
     fac = T * np.exp(1j * Ph)
     if extTr == 0:

@@ -373,10 +373,7 @@ int Planner::flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vecto
                 // mesh, centre = the mesh's centre, estimated focal lengths for the bookkeeping
                 const SRWLOptT* tr = (const SRWLOptT*)p;
                 if (tr->arTr == nullptr || tr->mesh.nx < 2 || tr->mesh.ny < 2) return UNKNOWN_OPTICAL_ELEMENT;
-                if (tr->mesh.ne != 1) {
-                    err = "transmission tables vs photon energy (ne > 1) are not supported on the GPU path";
-                    return SRWG_ERR_UNSUPPORTED;
-                }
+                if (tr->mesh.ne < 1) return UNKNOWN_OPTICAL_ELEMENT;
                 e.kind = E_TRANSM;
                 e.Fx = tr->Fx; e.Fy = tr->Fy;
                 e.x = 0.5 * (tr->mesh.xStart + tr->mesh.xFin);
@@ -384,7 +381,27 @@ int Planner::flatten(const SRWLOptC* opt, std::vector<ElemDesc>& els, std::vecto
                 e.trNx = (int)tr->mesh.nx; e.trNz = (int)tr->mesh.ny; e.extTr = tr->extTr;
                 e.trXs = tr->mesh.xStart; e.trXf = tr->mesh.xFin; e.trZs = tr->mesh.yStart; e.trZf = tr->mesh.yFin;
                 e.tr = (int)trTables_.size();
-                trTables_.emplace_back(tr->arTr, tr->arTr + 2 * (size_t)e.trNx * e.trNz);
+                if (tr->mesh.ne == 1) {
+                    trTables_.emplace_back(tr->arTr, tr->arTr + 2 * (size_t)e.trNx * e.trNz);
+                } else {
+                    // a table vs photon energy ([ny][nx][ne] pairs): linear in e at the wavefront's
+                    // photon energy (the e part of the trilinear lookup, sroptgtr.h:275-300: cell by
+                    // truncation with 1e-10, clamped to the last cell, extrapolating outside), then
+                    // the (x, z) lookup of a single-energy table
+                    const long long Ne = tr->mesh.ne;
+                    const double eS = tr->mesh.eStart, eSt = (tr->mesh.eFin - tr->mesh.eStart) / (Ne - 1);
+                    long long ie = (long long)((w.eStart - eS) / eSt + 1.e-10);
+                    if (ie < 0) ie = 0;
+                    else if (ie > Ne - 2) ie = Ne - 2;
+                    const double er = (w.eStart - (ie * eSt + eS)) / eSt;
+                    std::vector<double> t(2 * (size_t)e.trNx * e.trNz);
+                    for (size_t q = 0; q < (size_t)e.trNx * e.trNz; q++)
+                        for (int c2 = 0; c2 < 2; c2++) {
+                            const double* p0 = tr->arTr + (q * Ne + ie) * 2 + c2;
+                            t[2 * q + c2] = p0[0] * (1. - er) + p0[2] * er;
+                        }
+                    trTables_.push_back(std::move(t));
+                }
             } else if (strcmp(t, "container") == 0) {
                 // a nested container is one element of the outer chain (sroptcnt.cpp:171): the outer
                 // chain's pre-resize for it comes first, then every element inside it (nested

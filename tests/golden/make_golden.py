@@ -100,11 +100,22 @@ def build_beamline(L, elems):
         elif e[0] == 'lens':
             opts.append(L.SRWLOptL(e[1], e[2], e[3], e[4]))
         elif e[0] == 'transmission':
-            tr, nx, ny, rx, ry, x, y, ext, Fx, Fy = e[1:]
-            opts.append(L.SRWLOptT(nx, ny, rx, ry, array('d', np.asarray(tr, np.float64).tobytes()), ext, Fx, Fy, x, y))
+            tr, nx, ny, rx, ry, x, y, ext, Fx, Fy = e[1:11]
+            ne, e0, e1 = (e[11:14] if len(e) > 11 else (1, 0., 0.))
+            opts.append(L.SRWLOptT(nx, ny, rx, ry, array('d', np.asarray(tr, np.float64).tobytes()), ext, Fx, Fy, x, y,
+                                   ne, e0, e1))
         elif e[0] == 'container':
             opts.append(L.SRWLOptC(build_beamline(L, e[1]), [list(map(float, p)) for p in e[2]]))
     return opts
+
+
+def tr_table_e(nx, ny, rx, ry, x, y, F, ne, e0, e1):
+    """A table vs photon energy, [ny][nx][ne] pairs: tr_table at each energy, scaled."""
+    out = np.empty((ny, nx, ne, 2))
+    for k in range(ne):
+        t = tr_table(nx, ny, rx, ry, x, y, F * (1. + 0.1 * k), ripple=2e-11 * (1. + 0.5 * k), seed=10 + k)
+        out[:, :, k, :] = t.reshape(ny, nx, 2)
+    return out.ravel()
 
 
 def tr_table(nx, ny, rx, ry, x, y, F, amp=0.3, ripple=3e-10, seed=0):
@@ -211,6 +222,11 @@ def cases(L):
                                                               ('container', [('lens', 15., 15., 0., 0.),
                                                                              ('drift', 20., 0)], [pp(0), pp(0)])],
                                                [pp(0), pp(0)])], [pp(2)]),
+        # a table vs photon energy (ne = 3, the wavefront's energy between the 2nd and 3rd)
+        ('tr_vs_energy', g2(96, 0.5e-3), [('transmission', tr_table_e(31, 27, 0.12e-3, 0.1e-3, 0., 0., 200., 3, 9000.,
+                                                                      10400.),
+                                           31, 27, 0.12e-3, 0.1e-3, 0., 0., 0, 200., 200., 3, 9000., 10400.),
+                                          ('drift', 10., 0)], [pp(), pp()]),
         ('tr_aligned_lens', g0(64), [('transmission', tr_table(64, 64, 2e-3, 2e-3, 0., 0., 1e23, amp=0.1,
                                                                ripple=2e-10, seed=2),
                                       64, 64, 2e-3, 2e-3, 0., 0., 0, 1e23, 1e23), ('lens', 5., 5., 0., 0.),

@@ -43,8 +43,9 @@ def beamline(elements, props):
         elif e[0] == 'lens':
             opts.append(SRWLOptL(*e[1:]))
         elif e[0] == 'transmission':
-            tr, nx, ny, rx, ry, x, y, ext, Fx, Fy = e[1:]
-            opts.append(SRWLOptT(nx, ny, rx, ry, np.ascontiguousarray(tr, np.float64), ext, Fx, Fy, x, y))
+            tr, nx, ny, rx, ry, x, y, ext, Fx, Fy = e[1:11]
+            ne, e0, e1 = (e[11:14] if len(e) > 11 else (1, 0., 0.))
+            opts.append(SRWLOptT(nx, ny, rx, ry, np.ascontiguousarray(tr, np.float64), ext, Fx, Fy, x, y, ne, e0, e1))
         elif e[0] == 'container':
             opts.append(beamline(e[1], e[2]))
         else:

@@ -109,6 +109,8 @@ def test_unsupported_and_invalid_inputs_raise():
     from srw_b200.srwlib import SRWLOptC, SRWLOptT
     with pytest.raises(RuntimeError, match='not supported'):
         Plan(w, SRWLOptC([SRWLOptMirEl()], [PP()]))
-    # transmission tables vs photon energy are refused by the planner
-    with pytest.raises(RuntimeError, match='ne > 1'):
-        Plan(w, SRWLOptC([SRWLOptT(8, 8, 1e-3, 1e-3, _ne=2, _eStart=1e3, _eFin=2e3)], [PP()]))
+    # a transmission table without its data is refused
+    bad = SRWLOptT(8, 8, 1e-3, 1e-3)
+    bad.arTr = None
+    with pytest.raises(RuntimeError, match='Transmission'):
+        Plan(w, SRWLOptC([bad], [PP()]))

@@ -157,3 +157,35 @@ def test_gpu_unsupported_extraction_refused():
     w = make_wfr(i['ex'], i['ey'], i['mesh'])
     with pytest.raises(RuntimeError, match='dep 3'):
         srwlpy.PropagElecField(w, beamline(c['elements'], c['props']), [[1, 6, 0, 1, 0, SRWLRadMesh()]])
+
+
+@pytest.mark.gpu
+def test_gpu_extractions_across_stages():
+    """A chain planned in stages (a pp[3]=1 drift after an aperture that recomputes the moments): the
+    extractions of every stage reach the caller, against the oracle's state after each element."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from tests.golden_cases import case_io
+    name = 'quad1_clip'
+    c = next(c for c in load()[1] if c['name'] == name)
+    i, o = case_io(D, name)
+    w = make_wfr(i['ex'], i['ey'], i['mesh'], Rx=i['Rx'], Ry=i['Ry'], dRx=i['dRx'], dRy=i['dRy'], xc=i['xc'],
+                 yc=i['yc'], momX=i['momX'], momY=i['momY'], propM=i['prop'])
+    n = len(c['elements'])
+    intList = [[k + 1, 6, 0, 3, 0, SRWLRadMesh(i['mesh']['eStart'], i['mesh']['eStart'], 1)] for k in range(n)]
+    srwlpy.PropagElecField(w, beamline(c['elements'], c['props']), intList)
+    ow = O.Wfr.from_srwl(i['ex'], i['ey'], i['mesh'], i['Rx'], i['Ry'], i['dRx'], i['dRy'], i['xc'], i['yc'], 0,
+                         i['momX'], i['momY'], propM=i['prop'])
+    states = {}
+    O.propagate(ow, [tuple(e) for e in c['elements']], c['props'],
+                after=lambda k, s: states.setdefault(k, (s.ex.copy(), s.ey.copy(), s.out_mesh())))
+    for k in range(n):
+        ex, ey, m = states[k]
+        it = intList[k]
+        assert (it[5].nx, it[5].ny) == (m['nx'], m['ny'])
+        np.testing.assert_allclose([it[5].xStart, it[5].xFin, it[5].yStart, it[5].yFin],
+                                   [m['xStart'], m['xFin'], m['yStart'], m['yFin']], rtol=1e-8)
+        I = np.abs(ex) ** 2 + np.abs(ey) ** 2
+        assert rel_l2(np.asarray(it[6], np.float64), I.ravel()) < TOL_GPU, k
+    assert rel_l2(np.asarray(w.arEx, np.float64), D[name + '/out/ex']) < TOL_GPU

@@ -41,10 +41,12 @@ METRIC = "propagations/s at 1024² FP32, batched+learned vs plain GPU at ≤1e-3
 UNIT = "propagations/s"
 WORKLOAD = ("undulator beamline: 1024x1024 complex FP32 field (2012 eV, +-1.5 mm, R=20 m) -> circular aperture "
             "0.8 mm -> resize x2 range x2 resolution (4096x4096) -> thin lens f=10 m -> drift 10 m to waist; "
-            "macro-electron wavefronts (source offsets sigma x 30 um, x' 5 urad, y 5 um, y' 2 urad) in batches")
+            "macro-electron wavefronts (source offsets sigma x 30 um, x' 5 urad, y 5 um, y' 2 urad; relative energy "
+            "spread 1e-3 as a photon-energy rescale E (1 + 2 d)) in batches")
 PEAKS = os.path.join(HERE, 'MEASURED_PEAKS.json')
 BATCH = 16                                     # macro-electron wavefronts per step
 SIG = (30e-6, 5e-6, 5e-6, 2e-6)                # source: sigma x [m], x' [rad], y [m], y' [rad]
+SIG_E = 1e-3                                   # relative electron energy spread (photon energy E (1 + 2 d))
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a pass, from an ncu
 # capture of this workload (profiles/passes_4096_c1.md); keyed by the pass tuple of Plan.kernels().
 # Re-captured whenever the kernel changes.
@@ -389,11 +391,11 @@ def measure_batched(args, dev, world, dist, factors=(2., 2.), acc=None, e2e_leg=
     torch.cuda.synchronize(dev)
     rank = int(os.environ.get('RANK', '0'))
     for k in range(args.warmup):
-        me.add(sample_offsets(BATCH, *SIG, seed=1000 + rank, first=k * BATCH), stream.cuda_stream)
+        me.add(sample_offsets(BATCH, *SIG, seed=1000 + rank, first=k * BATCH, sig_e=SIG_E), stream.cuda_stream)
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
-    offs = [sample_offsets(BATCH, *SIG, seed=rank, first=k * BATCH) for k in range(args.steps)]
+    offs = [sample_offsets(BATCH, *SIG, seed=rank, first=k * BATCH, sig_e=SIG_E) for k in range(args.steps)]
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev.index) as clk, NvmlSampler(dev) as nv:
@@ -414,7 +416,7 @@ def measure_batched(args, dev, world, dist, factors=(2., 2.), acc=None, e2e_leg=
     e2e = None
     if e2e_leg and not args.no_e2e:
         me2 = MultiE(w, bl, acc, max_batch=BATCH, graph=True, device=dev.index)
-        me2.add(sample_offsets(BATCH, *SIG, seed=77))
+        me2.add(sample_offsets(BATCH, *SIG, seed=77, sig_e=SIG_E))
         me2.mean()
         n_e2e = max(3, min(args.steps, 20))
         t0 = time.perf_counter()
@@ -422,7 +424,7 @@ def measure_batched(args, dev, world, dist, factors=(2., 2.), acc=None, e2e_leg=
             me2.add(offs[k % len(offs)])
             mean = me2.mean()
         e2e_s = time.perf_counter() - t0
-        e2e = {"value": world * n_e2e * BATCH / e2e_s, "unit": UNIT, "h2d_bytes_per_step": BATCH * 4 * 8,
+        e2e = {"value": world * n_e2e * BATCH / e2e_s, "unit": UNIT, "h2d_bytes_per_step": BATCH * 5 * 8,
                "d2h_bytes_per_step": int(mean.nbytes),
                "path": "srw_b200.multie.MultiE.add (C-ABI srwgMultiEAdd; base field resident, electron offsets "
                        "from host) + MultiE.mean (D2H of the %dx%d FP64 mean intensity)" % (acc['nx'], acc['ny'])}
@@ -459,10 +461,10 @@ def measure_mixed(args, dev, n_elec, model=None):
             bl = beamline_objs(mod, *factors)
             b = batch or {256: 32, 512: 32, 1024: 16}[n]
             me = MultiE(w, bl, acc, max_batch=b, graph=graph, device=dev.index)
-            me.add(sample_offsets(b, *SIG, seed=999))                      # warm-up (plans, graph)
+            me.add(sample_offsets(b, *SIG, seed=999, sig_e=SIG_E))                      # warm-up (plans, graph)
             me.reset()
             cnt = n_elec // 3
-            offs = sample_offsets(cnt, *SIG, seed=5, first=cls * cnt)
+            offs = sample_offsets(cnt, *SIG, seed=5, first=cls * cnt, sig_e=SIG_E)
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
             me.add(offs)

@@ -236,6 +236,9 @@ typedef struct srwgMultiE srwgMultiE;
 SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* pOpt, const SRWLRadMesh* pAccMesh, int maxBatch,
                               int useGraph, int device, srwgMultiE** out);
 SRWG_API int srwgMultiEAdd(srwgMultiE* m, int n, const double* arOffsets, void* stream);
+/* as srwgMultiEAdd with 5 doubles per electron: the fifth is the relative energy deviation d of the
+ * electron, which rescales the photon energy of its wavefront to E (1 + 2 d) */
+SRWG_API int srwgMultiEAddE(srwgMultiE* m, int n, const double* arOffsets, void* stream);
 SRWG_API int srwgMultiEGetMean(srwgMultiE* m, double* arMean, long long* nElec, void* stream);
 /* device address of the FP64 intensity sum (pAccMesh ny x nx) and the electron count, e.g. for a
  * sum over ranks; srwgMultiESetAccumulator makes the object add into caller-owned device memory */

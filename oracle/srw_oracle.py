@@ -1534,12 +1534,16 @@ def propagate(w: Wfr, elements, props, after=None):
 # ----------------------------------------------------------------------------------------
 
 
-def electron_offset(ex, ey, mesh, sc, dx0, dxp, dy0, dyp):
+def electron_offset(ex, ey, mesh, sc, dx0, dxp, dy0, dyp, de=0.):
     """SRWLWfr.sim_src_offset with _move_mesh=True (env/python/srwpy/srwlib.py:2803-2849): the kick
     of srTOptAngle::RadPointModifier (cpp/src/core/sroptang.h:64-79; phase 5.06773065e6 e (x' x + y' z)
     in FP64 on the unshifted mesh, field stored back as FP32), then the mesh moved by
     (x + x' R, y + y' R), R = (Rx + Ry)/2, and xc += x, yc += y.  Returns (ex, ey, mesh, sc)."""
     ny, nx = ex.shape
+    if de != 0.:        # photon energy of the electron's wavefront: E (1 + 2 de) (undulator harmonic shift)
+        mesh = dict(mesh)
+        mesh['eStart'] = mesh['eStart'] * (1. + 2. * de)
+        mesh['eFin'] = mesh['eStart']
     xStep = (mesh['xFin'] - mesh['xStart']) / (nx - 1)
     zStep = (mesh['yFin'] - mesh['yStart']) / (ny - 1)
     x = mesh['xStart'] + np.arange(nx) * xStep

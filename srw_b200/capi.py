@@ -95,6 +95,7 @@ SYMBOLS = {
     'srwgMultiECreate': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.POINTER(SRWLRadMesh), C.c_int, C.c_int,
                                    C.c_int, C.POINTER(C.c_void_p)]),
     'srwgMultiEAdd': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    'srwgMultiEAddE': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     'srwgMultiEGetMean': (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong), C.c_void_p]),
     'srwgMultiEAccumulator': (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)]),
     'srwgMultiESetAccumulator': (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -158,15 +158,20 @@ namespace srwg {
 
 // the electron's wavefront description: kicked on the base mesh, then the mesh moved
 // (SRWLWfr.sim_src_offset with _move_mesh=True, srwlib.py:2803-2849; srTOptAngle moments, sroptang.h:81)
-static void electron_wfr(const srwgMultiE& m, const double* off, SRWLWfr& w, double* momX, double* momY,
+// With a fifth value (relative electron energy deviation d), the photon energy of the electron's
+// wavefront is rescaled to E (1 + 2 d), the shift of an undulator harmonic with the electron energy.
+static void electron_wfr(const srwgMultiE& m, const double* off, int stride, SRWLWfr& w, double* momX, double* momY,
                          ElecParams& ep)
 {
     const double dx0 = off[0], dxp = off[1], dy0 = off[2], dyp = off[3];
+    const double de = stride > 4 ? off[4] : 0.;
     w = m.base;
     for (int i = 0; i < 11; i++) { momX[i] = m.momX[i]; momY[i] = m.momY[i]; }
     w.arMomX = momX;
     w.arMomY = momY;
-    const double twoPiDLambda = 5.06773065e+06 * m.eStart;
+    const double E = de != 0. ? m.eStart * (1. + 2. * de) : m.eStart;
+    if (de != 0.) { w.mesh.eStart = E; w.mesh.eFin = E; }
+    const double twoPiDLambda = 5.06773065e+06 * E;
     ep.kx = twoPiDLambda * dxp;
     ep.kz = twoPiDLambda * dyp;
     momX[1] += dxp; momX[3] += dyp; momY[1] += dxp; momY[3] += dyp;     // srTOptAngle::PropagateRadMoments
@@ -371,7 +376,19 @@ extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* p
     return 0;
 }
 
+static int add_impl(srwgMultiE* m, int n, const double* arOffsets, int stride, void* stream);
+
 extern "C" SRWG_API int srwgMultiEAdd(srwgMultiE* m, int n, const double* arOffsets, void* stream)
+{
+    return add_impl(m, n, arOffsets, 4, stream);
+}
+
+extern "C" SRWG_API int srwgMultiEAddE(srwgMultiE* m, int n, const double* arOffsets, void* stream)
+{
+    return add_impl(m, n, arOffsets, 5, stream);
+}
+
+static int add_impl(srwgMultiE* m, int n, const double* arOffsets, int stride, void* stream)
 {
     std::lock_guard<std::mutex> lk(library_mutex());
     set_last_detail("");
@@ -399,7 +416,7 @@ extern "C" SRWG_API int srwgMultiEAdd(srwgMultiE* m, int n, const double* arOffs
                 for (int k = t0; k < cnt; k += nthr) {
                     SRWLWfr w;
                     memset(&eps[k], 0, sizeof(ElecParams));
-                    electron_wfr(*m, arOffsets + 4 * (size_t)(e + k), w, momX, momY, eps[k]);
+                    electron_wfr(*m, arOffsets + (size_t)stride * (e + k), stride, w, momX, momY, eps[k]);
                     pls[k] = Planner();
                     pls[k].numMoments = false;
                     rcs[k] = pls[k].plan(&w, m->opt);

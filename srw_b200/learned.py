@@ -28,7 +28,7 @@ import numpy as np
 from . import capi
 
 GRID = np.array([1.0, 1.25, 1.5, 1.75, 2.0])       # candidate range / resolution factors
-REF_FACTORS = (3.0, 3.0)                             # the oversampled propagation labels are judged against
+REF_FACTORS = (3.0, 3.0)                             # the oversampled propagation the labels are compared with
 CONSERVATIVE = (2.0, 2.0)                            # fallback
 TOL_LABEL = 1e-3                                     # relative L2 intensity error accepted by a label
 N_IMG = 64 * 64

@@ -23,14 +23,16 @@ from . import capi
 from .srwlpy import make_c_optc, make_c_wfr
 
 
-def sample_offsets(n, sig_x, sig_xp, sig_y, sig_yp, seed=0, first=0):
-    """Offsets of electrons first .. first+n-1: [n, 4] = (x, x', y, y'), independent normals.
-    Electron k always gets the same numbers (Philox stream keyed by the seed, advanced to k)."""
-    out = np.empty((n, 4), np.float64)
-    sig = np.array([sig_x, sig_xp, sig_y, sig_yp], np.float64)
+def sample_offsets(n, sig_x, sig_xp, sig_y, sig_yp, seed=0, first=0, sig_e=None):
+    """Offsets of electrons first .. first+n-1: [n, 4] = (x, x', y, y'), independent normals, and with
+    sig_e a fifth column, the relative energy deviation.  Electron k always gets the same numbers
+    (Philox stream keyed by the seed, advanced to k; the first four do not depend on sig_e)."""
+    m = 4 if sig_e is None else 5
+    out = np.empty((n, m), np.float64)
+    sig = np.array([sig_x, sig_xp, sig_y, sig_yp] + ([] if sig_e is None else [sig_e]), np.float64)
     for i in range(n):
         g = np.random.Generator(np.random.Philox(key=seed, counter=[first + i, 0, 0, 0]))
-        out[i] = g.standard_normal(4) * sig
+        out[i] = g.standard_normal(m) * sig
     return out
 
 
@@ -63,9 +65,13 @@ class MultiE(object):
         self.nx, self.ny = int(self._accm.nx), int(self._accm.ny)
 
     def add(self, offsets, stream=None):
-        off = np.ascontiguousarray(offsets, np.float64).reshape(-1, 4)
+        """offsets: [n, 4] (x, x', y, y') or [n, 5] with the relative energy deviation."""
+        a = np.asarray(offsets, np.float64)
+        m = a.shape[-1] if a.ndim == 2 and a.shape[-1] in (4, 5) else 4
+        off = np.ascontiguousarray(a).reshape(-1, m)
         st = C.c_void_p(stream) if stream else None
-        capi.check(capi.lib().srwgMultiEAdd(self._h, int(off.shape[0]), off.ctypes.data, st), 'multi-electron add')
+        f = capi.lib().srwgMultiEAddE if m == 5 else capi.lib().srwgMultiEAdd
+        capi.check(f(self._h, int(off.shape[0]), off.ctypes.data, st), 'multi-electron add')
 
     def count(self):
         n = C.c_longlong()

@@ -152,3 +152,19 @@ def test_multie_batch_sizes_and_graph_agree():
         got, n = _multie(batch, graph, offs)
         assert n == 9
         np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.gpu
+def test_multie_energy_spread_vs_oracle():
+    """Electrons with a relative energy deviation (fifth offset): each wavefront's photon energy is
+    rescaled to E (1 + 2 d); against the oracle loop, and visibly different from no spread."""
+    _gpu()
+    offs = sample_offsets(6, *SIG, seed=5, sig_e=5e-3)
+    assert offs.shape == (6, 5) and np.array_equal(offs[:, :4], sample_offsets(6, *SIG, seed=5))
+    got, n = _multie(4, True, offs)
+    i, sc, el, pp, acc = base_case()
+    want = oracle_sum(i, sc, el, pp, acc, offs) / 6
+    assert n == 6
+    assert rel_l2(got, want) < TOL
+    flat = oracle_sum(i, sc, el, pp, acc, offs[:, :4]) / 6
+    assert rel_l2(flat, want) > 10 * TOL

@@ -277,15 +277,35 @@ SRWG_API int srwgWfrFeatures(const float* dEx, const float* dEy, int nx, int ny,
  * this runs the propagation of srwgPlanCreate + srwgPlanExecute without allocating any device
  * memory: the caller passes the input fields (dExIn/dEyIn, read only) and the output fields
  * (dExOut/dEyOut, outCapacity complex points each, device memory), and all intermediate data
- * lives in one fixed device array inside the library (9 MiB, held by every GPU that loads the
- * library until the process exits).  Limit: intermediate grids of at most 512 x 512 points and
- * 1 MiB of plan tables; larger propagations return error 23904 (text: srwlUtiGetErrText).
- * Runs on the current device and `stream`; pWfrOut (optional) receives the output mesh and
- * scalars.  The first call on a device looks the array up (cudaGetSymbolAddress) with that
- * device current.  Calls share the array: calls that overlap on the GPU race. */
+ * lives in one fixed device array inside the library (11 MiB, held by every GPU that loads the
+ * library until the process exits).  Limits: intermediate grids of at most 512 x 512 points,
+ * 1 MiB of plan tables and 2 MiB of moment-pass results and scratch; larger propagations return
+ * error 23904 (text: srwlUtiGetErrText).  Runs on the current device and `stream`; pWfrOut
+ * (optional) receives the output mesh and scalars.  Where the propagation recomputes the moments
+ * from the field and pWfrOut has moment arrays, the call waits for `stream` to read them back.
+ * Every call copies its tables from host memory, so a call on a stream that is being captured
+ * returns error 23903 without queuing anything.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) with that device current; make it before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race. */
 SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRWLOptC* pOpt, const float* dExIn,
                                        const float* dEyIn, float* dExOut, float* dEyOut, long long outCapacity,
                                        void* stream, SRWLWfr* pWfrOut);
+
+/* Autotuned launch shapes (no counterpart in the reference, whose FFTs are FFTW's): lines per CTA of
+ * the line passes with compile-time lengths (powers of two, and the general lengths of
+ * linen_lengths.h), per axis (0 rows, 1 columns) and line length N.  The library reads the table
+ * measured by srw_b200.tune from models/line_tuning.txt beside its directory (or the file named by
+ * the environment variable SRWG_TUNING; "" for the built-in defaults) at its first plan.
+ *   srwgTuneSetLines: sets one entry (lines = 0 removes it); error 23903 for an invalid shape
+ *   srwgTuneGetLines: the value plans use now (0: not a compile-time length)
+ *   srwgTuneLoad:     replaces the table by a file's entries (NULL or "": defaults only) */
+SRWG_API int srwgTuneSetLines(int axis, int N, int lines);
+SRWG_API int srwgTuneGetLines(int axis, int N, int* lines);
+SRWG_API int srwgTuneLoad(const char* path, int* nEntries);
+
+/* The number of points a resize gives for a requested n: the next good FFT number at or above n
+ * (NextCorrectNumberForFFT, cpp/src/ext/genmath/gmfft.cpp:156), as the planner uses it. */
+SRWG_API long srwgNextFftNumber(long n);
 
 /* Human-readable list of the planned passes (one line per kernel) into buf. */
 SRWG_API int srwgPlanDescribe(const srwgPlan* plan, char* buf, int bufLen);

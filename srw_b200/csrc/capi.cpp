@@ -2,6 +2,7 @@
 // srwlUtiSetAllocArrayFunc / srwlUtiGetErrText (cpp/src/lib/srwlib.h:542, 549, 574, 821) and the srwgPlan* extensions, plus the
 // executor that runs a plan's passes on a CUDA stream.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -23,6 +24,7 @@ namespace srwg {
 
 static std::string g_lastDetail;                          // detail text of the last error
 void set_last_detail(const std::string& s) { g_lastDetail = s; }
+const std::string& last_detail() { return g_lastDetail; }
 static int (*g_modifFunc)(int, SRWLWfr*, char) = nullptr;  // client re-allocation callback
 static char* (*g_allocArrayFunc)(char, long long) = nullptr; // client array allocation (extracted intensities)
 static std::mutex g_mutex;
@@ -107,6 +109,65 @@ int radix_plan(int N, int* r)
     return ns;
 }
 
+// ------------------------------------------------------------------------------------------------
+// autotuned launch shapes: lines per CTA of the compile-time-length line kernels per (axis, N),
+// measured by srw_b200.tune and stored as lines "rows|cols N L" in models/line_tuning.txt next to
+// the library (or the file named by SRWG_TUNING); srwgTuneSetLines changes entries at run time
+// ------------------------------------------------------------------------------------------------
+static std::mutex g_tuneMutex;
+static std::map<std::pair<int, int>, int> g_tune;
+static bool g_tuneLoaded = false;
+
+static int tune_load_file(const char* path, int* nOut)
+{
+    FILE* f = fopen(path, "r");
+    if (!f) return -1;
+    char line[256];
+    int n = 0;
+    while (fgets(line, sizeof(line), f)) {
+        char ax[16];
+        int N = 0, L = 0;
+        if (line[0] == '#' || sscanf(line, "%15s %d %d", ax, &N, &L) != 3) continue;
+        const int axis = strcmp(ax, "rows") == 0 ? 0 : strcmp(ax, "cols") == 0 ? 1 : -1;
+        if (axis < 0 || !fixed_lines_valid(axis, N, L)) continue;
+        g_tune[std::make_pair(axis, N)] = L;
+        n++;
+    }
+    fclose(f);
+    if (nOut) *nOut = n;
+    return 0;
+}
+
+static void tune_ensure_loaded()
+{
+    if (g_tuneLoaded) return;
+    g_tuneLoaded = true;
+    const char* env = getenv("SRWG_TUNING");
+    if (env != nullptr) {
+        if (*env) tune_load_file(env, nullptr);           // SRWG_TUNING="" : defaults only
+        return;
+    }
+    Dl_info info;
+    if (dladdr((void*)&tune_load_file, &info) && info.dli_fname) {
+        std::string so(info.dli_fname);
+        const size_t cut = so.find_last_of('/');
+        const std::string dir = cut == std::string::npos ? std::string(".") : so.substr(0, cut);
+        tune_load_file((dir + "/../models/line_tuning.txt").c_str(), nullptr);
+    }
+}
+
+int fixed_lines_per_cta(int axis, int N)
+{
+    if (!line2_supported(N) && !linen_supported(N)) return 0;
+    {
+        std::lock_guard<std::mutex> lk(g_tuneMutex);
+        tune_ensure_loaded();
+        auto it = g_tune.find(std::make_pair(axis, N));
+        if (it != g_tune.end()) return it->second;
+    }
+    return line2_supported(N) ? line2_lines_per_cta(axis, N) : linen_lines_per_cta(axis, N);
+}
+
 int line_config(const LineDesc& d, LineLaunch& p)
 {
     p.d = d;
@@ -130,11 +191,25 @@ int line_config(const LineDesc& d, LineLaunch& p)
         // one pad point per 16 (conflict-free Stockham exchanges) plus 4 per line, so that the
         // lines of a tile start 8 banks apart
         p.P = N + N / 16 + 4;
-        const int L = line2_lines_per_cta(d.axis, N);
+        const int L = fixed_lines_per_cta(d.axis, N);
         if (p.T * L > 1024) { g_lastDetail = "line pass too large"; return SRWG_ERR_UNSUPPORTED; }
         p.L = L;
         p.G = L;
         if ((size_t)p.L * p.P * sizeof(float2) > cap) { g_lastDetail = "line too long for shared memory"; return SRWG_ERR_UNSUPPORTED; }
+        return 0;
+    }
+    // general length with a specialised kernel (linen.cuh): compile-time schedule, T = ceil(N/16)
+    if (linen_supported(N)) {
+        p.v2 = 3;
+        p.T = (N + 15) / 16;
+        p.P = N + N / 16 + 4;
+        p.L = fixed_lines_per_cta(d.axis, N);
+        p.G = p.L;
+        p.nst = 0;
+        if (p.T * p.L > 512 || (size_t)p.L * p.P * sizeof(float2) > cap) {
+            g_lastDetail = "line too long for shared memory";
+            return SRWG_ERR_UNSUPPORTED;
+        }
         return 0;
     }
     // general good number with radices 16/8/4/2, 3, 5, 7 and at least two stages: the fused pass of
@@ -720,12 +795,14 @@ int srwlPropagElecField(SRWLWfr* pWfr, SRWLOptC* pOpt, int nInt, char** arID, SR
 
 int srwgPlanCreate(const SRWLWfr* pWfr, const SRWLOptC* pOpt, int device, srwgPlan** ppPlan)
 {
-    std::lock_guard<std::mutex> lk(g_mutex);
-    g_lastDetail.clear();
     if (ppPlan == nullptr) return SRWG_ERR_BAD_ARG;
     *ppPlan = nullptr;
+    // the planner is host bookkeeping without shared state: plans are made outside the library lock,
+    // so that threads can plan concurrently
     srwgPlan* p = new srwgPlan();
     int r = p->pl.plan(pWfr, pOpt);
+    std::lock_guard<std::mutex> lk(g_mutex);
+    g_lastDetail.clear();
     if (r) { g_lastDetail = p->pl.err; delete p; return r; }
     p->device = device;
     // validate every pass configuration up front
@@ -863,6 +940,45 @@ int srwgPlanExecuteTimed(srwgPlan* plan, const float* dExIn, const float* dEyIn,
 int srwgPlanDestroy(srwgPlan* plan)
 {
     delete plan;
+    return 0;
+}
+
+long srwgNextFftNumber(long n)
+{
+    return srwg::next_correct_number_for_fft(n);
+}
+
+int srwgTuneSetLines(int axis, int N, int lines)
+{
+    std::lock_guard<std::mutex> lk(g_tuneMutex);
+    tune_ensure_loaded();
+    if (axis != 0 && axis != 1) return SRWG_ERR_BAD_ARG;
+    if (lines == 0) { g_tune.erase(std::make_pair(axis, N)); return 0; }
+    if (!fixed_lines_valid(axis, N, lines)) {
+        g_lastDetail = "not a valid launch shape for this line length";
+        return SRWG_ERR_BAD_ARG;
+    }
+    g_tune[std::make_pair(axis, N)] = lines;
+    return 0;
+}
+
+int srwgTuneGetLines(int axis, int N, int* lines)
+{
+    if (lines == nullptr || (axis != 0 && axis != 1)) return SRWG_ERR_BAD_ARG;
+    *lines = fixed_lines_per_cta(axis, N);
+    return 0;
+}
+
+int srwgTuneLoad(const char* path, int* nEntries)
+{
+    std::lock_guard<std::mutex> lk(g_tuneMutex);
+    g_tuneLoaded = true;
+    g_tune.clear();
+    if (path == nullptr || !*path) { if (nEntries) *nEntries = 0; return 0; }
+    if (tune_load_file(path, nEntries) != 0) {
+        g_lastDetail = std::string("cannot read ") + path;
+        return SRWG_ERR_BAD_ARG;
+    }
     return 0;
 }
 

@@ -125,6 +125,27 @@ template <int DIR> __device__ __forceinline__ void dft5(float2* v)
     v[2] = cadd(a2, b2); v[3] = csub(a2, b2);
 }
 
+// 7-point DFT from the symmetric pairs (v_k +/- v_(7-k)): 36 real multiply-adds, no table
+template <int DIR> __device__ __forceinline__ void dft7(float2* v)
+{
+    const float c1 = 0.62348980185873353053f, c2 = -0.22252093395631440429f, c3 = -0.90096886790241912624f;
+    const float s1 = 0.78183148246802980871f, s2 = 0.97492791218182360702f, s3 = 0.43388373911755812048f;
+    const float2 a1 = cadd(v[1], v[6]), a2 = cadd(v[2], v[5]), a3 = cadd(v[3], v[4]);
+    const float2 b1 = csub(v[1], v[6]), b2 = csub(v[2], v[5]), b3 = csub(v[3], v[4]);
+    const float2 x0 = v[0];
+    auto lin = [&](float p, float q, float r, float2 u1, float2 u2, float2 u3, float2 z) {
+        return make_float2(fmaf(p, u1.x, fmaf(q, u2.x, fmaf(r, u3.x, z.x))), fmaf(p, u1.y, fmaf(q, u2.y, fmaf(r, u3.y, z.y))));
+    };
+    const float2 z0 = make_float2(0.f, 0.f);
+    const float2 A1 = lin(c1, c2, c3, a1, a2, a3, x0), B1 = mul_mi<DIR>(lin(s1, s2, s3, b1, b2, b3, z0));
+    const float2 A2 = lin(c2, c3, c1, a1, a2, a3, x0), B2 = mul_mi<DIR>(lin(s2, -s3, -s1, b1, b2, b3, z0));
+    const float2 A3 = lin(c3, c1, c2, a1, a2, a3, x0), B3 = mul_mi<DIR>(lin(s3, -s1, s2, b1, b2, b3, z0));
+    v[0] = cadd(x0, cadd(a1, cadd(a2, a3)));
+    v[1] = cadd(A1, B1); v[6] = csub(A1, B1);
+    v[2] = cadd(A2, B2); v[5] = csub(A2, B2);
+    v[3] = cadd(A3, B3); v[4] = csub(A3, B3);
+}
+
 // generic odd radix (7, 11, 13): direct O(R^2) DFT; W_R^m = tw[m * N / R]
 template <int R, int DIR> __device__ __forceinline__ void dftg(float2* v, const float2* __restrict__ tw, int NdR)
 {
@@ -152,6 +173,7 @@ template <int R, int DIR> __device__ __forceinline__ void dftR(float2* v, const 
     else if (R == 5) dft5<DIR>(v);
     else if (R == 8) dft8<DIR>(v);
     else if (R == 16) dft16<DIR>(v);
+    else if (R == 7) dft7<DIR>(v);
     else dftg<R, DIR>(v, tw, N / R);
 }
 
@@ -520,5 +542,13 @@ __device__ __forceinline__ Chain2 make_chain2(const ChainTab& t, int rs1, int mi
     c.extra = extra;
     return c;
 }
+
+// element i of a line pass's output line: row-major (offset i * str) or, for a row pass feeding a
+// column pass, column-blocked: blocks of 2^lg columns stored contiguously per row, offset
+// (i >> lg) * bstr + (i & mask)
+struct OutMap {
+    int str, lg, bstr;
+    __device__ __forceinline__ int at(int i) const { return lg < 0 ? i * str : ((i >> lg) * bstr + (i & ((1 << lg) - 1))); }
+};
 
 }  // namespace srwg

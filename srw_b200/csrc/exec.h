@@ -38,4 +38,5 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
 int line_config(const LineDesc& d, LineLaunch& p);   // launch shape of a line pass (capi.cpp)
 int radix_plan(int N, int* r);
 void set_last_detail(const std::string& s);          // detail text for srwlUtiGetErrText
+const std::string& last_detail();
 }  // namespace srwg

@@ -5,9 +5,24 @@
 // no tensor cores.  Phase arguments are formed and reduced modulo 2*pi in FP64 and evaluated
 // with an FP32 sincosf, as the reference forms them in double before its float CosAndSin
 // (sroptelm.h:856-871).
+#include <mutex>
+#include <set>
+
 #include "common.cuh"
 
 namespace srwg {
+
+// CUDA function attributes (here: the dynamic shared-memory limit) belong to a device's context,
+// so they are set once per device and kernel group, before that group's first launch there
+static bool attrs_needed(int group)
+{
+    static std::mutex m;
+    static std::set<long long> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return true;
+    std::lock_guard<std::mutex> lk(m);
+    return done.insert(((long long)dev << 8) | group).second;
+}
 
 // ------------------------------------------------------------------------------------------------
 // LINE pass: a CTA owns L whole rows (axis 0) or L whole columns (axis 1) in shared memory; G
@@ -577,13 +592,20 @@ Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra, int f1, int f2)
     }
 }
 
+Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt)
+{
+#define SRWG_LINEN_CASE(M) if (N == M) return linen_get_##M(cols, extra, nt);
+    SRWG_LINEN_LENGTHS(SRWG_LINEN_CASE)
+#undef SRWG_LINEN_CASE
+    return nullptr;
+}
+
 cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
 {
     dim3 grid((p.nlines + p.L - 1) / p.L, 2, p.nb > 1 ? p.nb : 1);
     size_t smem = (size_t)p.L * p.P * sizeof(float2);
     if (smem > SRWG_LINE_SMEM_MAX) return cudaErrorInvalidValue;
-    static int attr_set = 0;
-    if (!attr_set) {
+    if (attrs_needed(0)) {
         cudaFuncSetAttribute(line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
         const int dirs[8][2] = {{1, 1}, {1, -1}, {-1, 1}, {-1, -1}, {1, 0}, {-1, 0}, {0, 1}, {0, -1}};
         for (int lg = 6; lg <= 14; lg++)
@@ -595,9 +617,18 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
             cudaFuncSetAttribute(lineg_get(e != 0), cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
             cudaFuncSetAttribute(lineg_e_get(e != 0), cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
         }
-        attr_set = 1;
+#define SRWG_LINEN_ATTR(M)                                                                                 \
+        for (int e = 0; e < 8; e++)                                                                        \
+            cudaFuncSetAttribute(linen_get_##M(e & 1, (e >> 1) & 1, 1 + (e >> 2)),                         \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
+        SRWG_LINEN_LENGTHS(SRWG_LINEN_ATTR)
+#undef SRWG_LINEN_ATTR
     }
-    if (p.v2 == 2) {
+    if (p.v2 == 3) {
+        Line2Fn f = linen_kernel_ptr(p.N, p.d.axis != 0, p.d.has_extra != 0, (p.d.f1 && p.d.f2) ? 2 : 1);
+        if (f == nullptr || p.T * p.L > 512) return cudaErrorInvalidValue;
+        f<<<grid, p.T * p.L, smem, st>>>(p);
+    } else if (p.v2 == 2) {
         Line2Fn f = p.d.has_extra ? lineg_e_get(p.d.axis != 0) : lineg_get(p.d.axis != 0);
         if (p.T * p.L > 512) return cudaErrorInvalidValue;
         f<<<grid, p.T * p.L, smem, st>>>(p);
@@ -623,11 +654,8 @@ cudaError_t launch_resize(const ResizeLaunch& q, cudaStream_t st)
         const size_t smem = (size_t)(2 * SRWG_RESIZE_TX + 2 * SRWG_RESIZE_TZ) * sizeof(float4) +
                             (size_t)2 * p.d.tile_or * SRWG_RESIZE_TX * sizeof(float4) +
                             (size_t)2 * p.d.tile_or * p.d.tile_oc * sizeof(float2);
-        static int attr = 0;
-        if (!attr) {
+        if (attrs_needed(1))
             cudaFuncSetAttribute(resize2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
-            attr = 1;
-        }
         dim3 grid((p.d.nxn + SRWG_RESIZE_TX - 1) / SRWG_RESIZE_TX, (p.d.nzn + SRWG_RESIZE_TZ - 1) / SRWG_RESIZE_TZ,
                   p.nb > 1 ? p.nb : 1);
         resize2_kernel<<<grid, 256, smem, st>>>(p);

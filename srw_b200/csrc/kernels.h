@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "kdesc.h"
+#include "linen_lengths.h"
 
 namespace srwg {
 
@@ -32,7 +33,8 @@ struct LineLaunch {
     int T, L, P, G;          // threads per line, lines per CTA, shared-memory pitch (float2), thread groups
     int nst;
     int radix[SRWG_MAX_STAGES];
-    int v2;                  // 1: power-of-two pass (line2_kernel), 2: general length (lineg_kernel)
+    int v2;                  // 1: power-of-two pass (line2_kernel), 2: general length (lineg_kernel),
+                             // 3: specialised general length (linen_kernel)
     const float2* tabs;      // the plan's separable point-wise tables
     const LineDesc* gd;      // this pass's descriptor in device memory
     int nb;                  // wavefronts in the launch (grid z; 0 or 1: one)
@@ -102,6 +104,52 @@ SRWG_LINE2_DECL(11) SRWG_LINE2_DECL(12) SRWG_LINE2_DECL(13) SRWG_LINE2_DECL(14)
 // general-length line pass kernels (lineg.cu, lineg_e.cu)
 Line2Fn lineg_get(bool cols);
 Line2Fn lineg_e_get(bool cols);
+// specialised general-length kernels (linen.cu, one unit per length of linen_lengths.h)
+#define SRWG_LINEN_DECL(N) Line2Fn linen_get_##N(bool cols, bool extra, int nt);
+SRWG_LINEN_LENGTHS(SRWG_LINEN_DECL)
+#undef SRWG_LINEN_DECL
+Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt);
+inline bool line2_supported(int N) { return N >= 64 && N <= 16384 && (N & (N - 1)) == 0; }
+inline bool linen_supported(int N)
+{
+#define SRWG_LINEN_IS(M) if (N == M) return true;
+    SRWG_LINEN_LENGTHS(SRWG_LINEN_IS)
+#undef SRWG_LINEN_IS
+    return false;
+}
+// lines per CTA of the specialised general-length pass (at most 512 threads, 128 registers each):
+// rows up to 512 threads, columns a power of two up to 512 threads / 32 columns (the column-block
+// width of the row pass before it), within the shared-memory budget; T = ceil(N/16) threads per
+// line, pitch N + N/16 + 4 points
+inline int linen_lines_per_cta(int axis, int N)
+{
+    const int T = (N + 15) / 16;
+    const size_t P = (size_t)N + N / 16 + 4;
+    int L;
+    if (axis == 0) {
+        L = 512 / T;
+        if (L < 1) L = 1;
+    } else {
+        L = 1;
+        while (2 * L * T <= 512 && 2 * L <= 32) L *= 2;
+    }
+    while (L > 1 && (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) L = axis == 0 ? L - 1 : L / 2;
+    return L;
+}
+// whether L lines per CTA is a valid launch shape of the compile-time-length kernel of N
+inline bool fixed_lines_valid(int axis, int N, int L)
+{
+    const size_t P = (size_t)N + N / 16 + 4;
+    if (L < 1 || (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) return false;
+    if (axis == 1 && (L > 32 || (L & (L - 1)) != 0)) return false;      // column blocks: a power of two
+    if (line2_supported(N)) return (N / 16) * L <= 1024;
+    if (linen_supported(N)) return ((N + 15) / 16) * L <= 512;
+    return false;
+}
+// lines per CTA of the line kernels with compile-time lengths (line2 / linen; they skip a zero
+// window and read / write column blocks): the autotuned value where the tuning table has one
+// (capi.cpp), else the default above; 0 for other lengths
+int fixed_lines_per_cta(int axis, int N);
 cudaError_t launch_resize(const ResizeLaunch& p, cudaStream_t st);
 cudaError_t launch_pw(const PwLaunch& p, cudaStream_t st);
 

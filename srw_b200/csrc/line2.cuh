@@ -16,13 +16,6 @@ namespace srwg {
 
 // IN: 0 shared, 1 shared through chain cin, 2 global through chain cin;  OUT: 0 shared, 1 global through chain cout
 // N (line length), R (radix) and Ns (product of the radices already applied) are compile-time.
-// element i of the output line: row-major (offset i * str) or, for a row pass feeding a column pass,
-// column-blocked: blocks of 2^lg columns stored contiguously per row, offset (i >> lg) * bstr + (i & mask)
-struct OutMap {
-    int str, lg, bstr;
-    __device__ __forceinline__ int at(int i) const { return lg < 0 ? i * str : ((i >> lg) * bstr + (i & ((1 << lg) - 1))); }
-};
-
 template <int N, int R, int NS, int DIR, int IN, int OUT, bool EXTRA>
 __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout,
                                         int gstr, const OutMap& om, int t, int line, const Chain2& cin, const Chain2& cout,

@@ -1,0 +1,291 @@
+// Line pass for general FFT lengths N = 2^a 3^b 5^c 7^d (a >= 1), specialised per length: the 1280 ..
+// 7168-point grids that resize factors such as 1.25, 1.5 or 1.75 produce.  Same organisation as the
+// power-of-two pass (line2.cuh): a CTA owns L whole lines in padded shared memory, the first
+// Stockham stage reads global memory directly through the input chain, the last one writes global
+// memory directly through the output chain (tables of the plan, per-line factor at the store),
+// intermediate stages exchange through shared memory.  N, the radix schedule (radix-16 stages, one
+// 8/4/2 stage, then 3, 5, 7), the threads per line (T = ceil(N/16)) and every index are
+// compile-time; a stage of radix R gives each thread ceil(N/R / T) butterflies.  Inverse transforms
+// are forward transforms of the conjugated line, conjugated back (conj(DFT(conj x)) = IDFT x), so one
+// instantiation serves both directions.  The centring rotation (k + N/2 mod N) and the mirror
+// (N - 1 - k) are an add and a compare.
+#pragma once
+#include "common.cuh"
+
+namespace srwg {
+
+#define PADN(p) ((p) + ((p) >> 4))
+
+// compile-time radix schedule of N
+struct NSched {
+    int n;
+    int r[SRWG_MAX_STAGES];
+};
+__host__ __device__ constexpr NSched nsched(int N)
+{
+    NSched s{0, {0}};
+    int m = N, p2 = 0;
+    while (m % 2 == 0) { m /= 2; p2++; }
+    while (p2 >= 4) { s.r[s.n++] = 16; p2 -= 4; }
+    if (p2 > 0) s.r[s.n++] = 1 << p2;
+    while (m % 3 == 0) { s.r[s.n++] = 3; m /= 3; }
+    while (m % 5 == 0) { s.r[s.n++] = 5; m /= 5; }
+    while (m % 7 == 0) { s.r[s.n++] = 7; m /= 7; }
+    if (m != 1) s.n = -1;
+    return s;
+}
+__host__ __device__ constexpr int nsched_ns(int N, int i)
+{
+    NSched s = nsched(N);
+    int ns = 1;
+    for (int k = 0; k < i; k++) ns *= s.r[k];
+    return ns;
+}
+template <int N> struct NPlan {
+    static constexpr NSched s = nsched(N);
+    static constexpr int T = (N + 15) / 16;
+};
+
+// (k + N/2) mod N
+template <int N> __device__ __forceinline__ int rot_n(int k)
+{
+    const int m = k + N / 2;
+    return m >= N ? m - N : m;
+}
+// source index of destination k through a chain (rotation rs2, mirror, rotation rs1); i: the index
+// at which the non-separable work is evaluated
+template <int N> __device__ __forceinline__ int chain_src_n(const ChainG& c, int k, int& i)
+{
+    const int m = c.rs2 ? rot_n<N>(k) : k;
+    i = c.mir ? (N - 1 - m) : m;
+    return c.rs1 ? rot_n<N>(i) : i;
+}
+// destination of transform output q through an output chain (rotation rs1, then mirror)
+template <int N> __device__ __forceinline__ int chain_dst_n(const ChainG& c, int q)
+{
+    const int k = c.rs1 ? rot_n<N>(q) : q;
+    return c.mir ? (N - 1 - k) : k;
+}
+
+// One stage of radix R (NS: product of the radices applied before it).  IN: 0 shared memory, 1
+// shared memory through chain cin, 2 global memory through chain cin; OUT: 0 shared memory, 1 global
+// memory through chain cout.  FIRST / LAST: first / last stage of its transform (conjugation of the
+// inputs after the input chain / of the outputs before the output chain when the transform is an
+// inverse one: cj = -1).
+template <int N, int R, int NS, int IN, int OUT, bool FIRST, bool LAST, bool EXTRA>
+__device__ __forceinline__ void nstage(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout, int gstr,
+                                       const OutMap& om, int t, int line, const ChainG& cin, const ChainG& cout, float cj,
+                                       const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
+                                       const float2* __restrict__ tabs, const PwOps* ex, int axis, int za0, int za1)
+{
+    constexpr int T = NPlan<N>::T;
+    constexpr int NR = N / R;
+    constexpr int B = (NR + T - 1) / T;              // butterflies per thread
+    constexpr bool PART = (NR % T) != 0;             // the last round has idle threads
+    constexpr int TWS = N / (NS * R);
+    float2 v[B][R];
+    if (IN == 2) {
+        // first stage from global memory: all loads issued before any dependent arithmetic
+#pragma unroll
+        for (int b = 0; b < B; b++) {
+            const int j = t + T * b;
+            const bool ok = active && (!PART || j < NR);
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                int i;
+                const int q = chain_src_n<N>(cin, j + r * NR, i);
+                const bool in = ok && q >= za0 && q <= za1;
+                v[b][r] = in ? __ldcs(&gin[q * gstr]) : make_float2(0.f, 0.f);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < B; b++) {
+            const int j = t + T * b;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int p = j + r * NR;
+                int i;
+                chain_src_n<N>(cin, p, i);
+                float2 x = cmul(chainG_factor<EXTRA>(cin, p, i, line, tabs, ex, axis), v[b][r]);
+                x.y *= cj;
+                v[b][r] = x;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int b = 0; b < B; b++) {
+            const int j = t + T * b;
+            const bool ok = active && (!PART || j < NR);
+            const int k = NS > 1 ? j % NS : 0;
+            float2 wp[4];
+            if (NS > 1) {
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    if ((1 << e) < R) wp[e] = ok ? __ldg(&tw[(k * TWS) << e]) : make_float2(1.f, 0.f);
+            }
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int p = j + r * NR;
+                float2 x = make_float2(0.f, 0.f);
+                if (ok) {
+                    if (IN == 0) {
+                        x = s[PADN(p)];
+                    } else {
+                        int i;
+                        const int q = chain_src_n<N>(cin, p, i);
+                        x = cmul(chainG_factor<EXTRA>(cin, p, i, line, tabs, ex, axis), s[PADN(q)]);
+                        if (FIRST) x.y *= cj;
+                    }
+                }
+                if (NS > 1 && r > 0) {
+                    // W^(k r) from the table powers W^k, W^2k, W^4k, W^8k
+                    float2 w = make_float2(1.f, 0.f);
+                    bool first = true;
+#pragma unroll
+                    for (int e = 0; e < 4; e++)
+                        if (r & (1 << e)) { w = first ? wp[e] : cmul(w, wp[e]); first = false; }
+                    x = cmul(x, w);
+                }
+                v[b][r] = x;
+            }
+        }
+    }
+    if (OUT == 0) __syncthreads();
+#pragma unroll
+    for (int b = 0; b < B; b++) {
+        const int j = t + T * b;
+        const bool ok = active && (!PART || j < NR);
+        dftR<R, 1>(v[b], tw, N);
+        const int k = NS > 1 ? j % NS : 0;
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int q = base + r * NS;
+            float2 o = v[b][r];
+            if (LAST) o.y *= cj;
+            if (ok) {
+                if (OUT == 0) {
+                    s[PADN(q)] = o;
+                } else {
+                    const int kk = chain_dst_n<N>(cout, q);
+                    int i;
+                    chain_src_n<N>(cout, kk, i);
+                    o = cmul(chainG_factor<EXTRA>(cout, kk, i, line, tabs, ex, axis), o);
+                    if (has_lf) o = cmul(lf, o);
+                    __stcs(&gout[om.at(kk)], o);
+                }
+            }
+        }
+    }
+    if (OUT == 0) __syncthreads();
+}
+
+// one transform along the line with the compile-time schedule of N; INM: mode of the first stage's
+// input (1 shared through cin, 2 global through cin), OUTM: of the last stage's output (0 shared, 1
+// global through cout)
+template <int N, int INM, int OUTM, bool EXTRA>
+__device__ __forceinline__ void fft_n(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout, int gstr,
+                                      const OutMap& om, int t, int line, const ChainG& cin, const ChainG& cout, float cj,
+                                      const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
+                                      const float2* __restrict__ tabs, const PwOps* ex, int axis, int za0, int za1)
+{
+    constexpr NSched S = NPlan<N>::s;
+    static_assert(S.n >= 2 && S.n <= 8, "radix schedule");
+#define SRWG_NSTAGE(I)                                                                                          \
+    if constexpr (S.n > (I))                                                                                    \
+        nstage<N, S.r[(I) < S.n ? (I) : 0], nsched_ns(N, (I)), (I) == 0 ? INM : 0, (I) == S.n - 1 ? OUTM : 0,   \
+               (I) == 0, (I) == S.n - 1, EXTRA>(s, gin, gout, gstr, om, t, line, cin, cout, cj, tw, active,    \
+                                                has_lf, lf, tabs, ex, axis, za0, za1);
+    SRWG_NSTAGE(0) SRWG_NSTAGE(1) SRWG_NSTAGE(2) SRWG_NSTAGE(3)
+    SRWG_NSTAGE(4) SRWG_NSTAGE(5) SRWG_NSTAGE(6) SRWG_NSTAGE(7)
+#undef SRWG_NSTAGE
+}
+
+// NT: transforms in the pass (1 or 2); their directions come from the descriptor
+template <int N, bool COLS, bool EXTRA, int NT>
+__global__ void __launch_bounds__(512, 1) linen_kernel(const LineLaunch p)
+{
+    constexpr int T = NPlan<N>::T;
+    extern __shared__ float2 smn[];
+    const LineDesc& d = *reinterpret_cast<const LineDesc*>(reinterpret_cast<const char*>(p.gd) + blockIdx.z * p.bDesc);
+    const int comp = blockIdx.y;
+    const float2* __restrict__ src = p.src[comp] + blockIdx.z * p.bSrc;
+    float2* __restrict__ dst = p.dst[comp] + blockIdx.z * p.bDst;
+    const int L = p.L, P = p.P, nl = p.nlines;
+    const int tid = threadIdx.x;
+    const int g = COLS ? (tid % L) : (tid / T);          // line of the tile
+    const int t = COLS ? (tid / L) : (tid - g * T);      // thread within the line
+    const int line = blockIdx.x * L + g;
+    const bool active = line < nl && g < L;
+    float2* s = smn + (size_t)(g < L ? g : 0) * P;
+    int gstr = COLS ? nl : 1;
+    const float2* gin = COLS ? (src + line) : (src + (size_t)line * N);
+    if (COLS && d.blk_in > 0) {
+        gstr = d.blk_in;
+        gin = src + (size_t)(line / d.blk_in) * N * d.blk_in + (line % d.blk_in);
+    }
+    const int oline = d.mirror_lines ? (nl - 1 - line) : line;
+    float2* gout = COLS ? (dst + oline) : (dst + (size_t)oline * N);
+    OutMap om;
+    om.str = COLS ? nl : 1;
+    om.lg = -1;
+    om.bstr = 0;
+    if (!COLS && d.blk_out > 0) {
+        om.lg = 31 - __clz(d.blk_out);
+        om.bstr = nl * d.blk_out;
+        gout = dst + (size_t)oline * d.blk_out;
+    }
+    int za0 = 0, za1 = N - 1;
+    if (d.zwin) {
+        const int l0 = blockIdx.x * L, l1 = min(l0 + L, nl) - 1;
+        if (l1 < d.zl0 || l0 > d.zl1) {
+            // the whole tile is zero: so is its transform
+            if (active)
+                for (int m = t; m < N; m += T) __stcs(&gout[om.at(m)], make_float2(0.f, 0.f));
+            return;
+        }
+        if (line < d.zl0 || line > d.zl1) { za0 = 1; za1 = 0; }
+        else { za0 = d.za0; za1 = d.za1; }
+    }
+    const float2* tabs = p.tabs + blockIdx.z * p.bTab;
+    const PwOps* ex = &d.extra;
+    const int axis = d.axis;
+    ChainG pre, mid, fin;
+    pre.rs1 = 0; pre.mir = 0; pre.rs2 = d.f1_pre.rs; pre.tab = (int)d.t_pre.tab; pre.extra = 0;
+    mid.rs1 = d.f1 ? d.f1_post.rs : 0; mid.mir = d.mirror_along; mid.rs2 = d.f2 ? d.f2_pre.rs : 0;
+    mid.tab = (int)d.t_mid.tab; mid.extra = EXTRA ? d.has_extra : 0;
+    fin.rs1 = d.f2 ? d.f2_post.rs : 0; fin.mir = 0; fin.rs2 = 0; fin.tab = (int)d.t_fin.tab; fin.extra = 0;
+    const bool has_lf = (d.t_pre.ltab >= 0) || (d.t_mid.ltab >= 0) || (d.t_fin.ltab >= 0);
+    float2 lf = make_float2(1.f, 0.f);
+    if (has_lf && active) {
+        if (d.t_pre.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_pre.ltab + line]));
+        if (d.t_mid.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_mid.ltab + line]));
+        if (d.t_fin.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_fin.ltab + line]));
+    }
+    const float2* tw = p.tw;
+    if constexpr (NT == 2) {
+        fft_n<N, 2, 0, EXTRA>(s, gin, nullptr, gstr, om, t, line, pre, mid, d.f1 < 0 ? -1.f : 1.f, tw, active, has_lf,
+                              lf, tabs, ex, axis, za0, za1);
+        fft_n<N, 1, 1, EXTRA>(s, nullptr, gout, gstr, om, t, line, mid, fin, d.f2 < 0 ? -1.f : 1.f, tw, active, has_lf,
+                              lf, tabs, ex, axis, 0, N - 1);
+    } else {
+        const bool one = d.f1 != 0;
+        const float cj = (one ? d.f1 : d.f2) < 0 ? -1.f : 1.f;
+        fft_n<N, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, one ? pre : mid, one ? mid : fin, cj, tw, active, has_lf,
+                              lf, tabs, ex, axis, za0, za1);
+    }
+}
+
+// the kernel of a (COLS, EXTRA, transforms) combination for length N
+template <int N>
+Line2Fn linen_select(bool cols, bool extra, int nt)
+{
+    if (cols) {
+        if (extra) return nt == 2 ? linen_kernel<N, true, true, 2> : linen_kernel<N, true, true, 1>;
+        return nt == 2 ? linen_kernel<N, true, false, 2> : linen_kernel<N, true, false, 1>;
+    }
+    if (extra) return nt == 2 ? linen_kernel<N, false, true, 2> : linen_kernel<N, false, true, 1>;
+    return nt == 2 ? linen_kernel<N, false, false, 2> : linen_kernel<N, false, false, 1>;
+}
+
+}  // namespace srwg

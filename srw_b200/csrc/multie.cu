@@ -113,6 +113,7 @@ struct srwgMultiE {
     int anx = 0, anz = 0;
     double axStart = 0, axStep = 0, azStart = 0, azStep = 0;
     double* dAcc = nullptr;
+    double* dSnap = nullptr;             // the accumulator as it was before the current add call
     bool ownAcc = true;                  // false: caller-provided accumulator (srwgMultiESetAccumulator)
     long long nAdded = 0;
     // batch buffers
@@ -135,6 +136,7 @@ struct srwgMultiE {
     {
         if (graph) cudaGraphExecDestroy(graph);
         if (ownAcc) cudaFree(dAcc);
+        cudaFree(dSnap);
         cudaFree(dBase); cudaFree(dIn); cudaFree(dOut); cudaFree(dWork); cudaFree(dConst);
         cudaFree(dParams);
         for (int i = 0; i < 2; i++) {
@@ -352,6 +354,7 @@ extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* p
     MALLOC(m->dConst, B * m->constStride);
     MALLOC(m->dParams, B * sizeof(ElecParams));
     MALLOC(m->dAcc, (size_t)m->anx * m->anz * sizeof(double));
+    MALLOC(m->dSnap, (size_t)m->anx * m->anz * sizeof(double));
 #undef MALLOC
     for (int i = 0; i < 2; i++) {
         if (cudaMallocHost(&m->hConst[i], B * m->constStride) != cudaSuccess ||
@@ -388,6 +391,11 @@ extern "C" SRWG_API int srwgMultiEAddE(srwgMultiE* m, int n, const double* arOff
     return add_impl(m, n, arOffsets, 5, stream);
 }
 
+static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, cudaStream_t st);
+
+// A call either adds all its electrons or none: the accumulator is copied aside first, and on an
+// error (an electron whose passes differ in size from the base wavefront's, a failed launch) the
+// batches already added are taken out again by restoring that copy and the electron count.
 static int add_impl(srwgMultiE* m, int n, const double* arOffsets, int stride, void* stream)
 {
     std::lock_guard<std::mutex> lk(library_mutex());
@@ -398,6 +406,26 @@ static int add_impl(srwgMultiE* m, int n, const double* arOffsets, int stride, v
     if (r) return r;
     // the library's own stream when none is given (stream capture needs a non-default stream)
     cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    if (n == 0) return 0;
+    const size_t accBytes = (size_t)m->anx * m->anz * sizeof(double);
+    MTRY(cudaMemcpyAsync(m->dSnap, m->dAcc, accBytes, cudaMemcpyDeviceToDevice, st));
+    const long long n0 = m->nAdded;
+    r = add_body(m, n, arOffsets, stride, st);
+    if (r) {
+        const std::string why = last_detail();
+        cudaMemcpyAsync(m->dAcc, m->dSnap, accBytes, cudaMemcpyDeviceToDevice, st);
+        cudaStreamSynchronize(st);
+        m->nAdded = n0;
+        set_last_detail(why);
+        return r;
+    }
+    if (!stream) MTRY(cudaStreamSynchronize(st));
+    return 0;
+}
+
+static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, cudaStream_t st)
+{
+    int r = 0;
     std::vector<KernelDesc> first, launchKs;
     int nb = 0;
     // electrons are planned on host threads a group at a time (the planner keeps no shared state);
@@ -463,10 +491,7 @@ static int add_impl(srwgMultiE* m, int n, const double* arOffsets, int stride, v
         m->hParams[m->slot][nb] = ep;
         nb++;
     }
-    r = flush(*m, nb, launchKs, st);
-    if (r) return r;
-    if (!stream) MTRY(cudaStreamSynchronize(st));
-    return 0;
+    return flush(*m, nb, launchKs, st);
 }
 
 extern "C" SRWG_API int srwgMultiEGetMean(srwgMultiE* m, double* arMean, long long* nElec, void* stream)

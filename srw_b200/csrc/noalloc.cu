@@ -29,6 +29,10 @@
 // The first call on a device does the set-up: it looks up the array's device address with
 // cudaGetSymbolAddress, with that device current, and keeps it for the following calls on that
 // device.  Make that first call before any stream capture.
+//
+// Every call copies the plan's tables and pass descriptors from host memory into the array (and
+// may wait for the stream, above); a call whose stream is being captured is refused with
+// SRWG_ERR_BAD_ARG before anything is queued.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -87,6 +91,19 @@ extern "C" SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRW
     if (pWfr == nullptr || pOpt == nullptr || dExIn == nullptr || dEyIn == nullptr || dExOut == nullptr ||
         dEyOut == nullptr)
         return SRWG_ERR_BAD_ARG;
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        const cudaError_t ce = cudaStreamIsCapturing((cudaStream_t)stream, &cs);
+        if (ce != cudaSuccess) {
+            set_last_detail(std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(ce));
+            return SRWG_ERR_CUDA;
+        }
+        if (cs != cudaStreamCaptureStatusNone) {
+            set_last_detail("the stream is being captured: this entry point copies the plan's tables from host memory "
+                            "on every call, which a stream capture does not take");
+            return SRWG_ERR_BAD_ARG;
+        }
+    }
     Planner pl;
     int r = pl.plan(pWfr, pOpt);
     if (r) { set_last_detail(pl.err); return r; }

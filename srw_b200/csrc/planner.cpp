@@ -3,6 +3,7 @@
 // transformed meshes are bit-identical to the reference's; the field work is only described
 // (kdesc.h) and fused into as few GPU passes as possible by Builder.
 #include "kernels.h"
+#include "exec.h"
 #include "planner.h"
 
 #include <algorithm>
@@ -1664,7 +1665,7 @@ int Planner::finalize()
             n.src != kernels[i].dst || n.line.nx != r.nxn || n.line.nz != r.nzn)
             continue;
         const int N = n.line.axis == 0 ? n.line.nx : n.line.nz;
-        if (N < 64 || (N & (N - 1)) != 0) continue;      // power-of-two line kernels only
+        if (fixed_lines_per_cta(n.line.axis, N) == 0) continue;      // compile-time-length line kernels only
         LineDesc& d = n.line;
         const int ixs = (int)std::max(0L, r.ixStart), ixe = (int)std::min((long)r.nxn - 1, r.ixEnd);
         const int izs = (int)std::max(0L, r.izStart), ize = (int)std::min((long)r.nzn - 1, r.izEnd);
@@ -1682,9 +1683,8 @@ int Planner::finalize()
             a.line.nx != n.line.nx || a.line.nz != n.line.nz)
             continue;
         const int Nr = a.line.nx, Nc = n.line.nz;
-        auto pow2 = [](int v) { return v >= 64 && v <= 16384 && (v & (v - 1)) == 0; };
-        if (!pow2(Nr) || !pow2(Nc)) continue;
-        const int bw = line2_lines_per_cta(1, Nc);
+        if (fixed_lines_per_cta(0, Nr) == 0 || fixed_lines_per_cta(1, Nc) == 0) continue;
+        const int bw = fixed_lines_per_cta(1, Nc);
         if (bw < 2 || (bw & (bw - 1)) != 0 || n.line.nx % bw != 0) continue;
         a.line.blk_out = bw;
         n.line.blk_in = bw;
@@ -1698,7 +1698,7 @@ int Planner::finalize()
             n.line.zwin || n.src != a.dst || a.line.nx != n.line.nx || a.line.nz != n.line.nz)
             continue;
         const int Nc = n.line.nz;
-        if (Nc < 64 || (Nc & (Nc - 1)) != 0) continue;
+        if (fixed_lines_per_cta(1, Nc) == 0) continue;
         const int nz = a.line.nz;
         LineDesc& d = n.line;
         d.zwin = 1;
@@ -1718,9 +1718,14 @@ std::string Planner::describe() const
         const KernelDesc& k = kernels[i];
         if (k.kind == K_LINE) {
             const LineDesc& d = k.line;
-            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d zwin=%d blk=%d/%d  buf %d->%d\n",
+            // kernel family of the pass: power-of-two, specialised general length, run-time
+            // scheduled general length, table-driven
+            LineLaunch lp;
+            memset(&lp, 0, sizeof(lp));
+            const char* fam = line_config(d, lp) ? "none" : lp.v2 == 1 ? "pow2" : lp.v2 == 3 ? "spec" : lp.v2 == 2 ? "gen" : "tab";
+            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d zwin=%d blk=%d/%d  buf %d->%d  fft=%s L=%d\n",
                      i, d.axis == 0 ? "rows" : "cols", d.nx, d.nz, d.f1, d.has_pw, d.pw.has_quad, d.pw.has_ang, d.pw.nmask,
-                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, d.zwin, d.blk_in, d.blk_out, k.src, k.dst);
+                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, d.zwin, d.blk_in, d.blk_out, k.src, k.dst, fam, lp.L);
         } else if (k.kind == K_RESIZE) {
             snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pre=%d pw=%d tile=%dx%d  buf %d->%d\n", i,
                      k.rs.nxo, k.rs.nzo, k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pre, k.rs.has_pw, k.rs.tile_or,

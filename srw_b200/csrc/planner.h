@@ -10,6 +10,9 @@
 
 namespace srwg {
 
+// next good FFT number >= n (NextCorrectNumberForFFT, gmfft.cpp:156-228)
+long next_correct_number_for_fft(long n);
+
 // Subset of srTSRWRadStructAccessData (cpp/src/core/srradstr.h:67) used by this path, ne == 1.
 struct WfrState {
     int nx = 0, nz = 0;

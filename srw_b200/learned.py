@@ -1,18 +1,24 @@
-"""Learned resize factors for the aperture -> lens -> to-waist drift beamline.
+"""Learned resize factors for the aperture -> lens -> drift beamlines.
 
 The reference's users choose the range / resolution resize factors (pp[5..8] of the propagation
-parameter lists, cpp/src/core/sroptcnt.cpp:307-316) by hand; too small factors alias, too large
-ones waste memory and time (the propagated grid grows with the square of their product).  This
-module learns them: a small MLP (64 x 64 downsampled intensity, fitted phase-curvature radii and
-the element parameters -> log2 of the range and resolution factors applied before the lens) is
-trained by the project's own CUDA kernels (srwgMlp*: GEMM, bias + GELU, their gradients, MSE, Adam)
-on labels that sweeps of the plain GPU propagation produce: for every training wavefront the
-cheapest factor pair whose intensity agrees with an oversampled propagation (factors 3, 3) within
-TOL_LABEL on a common mesh.  At run time ``choose_factors`` rounds the prediction up to the sweep
-grid and checks the result (energy outside the central part of the output window); when the check
-fails, the propagation falls back to the conservative factors (2, 2).
+parameter lists: pxm, pxd, pzm, pzd; cpp/src/core/sroptcnt.cpp:307-316) by hand; too small factors
+alias or under-resolve, too large ones waste memory and time (the propagated grid grows with the
+product of range and resolution per axis).  This module learns them: a small MLP (64 x 64
+downsampled intensity, fitted phase-curvature radii, the wavefront's extent and the element
+parameters -> log2 of the four factors of the resize before the lens) is trained by the project's
+own CUDA kernels (srwgMlp*: GEMM, bias + GELU, their gradients, MSE, Adam) on labels that sweeps of
+the plain GPU propagation produce: for every training wavefront and axis, the cheapest factor pair
+(by the autotuned per-length pass times, srw_b200.tune) whose intensity agrees with an oversampled
+propagation within TOL_LABEL, the other axis held at the conservative factors; the combined label
+is checked once more and replaced by the conservative factors when it fails.
 
-    python -m srw_b200.learned --samples 2000 --out srw_b200/models/resize_mlp.npz   # GPU: data + training
+At run time ``choose_factors`` rounds the prediction up to the factor grid and checks it: the
+wavefront propagated with the chosen factors against the same wavefront with the conservative
+factors (2, 2, 2, 2), relative L2 of the intensity on a common mesh; above the tolerance it falls
+back to the conservative factors.  ``CheckedMultiE`` applies the same check to one electron of
+every batch of a multi-electron run and runs the batch with the conservative factors when it fails.
+
+    python -m srw_b200.learned --samples 20000 --out srw_b200/models/resize_mlp.npz   # GPU
 
 torch provides device memory and streams only; every kernel is the library's.
 """
@@ -21,21 +27,30 @@ import ctypes as C
 import json
 import math
 import os
+import threading
 import time
 
 import numpy as np
 
 from . import capi
 
-GRID = np.array([1.0, 1.25, 1.5, 1.75, 2.0])       # candidate range / resolution factors
-REF_FACTORS = (3.0, 3.0)                             # the oversampled propagation the labels are compared with
-CONSERVATIVE = (2.0, 2.0)                            # fallback
-TOL_LABEL = 1e-3                                     # relative L2 intensity error accepted by a label
+GRID_R = np.array([0.5, 0.625, 0.75, 1.0, 1.25, 1.5, 1.75, 2.0])   # candidate range factors
+GRID_D = np.array([1.0, 1.25, 1.5, 1.75, 2.0])                     # candidate resolution factors
+CONSERVATIVE = (2.0, 2.0, 2.0, 2.0)                                # pxm, pxd, pzm, pzd of the fallback
+TOL_LABEL = 1e-3                                                   # relative L2 intensity error accepted
+AXIS_TOL = 0.7 * TOL_LABEL                                         # per-axis share of it in the sweeps
 N_IMG = 64 * 64
-N_EXTRA = 9
+N_EXTRA = 13
 N_IN = N_IMG + N_EXTRA
+N_OUT = 4
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_MODEL = os.path.join(HERE, 'models', 'resize_mlp.npz')
+
+
+def ref_factors(n):
+    """Factors of the oversampled propagation that labels are judged against (the grid stays within
+    the 8192-point general-length limit)."""
+    return (3.0, 3.0) if n <= 512 else (2.5, 2.5)
 
 
 def _check(r, what):
@@ -48,7 +63,7 @@ def _check(r, what):
 class ResizeMLP(object):
     """FP32 MLP n_in -> hidden... -> n_out, GELU between layers; weights W[l] (in x out), b[l]."""
 
-    def __init__(self, n_in=N_IN, hidden=(256, 256, 256), n_out=2, device=0, seed=0):
+    def __init__(self, n_in=N_IN, hidden=(256, 256, 256), n_out=N_OUT, device=0, seed=0):
         import torch
         self.torch = torch
         self.dev = torch.device('cuda', device)
@@ -195,14 +210,17 @@ class ResizeMLP(object):
         return m
 
 
+
+
 # ------------------------------------------------------------------------------------------------
 # features
 # ------------------------------------------------------------------------------------------------
-def features(ex, ey, mesh, energy, ap_d, f, L, torch_dev, Rx=0., Ry=0.):
-    """Feature vector of one wavefront (complex64 CUDA tensors [ny, nx]) and its beamline:
-    64 x 64 intensity (srwgWfrFeatures) normalised to its maximum and square-rooted, the fitted
-    curvature radii (as 1/R [1/m]; the wavefront's own radii Rx, Ry are removed before the fit and
-    added back), photon energy, aperture / wavefront size, f, L and the number of points per line."""
+def features(ex, ey, mesh, energy, ap, f, L, torch_dev, Rx=0., Ry=0.):
+    """Feature vector of one wavefront (complex64 CUDA tensors [ny, nx]) and its beamline: the 64 x 64
+    intensity (srwgWfrFeatures) normalised to its maximum and square-rooted, the fitted curvature
+    radii (as 1/R [1/m]; the wavefront's own radii Rx, Ry are removed before the fit and added
+    back), photon energy, the aperture (shape, Dx, Dy relative to the wavefront's extent), f, L, the
+    extent and the number of points per axis."""
     import torch
     ny, nx = ex.shape
     xs = (mesh['xFin'] - mesh['xStart']) / (nx - 1)
@@ -219,65 +237,83 @@ def features(ex, ey, mesh, energy, ap_d, f, L, torch_dev, Rx=0., Ry=0.):
     invRx = i0x + (s[0] / (k * xs * s[1]) if s[1] > 0 else 0.)     # dphi ~ k x dx / R
     invRz = i0z + (s[2] / (k * zs * s[3]) if s[3] > 0 else 0.)
     img = torch.sqrt(feat / torch.clamp(feat.max(), min=1e-30))
-    width = mesh['xFin'] - mesh['xStart']
-    extra = torch.tensor([invRx, invRz, math.log(energy / 1000.), ap_d / width, math.log(f), math.log(L),
-                          math.log(width * 1e3), math.log(L / f), math.log2(nx)], dtype=torch.float32,
-                         device=torch_dev)
+    wx = mesh['xFin'] - mesh['xStart']
+    wz = mesh['yFin'] - mesh['yStart']
+    shape, dx, dz = ap
+    extra = torch.tensor([invRx, invRz, math.log(energy / 1000.), dx / wx, dz / wz, 1. if shape == 'r' else 0.,
+                          math.log(f), math.log(L), math.log(L / f), math.log(wx * 1e3), math.log(wz * 1e3),
+                          math.log2(nx), math.log2(ny)], dtype=torch.float32, device=torch_dev)
     return torch.cat([img, extra])
 
 
 # ------------------------------------------------------------------------------------------------
 # synthetic wavefronts and beamlines (Gaussian and undulator-like, 1-20 keV, drifts 1-50 m,
-# f 1-30 m, apertures 0.1-2 mm)
+# f 1-30 m, circular and rectangular apertures 0.1-2 mm)
 # ------------------------------------------------------------------------------------------------
 def sample_case(rng, n=None):
     if n is None:
-        n = 256 if rng.random() < 0.5 else 512
+        u = rng.random()
+        n = 256 if u < 0.45 else (512 if u < 0.9 else 1024)
     E = math.exp(rng.uniform(math.log(1000.), math.log(20000.)))
     lam = 1.239842e-06 / E
     z = math.exp(rng.uniform(math.log(5.), math.log(50.)))              # source -> first element
     if rng.random() < 0.5:
-        sig0 = math.exp(rng.uniform(math.log(5e-6), math.log(60e-6)))     # waist rms
-        zr = 4. * math.pi * sig0 * sig0 / lam
-        sig = sig0 * math.sqrt(1. + (z / zr) ** 2)
-        R = z * (1. + (zr / z) ** 2)
-        r = 4. * sig
-        x = np.linspace(-r, r, n)
-        X, Y = np.meshgrid(x, x)
-        ex = np.exp(-(X * X + Y * Y) / (4. * sig * sig)) * np.exp(1j * math.pi * (X * X + Y * Y) / (lam * R))
+        sx0 = math.exp(rng.uniform(math.log(5e-6), math.log(60e-6)))       # waist rms, x
+        sz0 = sx0 * math.exp(rng.uniform(-0.5, 0.5))                       # and z
+        def prop(s0):
+            zr = 4. * math.pi * s0 * s0 / lam
+            return s0 * math.sqrt(1. + (z / zr) ** 2), z * (1. + (zr / z) ** 2)
+        (sx, Rx), (sz, Rz) = prop(sx0), prop(sz0)
+        rx, rz = 4. * sx, 4. * sz
+        x, y = np.linspace(-rx, rx, n), np.linspace(-rz, rz, n)
+        X, Y = np.meshgrid(x, y)
+        ex = np.exp(-X * X / (4. * sx * sx) - Y * Y / (4. * sz * sz)) * \
+            np.exp(1j * math.pi * (X * X / Rx + Y * Y / Rz) / lam)
         kind = 'gaussian'
     else:
         nper = int(rng.integers(40, 200))
-        r = z * math.sqrt(3. * lam / (nper * 0.02)) * rng.uniform(0.8, 1.6)   # ~ a few rings of the harmonic
-        x = np.linspace(-r, r, n)
-        X, Y = np.meshgrid(x, x)
+        rx = z * math.sqrt(3. * lam / (nper * 0.02)) * rng.uniform(0.8, 1.6)   # ~ a few rings of the harmonic
+        rz = rx * math.exp(rng.uniform(-0.3, 0.3))
+        x, y = np.linspace(-rx, rx, n), np.linspace(-rz, rz, n)
+        X, Y = np.meshgrid(x, y)
         th2 = (X * X + Y * Y) / (z * z)
         q = th2 * nper * 0.02 / (2. * lam)                              # detuning of the first harmonic
         ex = np.sinc(q) * np.exp(-1j * math.pi * q) * np.exp(1j * math.pi * (X * X + Y * Y) / (lam * z))
-        R = z
+        Rx = Rz = z
         kind = 'undulator'
     ex = (ex * 1e6).astype(np.complex64)
     ey = np.zeros_like(ex)
-    mesh = dict(nx=n, ny=n, xStart=-r, xFin=r, yStart=-r, yFin=r, eStart=E, eFin=E, zStart=z)
-    sc = dict(Rx=R, Ry=R, dRx=0.01 * R, dRy=0.01 * R)
-    ap_d = min(2e-3, max(1e-4, 2. * r * rng.uniform(0.3, 0.9)))
+    mesh = dict(nx=n, ny=n, xStart=-rx, xFin=rx, yStart=-rz, yFin=rz, eStart=E, eFin=E, zStart=z)
+    sc = dict(Rx=Rx, Ry=Rz, dRx=0.01 * Rx, dRy=0.01 * Rz)
+    if rng.random() < 0.5:
+        d = min(2e-3, max(1e-4, 2. * min(rx, rz) * rng.uniform(0.3, 0.9)))
+        ap = ('c', d, d)
+    else:
+        ap = ('r', min(2e-3, max(1e-4, 2. * rx * rng.uniform(0.3, 0.9))),
+              min(2e-3, max(1e-4, 2. * rz * rng.uniform(0.3, 0.9))))
     f = math.exp(rng.uniform(math.log(1.), math.log(30.)))
     L = f * math.exp(rng.uniform(-0.3, 0.3))
     L = min(50., max(1., L))
-    return dict(kind=kind, ex=ex, ey=ey, mesh=mesh, sc=sc, E=E, ap_d=ap_d, f=f, L=L)
+    return dict(kind=kind, ex=ex, ey=ey, mesh=mesh, sc=sc, E=E, ap=ap, f=f, L=L, drift_mode=4)
 
 
-def beamline(mod, ap_d, f, L, rng_f, res_f):
-    """aperture -> (resize) lens -> drift to the waist, as the undulator benchmark beamline."""
-    pp = lambda anal=0, pxm=1., pxd=1.: [0, 0, 1., anal, 0, pxm, pxd, pxm, pxd, 0, 0, 0]  # noqa: E731
-    return mod.SRWLOptC([mod.SRWLOptA('c', 'a', ap_d, ap_d), mod.SRWLOptL(f, f), mod.SRWLOptD(L)],
-                        [pp(), pp(0, rng_f, res_f), pp(4)])
+def bench_case(ex, ey, mesh, sc, ap_d=0.8e-3, f=10., L=10.):
+    """The undulator benchmark beamline's wavefront and elements as a case of this module."""
+    return dict(kind='undulator', ex=ex, ey=ey, mesh=mesh, sc=sc, E=mesh['eStart'], ap=('c', ap_d, ap_d), f=f, L=L,
+                drift_mode=4)
+
+
+def beamline(mod, ap, f, L, fac, drift_mode=4):
+    """aperture -> (resize fac = (pxm, pxd, pzm, pzd)) lens -> drift (to the waist by default)."""
+    pp = lambda anal=0, fc=(1., 1., 1., 1.): [0, 0, 1., anal, 0, fc[0], fc[1], fc[2], fc[3], 0, 0, 0]  # noqa: E731
+    return mod.SRWLOptC([mod.SRWLOptA(ap[0], 'a', ap[1], ap[2]), mod.SRWLOptL(f, f), mod.SRWLOptD(L)],
+                        [pp(), pp(0, tuple(fac)), pp(drift_mode)])
 
 
 def _wfr(mod, case):
     w = mod.SRWLWfr()
     n = case['mesh']['nx']
-    w.allocate(1, n, n)
+    w.allocate(1, n, case['mesh']['ny'])
     for name, fld in (('arEx', case['ex']), ('arEy', case['ey'])):
         a = np.empty(2 * fld.size, np.float32)
         a[0::2] = fld.real.ravel()
@@ -287,31 +323,6 @@ def _wfr(mod, case):
         setattr(w.mesh, k, case['mesh'][k])
     w.Rx, w.Ry, w.dRx, w.dRy = case['sc']['Rx'], case['sc']['Ry'], case['sc']['dRx'], case['sc']['dRy']
     return w
-
-
-def _interp_bilinear(I, om, em, torch):
-    """I (torch float64 [ny, nx] on mesh om) at the points of mesh em (bilinear, zero outside)."""
-    ny, nx = I.shape
-    xs = (om['xFin'] - om['xStart']) / (nx - 1)
-    ys = (om['yFin'] - om['yStart']) / (ny - 1)
-    xa = em['xStart'] + torch.arange(em['nx'], dtype=torch.float64, device=I.device) * (em['xFin'] - em['xStart']) / (em['nx'] - 1)
-    ya = em['yStart'] + torch.arange(em['ny'], dtype=torch.float64, device=I.device) * (em['yFin'] - em['yStart']) / (em['ny'] - 1)
-    fx = (xa - om['xStart']) / xs
-    fy = (ya - om['yStart']) / ys
-    ix = torch.floor(fx).long()
-    iy = torch.floor(fy).long()
-    okx = (ix >= 0) & (ix < nx - 1)
-    oky = (iy >= 0) & (iy < ny - 1)
-    ix = ix.clamp(0, nx - 2)
-    iy = iy.clamp(0, ny - 2)
-    tx = (fx - ix).unsqueeze(0)
-    ty = (fy - iy).unsqueeze(1)
-    a = I[iy][:, ix]
-    b = I[iy][:, ix + 1]
-    c = I[iy + 1][:, ix]
-    d = I[iy + 1][:, ix + 1]
-    v = a * (1 - tx) * (1 - ty) + b * tx * (1 - ty) + c * (1 - tx) * ty + d * tx * ty
-    return v * (oky.unsqueeze(1) & okx.unsqueeze(0))
 
 
 def _interp_cubic(I, om, em, torch):
@@ -343,17 +354,18 @@ def _interp_cubic(I, om, em, torch):
     return out * (oky.unsqueeze(1) & okx.unsqueeze(0))
 
 
-def propagate_intensity(case, rf, df, dev):
-    """Plain GPU propagation with factors (rf, df): (total intensity [ny, nx] float64 CUDA, mesh)."""
+def propagate_intensity(case, fac, dev, stream=None):
+    """Plain GPU propagation with factors fac = (pxm, pxd, pzm, pzd): (total intensity [ny, nx]
+    float64 CUDA, mesh)."""
     import torch
     from . import srwlib as mod
     from .plan import Plan
     w = _wfr(mod, case)
-    p = Plan(w, beamline(mod, case['ap_d'], case['f'], case['L'], rf, df), device=dev.index)
+    p = Plan(w, beamline(mod, case['ap'], case['f'], case['L'], fac, case.get('drift_mode', 4)), device=dev.index)
     ex = torch.from_numpy(case['ex']).to(dev)
     ey = torch.from_numpy(case['ey']).to(dev)
     ox, oy = p.new_output()
-    p.execute(ex, ey, ox, oy)
+    p.execute(ex, ey, ox, oy, stream)
     I = (ox.real.double() ** 2 + ox.imag.double() ** 2 + oy.real.double() ** 2 + oy.imag.double() ** 2)
     return I, p.output_mesh()
 
@@ -372,8 +384,7 @@ def eval_box(I_ref, om):
 
 def factor_error(I, om, I_ref, om_ref, box):
     """Relative L2 intensity error of a propagation at its own output nodes inside `box`, against
-    the oversampled reference interpolated to those nodes by cubic Lagrange interpolation (its
-    finer mesh and the fourth-order interpolation keep that error well below the tolerance); 1 when
+    the reference propagation interpolated to those nodes by cubic Lagrange interpolation; 1 when
     the output window does not cover the box."""
     import torch
     x0, x1, y0, y1 = box
@@ -393,30 +404,115 @@ def factor_error(I, om, I_ref, om_ref, box):
     return float(torch.linalg.norm(c - ref) / torch.linalg.norm(ref))
 
 
-def label_case(case, dev):
-    """Sweep of the candidate factor pairs against the oversampled propagation: returns
-    (best (rf, df): the cheapest by grid_cost within TOL_LABEL, errors [len(GRID), len(GRID)])."""
+# ------------------------------------------------------------------------------------------------
+# cost model: autotuned per-length pass times (srw_b200.tune), per point
+# ------------------------------------------------------------------------------------------------
+_TIMES = None
+
+
+def _times():
+    global _TIMES
+    if _TIMES is None:
+        from . import tune
+        _TIMES = tune.load_times()
+    return _TIMES
+
+
+def new_length(n, rf, df):
+    """Resized number of points: round-half-up of n rf df (RadResizeGen), then the next good FFT
+    number (NextCorrectNumberForFFT, gmfft.cpp:156), n itself when both factors are within 1e-4 of 1."""
+    if abs(rf - 1.) < 1e-4 and abs(df - 1.) < 1e-4:
+        return n
+    return int(capi.lib().srwgNextFftNumber(int(math.floor(n * rf * df + 0.5))))
+
+
+def point_costs(n):
+    """(row, column) pass time per point [ms] of length n from the tuning table: measured where it
+    has the length, else the largest measured per-point time of the neighbouring lengths times 3
+    (the run-time-scheduled kernel)."""
+    t = _times()
+    if n in t:
+        return t[n][0] / (n * n), t[n][1] / (n * n)
+    if not t:
+        return (1., 1.) if (n & (n - 1)) == 0 else (5., 5.)
+    near = sorted(t, key=lambda m: abs(math.log(m / n)))[:3]
+    return (3. * max(t[m][0] / (m * m) for m in near), 3. * max(t[m][1] / (m * m) for m in near))
+
+
+def grid_cost(nx, nz, fac):
+    """Modelled time of propagating an nx x nz wavefront with factors fac: the row and column
+    passes on the resized grid (per-point times of its lengths) plus the resize (proportional to
+    the points written, at the row-pass rate)."""
+    mx, mz = new_length(nx, fac[0], fac[1]), new_length(nz, fac[2], fac[3])
+    r, _ = point_costs(mx)
+    _, c = point_costs(mz)
+    return mx * mz * (r + c) + mx * mz * r
+
+
+def _pairs():
+    return [(float(r), float(d)) for r in GRID_R for d in GRID_D]
+
+
+def choose_grid(pred, nx, nz):
+    """Prediction (log2 of pxm, pxd, pzm, pzd) -> the cheapest grid factors (grid_cost) with every
+    factor not below the prediction (per axis)."""
+    lo = [2. ** float(v) - 1e-6 for v in pred]
+    px = [p for p in _pairs() if p[0] >= lo[0] and p[1] >= lo[1]] or [CONSERVATIVE[:2]]
+    pz = [p for p in _pairs() if p[0] >= lo[2] and p[1] >= lo[3]] or [CONSERVATIVE[2:]]
+    best, bc = CONSERVATIVE, None
+    for a in px:
+        for b in pz:
+            c = grid_cost(nx, nz, a + b)
+            if bc is None or c < bc:
+                best, bc = tuple(a) + tuple(b), c
+    return best
+
+
+# ------------------------------------------------------------------------------------------------
+# labels
+# ------------------------------------------------------------------------------------------------
+def label_case(case, dev, stream=None):
+    """Cheapest factors (pxm, pxd, pzm, pzd) within tolerance of the oversampled propagation: per
+    axis the candidate pairs in order of the resized length (the other axis at the conservative
+    factors), the first within AXIS_TOL; the combination is checked against TOL_LABEL and replaced
+    by the conservative factors when it fails.  Returns (factors, error of the label, evaluations)."""
     n = case['mesh']['nx']
-    Iref, omref = propagate_intensity(case, *REF_FACTORS, dev)
+    rf = ref_factors(n)
+    Iref, omref = propagate_intensity(case, rf + rf, dev, stream)
     box = eval_box(Iref, omref)
-    errs = np.full((len(GRID), len(GRID)), np.inf)
-    best, best_cost = CONSERVATIVE, None
-    for i, rf in enumerate(GRID):
-        for j, df in enumerate(GRID):
-            I, om = propagate_intensity(case, rf, df, dev)
-            e = factor_error(I, om, Iref, omref, box)
-            errs[i, j] = e
-            cost = grid_cost(n, rf, df)
-            if e <= TOL_LABEL and (best_cost is None or cost < best_cost):
-                best, best_cost = (rf, df), cost
-    return best, errs
+    cache = {}
+
+    def err(fac):
+        if fac not in cache:
+            I, om = propagate_intensity(case, fac, dev, stream)
+            cache[fac] = factor_error(I, om, Iref, omref, box)
+        return cache[fac]
+
+    best = []
+    for axis in (0, 1):
+        nn = case['mesh']['nx'] if axis == 0 else case['mesh']['ny']
+        cands = sorted(_pairs(), key=lambda p: (new_length(nn, *p), p[1], p[0]))
+        pick = CONSERVATIVE[:2]
+        for p in cands:
+            if new_length(nn, *p) >= new_length(nn, 2., 2.):
+                break
+            fac = (p + CONSERVATIVE[2:]) if axis == 0 else (CONSERVATIVE[:2] + p)
+            if err(fac) <= AXIS_TOL:
+                pick = p
+                break
+        best.append(tuple(pick))
+    lab = best[0] + best[1]
+    e = err(lab)
+    if e > TOL_LABEL:
+        lab, e = CONSERVATIVE, err(CONSERVATIVE)
+    return lab, e, len(cache) + 1
 
 
 def case_features(case, dev):
     import torch
     ex = torch.from_numpy(case['ex']).to(dev)
     ey = torch.from_numpy(case['ey']).to(dev)
-    return features(ex, ey, case['mesh'], case['E'], case['ap_d'], case['f'], case['L'], dev, case['sc']['Rx'],
+    return features(ex, ey, case['mesh'], case['E'], case['ap'], case['f'], case['L'], dev, case['sc']['Rx'],
                     case['sc']['Ry'])
 
 
@@ -424,114 +520,166 @@ def target(factors):
     return np.log2(np.array(factors, np.float32))
 
 
-GENERAL_COST = 5.0     # per-point time of a general-length (not power-of-two) grid relative to a power of two
+# ------------------------------------------------------------------------------------------------
+# run time
+# ------------------------------------------------------------------------------------------------
+def _common_error(I, om, I_c, om_c):
+    """Relative L2 of intensity I (mesh om) against I_c (mesh om_c, the conservative propagation)
+    at om's nodes inside the box where I_c exceeds 1e-3 of its maximum."""
+    return factor_error(I, om, I_c, om_c, eval_box(I_c, om_c))
 
 
-def grid_cost(n, rf, df):
-    """Cost model of propagating an n x n wavefront with factors (rf, df): points of the resized
-    grid (round-half-up of n rf df, as RadResizeGen) times GENERAL_COST when that size is not a power
-    of two (measured: the general-length passes take about five times longer per point)."""
-    m = int(math.floor(n * rf * df + 0.5))
-    return float(m) * m * (1. if (m & (m - 1)) == 0 else GENERAL_COST)
-
-
-def choose_grid(pred, n):
-    """Prediction (log2 factors) -> the cheapest grid pair (grid_cost) with both factors not below it."""
-    lo = [2. ** float(v) - 1e-6 for v in pred]
-    best, best_cost = (float(GRID[-1]), float(GRID[-1])), None
-    for rf in GRID:
-        for df in GRID:
-            if rf >= lo[0] and df >= lo[1]:
-                c = grid_cost(n, rf, df)
-                if best_cost is None or c < best_cost:
-                    best, best_cost = (float(rf), float(df)), c
-    return best
-
-
-def round_up(pred):
-    """Prediction (log2 factors) -> the smallest grid factors not below it."""
-    out = []
-    for v in pred:
-        f = 2. ** float(v)
-        cand = GRID[GRID >= f - 1e-6]
-        out.append(float(cand[0]) if len(cand) else float(GRID[-1]))
-    return tuple(out)
-
-
-def output_check(I):
-    """Run-time check of a propagation with predicted factors: the fraction of the intensity in
-    the outer eighth of the output window on each side (aliasing / clipping indicator)."""
-    ny, nx = I.shape
-    b = max(1, nx // 8), max(1, ny // 8)
-    tot = float(I.sum())
-    inner = float(I[b[1]:ny - b[1], b[0]:nx - b[0]].sum())
-    return (tot - inner) / tot if tot > 0 else 1.
-
-
-def choose_factors(model, case, dev, check_tol=1e-3):
-    """(factors, used_fallback): the model's factors when the propagation with them passes
-    output_check, else the conservative ones."""
+def choose_factors(model, case, dev, check_tol=TOL_LABEL):
+    """(factors, used_fallback, check_error): the network's factors, rounded up to the grid, when
+    the wavefront propagated with them agrees with its propagation at the conservative factors
+    within check_tol; else the conservative factors."""
     feat = case_features(case, dev).unsqueeze(0)
     pred = model.predict(feat)[0].cpu().numpy()
-    fac = choose_grid(pred, case['mesh']['nx'])
-    I, _ = propagate_intensity(case, *fac, dev)
-    if output_check(I) > check_tol:
-        return CONSERVATIVE, True
-    return fac, False
+    fac = choose_grid(pred, case['mesh']['nx'], case['mesh']['ny'])
+    if tuple(fac) == tuple(CONSERVATIVE):
+        return CONSERVATIVE, False, 0.
+    I, om = propagate_intensity(case, fac, dev)
+    Ic, omc = propagate_intensity(case, CONSERVATIVE, dev)
+    e = _common_error(I, om, Ic, omc)
+    if e > check_tol:
+        return CONSERVATIVE, True, e
+    return tuple(fac), False, e
+
+
+class CheckedMultiE(object):
+    """Multi-electron propagation (srw_b200.multie.MultiE) with learned factors and a run-time check
+    per batch: the first electron of every batch is also propagated with the conservative factors;
+    when the two intensities on the common mesh differ by more than `tol` (relative L2 where the
+    conservative one exceeds 1e-3 of its maximum) the batch runs with the conservative factors.
+    Both paths add into one FP64 accumulator (a torch tensor); ``mean()`` divides by the electrons
+    added."""
+
+    def __init__(self, base_wfr, make_beamline, factors, acc_mesh, max_batch=64, safe_batch=16, graph=True,
+                 device=0, tol=TOL_LABEL):
+        import torch
+        from .multie import MultiE
+        self.torch = torch
+        self.dev = torch.device('cuda', device)
+        self.acc = torch.zeros((acc_mesh['ny'], acc_mesh['nx']), dtype=torch.float64, device=self.dev)
+        self.chk = [torch.zeros_like(self.acc), torch.zeros_like(self.acc)]
+        self.fast = MultiE(base_wfr, make_beamline(factors), acc_mesh, max_batch=max_batch, graph=graph, device=device)
+        self.safe = MultiE(base_wfr, make_beamline(CONSERVATIVE), acc_mesh, max_batch=safe_batch, graph=graph,
+                           device=device)
+        self.cfast = MultiE(base_wfr, make_beamline(factors), acc_mesh, max_batch=1, graph=False, device=device)
+        self.csafe = MultiE(base_wfr, make_beamline(CONSERVATIVE), acc_mesh, max_batch=1, graph=False, device=device)
+        self.fast.use_accumulator(self.acc.data_ptr())
+        self.safe.use_accumulator(self.acc.data_ptr())
+        self.cfast.use_accumulator(self.chk[0].data_ptr())
+        self.csafe.use_accumulator(self.chk[1].data_ptr())
+        self.max_batch, self.tol = max_batch, tol
+        self.n, self.batches, self.fallbacks, self.check_errors = 0, 0, 0, []
+
+    def add(self, offsets, stream=None):
+        from .multie import offset_array
+        off = offset_array(offsets)
+        for i0 in range(0, len(off), self.max_batch):
+            b = off[i0:i0 + self.max_batch]
+            for c in self.chk:
+                c.zero_()
+            self.cfast.add(b[:1], stream)
+            self.csafe.add(b[:1], stream)
+            ref = self.chk[1]
+            sel = ref > 1e-3 * ref.max()
+            e = float(self.torch.linalg.norm((self.chk[0] - ref)[sel]) / self.torch.linalg.norm(ref[sel]))
+            self.check_errors.append(e)
+            (self.fast if e <= self.tol else self.safe).add(b, stream)
+            self.fallbacks += e > self.tol
+            self.batches += 1
+            self.n += len(b)
+
+    def mean(self):
+        self.torch.cuda.synchronize(self.dev)
+        return (self.acc / max(self.n, 1)).cpu().numpy()
+
+
+# ------------------------------------------------------------------------------------------------
+# training
+# ------------------------------------------------------------------------------------------------
+def make_data(n_samples, seed, dev, threads=8, log=print):
+    """Features, targets, label errors and evaluation counts of n_samples seeded cases, labelled on
+    `threads` host threads (each with its own CUDA stream: the planner runs on the host)."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    X = np.zeros((n_samples, N_IN), np.float32)
+    T = np.zeros((n_samples, N_OUT), np.float32)
+    E = np.zeros(n_samples)
+    NE = np.zeros(n_samples, np.int32)
+    t0 = time.time()
+    done = [0]
+    lock = threading.Lock()
+    local = threading.local()
+
+    def one(s):
+        if not hasattr(local, 'stream'):
+            local.stream = torch.cuda.Stream(dev)
+        rng = np.random.default_rng([seed, s])
+        case = sample_case(rng)
+        with torch.cuda.stream(local.stream):
+            X[s] = case_features(case, dev).cpu().numpy()
+            lab, e, ne = label_case(case, dev, local.stream)
+        T[s], E[s], NE[s] = target(lab), e, ne
+        with lock:
+            done[0] += 1
+            if done[0] % 500 == 0:
+                log('labelled %d (%.0f s)' % (done[0], time.time() - t0))
+
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(one, range(n_samples)))
+    return X, T, E, NE
 
 
 def main():
     import torch
     ap = argparse.ArgumentParser()
-    ap.add_argument('--samples', type=int, default=2000)
-    ap.add_argument('--val', type=float, default=0.15)
-    ap.add_argument('--epochs', type=int, default=300)
+    ap.add_argument('--samples', type=int, default=20000)
+    ap.add_argument('--val', type=float, default=0.1)
+    ap.add_argument('--epochs', type=int, default=200)
     ap.add_argument('--seed', type=int, default=0)
+    ap.add_argument('--threads', type=int, default=8)
     ap.add_argument('--out', default=DEFAULT_MODEL)
-    ap.add_argument('--data', default=None, help='npz with features/targets to reuse')
+    ap.add_argument('--data', default=None, help='npz with features/targets to reuse or to write')
     args = ap.parse_args()
     dev = torch.device('cuda', 0)
     t0 = time.time()
     if args.data and os.path.exists(args.data):
         d = np.load(args.data)
-        X, T, errs = d['X'], d['T'], d['errs']
+        X, T, E, NE = d['X'], d['T'], d['E'], d['NE']
     else:
-        rng = np.random.default_rng(args.seed)
-        X = np.zeros((args.samples, N_IN), np.float32)
-        T = np.zeros((args.samples, 2), np.float32)
-        errs = np.zeros((args.samples, len(GRID), len(GRID)))
-        for s in range(args.samples):
-            case = sample_case(rng)
-            X[s] = case_features(case, dev).cpu().numpy()
-            best, e = label_case(case, dev)
-            T[s] = target(best)
-            errs[s] = e
-            if s % 100 == 0:
-                print('sample %d (%.0f s)' % (s, time.time() - t0), flush=True)
+        X, T, E, NE = make_data(args.samples, args.seed, dev, args.threads)
         if args.data:
-            np.savez_compressed(args.data, X=X, T=T, errs=errs)
+            np.savez_compressed(args.data, X=X, T=T, E=E, NE=NE)
+    t_data = time.time() - t0
     nv = int(len(X) * args.val)
     Xt, Tt = torch.from_numpy(X[nv:]).to(dev), torch.from_numpy(T[nv:]).to(dev)
     Xv, Tv = torch.from_numpy(X[:nv]).to(dev), torch.from_numpy(T[:nv]).to(dev)
     m = ResizeMLP(device=0, seed=args.seed)
     hist = m.train(Xt, Tt, Xv, Tv, epochs=args.epochs, log=print)
-    # validation: chosen factors against the sweep errors; cost relative to the conservative factors
+    # validation: chosen factors vs labels, cost relative to the conservative factors (cost model)
     pred = m.predict(Xv).cpu().numpy()
-    ok, cost_pred, cost_label = 0, 0., 0.
+    cost_pred = cost_label = 0.
+    at_least_label = 0
     for i in range(nv):
-        n = int(round(2. ** float(X[i, N_IMG + 8])))
-        fac = choose_grid(pred[i], n)
-        a, b = int(np.argmin(np.abs(GRID - fac[0]))), int(np.argmin(np.abs(GRID - fac[1])))
-        ok += errs[i, a, b] <= TOL_LABEL
-        c2 = grid_cost(n, *CONSERVATIVE)
-        cost_pred += grid_cost(n, *fac) / c2
-        lab = 2. ** T[i]
-        cost_label += grid_cost(n, float(lab[0]), float(lab[1])) / c2
+        n = int(round(2. ** float(X[i, N_IMG + 11])))
+        fac = choose_grid(pred[i], n, n)
+        lab = tuple(float(v) for v in 2. ** T[i])
+        c2 = grid_cost(n, n, CONSERVATIVE)
+        cost_pred += grid_cost(n, n, fac) / c2
+        cost_label += grid_cost(n, n, lab) / c2
+        at_least_label += all(new_length(n, fac[2 * a], fac[2 * a + 1]) >= new_length(n, lab[2 * a], lab[2 * a + 1])
+                              for a in (0, 1))
     meta = dict(samples=int(len(X)), val=int(nv), epochs=int(args.epochs), final_train=float(hist[-1][1]),
-                final_val=float(hist[-1][2]), val_within_tol=float(ok) / max(nv, 1),
+                final_val=float(hist[-1][2]), val_grid_at_least_label=float(at_least_label) / max(nv, 1),
                 val_cost_pred=float(cost_pred) / max(nv, 1), val_cost_label=float(cost_label) / max(nv, 1),
-                cost_conservative=1.0, cost_model='grid_cost, relative to the conservative factors',
-                general_cost=GENERAL_COST, tol=TOL_LABEL, seconds=float(time.time() - t0))
+                labels_conservative=float(np.mean(np.all(np.abs(T - 1.) < 1e-6, axis=1))),
+                mean_evaluations_per_label=float(np.mean(NE)), cost_conservative=1.0,
+                cost_model='grid_cost: autotuned per-length pass times, relative to the conservative factors',
+                tol=TOL_LABEL, axis_tol=AXIS_TOL, grid_range=GRID_R.tolist(), grid_resolution=GRID_D.tolist(),
+                seconds_data=float(t_data), seconds=float(time.time() - t0))
     m.save(args.out, meta)
     print(json.dumps(meta))
 

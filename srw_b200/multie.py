@@ -41,6 +41,45 @@ def shard(n_total, rank, world):
     return np.arange(rank, n_total, world, dtype=np.int64)
 
 
+def shard_offsets(n_total, rank, world, sig_x, sig_xp, sig_y, sig_yp, seed=0, sig_e=None):
+    """Offsets of this rank's electrons (``shard``) out of n_total: [len(shard), 4 or 5], electron k
+    drawn exactly as ``sample_offsets`` draws it, so the union over ranks is the single-process set."""
+    idx = shard(n_total, rank, world)
+    m = 4 if sig_e is None else 5
+    out = np.empty((len(idx), m), np.float64)
+    for j, k in enumerate(idx):
+        out[j] = sample_offsets(1, sig_x, sig_xp, sig_y, sig_yp, seed=seed, first=int(k), sig_e=sig_e)[0]
+    return out
+
+
+def allreduce_mean(acc, n_local, group=None):
+    """Mean intensity over all ranks: sums the ranks' FP64 intensity accumulators (a torch tensor,
+    in place; NCCL for CUDA tensors, gloo for CPU ones) and their electron counts with one
+    all-reduce each, and returns (acc / n_total, n_total).  Every rank calls it, in the same order
+    as its other collectives."""
+    import torch
+    import torch.distributed as dist
+    cnt = torch.tensor([float(n_local)], dtype=torch.float64, device=acc.device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.all_reduce(acc, group=group)
+        dist.all_reduce(cnt, group=group)
+    n = int(round(float(cnt.item())))
+    return (acc / n if n > 0 else acc.clone()), n
+
+
+def offset_array(offsets, ncols=None):
+    """Electron offsets as a contiguous [n, 4] or [n, 5] float64 array.  A 2-D array gives its own
+    column count (ncols, when given, must agree); a flat array is split into rows of ncols values
+    and is refused without ncols, since its length alone does not tell 4 from 5 values per electron."""
+    a = np.asarray(offsets, np.float64)
+    if a.ndim == 2 and a.shape[1] in (4, 5) and ncols in (None, a.shape[1]):
+        return np.ascontiguousarray(a)
+    if a.ndim == 1 and ncols in (4, 5) and a.size % ncols == 0:
+        return np.ascontiguousarray(a).reshape(-1, ncols)
+    raise ValueError('electron offsets: an [n, 4] or [n, 5] array, or a flat array with ncols = 4 or 5 dividing its '
+                     'length (got shape %s, ncols %s)' % (a.shape, ncols))
+
+
 def _mesh_struct(m):
     """SRWLRadMesh from a dict or an object with the reference's mesh attribute names."""
     s = capi.SRWLRadMesh()
@@ -64,11 +103,11 @@ class MultiE(object):
         self._h = h
         self.nx, self.ny = int(self._accm.nx), int(self._accm.ny)
 
-    def add(self, offsets, stream=None):
-        """offsets: [n, 4] (x, x', y, y') or [n, 5] with the relative energy deviation."""
-        a = np.asarray(offsets, np.float64)
-        m = a.shape[-1] if a.ndim == 2 and a.shape[-1] in (4, 5) else 4
-        off = np.ascontiguousarray(a).reshape(-1, m)
+    def add(self, offsets, stream=None, ncols=None):
+        """offsets: [n, 4] (x, x', y, y') or [n, 5] with the relative energy deviation; a flat
+        array needs ncols (4 or 5).  All electrons of a call are added, or none (on an error)."""
+        off = offset_array(offsets, ncols)
+        m = off.shape[1]
         st = C.c_void_p(stream) if stream else None
         f = capi.lib().srwgMultiEAddE if m == 5 else capi.lib().srwgMultiEAdd
         capi.check(f(self._h, int(off.shape[0]), off.ctypes.data, st), 'multi-electron add')

@@ -1,0 +1,183 @@
+"""Autotuner of the FFT line passes' launch shapes (the reference has none: FFTW plans per call,
+gmfft.cpp:295; its CUDA build caches cuFFT plans, gmfft.h:182-187).
+
+For every line length with a compile-time kernel (powers of two and the general lengths of
+csrc/linen_lengths.h) it times the two passes of an N x N propagation to the waist (a row pass and
+a column pass, the headline beamline's FFT) for every valid number of lines per CTA of each pass
+-- which is also the CTA size and, for the column pass, the width of the column blocks the row pass
+writes -- with CUDA events on the launching stream and L2 flushed between repetitions, keeps the
+fastest pair and writes
+
+  models/line_tuning.txt    "rows|cols N L" lines, read by the library at its first plan
+  models/line_tuning.json   every measurement (ms per pass), read by the learned-factor cost model
+
+    python -m srw_b200.tune [--lengths 1280,2240] [--reps 7]          # GPU
+
+torch supplies device memory, streams and events only.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import time
+
+import numpy as np
+
+from . import capi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TXT = os.path.join(HERE, 'models', 'line_tuning.txt')
+JSN = os.path.join(HERE, 'models', 'line_tuning.json')
+LENGTHS_H = os.path.join(HERE, 'csrc', 'linen_lengths.h')
+SMEM_MAX = 220 * 1024
+
+
+def general_lengths():
+    return [int(v) for v in re.findall(r'X\((\d+)\)', open(LENGTHS_H).read())]
+
+
+def all_lengths(lo=256, hi=8192):
+    p2 = [1 << k for k in range(8, 14) if lo <= (1 << k) <= hi]
+    return sorted(set(p2 + [n for n in general_lengths() if lo <= n <= hi]))
+
+
+def is_pow2(n):
+    return n & (n - 1) == 0
+
+
+def candidates(axis, n):
+    """Valid lines per CTA (the library's fixed_lines_valid): shared memory, threads per CTA (1024
+    for powers of two, 512 for general lengths), columns a power of two up to 32."""
+    t = n // 16 if is_pow2(n) else (n + 15) // 16
+    tmax = 1024 if is_pow2(n) else 512
+    p = n + n // 16 + 4
+    out = []
+    for L in range(1, 33):
+        if L * p * 8 > SMEM_MAX or t * L > tmax:
+            break
+        if axis == 1 and (L & (L - 1)):
+            continue
+        if axis == 0 and L > 8:
+            break
+        out.append(L)
+    return out
+
+
+def _plan(n, dev):
+    """N x N Gaussian (2 keV, curved) through a 10 m drift to the waist: one row and one column pass."""
+    from . import srwlib as S
+    from .plan import Plan
+    r = 1.5e-3
+    w = S.SRWLWfr()
+    w.allocate(1, n, n)
+    x = np.linspace(-r, r, n)
+    X, Y = np.meshgrid(x, x)
+    ex = (np.exp(-(X * X + Y * Y) / (4. * (0.4e-3) ** 2)) * 1e6).astype(np.complex64)
+    a = np.empty(2 * n * n, np.float32)
+    a[0::2], a[1::2] = ex.real.ravel(), ex.imag.ravel()
+    w.arEx, w.arEy = a, a.copy()
+    w.mesh.xStart, w.mesh.xFin, w.mesh.yStart, w.mesh.yFin = -r, r, -r, r
+    w.mesh.eStart = w.mesh.eFin = 2012.
+    w.Rx = w.Ry = 20.
+    w.dRx = w.dRy = 0.2
+    opt = S.SRWLOptC([S.SRWLOptD(10.)], [[0, 0, 1., 4, 0, 1., 1., 1., 1., 0, 0, 0]])
+    return Plan(w, opt, device=dev.index), ex
+
+
+def time_passes(n, Lr, Lc, dev, reps=7, flush=None):
+    """Median CUDA-event time [ms] of the row and the column pass with Lr / Lc lines per CTA."""
+    import torch
+    L = capi.lib()
+    capi.check(L.srwgTuneSetLines(0, n, Lr), 'tune rows')
+    capi.check(L.srwgTuneSetLines(1, n, Lc), 'tune cols')
+    p, ex = _plan(n, dev)
+    kinds = [k[0] for k in p.kernels()]
+    if kinds != ['line_rows', 'line_cols']:
+        raise RuntimeError('unexpected passes %s' % kinds)
+    a = torch.from_numpy(ex).to(dev)
+    b = a.clone()
+    ox, oy = p.new_output()
+    st = torch.cuda.current_stream(dev)
+    for _ in range(2):
+        p.execute(a, b, ox, oy)
+    ms = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.fill_(1)
+        ms.append(p.execute_timed(a, b, ox, oy, st))
+    torch.cuda.synchronize(dev)
+    m = np.median(np.array(ms), 0)
+    return float(m[0]), float(m[1])
+
+
+def tune(lengths, dev, reps=7, log=print):
+    import torch
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)      # > L2 (126 MB)
+    L = capi.lib()
+    res = {}
+    for n in lengths:
+        t0 = time.time()
+        rows_c, cols_c = candidates(0, n), candidates(1, n)
+        meas = []
+        for Lc in cols_c:
+            for Lr in rows_c:
+                tr, tc = time_passes(n, Lr, Lc, dev, reps, flush)
+                meas.append((Lr, Lc, tr, tc))
+        # defaults (the library's own choice without a table entry), for the record
+        capi.check(L.srwgTuneSetLines(0, n, 0), 'tune')
+        capi.check(L.srwgTuneSetLines(1, n, 0), 'tune')
+        d = [C.c_int(), C.c_int()]
+        L.srwgTuneGetLines(0, n, C.byref(d[0]))
+        L.srwgTuneGetLines(1, n, C.byref(d[1]))
+        dflt = next((m for m in meas if m[0] == d[0].value and m[1] == d[1].value), None)
+        best = min(meas, key=lambda m: m[2] + m[3])
+        res[n] = dict(rows=best[0], cols=best[1], rows_ms=best[2], cols_ms=best[3],
+                      default=[d[0].value, d[1].value], default_ms=[dflt[2], dflt[3]] if dflt else None,
+                      measured=[list(m) for m in meas])
+        log('N %5d  best rows L=%d %.4f ms  cols L=%d %.4f ms  (default %s: %s)  %.1f s' % (
+            n, best[0], best[2], best[1], best[3], d[0].value, d[1].value,
+            '%.4f + %.4f ms' % (dflt[2], dflt[3]) if dflt else '-', time.time() - t0))
+    return res
+
+
+def write(res, txt=TXT, jsn=JSN, device_name=''):
+    os.makedirs(os.path.dirname(txt), exist_ok=True)
+    with open(txt, 'w') as f:
+        f.write('# lines per CTA of the line passes with compile-time lengths, measured by srw_b200.tune\n')
+        f.write('# on %s (row + column pass of an N x N propagation to the waist, median CUDA-event time)\n'
+                % device_name)
+        for n in sorted(res):
+            r = res[n]
+            f.write('rows %d %d\n' % (n, r['rows']))
+            f.write('cols %d %d\n' % (n, r['cols']))
+    with open(jsn, 'w') as f:
+        json.dump({'device': device_name, 'lengths': {str(n): res[n] for n in sorted(res)}}, f, indent=0)
+
+
+def load_times(jsn=JSN):
+    """{N: (rows ms, cols ms)} of the tuned launch shapes, or {} without a table."""
+    if not os.path.exists(jsn):
+        return {}
+    d = json.load(open(jsn))
+    return {int(n): (v['rows_ms'], v['cols_ms']) for n, v in d.get('lengths', {}).items()}
+
+
+def main():
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--lengths', default='')
+    ap.add_argument('--reps', type=int, default=7)
+    ap.add_argument('--txt', default=TXT)
+    ap.add_argument('--json', default=JSN)
+    args = ap.parse_args()
+    dev = torch.device('cuda', 0)
+    lengths = [int(v) for v in args.lengths.split(',') if v] or all_lengths()
+    capi.lib().srwgTuneLoad(None, None)            # measure from the built-in defaults
+    res = tune(lengths, dev, args.reps)
+    write(res, args.txt, args.json, torch.cuda.get_device_name(dev))
+    print('wrote %s, %s' % (args.txt, args.json))
+
+
+if __name__ == '__main__':
+    main()

@@ -1,6 +1,6 @@
 """Generates the golden fixtures in tests/golden/ by running the reference SRW itself.
 
-Run in a container that has the reference sources (default /root/reference) and the reference
+Run in a container that has the reference sources (--ref, else $SRW_REFERENCE, else /root/reference) and the reference
 built by ``make -C oracle`` (oracle/_ref/srwlpy.so, oracle/_ref/nextfft_probe):
 
     python tests/golden/make_golden.py [--ref /root/reference]
@@ -247,7 +247,7 @@ def no_moments(make):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--ref', default=os.environ.get('SRW_REFERENCE', '/root/reference'))
     a = ap.parse_args()
     L = load_reference(a.ref)
     # 1) good numbers

@@ -80,6 +80,24 @@ def full_case(which):
     return ex, ey, mesh, C2, C2PP, dict(Rx=30., Ry=30., dRx=0.3, dRy=0.3)
 
 
+def phase_err(a, b, rel=1e-3):
+    """Intensity-weighted RMS of the phase difference arg(a conj(b)) [rad] where |b|^2 exceeds `rel`
+    of its maximum."""
+    I = np.abs(b) ** 2
+    sel = I > rel * I.max()
+    d = np.angle(a[sel] * np.conj(b[sel]))
+    return float(np.sqrt(np.sum(I[sel] * d * d) / np.sum(I[sel])))
+
+
+def report(**kv):
+    """Appends the figures of a test to $SRWG_TEST_REPORT (JSON lines) when that is set."""
+    path = os.environ.get('SRWG_TEST_REPORT')
+    if path:
+        import json
+        with open(path, 'a') as f:
+            f.write(json.dumps(kv) + '\n')
+
+
 @pytest.mark.parametrize('which', ['c0', 'c1', 'c2', 'c2q1'])
 def test_full_size_vs_fp64_oracle(which):
     need_gpu()
@@ -92,10 +110,78 @@ def test_full_size_vs_fp64_oracle(which):
     if which == 'c2q1':
         assert moment_err(np.array(w.arMomX), o.momX) < TOL
     gx, gy = fields(w)
-    assert rel_l2(gx, o.ex) < TOL
+    e_field = rel_l2(gx, o.ex)
     I_g = np.abs(gx) ** 2 + np.abs(gy) ** 2
     I_o = np.abs(o.ex) ** 2 + np.abs(o.ey) ** 2
-    assert rel_l2(I_g, I_o) < TOL
+    e_int = rel_l2(I_g, I_o)
+    # phase of Ex against the FP64 oracle (intensity-weighted RMS where the intensity is above 1e-3 of
+    # its maximum): 1e-4 rad, the field bar
+    e_ph = phase_err(gx, o.ex)
+    report(test='full_vs_fp64_oracle', case=which, grid=[int(w.mesh.nx), int(w.mesh.ny)], field_rel_l2=e_field,
+           intensity_rel_l2=e_int, phase_rms_rad=e_ph)
+    assert e_field < TOL
+    assert e_int < TOL
+    assert e_ph < TOL
+
+
+def _reference():
+    if not os.path.exists(os.path.join(REF_DIR, 'srwlpy.so')):
+        pytest.skip('reference build (oracle/_ref) not present')
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    import srwlpy as ref
+    return ref
+
+
+def _copy_wfr(w):
+    ex, ey = fields(w)
+    m = w.mesh
+    mesh = dict(xStart=m.xStart, xFin=m.xFin, yStart=m.yStart, yFin=m.yFin, eStart=m.eStart, eFin=m.eFin,
+                zStart=m.zStart)
+    return make_wfr(ex, ey, mesh, Rx=w.Rx, Ry=w.Ry, dRx=w.dRx, dRy=w.dRy, xc=w.xc, yc=w.yc,
+                    momX=list(w.arMomX) if w.arMomX is not None else None,
+                    momY=list(w.arMomY) if w.arMomY is not None else None)
+
+
+def _vs_reference(w0, el, pp, name):
+    ref = _reference()
+    wr, wg = _copy_wfr(w0), _copy_wfr(w0)
+    ref.PropagElecField(wr, beamline(el, pp))
+    srwl.PropagElecField(wg, beamline(el, pp))
+    assert np.array_equal(mesh_tuple(wg), mesh_tuple(wr))
+    assert [wg.Rx, wg.Ry, wg.xc, wg.yc] == [wr.Rx, wr.Ry, wr.xc, wr.yc]
+    rx, ry = fields(wr)
+    gx, gy = fields(wg)
+    e_field = rel_l2(gx, rx)
+    e_int = rel_l2(np.abs(gx) ** 2 + np.abs(gy) ** 2, np.abs(rx) ** 2 + np.abs(ry) ** 2)
+    e_ph = phase_err(gx, rx)
+    report(test='full_vs_reference', case=name, grid=[int(wg.mesh.nx), int(wg.mesh.ny)], field_rel_l2=e_field,
+           intensity_rel_l2=e_int, phase_rms_rad=e_ph)
+    assert e_field < TOL
+    assert e_int < TOL
+    assert e_ph < TOL
+    return wg, wr
+
+
+def test_full_c1_undulator_field_vs_reference_built_from_source():
+    """The headline beamline (1024^2 -> 4096^2) on the reference's own undulator field (its
+    CalcElecFieldSR, 20000 trajectory points), against the reference's propagation of it: the field
+    carries the source's moments, so the aperture recomputes them from the field as the reference does."""
+    need_gpu()
+    from tests.sr_source import undulator_wfr
+    w0 = undulator_wfr(_reference(), 1024)
+    wg, wr = _vs_reference(w0, C1, C1PP, 'c1_undulator')
+    assert int(wg.mesh.nx) == 4096
+    assert moment_err(np.array(wg.arMomX), np.array(wr.arMomX)) < TOL
+
+
+def test_full_c2_vs_reference_built_from_source():
+    """4096^2 Gaussian with the imposed 30 m radius through the two quadratic-phase drifts and the
+    lens, against the reference's propagation of the same field."""
+    need_gpu()
+    ex, ey, mesh, el, pp, sc = full_case('c2')
+    w0 = make_wfr(ex, ey, mesh, **sc)
+    _vs_reference(w0, el, pp, 'c2')
 
 
 def test_full_c0_vs_reference_built_from_source():

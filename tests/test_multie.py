@@ -79,16 +79,16 @@ def _rank_main(rank, world, port, q):
     os.environ['MASTER_PORT'] = str(port)
     dist.init_process_group('gloo', rank=rank, world_size=world)
     try:
+        from srw_b200.multie import allreduce_mean, shard_offsets
         i, sc, el, pp, acc = base_case()
-        n = 6
-        offs = sample_offsets(n, *SIG, seed=11)
-        mine = shard(n, rank, world)
-        part = torch.from_numpy(oracle_sum(i, sc, el, pp, acc, offs[mine]))
-        cnt = torch.tensor([float(len(mine))], dtype=torch.float64)
-        dist.all_reduce(part)
-        dist.all_reduce(cnt)
+        n = 7
+        mine = shard_offsets(n, rank, world, *SIG, seed=11, sig_e=1e-3)
+        # this rank's FP64 intensity sum (the oracle's per-electron loop stands in for the device
+        # accumulator, which needs a GPU), reduced over the ranks by the library's own function
+        part = torch.from_numpy(oracle_sum(i, sc, el, pp, acc, mine))
+        mean, n_all = allreduce_mean(part, len(mine))
         if rank == 0:
-            q.put((part.numpy() / cnt.item(), oracle_sum(i, sc, el, pp, acc, offs) / n))
+            q.put((mean.numpy(), n_all, oracle_sum(i, sc, el, pp, acc, sample_offsets(n, *SIG, seed=11, sig_e=1e-3)) / n))
     finally:
         dist.destroy_process_group()
 
@@ -106,11 +106,31 @@ def test_sharded_sum_over_ranks_gloo():
     ps = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
     for p in ps:
         p.start()
-    got, want = q.get(timeout=300)
+    got, n_all, want = q.get(timeout=300)
     for p in ps:
         p.join(timeout=60)
         assert p.exitcode == 0
+    assert n_all == 7
     np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+
+
+def test_shard_offsets_union_and_offset_arrays():
+    """Per-rank offsets (counter-based) add up to the single-process set; flat offset arrays need
+    their column count."""
+    from srw_b200.multie import offset_array, shard_offsets
+    full = sample_offsets(11, *SIG, seed=4, sig_e=1e-3)
+    got = np.zeros_like(full)
+    for r in range(3):
+        got[shard(11, r, 3)] = shard_offsets(11, r, 3, *SIG, seed=4, sig_e=1e-3)
+    assert np.array_equal(got, full)
+    one = full[0]
+    assert offset_array(one, ncols=5).shape == (1, 5)
+    assert offset_array(full[:1]).shape == (1, 5)
+    assert offset_array(full[:4, :4].ravel(), ncols=4).shape == (4, 4)
+    for bad in (dict(offsets=one), dict(offsets=np.zeros(20)), dict(offsets=np.zeros(20), ncols=3),
+                dict(offsets=full, ncols=4), dict(offsets=np.zeros(7), ncols=5)):
+        with pytest.raises(ValueError):
+            offset_array(**bad)
 
 
 # ------------------------------------------------------------------------------------------------

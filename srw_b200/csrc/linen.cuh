@@ -67,6 +67,28 @@ template <int N> __device__ __forceinline__ int chain_dst_n(const ChainG& c, int
     return c.mir ? (N - 1 - k) : k;
 }
 
+// factor of the non-separable point-wise work at kernel index (i, j) (0 where it zeroes the point);
+// out of line: such passes are rare, and inlining it at every point of every stage multiplies the
+// kernels' code size
+static __device__ __noinline__ float2 linen_extra(const PwOps* ex, int i, int j, const float2* tabs)
+{
+    bool zero = false;
+    float2 f = make_float2(1.f, 0.f);
+    extra_eval(*ex, i, j, f, zero, tabs);
+    return zero ? make_float2(0.f, 0.f) : f;
+}
+
+// chain factor at destination k (evaluation index i): the along-line table and, in EXTRA kernels,
+// the non-separable work
+template <bool EXTRA>
+__device__ __forceinline__ float2 factor_n(const ChainG& c, int k, int i, int line, const float2* tabs,
+                                           const PwOps* ex, int axis)
+{
+    float2 f = c.tab >= 0 ? __ldg(&tabs[c.tab + k]) : make_float2(1.f, 0.f);
+    if (EXTRA && c.extra) f = cmul(f, linen_extra(ex, axis == 0 ? i : line, axis == 0 ? line : i, tabs));
+    return f;
+}
+
 // One stage of radix R (NS: product of the radices applied before it).  IN: 0 shared memory, 1
 // shared memory through chain cin, 2 global memory through chain cin; OUT: 0 shared memory, 1 global
 // memory through chain cout.  FIRST / LAST: first / last stage of its transform (conjugation of the
@@ -106,7 +128,7 @@ __device__ __forceinline__ void nstage(float2* s, const float2* __restrict__ gin
                 const int p = j + r * NR;
                 int i;
                 chain_src_n<N>(cin, p, i);
-                float2 x = cmul(chainG_factor<EXTRA>(cin, p, i, line, tabs, ex, axis), v[b][r]);
+                float2 x = cmul(factor_n<EXTRA>(cin, p, i, line, tabs, ex, axis), v[b][r]);
                 x.y *= cj;
                 v[b][r] = x;
             }
@@ -133,7 +155,7 @@ __device__ __forceinline__ void nstage(float2* s, const float2* __restrict__ gin
                     } else {
                         int i;
                         const int q = chain_src_n<N>(cin, p, i);
-                        x = cmul(chainG_factor<EXTRA>(cin, p, i, line, tabs, ex, axis), s[PADN(q)]);
+                        x = cmul(factor_n<EXTRA>(cin, p, i, line, tabs, ex, axis), s[PADN(q)]);
                         if (FIRST) x.y *= cj;
                     }
                 }
@@ -170,7 +192,7 @@ __device__ __forceinline__ void nstage(float2* s, const float2* __restrict__ gin
                     const int kk = chain_dst_n<N>(cout, q);
                     int i;
                     chain_src_n<N>(cout, kk, i);
-                    o = cmul(chainG_factor<EXTRA>(cout, kk, i, line, tabs, ex, axis), o);
+                    o = cmul(factor_n<EXTRA>(cout, kk, i, line, tabs, ex, axis), o);
                     if (has_lf) o = cmul(lf, o);
                     __stcs(&gout[om.at(kk)], o);
                 }

@@ -93,7 +93,7 @@ def test_resize_lens_to_waist(n, rf, df):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('nx,ny', [(320, 448), (2240, 1536), (560, 384)])
+@pytest.mark.parametrize("nx,ny", [(320, 448), (2240, 1536), (560, 384)])
 def test_angular_drifts_ragged(nx, ny):
     """Angular-representation drifts (two transforms per pass, forward then inverse, transfer
     function and its quartic term between them), a circular aperture and a lens on ragged meshes of
@@ -117,8 +117,8 @@ def test_quadratic_phase_drifts_general_length():
 
 @pytest.mark.gpu
 def test_runtime_scheduled_length_still_works():
-    """A general length outside the specialised list (radix 3 only at 2^1: 1.5 x 96 = 144 ... here
-    a 216 x 200 mesh) runs the run-time-scheduled kernel, against the oracle."""
+    """Lengths outside the specialised list (216 = 2^3 3^3 and 200 = 2^3 5^2: fewer than 16 points per
+    thread) run the run-time-scheduled kernel, against the oracle."""
     _gpu()
     ex, ey, mesh = gaussian(216, E=1000., sig=50e-6, r=1e-3, ny=200, ry=1e-3)
     el = [('drift', 10., 0), ('lens', 5., 5., 0., 0.), ('drift', 5., 0)]

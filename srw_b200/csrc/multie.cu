@@ -8,10 +8,12 @@
 // _move_mesh=True (srwlib.py:2803): the angular kick of srTOptAngle (cpp/src/core/sroptang.h:64,
 // phase 5.06773065e6 * e * (x' x + y' y) on the unshifted mesh) followed by a shift of the mesh by
 // (x + x' R, y + y' R), R = (Rx + Ry)/2, and xc += x, yc += y.  Each electron is planned on the host
-// (its own mesh, exact bookkeeping); electrons whose passes have the same kinds and sizes run
-// together: every pass is ONE launch over the batch (grid z = electron, per-electron descriptors
-// and tables), then one kernel adds the batch's intensities, interpolated bilinearly onto the
-// common mesh as avg_update_interp does with order 1, to an FP64 accumulator on the device.
+// (its own mesh, exact bookkeeping), the kick being a linear phase that the planner fuses into the
+// first pass (no kicked copy of the field is written: every electron's first pass reads the base
+// field); electrons whose passes have the same kinds and sizes run together: every pass is ONE
+// launch over the batch (grid z = electron, per-electron descriptors and tables), then one kernel
+// adds the batch's intensities, interpolated bilinearly onto the common mesh as avg_update_interp
+// does with order 1, to an FP64 accumulator on the device.
 // With `graph` set, the launch sequence of a full batch is captured once as a CUDA graph and
 // replayed (only the descriptor and parameter uploads change between batches).
 #include <cuda_runtime.h>
@@ -35,29 +37,12 @@ namespace srwg {
 
 // per-electron parameters in device memory
 struct ElecParams {
-    double kx, kz;                       // kick: phase = kx * x + kz * z on the base mesh
+    double kx, kz;                       // kick: phase kx x + kz z on the base mesh (fused by the planner)
+    double dx, dz;                       // mesh shift of the electron's wavefront
     double oxStart, oxStep, ozStart, ozStep;   // output mesh (steps as (Fin - Start)/(n - 1))
     int onx, onz;
     int pad[2];
 };
-
-// kicked copies of the base field for the electrons of a batch (grid z = electron)
-__global__ void __launch_bounds__(256) kick_kernel(const float2* __restrict__ bx, const float2* __restrict__ by,
-                                                   float2* __restrict__ ox, float2* __restrict__ oy, long long stride,
-                                                   int nx, int nz, double xStart, double xStep, double zStart,
-                                                   double zStep, const ElecParams* __restrict__ ep)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (i >= nx) return;
-    const ElecParams& e = ep[blockIdx.z];
-    const double x = xStart + (double)i * xStep, z = zStart + (double)j * zStep;
-    const float2 f = expi(e.kx * x + e.kz * z);
-    const size_t o = (size_t)j * nx + i;
-    const size_t ob = (size_t)blockIdx.z * stride + o;
-    ox[ob] = cmul(f, __ldg(&bx[o]));
-    oy[ob] = cmul(f, __ldg(&by[o]));
-}
 
 // acc[p] += sum over the batch of the bilinearly interpolated total intensity at common-mesh
 // point p (avg_update_interp, order 1: points outside an electron's mesh add nothing)
@@ -119,7 +104,6 @@ struct srwgMultiE {
     // batch buffers
     int maxBatch = 0;
     size_t nIn = 0, nOut = 0, perWork = 0, constStride = 0, descOff = 0;
-    float2* dIn = nullptr;               // [2][B][nIn]
     float2* dOut = nullptr;              // [2][B][nOut]
     float2* dWork = nullptr;             // [4][B][perWork]
     char* dConst = nullptr;              // [B][constStride]
@@ -137,7 +121,7 @@ struct srwgMultiE {
         if (graph) cudaGraphExecDestroy(graph);
         if (ownAcc) cudaFree(dAcc);
         cudaFree(dSnap);
-        cudaFree(dBase); cudaFree(dIn); cudaFree(dOut); cudaFree(dWork); cudaFree(dConst);
+        cudaFree(dBase); cudaFree(dOut); cudaFree(dWork); cudaFree(dConst);
         cudaFree(dParams);
         for (int i = 0; i < 2; i++) {
             cudaFreeHost(hConst[i]);
@@ -179,6 +163,8 @@ static void electron_wfr(const srwgMultiE& m, const double* off, int stride, SRW
     momX[1] += dxp; momX[3] += dyp; momY[1] += dxp; momY[3] += dyp;     // srTOptAngle::PropagateRadMoments
     const double R = 0.5 * (w.Rx + w.Ry);
     const double dx = dx0 + dxp * R, dy = dy0 + dyp * R;
+    ep.dx = dx;
+    ep.dz = dy;
     w.mesh.xStart += dx; w.mesh.xFin += dx;
     w.mesh.yStart += dy; w.mesh.yFin += dy;
     w.xc += dx0; w.yc += dy0;
@@ -210,28 +196,18 @@ static bool same_structure(const std::vector<KernelDesc>& a, const std::vector<K
     return true;
 }
 
-// runs one batch: kick -> passes -> accumulation; ks = launch shapes (largest resize tiles of the batch)
+// runs one batch: passes (the first one applies each electron's kick) -> accumulation; ks = launch
+// shapes (largest resize tiles of the batch)
 static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, cudaStream_t st)
 {
     dim3 blk(256);
-    dim3 gk((m.nx + 255) / 256, m.nz, nb);
-    kick_kernel<<<gk, blk, 0, st>>>(m.dBase, m.dBase + m.nIn, m.dIn, m.dIn + (size_t)m.maxBatch * m.nIn,
-                                    (long long)m.nIn, m.nx, m.nz, m.xStart, m.xStep, m.zStart, m.zStep, m.dParams);
-    MTRY(cudaGetLastError());
     float2* outX = m.dOut;
     float2* outY = m.dOut + (size_t)m.maxBatch * m.nOut;
-    if (ks.empty()) {
-        for (int b = 0; b < nb; b++) {
-            MTRY(cudaMemcpyAsync(outX + b * m.nOut, m.dIn + b * m.nIn, m.nIn * sizeof(float2), cudaMemcpyDeviceToDevice, st));
-            MTRY(cudaMemcpyAsync(outY + b * m.nOut, m.dIn + (size_t)m.maxBatch * m.nIn + b * m.nIn, m.nIn * sizeof(float2),
-                                 cudaMemcpyDeviceToDevice, st));
-        }
-    } else {
-        int r = execute_passes(ks, *m.ctx, nb, m.dIn, m.dIn + (size_t)m.maxBatch * m.nIn, (long long)m.nIn, outX, outY,
-                               (long long)m.nOut, m.dWork, m.perWork, m.dConst, (long long)m.constStride, m.descOff, st,
-                               nullptr, &ks);
-        if (r) return r;
-    }
+    if (ks.empty()) { set_last_detail("multi-electron plan without passes"); return SRWG_ERR_BAD_ARG; }
+    // every electron's first pass reads the base field (input stride 0) and applies its kick
+    int r = execute_passes(ks, *m.ctx, nb, m.dBase, m.dBase + m.nIn, 0, outX, outY, (long long)m.nOut, m.dWork,
+                           m.perWork, m.dConst, (long long)m.constStride, m.descOff, st, nullptr, &ks);
+    if (r) return r;
     dim3 ga((m.anx + 255) / 256, m.anz);
     accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams, m.dAcc, m.anx, m.anz, m.axStart,
                                      m.axStep, m.azStart, m.azStep);
@@ -329,6 +305,7 @@ extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* p
     // sizes from the unshifted electron's plan
     Planner pl;
     pl.numMoments = false;               // only the intensity is kept: no moment passes
+    pl.inPhase = true;                   // the electrons' kick (here zero): the same passes as theirs
     r = pl.plan(pBase, pOpt);
     if (r) { set_last_detail(pl.err); delete m; return r; }
     m->nIn = (size_t)m->nx * m->nz;
@@ -348,7 +325,6 @@ extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* p
     } while (0)
     const size_t B = (size_t)maxBatch;
     MALLOC(m->dBase, 2 * m->nIn * sizeof(float2));
-    MALLOC(m->dIn, 2 * B * m->nIn * sizeof(float2));
     MALLOC(m->dOut, 2 * B * m->nOut * sizeof(float2));
     MALLOC(m->dWork, 4 * B * m->perWork * sizeof(float2));
     MALLOC(m->dConst, B * m->constStride);
@@ -447,6 +423,11 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
                     electron_wfr(*m, arOffsets + (size_t)stride * (e + k), stride, w, momX, momY, eps[k]);
                     pls[k] = Planner();
                     pls[k].numMoments = false;
+                    // the kick kx (x - dx) + kz (z - dz) on the electron's (shifted) mesh
+                    pls[k].inPhase = true;
+                    pls[k].inKx = eps[k].kx;
+                    pls[k].inKz = eps[k].kz;
+                    pls[k].inC = -(eps[k].kx * eps[k].dx + eps[k].kz * eps[k].dz);
                     rcs[k] = pls[k].plan(&w, m->opt);
                 }
             };

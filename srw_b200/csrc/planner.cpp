@@ -1557,6 +1557,7 @@ int Planner::run()
     const std::vector<ElemDesc>& els = els_;
     const std::vector<PropDesc>& props = props_;
     try {
+        if (inPhase && nStages == 0 && elemIdx_ == 0 && !resizeDone_) b->quad(w, 0., inKx, 0., inKz, inC);
         size_t numRes = props.size();
         size_t& i = elemIdx_;
         for (; i < els.size(); i++, resizeDone_ = false) {

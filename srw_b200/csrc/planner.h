@@ -130,6 +130,10 @@ public:
     int resume(const double* slots);
     std::string describe() const;
     bool allowStages = false;            // staged planning (the one-shot entry point only)
+    // a linear phase kx x + kz z + c (physical coordinates of the input mesh) applied to the input
+    // field before the first element, fused into the first pass (the angular kick of a macro-electron)
+    bool inPhase = false;
+    double inKx = 0, inKz = 0, inC = 0;
     int nStages = 0;                     // stage boundaries passed
     WfrState stageIn;                    // mesh of the current stage's input
 

@@ -1290,6 +1290,47 @@ def _resize_core_only_larger_range(old: Wfr, new: Wfr):
     return outx, outy
 
 
+def _tune_step_keep_interp_limits(old: Wfr, new: Wfr, pm, axis, ic):
+    """TuneStepToKeepInterpLimitsTheSameAtResize (cpp/src/core/sroptel3.cpp:537-623): where the new
+    mesh reaches past the old one's first / last node, its step (and start) are tuned so that the
+    new nodes land on the old mesh's limits, keeping node ic of the old mesh at the new centre."""
+    if axis == 'x':
+        nStart, nStep, oStart, oStep, nNp = new.xStart, new.xStep, old.xStart, old.xStep, new.nx
+        OldEndInterp = old.xStart + (old.nx - 1) * old.xStep
+    else:
+        nStart, nStep, oStart, oStep, nNp = new.zStart, new.zStep, old.zStart, old.zStep, new.nz
+        OldEndInterp = old.zStart + (old.nz - 1) * old.zStep
+    NewEndInterp = nStart + (nNp - 1) * nStep
+    left = nStart <= oStart
+    right = NewEndInterp >= OldEndInterp
+    if not (left or right):
+        return
+    cArg = oStart + ic * oStep
+    half = nNp >> 1
+    if left and not right:
+        dist = cArg - nStart
+        nStep = dist / float(int(dist / nStep + 1.E-10))
+        nStart = cArg - half * nStep
+    elif right and not left:
+        dist = OldEndInterp - cArg
+        nStep = dist / float(int(dist / nStep + 1.E-10))
+        nStart = cArg - half * nStep
+    else:
+        OldRange = OldEndInterp - oStart
+        if pm != 1.:
+            nIn = int(OldRange / nStep + 1.E-10)
+            nLeft = int((oStart - nStart) / nStep + 1.E-10)
+            nStep = OldRange / float(nIn)
+            nStart = oStart - nLeft * nStep
+        else:
+            nStep = OldRange / float(nNp - 1)
+            nStart = oStart
+    if axis == 'x':
+        new.xStart, new.xStep = nStart, nStep
+    else:
+        new.zStart, new.zStep = nStart, nStep
+
+
 def rad_resize_gen(w: Wfr, pxm, pxd, pzm, pzd, shift_type=0, xCenShift=0., zCenShift=0., other_side=False):
     """RadResizeGen (sroptelm.cpp:2242-3036), ne == 1, no per-polarisation memory fallback."""
     if pxm == 1. and pxd == 1. and pzm == 1. and pzd == 1. and shift_type <= 0:
@@ -1350,8 +1391,6 @@ def rad_resize_gen(w: Wfr, pxm, pxd, pzm, pzd, shift_type=0, xCenShift=0., zCenS
         iZc = _int_offset_coord(w.zStart, w.zStep, zcAppr)
         centerOffset = True
     Zc = w.zStart + w.zStep * iZc
-    if centerOffset:
-        raise NotImplementedError("off-centre resize (pp[9] shift types) is not restated")
 
     def preserve(axis):
         """PreserveLogicsOfWfrLimitsAtRangeResizing (srradstr.cpp:1598)."""
@@ -1367,60 +1406,99 @@ def rad_resize_gen(w: Wfr, pxm, pxd, pzm, pzd, shift_type=0, xCenShift=0., zCenS
                 new.zWfrMin, new.zWfrMax = new.zStart, new.zStart + new.nz * new.zStep
             else:
                 new.zWfrMin, new.zWfrMax = old.zWfrMin, old.zWfrMax
-    xMagOld = (w.nx - 1) * w.xStep
-    if pxm > 1.:
-        NxInner = int(NewNx / pxm) if pxd != 1. else w.nx
-        d = NewNx - NxInner
-        left = d >> 1
-        if (left << 1) != d:
-            left += 1
-        new.xStep = xMagOld / (NxInner - 1)
-        new.xStart = w.xStart - left * new.xStep
-        new.AuxLong1 = left
-        new.AuxLong2 = left + NxInner - 1
-        preserve('x')
+    if centerOffset:
+        # centre of the new mesh at node iXc / iZc of the old one (sroptelm.cpp:2383-2433)
+        NewNxLeftHalf = NewNx >> 1
+        new.xStep = w.xStep / pxd
+        new.xStart = Xc - NewNxLeftHalf * new.xStep
+        NewNxEndInterp = new.xStart + (NewNx - 1) * new.xStep
+        OldNxEndInterp = w.xStart + (w.nx - 1) * w.xStep
+        _tune_step_keep_interp_limits(w, new, pxm, 'x', iXc)
+        new.AuxLong1 = _int_offset_coord(new.xStart, new.xStep, w.xStart) if new.xStart < w.xStart else 0
+        new.AuxLong2 = _int_offset_coord(new.xStart, new.xStep, OldNxEndInterp) if NewNxEndInterp > OldNxEndInterp \
+            else NewNx - 1
+        if pxm > 1.:
+            preserve('x')
+        else:
+            if new.xStart > new.xWfrMin:
+                new.xWfrMin = new.xStart
+            xEndNew = new.xStart + new.nx * new.xStep
+            if xEndNew < new.xWfrMax:
+                new.xWfrMax = xEndNew
+        NewNzLeftHalf = NewNz >> 1
+        new.zStep = w.zStep / pzd
+        new.zStart = Zc - NewNzLeftHalf * new.zStep
+        _tune_step_keep_interp_limits(w, new, pzm, 'z', iZc)
+        # (the reference's z branch starts one node later and takes the end limits after the tuning)
+        new.AuxLong3 = 1 + _int_offset_coord(new.zStart, new.zStep, w.zStart) if new.zStart < w.zStart else 0
+        NewNzEndInterp = new.zStart + (NewNz - 1) * new.zStep
+        OldNzEndInterp = w.zStart + (w.nz - 1) * w.zStep
+        new.AuxLong4 = _int_offset_coord(new.zStart, new.zStep, OldNzEndInterp) if NewNzEndInterp > OldNzEndInterp \
+            else NewNz - 1
+        if pzm > 1.:
+            preserve('z')
+        else:
+            if new.zStart > new.zWfrMin:
+                new.zWfrMin = new.zStart
+            zEndNew = new.zStart + new.nz * new.zStep
+            if zEndNew < new.zWfrMax:
+                new.zWfrMax = zEndNew
     else:
-        xEndOld = w.xStart + (w.nx - 1) * w.xStep
-        xMid = 0.5 * (w.xStart + xEndOld)
-        xMagNew = xMagOld * pxm
-        new.xStep = xMagNew / (NewNx - 1)
-        if pxd == 1:
-            new.xStep = w.xStep
-            xMagNew = (NewNx - 1) * new.xStep
-        new.xStart = xMid - 0.5 * xMagNew
-        new.AuxLong1 = 0
-        new.AuxLong2 = NewNx - 1
-        if new.xStart > new.xWfrMin:
-            new.xWfrMin = new.xStart
-        if (new.xStart + xMagNew) < new.xWfrMax:
-            new.xWfrMax = new.xStart + xMagNew
-    zMagOld = (w.nz - 1) * w.zStep
-    if pzm > 1.:
-        NzInner = int(NewNz / pzm) if pzd != 1. else w.nz
-        d = NewNz - NzInner
-        left = d >> 1
-        if (left << 1) != d:
-            left += 1
-        new.zStep = zMagOld / (NzInner - 1)
-        new.zStart = w.zStart - left * new.zStep
-        new.AuxLong3 = left
-        new.AuxLong4 = left + NzInner - 1
-        preserve('z')
-    else:
-        zEndOld = w.zStart + (w.nz - 1) * w.zStep
-        zMid = 0.5 * (w.zStart + zEndOld)
-        zMagNew = zMagOld * pzm
-        new.zStep = zMagNew / (NewNz - 1)
-        if pzd == 1:
-            new.zStep = w.zStep
-            zMagNew = (NewNz - 1) * new.zStep
-        new.zStart = zMid - 0.5 * zMagNew
-        new.AuxLong3 = 0
-        new.AuxLong4 = NewNz - 1
-        if new.zStart > new.zWfrMin:
-            new.zWfrMin = new.zStart
-        if (new.zStart + zMagNew) < new.zWfrMax:
-            new.zWfrMax = new.zStart + zMagNew
+        xMagOld = (w.nx - 1) * w.xStep
+        if pxm > 1.:
+            NxInner = int(NewNx / pxm) if pxd != 1. else w.nx
+            d = NewNx - NxInner
+            left = d >> 1
+            if (left << 1) != d:
+                left += 1
+            new.xStep = xMagOld / (NxInner - 1)
+            new.xStart = w.xStart - left * new.xStep
+            new.AuxLong1 = left
+            new.AuxLong2 = left + NxInner - 1
+            preserve('x')
+        else:
+            xEndOld = w.xStart + (w.nx - 1) * w.xStep
+            xMid = 0.5 * (w.xStart + xEndOld)
+            xMagNew = xMagOld * pxm
+            new.xStep = xMagNew / (NewNx - 1)
+            if pxd == 1:
+                new.xStep = w.xStep
+                xMagNew = (NewNx - 1) * new.xStep
+            new.xStart = xMid - 0.5 * xMagNew
+            new.AuxLong1 = 0
+            new.AuxLong2 = NewNx - 1
+            if new.xStart > new.xWfrMin:
+                new.xWfrMin = new.xStart
+            if (new.xStart + xMagNew) < new.xWfrMax:
+                new.xWfrMax = new.xStart + xMagNew
+        zMagOld = (w.nz - 1) * w.zStep
+        if pzm > 1.:
+            NzInner = int(NewNz / pzm) if pzd != 1. else w.nz
+            d = NewNz - NzInner
+            left = d >> 1
+            if (left << 1) != d:
+                left += 1
+            new.zStep = zMagOld / (NzInner - 1)
+            new.zStart = w.zStart - left * new.zStep
+            new.AuxLong3 = left
+            new.AuxLong4 = left + NzInner - 1
+            preserve('z')
+        else:
+            zEndOld = w.zStart + (w.nz - 1) * w.zStep
+            zMid = 0.5 * (w.zStart + zEndOld)
+            zMagNew = zMagOld * pzm
+            new.zStep = zMagNew / (NewNz - 1)
+            if pzd == 1:
+                new.zStep = w.zStep
+                zMagNew = (NewNz - 1) * new.zStep
+            new.zStart = zMid - 0.5 * zMagNew
+            new.AuxLong3 = 0
+            new.AuxLong4 = NewNz - 1
+            if new.zStart > new.zWfrMin:
+                new.zWfrMin = new.zStart
+            if (new.zStart + zMagNew) < new.zWfrMax:
+                new.zWfrMax = new.zStart + zMagNew
+
 
     grow = (pxmIn * pxdIn * pzmIn * pzdIn) >= 1.
     if grow and changed:

@@ -1320,6 +1320,45 @@ void Planner::treat_quad(char add_or_rem)
     b->quad(w, ax, -2. * ax * w.xc, az, -2. * az * w.zc, ax * w.xc * w.xc + az * w.zc * w.zc);
 }
 
+// TuneStepToKeepInterpLimitsTheSameAtResize (cpp/src/core/sroptel3.cpp:537-623): where the new mesh
+// reaches past the old one's first / last node, its step and start are tuned so that new nodes land
+// on the old mesh's limits, node ic of the old mesh staying at the new centre
+static void tune_step_keep_interp_limits(const WfrState& o, WfrState& n, double pm, char axis, long ic)
+{
+    double& nStart = axis == 'x' ? n.xStart : n.zStart;
+    double& nStep = axis == 'x' ? n.xStep : n.zStep;
+    const double oStart = axis == 'x' ? o.xStart : o.zStart, oStep = axis == 'x' ? o.xStep : o.zStep;
+    const long nNp = axis == 'x' ? n.nx : n.nz, oNp = axis == 'x' ? o.nx : o.nz;
+    const double NewEndInterp = nStart + (nNp - 1) * nStep;
+    const double OldEndInterp = oStart + (oNp - 1) * oStep;
+    const bool left = nStart <= oStart, right = NewEndInterp >= OldEndInterp;
+    if (!(left || right)) return;
+    const double cArg = oStart + ic * oStep;
+    const long half = nNp >> 1;
+    if (left && !right) {
+        const double dist = cArg - nStart;
+        const long steps = (long)(dist / nStep + 1.E-10);
+        nStep = dist / double(steps);
+        nStart = cArg - half * nStep;
+    } else if (!left && right) {
+        const double dist = OldEndInterp - cArg;
+        const long steps = (long)(dist / nStep + 1.E-10);
+        nStep = dist / double(steps);
+        nStart = cArg - half * nStep;
+    } else {
+        const double OldRange = OldEndInterp - oStart;
+        if (pm != 1.) {
+            const long nIn = (long)(OldRange / nStep + 1.E-10);
+            const long nLeft = (long)((oStart - nStart) / nStep + 1.E-10);
+            nStep = OldRange / double(nIn);
+            nStart = oStart - nLeft * nStep;
+        } else {
+            nStep = OldRange / double(nNp - 1);
+            nStart = oStart;
+        }
+    }
+}
+
 int Planner::resize(double pxm, double pxd, double pzm, double pzd, int shift, double xcs, double zcs, bool other_side)
 {
     if ((pxm == 1.) && (pxd == 1.) && (pzm == 1.) && (pzd == 1.) && (shift <= 0)) return 0;
@@ -1370,10 +1409,24 @@ int Planner::resize(double pxm, double pxd, double pzm, double pzd, int shift, d
         nw.nx = (int)NewNx;
         nw.nz = (int)NewNz;
     }
-    if ((::fabs(RelCenPosX - 0.5) > RelCenPosTol) || (::fabs(RelCenPosZ - 0.5) > RelCenPosTol)) {
-        err = "off-centre resizing (pp[9] shift types) is not supported on the GPU path";
-        return SRWG_ERR_UNSUPPORTED;
+    // centre of the new mesh: the old mesh's middle node, or the node nearest the requested centre
+    // (IntegerOffsetCoord, sroptelm.h:995)
+    auto ioc = [](double start, double step, double val) {
+        long i = (long)((val - start) / step);
+        if (::fabs(val - ((i + 1) * step + start)) < 1.E-05 * step) i++;
+        return i;
+    };
+    bool centerOffset = false;
+    long iXc = w.nx >> 1, iZc = w.nz >> 1;
+    if (::fabs(RelCenPosX - 0.5) > RelCenPosTol) {
+        iXc = ioc(w.xStart, w.xStep, w.xStart + w.nx * w.xStep * RelCenPosX);
+        centerOffset = true;
     }
+    if (::fabs(RelCenPosZ - 0.5) > RelCenPosTol) {
+        iZc = ioc(w.zStart, w.zStep, w.zStart + w.nz * w.zStep * RelCenPosZ);
+        centerOffset = true;
+    }
+    const double Xc = w.xStart + w.xStep * iXc, Zc = w.zStart + w.zStep * iZc;
     auto preserve = [&](char ax) {   // PreserveLogicsOfWfrLimitsAtRangeResizing (srradstr.cpp:1598)
         if (ax == 'x') {
             double tol = 0.01 * nw.xStep;
@@ -1387,51 +1440,85 @@ int Planner::resize(double pxm, double pxd, double pzm, double pzd, int shift, d
             } else { nw.zWfrMin = old.zWfrMin; nw.zWfrMax = old.zWfrMax; }
         }
     };
-    double xMagOld = (w.nx - 1) * w.xStep;
-    if (pxm > 1.) {
-        long NxInner = (pxd != 1.) ? (long)(NewNx / pxm) : w.nx;
-        long d = NewNx - NxInner;
-        long left = d >> 1;
-        if ((left << 1) != d) left++;
-        nw.xStep = xMagOld / (NxInner - 1);
-        nw.xStart = w.xStart - left * nw.xStep;
-        nw.AuxLong1 = left;
-        nw.AuxLong2 = left + NxInner - 1;
-        preserve('x');
+    if (centerOffset) {
+        // new mesh centred on node iXc / iZc of the old one (sroptelm.cpp:2383-2433), its step tuned
+        // so that the interpolation limits stay those of the old mesh
+        const long NewNxLeftHalf = NewNx >> 1;
+        nw.xStep = w.xStep / pxd;
+        nw.xStart = Xc - NewNxLeftHalf * nw.xStep;
+        const double NewNxEndInterp = nw.xStart + (NewNx - 1) * nw.xStep;
+        const double OldNxEndInterp = w.xStart + (w.nx - 1) * w.xStep;
+        tune_step_keep_interp_limits(w, nw, pxm, 'x', iXc);
+        nw.AuxLong1 = (nw.xStart < w.xStart) ? ioc(nw.xStart, nw.xStep, w.xStart) : 0;
+        nw.AuxLong2 = (NewNxEndInterp > OldNxEndInterp) ? ioc(nw.xStart, nw.xStep, OldNxEndInterp) : NewNx - 1;
+        if (pxm > 1.) preserve('x');
+        else {
+            if (nw.xStart > nw.xWfrMin) nw.xWfrMin = nw.xStart;
+            const double xEndNew = nw.xStart + nw.nx * nw.xStep;
+            if (xEndNew < nw.xWfrMax) nw.xWfrMax = xEndNew;
+        }
+        const long NewNzLeftHalf = NewNz >> 1;
+        nw.zStep = w.zStep / pzd;
+        nw.zStart = Zc - NewNzLeftHalf * nw.zStep;
+        tune_step_keep_interp_limits(w, nw, pzm, 'z', iZc);
+        // the reference's z branch starts one node later and takes the end limit after the tuning
+        nw.AuxLong3 = (nw.zStart < w.zStart) ? 1 + ioc(nw.zStart, nw.zStep, w.zStart) : 0;
+        const double NewNzEndInterp = nw.zStart + (NewNz - 1) * nw.zStep;
+        const double OldNzEndInterp = w.zStart + (w.nz - 1) * w.zStep;
+        nw.AuxLong4 = (NewNzEndInterp > OldNzEndInterp) ? ioc(nw.zStart, nw.zStep, OldNzEndInterp) : NewNz - 1;
+        if (pzm > 1.) preserve('z');
+        else {
+            if (nw.zStart > nw.zWfrMin) nw.zWfrMin = nw.zStart;
+            const double zEndNew = nw.zStart + nw.nz * nw.zStep;
+            if (zEndNew < nw.zWfrMax) nw.zWfrMax = zEndNew;
+        }
     } else {
-        double xEndOld = w.xStart + (w.nx - 1) * w.xStep;
-        double xMid = 0.5 * (w.xStart + xEndOld);
-        double xMagNew = xMagOld * pxm;
-        nw.xStep = xMagNew / (NewNx - 1);
-        if (pxd == 1) { nw.xStep = w.xStep; xMagNew = (NewNx - 1) * nw.xStep; }
-        nw.xStart = xMid - 0.5 * xMagNew;
-        nw.AuxLong1 = 0;
-        nw.AuxLong2 = NewNx - 1;
-        if (nw.xStart > nw.xWfrMin) nw.xWfrMin = nw.xStart;
-        if ((nw.xStart + xMagNew) < nw.xWfrMax) nw.xWfrMax = nw.xStart + xMagNew;
-    }
-    double zMagOld = (w.nz - 1) * w.zStep;
-    if (pzm > 1.) {
-        long NzInner = (pzd != 1.) ? (long)(NewNz / pzm) : w.nz;
-        long d = NewNz - NzInner;
-        long left = d >> 1;
-        if ((left << 1) != d) left++;
-        nw.zStep = zMagOld / (NzInner - 1);
-        nw.zStart = w.zStart - left * nw.zStep;
-        nw.AuxLong3 = left;
-        nw.AuxLong4 = left + NzInner - 1;
-        preserve('z');
-    } else {
-        double zEndOld = w.zStart + (w.nz - 1) * w.zStep;
-        double zMid = 0.5 * (w.zStart + zEndOld);
-        double zMagNew = zMagOld * pzm;
-        nw.zStep = zMagNew / (NewNz - 1);
-        if (pzd == 1) { nw.zStep = w.zStep; zMagNew = (NewNz - 1) * nw.zStep; }
-        nw.zStart = zMid - 0.5 * zMagNew;
-        nw.AuxLong3 = 0;
-        nw.AuxLong4 = NewNz - 1;
-        if (nw.zStart > nw.zWfrMin) nw.zWfrMin = nw.zStart;
-        if ((nw.zStart + zMagNew) < nw.zWfrMax) nw.zWfrMax = nw.zStart + zMagNew;
+        double xMagOld = (w.nx - 1) * w.xStep;
+        if (pxm > 1.) {
+            long NxInner = (pxd != 1.) ? (long)(NewNx / pxm) : w.nx;
+            long d = NewNx - NxInner;
+            long left = d >> 1;
+            if ((left << 1) != d) left++;
+            nw.xStep = xMagOld / (NxInner - 1);
+            nw.xStart = w.xStart - left * nw.xStep;
+            nw.AuxLong1 = left;
+            nw.AuxLong2 = left + NxInner - 1;
+            preserve('x');
+        } else {
+            double xEndOld = w.xStart + (w.nx - 1) * w.xStep;
+            double xMid = 0.5 * (w.xStart + xEndOld);
+            double xMagNew = xMagOld * pxm;
+            nw.xStep = xMagNew / (NewNx - 1);
+            if (pxd == 1) { nw.xStep = w.xStep; xMagNew = (NewNx - 1) * nw.xStep; }
+            nw.xStart = xMid - 0.5 * xMagNew;
+            nw.AuxLong1 = 0;
+            nw.AuxLong2 = NewNx - 1;
+            if (nw.xStart > nw.xWfrMin) nw.xWfrMin = nw.xStart;
+            if ((nw.xStart + xMagNew) < nw.xWfrMax) nw.xWfrMax = nw.xStart + xMagNew;
+        }
+        double zMagOld = (w.nz - 1) * w.zStep;
+        if (pzm > 1.) {
+            long NzInner = (pzd != 1.) ? (long)(NewNz / pzm) : w.nz;
+            long d = NewNz - NzInner;
+            long left = d >> 1;
+            if ((left << 1) != d) left++;
+            nw.zStep = zMagOld / (NzInner - 1);
+            nw.zStart = w.zStart - left * nw.zStep;
+            nw.AuxLong3 = left;
+            nw.AuxLong4 = left + NzInner - 1;
+            preserve('z');
+        } else {
+            double zEndOld = w.zStart + (w.nz - 1) * w.zStep;
+            double zMid = 0.5 * (w.zStart + zEndOld);
+            double zMagNew = zMagOld * pzm;
+            nw.zStep = zMagNew / (NewNz - 1);
+            if (pzd == 1) { nw.zStep = w.zStep; zMagNew = (NewNz - 1) * nw.zStep; }
+            nw.zStart = zMid - 0.5 * zMagNew;
+            nw.AuxLong3 = 0;
+            nw.AuxLong4 = NewNz - 1;
+            if (nw.zStart > nw.zWfrMin) nw.zWfrMin = nw.zStart;
+            if ((nw.zStart + zMagNew) < nw.zWfrMax) nw.zWfrMax = nw.zStart + zMagNew;
+        }
     }
     bool grow = (pxmIn * pxdIn * pzmIn * pzdIn) >= 1.;
     if (grow && changed) { WfrState t = w; w = nw; srwl_roundtrip(); nw = w; w = t; }

@@ -155,6 +155,8 @@ def cases(L):
     c1pp = [pp(), pp(0, 2., 2., 2., 2.), pp(4)]
     c2 = [('drift', 30., 0), ('lens', 15., 15., 0., 0.), ('drift', 30., 0)]
     c2pp = [pp(2), pp(), pp(2)]
+    # resize with its centre moved (pp[9] shift type: 1 x, 2 z, 3 both; pp[10], pp[11] the centre)
+    ppo = lambda pxm, pxd, pzm, pzd, sh, xc, zc, anal=0: [0, 0, 1., anal, 0, pxm, pxd, pzm, pzd, sh, xc, zc]  # noqa: E731
 
     def g0(n):
         return lambda: gaussian_wfr(L, 1000., 50e-6, n, n, 1e-3, 1e-3)
@@ -177,6 +179,16 @@ def cases(L):
         ('rs_res_only', g0(64), [('drift', 3., 0)], [pp(0, 1., 2., 1., 1.5)]),
         ('rs_range_only', g0(64), [('drift', 3., 0)], [pp(0, 2., 1., 1.5, 1.)]),
         ('rs_post', g0(64), [('drift', 3., 0)], [pp(), pp(0, 1.3, 1.7, 1.2, 1.1)]),
+        # off-centre resizing (sroptelm.cpp:2383-2433, TuneStepToKeepInterpLimitsTheSameAtResize
+        # sroptel3.cpp:537): both axes growing; x shrinking in range while z stays; a range-only z
+        # resize; centres near the edges (the new mesh reaches past both limits); a curved beam
+        # (quadratic-term treatment) after a lens
+        ('rs_offc_grow', g0(96), [('drift', 3., 0)], [ppo(1.5, 1.2, 1.3, 1.1, 3, 0.25e-3, -0.15e-3)]),
+        ('rs_offc_shrink_x', g0(128), [('drift', 3., 0)], [ppo(0.7, 1.5, 1., 1., 1, -0.3e-3, 0.)]),
+        ('rs_offc_range_z', g0(64), [('drift', 2., 0)], [ppo(1., 1., 1.6, 1., 2, 0., 0.4e-3)]),
+        ('rs_offc_edge', g0(80), [('drift', 2., 0)], [ppo(1., 2., 1., 2., 3, 0.8e-3, -0.85e-3)]),
+        ('rs_offc_quad', g2(96, 0.5e-3), [('lens', 15., 15., 0., 0.), ('drift', 10., 0)],
+         [pp(), ppo(1.4, 1.3, 1.4, 1.3, 3, 0.05e-3, 0.02e-3)]),
         ('ob_circ_lens_offc', g0(96), [('aperture', 'c', 'o', 0.3e-3, 0.3e-3, 0.1e-3, 0.), ('drift', 2., 0),
                                       ('lens', 3., 4., 0.2e-3, -0.1e-3), ('drift', 2., 0)], [PP0] * 4),
         ('rect_ob_towaist', g2(96, 0.5e-3), [('aperture', 'r', 'o', 0.2e-3, 0.1e-3, 0., 0.), ('lens', 20., 20., 0., 0.),

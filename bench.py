@@ -528,7 +528,8 @@ def measure_mixed(args, dev, n_elec, model=None):
             factors = CONFIGURED
             if mode == 'learned':
                 from srw_b200 import learned
-                factors, fb, _ = learned.choose_factors(model, learned.bench_case(ex, ey, mesh, sc), dev)
+                factors, fb, _ = learned.choose_factors(model, learned.bench_case(ex, ey, mesh, sc), dev,
+                                                        acc_mesh=acc)
                 facs[n] = list(factors) + (['fallback'] if fb else [])
             bl = beamline_objs(mod, factors)
             b = batch or {256: 32, 512: 32, 1024: 16}[n]
@@ -589,7 +590,7 @@ def measure_learned(args, dev, world, dist, acc):
         return None
     ex, ey, mesh, sc = synth_undulator_field(1024)
     t0 = time.perf_counter()
-    factors, fallback, chk = learned.choose_factors(model, learned.bench_case(ex, ey, mesh, sc), dev)
+    factors, fallback, chk = learned.choose_factors(model, learned.bench_case(ex, ey, mesh, sc), dev, acc_mesh=acc)
     choose_s = time.perf_counter() - t0
     w = make_wfr(mod, ex, ey, mesh, sc)
     cm = learned.CheckedMultiE(w, lambda f: beamline_objs(mod, f), factors, acc, max_batch=LEARNED_BATCH,

@@ -474,8 +474,9 @@ def choose_grid(pred, nx, nz):
 def label_case(case, dev, stream=None):
     """Cheapest factors (pxm, pxd, pzm, pzd) within tolerance of the oversampled propagation: per
     axis the candidate pairs in order of the resized length (the other axis at the conservative
-    factors), the first within AXIS_TOL; the combination is checked against TOL_LABEL and replaced
-    by the conservative factors when it fails.  Returns (factors, error of the label, evaluations)."""
+    factors), the first within AXIS_TOL found by bisection; the combination is checked against
+    TOL_LABEL and replaced by the conservative factors when it fails.  Returns (factors, error of
+    the label, evaluations)."""
     n = case['mesh']['nx']
     rf = ref_factors(n)
     Iref, omref = propagate_intensity(case, rf + rf, dev, stream)
@@ -491,16 +492,25 @@ def label_case(case, dev, stream=None):
     best = []
     for axis in (0, 1):
         nn = case['mesh']['nx'] if axis == 0 else case['mesh']['ny']
-        cands = sorted(_pairs(), key=lambda p: (new_length(nn, *p), p[1], p[0]))
-        pick = CONSERVATIVE[:2]
-        for p in cands:
-            if new_length(nn, *p) >= new_length(nn, 2., 2.):
-                break
+        full = new_length(nn, *CONSERVATIVE[:2])
+        cands = [p for p in sorted(_pairs(), key=lambda p: (new_length(nn, *p), p[1], p[0]))
+                 if new_length(nn, *p) < full]
+
+        def ok(p):
             fac = (p + CONSERVATIVE[2:]) if axis == 0 else (CONSERVATIVE[:2] + p)
-            if err(fac) <= AXIS_TOL:
-                pick = p
-                break
-        best.append(tuple(pick))
+            return err(fac) <= AXIS_TOL
+        # the error falls as the resized length grows: bisect for the first candidate within the
+        # tolerance, then walk up from there while the neighbours disagree with that assumption
+        lo, hi = 0, len(cands)
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if ok(cands[mid]):
+                hi = mid
+            else:
+                lo = mid + 1
+        while lo < len(cands) and not ok(cands[lo]):
+            lo += 1
+        best.append(tuple(cands[lo]) if lo < len(cands) else tuple(CONSERVATIVE[:2]))
     lab = best[0] + best[1]
     e = err(lab)
     if e > TOL_LABEL:
@@ -529,21 +539,69 @@ def _common_error(I, om, I_c, om_c):
     return factor_error(I, om, I_c, om_c, eval_box(I_c, om_c))
 
 
-def choose_factors(model, case, dev, check_tol=TOL_LABEL):
-    """(factors, used_fallback, check_error): the network's factors, rounded up to the grid, when
-    the wavefront propagated with them agrees with its propagation at the conservative factors
-    within check_tol; else the conservative factors."""
+def on_mesh(I, om, em):
+    """Intensity I (torch float64 [ny, nx] on mesh om) interpolated bilinearly at the nodes of mesh em,
+    zero outside om, as the multi-electron accumulation does (avg_update_interp, order 1)."""
+    import torch
+    ny, nx = I.shape
+    xs = (om['xFin'] - om['xStart']) / (nx - 1)
+    ys = (om['yFin'] - om['yStart']) / (ny - 1)
+    xa = em['xStart'] + torch.arange(em['nx'], dtype=torch.float64, device=I.device) * (em['xFin'] - em['xStart']) / (em['nx'] - 1)
+    ya = em['yStart'] + torch.arange(em['ny'], dtype=torch.float64, device=I.device) * (em['yFin'] - em['yStart']) / (em['ny'] - 1)
+    ix = torch.trunc((xa - om['xStart']) / xs + 1.e-09).long()
+    iy = torch.trunc((ya - om['yStart']) / ys + 1.e-09).long()
+    okx = (ix >= 0) & (ix < nx - 1)
+    oky = (iy >= 0) & (iy < ny - 1)
+    ix, iy = ix.clamp(0, nx - 2), iy.clamp(0, ny - 2)
+    tx = ((xa - (om['xStart'] + xs * ix)) / xs).unsqueeze(0)
+    ty = ((ya - (om['yStart'] + ys * iy)) / ys).unsqueeze(1)
+    a00, f10 = I[iy][:, ix], I[iy][:, ix + 1]
+    f01, f11 = I[iy + 1][:, ix], I[iy + 1][:, ix + 1]
+    v = a00 + tx * ((f10 - a00) + ty * (a00 - f01 - f10 + f11)) + ty * (f01 - a00)
+    return v * (oky.unsqueeze(1) & okx.unsqueeze(0))
+
+
+def mesh_error(I, om, I_c, om_c, em):
+    """Relative L2 of intensity I (mesh om) against the conservative one I_c (mesh om_c), both
+    interpolated onto the detector mesh em, where I_c exceeds 1e-3 of its maximum there."""
+    import torch
+    a, b = on_mesh(I, om, em), on_mesh(I_c, om_c, em)
+    sel = b > 1e-3 * b.max()
+    return float(torch.linalg.norm((a - b)[sel]) / torch.linalg.norm(b[sel]))
+
+
+def _next(grid, v):
+    larger = grid[grid > v + 1e-9]
+    return float(larger[0]) if len(larger) else float(v)
+
+
+def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=4):
+    """(factors, used_fallback, check_error): the network's factors, rounded up to the grid, checked
+    by propagating the wavefront with them and with the conservative factors (relative L2 of the
+    intensity on the detector mesh acc_mesh when given -- the mesh a multi-electron run accumulates
+    on --, else at the output nodes); when the check exceeds check_tol, the resolution and then the
+    range factors are raised a grid step at a time (up to `tries` candidates in all) before falling
+    back to the conservative factors."""
     feat = case_features(case, dev).unsqueeze(0)
     pred = model.predict(feat)[0].cpu().numpy()
-    fac = choose_grid(pred, case['mesh']['nx'], case['mesh']['ny'])
-    if tuple(fac) == tuple(CONSERVATIVE):
+    fac = tuple(choose_grid(pred, case['mesh']['nx'], case['mesh']['ny']))
+    if fac == tuple(CONSERVATIVE):
         return CONSERVATIVE, False, 0.
-    I, om = propagate_intensity(case, fac, dev)
     Ic, omc = propagate_intensity(case, CONSERVATIVE, dev)
-    e = _common_error(I, om, Ic, omc)
-    if e > check_tol:
-        return CONSERVATIVE, True, e
-    return tuple(fac), False, e
+    cands = [fac]
+    rx, dx, rz, dz = fac
+    cands.append((rx, _next(GRID_D, dx), rz, _next(GRID_D, dz)))
+    cands.append((_next(GRID_R, rx), dx, _next(GRID_R, rz), dz))
+    cands.append((_next(GRID_R, rx), _next(GRID_D, dx), _next(GRID_R, rz), _next(GRID_D, dz)))
+    e = None
+    for c in [c for i, c in enumerate(cands) if c not in cands[:i]][:tries]:
+        if c == tuple(CONSERVATIVE):
+            break
+        I, om = propagate_intensity(case, c, dev)
+        e = mesh_error(I, om, Ic, omc, acc_mesh) if acc_mesh is not None else _common_error(I, om, Ic, omc)
+        if e <= check_tol:
+            return c, False, e
+    return CONSERVATIVE, True, e
 
 
 class CheckedMultiE(object):
@@ -575,22 +633,29 @@ class CheckedMultiE(object):
         self.n, self.batches, self.fallbacks, self.check_errors = 0, 0, 0, []
 
     def add(self, offsets, stream=None):
+        """Adds the electrons (offsets as MultiE.add) in batches of max_batch, each checked first.
+        `stream`: a CUDA stream handle; the checks' reductions run on it too."""
+        import contextlib
         from .multie import offset_array
+        torch = self.torch
         off = offset_array(offsets)
-        for i0 in range(0, len(off), self.max_batch):
-            b = off[i0:i0 + self.max_batch]
-            for c in self.chk:
-                c.zero_()
-            self.cfast.add(b[:1], stream)
-            self.csafe.add(b[:1], stream)
-            ref = self.chk[1]
-            sel = ref > 1e-3 * ref.max()
-            e = float(self.torch.linalg.norm((self.chk[0] - ref)[sel]) / self.torch.linalg.norm(ref[sel]))
-            self.check_errors.append(e)
-            (self.fast if e <= self.tol else self.safe).add(b, stream)
-            self.fallbacks += e > self.tol
-            self.batches += 1
-            self.n += len(b)
+        ctx = torch.cuda.stream(torch.cuda.ExternalStream(stream, device=self.dev)) if stream else \
+            contextlib.nullcontext()
+        with ctx:
+            for i0 in range(0, len(off), self.max_batch):
+                b = off[i0:i0 + self.max_batch]
+                for c in self.chk:
+                    c.zero_()
+                self.cfast.add(b[:1], stream)
+                self.csafe.add(b[:1], stream)
+                ref = self.chk[1]
+                sel = ref > 1e-3 * ref.max()
+                e = float(torch.linalg.norm((self.chk[0] - ref)[sel]) / torch.linalg.norm(ref[sel]))
+                self.check_errors.append(e)
+                (self.fast if e <= self.tol else self.safe).add(b, stream)
+                self.fallbacks += e > self.tol
+                self.batches += 1
+                self.n += len(b)
 
     def mean(self):
         self.torch.cuda.synchronize(self.dev)

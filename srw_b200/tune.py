@@ -111,7 +111,7 @@ def time_passes(n, Lr, Lc, dev, reps=7, flush=None):
     return float(m[0]), float(m[1])
 
 
-def tune(lengths, dev, reps=7, log=print):
+def tune(lengths, dev, reps=7, log=print, on_length=None):
     import torch
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)      # > L2 (126 MB)
     L = capi.lib()
@@ -135,9 +135,11 @@ def tune(lengths, dev, reps=7, log=print):
         res[n] = dict(rows=best[0], cols=best[1], rows_ms=best[2], cols_ms=best[3],
                       default=[d[0].value, d[1].value], default_ms=[dflt[2], dflt[3]] if dflt else None,
                       measured=[list(m) for m in meas])
-        log('N %5d  best rows L=%d %.4f ms  cols L=%d %.4f ms  (default %s: %s)  %.1f s' % (
+        log('N %5d  best rows L=%d %.4f ms  cols L=%d %.4f ms  (default %d/%d: %s)  %.1f s' % (
             n, best[0], best[2], best[1], best[3], d[0].value, d[1].value,
             '%.4f + %.4f ms' % (dflt[2], dflt[3]) if dflt else '-', time.time() - t0))
+        if on_length is not None:
+            on_length(res)
     return res
 
 
@@ -174,8 +176,10 @@ def main():
     dev = torch.device('cuda', 0)
     lengths = [int(v) for v in args.lengths.split(',') if v] or all_lengths()
     capi.lib().srwgTuneLoad(None, None)            # measure from the built-in defaults
-    res = tune(lengths, dev, args.reps)
-    write(res, args.txt, args.json, torch.cuda.get_device_name(dev))
+    name = torch.cuda.get_device_name(dev)
+    # the table is rewritten after every length, so that an interrupted run keeps what it measured
+    res = tune(lengths, dev, args.reps, on_length=lambda r: write(r, args.txt, args.json, name))
+    write(res, args.txt, args.json, name)
     print('wrote %s, %s' % (args.txt, args.json))
 
 

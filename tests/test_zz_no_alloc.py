@@ -111,3 +111,27 @@ def test_static_refuses_above_limit():
     r, _, _, _ = run_static(w, optC, dx, dx, 16, 16)
     assert r == ERR_STATIC_LIMIT
     assert 'static limit' in capi.err_text(r)
+
+
+def test_static_refuses_capturing_stream():
+    """Each call copies its tables from host memory, so a call on a stream under capture is refused
+    before it queues anything (error 23903); the capture stays valid and later calls work."""
+    need_gpu()
+    w, optC = case('c0_128')
+    p = Plan(w, optC)
+    ex = to_dev(w.arEx, p.ny_in, p.nx_in)
+    ey = to_dev(w.arEy, p.ny_in, p.nx_in)
+    ox, oy = p.new_output()
+    keep = []
+    cw = make_c_wfr(w, keep)
+    co = make_c_optc(optC, keep)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        st = torch.cuda.current_stream().cuda_stream
+        r = capi.lib().srwgPropagElecFieldStatic(C.byref(cw), C.byref(co), ex.data_ptr(), ey.data_ptr(),
+                                                 ox.data_ptr(), oy.data_ptr(), ox.numel(), C.c_void_p(st), None)
+    assert r == 23903
+    assert 'captured' in capi.err_text(r)
+    r2, gx, _, _ = run_static(w, optC, ex, ey, p.nx_out, p.ny_out)
+    assert r2 == 0 and np.isfinite(gx.cpu().numpy()).all()

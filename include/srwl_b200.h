@@ -291,15 +291,21 @@ SRWG_API int srwgPropagElecFieldStatic(const SRWLWfr* pWfr, const SRWLOptC* pOpt
                                        const float* dEyIn, float* dExOut, float* dEyOut, long long outCapacity,
                                        void* stream, SRWLWfr* pWfrOut);
 
-/* Autotuned launch shapes (no counterpart in the reference, whose FFTs are FFTW's): lines per CTA of
- * the line passes with compile-time lengths (powers of two, and the general lengths of
- * linen_lengths.h), per axis (0 rows, 1 columns) and line length N.  The library reads the table
- * measured by srw_b200.tune from models/line_tuning.txt beside its directory (or the file named by
- * the environment variable SRWG_TUNING; "" for the built-in defaults) at its first plan.
- *   srwgTuneSetLines: sets one entry (lines = 0 removes it); error 23903 for an invalid shape
- *   srwgTuneGetLines: the value plans use now (0: not a compile-time length)
- *   srwgTuneLoad:     replaces the table by a file's entries (NULL or "": defaults only) */
+/* Autotuned launch shapes (no counterpart in the reference, whose FFTs are FFTW's): kernel family
+ * (1: the power-of-two pass, 3: the specialised pass of linen_lengths.h, which also serves the powers
+ * of two listed there) and lines per CTA of the line passes with compile-time lengths, per axis
+ * (0 rows, 1 columns) and line length N.  The library reads the table measured by srw_b200.tune from
+ * models/line_tuning.txt beside its directory (or the file named by the environment variable
+ * SRWG_TUNING; "" for the built-in defaults) at its first plan.
+ *   srwgTuneSetFamily: sets the family of one entry (0: the length's default); error 23903 when the
+ *                      family has no kernel for N
+ *   srwgTuneSetLines:  sets the lines per CTA of one entry in its family (0 removes the entry);
+ *                      error 23903 for an invalid shape
+ *   srwgTuneGetFamily / srwgTuneGetLines: what plans use now (0: not a compile-time length)
+ *   srwgTuneLoad:      replaces the table by a file's entries (NULL or "": defaults only) */
+SRWG_API int srwgTuneSetFamily(int axis, int N, int family);
 SRWG_API int srwgTuneSetLines(int axis, int N, int lines);
+SRWG_API int srwgTuneGetFamily(int axis, int N, int* family);
 SRWG_API int srwgTuneGetLines(int axis, int N, int* lines);
 SRWG_API int srwgTuneLoad(const char* path, int* nEntries);
 

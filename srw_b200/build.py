@@ -19,7 +19,7 @@ def linen_lengths():
     """Lengths of the specialised general-length line kernels (csrc/linen_lengths.h)."""
     import re
     txt = open(os.path.join(CSRC, 'linen_lengths.h')).read()
-    return [int(v) for v in re.findall(r'X\((\d+)\)', txt)]
+    return sorted(set(int(v) for v in re.findall(r'X\((\d+)\)', txt)))
 
 
 # host code: no FP contraction so the mesh bookkeeping rounds exactly like the reference

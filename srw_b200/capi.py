@@ -115,7 +115,9 @@ SYMBOLS = {
     'srwgPropagElecFieldStatic': (C.c_int, [C.POINTER(SRWLWfr), C.POINTER(SRWLOptC), C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(SRWLWfr)]),
     'srwgPlanDescribe': (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
+    'srwgTuneSetFamily': (C.c_int, [C.c_int, C.c_int, C.c_int]),
     'srwgTuneSetLines': (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    'srwgTuneGetFamily': (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
     'srwgTuneGetLines': (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
     'srwgTuneLoad': (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
     'srwgNextFftNumber': (C.c_long, [C.c_long]),

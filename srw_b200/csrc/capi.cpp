@@ -110,13 +110,24 @@ int radix_plan(int N, int* r)
 }
 
 // ------------------------------------------------------------------------------------------------
-// autotuned launch shapes: lines per CTA of the compile-time-length line kernels per (axis, N),
-// measured by srw_b200.tune and stored as lines "rows|cols N L" in models/line_tuning.txt next to
-// the library (or the file named by SRWG_TUNING); srwgTuneSetLines changes entries at run time
+// autotuned launch shapes: kernel family and lines per CTA of the compile-time-length line kernels
+// per (axis, N), measured by srw_b200.tune and stored as lines "rows|cols N L [spec]" in
+// models/line_tuning.txt next to the library (or the file named by SRWG_TUNING); "spec" selects the
+// specialised kernel for a power of two.  srwgTuneSetLines / srwgTuneSetFamily change entries at
+// run time.
 // ------------------------------------------------------------------------------------------------
 static std::mutex g_tuneMutex;
-static std::map<std::pair<int, int>, int> g_tune;
+struct TuneEntry {
+    int fam = 0;       // 0: the default family of the length
+    int lines = 0;     // 0: the family's default lines per CTA
+};
+static std::map<std::pair<int, int>, TuneEntry> g_tune;
 static bool g_tuneLoaded = false;
+
+static int default_family(int N)
+{
+    return line2_supported(N) ? FAM_POW2 : linen_supported(N) ? FAM_SPEC : 0;
+}
 
 static int tune_load_file(const char* path, int* nOut)
 {
@@ -125,12 +136,18 @@ static int tune_load_file(const char* path, int* nOut)
     char line[256];
     int n = 0;
     while (fgets(line, sizeof(line), f)) {
-        char ax[16];
+        char ax[16], fam[16] = {0};
         int N = 0, L = 0;
-        if (line[0] == '#' || sscanf(line, "%15s %d %d", ax, &N, &L) != 3) continue;
+        if (line[0] == '#') continue;
+        const int got = sscanf(line, "%15s %d %d %15s", ax, &N, &L, fam);
+        if (got < 3) continue;
         const int axis = strcmp(ax, "rows") == 0 ? 0 : strcmp(ax, "cols") == 0 ? 1 : -1;
-        if (axis < 0 || !fixed_lines_valid(axis, N, L)) continue;
-        g_tune[std::make_pair(axis, N)] = L;
+        const int f = (got == 4 && strcmp(fam, "spec") == 0) ? FAM_SPEC : default_family(N);
+        if (axis < 0 || !fixed_lines_valid(axis, N, L, f)) continue;
+        TuneEntry e;
+        e.fam = f;
+        e.lines = L;
+        g_tune[std::make_pair(axis, N)] = e;
         n++;
     }
     fclose(f);
@@ -156,16 +173,27 @@ static void tune_ensure_loaded()
     }
 }
 
+static TuneEntry tuned(int axis, int N)
+{
+    std::lock_guard<std::mutex> lk(g_tuneMutex);
+    tune_ensure_loaded();
+    auto it = g_tune.find(std::make_pair(axis, N));
+    return it != g_tune.end() ? it->second : TuneEntry();
+}
+
+int fixed_family(int axis, int N)
+{
+    const TuneEntry e = tuned(axis, N);
+    return e.fam ? e.fam : default_family(N);
+}
+
 int fixed_lines_per_cta(int axis, int N)
 {
-    if (!line2_supported(N) && !linen_supported(N)) return 0;
-    {
-        std::lock_guard<std::mutex> lk(g_tuneMutex);
-        tune_ensure_loaded();
-        auto it = g_tune.find(std::make_pair(axis, N));
-        if (it != g_tune.end()) return it->second;
-    }
-    return line2_supported(N) ? line2_lines_per_cta(axis, N) : linen_lines_per_cta(axis, N);
+    const int fam = fixed_family(axis, N);
+    if (fam != FAM_POW2 && fam != FAM_SPEC) return 0;
+    const TuneEntry e = tuned(axis, N);
+    if (e.lines > 0 && fixed_lines_valid(axis, N, e.lines, fam)) return e.lines;
+    return fam == FAM_POW2 ? line2_lines_per_cta(axis, N) : linen_lines_per_cta(axis, N);
 }
 
 int line_config(const LineDesc& d, LineLaunch& p)
@@ -175,7 +203,8 @@ int line_config(const LineDesc& d, LineLaunch& p)
     p.N = N;
     p.nlines = d.axis == 0 ? d.nz : d.nx;
     const size_t cap = SRWG_LINE_SMEM_MAX;
-    if (N >= 64 && N <= 16384 && (N & (N - 1)) == 0) {
+    const int fam = fixed_family(d.axis, N);
+    if (fam == FAM_POW2) {
         // power of two: 16 points per thread, radix-16 stages then a 16/8/4/2 stage
         p.v2 = 1;
         p.T = N / 16;
@@ -198,8 +227,9 @@ int line_config(const LineDesc& d, LineLaunch& p)
         if ((size_t)p.L * p.P * sizeof(float2) > cap) { g_lastDetail = "line too long for shared memory"; return SRWG_ERR_UNSUPPORTED; }
         return 0;
     }
-    // general length with a specialised kernel (linen.cuh): compile-time schedule, T = ceil(N/16)
-    if (linen_supported(N)) {
+    // general length (or a power of two the tuner gave it) with a specialised kernel (linen.cuh):
+    // compile-time schedule, T = ceil(N/16)
+    if (fam == FAM_SPEC) {
         p.v2 = 3;
         p.T = (N + 15) / 16;
         p.P = N + N / 16 + 4;
@@ -948,17 +978,40 @@ long srwgNextFftNumber(long n)
     return srwg::next_correct_number_for_fft(n);
 }
 
+int srwgTuneSetFamily(int axis, int N, int family)
+{
+    std::lock_guard<std::mutex> lk(g_tuneMutex);
+    tune_ensure_loaded();
+    if ((axis != 0 && axis != 1) || !default_family(N)) return SRWG_ERR_BAD_ARG;
+    const int f = family == 0 ? default_family(N) : family;
+    if (!(f == FAM_POW2 && line2_supported(N)) && !(f == FAM_SPEC && (linen_supported(N) || linen_pow2(N)))) {
+        g_lastDetail = "no kernel of this family for this line length";
+        return SRWG_ERR_BAD_ARG;
+    }
+    TuneEntry& e = g_tune[std::make_pair(axis, N)];
+    e.fam = f;
+    if (e.lines && !fixed_lines_valid(axis, N, e.lines, f)) e.lines = 0;
+    return 0;
+}
+
 int srwgTuneSetLines(int axis, int N, int lines)
 {
     std::lock_guard<std::mutex> lk(g_tuneMutex);
     tune_ensure_loaded();
     if (axis != 0 && axis != 1) return SRWG_ERR_BAD_ARG;
-    if (lines == 0) { g_tune.erase(std::make_pair(axis, N)); return 0; }
-    if (!fixed_lines_valid(axis, N, lines)) {
+    auto key = std::make_pair(axis, N);
+    auto it = g_tune.find(key);
+    const int fam = (it != g_tune.end() && it->second.fam) ? it->second.fam : default_family(N);
+    if (lines == 0) {
+        if (it != g_tune.end()) g_tune.erase(it);
+        return 0;
+    }
+    if (!fixed_lines_valid(axis, N, lines, fam)) {
         g_lastDetail = "not a valid launch shape for this line length";
         return SRWG_ERR_BAD_ARG;
     }
-    g_tune[std::make_pair(axis, N)] = lines;
+    g_tune[key].fam = fam;
+    g_tune[key].lines = lines;
     return 0;
 }
 
@@ -966,6 +1019,13 @@ int srwgTuneGetLines(int axis, int N, int* lines)
 {
     if (lines == nullptr || (axis != 0 && axis != 1)) return SRWG_ERR_BAD_ARG;
     *lines = fixed_lines_per_cta(axis, N);
+    return 0;
+}
+
+int srwgTuneGetFamily(int axis, int N, int* family)
+{
+    if (family == nullptr || (axis != 0 && axis != 1)) return SRWG_ERR_BAD_ARG;
+    *family = fixed_family(axis, N);
     return 0;
 }
 

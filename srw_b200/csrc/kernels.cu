@@ -596,6 +596,7 @@ Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt)
 {
 #define SRWG_LINEN_CASE(M) if (N == M) return linen_get_##M(cols, extra, nt);
     SRWG_LINEN_LENGTHS(SRWG_LINEN_CASE)
+    SRWG_LINEN_POW2(SRWG_LINEN_CASE)
 #undef SRWG_LINEN_CASE
     return nullptr;
 }
@@ -622,6 +623,7 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
             cudaFuncSetAttribute(linen_get_##M(e & 1, (e >> 1) & 1, 1 + (e >> 2)),                         \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
         SRWG_LINEN_LENGTHS(SRWG_LINEN_ATTR)
+        SRWG_LINEN_POW2(SRWG_LINEN_ATTR)
 #undef SRWG_LINEN_ATTR
     }
     if (p.v2 == 3) {

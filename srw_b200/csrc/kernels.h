@@ -107,9 +107,11 @@ Line2Fn lineg_e_get(bool cols);
 // specialised general-length kernels (linen.cu, one unit per length of linen_lengths.h)
 #define SRWG_LINEN_DECL(N) Line2Fn linen_get_##N(bool cols, bool extra, int nt);
 SRWG_LINEN_LENGTHS(SRWG_LINEN_DECL)
+SRWG_LINEN_POW2(SRWG_LINEN_DECL)
 #undef SRWG_LINEN_DECL
 Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt);
 inline bool line2_supported(int N) { return N >= 64 && N <= 16384 && (N & (N - 1)) == 0; }
+// general lengths of the specialised kernel
 inline bool linen_supported(int N)
 {
 #define SRWG_LINEN_IS(M) if (N == M) return true;
@@ -117,6 +119,16 @@ inline bool linen_supported(int N)
 #undef SRWG_LINEN_IS
     return false;
 }
+// powers of two that the specialised kernel is compiled for as well (the tuner's alternative)
+inline bool linen_pow2(int N)
+{
+#define SRWG_LINEN_IS(M) if (N == M) return true;
+    SRWG_LINEN_POW2(SRWG_LINEN_IS)
+#undef SRWG_LINEN_IS
+    return false;
+}
+// line-pass kernel families (LineLaunch::v2)
+enum { FAM_TAB = 0, FAM_POW2 = 1, FAM_GEN = 2, FAM_SPEC = 3 };
 // lines per CTA of the specialised general-length pass (at most 512 threads, 128 registers each):
 // rows up to 512 threads, columns a power of two up to 512 threads / 32 columns (the column-block
 // width of the row pass before it), within the shared-memory budget; T = ceil(N/16) threads per
@@ -136,19 +148,21 @@ inline int linen_lines_per_cta(int axis, int N)
     while (L > 1 && (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) L = axis == 0 ? L - 1 : L / 2;
     return L;
 }
-// whether L lines per CTA is a valid launch shape of the compile-time-length kernel of N
-inline bool fixed_lines_valid(int axis, int N, int L)
+// whether L lines per CTA is a valid launch shape of kernel family fam for length N
+inline bool fixed_lines_valid(int axis, int N, int L, int fam)
 {
     const size_t P = (size_t)N + N / 16 + 4;
     if (L < 1 || (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) return false;
     if (axis == 1 && (L > 32 || (L & (L - 1)) != 0)) return false;      // column blocks: a power of two
-    if (line2_supported(N)) return (N / 16) * L <= 1024;
-    if (linen_supported(N)) return ((N + 15) / 16) * L <= 512;
+    if (fam == FAM_POW2 && line2_supported(N)) return (N / 16) * L <= 1024;
+    if (fam == FAM_SPEC && (linen_supported(N) || linen_pow2(N))) return ((N + 15) / 16) * L <= 512;
     return false;
 }
-// lines per CTA of the line kernels with compile-time lengths (line2 / linen; they skip a zero
-// window and read / write column blocks): the autotuned value where the tuning table has one
-// (capi.cpp), else the default above; 0 for other lengths
+// kernel family and lines per CTA of the line kernels with compile-time lengths (line2 / linen; they
+// skip a zero window and read / write column blocks): the autotuned choice where the tuning table has
+// one (capi.cpp), else the power-of-two kernel for powers of two and the specialised one for the
+// listed general lengths with the defaults above; lines 0 for other lengths
+int fixed_family(int axis, int N);
 int fixed_lines_per_cta(int axis, int N);
 cudaError_t launch_resize(const ResizeLaunch& p, cudaStream_t st);
 cudaError_t launch_pw(const PwLaunch& p, cudaStream_t st);

@@ -89,16 +89,78 @@ __device__ __forceinline__ float2 factor_n(const ChainG& c, int k, int i, int li
     return f;
 }
 
-// One stage of radix R (NS: product of the radices applied before it).  IN: 0 shared memory, 1
-// shared memory through chain cin, 2 global memory through chain cin; OUT: 0 shared memory, 1 global
-// memory through chain cout.  FIRST / LAST: first / last stage of its transform (conjugation of the
-// inputs after the input chain / of the outputs before the output chain when the transform is an
-// inverse one: cj = -1).
+// Per-thread view of its line: global input and output, the plan's tables, the line factor.
+struct NLine {
+    const float2* gin;      // input line (point k at gin[k * gstr])
+    int gstr;
+    float2* gout;           // output line (point k at gout[om.at(k)])
+    OutMap om;
+    const float2* tabs;
+    const PwOps* ex;
+    int line, axis;
+    bool store;             // the line exists (inactive threads of the last tile compute on a copy of
+                            // the last line and store nothing)
+    bool has_lf;
+    float2 lf;
+    int za0, za1;           // input points outside [za0, za1] are zero
+};
+
+// padded shared-memory address of point p, and its separable form for a per-thread base plus a
+// compile-time step (exact when the step is a multiple of 16 and the base's low bits carry nothing)
+__device__ __forceinline__ float2* spad(float2* s, int p) { return s + PADN(p); }
+template <int STEP> __host__ __device__ constexpr int pstep() { return STEP + STEP / 16; }
+
+// the evaluation index of destination k through chain c (for the non-separable work)
+template <int N> __device__ __forceinline__ int chain_eval_n(const ChainG& c, int k)
+{
+    const int m = c.rs2 ? rot_n<N>(k) : k;
+    return c.mir ? (N - 1 - m) : m;
+}
+
+// the chain's factors at destinations p = j + r NR of butterfly round b (v *= tab[p] (and the
+// non-separable work)); rounds beyond the last butterfly (PART) are left alone
+template <int N, int R, int NR, int T, int B, bool PART, bool EXTRA>
+__device__ __forceinline__ void apply_factors(float2 (&v)[B][R], const NLine& x, const ChainG& c, int t)
+{
+    if (c.tab >= 0) {
+        const float2* tb = x.tabs + c.tab + t;
+#pragma unroll
+        for (int b = 0; b < B; b++)
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                if (!PART || b < B - 1 || t + T * b < NR) v[b][r] = cmul(__ldg(&tb[T * b + r * NR]), v[b][r]);
+    }
+    if (EXTRA && c.extra) {
+#pragma unroll
+        for (int b = 0; b < B; b++)
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int p = t + T * b + r * NR;
+                if (!PART || b < B - 1 || t + T * b < NR) {
+                    const int i = chain_eval_n<N>(c, p);
+                    v[b][r] = cmul(linen_extra(x.ex, x.axis == 0 ? i : x.line, x.axis == 0 ? x.line : i, x.tabs),
+                                   v[b][r]);
+                }
+            }
+    }
+}
+
+template <int B, int R> __device__ __forceinline__ void conj_all(float2 (&v)[B][R])
+{
+#pragma unroll
+    for (int b = 0; b < B; b++)
+#pragma unroll
+        for (int r = 0; r < R; r++) v[b][r].y = -v[b][r].y;
+}
+
+// One Stockham stage of radix R (NS: product of the radices applied before it).  IN: 0 shared memory,
+// 1 shared memory through chain cin (first stage of the second transform), 2 global memory through
+// chain cin; OUT: 0 shared memory, 1 global memory through chain cout.  Inverse transforms (cj < 0)
+// conjugate the inputs of their first stage after the chain and the outputs of their last stage
+// before the chain.
 template <int N, int R, int NS, int IN, int OUT, bool FIRST, bool LAST, bool EXTRA>
-__device__ __forceinline__ void nstage(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout, int gstr,
-                                       const OutMap& om, int t, int line, const ChainG& cin, const ChainG& cout, float cj,
-                                       const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
-                                       const float2* __restrict__ tabs, const PwOps* ex, int axis, int za0, int za1)
+__device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& cin, const ChainG& cout, float cj,
+                                       const float2* __restrict__ tw, int t)
 {
     constexpr int T = NPlan<N>::T;
     constexpr int NR = N / R;
@@ -107,125 +169,168 @@ __device__ __forceinline__ void nstage(float2* s, const float2* __restrict__ gin
     constexpr int TWS = N / (NS * R);
     float2 v[B][R];
     if (IN == 2) {
-        // first stage from global memory: all loads issued before any dependent arithmetic
+        // first stage from global memory: all loads issued before any dependent arithmetic; the
+        // source of destination p is p, p rotated by N/2 (a permutation of the radix index: R is even
+        // here), or the general map with the mirror
+        const bool rot = cin.rs1 != cin.rs2;
 #pragma unroll
         for (int b = 0; b < B; b++) {
             const int j = t + T * b;
-            const bool ok = active && (!PART || j < NR);
+            const bool okj = !PART || b < B - 1 || j < NR;
 #pragma unroll
             for (int r = 0; r < R; r++) {
-                int i;
-                const int q = chain_src_n<N>(cin, j + r * NR, i);
-                const bool in = ok && q >= za0 && q <= za1;
-                v[b][r] = in ? __ldcs(&gin[q * gstr]) : make_float2(0.f, 0.f);
+                int q;
+                if (!cin.mir) {
+                    const int rr = (R % 2 == 0 && rot) ? (r + R / 2) % R : r;
+                    q = j + rr * NR;
+                    if (R % 2 != 0 && rot) q = rot_n<N>(q);
+                } else {
+                    int i;
+                    q = chain_src_n<N>(cin, j + r * NR, i);
+                }
+                const bool in = okj && q >= x.za0 && q <= x.za1;
+                v[b][r] = in ? __ldcs(&x.gin[q * x.gstr]) : make_float2(0.f, 0.f);
             }
         }
-#pragma unroll
-        for (int b = 0; b < B; b++) {
-            const int j = t + T * b;
-#pragma unroll
-            for (int r = 0; r < R; r++) {
-                const int p = j + r * NR;
-                int i;
-                chain_src_n<N>(cin, p, i);
-                float2 x = cmul(factor_n<EXTRA>(cin, p, i, line, tabs, ex, axis), v[b][r]);
-                x.y *= cj;
-                v[b][r] = x;
-            }
-        }
+        apply_factors<N, R, NR, T, B, PART, EXTRA>(v, x, cin, t);
+        if (cj < 0.f) conj_all(v);
+        // NS == 1 for the first stage: no twiddles
     } else {
 #pragma unroll
         for (int b = 0; b < B; b++) {
             const int j = t + T * b;
-            const bool ok = active && (!PART || j < NR);
-            const int k = NS > 1 ? j % NS : 0;
-            float2 wp[4];
-            if (NS > 1) {
+            const bool okj = !PART || b < B - 1 || j < NR;
+            if (okj) {
+                if (IN == 0) {
+                    if constexpr (NR % 16 == 0) {
+                        const float2* sj = spad(s, j);
 #pragma unroll
-                for (int e = 0; e < 4; e++)
-                    if ((1 << e) < R) wp[e] = ok ? __ldg(&tw[(k * TWS) << e]) : make_float2(1.f, 0.f);
-            }
-#pragma unroll
-            for (int r = 0; r < R; r++) {
-                const int p = j + r * NR;
-                float2 x = make_float2(0.f, 0.f);
-                if (ok) {
-                    if (IN == 0) {
-                        x = s[PADN(p)];
+                        for (int r = 0; r < R; r++) v[b][r] = sj[r * pstep<NR>()];
                     } else {
+#pragma unroll
+                        for (int r = 0; r < R; r++) v[b][r] = *spad(s, j + r * NR);
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; r++) {
                         int i;
-                        const int q = chain_src_n<N>(cin, p, i);
-                        x = cmul(factor_n<EXTRA>(cin, p, i, line, tabs, ex, axis), s[PADN(q)]);
-                        if (FIRST) x.y *= cj;
+                        v[b][r] = *spad(s, chain_src_n<N>(cin, j + r * NR, i));
                     }
                 }
-                if (NS > 1 && r > 0) {
-                    // W^(k r) from the table powers W^k, W^2k, W^4k, W^8k
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; r++) v[b][r] = make_float2(0.f, 0.f);
+            }
+        }
+        if (IN == 1) {
+            apply_factors<N, R, NR, T, B, PART, EXTRA>(v, x, cin, t);
+            if (cj < 0.f) conj_all(v);
+        }
+        if (NS > 1) {
+            // twiddles W^(k r), k = j mod NS: the table powers W^k, W^2k, W^4k, W^8k and their products
+#pragma unroll
+            for (int b = 0; b < B; b++) {
+                const int j = t + T * b;
+                const int k = j % NS;
+                const bool okj = !PART || b < B - 1 || j < NR;
+                float2 wp[4];
+#pragma unroll
+                for (int e = 0; e < 4; e++)
+                    if ((1 << e) < R) wp[e] = okj ? __ldg(&tw[(k * TWS) << e]) : make_float2(1.f, 0.f);
+#pragma unroll
+                for (int r = 1; r < R; r++) {
                     float2 w = make_float2(1.f, 0.f);
                     bool first = true;
 #pragma unroll
                     for (int e = 0; e < 4; e++)
                         if (r & (1 << e)) { w = first ? wp[e] : cmul(w, wp[e]); first = false; }
-                    x = cmul(x, w);
+                    v[b][r] = cmul(v[b][r], w);
                 }
-                v[b][r] = x;
             }
         }
     }
     if (OUT == 0) __syncthreads();
 #pragma unroll
-    for (int b = 0; b < B; b++) {
-        const int j = t + T * b;
-        const bool ok = active && (!PART || j < NR);
-        dftR<R, 1>(v[b], tw, N);
-        const int k = NS > 1 ? j % NS : 0;
-        const int base = (j - k) * R + k;
+    for (int b = 0; b < B; b++) dftR<R, 1>(v[b], tw, N);
+    if (LAST && cj < 0.f) conj_all(v);
+    if (OUT == 0) {
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int q = base + r * NS;
-            float2 o = v[b][r];
-            if (LAST) o.y *= cj;
-            if (ok) {
-                if (OUT == 0) {
-                    s[PADN(q)] = o;
+        for (int b = 0; b < B; b++) {
+            const int j = t + T * b;
+            if (!PART || b < B - 1 || j < NR) {
+                const int k = NS > 1 ? j % NS : 0;
+                const int base = (j - k) * R + k;
+                if constexpr (NS % 16 == 0) {
+                    float2* sb = spad(s, base);
+#pragma unroll
+                    for (int r = 0; r < R; r++) sb[r * pstep<NS>()] = v[b][r];
+                } else if constexpr (NS == 1 && R == 16) {
+                    float2* sb = s + 17 * j;
+#pragma unroll
+                    for (int r = 0; r < R; r++) sb[r] = v[b][r];
                 } else {
-                    const int kk = chain_dst_n<N>(cout, q);
-                    int i;
-                    chain_src_n<N>(cout, kk, i);
-                    o = cmul(factor_n<EXTRA>(cout, kk, i, line, tabs, ex, axis), o);
-                    if (has_lf) o = cmul(lf, o);
-                    __stcs(&gout[om.at(kk)], o);
+#pragma unroll
+                    for (int r = 0; r < R; r++) *spad(s, base + r * NS) = v[b][r];
                 }
             }
         }
+        __syncthreads();
+    } else {
+        // last stage (NS R == N, so q = j + r NS): the destination is q, q rotated by N/2 (for an even
+        // radix a permutation of r), or the general map with the mirror; factors and the line factor,
+        // then the store
+        const bool rot = cout.rs1 != 0;
+#pragma unroll
+        for (int b = 0; b < B; b++) {
+            const int j = t + T * b;
+            if (!(!PART || b < B - 1 || j < NR)) continue;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                int kk;
+                if (!cout.mir) {
+                    const int rr = (R % 2 == 0 && rot) ? (r + R / 2) % R : r;
+                    kk = j + rr * NS;
+                    if (R % 2 != 0 && rot) kk = rot_n<N>(kk);
+                } else {
+                    kk = chain_dst_n<N>(cout, j + r * NS);
+                }
+                float2 o = v[b][r];
+                if (cout.tab >= 0) o = cmul(__ldg(&x.tabs[cout.tab + kk]), o);
+                if (EXTRA && cout.extra) {
+                    const int i = chain_eval_n<N>(cout, kk);
+                    o = cmul(linen_extra(x.ex, x.axis == 0 ? i : x.line, x.axis == 0 ? x.line : i, x.tabs), o);
+                }
+                if (x.has_lf) o = cmul(x.lf, o);
+                if (x.store) __stcs(&x.gout[x.om.at(kk)], o);
+            }
+        }
     }
-    if (OUT == 0) __syncthreads();
 }
 
 // one transform along the line with the compile-time schedule of N; INM: mode of the first stage's
 // input (1 shared through cin, 2 global through cin), OUTM: of the last stage's output (0 shared, 1
 // global through cout)
 template <int N, int INM, int OUTM, bool EXTRA>
-__device__ __forceinline__ void fft_n(float2* s, const float2* __restrict__ gin, float2* __restrict__ gout, int gstr,
-                                      const OutMap& om, int t, int line, const ChainG& cin, const ChainG& cout, float cj,
-                                      const float2* __restrict__ tw, bool active, bool has_lf, float2 lf,
-                                      const float2* __restrict__ tabs, const PwOps* ex, int axis, int za0, int za1)
+__device__ __forceinline__ void fft_n(float2* s, const NLine& x, const ChainG& cin, const ChainG& cout, float cj,
+                                      const float2* __restrict__ tw, int t)
 {
     constexpr NSched S = NPlan<N>::s;
     static_assert(S.n >= 2 && S.n <= 8, "radix schedule");
 #define SRWG_NSTAGE(I)                                                                                          \
     if constexpr (S.n > (I))                                                                                    \
         nstage<N, S.r[(I) < S.n ? (I) : 0], nsched_ns(N, (I)), (I) == 0 ? INM : 0, (I) == S.n - 1 ? OUTM : 0,   \
-               (I) == 0, (I) == S.n - 1, EXTRA>(s, gin, gout, gstr, om, t, line, cin, cout, cj, tw, active,    \
-                                                has_lf, lf, tabs, ex, axis, za0, za1);
+               (I) == 0, (I) == S.n - 1, EXTRA>(s, x, cin, cout, cj, tw, t);
     SRWG_NSTAGE(0) SRWG_NSTAGE(1) SRWG_NSTAGE(2) SRWG_NSTAGE(3)
     SRWG_NSTAGE(4) SRWG_NSTAGE(5) SRWG_NSTAGE(6) SRWG_NSTAGE(7)
 #undef SRWG_NSTAGE
 }
 
-// NT: transforms in the pass (1 or 2); their directions come from the descriptor
+// NT: transforms in the pass (1 or 2); their directions come from the descriptor.  Passes with one
+// transform and no non-separable work run at two 512-thread CTAs per SM (64 registers per thread,
+// measured: at most a few spilled words); the others keep 128 registers (their state spills heavily
+// at 64).
 template <int N, bool COLS, bool EXTRA, int NT>
-__global__ void __launch_bounds__(512, 1) linen_kernel(const LineLaunch p)
+__global__ void __launch_bounds__(512, (EXTRA || NT == 2) ? 1 : 2) linen_kernel(const LineLaunch p)
 {
     constexpr int T = NPlan<N>::T;
     extern __shared__ float2 smn[];
@@ -237,64 +342,64 @@ __global__ void __launch_bounds__(512, 1) linen_kernel(const LineLaunch p)
     const int tid = threadIdx.x;
     const int g = COLS ? (tid % L) : (tid / T);          // line of the tile
     const int t = COLS ? (tid / L) : (tid - g * T);      // thread within the line
-    const int line = blockIdx.x * L + g;
-    const bool active = line < nl && g < L;
-    float2* s = smn + (size_t)(g < L ? g : 0) * P;
-    int gstr = COLS ? nl : 1;
-    const float2* gin = COLS ? (src + line) : (src + (size_t)line * N);
+    const int line0 = blockIdx.x * L + g;
+    NLine x;
+    x.store = line0 < nl;
+    const int line = x.store ? line0 : nl - 1;           // inactive threads work on the last line
+    x.line = line;
+    x.axis = d.axis;
+    float2* s = smn + (size_t)g * P;
+    x.gstr = COLS ? nl : 1;
+    x.gin = COLS ? (src + line) : (src + (size_t)line * N);
     if (COLS && d.blk_in > 0) {
-        gstr = d.blk_in;
-        gin = src + (size_t)(line / d.blk_in) * N * d.blk_in + (line % d.blk_in);
+        x.gstr = d.blk_in;
+        x.gin = src + (size_t)(line / d.blk_in) * N * d.blk_in + (line % d.blk_in);
     }
     const int oline = d.mirror_lines ? (nl - 1 - line) : line;
-    float2* gout = COLS ? (dst + oline) : (dst + (size_t)oline * N);
-    OutMap om;
-    om.str = COLS ? nl : 1;
-    om.lg = -1;
-    om.bstr = 0;
+    x.gout = COLS ? (dst + oline) : (dst + (size_t)oline * N);
+    x.om.str = COLS ? nl : 1;
+    x.om.lg = -1;
+    x.om.bstr = 0;
     if (!COLS && d.blk_out > 0) {
-        om.lg = 31 - __clz(d.blk_out);
-        om.bstr = nl * d.blk_out;
-        gout = dst + (size_t)oline * d.blk_out;
+        x.om.lg = 31 - __clz(d.blk_out);
+        x.om.bstr = nl * d.blk_out;
+        x.gout = dst + (size_t)oline * d.blk_out;
     }
-    int za0 = 0, za1 = N - 1;
+    x.za0 = 0;
+    x.za1 = N - 1;
     if (d.zwin) {
         const int l0 = blockIdx.x * L, l1 = min(l0 + L, nl) - 1;
         if (l1 < d.zl0 || l0 > d.zl1) {
             // the whole tile is zero: so is its transform
-            if (active)
-                for (int m = t; m < N; m += T) __stcs(&gout[om.at(m)], make_float2(0.f, 0.f));
+            if (x.store)
+                for (int m = t; m < N; m += T) __stcs(&x.gout[x.om.at(m)], make_float2(0.f, 0.f));
             return;
         }
-        if (line < d.zl0 || line > d.zl1) { za0 = 1; za1 = 0; }
-        else { za0 = d.za0; za1 = d.za1; }
+        if (line < d.zl0 || line > d.zl1) { x.za0 = 1; x.za1 = 0; }
+        else { x.za0 = d.za0; x.za1 = d.za1; }
     }
-    const float2* tabs = p.tabs + blockIdx.z * p.bTab;
-    const PwOps* ex = &d.extra;
-    const int axis = d.axis;
+    x.tabs = p.tabs + blockIdx.z * p.bTab;
+    x.ex = &d.extra;
     ChainG pre, mid, fin;
     pre.rs1 = 0; pre.mir = 0; pre.rs2 = d.f1_pre.rs; pre.tab = (int)d.t_pre.tab; pre.extra = 0;
     mid.rs1 = d.f1 ? d.f1_post.rs : 0; mid.mir = d.mirror_along; mid.rs2 = d.f2 ? d.f2_pre.rs : 0;
     mid.tab = (int)d.t_mid.tab; mid.extra = EXTRA ? d.has_extra : 0;
     fin.rs1 = d.f2 ? d.f2_post.rs : 0; fin.mir = 0; fin.rs2 = 0; fin.tab = (int)d.t_fin.tab; fin.extra = 0;
-    const bool has_lf = (d.t_pre.ltab >= 0) || (d.t_mid.ltab >= 0) || (d.t_fin.ltab >= 0);
-    float2 lf = make_float2(1.f, 0.f);
-    if (has_lf && active) {
-        if (d.t_pre.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_pre.ltab + line]));
-        if (d.t_mid.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_mid.ltab + line]));
-        if (d.t_fin.ltab >= 0) lf = cmul(lf, __ldg(&tabs[d.t_fin.ltab + line]));
+    x.has_lf = (d.t_pre.ltab >= 0) || (d.t_mid.ltab >= 0) || (d.t_fin.ltab >= 0);
+    x.lf = make_float2(1.f, 0.f);
+    if (x.has_lf) {
+        if (d.t_pre.ltab >= 0) x.lf = cmul(x.lf, __ldg(&x.tabs[d.t_pre.ltab + line]));
+        if (d.t_mid.ltab >= 0) x.lf = cmul(x.lf, __ldg(&x.tabs[d.t_mid.ltab + line]));
+        if (d.t_fin.ltab >= 0) x.lf = cmul(x.lf, __ldg(&x.tabs[d.t_fin.ltab + line]));
     }
     const float2* tw = p.tw;
     if constexpr (NT == 2) {
-        fft_n<N, 2, 0, EXTRA>(s, gin, nullptr, gstr, om, t, line, pre, mid, d.f1 < 0 ? -1.f : 1.f, tw, active, has_lf,
-                              lf, tabs, ex, axis, za0, za1);
-        fft_n<N, 1, 1, EXTRA>(s, nullptr, gout, gstr, om, t, line, mid, fin, d.f2 < 0 ? -1.f : 1.f, tw, active, has_lf,
-                              lf, tabs, ex, axis, 0, N - 1);
+        fft_n<N, 2, 0, EXTRA>(s, x, pre, mid, d.f1 < 0 ? -1.f : 1.f, tw, t);
+        fft_n<N, 1, 1, EXTRA>(s, x, mid, fin, d.f2 < 0 ? -1.f : 1.f, tw, t);
     } else {
         const bool one = d.f1 != 0;
         const float cj = (one ? d.f1 : d.f2) < 0 ? -1.f : 1.f;
-        fft_n<N, 2, 1, EXTRA>(s, gin, gout, gstr, om, t, line, one ? pre : mid, one ? mid : fin, cj, tw, active, has_lf,
-                              lf, tabs, ex, axis, za0, za1);
+        fft_n<N, 2, 1, EXTRA>(s, x, one ? pre : mid, one ? mid : fin, cj, tw, t);
     }
 }
 

@@ -472,6 +472,7 @@ def choose_grid(pred, nx, nz):
 # labels
 # ------------------------------------------------------------------------------------------------
 def label_case(case, dev, stream=None):
+    import torch
     """Cheapest factors (pxm, pxd, pzm, pzd) within tolerance of the oversampled propagation: per
     axis the candidate pairs in order of the resized length (the other axis at the conservative
     factors), the first within AXIS_TOL found by bisection; the combination is checked against
@@ -480,6 +481,9 @@ def label_case(case, dev, stream=None):
     n = case['mesh']['nx']
     rf = ref_factors(n)
     Iref, omref = propagate_intensity(case, rf + rf, dev, stream)
+    mx = float(Iref.max())
+    if not math.isfinite(mx) or mx <= 0. or not bool(torch.isfinite(Iref).all()):
+        raise ValueError('no usable reference intensity (aperture blocks the beam?)')
     box = eval_box(Iref, omref)
     cache = {}
 
@@ -665,36 +669,49 @@ class CheckedMultiE(object):
 # ------------------------------------------------------------------------------------------------
 # training
 # ------------------------------------------------------------------------------------------------
-def make_data(n_samples, seed, dev, threads=8, log=print):
+def make_data(n_samples, seed, dev, threads=8, log=print, path=None, chunk=2000):
     """Features, targets, label errors and evaluation counts of n_samples seeded cases, labelled on
-    `threads` host threads (each with its own CUDA stream: the planner runs on the host)."""
+    `threads` host threads (each with its own CUDA stream: the planner runs on the host).  A case
+    whose labelling fails (no usable reference intensity) is replaced by the next seed.  With `path`
+    the data so far is saved after every `chunk` samples, and a run resumes from a saved file."""
     import torch
     from concurrent.futures import ThreadPoolExecutor
     X = np.zeros((n_samples, N_IN), np.float32)
     T = np.zeros((n_samples, N_OUT), np.float32)
     E = np.zeros(n_samples)
     NE = np.zeros(n_samples, np.int32)
+    done0 = 0
+    if path and os.path.exists(path):
+        d = np.load(path)
+        done0 = min(len(d['X']), n_samples)
+        X[:done0], T[:done0], E[:done0], NE[:done0] = d['X'][:done0], d['T'][:done0], d['E'][:done0], d['NE'][:done0]
+        log('resuming after %d saved samples' % done0)
     t0 = time.time()
-    done = [0]
-    lock = threading.Lock()
     local = threading.local()
 
     def one(s):
         if not hasattr(local, 'stream'):
             local.stream = torch.cuda.Stream(dev)
-        rng = np.random.default_rng([seed, s])
-        case = sample_case(rng)
-        with torch.cuda.stream(local.stream):
-            X[s] = case_features(case, dev).cpu().numpy()
-            lab, e, ne = label_case(case, dev, local.stream)
-        T[s], E[s], NE[s] = target(lab), e, ne
-        with lock:
-            done[0] += 1
-            if done[0] % 500 == 0:
-                log('labelled %d (%.0f s)' % (done[0], time.time() - t0))
+        for attempt in range(20):
+            rng = np.random.default_rng([seed, s, attempt])
+            case = sample_case(rng)
+            try:
+                with torch.cuda.stream(local.stream):
+                    x = case_features(case, dev).cpu().numpy()
+                    lab, e, ne = label_case(case, dev, local.stream)
+            except ValueError:
+                continue
+            X[s], T[s], E[s], NE[s] = x, target(lab), e, ne
+            return
+        raise RuntimeError('no usable case for sample %d' % s)
 
     with ThreadPoolExecutor(threads) as ex:
-        list(ex.map(one, range(n_samples)))
+        for c0 in range(done0, n_samples, chunk):
+            c1 = min(n_samples, c0 + chunk)
+            list(ex.map(one, range(c0, c1)))
+            log('labelled %d (%.0f s)' % (c1, time.time() - t0))
+            if path:
+                np.savez_compressed(path, X=X[:c1], T=T[:c1], E=E[:c1], NE=NE[:c1])
     return X, T, E, NE
 
 
@@ -711,13 +728,7 @@ def main():
     args = ap.parse_args()
     dev = torch.device('cuda', 0)
     t0 = time.time()
-    if args.data and os.path.exists(args.data):
-        d = np.load(args.data)
-        X, T, E, NE = d['X'], d['T'], d['E'], d['NE']
-    else:
-        X, T, E, NE = make_data(args.samples, args.seed, dev, args.threads)
-        if args.data:
-            np.savez_compressed(args.data, X=X, T=T, E=E, NE=NE)
+    X, T, E, NE = make_data(args.samples, args.seed, dev, args.threads, path=args.data)
     t_data = time.time() - t0
     nv = int(len(X) * args.val)
     Xt, Tt = torch.from_numpy(X[nv:]).to(dev), torch.from_numpy(T[nv:]).to(dev)

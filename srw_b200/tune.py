@@ -3,12 +3,13 @@ gmfft.cpp:295; its CUDA build caches cuFFT plans, gmfft.h:182-187).
 
 For every line length with a compile-time kernel (powers of two and the general lengths of
 csrc/linen_lengths.h) it times the two passes of an N x N propagation to the waist (a row pass and
-a column pass, the headline beamline's FFT) for every valid number of lines per CTA of each pass
--- which is also the CTA size and, for the column pass, the width of the column blocks the row pass
-writes -- with CUDA events on the launching stream and L2 flushed between repetitions, keeps the
-fastest pair and writes
+a column pass, the headline beamline's FFT) for every valid kernel family (powers of two: the
+power-of-two pass or the specialised pass) and number of lines per CTA of each pass -- which is
+also the CTA size and, for the column pass, the width of the column blocks the row pass writes --
+with CUDA events on the launching stream and L2 flushed between repetitions, keeps the fastest
+pair and writes
 
-  models/line_tuning.txt    "rows|cols N L" lines, read by the library at its first plan
+  models/line_tuning.txt    "rows|cols N L [spec]" lines, read by the library at its first plan
   models/line_tuning.json   every measurement (ms per pass), read by the learned-factor cost model
 
     python -m srw_b200.tune [--lengths 1280,2240] [--reps 7]          # GPU
@@ -34,7 +35,9 @@ SMEM_MAX = 220 * 1024
 
 
 def general_lengths():
-    return [int(v) for v in re.findall(r'X\((\d+)\)', open(LENGTHS_H).read())]
+    txt = open(LENGTHS_H).read()
+    block = txt[txt.index('SRWG_LINEN_LENGTHS(X)'):txt.index('SRWG_LINEN_POW2(X)')]
+    return [int(v) for v in re.findall(r'X\((\d+)\)', block)]
 
 
 def all_lengths(lo=256, hi=8192):
@@ -46,21 +49,33 @@ def is_pow2(n):
     return n & (n - 1) == 0
 
 
-def candidates(axis, n):
-    """Valid lines per CTA (the library's fixed_lines_valid): shared memory, threads per CTA (1024
-    for powers of two, 512 for general lengths), columns a power of two up to 32."""
-    t = n // 16 if is_pow2(n) else (n + 15) // 16
-    tmax = 1024 if is_pow2(n) else 512
-    p = n + n // 16 + 4
+FAM_POW2, FAM_SPEC = 1, 3          # kernel families: power-of-two pass, specialised pass
+POW2_SPEC = [256, 512, 1024, 2048, 4096, 8192]       # powers of two the specialised pass is built for
+
+
+def families(n):
+    if is_pow2(n):
+        return [FAM_POW2] + ([FAM_SPEC] if n in POW2_SPEC else [])
+    return [FAM_SPEC]
+
+
+def candidates(axis, n, fam=None):
+    """Valid (family, lines per CTA) pairs (the library's fixed_lines_valid): shared memory, threads
+    per CTA (1024 for the power-of-two pass, 512 for the specialised one), columns a power of two up
+    to 32; `fam` restricts them to one family (then plain lines per CTA are returned)."""
     out = []
-    for L in range(1, 33):
-        if L * p * 8 > SMEM_MAX or t * L > tmax:
-            break
-        if axis == 1 and (L & (L - 1)):
-            continue
-        if axis == 0 and L > 8:
-            break
-        out.append(L)
+    for f in families(n) if fam is None else [fam]:
+        t = n // 16 if f == FAM_POW2 else (n + 15) // 16
+        tmax = 1024 if f == FAM_POW2 else 512
+        p = n + n // 16 + 4
+        for L in range(1, 33):
+            if L * p * 8 > SMEM_MAX or t * L > tmax:
+                break
+            if axis == 1 and (L & (L - 1)):
+                continue
+            if axis == 0 and L > 8:
+                break
+            out.append(L if fam is not None else (f, L))
     return out
 
 
@@ -85,12 +100,15 @@ def _plan(n, dev):
     return Plan(w, opt, device=dev.index), ex
 
 
-def time_passes(n, Lr, Lc, dev, reps=7, flush=None):
-    """Median CUDA-event time [ms] of the row and the column pass with Lr / Lc lines per CTA."""
+def time_passes(n, cr, cc, dev, reps=7, flush=None):
+    """Median CUDA-event time [ms] of the row and the column pass with the (family, lines per CTA)
+    pairs cr / cc."""
     import torch
     L = capi.lib()
-    capi.check(L.srwgTuneSetLines(0, n, Lr), 'tune rows')
-    capi.check(L.srwgTuneSetLines(1, n, Lc), 'tune cols')
+    capi.check(L.srwgTuneSetFamily(0, n, cr[0]), 'tune rows')
+    capi.check(L.srwgTuneSetLines(0, n, cr[1]), 'tune rows')
+    capi.check(L.srwgTuneSetFamily(1, n, cc[0]), 'tune cols')
+    capi.check(L.srwgTuneSetLines(1, n, cc[1]), 'tune cols')
     p, ex = _plan(n, dev)
     kinds = [k[0] for k in p.kernels()]
     if kinds != ['line_rows', 'line_cols']:
@@ -120,23 +138,27 @@ def tune(lengths, dev, reps=7, log=print, on_length=None):
         t0 = time.time()
         rows_c, cols_c = candidates(0, n), candidates(1, n)
         meas = []
-        for Lc in cols_c:
-            for Lr in rows_c:
-                tr, tc = time_passes(n, Lr, Lc, dev, reps, flush)
-                meas.append((Lr, Lc, tr, tc))
+        for cc in cols_c:
+            for cr in rows_c:
+                tr, tc = time_passes(n, cr, cc, dev, reps, flush)
+                meas.append((cr, cc, tr, tc))
         # defaults (the library's own choice without a table entry), for the record
-        capi.check(L.srwgTuneSetLines(0, n, 0), 'tune')
-        capi.check(L.srwgTuneSetLines(1, n, 0), 'tune')
-        d = [C.c_int(), C.c_int()]
-        L.srwgTuneGetLines(0, n, C.byref(d[0]))
-        L.srwgTuneGetLines(1, n, C.byref(d[1]))
-        dflt = next((m for m in meas if m[0] == d[0].value and m[1] == d[1].value), None)
+        for ax in (0, 1):
+            capi.check(L.srwgTuneSetLines(ax, n, 0), 'tune')
+        d = [C.c_int() for _ in range(4)]
+        L.srwgTuneGetFamily(0, n, C.byref(d[0]))
+        L.srwgTuneGetLines(0, n, C.byref(d[1]))
+        L.srwgTuneGetFamily(1, n, C.byref(d[2]))
+        L.srwgTuneGetLines(1, n, C.byref(d[3]))
+        dr, dc = (d[0].value, d[1].value), (d[2].value, d[3].value)
+        dflt = next((m for m in meas if m[0] == dr and m[1] == dc), None)
         best = min(meas, key=lambda m: m[2] + m[3])
-        res[n] = dict(rows=best[0], cols=best[1], rows_ms=best[2], cols_ms=best[3],
-                      default=[d[0].value, d[1].value], default_ms=[dflt[2], dflt[3]] if dflt else None,
-                      measured=[list(m) for m in meas])
-        log('N %5d  best rows L=%d %.4f ms  cols L=%d %.4f ms  (default %d/%d: %s)  %.1f s' % (
-            n, best[0], best[2], best[1], best[3], d[0].value, d[1].value,
+        res[n] = dict(rows=best[0][1], rows_family=best[0][0], cols=best[1][1], cols_family=best[1][0],
+                      rows_ms=best[2], cols_ms=best[3], default=[list(dr), list(dc)],
+                      default_ms=[dflt[2], dflt[3]] if dflt else None,
+                      measured=[[list(m[0]), list(m[1]), m[2], m[3]] for m in meas])
+        log('N %5d  best rows %s %.4f ms  cols %s %.4f ms  (default %s / %s: %s)  %.1f s' % (
+            n, best[0], best[2], best[1], best[3], dr, dc,
             '%.4f + %.4f ms' % (dflt[2], dflt[3]) if dflt else '-', time.time() - t0))
         if on_length is not None:
             on_length(res)
@@ -151,8 +173,9 @@ def write(res, txt=TXT, jsn=JSN, device_name=''):
                 % device_name)
         for n in sorted(res):
             r = res[n]
-            f.write('rows %d %d\n' % (n, r['rows']))
-            f.write('cols %d %d\n' % (n, r['cols']))
+            for ax in ('rows', 'cols'):
+                spec = ' spec' if (is_pow2(n) and r[ax + '_family'] == FAM_SPEC) else ''
+                f.write('%s %d %d%s\n' % (ax, n, r[ax], spec))
     with open(jsn, 'w') as f:
         json.dump({'device': device_name, 'lengths': {str(n): res[n] for n in sorted(res)}}, f, indent=0)
 

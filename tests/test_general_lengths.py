@@ -15,7 +15,9 @@ LENGTHS_H = os.path.join(os.path.dirname(HERE), 'srw_b200', 'csrc', 'linen_lengt
 
 
 def linen_lengths():
-    return [int(v) for v in re.findall(r'X\((\d+)\)', open(LENGTHS_H).read())]
+    txt = open(LENGTHS_H).read()
+    block = txt[txt.index('SRWG_LINEN_LENGTHS(X)'):txt.index('SRWG_LINEN_POW2(X)')]
+    return [int(v) for v in re.findall(r'X\((\d+)\)', block)]
 
 
 def schedule(n):

@@ -17,17 +17,18 @@ def table():
         for line in open(tune.TXT):
             if line.startswith('#') or not line.strip():
                 continue
-            ax, n, L = line.split()
-            out.append((0 if ax == 'rows' else 1, int(n), int(L)))
+            f = line.split()
+            fam = tune.FAM_SPEC if (len(f) > 3 and f[3] == 'spec') or not tune.is_pow2(int(f[1])) else tune.FAM_POW2
+            out.append((0 if f[0] == 'rows' else 1, int(f[1]), int(f[2]), fam))
     return out
 
 
 def test_tuning_table_valid_shapes():
     t = table()
     lengths = set(tune.all_lengths(64, 16384))
-    for axis, n, L in t:
+    for axis, n, L, fam in t:
         assert n in lengths or (n & (n - 1)) == 0, n
-        assert L in tune.candidates(axis, n), (axis, n, L)
+        assert L in tune.candidates(axis, n, fam), (axis, n, L, fam)
 
 
 def test_tuning_entry_points_validate():
@@ -40,6 +41,13 @@ def test_tuning_entry_points_validate():
     assert L.srwgTuneSetLines(2, 4096, 1) != 0
     assert L.srwgTuneSetLines(0, 2240, 2) == 0
     assert L.srwgTuneGetLines(0, 2240, C.byref(got)) == 0 and got.value == 2
+    assert L.srwgTuneSetFamily(0, 2240, 1) != 0          # no power-of-two kernel for 2240
+    assert L.srwgTuneSetFamily(1, 4096, 3) == 0          # the specialised kernel also serves 4096
+    assert L.srwgTuneGetFamily(1, 4096, C.byref(got)) == 0 and got.value == 3
+    assert L.srwgTuneSetLines(1, 4096, 4) != 0           # 4 x 256 threads: above its 512
+    assert L.srwgTuneSetLines(1, 4096, 2) == 0
+    assert L.srwgTuneSetFamily(1, 4096, 0) == 0 and L.srwgTuneGetFamily(1, 4096, C.byref(got)) == 0
+    assert got.value == 1
     n = C.c_int()
     assert L.srwgTuneLoad(tune.TXT.encode() if os.path.exists(tune.TXT) else None, C.byref(n)) == 0
 
@@ -55,7 +63,7 @@ def test_tuned_shapes_give_identical_fields():
     dev = torch.device('cuda', 0)
     L = capi.lib()
     try:
-        for n in sorted({e[1] for e in t if e[1] <= 4096}):
+        for n in sorted({e[1] for e in t if e[1] <= 4096} | {1024, 4096}):
             outs = []
             for use_table in (False, True):
                 if use_table:

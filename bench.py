@@ -352,15 +352,15 @@ def kernel_bytes(k):
     return 2 * 8 * 2 * k[1] * k[2]
 
 
-def measure_plain(args, dev, world, dist):
+def measure_plain(args, dev, world, dist, factors=CONFIGURED):
     """Single-wavefront path: one propagation per step on a device-resident field, CUDA events per
-    step and per pass (roofline), L2 flushed between steps."""
+    step and per pass (roofline), L2 flushed between steps; `factors`: the resize before the lens."""
     import torch
     from srw_b200 import srwlib as mod
     from srw_b200.plan import Plan
     ex, ey, mesh, sc = synth_undulator_field(1024)
     w = make_wfr(mod, ex, ey, mesh, sc)
-    plan = Plan(w, beamline_objs(mod), device=dev.index)
+    plan = Plan(w, beamline_objs(mod, factors), device=dev.index)
     dex = torch.from_numpy(ex).to(dev)
     dey = torch.from_numpy(ey).to(dev)
     ox, oy = plan.new_output()
@@ -727,11 +727,13 @@ def run_ours(args, rank, world):
     if not args.no_learned:
         ln = measure_learned(args, dev, world, dist, bt['acc'])
     plan, kinfo, per_k = pl['plan'], pl['kinfo'], pl['per_k']
-
-    # roofline of the dominant pass (live, the plain path's timed steps; same kernels as the batch)
-    kd = int(np.argmax(per_k))
-    alg = kernel_bytes(kinfo[kd])
-    achieved = alg / (per_k[kd] / 1000.) / 1e9
+    # the single-wavefront passes at the learned factors (their dominant pass is the headline's)
+    pl_l = None
+    if ln is not None and not ln['fallback']:
+        pl_l = measure_plain(args, dev, world, dist, tuple(ln['factors']))
+        ln['plain_at_learned_factors'] = {"ms_per_propagation": pl_l['total_ms'] / pl_l['steps'],
+                                          "passes": [list(k) for k in pl_l['kinfo']],
+                                          "per_pass_ms": [round(float(v), 4) for v in pl_l['per_k']]}
     peak, peak_src = 6650., 'fallback'
     if os.path.exists(PEAKS):
         peak, peak_src = float(json.load(open(PEAKS))['hbm_gbs']), 'measured'
@@ -800,13 +802,11 @@ def run_ours(args, rank, world):
                               "reduced_over_ranks": world > 1},
            "batched_configured": {"value": bt['value'], "unit": UNIT, "factors": list(CONFIGURED), "batch": BATCH},
            "learned": ln,
-           "roofline": {"bound": "hbm", "kernel": "%s %s" % (kinfo[kd][0], 'x'.join(map(str, kinfo[kd][1:]))),
-                        "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "peak_source": peak_src, "traffic": TRAFFIC.get(kinfo[kd]),
-                        "algorithmic_bytes": alg, "avg_ms": float(per_k[kd]),
-                        "step_frac": (total_alg / (pl['total_ms'] / pl['steps'] / 1000.) / 1e9) / peak,
-                        "per_pass_ms": [round(float(v), 4) for v in per_k],
-                        "measured_on": "plain leg, CUDA events per pass"},
+           "roofline": roofline(pl_l if (use_learned and pl_l is not None) else pl, peak, peak_src,
+                                "%s leg, single-wavefront passes, CUDA events per pass" %
+                                ("learned-factor" if (use_learned and pl_l is not None) else "plain")),
+           "roofline_plain": dict(roofline(pl, peak, peak_src, "plain leg, CUDA events per pass"),
+                                  step_frac=(total_alg / (pl['total_ms'] / pl['steps'] / 1000.) / 1e9) / peak),
            "cpu_baseline": cpu,
            "rel_err_vs_fp64_oracle": (orc or {}).get('rel_err_learned_vs_fp64_oracle' if use_learned else
                                                      'rel_err_configured_vs_fp64_oracle'),
@@ -817,6 +817,20 @@ def run_ours(args, rank, world):
            "clocks": (ln['clocks'] if use_learned and ln.get('clocks') else bt['clocks']),
            "gpu_launches": (ln['launches_per_step'] if use_learned else plan.n_kernels + 2) * args.steps}
     print(json.dumps(out))
+
+
+def roofline(pl, peak, peak_src, where):
+    """Roofline object of the dominant pass of a measure_plain result: algorithmic bytes per launch
+    over its average CUDA-event time, against the HBM peak."""
+    kinfo, per_k = pl['kinfo'], pl['per_k']
+    kd = int(np.argmax(per_k))
+    alg = kernel_bytes(kinfo[kd])
+    achieved = alg / (per_k[kd] / 1000.) / 1e9
+    return {"bound": "hbm", "kernel": "%s %s" % (kinfo[kd][0], 'x'.join(map(str, kinfo[kd][1:]))),
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+            "traffic": TRAFFIC.get(kinfo[kd]), "algorithmic_bytes": alg, "avg_ms": float(per_k[kd]),
+            "per_pass_ms": [round(float(v), 4) for v in per_k], "passes": [list(k) for k in kinfo],
+            "measured_on": where}
 
 
 def e2e_drop_in(args, dev, plan, srwl, mod, world):

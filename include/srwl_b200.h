@@ -309,6 +309,14 @@ SRWG_API int srwgTuneGetFamily(int axis, int N, int* family);
 SRWG_API int srwgTuneGetLines(int axis, int N, int* lines);
 SRWG_API int srwgTuneLoad(const char* path, int* nEntries);
 
+/* Bounded waits of the kernels (the specialised line passes wait for the bulk copies of their input
+ * tiles): srwgSetWaitLimit sets the iteration limit of those waits (0: the built-in limit, far above
+ * any copy's time); a wait that reaches it counts the event in a per-device counter, lets the copies
+ * in flight land, and the CTA skips its work (the pass's output is then incomplete).
+ * srwgGetWaitStatus reads that counter of `device` (and clears it when reset != 0). */
+SRWG_API int srwgSetWaitLimit(long long iterations);
+SRWG_API int srwgGetWaitStatus(int device, int* count, int reset);
+
 /* The number of points a resize gives for a requested n: the next good FFT number at or above n
  * (NextCorrectNumberForFFT, cpp/src/ext/genmath/gmfft.cpp:156), as the planner uses it. */
 SRWG_API long srwgNextFftNumber(long n);

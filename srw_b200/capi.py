@@ -121,6 +121,8 @@ SYMBOLS = {
     'srwgTuneGetLines': (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int)]),
     'srwgTuneLoad': (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
     'srwgNextFftNumber': (C.c_long, [C.c_long]),
+    'srwgSetWaitLimit': (C.c_int, [C.c_longlong]),
+    'srwgGetWaitStatus': (C.c_int, [C.c_int, C.POINTER(C.c_int), C.c_int]),
 }
 
 _lib = None

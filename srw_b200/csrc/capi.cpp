@@ -31,6 +31,8 @@ static std::mutex g_mutex;
 std::mutex& library_mutex() { return g_mutex; }
 
 static std::map<int, DeviceCtx*> g_ctx;
+static long long g_waitLimit = 0;                           // 0: the kernels' own default
+long long wait_limit() { return g_waitLimit; }
 
 #define CUDA_TRY(x)                                                                     \
     do {                                                                                \
@@ -62,6 +64,8 @@ int device_ctx(int dev, DeviceCtx** out)
     DeviceCtx* c = new DeviceCtx();
     c->dev = dev;
     CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaMalloc(&c->status, sizeof(int)));
+    CUDA_TRY(cudaMemset(c->status, 0, sizeof(int)));
     g_ctx[dev] = c;
     *out = c;
     return 0;
@@ -219,7 +223,7 @@ int line_config(const LineDesc& d, LineLaunch& p)
         p.radix[p.nst++] = 1 << nb;          // 16, 8, 4 or 2
         // one pad point per 16 (conflict-free Stockham exchanges) plus 4 per line, so that the
         // lines of a tile start 8 banks apart
-        p.P = N + N / 16 + 4;
+        p.P = (int)line_pitch(N);
         const int L = fixed_lines_per_cta(d.axis, N);
         if (p.T * L > 1024) { g_lastDetail = "line pass too large"; return SRWG_ERR_UNSUPPORTED; }
         p.L = L;
@@ -232,7 +236,7 @@ int line_config(const LineDesc& d, LineLaunch& p)
     if (fam == FAM_SPEC) {
         p.v2 = 3;
         p.T = (N + 15) / 16;
-        p.P = N + N / 16 + 4;
+        p.P = (int)line_pitch(N);
         p.L = fixed_lines_per_cta(d.axis, N);
         p.G = p.L;
         p.nst = 0;
@@ -254,7 +258,7 @@ int line_config(const LineDesc& d, LineLaunch& p)
             int T = (N + 15) / 16;
             T = ((T + 31) / 32) * 32;
             p.T = T;
-            p.P = N + N / 16 + 4;
+            p.P = (int)line_pitch(N);
             int L = d.axis == 0 ? 256 / T : 512 / T;
             if (L < 1) L = 1;
             while (L > 1 && (size_t)L * p.P * sizeof(float2) > cap) L--;
@@ -395,6 +399,8 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
             p.tabs = tabs;
             p.gd = &gk[i].line;
             p.nb = nb; p.bDesc = constStride; p.bTab = tabStride; p.bSrc = bSrc; p.bDst = bDst;
+            p.status = c.status;
+            p.spin = g_waitLimit;
             e = launch_line(p, st);
         } else if (k.kind == K_RESIZE) {
             ResizeLaunch p;
@@ -970,6 +976,26 @@ int srwgPlanExecuteTimed(srwgPlan* plan, const float* dExIn, const float* dEyIn,
 int srwgPlanDestroy(srwgPlan* plan)
 {
     delete plan;
+    return 0;
+}
+
+int srwgSetWaitLimit(long long iterations)
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    if (iterations < 0) return SRWG_ERR_BAD_ARG;
+    g_waitLimit = iterations;
+    return 0;
+}
+
+int srwgGetWaitStatus(int device, int* count, int reset)
+{
+    std::lock_guard<std::mutex> lk(g_mutex);
+    if (count == nullptr) return SRWG_ERR_BAD_ARG;
+    DeviceCtx* c = nullptr;
+    int r = device_ctx(device, &c);
+    if (r) return r;
+    CUDA_TRY(cudaMemcpy(count, c->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (reset) CUDA_TRY(cudaMemset(c->status, 0, sizeof(int)));
     return 0;
 }
 

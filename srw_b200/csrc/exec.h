@@ -26,7 +26,9 @@ struct DeviceCtx {
     size_t genBytes = 0;
     size_t stgElems[2] = {0, 0};
     cudaStream_t stream = nullptr;
+    int* status = nullptr;              // device counter of bounded waits that gave up (kernels add to it)
 };
+long long wait_limit();                               // iteration limit of the kernels' bounded waits (0: default)
 std::mutex& library_mutex();                          // serialises the entry points
 int device_ctx(int dev, DeviceCtx** out);             // makes `dev` current, returns its state
 int device_twiddles(DeviceCtx& c, int N, const float2** out);

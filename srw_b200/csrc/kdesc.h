@@ -92,6 +92,9 @@ struct LineDesc {
     int zl0, zl1, za0, za1;         //   (the output window of the resize that produced it)
     int blk_out;                    // row pass: output in blocks of blk_out columns (0: row-major)
     int blk_in;                     // column pass: input in blocks of blk_in columns (0: row-major)
+    int out_int;                    // last pass of a multi-electron batch on a specialised kernel: one
+                                    //   CTA transforms both components of its lines and writes the
+                                    //   total intensity |Ex|^2 + |Ey|^2 (float, dst[0]) instead of them
 };
 
 struct ResizeDesc {

@@ -592,9 +592,9 @@ Line2Fn line2_kernel_ptr(int logn, bool cols, bool extra, int f1, int f2)
     }
 }
 
-Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt)
+Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt, bool inten)
 {
-#define SRWG_LINEN_CASE(M) if (N == M) return linen_get_##M(cols, extra, nt);
+#define SRWG_LINEN_CASE(M) if (N == M) return linen_get_##M(cols, extra, nt, inten);
     SRWG_LINEN_LENGTHS(SRWG_LINEN_CASE)
     SRWG_LINEN_POW2(SRWG_LINEN_CASE)
 #undef SRWG_LINEN_CASE
@@ -619,17 +619,26 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
             cudaFuncSetAttribute(lineg_e_get(e != 0), cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
         }
 #define SRWG_LINEN_ATTR(M)                                                                                 \
-        for (int e = 0; e < 8; e++)                                                                        \
-            cudaFuncSetAttribute(linen_get_##M(e & 1, (e >> 1) & 1, 1 + (e >> 2)),                         \
+        for (int e = 0; e < 10; e++)                                                                       \
+            cudaFuncSetAttribute(linen_get_##M(e & 1, (e >> 1) & 1, 1 + ((e >> 2) & 1), e >= 8),           \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
         SRWG_LINEN_LENGTHS(SRWG_LINEN_ATTR)
         SRWG_LINEN_POW2(SRWG_LINEN_ATTR)
 #undef SRWG_LINEN_ATTR
     }
+    if (p.d.out_int && p.v2 != 3) return cudaErrorInvalidValue;    // intensity passes: specialised kernels only
     if (p.v2 == 3) {
-        Line2Fn f = linen_kernel_ptr(p.N, p.d.axis != 0, p.d.has_extra != 0, (p.d.f1 && p.d.f2) ? 2 : 1);
+        const bool inten = p.d.out_int != 0;
+        if (inten && (p.d.has_extra || (p.d.f1 && p.d.f2))) return cudaErrorInvalidValue;
+        Line2Fn f = linen_kernel_ptr(p.N, p.d.axis != 0, p.d.has_extra != 0, (p.d.f1 && p.d.f2) ? 2 : 1, inten);
         if (f == nullptr || p.T * p.L > 512) return cudaErrorInvalidValue;
-        f<<<grid, p.T * p.L, smem, st>>>(p);
+        if (inten) grid.y = 1;                  // one CTA transforms both components of its lines
+        // input tiles by bulk async copies: 16-byte aligned sources; rows are contiguous, columns
+        // only when the row pass wrote them in blocks of exactly the tile's (even) width
+        LineLaunch q = p;
+        const bool aligned = ((((uintptr_t)p.src[0]) | ((uintptr_t)p.src[1])) & 15) == 0 && (p.bSrc & 1) == 0;
+        q.bulk = aligned && (p.d.axis == 0 || (p.d.blk_in == p.L && (p.L & 1) == 0));
+        f<<<grid, p.T * p.L, smem, st>>>(q);
     } else if (p.v2 == 2) {
         Line2Fn f = p.d.has_extra ? lineg_e_get(p.d.axis != 0) : lineg_get(p.d.axis != 0);
         if (p.T * p.L > 512) return cudaErrorInvalidValue;

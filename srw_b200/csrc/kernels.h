@@ -9,6 +9,15 @@ namespace srwg {
 // dynamic shared memory of a line pass (leaves room for the static descriptor copy)
 #define SRWG_LINE_SMEM_MAX (220 * 1024)
 
+// shared-memory pitch of a line of N points in the line passes: one pad point per 16 (conflict-free
+// Stockham exchanges) plus 4, so that the lines of a tile start 8 banks apart, rounded up to an even
+// count (every line's slot 16-byte aligned, for bulk copies into it)
+inline size_t line_pitch(int N)
+{
+    const size_t P = (size_t)N + N / 16 + 4;
+    return P + (P & 1);
+}
+
 // lines per CTA of the power-of-two line pass (line2_kernel): rows ~256 threads, columns up to
 // 1024 threads (at most 32 columns), within the shared-memory budget; pitch N + N/16 + 4 points.
 // (Column tiles of half the width, two CTAs per SM, measured slower: the row pass then writes
@@ -19,7 +28,7 @@ inline int line2_lines_per_cta(int axis, int N)
     int L = axis == 0 ? 256 / T : 1024 / T;
     if (L < 1) L = 1;
     if (axis == 1 && L > 32) L = 32;
-    const size_t P = (size_t)N + N / 16 + 4;
+    const size_t P = line_pitch(N);
     while (L > 1 && (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) L--;
     return L;
 }
@@ -40,6 +49,9 @@ struct LineLaunch {
     int nb;                  // wavefronts in the launch (grid z; 0 or 1: one)
     long long bDesc, bTab;   // per wavefront: descriptor stride (bytes), table stride (float2)
     long long bSrc, bDst;    // per wavefront: source / destination field stride (float2)
+    int bulk;                // specialised pass: each CTA's input tile arrives by bulk async copies
+    int* status;             // device counter of waits that gave up (NULL: not recorded)
+    long long spin;          // iteration limit of the bulk-copy wait
 };
 
 // tiled resize: a CTA makes TZ x TX new points from an old tile of at most OR_MAX x OC_MAX points
@@ -105,11 +117,11 @@ SRWG_LINE2_DECL(11) SRWG_LINE2_DECL(12) SRWG_LINE2_DECL(13) SRWG_LINE2_DECL(14)
 Line2Fn lineg_get(bool cols);
 Line2Fn lineg_e_get(bool cols);
 // specialised general-length kernels (linen.cu, one unit per length of linen_lengths.h)
-#define SRWG_LINEN_DECL(N) Line2Fn linen_get_##N(bool cols, bool extra, int nt);
+#define SRWG_LINEN_DECL(N) Line2Fn linen_get_##N(bool cols, bool extra, int nt, bool inten);
 SRWG_LINEN_LENGTHS(SRWG_LINEN_DECL)
 SRWG_LINEN_POW2(SRWG_LINEN_DECL)
 #undef SRWG_LINEN_DECL
-Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt);
+Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt, bool inten = false);
 inline bool line2_supported(int N) { return N >= 64 && N <= 16384 && (N & (N - 1)) == 0; }
 // general lengths of the specialised kernel
 inline bool linen_supported(int N)
@@ -136,7 +148,7 @@ enum { FAM_TAB = 0, FAM_POW2 = 1, FAM_GEN = 2, FAM_SPEC = 3 };
 inline int linen_lines_per_cta(int axis, int N)
 {
     const int T = (N + 15) / 16;
-    const size_t P = (size_t)N + N / 16 + 4;
+    const size_t P = line_pitch(N);
     int L;
     if (axis == 0) {
         L = 512 / T;
@@ -151,7 +163,7 @@ inline int linen_lines_per_cta(int axis, int N)
 // whether L lines per CTA is a valid launch shape of kernel family fam for length N
 inline bool fixed_lines_valid(int axis, int N, int L, int fam)
 {
-    const size_t P = (size_t)N + N / 16 + 4;
+    const size_t P = line_pitch(N);
     if (L < 1 || (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) return false;
     if (axis == 1 && (L > 32 || (L & (L - 1)) != 0)) return false;      // column blocks: a power of two
     if (fam == FAM_POW2 && line2_supported(N)) return (N / 16) * L <= 1024;

@@ -9,8 +9,8 @@
 #define SRWG_CAT(a, b) SRWG_CAT2(a, b)
 
 namespace srwg {
-Line2Fn SRWG_CAT(linen_get_, SRWG_LINEN)(bool cols, bool extra, int nt)
+Line2Fn SRWG_CAT(linen_get_, SRWG_LINEN)(bool cols, bool extra, int nt, bool inten)
 {
-    return linen_select<SRWG_LINEN>(cols, extra, nt);
+    return linen_select<SRWG_LINEN>(cols, extra, nt, inten);
 }
 }  // namespace srwg

@@ -16,6 +16,51 @@ namespace srwg {
 
 #define PADN(p) ((p) + ((p) >> 4))
 
+// ------------------------------------------------------------------------------------------------
+// bulk async copies into shared memory, completion through an mbarrier (one per CTA, phase 0)
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("{ .reg .b64 st; mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1; }" ::"r"(smem_addr(bar)),
+                 "r"(bytes) : "memory");
+}
+// global -> shared, `bytes` a multiple of 16, both addresses 16-byte aligned
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, unsigned phase)
+{
+    unsigned ok;
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                 : "=r"(ok) : "r"(smem_addr(bar)), "r"(phase) : "memory");
+    return ok != 0;
+}
+// waits for the phase of parity `phase` at most `limit` tries; on giving up it counts the event in *status and waits (at
+// most 2^26 more tries) for the copies still in flight, so that none lands after the CTA has left.
+// Returns false when any thread of the CTA gave up (the CTA then skips its work as a whole).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase, long long limit, int* status)
+{
+    long long it = 0;
+    bool done = mbar_try(bar, phase);
+    while (!done && ++it < limit) done = mbar_try(bar, phase);
+    const bool gave_up = !done;
+    if (gave_up) {
+        if (status) atomicAdd(status, 1);
+        long long k = 0;
+        while (!mbar_try(bar, phase) && ++k < (1ll << 26)) {
+        }
+    }
+    return !__syncthreads_or(gave_up);
+}
+
 // compile-time radix schedule of N
 struct NSched {
     int n;
@@ -45,6 +90,7 @@ template <int N> struct NPlan {
     static constexpr NSched s = nsched(N);
     static constexpr int T = (N + 15) / 16;
 };
+__host__ __device__ constexpr int NSched_last(int N) { return nsched(N).r[nsched(N).n - 1]; }
 
 // (k + N/2) mod N
 template <int N> __device__ __forceinline__ int rot_n(int k)
@@ -103,6 +149,8 @@ struct NLine {
     bool has_lf;
     float2 lf;
     int za0, za1;           // input points outside [za0, za1] are zero
+    const float2* sin;      // bulk-copied input tile: point k of the line at sin[k * sst]
+    int sst;
 };
 
 // padded shared-memory address of point p, and its separable form for a per-thread base plus a
@@ -158,9 +206,17 @@ template <int B, int R> __device__ __forceinline__ void conj_all(float2 (&v)[B][
 // chain cin; OUT: 0 shared memory, 1 global memory through chain cout.  Inverse transforms (cj < 0)
 // conjugate the inputs of their first stage after the chain and the outputs of their last stage
 // before the chain.
-template <int N, int R, int NS, int IN, int OUT, bool FIRST, bool LAST, bool EXTRA>
+// intensity of the points a thread stores in the last stage, carried from the first component's
+// transform to the second one's (OUTI passes)
+template <int N> struct IAcc {
+    static constexpr int R = NSched_last(N);
+    static constexpr int B = (N / R + NPlan<N>::T - 1) / NPlan<N>::T;
+    float v[B][R];
+};
+
+template <int N, int R, int NS, int IN, int OUT, bool FIRST, bool LAST, bool EXTRA, int OUTI = 0>
 __device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& cin, const ChainG& cout, float cj,
-                                       const float2* __restrict__ tw, int t)
+                                       const float2* __restrict__ tw, int t, IAcc<N>* acc = nullptr)
 {
     constexpr int T = NPlan<N>::T;
     constexpr int NR = N / R;
@@ -168,10 +224,11 @@ __device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& 
     constexpr bool PART = (NR % T) != 0;             // the last round has idle threads
     constexpr int TWS = N / (NS * R);
     float2 v[B][R];
-    if (IN == 2) {
-        // first stage from global memory: all loads issued before any dependent arithmetic; the
-        // source of destination p is p, p rotated by N/2 (a permutation of the radix index: R is even
-        // here), or the general map with the mirror
+    if (IN == 2 || IN == 3) {
+        // first stage from global memory (IN 2: all loads issued before any dependent arithmetic) or
+        // from the bulk-copied input tile in shared memory (IN 3); the source of destination p is p,
+        // p rotated by N/2 (a permutation of the radix index: R is even here), or the general map
+        // with the mirror
         const bool rot = cin.rs1 != cin.rs2;
 #pragma unroll
         for (int b = 0; b < B; b++) {
@@ -189,7 +246,8 @@ __device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& 
                     q = chain_src_n<N>(cin, j + r * NR, i);
                 }
                 const bool in = okj && q >= x.za0 && q <= x.za1;
-                v[b][r] = in ? __ldcs(&x.gin[q * x.gstr]) : make_float2(0.f, 0.f);
+                if (IN == 2) v[b][r] = in ? __ldcs(&x.gin[q * x.gstr]) : make_float2(0.f, 0.f);
+                else v[b][r] = in ? x.sin[q * x.sst] : make_float2(0.f, 0.f);
             }
         }
         apply_factors<N, R, NR, T, B, PART, EXTRA>(v, x, cin, t);
@@ -301,25 +359,32 @@ __device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& 
                     o = cmul(linen_extra(x.ex, x.axis == 0 ? i : x.line, x.axis == 0 ? x.line : i, x.tabs), o);
                 }
                 if (x.has_lf) o = cmul(x.lf, o);
-                if (x.store) __stcs(&x.gout[x.om.at(kk)], o);
+                if constexpr (OUTI == 0) {
+                    if (x.store) __stcs(&x.gout[x.om.at(kk)], o);
+                } else if constexpr (OUTI == 1) {
+                    acc->v[b][r] = o.x * o.x + o.y * o.y;            // first component
+                } else {
+                    const float I = acc->v[b][r] + o.x * o.x + o.y * o.y;
+                    if (x.store) __stcs(reinterpret_cast<float*>(x.gout) + x.om.at(kk), I);
+                }
             }
         }
     }
 }
 
 // one transform along the line with the compile-time schedule of N; INM: mode of the first stage's
-// input (1 shared through cin, 2 global through cin), OUTM: of the last stage's output (0 shared, 1
-// global through cout)
-template <int N, int INM, int OUTM, bool EXTRA>
+// input (1 shared through cin, 2 global through cin, 3 the bulk-copied input tile through cin), OUTM:
+// of the last stage's output (0 shared, 1 global through cout)
+template <int N, int INM, int OUTM, bool EXTRA, int OUTI = 0>
 __device__ __forceinline__ void fft_n(float2* s, const NLine& x, const ChainG& cin, const ChainG& cout, float cj,
-                                      const float2* __restrict__ tw, int t)
+                                      const float2* __restrict__ tw, int t, IAcc<N>* acc = nullptr)
 {
     constexpr NSched S = NPlan<N>::s;
     static_assert(S.n >= 2 && S.n <= 8, "radix schedule");
 #define SRWG_NSTAGE(I)                                                                                          \
     if constexpr (S.n > (I))                                                                                    \
         nstage<N, S.r[(I) < S.n ? (I) : 0], nsched_ns(N, (I)), (I) == 0 ? INM : 0, (I) == S.n - 1 ? OUTM : 0,   \
-               (I) == 0, (I) == S.n - 1, EXTRA>(s, x, cin, cout, cj, tw, t);
+               (I) == 0, (I) == S.n - 1, EXTRA, (I) == S.n - 1 ? OUTI : 0>(s, x, cin, cout, cj, tw, t, acc);
     SRWG_NSTAGE(0) SRWG_NSTAGE(1) SRWG_NSTAGE(2) SRWG_NSTAGE(3)
     SRWG_NSTAGE(4) SRWG_NSTAGE(5) SRWG_NSTAGE(6) SRWG_NSTAGE(7)
 #undef SRWG_NSTAGE
@@ -329,15 +394,21 @@ __device__ __forceinline__ void fft_n(float2* s, const NLine& x, const ChainG& c
 // transform and no non-separable work run at two 512-thread CTAs per SM (64 registers per thread,
 // measured: at most a few spilled words); the others keep 128 registers (their state spills heavily
 // at 64).
-template <int N, bool COLS, bool EXTRA, int NT>
-__global__ void __launch_bounds__(512, (EXTRA || NT == 2) ? 1 : 2) linen_kernel(const LineLaunch p)
+// The pass for one component of the CTA's lines.  OUTI 0: the component's field is written;
+// 1 / 2: the first / second component of an intensity pass (the intensity of the points each thread
+// stores is carried in `acc` and written after the second).  `phase`: parity of the bulk-copy
+// mbarrier use.  Returns false when the CTA gave its work up (a bounded wait ran out).
+template <int N, bool COLS, bool EXTRA, int NT, int OUTI>
+__device__ __forceinline__ bool linen_body(const LineLaunch& p, int comp, IAcc<N>* acc, uint64_t* barp, unsigned phase)
 {
     constexpr int T = NPlan<N>::T;
-    extern __shared__ float2 smn[];
+    extern __shared__ __align__(16) float2 smn[];
     const LineDesc& d = *reinterpret_cast<const LineDesc*>(reinterpret_cast<const char*>(p.gd) + blockIdx.z * p.bDesc);
-    const int comp = blockIdx.y;
     const float2* __restrict__ src = p.src[comp] + blockIdx.z * p.bSrc;
+    // intensity passes write floats (element stride bDst in floats) through dst[0]: the output
+    // offsets below are in elements of the output type
     float2* __restrict__ dst = p.dst[comp] + blockIdx.z * p.bDst;
+    float* __restrict__ fdst = reinterpret_cast<float*>(p.dst[0]) + blockIdx.z * p.bDst;
     const int L = p.L, P = p.P, nl = p.nlines;
     const int tid = threadIdx.x;
     const int g = COLS ? (tid % L) : (tid / T);          // line of the tile
@@ -356,30 +427,76 @@ __global__ void __launch_bounds__(512, (EXTRA || NT == 2) ? 1 : 2) linen_kernel(
         x.gin = src + (size_t)(line / d.blk_in) * N * d.blk_in + (line % d.blk_in);
     }
     const int oline = d.mirror_lines ? (nl - 1 - line) : line;
-    x.gout = COLS ? (dst + oline) : (dst + (size_t)oline * N);
+    size_t obase = COLS ? (size_t)oline : (size_t)oline * N;
     x.om.str = COLS ? nl : 1;
     x.om.lg = -1;
     x.om.bstr = 0;
     if (!COLS && d.blk_out > 0) {
         x.om.lg = 31 - __clz(d.blk_out);
         x.om.bstr = nl * d.blk_out;
-        x.gout = dst + (size_t)oline * d.blk_out;
+        obase = (size_t)oline * d.blk_out;
     }
+    x.gout = OUTI ? reinterpret_cast<float2*>(fdst + obase) : dst + obase;
     x.za0 = 0;
     x.za1 = N - 1;
     if (d.zwin) {
         const int l0 = blockIdx.x * L, l1 = min(l0 + L, nl) - 1;
         if (l1 < d.zl0 || l0 > d.zl1) {
             // the whole tile is zero: so is its transform
-            if (x.store)
+            if (x.store && OUTI == 0)
                 for (int m = t; m < N; m += T) __stcs(&x.gout[x.om.at(m)], make_float2(0.f, 0.f));
-            return;
+            if (x.store && OUTI == 2)
+                for (int m = t; m < N; m += T) __stcs(reinterpret_cast<float*>(x.gout) + x.om.at(m), 0.f);
+            return true;
         }
         if (line < d.zl0 || line > d.zl1) { x.za0 = 1; x.za1 = 0; }
         else { x.za0 = d.za0; x.za1 = d.za1; }
     }
     x.tabs = p.tabs + blockIdx.z * p.bTab;
     x.ex = &d.extra;
+    x.sin = nullptr;
+    x.sst = 1;
+    if (p.bulk) {
+        // the tile's input arrives in shared memory by bulk async copies (thread 0 issues them):
+        // rows: each line's nonzero window [za0, za1] (rounded out to even / odd ends: 16-byte pieces)
+        // into its own slot (line g at g P); columns: the column block (the tile's L columns stored
+        // together by the row pass) over the nonzero rows, as one piece (point k of column g at k L + g)
+        uint64_t& bar = *barp;
+        if (tid == 0) {
+            if (phase == 0) mbar_init(&bar);
+            unsigned bytes = 0;
+            if (COLS) {
+                if (x.za0 <= x.za1) bytes = (unsigned)((x.za1 - x.za0 + 1) * L * sizeof(float2));
+            } else {
+                for (int gg = 0; gg < L; gg++) {
+                    const int ln = min(blockIdx.x * L + gg, nl - 1);
+                    const bool inl = !d.zwin || (ln >= d.zl0 && ln <= d.zl1);
+                    const int lo = d.zwin ? (d.za0 & ~1) : 0, hi = d.zwin ? (d.za1 | 1) : N - 1;
+                    if (inl && lo <= hi) bytes += (unsigned)((hi - lo + 1) * sizeof(float2));
+                }
+            }
+            mbar_expect(&bar, bytes);
+            if (COLS) {
+                if (bytes) {
+                    const size_t blk = (size_t)(blockIdx.x * L / d.blk_in) * N * d.blk_in;
+                    bulk_load(smn + (size_t)x.za0 * L, src + blk + (size_t)x.za0 * L, bytes, &bar);
+                }
+            } else {
+                for (int gg = 0; gg < L; gg++) {
+                    const int ln = min(blockIdx.x * L + gg, nl - 1);
+                    const bool inl = !d.zwin || (ln >= d.zl0 && ln <= d.zl1);
+                    const int lo = d.zwin ? (d.za0 & ~1) : 0, hi = d.zwin ? (d.za1 | 1) : N - 1;
+                    if (inl && lo <= hi)
+                        bulk_load(smn + (size_t)gg * P + lo, src + (size_t)ln * N + lo,
+                                  (unsigned)((hi - lo + 1) * sizeof(float2)), &bar);
+                }
+            }
+        }
+        __syncthreads();
+        if (!mbar_wait_bounded(&bar, phase, p.spin > 0 ? p.spin : (1ll << 22), p.status)) return false;
+        x.sin = COLS ? (smn + g) : (smn + (size_t)g * P);
+        x.sst = COLS ? L : 1;
+    }
     ChainG pre, mid, fin;
     pre.rs1 = 0; pre.mir = 0; pre.rs2 = d.f1_pre.rs; pre.tab = (int)d.t_pre.tab; pre.extra = 0;
     mid.rs1 = d.f1 ? d.f1_post.rs : 0; mid.mir = d.mirror_along; mid.rs2 = d.f2 ? d.f2_pre.rs : 0;
@@ -394,19 +511,42 @@ __global__ void __launch_bounds__(512, (EXTRA || NT == 2) ? 1 : 2) linen_kernel(
     }
     const float2* tw = p.tw;
     if constexpr (NT == 2) {
-        fft_n<N, 2, 0, EXTRA>(s, x, pre, mid, d.f1 < 0 ? -1.f : 1.f, tw, t);
-        fft_n<N, 1, 1, EXTRA>(s, x, mid, fin, d.f2 < 0 ? -1.f : 1.f, tw, t);
+        if (p.bulk) fft_n<N, 3, 0, EXTRA>(s, x, pre, mid, d.f1 < 0 ? -1.f : 1.f, tw, t);
+        else fft_n<N, 2, 0, EXTRA>(s, x, pre, mid, d.f1 < 0 ? -1.f : 1.f, tw, t);
+        fft_n<N, 1, 1, EXTRA, OUTI>(s, x, mid, fin, d.f2 < 0 ? -1.f : 1.f, tw, t, acc);
     } else {
         const bool one = d.f1 != 0;
         const float cj = (one ? d.f1 : d.f2) < 0 ? -1.f : 1.f;
-        fft_n<N, 2, 1, EXTRA>(s, x, one ? pre : mid, one ? mid : fin, cj, tw, t);
+        if (p.bulk) fft_n<N, 3, 1, EXTRA, OUTI>(s, x, one ? pre : mid, one ? mid : fin, cj, tw, t, acc);
+        else fft_n<N, 2, 1, EXTRA, OUTI>(s, x, one ? pre : mid, one ? mid : fin, cj, tw, t, acc);
     }
+    return true;
 }
 
-// the kernel of a (COLS, EXTRA, transforms) combination for length N
-template <int N>
-Line2Fn linen_select(bool cols, bool extra, int nt)
+template <int N, bool COLS, bool EXTRA, int NT>
+__global__ void __launch_bounds__(512, (EXTRA || NT == 2) ? 1 : 2) linen_kernel(const LineLaunch p)
 {
+    __shared__ uint64_t bar;
+    linen_body<N, COLS, EXTRA, NT, 0>(p, blockIdx.y, nullptr, &bar, 0);
+}
+
+// intensity pass (the last pass of a multi-electron batch): both components of the CTA's lines one
+// after the other (one transform each, no non-separable work), |Ex|^2 + |Ey|^2 written as float
+template <int N, bool COLS>
+__global__ void __launch_bounds__(512, 1) linen_int_kernel(const LineLaunch p)
+{
+    __shared__ uint64_t bar;
+    IAcc<N> acc;
+    if (!linen_body<N, COLS, false, 1, 1>(p, 0, &acc, &bar, 0)) return;
+    __syncthreads();                          // the second component's copies overwrite the tile
+    linen_body<N, COLS, false, 1, 2>(p, 1, &acc, &bar, 1);
+}
+
+// the kernel of a (COLS, EXTRA, transforms) combination for length N; intensity passes: `inten`
+template <int N>
+Line2Fn linen_select(bool cols, bool extra, int nt, bool inten = false)
+{
+    if (inten) return cols ? linen_int_kernel<N, true> : linen_int_kernel<N, false>;
     if (cols) {
         if (extra) return nt == 2 ? linen_kernel<N, true, true, 2> : linen_kernel<N, true, true, 1>;
         return nt == 2 ? linen_kernel<N, true, false, 2> : linen_kernel<N, true, false, 1>;

@@ -80,6 +80,57 @@ __global__ void __launch_bounds__(256) accum_kernel(const float2* __restrict__ e
     acc[(size_t)j * anx + i] += sum;
 }
 
+// the same with the intensities written by the last pass (an intensity pass, float [onz][onx] per
+// electron at stride `stride` floats)
+__global__ void __launch_bounds__(256) accum_int_kernel(const float* __restrict__ in, long long stride, int nb,
+                                                        const ElecParams* __restrict__ ep, double* __restrict__ acc,
+                                                        int anx, int anz, double axStart, double axStep,
+                                                        double azStart, double azStep)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= anx) return;
+    const double x = axStart + (double)i * axStep, y = azStart + (double)j * azStep;
+    double sum = 0.;
+    for (int b = 0; b < nb; b++) {
+        const ElecParams& e = ep[b];
+        const int ix0 = (int)trunc((x - e.oxStart) / e.oxStep + 1.e-09);
+        if (ix0 < 0 || ix0 >= e.onx - 1) continue;
+        const int iy0 = (int)trunc((y - e.ozStart) / e.ozStep + 1.e-09);
+        if (iy0 < 0 || iy0 >= e.onz - 1) continue;
+        const double tx = (x - (e.oxStart + e.oxStep * ix0)) / e.oxStep;
+        const double ty = (y - (e.ozStart + e.ozStep * iy0)) / e.ozStep;
+        const float* pi = in + (size_t)b * stride + (size_t)iy0 * e.onx + ix0;
+        const double a00 = __ldg(&pi[0]), f10 = __ldg(&pi[1]), f01 = __ldg(&pi[e.onx]), f11 = __ldg(&pi[e.onx + 1]);
+        const double a10 = f10 - a00, a01 = f01 - a00, a11 = a00 - f01 - f10 + f11;
+        sum += a00 + tx * (a10 + ty * a11) + ty * a01;
+    }
+    acc[(size_t)j * anx + i] += sum;
+}
+
+// the last pass writes the total intensity instead of the two fields where it runs on a specialised
+// kernel with one transform and no non-separable work (the accumulation then reads one float per
+// sample instead of two complex values)
+static void mark_intensity_pass(std::vector<KernelDesc>& ks)
+{
+    for (size_t i = ks.size(); i-- > 0;) {
+        if (reads_only(ks[i].kind)) continue;
+        LineDesc& d = ks[i].line;
+        if (ks[i].kind == K_LINE && !d.has_extra && !(d.f1 && d.f2)) {
+            const int N = d.axis == 0 ? d.nx : d.nz;
+            if (fixed_family(d.axis, N) == FAM_SPEC) d.out_int = 1;
+        }
+        return;
+    }
+}
+
+static bool intensity_pass(const std::vector<KernelDesc>& ks)
+{
+    for (size_t i = ks.size(); i-- > 0;)
+        if (!reads_only(ks[i].kind)) return ks[i].kind == K_LINE && ks[i].line.out_int;
+    return false;
+}
+
 }  // namespace srwg
 
 using namespace srwg;
@@ -182,7 +233,8 @@ static bool same_structure(const std::vector<KernelDesc>& a, const std::vector<K
         if (x.kind == K_LINE) {
             const LineDesc &p = x.line, &q = y.line;
             if (p.axis != q.axis || p.nx != q.nx || p.nz != q.nz || p.f1 != q.f1 || p.f2 != q.f2 ||
-                p.has_extra != q.has_extra || p.zwin != q.zwin || p.blk_in != q.blk_in || p.blk_out != q.blk_out)
+                p.has_extra != q.has_extra || p.zwin != q.zwin || p.blk_in != q.blk_in || p.blk_out != q.blk_out ||
+                p.out_int != q.out_int)
                 return false;
         } else if (x.kind == K_RESIZE) {
             const ResizeDesc &p = x.rs, &q = y.rs;
@@ -209,8 +261,12 @@ static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, c
                            m.perWork, m.dConst, (long long)m.constStride, m.descOff, st, nullptr, &ks);
     if (r) return r;
     dim3 ga((m.anx + 255) / 256, m.anz);
-    accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams, m.dAcc, m.anx, m.anz, m.axStart,
-                                     m.axStep, m.azStart, m.azStep);
+    if (intensity_pass(ks))
+        accum_int_kernel<<<ga, blk, 0, st>>>(reinterpret_cast<const float*>(outX), (long long)m.nOut, nb, m.dParams,
+                                             m.dAcc, m.anx, m.anz, m.axStart, m.axStep, m.azStart, m.azStep);
+    else
+        accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams, m.dAcc, m.anx, m.anz,
+                                         m.axStart, m.axStep, m.azStart, m.azStep);
     MTRY(cudaGetLastError());
     return 0;
 }
@@ -307,6 +363,7 @@ extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* p
     pl.numMoments = false;               // only the intensity is kept: no moment passes
     pl.inPhase = true;                   // the electrons' kick (here zero): the same passes as theirs
     r = pl.plan(pBase, pOpt);
+    if (!r) mark_intensity_pass(pl.kernels);
     if (r) { set_last_detail(pl.err); delete m; return r; }
     m->nIn = (size_t)m->nx * m->nz;
     m->nOut = (size_t)pl.w.nx * pl.w.nz;
@@ -429,6 +486,7 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
                     pls[k].inKz = eps[k].kz;
                     pls[k].inC = -(eps[k].kx * eps[k].dx + eps[k].kz * eps[k].dz);
                     rcs[k] = pls[k].plan(&w, m->opt);
+                    if (!rcs[k]) mark_intensity_pass(pls[k].kernels);
                 }
             };
             std::vector<std::thread> th;

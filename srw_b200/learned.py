@@ -709,6 +709,8 @@ def make_data(n_samples, seed, dev, threads=8, log=print, path=None, chunk=2000)
         for c0 in range(done0, n_samples, chunk):
             c1 = min(n_samples, c0 + chunk)
             list(ex.map(one, range(c0, c1)))
+            torch.cuda.synchronize(dev)
+            torch.cuda.empty_cache()           # the threads' streams each keep freed blocks otherwise
             log('labelled %d (%.0f s)' % (c1, time.time() - t0))
             if path:
                 np.savez_compressed(path, X=X[:c1], T=T[:c1], E=E[:c1], NE=NE[:c1])

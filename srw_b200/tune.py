@@ -68,6 +68,7 @@ def candidates(axis, n, fam=None):
         t = n // 16 if f == FAM_POW2 else (n + 15) // 16
         tmax = 1024 if f == FAM_POW2 else 512
         p = n + n // 16 + 4
+        p += p & 1                              # the library's line_pitch
         for L in range(1, 33):
             if L * p * 8 > SMEM_MAX or t * L > tmax:
                 break

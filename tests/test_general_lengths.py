@@ -125,3 +125,32 @@ def test_runtime_scheduled_length_still_works():
     ex, ey, mesh = gaussian(216, E=1000., sig=50e-6, r=1e-3, ny=200, ry=1e-3)
     el = [('drift', 10., 0), ('lens', 5., 5., 0., 0.), ('drift', 5., 0)]
     _check(ex, ey, mesh, el, [PP()] * 3, {}, want_family='gen')
+
+
+@pytest.mark.gpu
+def test_bulk_copy_wait_limit_reports_and_recovers():
+    """The specialised passes wait for the bulk copies of their input tiles with an iteration limit.
+    With the limit at one try the waits give up: the library counts them (srwgGetWaitStatus) and the
+    CTAs skip their work, with no fault; with the default limit the same propagation is exact again
+    and counts nothing."""
+    _gpu()
+    import ctypes as C
+    from srw_b200 import capi
+    from srw_b200 import srwlpy as srwl
+    L = capi.lib()
+    ex, _, mesh = gaussian(1024, E=2012., sig=0.35e-3, r=1.5e-3, R=20.)
+    ey = 0.05j * ex
+    el, pp, sc = C1, [PP(), PP(0, 1., 1.25, 1., 1.25), PP(4)], dict(Rx=20., Ry=20., dRx=0.2, dRy=0.2)
+    assert 'spec' in _families(ex, ey, mesh, el, pp, sc)
+    n = C.c_int()
+    try:
+        assert L.srwgGetWaitStatus(0, C.byref(n), 1) == 0
+        assert L.srwgSetWaitLimit(1) == 0
+        w = make_wfr(ex, ey, mesh, **sc)
+        srwl.PropagElecField(w, beamline(el, pp))
+        assert L.srwgGetWaitStatus(0, C.byref(n), 1) == 0
+        assert n.value > 0
+    finally:
+        L.srwgSetWaitLimit(0)
+    w = _check(ex, ey, mesh, el, pp, sc)
+    assert L.srwgGetWaitStatus(0, C.byref(n), 1) == 0 and n.value == 0

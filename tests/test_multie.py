@@ -188,3 +188,35 @@ def test_multie_energy_spread_vs_oracle():
     assert rel_l2(got, want) < TOL
     flat = oracle_sum(i, sc, el, pp, acc, offs[:, :4]) / 6
     assert rel_l2(flat, want) > 10 * TOL
+
+
+@pytest.mark.gpu
+def test_multie_intensity_pass_vs_oracle():
+    """Electrons on a grid of a specialised length (128^2 -> 320^2): the last pass transforms both
+    components per CTA and writes the total intensity (the accumulation reads one float per sample);
+    the mean against the oracle's electron-by-electron loop."""
+    _gpu()
+    import ctypes as C
+    from srw_b200 import capi
+    from srw_b200.multie import MultiE
+    from tests.helpers import C1, PP, gaussian
+    fam = C.c_int()
+    assert capi.lib().srwgTuneGetFamily(1, 320, C.byref(fam)) == 0 and fam.value == 3
+    ex, _, mesh = gaussian(128, E=2012., sig=0.35e-3, r=1.5e-3, R=20.)
+    ey = 0.05j * ex
+    sc = dict(Rx=20., Ry=20., dRx=0.2, dRy=0.2, xc=0., yc=0.)
+    pp = [PP(), PP(0, 1.25, 2., 1.25, 2.), PP(4)]
+    o = O.Wfr.from_srwl(ex, ey, mesh, 20., 20., 0.2, 0.2, 0., 0.)
+    O.propagate(o, [tuple(e) for e in C1], pp)
+    m = o.out_mesh()
+    assert (m['nx'], m['ny']) == (320, 320)
+    acc = dict(nx=96, ny=80, xStart=0.6 * m['xStart'], xFin=0.6 * m['xFin'], yStart=0.6 * m['yStart'],
+               yFin=0.6 * m['yFin'], eStart=mesh['eStart'])
+    offs = sample_offsets(6, *SIG, seed=21, sig_e=1e-3)
+    w = make_wfr(ex, ey, mesh, **sc)
+    me = MultiE(w, beamline(C1, pp), acc, max_batch=4, graph=True)
+    me.add(offs)
+    got = me.mean()
+    want = oracle_sum(dict(ex=ex, ey=ey, mesh=mesh), sc, C1, pp, acc, offs) / 6
+    assert np.abs(want).max() > 0
+    assert rel_l2(got, want) < TOL

@@ -533,9 +533,16 @@ def measure_mixed(args, dev, n_elec, model=None):
                 facs[n] = list(factors) + (['fallback'] if fb else [])
             bl = beamline_objs(mod, factors)
             b = batch or {256: 32, 512: 32, 1024: 16}[n]
-            me = MultiE(w, bl, acc, max_batch=b, graph=graph, device=dev.index)
-            me.add(sample_offsets(b, *SIG, seed=999, sig_e=SIG_E))                      # warm-up (plans, graph)
-            me.reset()
+            if mode == 'learned':
+                # one electron of every batch checked against its conservative propagation
+                me = learned.CheckedMultiE(w, lambda f: beamline_objs(mod, f), factors, acc, max_batch=64,
+                                           graph=graph, device=dev.index)
+                me.add(sample_offsets(64, *SIG, seed=999, sig_e=SIG_E))                 # warm-up (plans, graph)
+                me.reset()
+            else:
+                me = MultiE(w, bl, acc, max_batch=b, graph=graph, device=dev.index)
+                me.add(sample_offsets(b, *SIG, seed=999, sig_e=SIG_E))                  # warm-up (plans, graph)
+                me.reset()
             cnt = n_elec // 3
             offs = sample_offsets(cnt, *SIG, seed=5, first=cls * cnt, sig_e=SIG_E)
             torch.cuda.synchronize(dev)
@@ -555,7 +562,8 @@ def measure_mixed(args, dev, n_elec, model=None):
            "batched": res['batched'], "plain": res['plain'], "speedup": res['batched'] / res['plain'],
            "note": "each electron: offset field, C1 beamline (resize before the lens), intensity added in FP64 "
                    "onto a 512x512 common mesh; plain = the same electrons one per launch sequence with the "
-                   "configured factors (2, 2)"}
+                   "configured factors (2, 2); learned = per grid class the network's factors, batches of 64 with "
+                   "one electron checked against its conservative propagation"}
     if model is not None:
         out.update({"batched_learned": res['learned'], "learned_speedup_vs_plain": res['learned'] / res['plain'],
                     "learned_factors": {str(k): v for k, v in facs.items()},
@@ -906,7 +914,7 @@ def main():
     ap.add_argument('--no-e2e', action='store_true', help='skip the end-to-end legs (profiling runs)')
     ap.add_argument('--no-mixed', action='store_true', help='skip the mixed-grid multi-electron workload')
     ap.add_argument('--no-learned', action='store_true', help='skip the learned-factor leg')
-    ap.add_argument('--mixed-electrons', type=int, default=600)
+    ap.add_argument('--mixed-electrons', type=int, default=2000)
     ap.add_argument('--no-oracle', action='store_true', help='skip the FP64-oracle error leg')
     args = ap.parse_args()
     if args.gpus > 1 and 'WORLD_SIZE' not in os.environ:

@@ -665,6 +665,14 @@ class CheckedMultiE(object):
         self.torch.cuda.synchronize(self.dev)
         return (self.acc / max(self.n, 1)).cpu().numpy()
 
+    def reset(self):
+        """Clears the accumulated intensity and the counters (plans and captured graphs are kept)."""
+        self.torch.cuda.synchronize(self.dev)
+        self.acc.zero_()
+        for m in (self.fast, self.safe):
+            m.reset()
+        self.n, self.batches, self.fallbacks, self.check_errors = 0, 0, 0, []
+
 
 # ------------------------------------------------------------------------------------------------
 # training

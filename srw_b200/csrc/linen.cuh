@@ -36,27 +36,32 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
 }
+// non-blocking test of the phase of parity `phase` (try_wait would suspend the thread for a
+// hardware-defined time, which would make an iteration limit meaningless)
 __device__ __forceinline__ bool mbar_try(uint64_t* bar, unsigned phase)
 {
     unsigned ok;
-    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+    asm volatile("{ .reg .pred p; mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
                  : "=r"(ok) : "r"(smem_addr(bar)), "r"(phase) : "memory");
     return ok != 0;
 }
-// waits for the phase of parity `phase` at most `limit` tries; on giving up it counts the event in *status and waits (at
-// most 2^26 more tries) for the copies still in flight, so that none lands after the CTA has left.
+// waits for the phase of parity `phase` at most `limit` tries (32 ns apart); on giving up it counts
+// the event in *status and waits (at most 2^24 more tries, about a second) for the copies still in
+// flight, so that none lands after the CTA has left.
 // Returns false when any thread of the CTA gave up (the CTA then skips its work as a whole).
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase, long long limit, int* status)
 {
     long long it = 0;
     bool done = mbar_try(bar, phase);
-    while (!done && ++it < limit) done = mbar_try(bar, phase);
+    while (!done && ++it < limit) {
+        __nanosleep(32);
+        done = mbar_try(bar, phase);
+    }
     const bool gave_up = !done;
     if (gave_up) {
         if (status) atomicAdd(status, 1);
         long long k = 0;
-        while (!mbar_try(bar, phase) && ++k < (1ll << 26)) {
-        }
+        while (!mbar_try(bar, phase) && ++k < (1ll << 24)) __nanosleep(64);
     }
     return !__syncthreads_or(gave_up);
 }

@@ -352,6 +352,38 @@ def kernel_bytes(k):
     return 2 * 8 * 2 * k[1] * k[2]
 
 
+def hbm_peak():
+    """(HBM GB/s, 'measured' | 'fallback'): the measured copy bandwidth of this GPU pool when the
+    peaks file is present, else the earlier measured fallback figure."""
+    if os.path.exists(PEAKS):
+        return float(json.load(open(PEAKS))['hbm_gbs']), 'measured'
+    return 6650., 'fallback'
+
+
+def batched_passes(me, offs, stream, peak, peak_src, where):
+    """One batch of the multi-electron object `me` (MultiE) run without its graph, with CUDA events
+    around every pass (srwgMultiEAddTimed; adds the electrons): per-pass times and the roofline of the
+    dominant pass -- algorithmic bytes per electron (kernel_bytes; a last pass that writes the
+    intensity writes one float per point instead of two complex values) times the electrons of the
+    launch, over the pass's CUDA-event time."""
+    ks, inten = me.info()
+    ms = me.add_timed(offs, stream)
+    nb = len(offs)
+    per = ms[:len(ks)]
+    alg = [kernel_bytes(k) for k in ks]
+    if inten:
+        k = ks[-1]
+        alg[-1] = 2 * 8 * k[1] * k[2] + 4 * k[1] * k[2]
+    kd = int(np.argmax(per))
+    achieved = alg[kd] * nb / (per[kd] / 1000.) / 1e9
+    return {"bound": "hbm", "kernel": "%s %s (batch of %d)" % (ks[kd][0], 'x'.join(map(str, ks[kd][1:])), nb),
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+            "traffic": None, "algorithmic_bytes": alg[kd] * nb, "avg_ms": float(per[kd]),
+            "per_pass_ms": [round(float(v), 4) for v in per], "accumulation_ms": round(float(ms[-1]), 4),
+            "per_electron_ms": round(float(sum(ms)) / nb, 5), "passes": [list(k) for k in ks],
+            "last_pass_writes_intensity": inten, "measured_on": where}
+
+
 def measure_plain(args, dev, world, dist, factors=CONFIGURED):
     """Single-wavefront path: one propagation per step on a device-resident field, CUDA events per
     step and per pass (roofline), L2 flushed between steps; `factors`: the resize before the lens."""
@@ -484,6 +516,10 @@ def measure_batched(args, dev, world, dist, factors=CONFIGURED, acc=None, e2e_le
         dist.all_reduce(acc_t)                   # mean intensity over all ranks' electrons
     n_all = world * (args.warmup + args.steps) * BATCH
     mean_peak = float(acc_t.max().item()) / n_all
+    mean = acc_t.cpu().numpy() / n_all
+    peak, peak_src = hbm_peak()
+    passes = batched_passes(me, offs[0], stream.cuda_stream, peak, peak_src,
+                            "batched leg (configured factors), one batch of %d electrons, CUDA events per pass" % BATCH)
 
     # end to end through the public API: host offsets in, mean intensity (host) out, every step
     e2e = None
@@ -502,7 +538,7 @@ def measure_batched(args, dev, world, dist, factors=CONFIGURED, acc=None, e2e_le
                "path": "srw_b200.multie.MultiE.add (C-ABI srwgMultiEAdd; base field resident, electron offsets "
                        "from host) + MultiE.mean (D2H of the %dx%d FP64 mean intensity)" % (acc['nx'], acc['ny'])}
     return dict(value=value, total_ms=total_ms, e2e=e2e, clocks=nv.summary() or clk.summary(), mean_peak=mean_peak,
-                n_all=n_all, mean=acc_t.cpu().numpy() / n_all, acc=acc)
+                n_all=n_all, mean=mean, acc=acc, passes=passes)
 
 
 def measure_mixed(args, dev, n_elec, model=None):
@@ -528,15 +564,16 @@ def measure_mixed(args, dev, n_elec, model=None):
             factors = CONFIGURED
             if mode == 'learned':
                 from srw_b200 import learned
+                chk_set = sample_offsets(N_CHECK, *SIG, seed=31337 + n, sig_e=SIG_E)
                 factors, fb, _ = learned.choose_factors(model, learned.bench_case(ex, ey, mesh, sc), dev,
-                                                        acc_mesh=acc)
+                                                        acc_mesh=acc, check_offsets=chk_set)
                 facs[n] = list(factors) + (['fallback'] if fb else [])
             bl = beamline_objs(mod, factors)
             b = batch or {256: 32, 512: 32, 1024: 16}[n]
             if mode == 'learned':
-                # one electron of every batch checked against its conservative propagation
+                # the mean intensity of the check set (grown by one electron per batch) checked before every batch
                 me = learned.CheckedMultiE(w, lambda f: beamline_objs(mod, f), factors, acc, max_batch=64,
-                                           graph=graph, device=dev.index)
+                                           graph=graph, device=dev.index, check_offsets=chk_set)
                 me.add(sample_offsets(64, *SIG, seed=999, sig_e=SIG_E))                 # warm-up (plans, graph)
                 me.reset()
             else:
@@ -562,8 +599,9 @@ def measure_mixed(args, dev, n_elec, model=None):
            "batched": res['batched'], "plain": res['plain'], "speedup": res['batched'] / res['plain'],
            "note": "each electron: offset field, C1 beamline (resize before the lens), intensity added in FP64 "
                    "onto a 512x512 common mesh; plain = the same electrons one per launch sequence with the "
-                   "configured factors (2, 2); learned = per grid class the network's factors, batches of 64 with "
-                   "one electron checked against its conservative propagation"}
+                   "configured factors (2, 2); learned = per grid class the network's factors (checked on the mean "
+                   "intensity of a 16-electron check set), batches of 64, the first electron of every batch added "
+                   "to the check set at both factors and the check repeated"}
     if model is not None:
         out.update({"batched_learned": res['learned'], "learned_speedup_vs_plain": res['learned'] / res['plain'],
                     "learned_factors": {str(k): v for k, v in facs.items()},
@@ -572,6 +610,7 @@ def measure_mixed(args, dev, n_elec, model=None):
 
 
 LEARNED_BATCH = 64               # macro-electron wavefronts per step of the learned leg (one checked batch)
+N_CHECK = 16                     # electrons of the learned factors' check set
 
 
 def load_model(dev):
@@ -585,10 +624,12 @@ def load_model(dev):
 
 def measure_learned(args, dev, world, dist, acc):
     """Batched path with the resize factors the trained network chooses for this wavefront and
-    beamline (srw_b200.learned.choose_factors: the wavefront propagated with them checked against the
-    conservative factors, fallback above 1e-3), run through learned.CheckedMultiE: batches of
-    LEARNED_BATCH electrons, one electron of every batch checked again against its conservative
-    propagation (fallback of the batch above 1e-3).  K steps between CUDA events, checks included."""
+    beamline (srw_b200.learned.choose_factors: the mean intensity of a seeded check set of N_CHECK
+    electrons propagated with them checked against the conservative factors', fallback above 1e-3),
+    run through learned.CheckedMultiE: batches of LEARNED_BATCH electrons, the first electron of every
+    batch added to the check set at both factors and the check repeated before the batch (above 1e-3
+    the run falls back to the conservative factors for good).  K steps between CUDA events, checks
+    included."""
     import torch
     from srw_b200 import learned
     from srw_b200 import srwlib as mod
@@ -597,12 +638,15 @@ def measure_learned(args, dev, world, dist, acc):
     if model is None:
         return None
     ex, ey, mesh, sc = synth_undulator_field(1024)
+    chk_set = sample_offsets(N_CHECK, *SIG, seed=31337, sig_e=SIG_E)
+    trace = []
     t0 = time.perf_counter()
-    factors, fallback, chk = learned.choose_factors(model, learned.bench_case(ex, ey, mesh, sc), dev, acc_mesh=acc)
+    factors, fallback, chk = learned.choose_factors(model, learned.bench_case(ex, ey, mesh, sc), dev, acc_mesh=acc,
+                                                    check_offsets=chk_set, trace=trace)
     choose_s = time.perf_counter() - t0
     w = make_wfr(mod, ex, ey, mesh, sc)
     cm = learned.CheckedMultiE(w, lambda f: beamline_objs(mod, f), factors, acc, max_batch=LEARNED_BATCH,
-                               graph=True, device=dev.index)
+                               graph=True, device=dev.index, check_offsets=chk_set)
     stream = torch.cuda.Stream(dev)
     rank = int(os.environ.get('RANK', '0'))
     for k in range(args.warmup):
@@ -624,7 +668,10 @@ def measure_learned(args, dev, world, dist, acc):
         torch.cuda.synchronize(dev)
     total_ms = _max_over_ranks(e0.elapsed_time(e1), dev, world, dist)
     value = world * args.steps * LEARNED_BATCH / (total_ms / 1000.)
-    ce = cm.check_errors[args.warmup:]
+    ce = cm.check_errors
+    peak, peak_src = hbm_peak()
+    passes = batched_passes(cm.safe if cm.fell_back else cm.fast, offs[0], stream.cuda_stream, peak, peak_src,
+                            "learned leg, one batch of %d electrons, CUDA events per pass" % LEARNED_BATCH)
     from srw_b200.plan import Plan
     nk_f = Plan(w, beamline_objs(mod, factors), device=dev.index).n_kernels
     nk_c = Plan(w, beamline_objs(mod), device=dev.index).n_kernels
@@ -632,13 +679,21 @@ def measure_learned(args, dev, world, dist, acc):
             # per step: the batch and the checked electron (kick, passes, accumulation each), and the
             # checked electron with the conservative factors
             "launches_per_step": 2 * (nk_f + 2) + (nk_c + 2),
-            "factors": list(factors), "configured_factors": list(CONFIGURED), "fallback": bool(fallback),
+            "factors": list(factors), "configured_factors": list(CONFIGURED),
+            "fallback": bool(fallback or cm.fell_back),
             "choice_check_rel_err": chk, "choose_seconds": choose_s,
-            "batch_checks": {"batches": len(ce), "fallbacks": int(sum(e > learned.TOL_LABEL for e in ce)),
-                             "max_rel_err": max(ce) if ce else None,
-                             "what": "first electron of each batch vs its conservative-factor propagation, "
-                                     "relative L2 of the intensity on the common mesh"},
-            "clocks": nv.summary(),
+            "choice_trace": [[list(f), e] for f, e in trace],
+            "choice_check": "mean intensity of %d electrons (seeded check set) on the detector mesh, candidate vs "
+                            "conservative factors, relative L2 where the conservative one exceeds 1e-3 of its "
+                            "maximum; tolerance %g" % (N_CHECK, learned.TOL_LABEL),
+            "run_checks": {"batches": len(ce), "fell_back": bool(cm.fell_back), "rerun_electrons": cm.rerun,
+                           "check_electrons": cm.n_check, "max_rel_err": max(ce) if ce else None,
+                           "last_rel_err": ce[-1] if ce else None,
+                           "what": "before every batch: the check set (the choice's electrons plus the first "
+                                   "electron of every batch so far) at both factors, relative L2 of the two mean "
+                                   "intensities; above the tolerance the run falls back to the conservative factors "
+                                   "for good and propagates the learned batches again"},
+            "clocks": nv.summary(), "passes": passes,
             "model": {k: v for k, v in getattr(model, 'meta', {}).items()
                       if k in ('samples', 'val_grid_at_least_label', 'val_cost_pred', 'labels_conservative', 'tol')}}
 
@@ -742,9 +797,7 @@ def run_ours(args, rank, world):
         ln['plain_at_learned_factors'] = {"ms_per_propagation": pl_l['total_ms'] / pl_l['steps'],
                                           "passes": [list(k) for k in pl_l['kinfo']],
                                           "per_pass_ms": [round(float(v), 4) for v in pl_l['per_k']]}
-    peak, peak_src = 6650., 'fallback'
-    if os.path.exists(PEAKS):
-        peak, peak_src = float(json.load(open(PEAKS))['hbm_gbs']), 'measured'
+    peak, peak_src = hbm_peak()
     pass_bytes = sum(kernel_bytes(k) for k in kinfo)
     # algorithmic bytes of one propagation (model: resize reads the old and writes the new mesh,
     # one 2D FFT = one read + one write pass per axis at the new mesh, point-wise work fused; both
@@ -791,8 +844,9 @@ def run_ours(args, rank, world):
            "config": {"workload": WORKLOAD, "step": "one batch of %d macro-electron wavefronts (1024^2 field with "
                                                     "its electron's source offset) through the beamline, intensities "
                                                     "added on the device%s" % (
-                                                        step_batch, ", learned factors %s with one electron of "
-                                                        "the batch checked against the configured factors"
+                                                        step_batch, ", learned factors %s, the mean intensity "
+                                                        "of the check set checked against the configured factors "
+                                                        "before the batch"
                                                         % (ln['factors'],) if use_learned else ""),
                       "grid_in": [1024, 1024], "grid_out": [plan.nx_out, plan.ny_out],
                       "passes": plan.n_kernels, "algorithmic_bytes_per_propagation": total_alg,
@@ -810,9 +864,12 @@ def run_ours(args, rank, world):
                               "reduced_over_ranks": world > 1},
            "batched_configured": {"value": bt['value'], "unit": UNIT, "factors": list(CONFIGURED), "batch": BATCH},
            "learned": ln,
-           "roofline": roofline(pl_l if (use_learned and pl_l is not None) else pl, peak, peak_src,
-                                "%s leg, single-wavefront passes, CUDA events per pass" %
-                                ("learned-factor" if (use_learned and pl_l is not None) else "plain")),
+           # the dominant pass of the leg that gives `value`, timed inside a batch as it runs there
+           "roofline": ln['passes'] if use_learned else bt['passes'],
+           "roofline_single_wavefront": roofline(pl_l if (use_learned and pl_l is not None) else pl, peak, peak_src,
+                                                 "%s leg, single-wavefront passes, CUDA events per pass" %
+                                                 ("learned-factor" if (use_learned and pl_l is not None)
+                                                  else "plain")),
            "roofline_plain": dict(roofline(pl, peak, peak_src, "plain leg, CUDA events per pass"),
                                   step_frac=(total_alg / (pl['total_ms'] / pl['steps'] / 1000.) / 1e9) / peak),
            "cpu_baseline": cpu,

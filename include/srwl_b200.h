@@ -239,6 +239,16 @@ SRWG_API int srwgMultiEAdd(srwgMultiE* m, int n, const double* arOffsets, void* 
 /* as srwgMultiEAdd with 5 doubles per electron: the fifth is the relative energy deviation d of the
  * electron, which rescales the photon energy of its wavefront to E (1 + 2 d) */
 SRWG_API int srwgMultiEAddE(srwgMultiE* m, int n, const double* arOffsets, void* stream);
+/* number of passes of a batch, whether the last one writes the total intensity (float) instead of
+ * the two fields (then the accumulation reads one float per sample), and (desc, optional) the text
+ * description of the passes as srwgPlanDescribe gives it */
+SRWG_API int srwgMultiEInfo(srwgMultiE* m, int* nPasses, int* intensityPass, char* desc, int descLen);
+/* adds 1 <= n <= maxBatch electrons (stride 4 or 5 doubles each) as ONE batch, without the CUDA graph,
+ * with CUDA events around every pass: passMs[i] = device time of pass i [ms] (at most maxPasses
+ * values), the last one the accumulation's; *nPasses = passes + 1.  Measurement aid (no reference
+ * counterpart). */
+SRWG_API int srwgMultiEAddTimed(srwgMultiE* m, int n, const double* arOffsets, int stride, void* stream,
+                                float* passMs, int maxPasses, int* nPasses);
 SRWG_API int srwgMultiEGetMean(srwgMultiE* m, double* arMean, long long* nElec, void* stream);
 /* device address of the FP64 intensity sum (pAccMesh ny x nx) and the electron count, e.g. for a
  * sum over ranks; srwgMultiESetAccumulator makes the object add into caller-owned device memory */

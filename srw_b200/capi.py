@@ -96,6 +96,9 @@ SYMBOLS = {
                                    C.c_int, C.POINTER(C.c_void_p)]),
     'srwgMultiEAdd': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     'srwgMultiEAddE': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    'srwgMultiEInfo': (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_int]),
+    'srwgMultiEAddTimed': (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_void_p]),
     'srwgMultiEGetMean': (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong), C.c_void_p]),
     'srwgMultiEAccumulator': (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong)]),
     'srwgMultiESetAccumulator': (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -167,8 +167,11 @@ struct srwgMultiE {
     cudaGraphExec_t graph = nullptr;
     int graphNb = 0;
     std::vector<KernelDesc> graphKs;     // host copy (launch shapes) the graph was captured with
+    std::vector<cudaEvent_t> tev;        // srwgMultiEAddTimed: events around every pass and the accumulation
+    long long nFlush = 0;                // batches run so far
     ~srwgMultiE()
     {
+        for (cudaEvent_t e : tev) cudaEventDestroy(e);
         if (graph) cudaGraphExecDestroy(graph);
         if (ownAcc) cudaFree(dAcc);
         cudaFree(dSnap);
@@ -257,10 +260,12 @@ static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, c
     float2* outY = m.dOut + (size_t)m.maxBatch * m.nOut;
     if (ks.empty()) { set_last_detail("multi-electron plan without passes"); return SRWG_ERR_BAD_ARG; }
     // every electron's first pass reads the base field (input stride 0) and applies its kick
+    cudaEvent_t* ev = m.tev.size() >= 2 * ks.size() + 2 ? m.tev.data() : nullptr;
     int r = execute_passes(ks, *m.ctx, nb, m.dBase, m.dBase + m.nIn, 0, outX, outY, (long long)m.nOut, m.dWork,
-                           m.perWork, m.dConst, (long long)m.constStride, m.descOff, st, nullptr, &ks);
+                           m.perWork, m.dConst, (long long)m.constStride, m.descOff, st, ev, &ks);
     if (r) return r;
     dim3 ga((m.anx + 255) / 256, m.anz);
+    if (ev) MTRY(cudaEventRecord(ev[2 * ks.size()], st));
     if (intensity_pass(ks))
         accum_int_kernel<<<ga, blk, 0, st>>>(reinterpret_cast<const float*>(outX), (long long)m.nOut, nb, m.dParams,
                                              m.dAcc, m.anx, m.anz, m.axStart, m.axStep, m.azStart, m.azStep);
@@ -268,6 +273,7 @@ static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, c
         accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams, m.dAcc, m.anx, m.anz,
                                          m.axStart, m.axStep, m.azStart, m.azStep);
     MTRY(cudaGetLastError());
+    if (ev) MTRY(cudaEventRecord(ev[2 * ks.size() + 1], st));
     return 0;
 }
 
@@ -275,6 +281,7 @@ static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, c
 static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_t st)
 {
     if (nb == 0) return 0;
+    m.nFlush++;
     MTRY(cudaMemcpyAsync(m.dConst, m.hConst[m.slot], (size_t)nb * m.constStride, cudaMemcpyHostToDevice, st));
     MTRY(cudaMemcpyAsync(m.dParams, m.hParams[m.slot], (size_t)nb * sizeof(ElecParams), cudaMemcpyHostToDevice, st));
     MTRY(cudaEventRecord(m.staged[m.slot], st));
@@ -282,7 +289,7 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
     // the next batch is staged in the other slot once that slot's previous upload has completed
     MTRY(cudaEventSynchronize(m.staged[m.slot]));
     int r = 0;
-    if (m.useGraph && nb == m.maxBatch) {
+    if (m.useGraph && nb == m.maxBatch && m.tev.empty()) {
         // the graph holds the launch shapes; a batch whose resize tiles are larger needs a new one
         bool fits = m.graph != nullptr && m.graphKs.size() == ks.size();
         for (size_t i = 0; fits && i < ks.size(); i++)
@@ -426,6 +433,51 @@ extern "C" SRWG_API int srwgMultiEAddE(srwgMultiE* m, int n, const double* arOff
 
 static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, cudaStream_t st);
 
+// one batch (1 <= n <= maxBatch electrons of one pass structure) added without the graph, with CUDA
+// events around every pass and the accumulation; passMs[i] = the device time of pass i, the last
+// value the accumulation's.  The electrons are added as by srwgMultiEAdd(E).
+extern "C" SRWG_API int srwgMultiEAddTimed(srwgMultiE* m, int n, const double* arOffsets, int stride, void* stream,
+                                           float* passMs, int maxPasses, int* nPasses)
+{
+    if (!m || n < 1 || n > m->maxBatch || !arOffsets || (stride != 4 && stride != 5) || !passMs || maxPasses < 1)
+        return SRWG_ERR_BAD_ARG;
+    int r = 0;
+    {
+        std::lock_guard<std::mutex> lk(library_mutex());
+        Planner pl;
+        pl.numMoments = false;
+        pl.inPhase = true;
+        r = pl.plan(&m->base, m->opt);
+        if (r) { set_last_detail(pl.err); return r; }
+        const size_t ne = 2 * pl.kernels.size() + 2;
+        for (cudaEvent_t e : m->tev) cudaEventDestroy(e);
+        m->tev.assign(ne, nullptr);
+        for (size_t i = 0; i < ne; i++) MTRY(cudaEventCreate(&m->tev[i]));
+    }
+    const long long n0 = m->nAdded, f0 = m->nFlush;
+    r = add_impl(m, n, arOffsets, stride, stream);
+    std::lock_guard<std::mutex> lk(library_mutex());
+    if (r == 0 && (m->nAdded - n0 != n || m->nFlush - f0 != 1)) {
+        set_last_detail("timed add: the electrons did not run as one batch");
+        r = SRWG_ERR_BAD_ARG;
+    }
+    const int np = (int)(m->tev.size() / 2);
+    if (r == 0) {
+        DeviceCtx* c = nullptr;
+        r = device_ctx(m->device, &c);
+        if (r == 0 && cudaStreamSynchronize(stream ? (cudaStream_t)stream : c->stream) != cudaSuccess) r = SRWG_ERR_CUDA;
+        for (int i = 0; r == 0 && i < np && i < maxPasses; i++) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, m->tev[2 * i], m->tev[2 * i + 1]) != cudaSuccess) r = SRWG_ERR_CUDA;
+            passMs[i] = ms;
+        }
+        if (nPasses) *nPasses = np;
+    }
+    for (cudaEvent_t e : m->tev) cudaEventDestroy(e);
+    m->tev.clear();
+    return r;
+}
+
 // A call either adds all its electrons or none: the accumulator is copied aside first, and on an
 // error (an electron whose passes differ in size from the base wavefront's, a failed launch) the
 // batches already added are taken out again by restoring that copy and the electron count.
@@ -531,6 +583,28 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
         nb++;
     }
     return flush(*m, nb, launchKs, st);
+}
+
+// passes of a batch, whether the last one writes the intensity instead of the two fields, and the
+// planner's description of the passes (the base electron's)
+extern "C" SRWG_API int srwgMultiEInfo(srwgMultiE* m, int* nPasses, int* intensityPass, char* desc, int descLen)
+{
+    std::lock_guard<std::mutex> lk(library_mutex());
+    if (!m) return SRWG_ERR_BAD_ARG;
+    Planner pl;
+    pl.numMoments = false;
+    pl.inPhase = true;
+    int r = pl.plan(&m->base, m->opt);
+    if (r) { set_last_detail(pl.err); return r; }
+    mark_intensity_pass(pl.kernels);
+    if (nPasses) *nPasses = (int)pl.kernels.size();
+    if (intensityPass) *intensityPass = intensity_pass(pl.kernels) ? 1 : 0;
+    if (desc && descLen > 0) {
+        const std::string s = pl.describe();
+        strncpy(desc, s.c_str(), descLen - 1);
+        desc[descLen - 1] = 0;
+    }
+    return 0;
 }
 
 extern "C" SRWG_API int srwgMultiEGetMean(srwgMultiE* m, double* arMean, long long* nElec, void* stream)

@@ -426,15 +426,27 @@ def new_length(n, rf, df):
     return int(capi.lib().srwgNextFftNumber(int(math.floor(n * rf * df + 0.5))))
 
 
+FILLED = 1024            # shortest line length whose single-wavefront passes fill the GPU
+
+
 def point_costs(n):
-    """(row, column) pass time per point [ms] of length n from the tuning table: measured where it
-    has the length, else the largest measured per-point time of the neighbouring lengths times 3
-    (the run-time-scheduled kernel)."""
+    """(row, column) pass time per point [ms] of length n from the tuning table.  The table times
+    one wavefront; below FILLED points per line its passes are too small to fill the GPU and the
+    time is mostly launch and tail latency, which a batch of wavefronts does not pay per wavefront,
+    so there the per-point time of the shortest measured length from FILLED up of the same kind
+    (power of two or not) stands in.  A length the table lacks gets the largest per-point time of
+    its measured neighbours times 3 (the run-time-scheduled kernel)."""
     t = _times()
-    if n in t:
-        return t[n][0] / (n * n), t[n][1] / (n * n)
     if not t:
         return (1., 1.) if (n & (n - 1)) == 0 else (5., 5.)
+    pow2 = (n & (n - 1)) == 0
+    if n < FILLED:
+        same = sorted(m for m in t if m >= FILLED and ((m & (m - 1)) == 0) == pow2)
+        if same:
+            m = same[0]
+            return t[m][0] / (m * m), t[m][1] / (m * m)
+    if n in t:
+        return t[n][0] / (n * n), t[n][1] / (n * n)
     near = sorted(t, key=lambda m: abs(math.log(m / n)))[:3]
     return (3. * max(t[m][0] / (m * m) for m in near), 3. * max(t[m][1] / (m * m) for m in near))
 
@@ -579,30 +591,72 @@ def _next(grid, v):
     return float(larger[0]) if len(larger) else float(v)
 
 
-def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=4):
+def mean_intensity(case, fac, offsets, acc_mesh, dev):
+    """Mean intensity (torch float64 [ny, nx] on dev) on mesh acc_mesh of the electrons `offsets`
+    ([n, 4] or [n, 5], srw_b200.multie.MultiE): the case's wavefront offset per electron,
+    propagated with factors fac."""
+    import torch
+    from . import srwlib as mod
+    from .multie import MultiE
+    acc = torch.zeros((acc_mesh['ny'], acc_mesh['nx']), dtype=torch.float64, device=dev)
+    me = MultiE(_wfr(mod, case), beamline(mod, case['ap'], case['f'], case['L'], fac, case.get('drift_mode', 4)),
+                acc_mesh, max_batch=min(16, len(offsets)), graph=False, device=dev.index)
+    me.use_accumulator(acc.data_ptr())
+    me.add(offsets, torch.cuda.current_stream(dev).cuda_stream)
+    torch.cuda.synchronize(dev)
+    del me
+    return acc / len(offsets)
+
+
+def rel_err(a, ref):
+    """Relative L2 of intensity a against ref (same mesh) where ref exceeds 1e-3 of its maximum."""
+    import torch
+    sel = ref > 1e-3 * ref.max()
+    d = torch.linalg.norm(ref[sel])
+    return float(torch.linalg.norm((a - ref)[sel]) / d) if float(d) > 0. else float('inf')
+
+
+def candidates_from(fac, tries):
+    """The prediction rounded to the grid, then the resolution, the range and both raised a grid step."""
+    rx, dx, rz, dz = fac
+    c = [tuple(fac), (rx, _next(GRID_D, dx), rz, _next(GRID_D, dz)), (_next(GRID_R, rx), dx, _next(GRID_R, rz), dz),
+         (_next(GRID_R, rx), _next(GRID_D, dx), _next(GRID_R, rz), _next(GRID_D, dz))]
+    return [v for i, v in enumerate(c) if v not in c[:i]][:tries]
+
+
+def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=4, check_offsets=None, trace=None):
     """(factors, used_fallback, check_error): the network's factors, rounded up to the grid, checked
-    by propagating the wavefront with them and with the conservative factors (relative L2 of the
-    intensity on the detector mesh acc_mesh when given -- the mesh a multi-electron run accumulates
-    on --, else at the output nodes); when the check exceeds check_tol, the resolution and then the
+    against the conservative factors; when the check exceeds check_tol, the resolution and then the
     range factors are raised a grid step at a time (up to `tries` candidates in all) before falling
-    back to the conservative factors."""
+    back to the conservative factors.
+
+    The check compares what the run produces.  With check_offsets (electrons [n, 4|5], and acc_mesh)
+    it is the mean intensity of those electrons on the detector mesh acc_mesh, propagated with the
+    candidate and with the conservative factors (a multi-electron run's result); otherwise the
+    wavefront itself, relative L2 of the intensity on acc_mesh when given, else at the candidate's
+    output nodes.  `trace`, a list, receives (factors, error) of every candidate checked."""
     feat = case_features(case, dev).unsqueeze(0)
     pred = model.predict(feat)[0].cpu().numpy()
     fac = tuple(choose_grid(pred, case['mesh']['nx'], case['mesh']['ny']))
     if fac == tuple(CONSERVATIVE):
         return CONSERVATIVE, False, 0.
-    Ic, omc = propagate_intensity(case, CONSERVATIVE, dev)
-    cands = [fac]
-    rx, dx, rz, dz = fac
-    cands.append((rx, _next(GRID_D, dx), rz, _next(GRID_D, dz)))
-    cands.append((_next(GRID_R, rx), dx, _next(GRID_R, rz), dz))
-    cands.append((_next(GRID_R, rx), _next(GRID_D, dx), _next(GRID_R, rz), _next(GRID_D, dz)))
+    if check_offsets is not None:
+        if acc_mesh is None:
+            raise ValueError('a check on electrons needs the detector mesh')
+        Ic = mean_intensity(case, CONSERVATIVE, check_offsets, acc_mesh, dev)
+    else:
+        Ic, omc = propagate_intensity(case, CONSERVATIVE, dev)
     e = None
-    for c in [c for i, c in enumerate(cands) if c not in cands[:i]][:tries]:
+    for c in candidates_from(fac, tries):
         if c == tuple(CONSERVATIVE):
             break
-        I, om = propagate_intensity(case, c, dev)
-        e = mesh_error(I, om, Ic, omc, acc_mesh) if acc_mesh is not None else _common_error(I, om, Ic, omc)
+        if check_offsets is not None:
+            e = rel_err(mean_intensity(case, c, check_offsets, acc_mesh, dev), Ic)
+        else:
+            I, om = propagate_intensity(case, c, dev)
+            e = mesh_error(I, om, Ic, omc, acc_mesh) if acc_mesh is not None else _common_error(I, om, Ic, omc)
+        if trace is not None:
+            trace.append((c, e))
         if e <= check_tol:
             return c, False, e
     return CONSERVATIVE, True, e
@@ -610,34 +664,59 @@ def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=4
 
 class CheckedMultiE(object):
     """Multi-electron propagation (srw_b200.multie.MultiE) with learned factors and a run-time check
-    per batch: the first electron of every batch is also propagated with the conservative factors;
-    when the two intensities on the common mesh differ by more than `tol` (relative L2 where the
-    conservative one exceeds 1e-3 of its maximum) the batch runs with the conservative factors.
-    Both paths add into one FP64 accumulator (a torch tensor); ``mean()`` divides by the electrons
-    added."""
+    of the mean intensity.  A check set of electrons is propagated with both the learned and the
+    conservative factors into two FP64 sums on the detector mesh: the electrons `check_offsets`
+    given at construction (those of choose_factors' check), then the first electron of every batch.
+    Before a batch runs, the relative L2 of the two sums (where the conservative one exceeds 1e-3 of
+    its maximum) is compared with `tol`; above it the run falls back for good: the electrons added
+    so far with the learned factors are propagated again with the conservative ones (the sum is
+    rebuilt), and so are all later batches.  ``mean()`` divides by the electrons added."""
 
     def __init__(self, base_wfr, make_beamline, factors, acc_mesh, max_batch=64, safe_batch=16, graph=True,
-                 device=0, tol=TOL_LABEL):
+                 device=0, tol=TOL_LABEL, check_offsets=None):
         import torch
-        from .multie import MultiE
+        from .multie import MultiE, offset_array
         self.torch = torch
         self.dev = torch.device('cuda', device)
         self.acc = torch.zeros((acc_mesh['ny'], acc_mesh['nx']), dtype=torch.float64, device=self.dev)
         self.chk = [torch.zeros_like(self.acc), torch.zeros_like(self.acc)]
+        self.learned = tuple(factors) != tuple(CONSERVATIVE)
         self.fast = MultiE(base_wfr, make_beamline(factors), acc_mesh, max_batch=max_batch, graph=graph, device=device)
         self.safe = MultiE(base_wfr, make_beamline(CONSERVATIVE), acc_mesh, max_batch=safe_batch, graph=graph,
                            device=device)
-        self.cfast = MultiE(base_wfr, make_beamline(factors), acc_mesh, max_batch=1, graph=False, device=device)
-        self.csafe = MultiE(base_wfr, make_beamline(CONSERVATIVE), acc_mesh, max_batch=1, graph=False, device=device)
         self.fast.use_accumulator(self.acc.data_ptr())
         self.safe.use_accumulator(self.acc.data_ptr())
-        self.cfast.use_accumulator(self.chk[0].data_ptr())
-        self.csafe.use_accumulator(self.chk[1].data_ptr())
+        self.cfast = self.csafe = None
+        if self.learned:
+            self.cfast = MultiE(base_wfr, make_beamline(factors), acc_mesh, max_batch=16, graph=False, device=device)
+            self.csafe = MultiE(base_wfr, make_beamline(CONSERVATIVE), acc_mesh, max_batch=16, graph=False,
+                                device=device)
+            self.cfast.use_accumulator(self.chk[0].data_ptr())
+            self.csafe.use_accumulator(self.chk[1].data_ptr())
+        self.check0 = None if check_offsets is None else offset_array(check_offsets)
         self.max_batch, self.tol = max_batch, tol
-        self.n, self.batches, self.fallbacks, self.check_errors = 0, 0, 0, []
+        self._start()
+
+    def _start(self):
+        self.n, self.n_check, self.batches, self.check_errors = 0, 0, 0, []
+        self.fell_back, self.rerun, self.added_fast = False, 0, []
+        for c in self.chk:
+            c.zero_()
+        if self.learned and self.check0 is not None and len(self.check0):
+            self.cfast.add(self.check0)
+            self.csafe.add(self.check0)
+            self.n_check = len(self.check0)
+
+    def _fall_back(self, stream):
+        self.fell_back = True
+        self.acc.zero_()
+        for b in self.added_fast:
+            self.safe.add(b, stream)
+            self.rerun += len(b)
+        self.added_fast = []
 
     def add(self, offsets, stream=None):
-        """Adds the electrons (offsets as MultiE.add) in batches of max_batch, each checked first.
+        """Adds the electrons (offsets as MultiE.add) in batches of max_batch, each after the check.
         `stream`: a CUDA stream handle; the checks' reductions run on it too."""
         import contextlib
         from .multie import offset_array
@@ -648,30 +727,39 @@ class CheckedMultiE(object):
         with ctx:
             for i0 in range(0, len(off), self.max_batch):
                 b = off[i0:i0 + self.max_batch]
-                for c in self.chk:
-                    c.zero_()
-                self.cfast.add(b[:1], stream)
-                self.csafe.add(b[:1], stream)
-                ref = self.chk[1]
-                sel = ref > 1e-3 * ref.max()
-                e = float(torch.linalg.norm((self.chk[0] - ref)[sel]) / torch.linalg.norm(ref[sel]))
-                self.check_errors.append(e)
-                (self.fast if e <= self.tol else self.safe).add(b, stream)
-                self.fallbacks += e > self.tol
+                if self.learned and not self.fell_back:
+                    self.cfast.add(b[:1], stream)
+                    self.csafe.add(b[:1], stream)
+                    self.n_check += 1
+                    e = rel_err(self.chk[0], self.chk[1])
+                    self.check_errors.append(e)
+                    if e > self.tol:
+                        self._fall_back(stream)
+                if self.learned and not self.fell_back:
+                    self.fast.add(b, stream)
+                    self.added_fast.append(b)
+                else:
+                    self.safe.add(b, stream)
                 self.batches += 1
                 self.n += len(b)
+
+    @property
+    def fallbacks(self):
+        return int(self.fell_back)
 
     def mean(self):
         self.torch.cuda.synchronize(self.dev)
         return (self.acc / max(self.n, 1)).cpu().numpy()
 
     def reset(self):
-        """Clears the accumulated intensity and the counters (plans and captured graphs are kept)."""
+        """Clears the accumulated intensity, the check sums (the construction-time check set is
+        propagated again) and the counters; plans and captured graphs are kept."""
         self.torch.cuda.synchronize(self.dev)
         self.acc.zero_()
-        for m in (self.fast, self.safe):
-            m.reset()
-        self.n, self.batches, self.fallbacks, self.check_errors = 0, 0, 0, []
+        for m in (self.fast, self.safe, self.cfast, self.csafe):
+            if m is not None:
+                m.reset()
+        self._start()
 
 
 # ------------------------------------------------------------------------------------------------

@@ -112,6 +112,29 @@ class MultiE(object):
         f = capi.lib().srwgMultiEAddE if m == 5 else capi.lib().srwgMultiEAdd
         capi.check(f(self._h, int(off.shape[0]), off.ctypes.data, st), 'multi-electron add')
 
+    def add_timed(self, offsets, stream=None, ncols=None):
+        """Adds up to max_batch electrons as one batch without the graph and returns the device time
+        [ms] of each pass and, last, of the accumulation (CUDA events on the stream)."""
+        off = offset_array(offsets, ncols)
+        ms = (C.c_float * 64)()
+        n = C.c_int()
+        st = C.c_void_p(stream) if stream else None
+        capi.check(capi.lib().srwgMultiEAddTimed(self._h, int(off.shape[0]), off.ctypes.data, int(off.shape[1]), st,
+                                                 ms, 64, C.byref(n)), 'multi-electron timed add')
+        return [float(ms[i]) for i in range(min(n.value, 64))]
+
+    def info(self):
+        """(passes of a batch [(kind, sizes...)] as Plan.kernels gives them, whether the last pass
+        writes the intensity instead of the fields)."""
+        from .plan import parse_passes
+        n, i = C.c_int(), C.c_int()
+        buf = C.create_string_buffer(1 << 16)
+        capi.check(capi.lib().srwgMultiEInfo(self._h, C.byref(n), C.byref(i), buf, len(buf)), 'multi-electron info')
+        ks = parse_passes(buf.value.decode())
+        if len(ks) != n.value:
+            raise RuntimeError('multi-electron info: %d passes described, %d planned' % (len(ks), n.value))
+        return ks, bool(i.value)
+
     def count(self):
         n = C.c_longlong()
         capi.check(capi.lib().srwgMultiEGetMean(self._h, None, C.byref(n), None))

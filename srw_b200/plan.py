@@ -15,6 +15,31 @@ from . import capi
 from .srwlpy import make_c_optc, make_c_wfr
 
 
+def parse_passes(text):
+    """[(kind, sizes...), ...] of the passes in a plan description (srwgPlanDescribe's text):
+    ('line_rows'|'line_cols', nx, ny), ('resize', nx_old, ny_old, nx_new, ny_new), ('moments', nx, ny)
+    or ('pw', nx, ny)."""
+    out = []
+    for line in text.splitlines():
+        f = line.split()
+        if len(f) < 3:
+            continue
+        if f[1] == 'LINE':
+            nx, ny = f[3].split('x')
+            out.append(('line_' + f[2], int(nx), int(ny)))
+        elif f[1] == 'RESIZE':
+            nxo, nyo = f[2].split('x')
+            nxn, nyn = f[4].split('x')
+            out.append(('resize', int(nxo), int(nyo), int(nxn), int(nyn)))
+        elif f[1] == 'MOM':
+            nx, ny = f[2].split('x')
+            out.append(('moments', int(nx), int(ny)))
+        else:
+            nx, ny = f[2].split('x')
+            out.append(('pw', int(nx), int(ny)))
+    return out
+
+
 class Plan(object):
     def __init__(self, wfr, optC, device=0):
         L = capi.lib()
@@ -88,25 +113,7 @@ class Plan(object):
 
     def kernels(self):
         """[(kind, nx, ny), ...] of the planned passes, parsed from describe()."""
-        out = []
-        for line in self.describe().splitlines():
-            f = line.split()
-            if len(f) < 3:
-                continue
-            if f[1] == 'LINE':
-                nx, ny = f[3].split('x')
-                out.append(('line_' + f[2], int(nx), int(ny)))
-            elif f[1] == 'RESIZE':
-                nxo, nyo = f[2].split('x')
-                nxn, nyn = f[4].split('x')
-                out.append(('resize', int(nxo), int(nyo), int(nxn), int(nyn)))
-            elif f[1] == 'MOM':
-                nx, ny = f[2].split('x')
-                out.append(('moments', int(nx), int(ny)))
-            else:
-                nx, ny = f[2].split('x')
-                out.append(('pw', int(nx), int(ny)))
-        return out
+        return parse_passes(self.describe())
 
     def execute_batch(self, ex_in, ey_in, ex_out, ey_out, stream=None):
         B = ex_in.shape[0]

@@ -610,7 +610,7 @@ def measure_mixed(args, dev, n_elec, model=None):
 
 
 LEARNED_BATCH = 64               # macro-electron wavefronts per step of the learned leg (one checked batch)
-N_CHECK = 16                     # electrons of the learned factors' check set
+N_CHECK = 32                     # electrons of the learned factors' check set
 
 
 def load_model(dev):

@@ -632,7 +632,13 @@ cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
         if (inten && (p.d.has_extra || (p.d.f1 && p.d.f2))) return cudaErrorInvalidValue;
         Line2Fn f = linen_kernel_ptr(p.N, p.d.axis != 0, p.d.has_extra != 0, (p.d.f1 && p.d.f2) ? 2 : 1, inten);
         if (f == nullptr || p.T * p.L > 512) return cudaErrorInvalidValue;
-        if (inten) grid.y = 1;                  // one CTA transforms both components of its lines
+        if (inten) {
+            grid.y = 1;                         // one CTA transforms both components of its lines
+            // the first component's intensity of every point a thread stores, in shared memory
+            // after the line slots
+            smem += (size_t)linen_int_floats(p.N) * p.T * p.L * sizeof(float);
+            if (smem > SRWG_LINE_SMEM_MAX) return cudaErrorInvalidValue;
+        }
         // input tiles by bulk async copies: 16-byte aligned sources; rows are contiguous, columns
         // only when the row pass wrote them in blocks of exactly the tile's (even) width
         LineLaunch q = p;

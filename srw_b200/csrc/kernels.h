@@ -139,6 +139,17 @@ inline bool linen_pow2(int N)
 #undef SRWG_LINEN_IS
     return false;
 }
+// floats per thread that an intensity pass of the specialised kernel keeps between its two
+// components: the last stage's butterflies per thread times its radix (the radix schedule of
+// linen.cuh: radix-16 stages, one 8/4/2 stage, then 3, 5, 7; ceil(N/16) threads per line)
+__host__ __device__ constexpr int linen_int_floats(int N)
+{
+    int m = N, p2 = 0;
+    while (m % 2 == 0) { m /= 2; p2++; }
+    const int R = m % 7 == 0 ? 7 : m % 5 == 0 ? 5 : m % 3 == 0 ? 3 : (p2 % 4 ? 1 << (p2 % 4) : 16);
+    const int T = (N + 15) / 16;
+    return ((N / R + T - 1) / T) * R;
+}
 // line-pass kernel families (LineLaunch::v2)
 enum { FAM_TAB = 0, FAM_POW2 = 1, FAM_GEN = 2, FAM_SPEC = 3 };
 // lines per CTA of the specialised general-length pass (at most 512 threads, 128 registers each):

@@ -216,7 +216,11 @@ template <int B, int R> __device__ __forceinline__ void conj_all(float2 (&v)[B][
 template <int N> struct IAcc {
     static constexpr int R = NSched_last(N);
     static constexpr int B = (N / R + NPlan<N>::T - 1) / NPlan<N>::T;
-    float v[B][R];
+    // in shared memory (registers would halve the CTAs per SM): value (b, r) of thread tid at
+    // v[(b R + r) nt + tid], nt threads per CTA (consecutive threads, consecutive words)
+    float* v;
+    int nt, tid;
+    __device__ __forceinline__ float& at(int b, int r) const { return v[(b * R + r) * nt + tid]; }
 };
 
 template <int N, int R, int NS, int IN, int OUT, bool FIRST, bool LAST, bool EXTRA, int OUTI = 0>
@@ -367,9 +371,9 @@ __device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& 
                 if constexpr (OUTI == 0) {
                     if (x.store) __stcs(&x.gout[x.om.at(kk)], o);
                 } else if constexpr (OUTI == 1) {
-                    acc->v[b][r] = o.x * o.x + o.y * o.y;            // first component
+                    acc->at(b, r) = o.x * o.x + o.y * o.y;           // first component
                 } else {
-                    const float I = acc->v[b][r] + o.x * o.x + o.y * o.y;
+                    const float I = acc->at(b, r) + o.x * o.x + o.y * o.y;
                     if (x.store) __stcs(reinterpret_cast<float*>(x.gout) + x.om.at(kk), I);
                 }
             }
@@ -538,10 +542,15 @@ __global__ void __launch_bounds__(512, (EXTRA || NT == 2) ? 1 : 2) linen_kernel(
 // intensity pass (the last pass of a multi-electron batch): both components of the CTA's lines one
 // after the other (one transform each, no non-separable work), |Ex|^2 + |Ey|^2 written as float
 template <int N, bool COLS>
-__global__ void __launch_bounds__(512, 1) linen_int_kernel(const LineLaunch p)
+__global__ void __launch_bounds__(512, 2) linen_int_kernel(const LineLaunch p)
 {
+    static_assert(linen_int_floats(N) == IAcc<N>::B * IAcc<N>::R, "host size of the intensity carry");
+    extern __shared__ __align__(16) float2 smn[];
     __shared__ uint64_t bar;
     IAcc<N> acc;
+    acc.v = reinterpret_cast<float*>(smn + (size_t)p.L * p.P);
+    acc.nt = blockDim.x;
+    acc.tid = threadIdx.x;
     if (!linen_body<N, COLS, false, 1, 1>(p, 0, &acc, &bar, 0)) return;
     __syncthreads();                          // the second component's copies overwrite the tile
     linen_body<N, COLS, false, 1, 2>(p, 1, &acc, &bar, 1);

@@ -1704,6 +1704,52 @@ int Planner::run()
     return finalize();
 }
 
+// Box of old-mesh indices [i0, i1] x [j0, j1] outside which the point-wise work `pw` (indices of an
+// nx x nz mesh) zeroes the field: the intersection of its apertures' (not obstacles') rectangles or
+// the squares around their circles, widened by 2 indices against rounding of the coordinates.
+// False when it has no aperture mask.
+static bool aperture_box(const PwOps& pw, int nx, int nz, int& i0, int& i1, int& j0, int& j1)
+{
+    bool any = false;
+    i0 = 0; i1 = nx - 1; j0 = 0; j1 = nz - 1;
+    for (int m = 0; m < pw.nmask; m++) {
+        const PwMask& k = pw.mask[m];
+        if (k.obstacle || k.dx == 0. || k.dz == 0.) continue;
+        const double hx = k.type == 1 ? k.hx : std::sqrt(k.r2), hz = k.type == 1 ? k.hz : std::sqrt(k.r2);
+        auto range = [](double lo, double hi, double x0, double dx, int n, int& a, int& b) {
+            double u = (lo - x0) / dx, v = (hi - x0) / dx;
+            if (u > v) std::swap(u, v);
+            const double fa = std::floor(u) - 2., fb = std::ceil(v) + 2.;
+            a = std::max(a, (int)std::max(-1., std::min((double)n, fa)));
+            b = std::min(b, (int)std::max(-1., std::min((double)n, fb)));
+        };
+        range(k.cx - hx, k.cx + hx, k.x0, k.dx, nx, i0, i1);
+        range(k.cz - hz, k.cz + hz, k.z0, k.dz, nz, j0, j1);
+        any = true;
+    }
+    return any;
+}
+
+// new indices in [s, e] whose gather stencil (old nodes st .. st+3, ResizeAxis at float2 offset
+// `off` of the tables) meets the old indices [lo, hi]: a contiguous range (st is non-decreasing)
+static void stencil_window(const std::vector<float2>& T, long long off, int lo, int hi, int& s, int& e)
+{
+    int a = s, b = e;
+    ResizeAxis x;
+    while (a <= b) {
+        memcpy(&x, &T[off + 2 * a], sizeof(x));
+        if (x.st + 3 >= lo) break;
+        a++;
+    }
+    while (b >= a) {
+        memcpy(&x, &T[off + 2 * b], sizeof(x));
+        if (x.st <= hi) break;
+        b--;
+    }
+    s = a;
+    e = b;
+}
+
 // checks the passes of the plan (or stage), fills their tables and links neighbouring passes
 int Planner::finalize()
 {
@@ -1755,8 +1801,21 @@ int Planner::finalize()
         const int N = n.line.axis == 0 ? n.line.nx : n.line.nz;
         if (fixed_lines_per_cta(n.line.axis, N) == 0) continue;      // compile-time-length line kernels only
         LineDesc& d = n.line;
-        const int ixs = (int)std::max(0L, r.ixStart), ixe = (int)std::min((long)r.nxn - 1, r.ixEnd);
-        const int izs = (int)std::max(0L, r.izStart), ize = (int)std::min((long)r.nzn - 1, r.izEnd);
+        int ixs = (int)std::max(0L, r.ixStart), ixe = (int)std::min((long)r.nxn - 1, r.ixEnd);
+        int izs = (int)std::max(0L, r.izStart), ize = (int)std::min((long)r.nzn - 1, r.izEnd);
+        // an aperture folded in before the resampling zeroes the old field outside its box: the new
+        // points whose stencils miss the box are zeros, so the window (what the resize computes and
+        // the line pass loads) shrinks to the new points whose stencils meet it
+        int i0, i1, j0, j1;
+        if (r.has_pre && ixs <= ixe && izs <= ize && aperture_box(r.pre, r.nxo, r.nzo, i0, i1, j0, j1)) {
+            int a = ixs, b = ixe, c = izs, e = ize;
+            stencil_window(tables, r.axx, i0, i1, a, b);
+            stencil_window(tables, r.axz, j0, j1, c, e);
+            if (a <= b && c <= e) {
+                ixs = a; ixe = b; izs = c; ize = e;
+                r.ixStart = a; r.ixEnd = b; r.izStart = c; r.izEnd = e;
+            }
+        }
         r.skip_zero = 1;
         d.zwin = 1;
         if (d.axis == 0) { d.zl0 = izs; d.zl1 = ize; d.za0 = ixs; d.za1 = ixe; }
@@ -1811,13 +1870,16 @@ std::string Planner::describe() const
             LineLaunch lp;
             memset(&lp, 0, sizeof(lp));
             const char* fam = line_config(d, lp) ? "none" : lp.v2 == 1 ? "pow2" : lp.v2 == 3 ? "spec" : lp.v2 == 2 ? "gen" : "tab";
-            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d zwin=%d blk=%d/%d  buf %d->%d  fft=%s L=%d\n",
+            char win[64] = "";
+            if (d.zwin) snprintf(win, sizeof(win), "  lines=%d:%d points=%d:%d", d.zl0, d.zl1, d.za0, d.za1);
+            snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d zwin=%d blk=%d/%d  buf %d->%d  fft=%s L=%d%s\n",
                      i, d.axis == 0 ? "rows" : "cols", d.nx, d.nz, d.f1, d.has_pw, d.pw.has_quad, d.pw.has_ang, d.pw.nmask,
-                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, d.zwin, d.blk_in, d.blk_out, k.src, k.dst, fam, lp.L);
+                     d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, d.zwin, d.blk_in, d.blk_out, k.src, k.dst, fam, lp.L,
+                     win);
         } else if (k.kind == K_RESIZE) {
-            snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pre=%d pw=%d tile=%dx%d  buf %d->%d\n", i,
-                     k.rs.nxo, k.rs.nzo, k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pre, k.rs.has_pw, k.rs.tile_or,
-                     k.rs.tile_oc, k.src, k.dst);
+            snprintf(buf, sizeof(buf), "%zu RESIZE %dx%d -> %dx%d only_larger=%d pre=%d pw=%d tile=%dx%d  buf %d->%d  window=x%ld:%ld,z%ld:%ld\n",
+                     i, k.rs.nxo, k.rs.nzo, k.rs.nxn, k.rs.nzn, k.rs.only_larger, k.rs.has_pre, k.rs.has_pw, k.rs.tile_or,
+                     k.rs.tile_oc, k.src, k.dst, k.rs.ixStart, k.rs.ixEnd, k.rs.izStart, k.rs.izEnd);
         } else if (k.kind == K_MOM) {
             snprintf(buf, sizeof(buf), "%zu MOM %dx%d (q%d a%d m%d s%d) slot=%d  buf %d\n", i, k.mom.nx, k.mom.nz,
                      k.mom.pw.has_quad, k.mom.pw.has_ang, k.mom.pw.nmask, k.mom.pw.has_scale, k.mom.slot, k.src);

@@ -616,19 +616,36 @@ def rel_err(a, ref):
     return float(torch.linalg.norm((a - ref)[sel]) / d) if float(d) > 0. else float('inf')
 
 
-def candidates_from(fac, tries):
-    """The prediction rounded to the grid, then the resolution, the range and both raised a grid step."""
+def candidates_from(fac, tries, nx=None, nz=None):
+    """Candidates for the check, in order: the prediction rounded to the grid, then the prediction
+    with its range factors raised 1, 2, 3 grid steps and its resolution factors 0 or 1 step (range sets
+    the output mesh step of a propagation to the waist, resolution its extent), cheapest first (grid
+    cost on an nx x nz input when given), none as dear as the conservative factors; at most `tries`."""
     rx, dx, rz, dz = fac
-    c = [tuple(fac), (rx, _next(GRID_D, dx), rz, _next(GRID_D, dz)), (_next(GRID_R, rx), dx, _next(GRID_R, rz), dz),
-         (_next(GRID_R, rx), _next(GRID_D, dx), _next(GRID_R, rz), _next(GRID_D, dz))]
-    return [v for i, v in enumerate(c) if v not in c[:i]][:tries]
+    out = [tuple(fac)]
+    more = []
+    for sr in (1, 2, 3):
+        for sd in (0, 1):
+            ax, az, bx, bz = rx, rz, dx, dz
+            for _ in range(sr):
+                ax, az = _next(GRID_R, ax), _next(GRID_R, az)
+            for _ in range(sd):
+                bx, bz = _next(GRID_D, bx), _next(GRID_D, bz)
+            more.append((ax, bx, az, bz))
+    if nx is not None:
+        cmax = grid_cost(nx, nz, CONSERVATIVE)
+        more = sorted((c for c in more if grid_cost(nx, nz, c) < cmax), key=lambda c: grid_cost(nx, nz, c))
+    for c in more:
+        if c not in out and c != tuple(CONSERVATIVE):
+            out.append(c)
+    return out[:tries]
 
 
-def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=4, check_offsets=None, trace=None):
+def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=6, check_offsets=None, trace=None):
     """(factors, used_fallback, check_error): the network's factors, rounded up to the grid, checked
-    against the conservative factors; when the check exceeds check_tol, the resolution and then the
-    range factors are raised a grid step at a time (up to `tries` candidates in all) before falling
-    back to the conservative factors.
+    against the conservative factors; when the check exceeds check_tol, the candidates of
+    candidates_from (range raised first, cheapest first; up to `tries` in all) follow before the
+    conservative factors are used.
 
     The check compares what the run produces.  With check_offsets (electrons [n, 4|5], and acc_mesh)
     it is the mean intensity of those electrons on the detector mesh acc_mesh, propagated with the
@@ -647,7 +664,7 @@ def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=4
     else:
         Ic, omc = propagate_intensity(case, CONSERVATIVE, dev)
     e = None
-    for c in candidates_from(fac, tries):
+    for c in candidates_from(fac, tries, case['mesh']['nx'], case['mesh']['ny']):
         if c == tuple(CONSERVATIVE):
             break
         if check_offsets is not None:

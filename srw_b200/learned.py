@@ -641,11 +641,19 @@ def candidates_from(fac, tries, nx=None, nz=None):
     return out[:tries]
 
 
-def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=6, check_offsets=None, trace=None):
+def _prev(grid, v):
+    smaller = grid[grid < v - 1e-9]
+    return float(smaller[-1]) if len(smaller) else float(v)
+
+
+def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=6, check_offsets=None, trace=None,
+                   refine=0):
     """(factors, used_fallback, check_error): the network's factors, rounded up to the grid, checked
     against the conservative factors; when the check exceeds check_tol, the candidates of
     candidates_from (range raised first, cheapest first; up to `tries` in all) follow before the
-    conservative factors are used.
+    conservative factors are used.  With refine > 0, a passing choice is then refined by the check:
+    its resolution factors lowered a grid step at a time (both axes, then x alone, then z alone) while
+    the check still passes, at most `refine` more checks.
 
     The check compares what the run produces.  With check_offsets (electrons [n, 4|5], and acc_mesh)
     it is the mean intensity of those electrons on the detector mesh acc_mesh, propagated with the
@@ -663,10 +671,8 @@ def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=6
         Ic = mean_intensity(case, CONSERVATIVE, check_offsets, acc_mesh, dev)
     else:
         Ic, omc = propagate_intensity(case, CONSERVATIVE, dev)
-    e = None
-    for c in candidates_from(fac, tries, case['mesh']['nx'], case['mesh']['ny']):
-        if c == tuple(CONSERVATIVE):
-            break
+
+    def check(c):
         if check_offsets is not None:
             e = rel_err(mean_intensity(case, c, check_offsets, acc_mesh, dev), Ic)
         else:
@@ -674,9 +680,34 @@ def choose_factors(model, case, dev, check_tol=TOL_LABEL, acc_mesh=None, tries=6
             e = mesh_error(I, om, Ic, omc, acc_mesh) if acc_mesh is not None else _common_error(I, om, Ic, omc)
         if trace is not None:
             trace.append((c, e))
+        return e
+
+    e, got = None, None
+    for c in candidates_from(fac, tries, case['mesh']['nx'], case['mesh']['ny']):
+        if c == tuple(CONSERVATIVE):
+            break
+        e = check(c)
         if e <= check_tol:
-            return c, False, e
-    return CONSERVATIVE, True, e
+            got = c
+            break
+    if got is None:
+        return CONSERVATIVE, True, e
+    left = refine
+    while left > 0:
+        rx, dx, rz, dz = got
+        better = False
+        for c in ((rx, _prev(GRID_D, dx), rz, _prev(GRID_D, dz)), (rx, _prev(GRID_D, dx), rz, dz),
+                  (rx, dx, rz, _prev(GRID_D, dz))):
+            if c == got or left <= 0:
+                continue
+            left -= 1
+            e2 = check(c)
+            if e2 <= check_tol:
+                got, e, better = c, e2, True
+                break
+        if not better:
+            break
+    return got, False, e
 
 
 class CheckedMultiE(object):
@@ -684,10 +715,12 @@ class CheckedMultiE(object):
     of the mean intensity.  A check set of electrons is propagated with both the learned and the
     conservative factors into two FP64 sums on the detector mesh: the electrons `check_offsets`
     given at construction (those of choose_factors' check), then the first electron of every batch.
-    Before a batch runs, the relative L2 of the two sums (where the conservative one exceeds 1e-3 of
-    its maximum) is compared with `tol`; above it the run falls back for good: the electrons added
-    so far with the learned factors are propagated again with the conservative ones (the sum is
-    rebuilt), and so are all later batches.  ``mean()`` divides by the electrons added."""
+    With every batch the relative L2 of the two sums (where the conservative one exceeds 1e-3 of its
+    maximum) is queued on the stream; it is read before the next batch is queued, or by ``mean()``,
+    so the host never waits for the batch it has just queued.  Above `tol` the run falls back for
+    good: every electron added so far with the learned factors (the checked batch included) is
+    propagated again with the conservative ones (the sum is rebuilt), and so are all later batches.
+    ``mean()`` divides by the electrons added."""
 
     def __init__(self, base_wfr, make_beamline, factors, acc_mesh, max_batch=64, safe_batch=16, graph=True,
                  device=0, tol=TOL_LABEL, check_offsets=None):
@@ -712,11 +745,13 @@ class CheckedMultiE(object):
             self.csafe.use_accumulator(self.chk[1].data_ptr())
         self.check0 = None if check_offsets is None else offset_array(check_offsets)
         self.max_batch, self.tol = max_batch, tol
+        self._host = torch.empty(2, dtype=torch.float64, pin_memory=True)
         self._start()
 
     def _start(self):
         self.n, self.n_check, self.batches, self.check_errors = 0, 0, 0, []
         self.fell_back, self.rerun, self.added_fast = False, 0, []
+        self._pending = None
         for c in self.chk:
             c.zero_()
         if self.learned and self.check0 is not None and len(self.check0):
@@ -724,35 +759,62 @@ class CheckedMultiE(object):
             self.csafe.add(self.check0)
             self.n_check = len(self.check0)
 
+    def _queue_check(self):
+        """Queues the check error of the sums so far on the current stream (no host synchronisation)."""
+        torch = self.torch
+        a, ref = self.chk
+        sel = ref > 1e-3 * ref.max()
+        zero = torch.zeros((), dtype=ref.dtype, device=ref.device)
+        num = torch.linalg.norm(torch.where(sel, a - ref, zero))
+        den = torch.linalg.norm(torch.where(sel, ref, zero))
+        self._host.copy_(torch.stack([num, den]), non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self._pending = ev
+
+    def _resolve(self, stream):
+        """Reads the queued check; above the tolerance, falls back."""
+        if self._pending is None:
+            return
+        self._pending.synchronize()
+        self._pending = None
+        num, den = float(self._host[0]), float(self._host[1])
+        e = num / den if den > 0. else float('inf')
+        self.check_errors.append(e)
+        if e > self.tol:
+            self._fall_back(stream)
+
     def _fall_back(self, stream):
         self.fell_back = True
         self.acc.zero_()
+        if stream is None:
+            self.torch.cuda.synchronize(self.dev)      # the library's own stream adds next
         for b in self.added_fast:
             self.safe.add(b, stream)
             self.rerun += len(b)
         self.added_fast = []
 
-    def add(self, offsets, stream=None):
-        """Adds the electrons (offsets as MultiE.add) in batches of max_batch, each after the check.
-        `stream`: a CUDA stream handle; the checks' reductions run on it too."""
+    def _ctx(self, stream):
         import contextlib
-        from .multie import offset_array
         torch = self.torch
-        off = offset_array(offsets)
-        ctx = torch.cuda.stream(torch.cuda.ExternalStream(stream, device=self.dev)) if stream else \
+        return torch.cuda.stream(torch.cuda.ExternalStream(stream, device=self.dev)) if stream else \
             contextlib.nullcontext()
-        with ctx:
+
+    def add(self, offsets, stream=None):
+        """Adds the electrons (offsets as MultiE.add) in batches of max_batch, each with its check.
+        `stream`: a CUDA stream handle; the checks' reductions run on it too."""
+        from .multie import offset_array
+        off = offset_array(offsets)
+        with self._ctx(stream):
             for i0 in range(0, len(off), self.max_batch):
                 b = off[i0:i0 + self.max_batch]
+                if self.learned and not self.fell_back:
+                    self._resolve(stream)
                 if self.learned and not self.fell_back:
                     self.cfast.add(b[:1], stream)
                     self.csafe.add(b[:1], stream)
                     self.n_check += 1
-                    e = rel_err(self.chk[0], self.chk[1])
-                    self.check_errors.append(e)
-                    if e > self.tol:
-                        self._fall_back(stream)
-                if self.learned and not self.fell_back:
+                    self._queue_check()
                     self.fast.add(b, stream)
                     self.added_fast.append(b)
                 else:
@@ -760,11 +822,17 @@ class CheckedMultiE(object):
                 self.batches += 1
                 self.n += len(b)
 
+    def resolve(self, stream=None):
+        """Reads the last queued check (falling back if it fails); mean() calls it."""
+        with self._ctx(stream):
+            self._resolve(stream)
+
     @property
     def fallbacks(self):
         return int(self.fell_back)
 
-    def mean(self):
+    def mean(self, stream=None):
+        self.resolve(stream)
         self.torch.cuda.synchronize(self.dev)
         return (self.acc / max(self.n, 1)).cpu().numpy()
 

@@ -203,9 +203,11 @@ def test_trained_model_gain_over_conservative_factors():
 @pytest.mark.gpu
 def test_checked_multie_falls_back_and_rebuilds():
     """learned.CheckedMultiE: a check that every batch meets gives the learned factors' mean
-    intensity; a check that fails before the first batch gives the conservative factors' mean; a
-    check that fails after two batches propagates those two again with the conservative factors, so
-    the result is again the conservative factors' mean of all electrons (same batches, FP64 sums)."""
+    intensity, its errors those of the check set's two mean intensities; a check that fails at the
+    first batch gives the conservative factors' mean (the first batch, checked while it ran, is
+    propagated again); a check that fails after two batches propagates those two again with the
+    conservative factors, so the result is again the conservative factors' mean of all electrons
+    (same batches, FP64 sums)."""
     torch = _torch()
     from srw_b200 import srwlib as mod
     from srw_b200.multie import MultiE, sample_offsets
@@ -229,21 +231,20 @@ def test_checked_multie_falls_back_and_rebuilds():
     kw = dict(max_batch=8, safe_batch=8, graph=False, device=0, check_offsets=chk)
     ok = learned.CheckedMultiE(w, mk, fac, acc, tol=1.0, **kw)
     ok.add(offs)
-    assert not ok.fell_back and ok.n_check == 4 + 3 and len(ok.check_errors) == 3
     np.testing.assert_allclose(ok.mean(), m_fast, rtol=1e-12, atol=0)
-    # the check errors are those of the two mean intensities of the check set
+    assert not ok.fell_back and ok.n_check == 4 + 3 and len(ok.check_errors) == 3
     Ia = learned.mean_intensity(case, fac, np.vstack([chk, offs[0:1], offs[8:9], offs[16:17]]), acc, dev)
     Ib = learned.mean_intensity(case, learned.CONSERVATIVE, np.vstack([chk, offs[0:1], offs[8:9], offs[16:17]]), acc,
                                 dev)
     assert abs(ok.check_errors[-1] - learned.rel_err(Ia, Ib)) <= 1e-9 * max(1e-12, learned.rel_err(Ia, Ib))
     first = learned.CheckedMultiE(w, mk, fac, acc, tol=-1.0, **kw)
     first.add(offs)
-    assert first.fell_back and first.rerun == 0 and len(first.check_errors) == 1
     np.testing.assert_allclose(first.mean(), m_cons, rtol=1e-12, atol=0)
+    assert first.fell_back and first.rerun == 8 and len(first.check_errors) == 1
     late = learned.CheckedMultiE(w, mk, fac, acc, tol=1.0, **kw)
     late.add(offs[:16])
     late.tol = -1.0
     late.add(offs[16:])
-    assert late.fell_back and late.rerun == 16
     np.testing.assert_allclose(late.mean(), m_cons, rtol=1e-12, atol=0)
+    assert late.fell_back and late.rerun == 16
     assert np.linalg.norm(m_fast - m_cons) > 0

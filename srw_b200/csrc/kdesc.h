@@ -90,7 +90,9 @@ struct LineDesc {
     PwOps extra;
     int zwin;                       // the input is zero outside lines [zl0, zl1] x along [za0, za1]
     int zl0, zl1, za0, za1;         //   (the output window of the resize that produced it)
-    int blk_out;                    // row pass: output in blocks of blk_out columns (0: row-major)
+    int blk_out;                    // row pass: output in blocks of blk_out columns (0: row-major);
+                                    //   column intensity pass (out_int): the intensity of column c at
+                                    //   point i at ((c / blk_out) N + i) blk_out + c % blk_out
     int blk_in;                     // column pass: input in blocks of blk_in columns (0: row-major)
     int out_int;                    // last pass of a multi-electron batch on a specialised kernel: one
                                     //   CTA transforms both components of its lines and writes the

@@ -445,6 +445,12 @@ __device__ __forceinline__ bool linen_body(const LineLaunch& p, int comp, IAcc<N
         x.om.bstr = nl * d.blk_out;
         obase = (size_t)oline * d.blk_out;
     }
+    if (COLS && OUTI && d.blk_out > 0) {
+        // the intensity in blocks of blk_out columns: a tile of blk_out columns writes one
+        // contiguous piece
+        x.om.str = d.blk_out;
+        obase = (size_t)(oline / d.blk_out) * N * d.blk_out + (oline % d.blk_out);
+    }
     x.gout = OUTI ? reinterpret_cast<float2*>(fdst + obase) : dst + obase;
     x.za0 = 0;
     x.za1 = N - 1;

@@ -80,12 +80,13 @@ __global__ void __launch_bounds__(256) accum_kernel(const float2* __restrict__ e
     acc[(size_t)j * anx + i] += sum;
 }
 
-// the same with the intensities written by the last pass (an intensity pass, float [onz][onx] per
-// electron at stride `stride` floats)
+// the same with the intensities written by the last pass (an intensity pass, float per point of the
+// electron's onz x onx mesh at stride `stride` floats): row-major (bw 0) or in blocks of bw columns
+// (point (ix, iy) at ((ix / bw) onz + iy) bw + ix % bw)
 __global__ void __launch_bounds__(256) accum_int_kernel(const float* __restrict__ in, long long stride, int nb,
                                                         const ElecParams* __restrict__ ep, double* __restrict__ acc,
                                                         int anx, int anz, double axStart, double axStep,
-                                                        double azStart, double azStep)
+                                                        double azStart, double azStep, int bw)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
@@ -100,8 +101,17 @@ __global__ void __launch_bounds__(256) accum_int_kernel(const float* __restrict_
         if (iy0 < 0 || iy0 >= e.onz - 1) continue;
         const double tx = (x - (e.oxStart + e.oxStep * ix0)) / e.oxStep;
         const double ty = (y - (e.ozStart + e.ozStep * iy0)) / e.ozStep;
-        const float* pi = in + (size_t)b * stride + (size_t)iy0 * e.onx + ix0;
-        const double a00 = __ldg(&pi[0]), f10 = __ldg(&pi[1]), f01 = __ldg(&pi[e.onx]), f11 = __ldg(&pi[e.onx + 1]);
+        const float* pe = in + (size_t)b * stride;
+        double a00, f10, f01, f11;
+        if (bw > 0) {
+            const size_t c0 = ((size_t)(ix0 / bw) * e.onz + iy0) * bw + ix0 % bw;
+            const size_t c1 = ((size_t)((ix0 + 1) / bw) * e.onz + iy0) * bw + (ix0 + 1) % bw;
+            a00 = __ldg(&pe[c0]); f01 = __ldg(&pe[c0 + bw]);
+            f10 = __ldg(&pe[c1]); f11 = __ldg(&pe[c1 + bw]);
+        } else {
+            const float* pi = pe + (size_t)iy0 * e.onx + ix0;
+            a00 = __ldg(&pi[0]); f10 = __ldg(&pi[1]); f01 = __ldg(&pi[e.onx]); f11 = __ldg(&pi[e.onx + 1]);
+        }
         const double a10 = f10 - a00, a01 = f01 - a00, a11 = a00 - f01 - f10 + f11;
         sum += a00 + tx * (a10 + ty * a11) + ty * a01;
     }
@@ -118,16 +128,26 @@ static void mark_intensity_pass(std::vector<KernelDesc>& ks)
         LineDesc& d = ks[i].line;
         if (ks[i].kind == K_LINE && !d.has_extra && !(d.f1 && d.f2)) {
             const int N = d.axis == 0 ? d.nx : d.nz;
-            if (fixed_family(d.axis, N) == FAM_SPEC) d.out_int = 1;
+            if (fixed_family(d.axis, N) == FAM_SPEC) {
+                d.out_int = 1;
+                // a column pass writes the intensity in blocks of its tile's columns (contiguous
+                // pieces); the accumulation reads that layout
+                const int bw = fixed_lines_per_cta(1, N);
+                if (d.axis == 1 && d.blk_out == 0 && bw > 1 && d.nx % bw == 0) d.blk_out = bw;
+            }
         }
         return;
     }
 }
 
-static bool intensity_pass(const std::vector<KernelDesc>& ks)
+static bool intensity_pass(const std::vector<KernelDesc>& ks, int* bw = nullptr)
 {
     for (size_t i = ks.size(); i-- > 0;)
-        if (!reads_only(ks[i].kind)) return ks[i].kind == K_LINE && ks[i].line.out_int;
+        if (!reads_only(ks[i].kind)) {
+            const bool yes = ks[i].kind == K_LINE && ks[i].line.out_int;
+            if (bw) *bw = yes && ks[i].line.axis == 1 ? ks[i].line.blk_out : 0;
+            return yes;
+        }
     return false;
 }
 
@@ -266,9 +286,10 @@ static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, c
     if (r) return r;
     dim3 ga((m.anx + 255) / 256, m.anz);
     if (ev) MTRY(cudaEventRecord(ev[2 * ks.size()], st));
-    if (intensity_pass(ks))
+    int bw = 0;
+    if (intensity_pass(ks, &bw))
         accum_int_kernel<<<ga, blk, 0, st>>>(reinterpret_cast<const float*>(outX), (long long)m.nOut, nb, m.dParams,
-                                             m.dAcc, m.anx, m.anz, m.axStart, m.axStep, m.azStart, m.azStep);
+                                             m.dAcc, m.anx, m.anz, m.axStart, m.axStep, m.azStart, m.azStep, bw);
     else
         accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams, m.dAcc, m.anx, m.anz,
                                          m.axStart, m.axStep, m.azStart, m.azStep);

@@ -672,7 +672,22 @@ def measure_learned(args, dev, world, dist, acc):
         torch.cuda.synchronize(dev)
     total_ms = _max_over_ranks(e0.elapsed_time(e1), dev, world, dist)
     value = world * args.steps * LEARNED_BATCH / (total_ms / 1000.)
-    ce = cm.check_errors
+    ce = list(cm.check_errors)
+    fell_back, rerun, n_check = cm.fell_back, cm.rerun, cm.n_check
+    # end to end through the public API: host offsets in, the mean intensity (host) out, every step
+    e2e = None
+    if not args.no_e2e:
+        n_e2e = max(3, min(args.steps, 10))
+        t0 = time.perf_counter()
+        for k in range(n_e2e):
+            cm.add(offs[k % len(offs)])
+            mean = cm.mean()
+        e2e_s = time.perf_counter() - t0
+        e2e = {"value": world * n_e2e * LEARNED_BATCH / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(offs[0].nbytes), "d2h_bytes_per_step": int(mean.nbytes),
+               "path": "srw_b200.learned.CheckedMultiE.add (C-ABI srwgMultiEAdd; base field resident, electron "
+                       "offsets from host, the run-time check included) + CheckedMultiE.mean (D2H of the %dx%d FP64 "
+                       "mean intensity)" % (acc['nx'], acc['ny'])}
     peak, peak_src = hbm_peak()
     passes = batched_passes(cm.safe if cm.fell_back else cm.fast, offs[0], stream.cuda_stream, peak, peak_src,
                             "learned leg, one batch of %d electrons, CUDA events per pass" % LEARNED_BATCH)
@@ -684,20 +699,20 @@ def measure_learned(args, dev, world, dist, acc):
             # checked electron with the conservative factors
             "launches_per_step": 2 * (nk_f + 2) + (nk_c + 2),
             "factors": list(factors), "configured_factors": list(CONFIGURED),
-            "fallback": bool(fallback or cm.fell_back),
+            "fallback": bool(fallback or fell_back),
             "choice_check_rel_err": chk, "choose_seconds": choose_s,
             "choice_trace": [[list(f), e] for f, e in trace],
             "choice_check": "mean intensity of %d electrons (seeded check set) on the detector mesh, candidate vs "
                             "conservative factors, relative L2 where the conservative one exceeds 1e-3 of its "
                             "maximum; tolerance %g" % (N_CHECK, learned.TOL_LABEL),
-            "run_checks": {"batches": len(ce), "fell_back": bool(cm.fell_back), "rerun_electrons": cm.rerun,
-                           "check_electrons": cm.n_check, "max_rel_err": max(ce) if ce else None,
+            "run_checks": {"batches": len(ce), "fell_back": bool(fell_back), "rerun_electrons": rerun,
+                           "check_electrons": n_check, "max_rel_err": max(ce) if ce else None,
                            "last_rel_err": ce[-1] if ce else None,
                            "what": "before every batch: the check set (the choice's electrons plus the first "
                                    "electron of every batch so far) at both factors, relative L2 of the two mean "
                                    "intensities; above the tolerance the run falls back to the conservative factors "
                                    "for good and propagates the learned batches again"},
-            "clocks": nv.summary(), "passes": passes,
+            "clocks": nv.summary(), "passes": passes, "e2e": e2e,
             "model": {k: v for k, v in getattr(model, 'meta', {}).items()
                       if k in ('samples', 'val_grid_at_least_label', 'val_cost_pred', 'labels_conservative', 'tol')}}
 
@@ -880,7 +895,8 @@ def run_ours(args, rank, world):
            "rel_err_vs_fp64_oracle": (orc or {}).get('rel_err_learned_vs_fp64_oracle' if use_learned else
                                                      'rel_err_configured_vs_fp64_oracle'),
            "oracle_comparison": orc,
-           "e2e": bt['e2e'],
+           "e2e": (ln['e2e'] if use_learned and ln.get('e2e') else bt['e2e']),
+           "e2e_batched_configured": bt['e2e'],
            "e2e_single_wavefront": e2e_single,
            "mixed_grid_multi_electron": mixed,
            "clocks": (ln['clocks'] if use_learned and ln.get('clocks') else bt['clocks']),

@@ -90,6 +90,8 @@ struct LineDesc {
     PwOps extra;
     int zwin;                       // the input is zero outside lines [zl0, zl1] x along [za0, za1]
     int zl0, zl1, za0, za1;         //   (the output window of the resize that produced it)
+    int zskip;                      // with zwin: the (zero) lines outside [zl0, zl1] are not written,
+                                    //   the next pass loads only those lines' window
     int blk_out;                    // row pass: output in blocks of blk_out columns (0: row-major);
                                     //   column intensity pass (out_int): the intensity of column c at
                                     //   point i at ((c / blk_out) N + i) blk_out + c % blk_out

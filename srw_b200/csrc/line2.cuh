@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     const int g = COLS ? (tid % L) : (tid / T);          // line of the tile
     const int t = COLS ? (tid / L) : (tid - g * T);      // thread within the line
     const int line = blockIdx.x * L + g;
-    const bool active = line < nl;
+    bool active = line < nl;
     float2* s = sm + (size_t)g * P;
     // input: row-major, or (column pass after a row pass) blocks of blk_in columns stored together
     int gstr = COLS ? nl : 1;
@@ -172,14 +172,20 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     if (d.zwin) {
         const int l0 = blockIdx.x * L, l1 = min(l0 + L, nl) - 1;
         if (l1 < d.zl0 || l0 > d.zl1) {
-            if (active) {
+            if (active && !d.zskip) {
 #pragma unroll
                 for (int m = 0; m < 16; m++) __stcs(&gout[om.at(t + T * m)], make_float2(0.f, 0.f));
             }
             return;
         }
-        if (line < d.zl0 || line > d.zl1) { za0 = 1; za1 = 0; }
-        else { za0 = d.za0; za1 = d.za1; }
+        if (line < d.zl0 || line > d.zl1) {
+            za0 = 1;
+            za1 = 0;
+            if (d.zskip) active = false;        // a zero line that nothing reads
+        } else {
+            za0 = d.za0;
+            za1 = d.za1;
+        }
     }
     const float2* tabs = p.tabs + blockIdx.z * p.bTab;
     const PwOps* ex = &d.extra;

@@ -458,14 +458,20 @@ __device__ __forceinline__ bool linen_body(const LineLaunch& p, int comp, IAcc<N
         const int l0 = blockIdx.x * L, l1 = min(l0 + L, nl) - 1;
         if (l1 < d.zl0 || l0 > d.zl1) {
             // the whole tile is zero: so is its transform
-            if (x.store && OUTI == 0)
+            if (x.store && OUTI == 0 && !d.zskip)
                 for (int m = t; m < N; m += T) __stcs(&x.gout[x.om.at(m)], make_float2(0.f, 0.f));
             if (x.store && OUTI == 2)
                 for (int m = t; m < N; m += T) __stcs(reinterpret_cast<float*>(x.gout) + x.om.at(m), 0.f);
             return true;
         }
-        if (line < d.zl0 || line > d.zl1) { x.za0 = 1; x.za1 = 0; }
-        else { x.za0 = d.za0; x.za1 = d.za1; }
+        if (line < d.zl0 || line > d.zl1) {
+            x.za0 = 1;
+            x.za1 = 0;
+            if (d.zskip && OUTI == 0) x.store = false;      // a zero line that nothing reads
+        } else {
+            x.za0 = d.za0;
+            x.za1 = d.za1;
+        }
     }
     x.tabs = p.tabs + blockIdx.z * p.bTab;
     x.ex = &d.extra;

@@ -1836,8 +1836,9 @@ int Planner::finalize()
         a.line.blk_out = bw;
         n.line.blk_in = bw;
     }
-    // a row pass that transforms only the rows of a resize window writes zeros in the other rows;
-    // the column pass on its output then skips loading them (the same window along its lines)
+    // a row pass that transforms only the rows of a resize window: the column pass on its output
+    // loads only those rows of every column (the same window along its lines), so the row pass does
+    // not write the other (zero) rows at all
     for (size_t i = 0; i + 1 < kernels.size(); i++) {
         KernelDesc& a = kernels[i];
         KernelDesc& n = kernels[i + 1];
@@ -1853,6 +1854,7 @@ int Planner::finalize()
         d.zl1 = n.line.nx - 1;
         d.za0 = a.line.mirror_lines ? nz - 1 - a.line.zl1 : a.line.zl0;
         d.za1 = a.line.mirror_lines ? nz - 1 - a.line.zl0 : a.line.zl1;
+        a.line.zskip = 1;
     }
     return 0;
 }

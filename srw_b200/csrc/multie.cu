@@ -177,31 +177,38 @@ struct srwgMultiE {
     size_t nIn = 0, nOut = 0, perWork = 0, constStride = 0, descOff = 0;
     float2* dOut = nullptr;              // [2][B][nOut]
     float2* dWork = nullptr;             // [4][B][perWork]
-    char* dConst = nullptr;              // [B][constStride]
-    ElecParams* dParams = nullptr;       // [B]
-    char* hConst[2] = {nullptr, nullptr};          // pinned staging, two slots used in turn
+    // per-electron constants (tables, descriptors) and parameters in two slots used in turn: the
+    // host stages batch k+1 in pinned memory and a copy stream uploads it while batch k runs
+    char* dConst[2] = {nullptr, nullptr};          // [B][constStride] per slot
+    ElecParams* dParams[2] = {nullptr, nullptr};   // [B] per slot
+    char* hConst[2] = {nullptr, nullptr};          // pinned staging
     ElecParams* hParams[2] = {nullptr, nullptr};
     cudaEvent_t staged[2] = {nullptr, nullptr};    // the slot's upload has completed
+    cudaEvent_t used[2] = {nullptr, nullptr};      // the last batch that read the slot has completed
+    cudaStream_t copy = nullptr;                   // upload stream
     int slot = 0;
     bool useGraph = false;
-    cudaGraphExec_t graph = nullptr;
-    int graphNb = 0;
-    std::vector<KernelDesc> graphKs;     // host copy (launch shapes) the graph was captured with
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // per slot
+    std::vector<KernelDesc> graphKs[2];  // host copy (launch shapes) each graph was captured with
     std::vector<cudaEvent_t> tev;        // srwgMultiEAddTimed: events around every pass and the accumulation
     long long nFlush = 0;                // batches run so far
     ~srwgMultiE()
     {
         for (cudaEvent_t e : tev) cudaEventDestroy(e);
-        if (graph) cudaGraphExecDestroy(graph);
+        for (int i = 0; i < 2; i++)
+            if (graph[i]) cudaGraphExecDestroy(graph[i]);
         if (ownAcc) cudaFree(dAcc);
         cudaFree(dSnap);
-        cudaFree(dBase); cudaFree(dOut); cudaFree(dWork); cudaFree(dConst);
-        cudaFree(dParams);
+        cudaFree(dBase); cudaFree(dOut); cudaFree(dWork);
         for (int i = 0; i < 2; i++) {
+            cudaFree(dConst[i]);
+            cudaFree(dParams[i]);
             cudaFreeHost(hConst[i]);
             cudaFreeHost(hParams[i]);
             if (staged[i]) cudaEventDestroy(staged[i]);
+            if (used[i]) cudaEventDestroy(used[i]);
         }
+        if (copy) cudaStreamDestroy(copy);
     }
 };
 
@@ -273,7 +280,7 @@ static bool same_structure(const std::vector<KernelDesc>& a, const std::vector<K
 
 // runs one batch: passes (the first one applies each electron's kick) -> accumulation; ks = launch
 // shapes (largest resize tiles of the batch)
-static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, cudaStream_t st)
+static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, cudaStream_t st, int slot)
 {
     dim3 blk(256);
     float2* outX = m.dOut;
@@ -282,42 +289,45 @@ static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, c
     // every electron's first pass reads the base field (input stride 0) and applies its kick
     cudaEvent_t* ev = m.tev.size() >= 2 * ks.size() + 2 ? m.tev.data() : nullptr;
     int r = execute_passes(ks, *m.ctx, nb, m.dBase, m.dBase + m.nIn, 0, outX, outY, (long long)m.nOut, m.dWork,
-                           m.perWork, m.dConst, (long long)m.constStride, m.descOff, st, ev, &ks);
+                           m.perWork, m.dConst[slot], (long long)m.constStride, m.descOff, st, ev, &ks);
     if (r) return r;
     dim3 ga((m.anx + 255) / 256, m.anz);
     if (ev) MTRY(cudaEventRecord(ev[2 * ks.size()], st));
     int bw = 0;
     if (intensity_pass(ks, &bw))
-        accum_int_kernel<<<ga, blk, 0, st>>>(reinterpret_cast<const float*>(outX), (long long)m.nOut, nb, m.dParams,
+        accum_int_kernel<<<ga, blk, 0, st>>>(reinterpret_cast<const float*>(outX), (long long)m.nOut, nb, m.dParams[slot],
                                              m.dAcc, m.anx, m.anz, m.axStart, m.axStep, m.azStart, m.azStep, bw);
     else
-        accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams, m.dAcc, m.anx, m.anz,
+        accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams[slot], m.dAcc, m.anx, m.anz,
                                          m.axStart, m.axStep, m.azStart, m.azStep);
     MTRY(cudaGetLastError());
     if (ev) MTRY(cudaEventRecord(ev[2 * ks.size() + 1], st));
     return 0;
 }
 
-// uploads the staged constants of nb electrons and runs (or replays) the batch
+// uploads the staged constants of nb electrons (copy stream, after the last batch that read the slot)
+// and runs (or replays) the batch on `st` once the upload has landed; the host then stages the next
+// batch in the other slot, once that slot's previous upload has completed
 static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_t st)
 {
     if (nb == 0) return 0;
     m.nFlush++;
-    MTRY(cudaMemcpyAsync(m.dConst, m.hConst[m.slot], (size_t)nb * m.constStride, cudaMemcpyHostToDevice, st));
-    MTRY(cudaMemcpyAsync(m.dParams, m.hParams[m.slot], (size_t)nb * sizeof(ElecParams), cudaMemcpyHostToDevice, st));
-    MTRY(cudaEventRecord(m.staged[m.slot], st));
-    m.slot ^= 1;
-    // the next batch is staged in the other slot once that slot's previous upload has completed
-    MTRY(cudaEventSynchronize(m.staged[m.slot]));
+    const int s = m.slot;
+    MTRY(cudaStreamWaitEvent(m.copy, m.used[s], 0));
+    MTRY(cudaMemcpyAsync(m.dConst[s], m.hConst[s], (size_t)nb * m.constStride, cudaMemcpyHostToDevice, m.copy));
+    MTRY(cudaMemcpyAsync(m.dParams[s], m.hParams[s], (size_t)nb * sizeof(ElecParams), cudaMemcpyHostToDevice, m.copy));
+    MTRY(cudaEventRecord(m.staged[s], m.copy));
+    MTRY(cudaStreamWaitEvent(st, m.staged[s], 0));
     int r = 0;
     if (m.useGraph && nb == m.maxBatch && m.tev.empty()) {
         // the graph holds the launch shapes; a batch whose resize tiles are larger needs a new one
-        bool fits = m.graph != nullptr && m.graphKs.size() == ks.size();
+        bool fits = m.graph[s] != nullptr && m.graphKs[s].size() == ks.size();
         for (size_t i = 0; fits && i < ks.size(); i++)
-            if (ks[i].kind == K_RESIZE && (ks[i].rs.tile_or > m.graphKs[i].rs.tile_or || ks[i].rs.tile_oc > m.graphKs[i].rs.tile_oc))
+            if (ks[i].kind == K_RESIZE &&
+                (ks[i].rs.tile_or > m.graphKs[s][i].rs.tile_or || ks[i].rs.tile_oc > m.graphKs[s][i].rs.tile_oc))
                 fits = false;
         if (!fits) {
-            if (m.graph) { cudaGraphExecDestroy(m.graph); m.graph = nullptr; }
+            if (m.graph[s]) { cudaGraphExecDestroy(m.graph[s]); m.graph[s] = nullptr; }
             std::vector<KernelDesc> cap = ks;
             for (size_t i = 0; i < cap.size(); i++)
                 if (cap[i].kind == K_RESIZE && cap[i].rs.tile_or > 0) {     // headroom for other batches
@@ -326,26 +336,28 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
                 }
             // this batch runs directly (which also creates every lazily made resource -- twiddle
             // tables, kernel attributes -- before the capture); the capture only records the launches
-            r = run_batch(m, nb, cap, st);
+            r = run_batch(m, nb, cap, st, s);
             if (r) return r;
             cudaGraph_t g;
             MTRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            r = run_batch(m, nb, cap, st);
+            r = run_batch(m, nb, cap, st, s);
             cudaError_t e = cudaStreamEndCapture(st, &g);
             if (r) return r;
             MTRY(e);
-            MTRY(cudaGraphInstantiate(&m.graph, g, 0));
+            MTRY(cudaGraphInstantiate(&m.graph[s], g, 0));
             cudaGraphDestroy(g);
-            m.graphKs = cap;
-            m.nAdded += nb;
-            return 0;
+            m.graphKs[s] = cap;
+        } else {
+            MTRY(cudaGraphLaunch(m.graph[s], st));
         }
-        MTRY(cudaGraphLaunch(m.graph, st));
     } else {
-        r = run_batch(m, nb, ks, st);
+        r = run_batch(m, nb, ks, st, s);
         if (r) return r;
     }
+    MTRY(cudaEventRecord(m.used[s], st));
     m.nAdded += nb;
+    m.slot ^= 1;
+    MTRY(cudaEventSynchronize(m.staged[m.slot]));
     return 0;
 }
 
@@ -412,20 +424,29 @@ extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* p
     MALLOC(m->dBase, 2 * m->nIn * sizeof(float2));
     MALLOC(m->dOut, 2 * B * m->nOut * sizeof(float2));
     MALLOC(m->dWork, 4 * B * m->perWork * sizeof(float2));
-    MALLOC(m->dConst, B * m->constStride);
-    MALLOC(m->dParams, B * sizeof(ElecParams));
+    for (int i = 0; i < 2; i++) {
+        MALLOC(m->dConst[i], B * m->constStride);
+        MALLOC(m->dParams[i], B * sizeof(ElecParams));
+    }
     MALLOC(m->dAcc, (size_t)m->anx * m->anz * sizeof(double));
     MALLOC(m->dSnap, (size_t)m->anx * m->anz * sizeof(double));
 #undef MALLOC
     for (int i = 0; i < 2; i++) {
         if (cudaMallocHost(&m->hConst[i], B * m->constStride) != cudaSuccess ||
             cudaMallocHost(&m->hParams[i], B * sizeof(ElecParams)) != cudaSuccess ||
-            cudaEventCreateWithFlags(&m->staged[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&m->staged[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&m->used[i], cudaEventDisableTiming) != cudaSuccess) {
             set_last_detail("pinned staging buffers could not be allocated");
             delete m;
             return MEMORY_ALLOCATION_FAILURE;
         }
         cudaEventRecord(m->staged[i], 0);
+        cudaEventRecord(m->used[i], 0);
+    }
+    if (cudaStreamCreateWithFlags(&m->copy, cudaStreamNonBlocking) != cudaSuccess) {
+        set_last_detail("upload stream could not be created");
+        delete m;
+        return SRWG_ERR_CUDA;
     }
     if (cudaMemcpy(m->dBase, pBase->arEx, m->nIn * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(m->dBase + m->nIn, pBase->arEy, m->nIn * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -662,6 +683,12 @@ extern "C" SRWG_API int srwgMultiESetAccumulator(srwgMultiE* m, double* dAcc)
     cudaFree(m->dAcc);
     m->dAcc = dAcc;
     m->ownAcc = false;
+    for (int i = 0; i < 2; i++)              // captured launches name the old accumulator
+        if (m->graph[i]) {
+            cudaGraphExecDestroy(m->graph[i]);
+            m->graph[i] = nullptr;
+            m->graphKs[i].clear();
+        }
     return 0;
 }
 

@@ -93,6 +93,28 @@ def test_full_size_c1_plan():
     assert 'pre=1' in p.describe() and 'tile=' in p.describe()
 
 
+def test_aperture_bounds_the_resize_window():
+    """The undulator beamline's circular aperture (0.8 mm, folded into the resize before the lens)
+    bounds the resize window: the new points whose 4-point stencils reach the aperture's box (its
+    radius in old steps, widened by 2 nodes against coordinate rounding, plus the stencil), not the
+    whole old range; the row pass transforms only those rows and does not write the others, and the
+    column pass loads only that window of every column."""
+    import re
+    ex, ey, mesh = gaussian(1024, E=2000., sig=0.4e-3, r=1.5e-3)
+    w = make_wfr(ex, ey, mesh, Rx=20., Ry=20., dRx=0.2, dRy=0.2)
+    d = Plan(w, beamline(C1, C1PP)).describe().splitlines()
+    x0, x1, z0, z1 = map(int, re.search(r'window=x(\d+):(\d+),z(\d+):(\d+)', d[0]).groups())
+    step_old, step_new = 3e-3 / 1023, 6e-3 / 4095          # range x2, resolution x2
+    r = 0.4e-3
+    half_old = int(np.ceil(r / step_old)) + 2 + 1             # aperture box half-width in old nodes (+ margin)
+    half_new = (half_old + 2) * step_old / step_new           # ... and the stencil reach, in new steps
+    assert (x0, x1) == (z0, z1)
+    assert abs((x1 - x0) / 2. - half_new) < 4 and x1 - x0 < 4096 // 4
+    assert abs((x0 + x1) / 2. - 2047.5) <= 1.
+    assert 'lines=%d:%d points=%d:%d' % (z0, z1, x0, x1) in d[1]
+    assert 'lines=0:4095 points=%d:%d' % (z0, z1) in d[2]
+
+
 def test_unsupported_and_invalid_inputs_raise():
     ex, ey, mesh = gaussian(64)
     w = make_wfr(ex, ey, mesh)

@@ -562,9 +562,32 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
     std::vector<Planner> pls(group);
     std::vector<ElecParams> eps(group);
     std::vector<int> rcs(group);
+    // the electrons' tables and descriptors are copied into the pinned staging slot by the host
+    // threads too (≈130 KB per electron at 1536 x 1600: one thread would take about as long as the
+    // GPU takes for the batch): (electron of the group, position in the batch), copied before the
+    // batch is flushed or the group is planned again
+    std::vector<std::pair<int, int>> pending;
+    auto copy_pending = [&]() {
+        if (pending.empty()) return;
+        char* base = m->hConst[m->slot];
+        auto cp = [&](int t0) {
+            for (size_t i = t0; i < pending.size(); i += nthr) {
+                const Planner& q = pls[pending[i].first];
+                char* blk = base + (size_t)pending[i].second * m->constStride;
+                memcpy(blk, q.tables.data(), q.tables.size() * sizeof(float2));
+                memcpy(blk + m->descOff, q.kernels.data(), q.kernels.size() * sizeof(KernelDesc));
+            }
+        };
+        std::vector<std::thread> th;
+        for (int t = 1; t < std::min(nthr, (int)pending.size()); t++) th.emplace_back(cp, t);
+        cp(0);
+        for (auto& t : th) t.join();
+        pending.clear();
+    };
     for (int e = 0; e < n; e++) {
         const int g = e % group;
         if (g == 0) {
+            copy_pending();
             const int cnt = std::min(group, n - e);
             auto work = [&](int t0) {
                 double momX[11], momY[11];
@@ -599,6 +622,7 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
             return SRWG_ERR_UNSUPPORTED;
         }
         if (nb > 0 && (!same_structure(first, pl.kernels) || nb == m->maxBatch)) {
+            copy_pending();
             r = flush(*m, nb, launchKs, st);
             if (r) return r;
             nb = 0;
@@ -609,9 +633,7 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
                 launchKs[i].rs.tile_or = std::max(launchKs[i].rs.tile_or, pl.kernels[i].rs.tile_or);
                 launchKs[i].rs.tile_oc = std::max(launchKs[i].rs.tile_oc, pl.kernels[i].rs.tile_oc);
             }
-        char* blk = m->hConst[m->slot] + (size_t)nb * m->constStride;
-        memcpy(blk, pl.tables.data(), tb);
-        memcpy(blk + m->descOff, pl.kernels.data(), pl.kernels.size() * sizeof(KernelDesc));
+        pending.emplace_back(g, nb);
         // output mesh as the reference's SRWLWfr holds it, step re-derived from (Fin - Start)/(n - 1)
         const double xFin = pl.w.xStart + pl.w.xStep * (pl.w.nx - 1);
         const double zFin = pl.w.zStart + pl.w.zStep * (pl.w.nz - 1);
@@ -624,6 +646,7 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
         m->hParams[m->slot][nb] = ep;
         nb++;
     }
+    copy_pending();
     return flush(*m, nb, launchKs, st);
 }
 

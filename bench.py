@@ -48,11 +48,16 @@ BATCH = 16                                     # macro-electron wavefronts per s
 SIG = (30e-6, 5e-6, 5e-6, 2e-6)                # source: sigma x [m], x' [rad], y [m], y' [rad]
 SIG_E = 1e-3                                   # relative electron energy spread (photon energy E (1 + 2 d))
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a pass, from an ncu
-# capture of this workload (profiles/passes_4096_c1.md); keyed by the pass tuple of Plan.kernels().
-# Re-captured whenever the kernel changes.
-TRAFFIC = {('line_cols', 4096, 4096): 134334464 + 219883776,
-           ('line_rows', 4096, 4096): 67189504 + 216088320,
-           ('resize', 1024, 1024, 4096, 4096): 16922624 + 15437824}
+# capture of this workload (the plain passes' summary under profiles/); keyed by the pass tuple of
+# Plan.kernels().  Re-captured whenever the kernel changes.
+TRAFFIC = {('line_cols', 4096, 4096): 37370624 + 216581888,
+           ('line_rows', 4096, 4096): 5258752 + 2208256,
+           ('resize', 1024, 1024, 4096, 4096): 1377024 + 0}
+# the same per electron of the batched passes at the learned factors (ncu on a batch of 8, the
+# learned batch's summary under profiles/); a launch moves this times its electrons
+TRAFFIC_PER_ELECTRON = {('line_cols', 1536, 1600): (70055936 + 28697856) // 8,
+                        ('line_rows', 1536, 1600): (19816704 + 22441472) // 8,
+                        ('resize', 1024, 1024, 1536, 1600): (2240512 + 27136) // 8}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -378,7 +383,8 @@ def batched_passes(me, offs, stream, peak, peak_src, where):
     achieved = alg[kd] * nb / (per[kd] / 1000.) / 1e9
     return {"bound": "hbm", "kernel": "%s %s (batch of %d)" % (ks[kd][0], 'x'.join(map(str, ks[kd][1:])), nb),
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-            "traffic": None, "algorithmic_bytes": alg[kd] * nb, "avg_ms": float(per[kd]),
+            "traffic": (TRAFFIC_PER_ELECTRON[tuple(ks[kd])] * nb if tuple(ks[kd]) in TRAFFIC_PER_ELECTRON else None),
+            "algorithmic_bytes": alg[kd] * nb, "avg_ms": float(per[kd]),
             "per_pass_ms": [round(float(v), 4) for v in per], "accumulation_ms": round(float(ms[-1]), 4),
             "per_electron_ms": round(float(sum(ms)) / nb, 5), "passes": [list(k) for k in ks],
             "last_pass_writes_intensity": inten, "measured_on": where}

@@ -617,7 +617,7 @@ def measure_mixed(args, dev, n_elec, model=None):
     return out
 
 
-LEARNED_BATCH = 128              # macro-electron wavefronts per step of the learned leg (one checked batch)
+LEARNED_BATCH = 256              # macro-electron wavefronts per step of the learned leg (one checked batch)
 N_CHECK = 32                     # electrons of the learned factors' check set
 REFINE = 4                       # checks spent lowering the resolution of a passing choice
 

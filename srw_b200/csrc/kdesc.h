@@ -99,6 +99,9 @@ struct LineDesc {
     int out_int;                    // last pass of a multi-electron batch on a specialised kernel: one
                                     //   CTA transforms both components of its lines and writes the
                                     //   total intensity |Ex|^2 + |Ey|^2 (float, dst[0]) instead of them
+    int int_flat;                   // intensity pass whose output factors (the output chain's table,
+    float int_scale;                //   the line factors) have one magnitude everywhere: they are not
+                                    //   applied, the intensity is scaled by int_scale = that magnitude^2
 };
 
 struct ResizeDesc {

@@ -156,6 +156,7 @@ struct NLine {
     int za0, za1;           // input points outside [za0, za1] are zero
     const float2* sin;      // bulk-copied input tile: point k of the line at sin[k * sst]
     int sst;
+    float iscale;           // intensity passes: factor of the stored intensity
 };
 
 // padded shared-memory address of point p, and its separable form for a per-thread base plus a
@@ -373,7 +374,7 @@ __device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& 
                 } else if constexpr (OUTI == 1) {
                     acc->at(b, r) = o.x * o.x + o.y * o.y;           // first component
                 } else {
-                    const float I = acc->at(b, r) + o.x * o.x + o.y * o.y;
+                    const float I = (acc->at(b, r) + o.x * o.x + o.y * o.y) * x.iscale;
                     if (x.store) __stcs(reinterpret_cast<float*>(x.gout) + x.om.at(kk), I);
                 }
             }
@@ -525,6 +526,15 @@ __device__ __forceinline__ bool linen_body(const LineLaunch& p, int comp, IAcc<N
     fin.rs1 = d.f2 ? d.f2_post.rs : 0; fin.mir = 0; fin.rs2 = 0; fin.tab = (int)d.t_fin.tab; fin.extra = 0;
     x.has_lf = (d.t_pre.ltab >= 0) || (d.t_mid.ltab >= 0) || (d.t_fin.ltab >= 0);
     x.lf = make_float2(1.f, 0.f);
+    x.iscale = 1.f;
+    if (OUTI && d.int_flat) {
+        // the output factors have one magnitude: the intensity is scaled instead (the single
+        // transform's output chain is mid after f1, fin after f2)
+        if (d.f1) mid.tab = -1;
+        else fin.tab = -1;
+        x.has_lf = false;
+        x.iscale = d.int_scale;
+    }
     if (x.has_lf) {
         if (d.t_pre.ltab >= 0) x.lf = cmul(x.lf, __ldg(&x.tabs[d.t_pre.ltab + line]));
         if (d.t_mid.ltab >= 0) x.lf = cmul(x.lf, __ldg(&x.tabs[d.t_mid.ltab + line]));

@@ -118,22 +118,46 @@ __global__ void __launch_bounds__(256) accum_int_kernel(const float* __restrict_
     acc[(size_t)j * anx + i] += sum;
 }
 
+// magnitude^2 of the n complex values at float2 offset `off` of the plan's tables when all of them
+// have it (relative spread within 1e-6), else -1
+static double flat_mag2(const std::vector<float2>& T, long long off, int n)
+{
+    if (off < 0) return 1.;
+    if (n <= 0 || off + n > (long long)T.size()) return -1.;
+    double lo = 1e300, hi = 0.;
+    for (int i = 0; i < n; i++) {
+        const double a = (double)T[off + i].x * T[off + i].x + (double)T[off + i].y * T[off + i].y;
+        lo = std::min(lo, a);
+        hi = std::max(hi, a);
+    }
+    return (hi > 0. && hi - lo <= 1e-6 * hi) ? 0.5 * (lo + hi) : -1.;
+}
+
 // the last pass writes the total intensity instead of the two fields where it runs on a specialised
 // kernel with one transform and no non-separable work (the accumulation then reads one float per
-// sample instead of two complex values)
-static void mark_intensity_pass(std::vector<KernelDesc>& ks)
+// sample instead of two complex values).  Where its output factors -- the output chain's table along
+// the lines and every chain's line factor -- have one magnitude, |f v|^2 = |f|^2 |v|^2: the pass
+// skips them and scales the intensity by that magnitude squared.
+static void mark_intensity_pass(std::vector<KernelDesc>& ks, const std::vector<float2>& tables)
 {
     for (size_t i = ks.size(); i-- > 0;) {
         if (reads_only(ks[i].kind)) continue;
         LineDesc& d = ks[i].line;
         if (ks[i].kind == K_LINE && !d.has_extra && !(d.f1 && d.f2)) {
-            const int N = d.axis == 0 ? d.nx : d.nz;
+            const int N = d.axis == 0 ? d.nx : d.nz, nl = d.axis == 0 ? d.nz : d.nx;
             if (fixed_family(d.axis, N) == FAM_SPEC) {
                 d.out_int = 1;
                 // a column pass writes the intensity in blocks of its tile's columns (contiguous
                 // pieces); the accumulation reads that layout
                 const int bw = fixed_lines_per_cta(1, N);
                 if (d.axis == 1 && d.blk_out == 0 && bw > 1 && d.nx % bw == 0) d.blk_out = bw;
+                const ChainTab& out = d.f1 ? d.t_mid : d.t_fin;
+                const double a = flat_mag2(tables, out.tab, N), b = flat_mag2(tables, d.t_pre.ltab, nl),
+                             c = flat_mag2(tables, d.t_mid.ltab, nl), e = flat_mag2(tables, d.t_fin.ltab, nl);
+                if (a >= 0. && b >= 0. && c >= 0. && e >= 0.) {
+                    d.int_flat = 1;
+                    d.int_scale = (float)(a * b * c * e);
+                }
             }
         }
         return;
@@ -264,7 +288,7 @@ static bool same_structure(const std::vector<KernelDesc>& a, const std::vector<K
             const LineDesc &p = x.line, &q = y.line;
             if (p.axis != q.axis || p.nx != q.nx || p.nz != q.nz || p.f1 != q.f1 || p.f2 != q.f2 ||
                 p.has_extra != q.has_extra || p.zwin != q.zwin || p.blk_in != q.blk_in || p.blk_out != q.blk_out ||
-                p.out_int != q.out_int)
+                p.out_int != q.out_int || p.int_flat != q.int_flat)
                 return false;
         } else if (x.kind == K_RESIZE) {
             const ResizeDesc &p = x.rs, &q = y.rs;
@@ -403,7 +427,7 @@ extern "C" SRWG_API int srwgMultiECreate(const SRWLWfr* pBase, const SRWLOptC* p
     pl.numMoments = false;               // only the intensity is kept: no moment passes
     pl.inPhase = true;                   // the electrons' kick (here zero): the same passes as theirs
     r = pl.plan(pBase, pOpt);
-    if (!r) mark_intensity_pass(pl.kernels);
+    if (!r) mark_intensity_pass(pl.kernels, pl.tables);
     if (r) { set_last_detail(pl.err); delete m; return r; }
     m->nIn = (size_t)m->nx * m->nz;
     m->nOut = (size_t)pl.w.nx * pl.w.nz;
@@ -603,7 +627,7 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
                     pls[k].inKz = eps[k].kz;
                     pls[k].inC = -(eps[k].kx * eps[k].dx + eps[k].kz * eps[k].dz);
                     rcs[k] = pls[k].plan(&w, m->opt);
-                    if (!rcs[k]) mark_intensity_pass(pls[k].kernels);
+                    if (!rcs[k]) mark_intensity_pass(pls[k].kernels, pls[k].tables);
                 }
             };
             std::vector<std::thread> th;
@@ -661,7 +685,7 @@ extern "C" SRWG_API int srwgMultiEInfo(srwgMultiE* m, int* nPasses, int* intensi
     pl.inPhase = true;
     int r = pl.plan(&m->base, m->opt);
     if (r) { set_last_detail(pl.err); return r; }
-    mark_intensity_pass(pl.kernels);
+    mark_intensity_pass(pl.kernels, pl.tables);
     if (nPasses) *nPasses = (int)pl.kernels.size();
     if (intensityPass) *intensityPass = intensity_pass(pl.kernels) ? 1 : 0;
     if (desc && descLen > 0) {

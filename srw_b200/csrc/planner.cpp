@@ -1872,8 +1872,10 @@ std::string Planner::describe() const
             LineLaunch lp;
             memset(&lp, 0, sizeof(lp));
             const char* fam = line_config(d, lp) ? "none" : lp.v2 == 1 ? "pow2" : lp.v2 == 3 ? "spec" : lp.v2 == 2 ? "gen" : "tab";
-            char win[64] = "";
+            char win[96] = "";
             if (d.zwin) snprintf(win, sizeof(win), "  lines=%d:%d points=%d:%d", d.zl0, d.zl1, d.za0, d.za1);
+            if (d.out_int)
+                snprintf(win + strlen(win), sizeof(win) - strlen(win), "  intensity%s", d.int_flat ? " flat" : "");
             snprintf(buf, sizeof(buf), "%zu LINE %s %dx%d f1=%d pw=%d(q%d a%d m%d s%d) mir=%d/%d f2=%d zwin=%d blk=%d/%d  buf %d->%d  fft=%s L=%d%s\n",
                      i, d.axis == 0 ? "rows" : "cols", d.nx, d.nz, d.f1, d.has_pw, d.pw.has_quad, d.pw.has_ang, d.pw.nmask,
                      d.pw.has_scale, d.mirror_along, d.mirror_lines, d.f2, d.zwin, d.blk_in, d.blk_out, k.src, k.dst, fam, lp.L,

@@ -123,6 +123,12 @@ class MultiE(object):
                                                  ms, 64, C.byref(n)), 'multi-electron timed add')
         return [float(ms[i]) for i in range(min(n.value, 64))]
 
+    def describe(self):
+        """The planner's description of a batch's passes (the base electron's), as srwgPlanDescribe."""
+        buf = C.create_string_buffer(1 << 16)
+        capi.check(capi.lib().srwgMultiEInfo(self._h, None, None, buf, len(buf)), 'multi-electron info')
+        return buf.value.decode()
+
     def info(self):
         """(passes of a batch [(kind, sizes...)] as Plan.kernels gives them, whether the last pass
         writes the intensity instead of the fields)."""

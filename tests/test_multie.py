@@ -193,8 +193,9 @@ def test_multie_energy_spread_vs_oracle():
 @pytest.mark.gpu
 def test_multie_intensity_pass_vs_oracle():
     """Electrons on a grid of a specialised length (128^2 -> 320^2): the last pass transforms both
-    components per CTA and writes the total intensity (the accumulation reads one float per sample);
-    the mean against the oracle's electron-by-electron loop."""
+    components per CTA and writes the total intensity in column blocks (the accumulation reads one
+    float per sample), its output factors folded into one scale; the mean against the oracle's
+    electron-by-electron loop."""
     _gpu()
     import ctypes as C
     from srw_b200 import capi
@@ -215,6 +216,8 @@ def test_multie_intensity_pass_vs_oracle():
     offs = sample_offsets(6, *SIG, seed=21, sig_e=1e-3)
     w = make_wfr(ex, ey, mesh, **sc)
     me = MultiE(w, beamline(C1, pp), acc, max_batch=4, graph=True)
+    # the to-waist output factors have one magnitude: applied as a scale of the intensity
+    assert 'intensity flat' in me.describe().splitlines()[-1]
     me.add(offs)
     got = me.mean()
     want = oracle_sum(dict(ex=ex, ey=ey, mesh=mesh), sc, C1, pp, acc, offs) / 6

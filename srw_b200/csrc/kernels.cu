@@ -131,6 +131,14 @@ __global__ void __launch_bounds__(512, 1) line_kernel(const LineLaunch p)
 // ------------------------------------------------------------------------------------------------
 // RESIZE pass (RadResizeCore, sroptelm.cpp:3038-3337; OnlyLargerRange :4231)
 // ------------------------------------------------------------------------------------------------
+// sqrt(FI / app), the amplitude correction of ImproveReAndIm, from two reciprocal square roots (no
+// division, and FI * app cannot overflow); within a few ulp of the correctly rounded value; FI >= 0,
+// app > 0
+__device__ __forceinline__ float amp_ratio(float FI, float app)
+{
+    return FI > 0.f ? FI * rsqrtf(FI) * rsqrtf(app) : 0.f;
+}
+
 __device__ __forceinline__ void lagrange4(float t, float* w)
 {
     // cubic through nodes -1, 0, 1, 2 (the reference's SetupInterpolAux02 polynomial)
@@ -205,7 +213,7 @@ __device__ __forceinline__ float2 resize_point(const float2* __restrict__ o, int
     FI = FI > 0.f ? FI : 0.f;
     float app = F.x * F.x + F.y * F.y;          // ImproveReAndIm
     if (app != 0.f) {
-        float fac = sqrtf(FI / app);
+        float fac = amp_ratio(FI, app);
         F.x *= fac; F.y *= fac;
     }
     return F;
@@ -258,7 +266,7 @@ __device__ __forceinline__ float2 interp_stencil(const float2 (&f)[4][4], const 
     FI = FI > 0.f ? FI : 0.f;
     float app = F.x * F.x + F.y * F.y;          // ImproveReAndIm
     if (app != 0.f) {
-        float fac = sqrtf(FI / app);
+        float fac = amp_ratio(FI, app);
         F.x *= fac; F.y *= fac;
     }
     return F;
@@ -530,7 +538,7 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
                 FI = FI > 0.f ? FI : 0.f;
                 const float app = F.x * F.x + F.y * F.y;      // ImproveReAndIm
                 if (app != 0.f) {
-                    const float fac = sqrtf(FI / app);
+                    const float fac = amp_ratio(FI, app);
                     F.x *= fac;
                     F.y *= fac;
                 }

@@ -40,6 +40,7 @@ struct ElecParams {
     double kx, kz;                       // kick: phase kx x + kz z on the base mesh (fused by the planner)
     double dx, dz;                       // mesh shift of the electron's wavefront
     double oxStart, oxStep, ozStart, ozStep;   // output mesh (steps as (Fin - Start)/(n - 1))
+    double oxInv, ozInv;                       // 1 / step: the accumulation multiplies (no FP64 divisions)
     int onx, onz;
     int pad[2];
 };
@@ -58,12 +59,12 @@ __global__ void __launch_bounds__(256) accum_kernel(const float2* __restrict__ e
     double sum = 0.;
     for (int b = 0; b < nb; b++) {
         const ElecParams& e = ep[b];
-        const int ix0 = (int)trunc((x - e.oxStart) / e.oxStep + 1.e-09);
+        const int ix0 = (int)trunc((x - e.oxStart) * e.oxInv + 1.e-09);
         if (ix0 < 0 || ix0 >= e.onx - 1) continue;
-        const int iy0 = (int)trunc((y - e.ozStart) / e.ozStep + 1.e-09);
+        const int iy0 = (int)trunc((y - e.ozStart) * e.ozInv + 1.e-09);
         if (iy0 < 0 || iy0 >= e.onz - 1) continue;
-        const double tx = (x - (e.oxStart + e.oxStep * ix0)) / e.oxStep;
-        const double ty = (y - (e.ozStart + e.ozStep * iy0)) / e.ozStep;
+        const double tx = (x - (e.oxStart + e.oxStep * ix0)) * e.oxInv;
+        const double ty = (y - (e.ozStart + e.ozStep * iy0)) * e.ozInv;
         const float2* px = ex + (size_t)b * stride + (size_t)iy0 * e.onx + ix0;
         const float2* py = ey + (size_t)b * stride + (size_t)iy0 * e.onx + ix0;
         float I[4];
@@ -95,12 +96,12 @@ __global__ void __launch_bounds__(256) accum_int_kernel(const float* __restrict_
     double sum = 0.;
     for (int b = 0; b < nb; b++) {
         const ElecParams& e = ep[b];
-        const int ix0 = (int)trunc((x - e.oxStart) / e.oxStep + 1.e-09);
+        const int ix0 = (int)trunc((x - e.oxStart) * e.oxInv + 1.e-09);
         if (ix0 < 0 || ix0 >= e.onx - 1) continue;
-        const int iy0 = (int)trunc((y - e.ozStart) / e.ozStep + 1.e-09);
+        const int iy0 = (int)trunc((y - e.ozStart) * e.ozInv + 1.e-09);
         if (iy0 < 0 || iy0 >= e.onz - 1) continue;
-        const double tx = (x - (e.oxStart + e.oxStep * ix0)) / e.oxStep;
-        const double ty = (y - (e.ozStart + e.ozStep * iy0)) / e.ozStep;
+        const double tx = (x - (e.oxStart + e.oxStep * ix0)) * e.oxInv;
+        const double ty = (y - (e.ozStart + e.ozStep * iy0)) * e.ozInv;
         const float* pe = in + (size_t)b * stride;
         double a00, f10, f01, f11;
         if (bw > 0) {
@@ -665,6 +666,8 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
         ep.oxStep = (xFin - pl.w.xStart) / (pl.w.nx - 1);
         ep.ozStart = pl.w.zStart;
         ep.ozStep = (zFin - pl.w.zStart) / (pl.w.nz - 1);
+        ep.oxInv = 1. / ep.oxStep;
+        ep.ozInv = 1. / ep.ozStep;
         ep.onx = pl.w.nx;
         ep.onz = pl.w.nz;
         m->hParams[m->slot][nb] = ep;

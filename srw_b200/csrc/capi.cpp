@@ -335,6 +335,32 @@ static int upload_tables(const Planner& pl, float2** buf, size_t* capElems, cuda
 // work buffers (layout [buffer][component][wavefront][workElems]); the last pass writes the output
 // (outX + b * outStride).  dconst holds per wavefront (stride constStride bytes) the tables and, at
 // descOff, the pass descriptors; all wavefronts have passes of the same kinds and sizes.
+// a row pass whose lines outside its window are zero and read by nothing (zskip) launches only the
+// window's line blocks; `d` holds the window of the launch (for a batch: the union of its electrons')
+void line_window(const LineDesc& d, LineLaunch& p)
+{
+    if (d.zwin && d.zskip && d.zl0 <= d.zl1 && p.L > 0) {
+        const int l0 = std::max(0, d.zl0), l1 = std::min(p.nlines - 1, d.zl1);
+        if (l0 <= l1) {
+            p.blk0 = l0 / p.L;
+            p.nblk = l1 / p.L - p.blk0 + 1;
+        }
+    }
+}
+
+// a tiled resize that writes only its window launches only the window's tiles
+void resize_window(const ResizeDesc& r, ResizeLaunch& p)
+{
+    if (!r.skip_zero || r.tile_or <= 0) return;
+    const long xs = std::max(0L, r.ixStart), xe = std::min((long)r.nxn - 1, r.ixEnd);
+    const long zs = std::max(0L, r.izStart), ze = std::min((long)r.nzn - 1, r.izEnd);
+    if (xs > xe || zs > ze) return;
+    p.tx0 = (int)(xs / SRWG_RESIZE_TX);
+    p.ntx = (int)(xe / SRWG_RESIZE_TX) - p.tx0 + 1;
+    p.tz0 = (int)(zs / SRWG_RESIZE_TZ);
+    p.ntz = (int)(ze / SRWG_RESIZE_TZ) - p.tz0 + 1;
+}
+
 int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, const float2* inX, const float2* inY,
                    long long inStride, float2* outX, float2* outY, long long outStride, float2* work, size_t workElems,
                    const char* dconst, long long constStride, size_t descOff, cudaStream_t st, cudaEvent_t* ev,
@@ -401,6 +427,7 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
             p.nb = nb; p.bDesc = constStride; p.bTab = tabStride; p.bSrc = bSrc; p.bDst = bDst;
             p.status = c.status;
             p.spin = g_waitLimit;
+            line_window(k.line, p);
             e = launch_line(p, st);
         } else if (k.kind == K_RESIZE) {
             ResizeLaunch p;
@@ -409,6 +436,7 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
             p.src[0] = s0; p.src[1] = s1; p.dst[0] = d0; p.dst[1] = d1;
             p.xStepInvO = 1. / k.rs.xStepO;
             p.zStepInvO = 1. / k.rs.zStepO;
+            resize_window(k.rs, p);
             p.tabs = tabs;
             p.gd = &gk[i].rs;
             p.nb = nb; p.bDesc = constStride; p.bTab = tabStride; p.bSrc = bSrc; p.bDst = bDst;

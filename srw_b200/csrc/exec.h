@@ -38,6 +38,8 @@ int execute_passes(const std::vector<KernelDesc>& ks, DeviceCtx& c, int nb, cons
                    const std::vector<KernelDesc>* hostMax, double* momScratch = nullptr, double* momSlots = nullptr,
                    int nSlots = 0, char* intOut = nullptr);
 int line_config(const LineDesc& d, LineLaunch& p);   // launch shape of a line pass (capi.cpp)
+void line_window(const LineDesc& d, LineLaunch& p);  // only the window's line blocks (zskip row passes)
+void resize_window(const ResizeDesc& r, ResizeLaunch& p);   // only the window's tiles (skip_zero)
 int radix_plan(int N, int* r);
 void set_last_detail(const std::string& s);          // detail text for srwlUtiGetErrText
 const std::string& last_detail();

@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(512, 1) line_kernel(const LineLaunch p)
     const int tid = threadIdx.x, nth = blockDim.x;
     const int G = nth / T;
     const int g = tid / T, t = tid - g * T;
-    const int line0 = blockIdx.x * L;
+    const int line0 = (blockIdx.x + p.blk0) * L;
 
     // ---- load the tile
     if (d.axis == 0) {
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(256) resize2_kernel(const ResizeLaunch p)
     float2* old = reinterpret_cast<float2*>(H + 2 * OR * TX);   // [comp][old row][old column]
     __shared__ int ext[4];
     const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * TX, z0 = blockIdx.y * TZ;
+    const int x0 = (blockIdx.x + p.tx0) * TX, z0 = (blockIdx.y + p.tz0) * TZ;
     const int xa = max(x0, (int)d.ixStart), xb = min(min(x0 + TX, d.nxn) - 1, (int)d.ixEnd);
     const int za = max(z0, (int)d.izStart), zb = min(min(z0 + TZ, d.nzn) - 1, (int)d.izEnd);
     if (xa > xb || za > zb) {
@@ -609,9 +609,17 @@ Line2Fn linen_kernel_ptr(int N, bool cols, bool extra, int nt, bool inten)
     return nullptr;
 }
 
-cudaError_t launch_line(const LineLaunch& p, cudaStream_t st)
+cudaError_t launch_line(const LineLaunch& pin, cudaStream_t st)
 {
+    LineLaunch p = pin;
     dim3 grid((p.nlines + p.L - 1) / p.L, 2, p.nb > 1 ? p.nb : 1);
+    if (p.nblk > 0) {
+        // only the line blocks of the window (the others would write nothing)
+        if (p.blk0 < 0 || p.blk0 + p.nblk > (int)grid.x) return cudaErrorInvalidValue;
+        grid.x = p.nblk;
+    } else {
+        p.blk0 = 0;
+    }
     size_t smem = (size_t)p.L * p.P * sizeof(float2);
     if (smem > SRWG_LINE_SMEM_MAX) return cudaErrorInvalidValue;
     if (attrs_needed(0)) {
@@ -683,7 +691,17 @@ cudaError_t launch_resize(const ResizeLaunch& q, cudaStream_t st)
             cudaFuncSetAttribute(resize2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SRWG_LINE_SMEM_MAX);
         dim3 grid((p.d.nxn + SRWG_RESIZE_TX - 1) / SRWG_RESIZE_TX, (p.d.nzn + SRWG_RESIZE_TZ - 1) / SRWG_RESIZE_TZ,
                   p.nb > 1 ? p.nb : 1);
-        resize2_kernel<<<grid, 256, smem, st>>>(p);
+        ResizeLaunch q = p;
+        if (p.ntx > 0 && p.ntz > 0) {
+            // only the tiles of the window (the others would write nothing)
+            if (p.tx0 < 0 || p.tz0 < 0 || p.tx0 + p.ntx > (int)grid.x || p.tz0 + p.ntz > (int)grid.y)
+                return cudaErrorInvalidValue;
+            grid.x = p.ntx;
+            grid.y = p.ntz;
+        } else {
+            q.tx0 = q.tz0 = 0;
+        }
+        resize2_kernel<<<grid, 256, smem, st>>>(q);
         return cudaGetLastError();
     }
     dim3 blk(64, 4);

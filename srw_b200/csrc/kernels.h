@@ -52,6 +52,7 @@ struct LineLaunch {
     int bulk;                // specialised pass: each CTA's input tile arrives by bulk async copies
     int* status;             // device counter of waits that gave up (NULL: not recorded)
     long long spin;          // iteration limit of the bulk-copy wait
+    int blk0, nblk;          // the line blocks launched: blk0 .. blk0 + nblk - 1 (nblk 0: all)
 };
 
 // tiled resize: a CTA makes TZ x TX new points from an old tile of at most OR_MAX x OC_MAX points
@@ -71,6 +72,7 @@ struct ResizeLaunch {
     int nb;                  // wavefronts in the launch (grid z; 0 or 1: one)
     long long bDesc, bTab;   // per wavefront: descriptor stride (bytes), table stride (float2)
     long long bSrc, bDst;    // per wavefront: source / destination field stride (float2)
+    int tx0, tz0, ntx, ntz;  // tiled kernel: the tiles launched (first, count per axis; ntx 0: all)
 };
 
 struct PwLaunch {

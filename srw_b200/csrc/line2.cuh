@@ -157,7 +157,8 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     const int tid = threadIdx.x;
     const int g = COLS ? (tid % L) : (tid / T);          // line of the tile
     const int t = COLS ? (tid / L) : (tid - g * T);      // thread within the line
-    const int line = blockIdx.x * L + g;
+    const int bx = blockIdx.x + p.blk0;                 // line block
+    const int line = bx * L + g;
     bool active = line < nl;
     float2* s = sm + (size_t)g * P;
     // input: row-major, or (column pass after a row pass) blocks of blk_in columns stored together
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(1024, 1) line2_kernel(const LineLaunch p)
     // wrote only its window): loads outside are skipped, all-zero tiles write zeros directly
     int za0 = 0, za1 = N - 1;
     if (d.zwin) {
-        const int l0 = blockIdx.x * L, l1 = min(l0 + L, nl) - 1;
+        const int l0 = bx * L, l1 = min(l0 + L, nl) - 1;
         if (l1 < d.zl0 || l0 > d.zl1) {
             if (active && !d.zskip) {
 #pragma unroll

@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(512, 1) lineg_kernel(const LineLaunch p)
     const int g = COLS ? (tid % L) : (tid / T);
     const int t = COLS ? (tid / L) : (tid - g * T);
     GLine x;
-    x.line = blockIdx.x * L + g;
+    x.line = (blockIdx.x + p.blk0) * L + g;
     x.active = x.line < nl;
     x.axis = d.axis;
     float2* s = smg + (size_t)g * p.P;

@@ -453,7 +453,8 @@ __device__ __forceinline__ bool linen_body(const LineLaunch& p, int comp, IAcc<N
     const int tid = threadIdx.x;
     const int g = COLS ? (tid % L) : (tid / T);          // line of the tile
     const int t = COLS ? (tid / L) : (tid - g * T);      // thread within the line
-    const int line0 = blockIdx.x * L + g;
+    const int bx = blockIdx.x + p.blk0;                 // line block
+    const int line0 = bx * L + g;
     NLine x;
     x.store = line0 < nl;
     const int line = x.store ? line0 : nl - 1;           // inactive threads work on the last line
@@ -486,7 +487,7 @@ __device__ __forceinline__ bool linen_body(const LineLaunch& p, int comp, IAcc<N
     x.za0 = 0;
     x.za1 = N - 1;
     if (d.zwin) {
-        const int l0 = blockIdx.x * L, l1 = min(l0 + L, nl) - 1;
+        const int l0 = bx * L, l1 = min(l0 + L, nl) - 1;
         if (l1 < d.zl0 || l0 > d.zl1) {
             // the whole tile is zero: so is its transform
             if (x.store && OUTI == 0 && !d.zskip)
@@ -521,7 +522,7 @@ __device__ __forceinline__ bool linen_body(const LineLaunch& p, int comp, IAcc<N
                 if (x.za0 <= x.za1) bytes = (unsigned)((x.za1 - x.za0 + 1) * L * sizeof(float2));
             } else {
                 for (int gg = 0; gg < L; gg++) {
-                    const int ln = min(blockIdx.x * L + gg, nl - 1);
+                    const int ln = min(bx * L + gg, nl - 1);
                     const bool inl = !d.zwin || (ln >= d.zl0 && ln <= d.zl1);
                     const int lo = d.zwin ? (d.za0 & ~1) : 0, hi = d.zwin ? (d.za1 | 1) : N - 1;
                     if (inl && lo <= hi) bytes += (unsigned)((hi - lo + 1) * sizeof(float2));
@@ -530,12 +531,12 @@ __device__ __forceinline__ bool linen_body(const LineLaunch& p, int comp, IAcc<N
             mbar_expect(&bar, bytes);
             if (COLS) {
                 if (bytes) {
-                    const size_t blk = (size_t)(blockIdx.x * L / d.blk_in) * N * d.blk_in;
+                    const size_t blk = (size_t)(bx * L / d.blk_in) * N * d.blk_in;
                     bulk_load(smn + (size_t)x.za0 * L, src + blk + (size_t)x.za0 * L, bytes, &bar);
                 }
             } else {
                 for (int gg = 0; gg < L; gg++) {
-                    const int ln = min(blockIdx.x * L + gg, nl - 1);
+                    const int ln = min(bx * L + gg, nl - 1);
                     const bool inl = !d.zwin || (ln >= d.zl0 && ln <= d.zl1);
                     const int lo = d.zwin ? (d.za0 & ~1) : 0, hi = d.zwin ? (d.za1 | 1) : N - 1;
                     if (inl && lo <= hi)

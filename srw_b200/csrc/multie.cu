@@ -346,19 +346,40 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
     int r = 0;
     if (m.useGraph && nb == m.maxBatch && m.tev.empty()) {
         // the graph holds the launch shapes; a batch whose resize tiles are larger needs a new one
+        // (and launches only the windows' CTAs: a batch whose windows reach beyond them too)
         bool fits = m.graph[s] != nullptr && m.graphKs[s].size() == ks.size();
-        for (size_t i = 0; fits && i < ks.size(); i++)
-            if (ks[i].kind == K_RESIZE &&
-                (ks[i].rs.tile_or > m.graphKs[s][i].rs.tile_or || ks[i].rs.tile_oc > m.graphKs[s][i].rs.tile_oc))
+        for (size_t i = 0; fits && i < ks.size(); i++) {
+            const KernelDesc &a = ks[i], &g = m.graphKs[s][i];
+            if (a.kind == K_RESIZE &&
+                (a.rs.tile_or > g.rs.tile_or || a.rs.tile_oc > g.rs.tile_oc || a.rs.ixStart < g.rs.ixStart ||
+                 a.rs.ixEnd > g.rs.ixEnd || a.rs.izStart < g.rs.izStart || a.rs.izEnd > g.rs.izEnd))
                 fits = false;
+            if (a.kind == K_LINE && a.line.zwin && (a.line.zl0 < g.line.zl0 || a.line.zl1 > g.line.zl1)) fits = false;
+        }
         if (!fits) {
             if (m.graph[s]) { cudaGraphExecDestroy(m.graph[s]); m.graph[s] = nullptr; }
             std::vector<KernelDesc> cap = ks;
-            for (size_t i = 0; i < cap.size(); i++)
-                if (cap[i].kind == K_RESIZE && cap[i].rs.tile_or > 0) {     // headroom for other batches
-                    cap[i].rs.tile_or = std::min(SRWG_RESIZE_OR_MAX, cap[i].rs.tile_or + 2);
-                    cap[i].rs.tile_oc = std::min(SRWG_RESIZE_OC_MAX, cap[i].rs.tile_oc + 2);
+            for (size_t i = 0; i < cap.size(); i++) {
+                // headroom for other batches: larger tiles, windows wider by a quarter of theirs
+                if (cap[i].kind == K_RESIZE && cap[i].rs.tile_or > 0) {
+                    ResizeDesc& r = cap[i].rs;
+                    r.tile_or = std::min(SRWG_RESIZE_OR_MAX, r.tile_or + 2);
+                    r.tile_oc = std::min(SRWG_RESIZE_OC_MAX, r.tile_oc + 2);
+                    const long mx = std::max(2L * SRWG_RESIZE_TX, (r.ixEnd - r.ixStart) / 4);
+                    const long mz = std::max(2L * SRWG_RESIZE_TZ, (r.izEnd - r.izStart) / 4);
+                    r.ixStart = std::max(0L, r.ixStart - mx);
+                    r.ixEnd = std::min((long)r.nxn - 1, r.ixEnd + mx);
+                    r.izStart = std::max(0L, r.izStart - mz);
+                    r.izEnd = std::min((long)r.nzn - 1, r.izEnd + mz);
                 }
+                if (cap[i].kind == K_LINE && cap[i].line.zwin) {
+                    LineDesc& d = cap[i].line;
+                    const int nl = d.axis == 0 ? d.nz : d.nx;
+                    const int ml = std::max(64, (d.zl1 - d.zl0) / 4);
+                    d.zl0 = std::max(0, d.zl0 - ml);
+                    d.zl1 = std::min(nl - 1, d.zl1 + ml);
+                }
+            }
             // this batch runs directly (which also creates every lazily made resource -- twiddle
             // tables, kernel attributes -- before the capture); the capture only records the launches
             r = run_batch(m, nb, cap, st, s);
@@ -653,10 +674,21 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
             nb = 0;
         }
         if (nb == 0) { first = pl.kernels; launchKs = pl.kernels; }
+        // launch shapes of the batch: the largest resize tiles and the union of the windows (the
+        // kernels read every electron's own descriptor)
         for (size_t i = 0; i < launchKs.size(); i++)
             if (launchKs[i].kind == K_RESIZE) {
-                launchKs[i].rs.tile_or = std::max(launchKs[i].rs.tile_or, pl.kernels[i].rs.tile_or);
-                launchKs[i].rs.tile_oc = std::max(launchKs[i].rs.tile_oc, pl.kernels[i].rs.tile_oc);
+                ResizeDesc &a = launchKs[i].rs;
+                const ResizeDesc& b = pl.kernels[i].rs;
+                a.tile_or = std::max(a.tile_or, b.tile_or);
+                a.tile_oc = std::max(a.tile_oc, b.tile_oc);
+                a.ixStart = std::min(a.ixStart, b.ixStart);
+                a.ixEnd = std::max(a.ixEnd, b.ixEnd);
+                a.izStart = std::min(a.izStart, b.izStart);
+                a.izEnd = std::max(a.izEnd, b.izEnd);
+            } else if (launchKs[i].kind == K_LINE && launchKs[i].line.zwin) {
+                launchKs[i].line.zl0 = std::min(launchKs[i].line.zl0, pl.kernels[i].line.zl0);
+                launchKs[i].line.zl1 = std::max(launchKs[i].line.zl1, pl.kernels[i].line.zl1);
             }
         pending.emplace_back(g, nb);
         // output mesh as the reference's SRWLWfr holds it, step re-derived from (Fin - Start)/(n - 1)

@@ -29,33 +29,20 @@ __device__ __forceinline__ void stage16(float2* s, const float2* __restrict__ gi
     constexpr int TWS = N / (NS * R);
     float2 v[B][R];
     if (IN == 2) {
-        // first stage from global memory: all 16 loads are issued before any dependent arithmetic.
-        // The sources of radix index r are the block r NR .. r NR + NR - 1 XOR the source mask,
-        // itself a block of NR (NR a power of two dividing N/2): a block outside the nonzero window
-        // [za0, za1] is zero with no loads and no factors (a branch uniform over the CTA)
-        bool seg[R];
+        // first stage from global memory: all 16 loads are issued before any dependent arithmetic
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int a = (r * NR) ^ (cin.xs & ~(NR - 1));
-            seg[r] = !(a + NR - 1 < za0 || a > za1);
-        }
+        for (int b = 0; b < B; b++)
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-#pragma unroll
-            for (int b = 0; b < B; b++) {
+            for (int r = 0; r < R; r++) {
                 const int p = t + T * b + r * NR;
                 const int q = p ^ cin.xs;
-                const bool in = seg[r] && active && q >= za0 && q <= za1;
+                const bool in = active && q >= za0 && q <= za1;
                 v[b][r] = in ? __ldcs(&gin[q * gstr]) : make_float2(0.f, 0.f);
             }
-        }
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            if (!seg[r]) continue;
+        for (int b = 0; b < B; b++)
 #pragma unroll
-            for (int b = 0; b < B; b++)
-                v[b][r] = chain2_apply<EXTRA>(cin, t + T * b + r * NR, line, v[b][r], tabs, ex, axis);
-        }
+            for (int r = 0; r < R; r++) v[b][r] = chain2_apply<EXTRA>(cin, t + T * b + r * NR, line, v[b][r], tabs, ex, axis);
         // NS == 1 for the first stage: no twiddles
     } else {
 #pragma unroll

@@ -174,18 +174,15 @@ template <int N> __device__ __forceinline__ int chain_eval_n(const ChainG& c, in
 // the chain's factors at destinations p = j + r NR of butterfly round b (v *= tab[p] (and the
 // non-separable work)); rounds beyond the last butterfly (PART) are left alone
 template <int N, int R, int NR, int T, int B, bool PART, bool EXTRA>
-__device__ __forceinline__ void apply_factors(float2 (&v)[B][R], const NLine& x, const ChainG& c, int t,
-                                              const bool* seg = nullptr)
+__device__ __forceinline__ void apply_factors(float2 (&v)[B][R], const NLine& x, const ChainG& c, int t)
 {
     if (c.tab >= 0) {
         const float2* tb = x.tabs + c.tab + t;
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            if (seg && !seg[r]) continue;
+        for (int b = 0; b < B; b++)
 #pragma unroll
-            for (int b = 0; b < B; b++)
+            for (int r = 0; r < R; r++)
                 if (!PART || b < B - 1 || t + T * b < NR) v[b][r] = cmul(__ldg(&tb[T * b + r * NR]), v[b][r]);
-        }
     }
     if (EXTRA && c.extra) {
 #pragma unroll
@@ -243,39 +240,12 @@ __device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& 
         // p rotated by N/2 (a permutation of the radix index: R is even here), or the general map
         // with the mirror
         const bool rot = cin.rs1 != cin.rs2;
-        // per radix index r: do the sources of its NR destinations r NR .. r NR + NR - 1 meet the
-        // nonzero window [za0, za1]?  For an even radix they are one contiguous block (the rotation
-        // by N/2 moves whole blocks, the mirror reverses them), so a block outside the window is zero
-        // with no loads and no factors (a branch uniform over the CTA); odd radices load as before
-        bool seg[R];
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            if (R % 2 == 0) {
-                int a, c;
-                if (!cin.mir) {
-                    a = (rot ? (r + R / 2) % R : r) * NR;
-                    c = a + NR - 1;
-                } else {
-                    int i;
-                    a = chain_src_n<N>(cin, r * NR, i);
-                    c = chain_src_n<N>(cin, r * NR + NR - 1, i);
-                }
-                seg[r] = !(max(a, c) < x.za0 || min(a, c) > x.za1);
-            } else {
-                seg[r] = true;
-            }
-        }
+        for (int b = 0; b < B; b++) {
+            const int j = t + T * b;
+            const bool okj = !PART || b < B - 1 || j < NR;
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            if (!seg[r]) {
-#pragma unroll
-                for (int b = 0; b < B; b++) v[b][r] = make_float2(0.f, 0.f);
-                continue;
-            }
-#pragma unroll
-            for (int b = 0; b < B; b++) {
-                const int j = t + T * b;
-                const bool okj = !PART || b < B - 1 || j < NR;
+            for (int r = 0; r < R; r++) {
                 int q;
                 if (!cin.mir) {
                     const int rr = (R % 2 == 0 && rot) ? (r + R / 2) % R : r;
@@ -290,7 +260,7 @@ __device__ __forceinline__ void nstage(float2* s, const NLine& x, const ChainG& 
                 else v[b][r] = in ? x.sin[q * x.sst] : make_float2(0.f, 0.f);
             }
         }
-        apply_factors<N, R, NR, T, B, PART, EXTRA>(v, x, cin, t, seg);
+        apply_factors<N, R, NR, T, B, PART, EXTRA>(v, x, cin, t);
         if (cj < 0.f) conj_all(v);
         // NS == 1 for the first stage: no twiddles
     } else {

@@ -10,12 +10,13 @@ namespace srwg {
 #define SRWG_LINE_SMEM_MAX (220 * 1024)
 
 // shared-memory pitch of a line of N points in the line passes: one pad point per 16 (conflict-free
-// Stockham exchanges) plus 4, so that the lines of a tile start 8 banks apart, rounded up to an even
-// count (every line's slot 16-byte aligned, for bulk copies into it)
+// Stockham exchanges), then rounded up to 4 modulo 16 points, so that the lines of a tile start 8
+// banks apart (a half-warp of a column pass reads 4 points of each of 4 lines: 4 x 8 banks, no
+// conflict) and every line's slot is 16-byte aligned (bulk copies into it)
 inline size_t line_pitch(int N)
 {
-    const size_t P = (size_t)N + N / 16 + 4;
-    return P + (P & 1);
+    const size_t P = (size_t)N + N / 16;
+    return P + ((4 + 16 - P % 16) % 16);
 }
 
 // lines per CTA of the power-of-two line pass (line2_kernel): rows ~256 threads, columns up to

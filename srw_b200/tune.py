@@ -67,8 +67,8 @@ def candidates(axis, n, fam=None):
     for f in families(n) if fam is None else [fam]:
         t = n // 16 if f == FAM_POW2 else (n + 15) // 16
         tmax = 1024 if f == FAM_POW2 else 512
-        p = n + n // 16 + 4
-        p += p & 1                              # the library's line_pitch
+        p = n + n // 16
+        p += (4 + 16 - p % 16) % 16             # the library's line_pitch
         for L in range(1, 33):
             if L * p * 8 > SMEM_MAX or t * L > tmax:
                 break

@@ -46,7 +46,9 @@ def test_specialised_lengths_have_valid_schedules():
         assert r is not None and 2 <= len(r) <= 8, n
         assert int(np.prod(r)) == n
         assert n % 16 == 0 and (n & (n - 1)) != 0          # 16 points per thread; powers of two go to line2
-        assert (n + n // 16 + 4) * 8 <= 220 * 1024         # one line fits the shared-memory budget
+        p = n + n // 16
+        p += (4 + 16 - p % 16) % 16                         # the library's line pitch
+        assert p % 16 == 4 and p >= n + n // 16 and p * 8 <= 220 * 1024
 
 
 # ------------------------------------------------------------------------------------------------

@@ -221,10 +221,8 @@ int line_config(const LineDesc& d, LineLaunch& p)
             nb -= 4;
         }
         p.radix[p.nst++] = 1 << nb;          // 16, 8, 4 or 2
-        // one pad point per 16 (conflict-free Stockham exchanges) plus 4 per line, so that the
-        // lines of a tile start 8 banks apart
-        p.P = (int)line_pitch(N);
         const int L = fixed_lines_per_cta(d.axis, N);
+        p.P = (int)line_pitch(N, L, d.axis == 1);
         if (p.T * L > 1024) { g_lastDetail = "line pass too large"; return SRWG_ERR_UNSUPPORTED; }
         p.L = L;
         p.G = L;
@@ -236,8 +234,8 @@ int line_config(const LineDesc& d, LineLaunch& p)
     if (fam == FAM_SPEC) {
         p.v2 = 3;
         p.T = (N + 15) / 16;
-        p.P = (int)line_pitch(N);
         p.L = fixed_lines_per_cta(d.axis, N);
+        p.P = (int)line_pitch(N, p.L, d.axis == 1);
         p.G = p.L;
         p.nst = 0;
         if (p.T * p.L > 512 || (size_t)p.L * p.P * sizeof(float2) > cap) {
@@ -258,10 +256,10 @@ int line_config(const LineDesc& d, LineLaunch& p)
             int T = (N + 15) / 16;
             T = ((T + 31) / 32) * 32;
             p.T = T;
-            p.P = (int)line_pitch(N);
             int L = d.axis == 0 ? 256 / T : 512 / T;
             if (L < 1) L = 1;
-            while (L > 1 && (size_t)L * p.P * sizeof(float2) > cap) L--;
+            while (L > 1 && (size_t)L * line_pitch(N, L, d.axis == 1) * sizeof(float2) > cap) L--;
+            p.P = (int)line_pitch(N, L, d.axis == 1);
             if (T * L > 512 || (size_t)L * p.P * sizeof(float2) > cap) {
                 g_lastDetail = "line too long for shared memory";
                 return SRWG_ERR_UNSUPPORTED;

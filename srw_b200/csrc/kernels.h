@@ -10,13 +10,16 @@ namespace srwg {
 #define SRWG_LINE_SMEM_MAX (220 * 1024)
 
 // shared-memory pitch of a line of N points in the line passes: one pad point per 16 (conflict-free
-// Stockham exchanges), then rounded up to 4 modulo 16 points, so that the lines of a tile start 8
-// banks apart (a half-warp of a column pass reads 4 points of each of 4 lines: 4 x 8 banks, no
-// conflict) and every line's slot is 16-byte aligned (bulk copies into it)
-inline size_t line_pitch(int N)
+// Stockham exchanges), then rounded up so that the lines of a column tile start 32 / L banks apart
+// (a half-warp of a column pass reads 16 / L points of each of L lines, 8 bytes each: together 32
+// distinct banks): P = 16 / L modulo 16 points for L = 2, 4, 8, 1 for L >= 16; rows (their lanes
+// stay within one line) and L = 1: 4 modulo 16, which keeps every slot 16-byte aligned for the
+// bulk copies of row tiles
+inline size_t line_pitch(int N, int L = 1, bool cols = false)
 {
     const size_t P = (size_t)N + N / 16;
-    return P + ((4 + 16 - P % 16) % 16);
+    const size_t r = (cols && L >= 2) ? (L >= 16 ? 1 : 16 / L) : 4;
+    return P + ((r + 16 - P % 16) % 16);
 }
 
 // lines per CTA of the power-of-two line pass (line2_kernel): rows ~256 threads, columns up to
@@ -29,8 +32,7 @@ inline int line2_lines_per_cta(int axis, int N)
     int L = axis == 0 ? 256 / T : 1024 / T;
     if (L < 1) L = 1;
     if (axis == 1 && L > 32) L = 32;
-    const size_t P = line_pitch(N);
-    while (L > 1 && (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) L--;
+    while (L > 1 && (size_t)L * line_pitch(N, L, axis == 1) * 8 > SRWG_LINE_SMEM_MAX) L--;
     return L;
 }
 
@@ -162,7 +164,6 @@ enum { FAM_TAB = 0, FAM_POW2 = 1, FAM_GEN = 2, FAM_SPEC = 3 };
 inline int linen_lines_per_cta(int axis, int N)
 {
     const int T = (N + 15) / 16;
-    const size_t P = line_pitch(N);
     int L;
     if (axis == 0) {
         L = 512 / T;
@@ -171,14 +172,13 @@ inline int linen_lines_per_cta(int axis, int N)
         L = 1;
         while (2 * L * T <= 512 && 2 * L <= 32) L *= 2;
     }
-    while (L > 1 && (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) L = axis == 0 ? L - 1 : L / 2;
+    while (L > 1 && (size_t)L * line_pitch(N, L, axis == 1) * 8 > SRWG_LINE_SMEM_MAX) L = axis == 0 ? L - 1 : L / 2;
     return L;
 }
 // whether L lines per CTA is a valid launch shape of kernel family fam for length N
 inline bool fixed_lines_valid(int axis, int N, int L, int fam)
 {
-    const size_t P = line_pitch(N);
-    if (L < 1 || (size_t)L * P * 8 > SRWG_LINE_SMEM_MAX) return false;
+    if (L < 1 || (size_t)L * line_pitch(N, L, axis == 1) * 8 > SRWG_LINE_SMEM_MAX) return false;
     if (axis == 1 && (L > 32 || (L & (L - 1)) != 0)) return false;      // column blocks: a power of two
     if (fam == FAM_POW2 && line2_supported(N)) return (N / 16) * L <= 1024;
     if (fam == FAM_SPEC && (linen_supported(N) || linen_pow2(N))) return ((N + 15) / 16) * L <= 512;

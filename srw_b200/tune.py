@@ -50,6 +50,13 @@ def is_pow2(n):
 
 
 FAM_POW2, FAM_SPEC = 1, 3          # kernel families: power-of-two pass, specialised pass
+
+
+def line_pitch(n, lines=1, cols=False):
+    """The library's shared-memory pitch of a line (kernels.h line_pitch)."""
+    p = n + n // 16
+    r = (1 if lines >= 16 else 16 // lines) if (cols and lines >= 2) else 4
+    return p + (r + 16 - p % 16) % 16
 POW2_SPEC = [256, 512, 1024, 2048, 4096, 8192]       # powers of two the specialised pass is built for
 
 
@@ -67,10 +74,8 @@ def candidates(axis, n, fam=None):
     for f in families(n) if fam is None else [fam]:
         t = n // 16 if f == FAM_POW2 else (n + 15) // 16
         tmax = 1024 if f == FAM_POW2 else 512
-        p = n + n // 16
-        p += (4 + 16 - p % 16) % 16             # the library's line_pitch
         for L in range(1, 33):
-            if L * p * 8 > SMEM_MAX or t * L > tmax:
+            if L * line_pitch(n, L, axis == 1) * 8 > SMEM_MAX or t * L > tmax:
                 break
             if axis == 1 and (L & (L - 1)):
                 continue

@@ -89,9 +89,11 @@ __global__ void __launch_bounds__(256) accum_int_kernel(const float* __restrict_
                                                         int anx, int anz, double axStart, double axStep,
                                                         double azStart, double azStep, int bw)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (i >= anx) return;
+    // column blocks (bw > 0): the threads of a CTA walk a common-mesh column, so that neighbouring
+    // threads read neighbouring rows of one block (contiguous); row-major: they walk a row
+    const int i = bw > 0 ? (int)blockIdx.y : (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int j = bw > 0 ? (int)(blockIdx.x * blockDim.x + threadIdx.x) : (int)blockIdx.y;
+    if (i >= anx || j >= anz) return;
     const double x = axStart + (double)i * axStep, y = azStart + (double)j * azStep;
     double sum = 0.;
     for (int b = 0; b < nb; b++) {
@@ -320,7 +322,8 @@ static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, c
     if (ev) MTRY(cudaEventRecord(ev[2 * ks.size()], st));
     int bw = 0;
     if (intensity_pass(ks, &bw))
-        accum_int_kernel<<<ga, blk, 0, st>>>(reinterpret_cast<const float*>(outX), (long long)m.nOut, nb, m.dParams[slot],
+        accum_int_kernel<<<bw > 0 ? dim3((m.anz + 255) / 256, m.anx) : ga, blk, 0, st>>>(
+            reinterpret_cast<const float*>(outX), (long long)m.nOut, nb, m.dParams[slot],
                                              m.dAcc, m.anx, m.anz, m.axStart, m.axStep, m.azStart, m.azStep, bw);
     else
         accum_kernel<<<ga, blk, 0, st>>>(outX, outY, (long long)m.nOut, nb, m.dParams[slot], m.dAcc, m.anx, m.anz,

@@ -214,6 +214,8 @@ struct srwgMultiE {
     cudaEvent_t used[2] = {nullptr, nullptr};      // the last batch that read the slot has completed
     cudaStream_t copy = nullptr;                   // upload stream
     int slot = 0;
+    int upTo = 0;                        // electrons of the current slot already uploaded
+    bool upWaited = false;               // the copy stream waits for the slot's last reader
     bool useGraph = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // per slot
     std::vector<KernelDesc> graphKs[2];  // host copy (launch shapes) each graph was captured with
@@ -336,14 +338,32 @@ static int run_batch(srwgMultiE& m, int nb, const std::vector<KernelDesc>& ks, c
 // uploads the staged constants of nb electrons (copy stream, after the last batch that read the slot)
 // and runs (or replays) the batch on `st` once the upload has landed; the host then stages the next
 // batch in the other slot, once that slot's previous upload has completed
+// uploads the staged constants of electrons upTo .. nb - 1 of the current slot (copy stream, after
+// the last batch that read the slot): a batch is uploaded in pieces while its later electrons are
+// still being planned
+static int upload_staged(srwgMultiE& m, int nb)
+{
+    const int s = m.slot;
+    if (nb <= m.upTo) return 0;
+    if (!m.upWaited) {
+        MTRY(cudaStreamWaitEvent(m.copy, m.used[s], 0));
+        m.upWaited = true;
+    }
+    const size_t a = (size_t)m.upTo, n = (size_t)(nb - m.upTo);
+    MTRY(cudaMemcpyAsync(m.dConst[s] + a * m.constStride, m.hConst[s] + a * m.constStride, n * m.constStride,
+                         cudaMemcpyHostToDevice, m.copy));
+    MTRY(cudaMemcpyAsync(m.dParams[s] + a, m.hParams[s] + a, n * sizeof(ElecParams), cudaMemcpyHostToDevice, m.copy));
+    m.upTo = nb;
+    return 0;
+}
+
 static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_t st)
 {
     if (nb == 0) return 0;
     m.nFlush++;
     const int s = m.slot;
-    MTRY(cudaStreamWaitEvent(m.copy, m.used[s], 0));
-    MTRY(cudaMemcpyAsync(m.dConst[s], m.hConst[s], (size_t)nb * m.constStride, cudaMemcpyHostToDevice, m.copy));
-    MTRY(cudaMemcpyAsync(m.dParams[s], m.hParams[s], (size_t)nb * sizeof(ElecParams), cudaMemcpyHostToDevice, m.copy));
+    int ru = upload_staged(m, nb);
+    if (ru) return ru;
     MTRY(cudaEventRecord(m.staged[s], m.copy));
     MTRY(cudaStreamWaitEvent(st, m.staged[s], 0));
     int r = 0;
@@ -406,6 +426,8 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
     MTRY(cudaEventRecord(m.used[s], st));
     m.nAdded += nb;
     m.slot ^= 1;
+    m.upTo = 0;
+    m.upWaited = false;
     MTRY(cudaEventSynchronize(m.staged[m.slot]));
     return 0;
 }
@@ -602,11 +624,14 @@ static int add_impl(srwgMultiE* m, int n, const double* arOffsets, int stride, v
 static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, cudaStream_t st)
 {
     int r = 0;
+    m->upTo = 0;                          // a batch abandoned by an error left nothing to keep
+    m->upWaited = false;
     std::vector<KernelDesc> first, launchKs;
     int nb = 0;
     // electrons are planned on host threads a group at a time (the planner keeps no shared state);
     // the GPU runs the previous batches meanwhile
-    const int group = std::max(m->maxBatch, 16);
+    // (groups of at most 64: each group's constants are uploaded while the next group is planned)
+    const int group = std::min(std::max(m->maxBatch, 16), 64);
     const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     std::vector<Planner> pls(group);
     std::vector<ElecParams> eps(group);
@@ -637,6 +662,10 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
         const int g = e % group;
         if (g == 0) {
             copy_pending();
+            if (nb > 0) {
+                r = upload_staged(*m, nb);
+                if (r) return r;
+            }
             const int cnt = std::min(group, n - e);
             auto work = [&](int t0) {
                 double momX[11], momY[11];

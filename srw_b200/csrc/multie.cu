@@ -380,16 +380,35 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
             if (a.kind == K_LINE && a.line.zwin && (a.line.zl0 < g.line.zl0 || a.line.zl1 > g.line.zl1)) fits = false;
         }
         if (!fits) {
-            if (m.graph[s]) { cudaGraphExecDestroy(m.graph[s]); m.graph[s] = nullptr; }
+            // the new graph's shapes cover this batch, the graph it replaces (so that the windows
+            // grow to what the electrons' distribution needs in a few captures; an instantiation
+            // costs milliseconds of host time) and headroom for other batches: larger tiles,
+            // windows wider by half of theirs
             std::vector<KernelDesc> cap = ks;
+            if (m.graph[s] && m.graphKs[s].size() == cap.size())
+                for (size_t i = 0; i < cap.size(); i++) {
+                    const KernelDesc& o = m.graphKs[s][i];
+                    if (cap[i].kind == K_RESIZE) {
+                        ResizeDesc& r = cap[i].rs;
+                        r.tile_or = std::max(r.tile_or, o.rs.tile_or);
+                        r.tile_oc = std::max(r.tile_oc, o.rs.tile_oc);
+                        r.ixStart = std::min(r.ixStart, o.rs.ixStart);
+                        r.ixEnd = std::max(r.ixEnd, o.rs.ixEnd);
+                        r.izStart = std::min(r.izStart, o.rs.izStart);
+                        r.izEnd = std::max(r.izEnd, o.rs.izEnd);
+                    } else if (cap[i].kind == K_LINE && cap[i].line.zwin) {
+                        cap[i].line.zl0 = std::min(cap[i].line.zl0, o.line.zl0);
+                        cap[i].line.zl1 = std::max(cap[i].line.zl1, o.line.zl1);
+                    }
+                }
+            if (m.graph[s]) { cudaGraphExecDestroy(m.graph[s]); m.graph[s] = nullptr; }
             for (size_t i = 0; i < cap.size(); i++) {
-                // headroom for other batches: larger tiles, windows wider by a quarter of theirs
                 if (cap[i].kind == K_RESIZE && cap[i].rs.tile_or > 0) {
                     ResizeDesc& r = cap[i].rs;
                     r.tile_or = std::min(SRWG_RESIZE_OR_MAX, r.tile_or + 2);
                     r.tile_oc = std::min(SRWG_RESIZE_OC_MAX, r.tile_oc + 2);
-                    const long mx = std::max(2L * SRWG_RESIZE_TX, (r.ixEnd - r.ixStart) / 4);
-                    const long mz = std::max(2L * SRWG_RESIZE_TZ, (r.izEnd - r.izStart) / 4);
+                    const long mx = std::max(2L * SRWG_RESIZE_TX, (r.ixEnd - r.ixStart) / 2);
+                    const long mz = std::max(2L * SRWG_RESIZE_TZ, (r.izEnd - r.izStart) / 2);
                     r.ixStart = std::max(0L, r.ixStart - mx);
                     r.ixEnd = std::min((long)r.nxn - 1, r.ixEnd + mx);
                     r.izStart = std::max(0L, r.izStart - mz);
@@ -398,7 +417,7 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
                 if (cap[i].kind == K_LINE && cap[i].line.zwin) {
                     LineDesc& d = cap[i].line;
                     const int nl = d.axis == 0 ? d.nz : d.nx;
-                    const int ml = std::max(64, (d.zl1 - d.zl0) / 4);
+                    const int ml = std::max(64, (d.zl1 - d.zl0) / 2);
                     d.zl0 = std::max(0, d.zl0 - ml);
                     d.zl1 = std::min(nl - 1, d.zl1 + ml);
                 }

@@ -383,7 +383,8 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
             // the new graph's shapes cover this batch, the graph it replaces (so that the windows
             // grow to what the electrons' distribution needs in a few captures; an instantiation
             // costs milliseconds of host time) and headroom for other batches: larger tiles,
-            // windows wider by half of theirs
+            // windows wider by a quarter of theirs (every CTA launched outside an electron's window
+            // costs a little)
             std::vector<KernelDesc> cap = ks;
             if (m.graph[s] && m.graphKs[s].size() == cap.size())
                 for (size_t i = 0; i < cap.size(); i++) {
@@ -407,8 +408,8 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
                     ResizeDesc& r = cap[i].rs;
                     r.tile_or = std::min(SRWG_RESIZE_OR_MAX, r.tile_or + 2);
                     r.tile_oc = std::min(SRWG_RESIZE_OC_MAX, r.tile_oc + 2);
-                    const long mx = std::max(2L * SRWG_RESIZE_TX, (r.ixEnd - r.ixStart) / 2);
-                    const long mz = std::max(2L * SRWG_RESIZE_TZ, (r.izEnd - r.izStart) / 2);
+                    const long mx = std::max(2L * SRWG_RESIZE_TX, (r.ixEnd - r.ixStart) / 4);
+                    const long mz = std::max(2L * SRWG_RESIZE_TZ, (r.izEnd - r.izStart) / 4);
                     r.ixStart = std::max(0L, r.ixStart - mx);
                     r.ixEnd = std::min((long)r.nxn - 1, r.ixEnd + mx);
                     r.izStart = std::max(0L, r.izStart - mz);
@@ -417,7 +418,7 @@ static int flush(srwgMultiE& m, int nb, std::vector<KernelDesc>& ks, cudaStream_
                 if (cap[i].kind == K_LINE && cap[i].line.zwin) {
                     LineDesc& d = cap[i].line;
                     const int nl = d.axis == 0 ? d.nz : d.nx;
-                    const int ml = std::max(64, (d.zl1 - d.zl0) / 2);
+                    const int ml = std::max(64, (d.zl1 - d.zl0) / 4);
                     d.zl0 = std::max(0, d.zl0 - ml);
                     d.zl1 = std::min(nl - 1, d.zl1 + ml);
                 }
@@ -649,8 +650,7 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
     int nb = 0;
     // electrons are planned on host threads a group at a time (the planner keeps no shared state);
     // the GPU runs the previous batches meanwhile
-    // (groups of at most 64: each group's constants are uploaded while the next group is planned)
-    const int group = std::min(std::max(m->maxBatch, 16), 64);
+    const int group = std::max(m->maxBatch, 16);
     const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     std::vector<Planner> pls(group);
     std::vector<ElecParams> eps(group);

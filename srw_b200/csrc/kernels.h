@@ -60,7 +60,7 @@ struct LineLaunch {
 
 // tiled resize: a CTA makes TZ x TX new points from an old tile of at most OR_MAX x OC_MAX points
 #define SRWG_RESIZE_TX 64
-#define SRWG_RESIZE_TZ 32
+#define SRWG_RESIZE_TZ 16
 #define SRWG_RESIZE_OR_MAX 40
 #define SRWG_RESIZE_OC_MAX 80
 

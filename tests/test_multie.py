@@ -223,3 +223,27 @@ def test_multie_intensity_pass_vs_oracle():
     want = oracle_sum(dict(ex=ex, ey=ey, mesh=mesh), sc, C1, pp, acc, offs) / 6
     assert np.abs(want).max() > 0
     assert rel_l2(got, want) < TOL
+
+
+@pytest.mark.gpu
+def test_multie_timed_batch_and_info():
+    """srwgMultiEAddTimed runs one batch with CUDA events around every pass (the electrons are added
+    as by srwgMultiEAdd: the same mean); srwgMultiEInfo lists the batch's passes as the plan API does
+    and tells whether the last one writes the intensity."""
+    _gpu()
+    from srw_b200.multie import MultiE
+    from srw_b200.plan import Plan
+    i, sc, el, pp, acc = base_case()
+    w = make_wfr(i['ex'], i['ey'], i['mesh'], **sc)
+    offs = sample_offsets(4, *SIG, seed=31, sig_e=1e-3)
+    a = MultiE(w, beamline(el, pp), acc, max_batch=4, graph=False)
+    ks, inten = a.info()
+    assert [k[0] for k in ks] == [k[0] for k in Plan(w, beamline(el, pp)).kernels() if k[0] != 'moments']
+    ms = a.add_timed(offs)
+    assert len(ms) == len(ks) + 1 and all(v > 0 for v in ms)
+    assert a.count() == 4
+    b = MultiE(w, beamline(el, pp), acc, max_batch=4, graph=False)
+    b.add(offs)
+    np.testing.assert_array_equal(a.mean(), b.mean())
+    with pytest.raises(RuntimeError):
+        a.add_timed(sample_offsets(5, *SIG, seed=32, sig_e=1e-3))      # more than one batch

@@ -50,14 +50,14 @@ SIG_E = 1e-3                                   # relative electron energy spread
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a pass, from an ncu
 # capture of this workload (the plain passes' summary under profiles/); keyed by the pass tuple of
 # Plan.kernels().  Re-captured whenever the kernel changes.
-TRAFFIC = {('line_cols', 4096, 4096): 37342208 + 216858624,
-           ('line_rows', 4096, 4096): 5258496 + 2020864,
-           ('resize', 1024, 1024, 4096, 4096): 1374976 + 0}
+TRAFFIC = {('line_cols', 4096, 4096): 37369856 + 216899840,
+           ('line_rows', 4096, 4096): 5258752 + 2144256,
+           ('resize', 1024, 1024, 4096, 4096): 1373696 + 512}
 # the same per electron of the batched passes at the learned factors (ncu on a batch of 8, the
 # learned batch's summary under profiles/); a launch moves this times its electrons
-TRAFFIC_PER_ELECTRON = {('line_cols', 1536, 1600): (69830400 + 31267840) // 8,
-                        ('line_rows', 1536, 1600): (19812864 + 21017344) // 8,
-                        ('resize', 1024, 1024, 1536, 1600): (2238208 + 34048) // 8}
+TRAFFIC_PER_ELECTRON = {('line_cols', 1536, 1600): (69851904 + 29201664) // 8,
+                        ('line_rows', 1536, 1600): (19814912 + 20619776) // 8,
+                        ('resize', 1024, 1024, 1536, 1600): (2238208 + 202240) // 8}
 
 
 # ------------------------------------------------------------------------------------------------

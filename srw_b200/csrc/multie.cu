@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -32,6 +33,7 @@
 #include "exec.h"
 #include "kernels.h"
 #include "planner.h"
+#include "workers.h"
 
 namespace srwg {
 
@@ -221,8 +223,10 @@ struct srwgMultiE {
     std::vector<KernelDesc> graphKs[2];  // host copy (launch shapes) each graph was captured with
     std::vector<cudaEvent_t> tev;        // srwgMultiEAddTimed: events around every pass and the accumulation
     long long nFlush = 0;                // batches run so far
+    std::unique_ptr<WorkerPool> pool;    // host threads planning the electrons and staging their constants
     ~srwgMultiE()
     {
+        pool.reset();
         for (cudaEvent_t e : tev) cudaEventDestroy(e);
         for (int i = 0; i < 2; i++)
             if (graph[i]) cudaGraphExecDestroy(graph[i]);
@@ -651,7 +655,8 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
     // electrons are planned on host threads a group at a time (the planner keeps no shared state);
     // the GPU runs the previous batches meanwhile
     const int group = std::max(m->maxBatch, 16);
-    const int nthr = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (!m->pool) m->pool.reset(new WorkerPool((int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()))));
+    const int nthr = m->pool->size();
     std::vector<Planner> pls(group);
     std::vector<ElecParams> eps(group);
     std::vector<int> rcs(group);
@@ -671,10 +676,7 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
                 memcpy(blk + m->descOff, q.kernels.data(), q.kernels.size() * sizeof(KernelDesc));
             }
         };
-        std::vector<std::thread> th;
-        for (int t = 1; t < std::min(nthr, (int)pending.size()); t++) th.emplace_back(cp, t);
-        cp(0);
-        for (auto& t : th) t.join();
+        m->pool->run(std::min(nthr, (int)pending.size()), cp);
         pending.clear();
     };
     for (int e = 0; e < n; e++) {
@@ -703,10 +705,7 @@ static int add_body(srwgMultiE* m, int n, const double* arOffsets, int stride, c
                     if (!rcs[k]) mark_intensity_pass(pls[k].kernels, pls[k].tables);
                 }
             };
-            std::vector<std::thread> th;
-            for (int t = 1; t < std::min(nthr, cnt); t++) th.emplace_back(work, t);
-            work(0);
-            for (auto& t : th) t.join();
+            m->pool->run(std::min(nthr, cnt), work);
         }
         Planner& pl = pls[g];
         ElecParams& ep = eps[g];

@@ -723,7 +723,7 @@ class CheckedMultiE(object):
     ``mean()`` divides by the electrons added."""
 
     def __init__(self, base_wfr, make_beamline, factors, acc_mesh, max_batch=64, safe_batch=16, graph=True,
-                 device=0, tol=TOL_LABEL, check_offsets=None):
+                 device=0, tol=TOL_LABEL, check_offsets=None, launch_batch=None):
         import torch
         from .multie import MultiE, offset_array
         self.torch = torch
@@ -731,7 +731,10 @@ class CheckedMultiE(object):
         self.acc = torch.zeros((acc_mesh['ny'], acc_mesh['nx']), dtype=torch.float64, device=self.dev)
         self.chk = [torch.zeros_like(self.acc), torch.zeros_like(self.acc)]
         self.learned = tuple(factors) != tuple(CONSERVATIVE)
-        self.fast = MultiE(base_wfr, make_beamline(factors), acc_mesh, max_batch=max_batch, graph=graph, device=device)
+        # a checked batch of max_batch electrons runs as launches of launch_batch electrons (default: one
+        # launch), so that the device starts on the first launch while the host plans the next
+        self.fast = MultiE(base_wfr, make_beamline(factors), acc_mesh, max_batch=launch_batch or max_batch,
+                           graph=graph, device=device)
         self.safe = MultiE(base_wfr, make_beamline(CONSERVATIVE), acc_mesh, max_batch=safe_batch, graph=graph,
                            device=device)
         self.fast.use_accumulator(self.acc.data_ptr())
@@ -746,6 +749,9 @@ class CheckedMultiE(object):
         self.check0 = None if check_offsets is None else offset_array(check_offsets)
         self.max_batch, self.tol = max_batch, tol
         self._host = torch.empty(2, dtype=torch.float64, pin_memory=True)
+        # the batches, the checks and the fallback run on this stream when the caller gives none, so
+        # that the host plans the next batch while the device runs the last one
+        self._stream = torch.cuda.Stream(self.dev)
         self._start()
 
     def _start(self):
@@ -754,6 +760,7 @@ class CheckedMultiE(object):
         self._pending = None
         for c in self.chk:
             c.zero_()
+        self.torch.cuda.synchronize(self.dev)      # the sums are zero before any stream adds to them
         if self.learned and self.check0 is not None and len(self.check0):
             self.cfast.add(self.check0)
             self.csafe.add(self.check0)
@@ -786,25 +793,23 @@ class CheckedMultiE(object):
 
     def _fall_back(self, stream):
         self.fell_back = True
-        self.acc.zero_()
-        if stream is None:
-            self.torch.cuda.synchronize(self.dev)      # the library's own stream adds next
+        self.acc.zero_()                               # on `stream` (the caller's context)
         for b in self.added_fast:
             self.safe.add(b, stream)
             self.rerun += len(b)
         self.added_fast = []
 
     def _ctx(self, stream):
-        import contextlib
         torch = self.torch
-        return torch.cuda.stream(torch.cuda.ExternalStream(stream, device=self.dev)) if stream else \
-            contextlib.nullcontext()
+        return torch.cuda.stream(torch.cuda.ExternalStream(stream, device=self.dev))
 
     def add(self, offsets, stream=None):
         """Adds the electrons (offsets as MultiE.add) in batches of max_batch, each with its check.
-        `stream`: a CUDA stream handle; the checks' reductions run on it too."""
+        `stream`: a CUDA stream handle (default: the object's own stream); the checks' reductions run
+        on it too.  The work is queued, not waited for: ``mean()`` waits."""
         from .multie import offset_array
         off = offset_array(offsets)
+        stream = stream or self._stream.cuda_stream
         with self._ctx(stream):
             for i0 in range(0, len(off), self.max_batch):
                 b = off[i0:i0 + self.max_batch]
@@ -824,6 +829,7 @@ class CheckedMultiE(object):
 
     def resolve(self, stream=None):
         """Reads the last queued check (falling back if it fails); mean() calls it."""
+        stream = stream or self._stream.cuda_stream
         with self._ctx(stream):
             self._resolve(stream)
 

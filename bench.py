@@ -618,6 +618,7 @@ def measure_mixed(args, dev, n_elec, model=None):
 
 
 LEARNED_BATCH = 256              # macro-electron wavefronts per step of the learned leg (one checked batch)
+LEARNED_LAUNCH = 64              # electrons per launch inside it (the device starts while the host plans the rest)
 N_CHECK = 32                     # electrons of the learned factors' check set
 REFINE = 4                       # checks spent lowering the resolution of a passing choice
 
@@ -635,8 +636,8 @@ def measure_learned(args, dev, world, dist, acc):
     """Batched path with the resize factors the trained network chooses for this wavefront and
     beamline (srw_b200.learned.choose_factors: the mean intensity of a seeded check set of N_CHECK
     electrons propagated with them checked against the conservative factors', fallback above 1e-3),
-    run through learned.CheckedMultiE: batches of LEARNED_BATCH electrons, the first electron of every
-    batch added to the check set at both factors and the check repeated before the batch (above 1e-3
+    run through learned.CheckedMultiE: batches of LEARNED_BATCH electrons (launched LEARNED_LAUNCH at a
+    time), the first electron of every batch added to the check set at both factors and the check repeated before the batch (above 1e-3
     the run falls back to the conservative factors for good).  K steps between CUDA events, checks
     included."""
     import torch
@@ -655,7 +656,7 @@ def measure_learned(args, dev, world, dist, acc):
     choose_s = time.perf_counter() - t0
     w = make_wfr(mod, ex, ey, mesh, sc)
     cm = learned.CheckedMultiE(w, lambda f: beamline_objs(mod, f), factors, acc, max_batch=LEARNED_BATCH,
-                               graph=True, device=dev.index, check_offsets=chk_set)
+                               graph=True, device=dev.index, check_offsets=chk_set, launch_batch=LEARNED_LAUNCH)
     stream = torch.cuda.Stream(dev)
     rank = int(os.environ.get('RANK', '0'))
     for k in range(args.warmup):
@@ -695,15 +696,16 @@ def measure_learned(args, dev, world, dist, acc):
                        "offsets from host, the run-time check included) + CheckedMultiE.mean (D2H of the %dx%d FP64 "
                        "mean intensity)" % (acc['nx'], acc['ny'])}
     peak, peak_src = hbm_peak()
-    passes = batched_passes(cm.safe if cm.fell_back else cm.fast, offs[0], stream.cuda_stream, peak, peak_src,
-                            "learned leg, one batch of %d electrons, CUDA events per pass" % LEARNED_BATCH)
+    passes = batched_passes(cm.safe if cm.fell_back else cm.fast, offs[0][:LEARNED_LAUNCH], stream.cuda_stream, peak,
+                            peak_src, "learned leg, one launch of %d electrons, CUDA events per pass" % LEARNED_LAUNCH)
     from srw_b200.plan import Plan
     nk_f = Plan(w, beamline_objs(mod, factors), device=dev.index).n_kernels
     nk_c = Plan(w, beamline_objs(mod), device=dev.index).n_kernels
     return {"value": value, "unit": UNIT, "ms_per_step": total_ms / args.steps, "batch": LEARNED_BATCH,
-            # per step: the batch and the checked electron (kick, passes, accumulation each), and the
-            # checked electron with the conservative factors
-            "launches_per_step": 2 * (nk_f + 2) + (nk_c + 2),
+            # per step: the batch's launches and the checked electron (kick, passes, accumulation each),
+            # and the checked electron with the conservative factors
+            "launches_per_step": (LEARNED_BATCH // LEARNED_LAUNCH + 1) * (nk_f + 2) + (nk_c + 2),
+            "launch_batch": LEARNED_LAUNCH,
             "factors": list(factors), "configured_factors": list(CONFIGURED),
             "fallback": bool(fallback or fell_back),
             "choice_check_rel_err": chk, "choose_seconds": choose_s,
@@ -869,10 +871,10 @@ def run_ours(args, rank, world):
            "config": {"workload": WORKLOAD, "step": "one batch of %d macro-electron wavefronts (1024^2 field with "
                                                     "its electron's source offset) through the beamline, intensities "
                                                     "added on the device%s" % (
-                                                        step_batch, ", learned factors %s, the mean intensity "
-                                                        "of the check set checked against the configured factors "
-                                                        "before the batch"
-                                                        % (ln['factors'],) if use_learned else ""),
+                                                        step_batch, ", learned factors %s, launched %d electrons "
+                                                        "at a time, the mean intensity of the check set checked "
+                                                        "against the configured factors before the batch"
+                                                        % (ln['factors'], LEARNED_LAUNCH) if use_learned else ""),
                       "grid_in": [1024, 1024], "grid_out": [plan.nx_out, plan.ny_out],
                       "passes": plan.n_kernels, "algorithmic_bytes_per_propagation": total_alg,
                       "pass_bytes_per_propagation": pass_bytes,

@@ -247,4 +247,14 @@ def test_checked_multie_falls_back_and_rebuilds():
     late.add(offs[16:])
     np.testing.assert_allclose(late.mean(), m_cons, rtol=1e-12, atol=0)
     assert late.fell_back and late.rerun == 16
+    # a checked batch of 8 run as launches of 4: the same electrons and checks, the sums in another order
+    split = learned.CheckedMultiE(w, mk, fac, acc, tol=1.0, launch_batch=4, **kw)
+    split.add(offs)
+    np.testing.assert_allclose(split.mean(), m_fast, rtol=1e-10, atol=0)
+    assert not split.fell_back and len(split.check_errors) == 3
+    np.testing.assert_allclose(split.check_errors, ok.check_errors, rtol=1e-12)
+    split_fb = learned.CheckedMultiE(w, mk, fac, acc, tol=-1.0, launch_batch=4, **kw)
+    split_fb.add(offs)
+    np.testing.assert_allclose(split_fb.mean(), m_cons, rtol=1e-12, atol=0)
+    assert split_fb.fell_back and split_fb.rerun == 8
     assert np.linalg.norm(m_fast - m_cons) > 0

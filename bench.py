@@ -578,9 +578,10 @@ def measure_mixed(args, dev, n_elec, model=None):
             b = batch or {256: 32, 512: 32, 1024: 16}[n]
             if mode == 'learned':
                 # the mean intensity of the check set (grown by one electron per batch) checked before every batch
-                me = learned.CheckedMultiE(w, lambda f: beamline_objs(mod, f), factors, acc, max_batch=64,
-                                           graph=graph, device=dev.index, check_offsets=chk_set)
-                me.add(sample_offsets(64, *SIG, seed=999, sig_e=SIG_E))                 # warm-up (plans, graph)
+                me = learned.CheckedMultiE(w, lambda f: beamline_objs(mod, f), factors, acc,
+                                           max_batch=LEARNED_BATCH, launch_batch=LEARNED_LAUNCH, graph=graph,
+                                           device=dev.index, check_offsets=chk_set)
+                me.add(sample_offsets(LEARNED_LAUNCH, *SIG, seed=999, sig_e=SIG_E))     # warm-up (plans, graph)
                 me.reset()
             else:
                 me = MultiE(w, bl, acc, max_batch=b, graph=graph, device=dev.index)
@@ -608,8 +609,8 @@ def measure_mixed(args, dev, n_elec, model=None):
            "note": "each electron: offset field, C1 beamline (resize before the lens), intensity added in FP64 "
                    "onto a 512x512 common mesh; plain = the same electrons one per launch sequence with the "
                    "configured factors (2, 2); learned = per grid class the network's factors (checked on the mean "
-                   "intensity of a 16-electron check set), batches of 64, the first electron of every batch added "
-                   "to the check set at both factors and the check repeated"}
+                   "intensity of a 32-electron check set), checked batches of 256 launched 64 at a time, the first "
+                   "electron of every batch added to the check set at both factors and the check repeated"}
     if model is not None:
         out.update({"batched_learned": res['learned'], "learned_speedup_vs_plain": res['learned'] / res['plain'],
                     "learned_factors": {str(k): v for k, v in facs.items()},

@@ -173,7 +173,8 @@ def test_trained_model_gain_over_conservative_factors():
     t_fac, t_con, errs, n_fallback = 0., 0., [], 0
 
     def timed(case, fac):
-        # the propagation's device time: planned once, field resident, three executions between events
+        # the propagation's device time: planned once, field resident, the passes' CUDA-event times
+        # (no host gaps between launches) summed, best of three executions
         from srw_b200 import srwlib as mod
         from srw_b200.plan import Plan
         p = Plan(learned._wfr(mod, case),
@@ -182,14 +183,9 @@ def test_trained_model_gain_over_conservative_factors():
         ox, oy = p.new_output()
         p.execute(ex, ey, ox, oy)                                       # warm-up
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(3):
-            p.execute(ex, ey, ox, oy)
-        e1.record()
-        torch.cuda.synchronize()
+        t = min(sum(p.execute_timed(ex, ey, ox, oy)) for _ in range(3))
         I, om = learned.propagate_intensity(case, fac, dev)
-        return I, om, e0.elapsed_time(e1) / 3.
+        return I, om, t
 
     for _ in range(16):
         case = learned.sample_case(rng)

@@ -910,6 +910,10 @@ def run_ours(args, rank, world):
            "mixed_grid_multi_electron": mixed,
            "clocks": (ln['clocks'] if use_learned and ln.get('clocks') else bt['clocks']),
            "gpu_launches": (ln['launches_per_step'] if use_learned else plan.n_kernels + 2) * args.steps}
+    from srw_b200 import tune
+    out["tuning"] = {"table": os.environ.get('SRWG_TUNING', os.path.relpath(tune.TXT, HERE)),
+                     "headline": tune.pass_shapes(ln['passes']['passes']) if use_learned else None,
+                     "plain": tune.pass_shapes(plan.kernels())}
     print(json.dumps(out))
 
 

@@ -66,6 +66,29 @@ def families(n):
     return [FAM_SPEC]
 
 
+def launch_shape(axis, n):
+    """(kernel family name, lines per CTA) the library uses for a line pass of n points along axis 0
+    (rows) or 1 (columns): the tuning table's entry, else its defaults; (None, 0) for lengths that
+    run the run-time-scheduled pass."""
+    L = capi.lib()
+    fam, lines = C.c_int(), C.c_int()
+    capi.check(L.srwgTuneGetFamily(int(axis), int(n), C.byref(fam)), 'tune family')
+    capi.check(L.srwgTuneGetLines(int(axis), int(n), C.byref(lines)), 'tune lines')
+    name = {FAM_POW2: 'pow2', FAM_SPEC: 'spec'}.get(fam.value)
+    return name, (lines.value if name else 0)
+
+
+def pass_shapes(passes):
+    """Launch shapes of the line passes of a plan (Plan.kernels() / MultiE.info() tuples)."""
+    out = []
+    for k in passes:
+        if k[0] in ('line_rows', 'line_cols'):
+            axis = 0 if k[0] == 'line_rows' else 1
+            fam, lines = launch_shape(axis, k[1] if axis == 0 else k[2])
+            out.append({"pass": "%s %dx%d" % (k[0], k[1], k[2]), "family": fam, "lines_per_cta": lines})
+    return out
+
+
 def candidates(axis, n, fam=None):
     """Valid (family, lines per CTA) pairs (the library's fixed_lines_valid): shared memory, threads
     per CTA (1024 for the power-of-two pass, 512 for the specialised one), columns a power of two up

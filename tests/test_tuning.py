@@ -52,6 +52,27 @@ def test_tuning_entry_points_validate():
     assert L.srwgTuneLoad(tune.TXT.encode() if os.path.exists(tune.TXT) else None, C.byref(n)) == 0
 
 
+def test_pass_shapes_report_the_table():
+    """tune.pass_shapes (the bench's record of the launch shapes) reports the family and lines per
+    CTA of the packaged table's entries, valid shapes for every line pass, nothing for other passes."""
+    L = capi.lib()
+    n = C.c_int()
+    assert L.srwgTuneLoad(tune.TXT.encode() if os.path.exists(tune.TXT) else None, C.byref(n)) == 0
+    passes = [('resize', 1024, 1024, 1536, 1600), ('line_rows', 1536, 1600), ('line_cols', 1536, 1600),
+              ('line_rows', 4096, 4096), ('line_cols', 4096, 4096)]
+    got = tune.pass_shapes(passes)
+    assert [g['pass'] for g in got] == ['line_rows 1536x1600', 'line_cols 1536x1600', 'line_rows 4096x4096',
+                                        'line_cols 4096x4096']
+    entries = {(axis, m): (lines, fam) for axis, m, lines, fam in table()}
+    for g, (kind, nx, nz) in zip(got, passes[1:]):
+        axis = 0 if kind == 'line_rows' else 1
+        m = nx if axis == 0 else nz
+        fam = tune.FAM_POW2 if g['family'] == 'pow2' else tune.FAM_SPEC
+        assert g['lines_per_cta'] in tune.candidates(axis, m, fam), g
+        if (axis, m) in entries:
+            assert (g['lines_per_cta'], fam) == entries[(axis, m)], g
+
+
 @pytest.mark.gpu
 def test_tuned_shapes_give_identical_fields():
     torch = pytest.importorskip('torch')

@@ -675,7 +675,7 @@ def measure_learned(args, dev, world, dist, acc):
         e0.record(stream)
         for k in range(args.steps):
             cm.add(offs[k], stream.cuda_stream)
-        cm.resolve(stream.cuda_stream)              # the last batch's check (a failure reruns inside the timing)
+        cm.resolve(stream.cuda_stream)              # the last checks (a failure reruns inside the timing)
         e1.record(stream)
         torch.cuda.synchronize(dev)
     total_ms = _max_over_ranks(e0.elapsed_time(e1), dev, world, dist)
@@ -717,10 +717,11 @@ def measure_learned(args, dev, world, dist, acc):
             "run_checks": {"batches": len(ce), "fell_back": bool(fell_back), "rerun_electrons": rerun,
                            "check_electrons": n_check, "max_rel_err": max(ce) if ce else None,
                            "last_rel_err": ce[-1] if ce else None,
-                           "what": "before every batch: the check set (the choice's electrons plus the first "
-                                   "electron of every batch so far) at both factors, relative L2 of the two mean "
-                                   "intensities; above the tolerance the run falls back to the conservative factors "
-                                   "for good and propagates the learned batches again"},
+                           "what": "with every batch, queued behind it: the check set (the choice's electrons plus "
+                                   "the first electron of every batch so far) at both factors, relative L2 of the two "
+                                   "mean intensities, read when the batch after next is queued; above the tolerance "
+                                   "the run falls back to the conservative factors for good and propagates the "
+                                   "learned batches again"},
             "clocks": nv.summary(), "passes": passes, "e2e": e2e,
             "model": {k: v for k, v in getattr(model, 'meta', {}).items()
                       if k in ('samples', 'val_grid_at_least_label', 'val_cost_pred', 'labels_conservative', 'tol')}}

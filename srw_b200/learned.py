@@ -716,10 +716,11 @@ class CheckedMultiE(object):
     conservative factors into two FP64 sums on the detector mesh: the electrons `check_offsets`
     given at construction (those of choose_factors' check), then the first electron of every batch.
     With every batch the relative L2 of the two sums (where the conservative one exceeds 1e-3 of its
-    maximum) is queued on the stream; it is read before the next batch is queued, or by ``mean()``,
-    so the host never waits for the batch it has just queued.  Above `tol` the run falls back for
-    good: every electron added so far with the learned factors (the checked batch included) is
-    propagated again with the conservative ones (the sum is rebuilt), and so are all later batches.
+    maximum) is queued on the stream behind the batch; it is read before the batch after next is
+    queued, or by ``mean()``, so the host never waits for the batch it has just queued.  Above `tol`
+    the run falls back for good: every electron added so far with the learned factors (the checked
+    batch and the one after it included) is propagated again with the conservative ones (the sum is
+    rebuilt), and so are all later batches.
     ``mean()`` divides by the electrons added."""
 
     def __init__(self, base_wfr, make_beamline, factors, acc_mesh, max_batch=64, safe_batch=16, graph=True,
@@ -748,7 +749,9 @@ class CheckedMultiE(object):
             self.csafe.use_accumulator(self.chk[1].data_ptr())
         self.check0 = None if check_offsets is None else offset_array(check_offsets)
         self.max_batch, self.tol = max_batch, tol
-        self._host = torch.empty(2, dtype=torch.float64, pin_memory=True)
+        # pinned read-back slots of the queued checks (at most two are in flight: see add)
+        self._hosts = [torch.empty(2, dtype=torch.float64, pin_memory=True) for _ in range(3)]
+        self._next_host = 0
         # the batches, the checks and the fallback run on this stream when the caller gives none, so
         # that the host plans the next batch while the device runs the last one
         self._stream = torch.cuda.Stream(self.dev)
@@ -757,7 +760,7 @@ class CheckedMultiE(object):
     def _start(self):
         self.n, self.n_check, self.batches, self.check_errors = 0, 0, 0, []
         self.fell_back, self.rerun, self.added_fast = False, 0, []
-        self._pending = None
+        self._pending = []                         # queued checks, oldest first: (event, host slot)
         for c in self.chk:
             c.zero_()
         self.torch.cuda.synchronize(self.dev)      # the sums are zero before any stream adds to them
@@ -774,22 +777,26 @@ class CheckedMultiE(object):
         zero = torch.zeros((), dtype=ref.dtype, device=ref.device)
         num = torch.linalg.norm(torch.where(sel, a - ref, zero))
         den = torch.linalg.norm(torch.where(sel, ref, zero))
-        self._host.copy_(torch.stack([num, den]), non_blocking=True)
+        host = self._hosts[self._next_host]
+        self._next_host = (self._next_host + 1) % len(self._hosts)
+        host.copy_(torch.stack([num, den]), non_blocking=True)
         ev = torch.cuda.Event()
         ev.record()
-        self._pending = ev
+        self._pending.append((ev, host))
 
-    def _resolve(self, stream):
-        """Reads the queued check; above the tolerance, falls back."""
-        if self._pending is None:
-            return
-        self._pending.synchronize()
-        self._pending = None
-        num, den = float(self._host[0]), float(self._host[1])
-        e = num / den if den > 0. else float('inf')
-        self.check_errors.append(e)
-        if e > self.tol:
-            self._fall_back(stream)
+    def _resolve(self, stream, keep=0):
+        """Reads the queued checks but the `keep` newest, oldest first; above the tolerance, falls back
+        (the checks still queued then no longer matter)."""
+        while len(self._pending) > keep:
+            ev, host = self._pending.pop(0)
+            ev.synchronize()
+            num, den = float(host[0]), float(host[1])
+            e = num / den if den > 0. else float('inf')
+            self.check_errors.append(e)
+            if e > self.tol:
+                self._pending = []
+                self._fall_back(stream)
+                return
 
     def _fall_back(self, stream):
         self.fell_back = True
@@ -813,22 +820,26 @@ class CheckedMultiE(object):
         with self._ctx(stream):
             for i0 in range(0, len(off), self.max_batch):
                 b = off[i0:i0 + self.max_batch]
+                # the check of the batch before last (queued behind that batch) is read: the host
+                # then plans this batch while the device still runs the last one
                 if self.learned and not self.fell_back:
-                    self._resolve(stream)
+                    self._resolve(stream, keep=1)
                 if self.learned and not self.fell_back:
+                    # the batch first (the device starts on it while the host plans the check
+                    # electrons), then its check electron at both factors and the check
+                    self.fast.add(b, stream)
+                    self.added_fast.append(b)
                     self.cfast.add(b[:1], stream)
                     self.csafe.add(b[:1], stream)
                     self.n_check += 1
                     self._queue_check()
-                    self.fast.add(b, stream)
-                    self.added_fast.append(b)
                 else:
                     self.safe.add(b, stream)
                 self.batches += 1
                 self.n += len(b)
 
     def resolve(self, stream=None):
-        """Reads the last queued check (falling back if it fails); mean() calls it."""
+        """Reads the queued checks (falling back if one fails); mean() calls it."""
         stream = stream or self._stream.cuda_stream
         with self._ctx(stream):
             self._resolve(stream)

@@ -214,10 +214,10 @@ def test_trained_model_gain_over_conservative_factors():
 def test_checked_multie_falls_back_and_rebuilds():
     """learned.CheckedMultiE: a check that every batch meets gives the learned factors' mean
     intensity, its errors those of the check set's two mean intensities; a check that fails at the
-    first batch gives the conservative factors' mean (the first batch, checked while it ran, is
-    propagated again); a check that fails after two batches propagates those two again with the
-    conservative factors, so the result is again the conservative factors' mean of all electrons
-    (same batches, FP64 sums)."""
+    first batch gives the conservative factors' mean (the first batch and the one queued after it,
+    both run before the check was read, are propagated again); a check that fails after two batches
+    propagates those two again with the conservative factors, so the result is again the
+    conservative factors' mean of all electrons (same batches, FP64 sums)."""
     torch = _torch()
     from srw_b200 import srwlib as mod
     from srw_b200.multie import MultiE, sample_offsets
@@ -250,7 +250,7 @@ def test_checked_multie_falls_back_and_rebuilds():
     first = learned.CheckedMultiE(w, mk, fac, acc, tol=-1.0, **kw)
     first.add(offs)
     np.testing.assert_allclose(first.mean(), m_cons, rtol=1e-12, atol=0)
-    assert first.fell_back and first.rerun == 8 and len(first.check_errors) == 1
+    assert first.fell_back and first.rerun == 16 and len(first.check_errors) == 1
     late = learned.CheckedMultiE(w, mk, fac, acc, tol=1.0, **kw)
     late.add(offs[:16])
     late.tol = -1.0
@@ -266,5 +266,5 @@ def test_checked_multie_falls_back_and_rebuilds():
     split_fb = learned.CheckedMultiE(w, mk, fac, acc, tol=-1.0, launch_batch=4, **kw)
     split_fb.add(offs)
     np.testing.assert_allclose(split_fb.mean(), m_cons, rtol=1e-12, atol=0)
-    assert split_fb.fell_back and split_fb.rerun == 8
+    assert split_fb.fell_back and split_fb.rerun == 16
     assert np.linalg.norm(m_fast - m_cons) > 0

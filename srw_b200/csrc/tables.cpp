@@ -98,6 +98,10 @@ static void separate(const PwOps& pw, int axis, int nAlong, int nLine, SepPart& 
 // swaps and signs them.  Phases beyond 2^20 pi/2 (1.6e6 rad) and non-finite ones go to the C
 // library.  The loop has no branches, so that the compiler vectorises it; the tables of a plan hold
 // about ten thousand factors, and the C library's sincos was two thirds of the planning time.
+// Compiled for AVX2 as well (chosen at load time where the CPU has it; the same operations, so the
+// same results), with the vectoriser's full cost model (the cheap one at -O2 leaves the loop scalar:
+// 9 ns per value instead of 4).  The values go to separate cosine and sine arrays first.
+__attribute__((target_clones("avx2", "default"), optimize("vect-cost-model=dynamic", "fp-contract=off")))
 static void cis_n(const double* ph, cd* out, int n)
 {
     const double P1 = 0x1.921fb544p+0, P2 = 0x1.0b4611a6p-34, P3 = 0x1.3198a2e037073p-69;
@@ -107,7 +111,10 @@ static void cis_n(const double* ph, cd* out, int n)
                  s13 = 1. / 6227020800., s15 = -1. / 1307674368000.;
     const double c2 = -0.5, c4 = 1. / 24., c6 = -1. / 720., c8 = 1. / 40320., c10 = -1. / 3628800.,
                  c12 = 1. / 479001600., c14 = -1. / 87178291200., c16 = 1. / 20922789888000.;
-    std::vector<double> re(n), im(n);
+    thread_local std::vector<double> re, im;        // scratch of the calling planner thread
+    if ((int)re.size() < n) { re.resize(n); im.resize(n); }
+    double* __restrict__ pr = re.data();
+    double* __restrict__ pi = im.data();
     for (int i = 0; i < n; i++) {
         const double x = ph[i];
         const double k = (x * TWO_OVER_PI + RND) - RND;
@@ -118,24 +125,26 @@ static void cis_n(const double* ph, cd* out, int n)
             1. + r2 * (c2 + r2 * (c4 + r2 * (c6 + r2 * (c8 + r2 * (c10 + r2 * (c12 + r2 * (c14 + r2 * c16)))))));
         const int q = (int)k & 3;
         const double a = (q & 1) ? cs : sn, b = (q & 1) ? sn : cs;     // sin x, cos x up to signs
-        im[i] = (q & 2) ? -a : a;
-        re[i] = ((q + 1) & 2) ? -b : b;
+        pi[i] = (q & 2) ? -a : a;
+        pr[i] = ((q + 1) & 2) ? -b : b;
     }
     for (int i = 0; i < n; i++) {
         if (!(std::fabs(ph[i]) < 1.6e6)) {
             double sn, cs;
             ::sincos(ph[i], &sn, &cs);
-            re[i] = cs;
-            im[i] = sn;
+            pr[i] = cs;
+            pi[i] = sn;
         }
-        out[i] = cd(re[i], im[i]);
+        out[i] = cd(pr[i], pi[i]);
     }
 }
 
 static long long push(std::vector<float2>& T, const std::vector<cd>& v)
 {
-    long long off = (long long)T.size();
-    for (const cd& c : v) { float2 f; f.x = (float)c.real(); f.y = (float)c.imag(); T.push_back(f); }
+    const long long off = (long long)T.size();
+    T.resize(T.size() + v.size());
+    float2* d = T.data() + off;
+    for (size_t i = 0; i < v.size(); i++) { d[i].x = (float)v[i].real(); d[i].y = (float)v[i].imag(); }
     return off;
 }
 
@@ -168,7 +177,13 @@ static ChainTab chain_table(std::vector<float2>& T, int N, int nLine, int rs1, i
             sg[k] = g;
         }
         cis_n(ph.data(), v.data(), N);
-        for (int k = 0; k < N; k++) v[k] = z[k] ? cd(0., 0.) : (sg[k] * (double)sc1) * scale * v[k];
+        for (int k = 0; k < N; k++) {
+            // (sg sc1 scale) v, the complex product written out (std::complex's operator* goes through
+            // a library call that also handles infinities and NaNs: none arise here)
+            const cd f = (sg[k] * (double)sc1) * scale;
+            const double vr = v[k].real(), vi = v[k].imag();
+            v[k] = z[k] ? cd(0., 0.) : cd(f.real() * vr - f.imag() * vi, f.real() * vi + f.imag() * vr);
+        }
         ct.tab = push(T, v);
     }
     if (Lp && Lp->any) {

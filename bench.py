@@ -685,7 +685,10 @@ def measure_learned(args, dev, world, dist, acc):
     # end to end through the public API: host offsets in, the mean intensity (host) out, every step
     e2e = None
     if not args.no_e2e:
-        n_e2e = max(3, min(args.steps, 10))
+        for k in range(max(1, args.warmup)):     # untimed: the object's own stream and its buffers
+            cm.add(sample_offsets(LEARNED_BATCH, *SIG, seed=3000 + rank, first=k * LEARNED_BATCH, sig_e=SIG_E))
+            cm.mean()
+        n_e2e = max(3, min(args.steps, 20))
         t0 = time.perf_counter()
         for k in range(n_e2e):
             cm.add(offs[k % len(offs)])

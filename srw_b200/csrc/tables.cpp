@@ -264,6 +264,15 @@ static int tile_extent(const std::vector<float2>& T, long long off, int nNew, lo
 void build_tables(std::vector<KernelDesc>& ks, std::vector<float2>& T)
 {
     T.clear();
+    // room for the largest tables the passes can ask for (no reallocation while they are added)
+    size_t most = 0;
+    for (const KernelDesc& k : ks) {
+        if (k.kind == K_LINE) most += 3 * (size_t)(k.line.nx + k.line.nz);
+        else if (k.kind == K_RESIZE) most += 4 * (size_t)(k.rs.nxn + k.rs.nzn) + 2 * (size_t)(k.rs.nxo + k.rs.nzo) + 2;
+        else if (reads_only(k.kind)) most += (size_t)(k.mom.nx + k.mom.nz);
+        else most += (size_t)(k.pwk.nx + k.pwk.nz);
+    }
+    T.reserve(most);
     for (KernelDesc& k : ks) {
         if (k.kind == K_LINE) {
             LineDesc& d = k.line;
